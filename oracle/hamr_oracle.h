@@ -1,0 +1,72 @@
+/*
+ * Test infrastructure (oracle) -- never product code.
+ *
+ * CPU restatement of H-AMR's single-block RK2 sub-step (the `advance_GPU`
+ * pipeline, step_ch.c:997-1335) in plain C99 with runtime grid sizes. Only the
+ * tests, the smoke check and the bench's CPU-baseline leg call it; the CUDA
+ * product never links it.
+ *
+ * Layout (identical to the reference device layout and to the product):
+ *   cell arrays   plane k of ksize doubles, cell (i, j, z) at (i*G2 + j)*G3 + z,
+ *                 G1 = n1 + 2*ng, G2 = n2 + 2*ng, G3 = n3 + 2*ng (G3 = 1, no
+ *                 ghosts, when n3 == 1)           GPU_program1.cu:90-94
+ *   face B (ps)   3 planes, plane d-1 holds B^d on the lower d-face
+ *   metric        gcov/gcon: plane (s*5 + loc), gdet: plane loc, conn: plane
+ *                 (s*4 + l), all indexed (i*G2 + j)   GPU_main.cu:139-300
+ */
+#ifndef HAMR_ORACLE_H
+#define HAMR_ORACLE_H
+
+#define HO_NPR 9
+
+enum { HO_BC_PERIODIC = 0, HO_BC_OUTFLOW = 1, HO_BC_POLE_TRANS = 2, HO_BC_POLE_REFL = 3 };
+
+typedef struct {
+    int n1, n2, n3;      /* active cells */
+    int ng;              /* ghost layers (3 for PPM) */
+    long ksize, gsize;   /* plane strides: cell arrays, metric tables */
+    double dx1, dx2, dx3;
+    double gam;          /* adiabatic index */
+    double cour;         /* Courant factor */
+    int pole1, pole2;    /* lower/upper x2 edge is a polar axis (GPU_main.cu:566) */
+    int bc1, bc2, bc3;   /* HO_BC_* per direction */
+    int inversion;       /* 0: Noble 2D (default); 1: Newman-Hamlin */
+    int ct_upwind;       /* 1: upwinded edge-EMF corrections; 0: plain average of
+                            the four face EMFs (the reference's CARTESIAN build,
+                            GPU_const_trans.h:187-211) */
+} ho_grid;
+
+typedef struct {
+    const double *gcov, *gcon, *gdet, *conn;
+} ho_geom;
+
+typedef struct {
+    double *p, *ph, *ps, *psh;   /* primitives and face B at t^n / half step */
+    double *U;                   /* conserved U(p^n), NPR planes (storage2) */
+    double *F1, *F2, *F3;        /* face fluxes, NPR planes each */
+    double *E_cent, *emf;        /* 4 planes each (index 1..3 used) */
+    int *pflag, *failimage;      /* failimage: 4 planes of ksize ints */
+} ho_state;
+
+/* One sub-step: full == 0 advances (p, ps) by Dt into (ph, psh), caching U(p);
+ * full == 1 advances the cached U by Dt with fluxes of (ph, psh) into (p, ps).
+ * dt is the step's dt (pole EMF averaging scales by it). With calc_dt != 0 the
+ * directional CFL limits are returned in dtdir[1..3]. */
+void ho_stage(const ho_grid *g, const ho_geom *m, ho_state *s, int full,
+              double Dt, double dt, int calc_dt, double *dtdir);
+
+/* Ghost fill of (pv, ps) for the boundary types in g (direction 1, then 3, then 2). */
+void ho_bound(const ho_grid *g, const ho_geom *m, double *pv, double *ps);
+
+/* Single-cell pieces (pinned one by one against the reference). */
+void ho_para(const double *x, double *l, double *r);
+void ho_primtoflux(double gam, const double *pr, const double *gcov10, const double *gcon10,
+                   double gdet, int dir, double *flux, double *vmax, double *vmin);
+int ho_utoprim_2d(double gam, double *U, const double *gcov10, const double *gcon10, double gdet, double *prim);
+int ho_utoprim_1dvsq2fix1(double gam, double *U, const double *gcov10, const double *gcon10, double gdet, double *prim);
+int ho_utoprim_1dfix1(double gam, double *U, const double *gcov10, const double *gcon10, double gdet, double *prim);
+
+/* Diagnostics */
+double ho_divb_max(const ho_grid *g, const ho_geom *m, const double *ps);
+
+#endif

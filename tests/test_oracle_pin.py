@@ -1,0 +1,180 @@
+"""Pins the C restatement (oracle/hamr_oracle.c) to the reference's own kernel
+code, built for the host from the reference sources (oracle/Makefile, variants
+t3: 3-D torus 16x8x8, t2: 2-D torus 24x24, ot: 2-D Cartesian 32x32).
+
+Both sides get identical inputs and identical metric tables (computed by the
+reference's metric.c), and must agree bit for bit.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests._setups import clone, make_setup
+
+VARIANTS = ["t3", "t2", "ot"]
+
+
+def need_ref(v):
+    if not O.ref_available(v):
+        pytest.skip(f"reference host build {v} not present (reference sources absent)")
+
+
+def _ref_bound(variant):
+    def bound(s, pn, psn):
+        O.oracle_bound(s, pn, psn)
+    return bound
+
+
+def _stage_ref(variant):
+    return lambda s, full, Dt, dt, cd: O.ref_stage(variant, s, full, Dt, dt, cd)
+
+
+def _stage_orc(s, full, Dt, dt, cd):
+    return O.oracle_stage(s, full, Dt, dt, cd)
+
+
+def _same(a, b, name):
+    d = np.abs(a - b)
+    assert np.array_equal(a, b), f"{name}: {np.count_nonzero(d)} entries differ, max |diff| {d.max():.3e}"
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_half_stage_bitwise(variant):
+    need_ref(variant)
+    s1 = make_setup(variant, seed=3)
+    s2 = clone(s1)
+    dt = 0.004
+    d1 = O.ref_stage(variant, s1, 0, 0.5 * dt, dt, True)
+    d2 = O.oracle_stage(s2, 0, 0.5 * dt, dt, True)
+    fluxes = ["F1", "F2"] + (["F3"] if s1.blk.n3 > 1 else [])
+    for name in fluxes + ["E_cent", "emf", "psh", "U", "ph"]:
+        _same(s1.blk.arrays[name], s2.blk.arrays[name], name)
+    _same(s1.blk.pflag, s2.blk.pflag, "pflag")
+    np.testing.assert_array_equal(d1, d2)
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_rk2_steps_bitwise(variant):
+    """Several full RK2 steps (half, ghost fill, full, ghost fill) with the
+    CFL-chosen timestep, as GPU_step_ch drives them."""
+    need_ref(variant)
+    s1 = make_setup(variant, seed=5)
+    s2 = clone(s1)
+    dt = 0.002
+    for _ in range(4):
+        n1 = O.step(_stage_ref(variant), _ref_bound(variant), s1, dt)
+        n2 = O.step(_stage_orc, _ref_bound(variant), s2, dt)
+        assert n1 == n2
+        for name in ("p", "ps", "ph", "psh"):
+            _same(s1.blk.arrays[name], s2.blk.arrays[name], name)
+        dt = min(n1, 1.3 * dt)
+
+
+@pytest.mark.parametrize("variant", ["t3", "t2"])
+def test_fallback_inversions_bitwise(variant):
+    """Cells where the Noble 2D solve fails walk the entropy fallbacks
+    (GPU_fixup.h:360-382); flags, failure counters and primitives agree."""
+    need_ref(variant)
+    s1 = make_setup(variant, seed=7, stress=True)
+    s2 = clone(s1)
+    dt = 0.001
+    O.ref_stage(variant, s1, 0, 0.5 * dt, dt, False)
+    O.oracle_stage(s2, 0, 0.5 * dt, dt, False)
+    fi = s1.blk.failimage.reshape(5, -1).sum(axis=1)
+    assert fi[0] > 0, "stress cells did not reach the fallback chain"
+    _same(s1.blk.failimage, s2.blk.failimage, "failimage")
+    _same(s1.blk.pflag[1:], s2.blk.pflag[1:], "pflag")
+    _same(s1.blk.ph, s2.blk.ph, "ph")
+
+
+def test_transmissive_pole_fill_matches_reference_kernel():
+    need_ref("t3")
+    s1 = make_setup("t3", seed=9)
+    s2 = clone(s1)
+    a1 = s1.blk.arrays
+    O.ref("t3").ref_bound_pole_trans(O._ptr(a1["p"]), O._ptr(a1["ps"]), O._ptr(s1.geo.gdet), 1, 1)
+    O.oracle_bound(s2, "p", "ps")
+    # the restated fill also redoes the radial and phi ghosts; poles must agree
+    g, n2 = s1.blk.ng, s1.blk.n2
+    for name in ("p",):
+        v1, v2 = s1.blk.view(name), s2.blk.view(name)
+        _same(v1[:, :, :g, :], v2[:, :, :g, :], name + " lower pole")
+        _same(v1[:, :, g + n2:, :], v2[:, :, g + n2:, :], name + " upper pole")
+    v1, v2 = s1.blk.view("ps"), s2.blk.view("ps")
+    for c in (0, 2):
+        _same(v1[c, :, :g, :], v2[c, :, :g, :], f"ps[{c}] lower pole")
+        _same(v1[c, :, g + n2:, :], v2[c, :, g + n2:, :], f"ps[{c}] upper pole")
+
+
+@pytest.mark.parametrize("variant", ["t3"])
+def test_single_cell_pieces(variant):
+    need_ref(variant)
+    rng = np.random.default_rng(11)
+    L = O.ref(variant)
+    # para
+    for _ in range(200):
+        x = rng.normal(size=5) * rng.choice([1e-3, 1.0, 1e3])
+        l1, r1 = np.zeros(1), np.zeros(1)
+        L.ref_para(O._ptr(x), O._ptr(l1), O._ptr(r1))
+        assert (l1[0], r1[0]) == O.para(x)
+    # primtoflux with wave speeds on the reference's own metric
+    s = make_setup(variant, seed=2)
+    geo, gs, g2 = s.geo, s.blk.gsize, s.blk.g2
+    _, gam = O.ref_dims(variant)
+    for _ in range(50):
+        i, j, loc, d = rng.integers(3, 12), rng.integers(3, 10), rng.integers(0, 5), rng.integers(0, 4)
+        if loc == O.CORN:
+            continue
+        idx = i * g2 + j
+        gcov = np.array([geo.gcov[(c * 5 + loc) * gs + idx] for c in range(10)])
+        gcon = np.array([geo.gcon[(c * 5 + loc) * gs + idx] for c in range(10)])
+        gdet = geo.gdet[loc * gs + idx]
+        pr = np.array([1.0, 0.2, 0.1, 0.01, 0.2, 0.3, 0.02, 0.1, 0.01]) * (1 + 0.2 * rng.random(9))
+        f1, f2 = np.zeros(9), np.zeros(9)
+        v1 = np.zeros(2)
+        v2 = np.zeros(2)
+        L.ref_primtoflux(O._ptr(pr.copy()), O._ptr(gcov), O._ptr(gcon), gdet, int(d), O._ptr(f1),
+                         O._ptr(v1[:1]), O._ptr(v1[1:]))
+        O.lib().ho_primtoflux(gam, O._ptr(pr.copy()), O._ptr(gcov), O._ptr(gcon), gdet, int(d),
+                              O._ptr(f2), O._ptr(v2[:1]), O._ptr(v2[1:]))
+        np.testing.assert_array_equal(f1, f2)
+        np.testing.assert_array_equal(v1, v2)
+
+
+@pytest.mark.parametrize("name", ["2d", "1dvsq2fix1", "1dfix1"])
+def test_inversions_single_cell_bitwise(name):
+    """Each inversion of the chain on sampled states whose energy was lowered
+    (so that the primary solve is stressed or fails) and whose entropy
+    variable is consistent, at metric points of the reference's torus grid."""
+    need_ref("t3")
+    rng = np.random.default_rng(21)
+    s = make_setup("t3", seed=2)
+    geo, gs, g2 = s.geo, s.blk.gsize, s.blk.g2
+    _, gam = O.ref_dims("t3")
+    n_ok = n_fail = 0
+    for trial in range(300):
+        i, j = rng.integers(3, 19), rng.integers(3, 11)
+        idx = i * g2 + j
+        gcov = np.array([geo.gcov[(c * 5 + O.CENT) * gs + idx] for c in range(10)])
+        gcon = np.array([geo.gcon[(c * 5 + O.CENT) * gs + idx] for c in range(10)])
+        gdet = geo.gdet[O.CENT * gs + idx]
+        rho = 10 ** rng.uniform(-6, 0)
+        u = rho * 10 ** rng.uniform(-4, 0)
+        pr = np.array([rho, u, *(rng.normal(size=3) * 10 ** rng.uniform(-2, 0.5)),
+                       *(rng.normal(size=3) * np.sqrt(rho) * 10 ** rng.uniform(-1, 1.5)), 0.0])
+        flux = np.zeros(9)
+        vv = np.zeros(2)
+        O.lib().ho_primtoflux(gam, O._ptr(pr), O._ptr(gcov), O._ptr(gcon), gdet, 0, O._ptr(flux),
+                              O._ptr(vv[:1]), O._ptr(vv[1:]))
+        U = flux.copy()
+        U[O.UU] += rng.uniform(0, 3.0) * gdet * u  # removes up to ~2u of internal energy
+        if trial % 3 == 0:
+            U[O.KTOT] *= -1.0  # no admissible entropy state: the fallbacks must fail too
+        guess = pr * (1 + 0.01 * rng.normal(size=9))
+        r1, p1 = O.ref_utoprim("t3", name, U, gcov, gcon, gdet, guess)
+        r2, p2 = O.utoprim(name, gam, U, gcov, gcon, gdet, guess)
+        assert r1 == r2, (trial, r1, r2)
+        np.testing.assert_array_equal(p1, p2)
+        n_ok += r1 == 0
+        n_fail += r1 != 0
+    assert n_ok > 20 and n_fail > 20, (n_ok, n_fail)
