@@ -1,0 +1,301 @@
+"""Throughput of the single-block GRMHD RK2 step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c3|c2] [--precision fp64]
+
+Workload (default c3): the 3-D Fishbone-Moncrief torus around a Kerr hole,
+a = 0.9375, r_in = 6, r_max = 12, gamma = 13/9, beta_min = 100, 4 % seeded
+pressure noise, 384 x 192 x 192 zones (14.2 M cells; c2: 192 x 96 x 64),
+synthetic initial data, inputs (~1 GB of primitives) larger than L2.
+
+A step is one RK2 step (half + full sub-step with ghost fills) of every zone.
+value = zones x steps / device time (cell-updates/s, the ZCPS of main.c:225),
+timed with CUDA events on the stream the kernels run on, after W warm-up
+steps, max over ranks. N > 1 runs independent replicas (one block per GPU,
+no exchange): scaling "weak".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "c3": dict(n1=384, n2=192, n3=192, rout=1000.0),
+    "c2": dict(n1=192, n2=96, n3=64, rout=1000.0),
+}
+# CPU sample of the same torus (same per-zone work, fewer zones)
+CPU_SAMPLE = dict(n1=64, n2=32, n3=32, rout=1000.0)
+
+
+def _dist():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def algorithmic_bytes_per_cell_update(n3: int) -> float:
+    """Minimal FP64 traffic of one cell advanced one full RK2 step: half stage
+    reads p^n (8) + ps^n (3), writes p* (8) + ps* (3) + U^n (6); full stage
+    reads p* (8) + ps* (3) + ps^n (3) + U^n (6), writes p^{n+1} (8) +
+    ps^{n+1} (3): 59 words; plus the axisymmetric metric (5 locations x 21 +
+    40 connection = 145 words per (i, j) column) read once per sub-step."""
+    return 59 * 8 + 2 * 1160.0 / n3
+
+
+def kernel_bytes(slot: str, d: dict) -> float:
+    """Algorithmic bytes of one launch of a kernel group (FP64):
+    flux_d   per face: 9 primitives + 1 normal face field read, 9 fluxes written,
+             plus the face metric (21 words) once per (i, j) column;
+    update   per zone: 9 primitives, 27 face fluxes, 3 face fields and 9 cached
+             conserved values read or written, 9 primitives written, plus the
+             centre metric and connection (61 words) per column."""
+    n1, n2, n3 = d["n1"], d["n2"], d["n3"]
+    if slot.startswith("flux"):
+        k = int(slot[-1])
+        nf = (n1 + 2 - (k == 1)) * (n2 + 2 - (k == 2)) * (n3 + 2 - (k == 3))
+        ncol = (n1 + 2 - (k == 1)) * (n2 + 2 - (k == 2))
+        return 19 * 8.0 * nf + 21 * 8.0 * ncol
+    if slot == "update":
+        return 57 * 8.0 * n1 * n2 * n3 + 61 * 8.0 * n1 * n2
+    if slot == "emf_centre":
+        return 12 * 8.0 * (n1 + 2) * (n2 + 2) * (n3 + 2)
+    if slot == "emf_edge":
+        return 15 * 8.0 * (n1 + 1) * (n2 + 1) * (n3 + 1)
+    if slot == "face_update":
+        return 9 * 8.0 * (n1 + 1) * (n2 + 1) * (n3 + 1)
+    return 0.0
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, n in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def cpu_baseline(steps: int = 1):
+    """The oracle (a C restatement of the reference step, bit-identical to the
+    reference kernels) on the host cores, OpenMP over zones."""
+    from hamr_gamma_wind_b200 import problems
+    from oracle import oracle as O
+    pb = problems.fm_torus(CPU_SAMPLE["n1"], CPU_SAMPLE["n2"], CPU_SAMPLE["n3"], rout=CPU_SAMPLE["rout"])
+    ob = O.Block(pb.n1, pb.n2, pb.n3, pb.ng, pb.ksize, pb.gsize)
+    ob.arrays["p"][:] = pb.p
+    ob.arrays["ps"][:] = pb.ps
+    geo = O.Geometry(pb.geo.gsize, pb.geo.gcov, pb.geo.gcon, pb.geo.gdet, pb.geo.conn)
+    s = O.Setup(ob, geo, pb.dx, pb.gam, pb.cour, 1, 1, (O.BC_OUTFLOW, O.BC_POLE_TRANS, O.BC_PERIODIC), 1)
+    O.oracle_bound(s)
+    stage = lambda s_, f, Dt, d, c: O.oracle_stage(s_, f, Dt, d, c)
+    bound = lambda s_, a, b: O.oracle_bound(s_, a, b)
+    dt = 0.2 * min(pb.dx[:2])
+    dt = min(O.step(stage, bound, s, dt), 1.3 * dt)   # warm-up
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        dt = min(O.step(stage, bound, s, dt), 1.3 * dt)
+    el = time.perf_counter() - t0
+    cells = pb.n1 * pb.n2 * pb.n3
+    return {"value": cells * steps / el, "unit": "cell-updates/s",
+            "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)), "kind": "port",
+            "sample": f"{pb.n1}x{pb.n2}x{pb.n3} torus zones, {steps} RK2 step(s) after 1 warm-up"}
+
+
+def run_reference(args):
+    rank, world, _ = _dist()
+    if rank != 0:
+        return
+    cb = cpu_baseline(steps=max(1, args.steps // 10))
+    out = {"metric": "cell-updates/s", "value": cb["value"], "unit": "cell-updates/s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
+           "dtype": "f64", "data": "synthetic", "vs_baseline": None,
+           "config": {"workload": f"torus {args.workload} sample", "sample": cb["sample"]},
+           "cpu_baseline": cb,
+           "e2e": {"value": cb["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    from hamr_gamma_wind_b200 import _lib, problems
+    from hamr_gamma_wind_b200.api import Block
+
+    wl = WORKLOADS[args.workload]
+    pb = problems.fm_torus(wl["n1"], wl["n2"], wl["n3"], rout=wl["rout"])
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    blk = Block(**pb.block_kwargs(), precision=args.precision, stream=ctypes_stream(stream))
+    blk.set_geometry(pb.geo)
+    blk.upload(pb.p, pb.ps)
+    blk.bound()
+    cells = pb.n1 * pb.n2 * pb.n3
+    dt = 0.2 * min(pb.dx[:2])
+    # warm-up: captures the K-step graph, then W more steps
+    dt = blk.step_ch(args.steps, dt, interval=16)
+    dt = blk.step_ch(args.warmup, dt, interval=16)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        dt = blk.step_ch(args.steps, dt, interval=16)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        torch.distributed.barrier()
+    value = world * cells * args.steps / (ms * 1e-3)
+
+    # per-kernel device times (outside the timed region)
+    prof = np.zeros(len(_lib.PROF_SLOTS))
+    blk._check(blk.L.hamr_profile_step(blk.ctx, dt, 2, prof.ctypes.data_as(__import__("ctypes").c_void_p),
+                                       len(prof)), "hamr_profile_step")
+    slots = dict(zip(_lib.PROF_SLOTS, prof.tolist()))
+    top = max(slots, key=slots.get)
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    kb = kernel_bytes(top, wl)
+    achieved = 2 * kb / (slots[top] * 1e-3) / 1e9 if slots[top] > 0 else 0.0
+    step_gbs = algorithmic_bytes_per_cell_update(pb.n3) * cells / (ms * 1e-3 / args.steps) / 1e9
+
+    # end to end through the public API with host buffers: upload from pinned
+    # memory, one step, download of the new state, every step
+    import ctypes
+    nk = 9 * blk.ksize
+    hp = torch.empty(nk, dtype=torch.float64, pin_memory=True).numpy()
+    hs = torch.empty(3 * blk.ksize, dtype=torch.float64, pin_memory=True).numpy()
+    p_now, ps_now = blk.download()
+    hp[:] = p_now
+    hs[:] = ps_now
+    n_e2e = max(1, min(args.steps, 5))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        blk.L.hamr_upload(blk.ctx, hp.ctypes.data_as(ctypes.c_void_p), hs.ctypes.data_as(ctypes.c_void_p))
+        dt = min(blk.step(dt), 1.3 * dt)
+        blk.L.hamr_download(blk.ctx, hp.ctypes.data_as(ctypes.c_void_p), hs.ctypes.data_as(ctypes.c_void_p))
+    e2e_s = time.perf_counter() - t0
+    e2e_val = world * cells * n_e2e / e2e_s
+    bytes_io = (nk + 3 * blk.ksize) * 8
+    p_end, _ = blk.download()
+    finite = bool(np.isfinite(blk.active(p_end)).all())
+
+    if rank == 0:
+        out = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "mixed f32/f64", "data": "synthetic",
+            "config": {"workload": f"3-D FM torus {wl['n1']}x{wl['n2']}x{wl['n3']} (a=0.9375, r_in=6, r_max=12, "
+                                   f"gamma=13/9, beta_min=100), {args.precision}",
+                       "zones": cells, "precision": args.precision, "l2": "inputs larger than L2 (no flush)",
+                       "dt_update_interval": 16, "parallelism": f"replicas x{world}"},
+            "gpu_launches": args.steps * 23 + 1,
+            "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": None, "peak_source": peak_src,
+                         "kernel_ms_per_step": slots},
+            "step_roofline": {"algorithmic_bytes_per_cell_update": algorithmic_bytes_per_cell_update(pb.n3),
+                              "achieved_gbs": step_gbs, "frac": step_gbs / hbm},
+            "clocks": clk.summary(),
+            "e2e": {"value": e2e_val, "unit": "cell-updates/s", "h2d_bytes_per_step": bytes_io,
+                    "d2h_bytes_per_step": bytes_io, "steps": n_e2e},
+            "state_finite": finite,
+        }
+        try:
+            out["cpu_baseline"] = cpu_baseline(steps=1)
+        except Exception as exc:  # the oracle is test infrastructure; report, do not fail the bench
+            out["cpu_baseline"] = {"value": None, "error": str(exc)}
+        print(json.dumps(out), flush=True)
+    blk.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def ctypes_stream(stream):
+    import ctypes
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c3", choices=list(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,53 @@
+"""Builds the in-tree CUDA library for sm_100a.
+
+Two shared objects come out of the same sources:
+  libhamr_b200.so         production build (fused multiply-add contraction on)
+  libhamr_b200_strict.so  --fmad=false: reproduces the reference's operation
+                          order, used by the bit-level parity tests
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+SOURCES = [os.path.join(CSRC, "hamr_kernels.cu"), os.path.join(CSRC, "hamr_geometry.cpp")]
+DEPS = SOURCES + [os.path.join(CSRC, "hamr_physics.cuh"),
+                  os.path.join(os.path.dirname(HERE), "include", "hamr_b200.h")]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+
+TARGETS = {
+    "libhamr_b200.so": [],
+    "libhamr_b200_strict.so": ["--fmad=false"],
+}
+
+
+def _stale(out):
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(d) > t for d in DEPS)
+
+
+def build(force=False, verbose=False):
+    outs = []
+    for name, extra in TARGETS.items():
+        out = os.path.join(HERE, name)
+        outs.append(out)
+        if not force and not _stale(out):
+            continue
+        cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
+               "-Xcompiler", "-ffp-contract=off", "-Xptxas", "-v" if verbose else "-O3",
+               *extra, *SOURCES, "-o", out]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError(f"nvcc failed building {name}")
+        if verbose:
+            sys.stderr.write(r.stderr)
+    return outs
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="-v" in sys.argv)

@@ -1,0 +1,1034 @@
+// sm_100a kernels of the single-block RK2 sub-step and the C ABI
+// (include/hamr_b200.h) that drives them.
+//
+// One sub-step (the work of advance_GPU, step_ch.c:997-1335, for one block):
+//   k_flux<3>, k_flux<2>, k_flux<1>   PPM + HLL face fluxes and the directional
+//                                      CFL minimum (fluxcalcprep + fluxcalc2D2)
+//   k_fix_flux                         reflective-pole flux rules (2-D)
+//   k_emf_centre, k_emf_edge           cell-centre and edge EMFs (consttransport1/2)
+//   k_pole_average                     phi-averaged polar EMF (E_average, 3-D)
+//   k_face_update                      staggered B update (consttransport3)
+//   k_update                           conserved update, source, inversion (fixup)
+//   k_bound_x1/x3/x2                   ghost fill of the written state
+// All arrays use the reference's structure-of-arrays layout; cell index
+// (i*G2 + j)*G3 + z puts phi (or x3) innermost, so consecutive threads touch
+// consecutive addresses.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/hamr_b200.h"
+#include "hamr_physics.cuh"
+
+using namespace hamr;
+
+namespace {
+
+constexpr int BLK = 128;
+
+struct Dims {
+    int n1, n2, n3, ng1, ng2, ng3, G1, G2, G3, d1, d2, d3;
+    long ks, gs;
+    double dx1, dx2, dx3, gam, cour;
+    int pole1, pole2, bc1, bc2, bc3, ct_upwind;
+};
+
+struct Geom {
+    const double *gcov, *gcon, *gdet, *conn;
+};
+
+__device__ __forceinline__ long cix(const Dims &d, int i, int j, int z) { return ((long)i * d.G2 + j) * d.G3 + z; }
+__device__ __forceinline__ long gix(const Dims &d, int i, int j) { return (long)i * d.G2 + j; }
+
+__device__ __forceinline__ void load_geo(const Dims &d, const Geom &m, int i, int j, int loc, Geo<double> &o) {
+    long idx = gix(d, i, j);
+#pragma unroll
+    for (int s = 0; s < 10; s++) {
+        o.gcon[s] = __ldg(&m.gcon[(long)(s * 5 + loc) * d.gs + idx]);
+        o.gcov[s] = __ldg(&m.gcov[(long)(s * 5 + loc) * d.gs + idx]);
+    }
+    o.g = __ldg(&m.gdet[(long)loc * d.gs + idx]);
+}
+
+// Sub-step sizes either come by value (hamr_stage) or from device memory
+// (hamr_advance replays a captured graph while the step size evolves).
+struct StepSize {
+    const double *dev;  // dev[0] = dt when not NULL
+    double frac;        // Dt = frac * dt
+    double Dt, dt;      // used when dev == NULL
+    __device__ __forceinline__ double sub() const { return dev ? frac * dev[0] : Dt; }
+    __device__ __forceinline__ double full() const { return dev ? dev[0] : dt; }
+};
+
+// ---------------------------------------------------------------------------
+// Face fluxes of direction DIR over the normal range [ng, n + ng] and one ghost
+// layer either side transversally (fluxcalc2D2's face set).
+template <int DIR>
+__global__ void __launch_bounds__(BLK) k_flux(const Dims d, const Geom m, const double *__restrict__ pv,
+                                               const double *__restrict__ ps, double *__restrict__ F,
+                                               unsigned long long *__restrict__ dtbits, int calc_dt) {
+    constexpr int idel = DIR == 1, jdel = DIR == 2, zdel = DIR == 3;
+    const int i0 = (d.ng1 - 1) * d.d1 + idel, ni = d.n1 + 2 * d.d1 - idel;
+    const int j0 = (d.ng2 - 1) * d.d2 + jdel, nj = d.n2 + 2 * d.d2 - jdel;
+    const int z0 = (d.ng3 - 1) * d.d3 + zdel, nz = d.n3 + 2 * d.d3 - zdel;
+    const long nf = (long)ni * nj * nz;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double dtf = 1.e9;
+    if (t < nf) {
+        const int z = z0 + (int)(t % nz);
+        const int j = j0 + (int)((t / nz) % nj);
+        const int i = i0 + (int)(t / ((long)nz * nj));
+        const long c = cix(d, i, j, z);
+        const long stride = idel ? (long)d.G2 * d.G3 : (jdel ? (long)d.G3 : 1L);
+        const int face = DIR == 1 ? FACE1 : (DIR == 2 ? FACE2 : FACE3);
+        Geo<double> gm;
+        load_geo(d, m, i, j, face, gm);
+        double pl[NPR], pr[NPR];
+#pragma unroll
+        for (int k = 0; k < NPR; k++) {
+            const double *pk = pv + (long)k * d.ks + c;
+            double x[6];
+#pragma unroll
+            for (int s = 0; s < 6; s++) x[s] = __ldg(pk + (s - 3) * stride);
+            double lo, hi;
+            para(x, lo, hi);       // zone c-1: upper edge is the left state
+            pl[k] = hi;
+            para(x + 1, lo, hi);   // zone c: lower edge is the right state
+            pr[k] = lo;
+        }
+        const double bn = __ldg(&ps[(long)(DIR - 1) * d.ks + c]);
+        pl[B1 + DIR - 1] = bn;
+        pr[B1 + DIR - 1] = bn;
+        if (DIR == 2 && ((j == d.n2 + d.ng2 && d.pole2) || (j == d.ng2 && d.pole1))) {
+            pl[B1] = 0.;
+            pr[B1] = 0.;
+        }
+        State<double> q;
+        double t1[NPR], t2[NPR], t3[NPR], t4[NPR];
+        double cmax_l, cmin_l, cmax_r, cmin_r, vd;
+        get_state(pl, gm, q);
+        double e = entropy(d.gam, pl);
+        primtoflux(d.gam, pl, q, DIR, gm, e, t1, &cmax_l, &cmin_l);
+        primtoflux(d.gam, pl, q, 0, gm, e, t2, &vd, &vd);
+        get_state(pr, gm, q);
+        e = entropy(d.gam, pr);
+        primtoflux(d.gam, pr, q, DIR, gm, e, t3, &cmax_r, &cmin_r);
+        primtoflux(d.gam, pr, q, 0, gm, e, t4, &vd, &vd);
+        const double cmax = fabs(d_max(d_max(0., cmax_l), cmax_r));
+        const double cmin = fabs(d_max(d_max(0., -cmin_l), -cmin_r));
+        const double ctop = d_max(cmax, cmin);
+#pragma unroll
+        for (int k = 0; k < NPR; k++)
+            F[(long)k * d.ks + c] = (cmax * t1[k] + cmin * t3[k] - cmax * cmin * (t4[k] - t2[k])) / (cmax + cmin + SMALL_D);
+        const double dxd = DIR == 1 ? d.dx1 : (DIR == 2 ? d.dx2 : d.dx3);
+        const double v = d.cour * dxd / ctop;
+        if (v > 1.e-6 && v < dtf) dtf = v;
+    }
+    if (calc_dt) {
+        // block minimum by warp shuffles, one atomic per block
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) dtf = d_min(dtf, __shfl_xor_sync(0xffffffffu, dtf, o));
+        __shared__ double wmin[BLK / 32];
+        if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = dtf;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double b = wmin[0];
+            for (int w = 1; w < BLK / 32; w++) b = d_min(b, wmin[w]);
+            // positive doubles order like their bit patterns
+            atomicMin(&dtbits[DIR], (unsigned long long)__double_as_longlong(b));
+        }
+    }
+}
+
+// reflective polar axis and no-inflow radial edges (fix_flux, GPU_const_trans.h:3-61)
+__global__ void k_fix_flux(const Dims d, double *F1, double *F2, double *F3) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long ks = d.ks;
+    const long na = (long)d.G1 * d.G3;
+    if (t < na) {
+        const int z = (int)(t % d.G3), i = (int)(t / d.G3);
+        if (!(i >= d.ng1 - d.d1 && z >= d.ng3 - d.d3 && i < d.n1 + d.ng1 + d.d1 && z < d.n3 + d.ng3 + d.d3)) return;
+        if (d.pole1) {
+            F1[B2 * ks + cix(d, i, d.ng2 - 1, z)] = -F1[B2 * ks + cix(d, i, d.ng2, z)];
+            if (d.ng3 > 0) F3[B2 * ks + cix(d, i, d.ng2 - 1, z)] = -F3[B2 * ks + cix(d, i, d.ng2, z)];
+            for (int k = 0; k < NPR; k++) F2[k * ks + cix(d, i, d.ng2, z)] = 0.;
+        }
+        if (d.pole2) {
+            F1[B2 * ks + cix(d, i, d.n2 + d.ng2, z)] = -F1[B2 * ks + cix(d, i, d.n2 + d.ng2 - 1, z)];
+            if (d.ng3 > 0) F3[B2 * ks + cix(d, i, d.n2 + d.ng2, z)] = -F3[B2 * ks + cix(d, i, d.n2 + d.ng2 - 1, z)];
+            for (int k = 0; k < NPR; k++) F2[k * ks + cix(d, i, d.n2 + d.ng2, z)] = 0.;
+        }
+        return;
+    }
+    const long u = t - na;
+    if (u >= (long)d.G2 * d.G3) return;
+    const int z = (int)(u % d.G3), j = (int)(u / d.G3);
+    if (!(j >= d.ng2 - d.d2 && z >= d.ng3 - d.d3 && j < d.n2 + d.ng2 + d.d2 && z < d.n3 + d.ng3 + d.d3)) return;
+    const long ci = RHO * ks + cix(d, d.ng1, j, z);
+    if (F1[ci] > 0.) F1[ci] = 0.;
+    const long co = RHO * ks + cix(d, d.n1 + d.ng1, j, z);
+    if (F1[co] < 0.) F1[co] = 0.;
+}
+
+// cell-centre EMF, -gdet (u x b), on the active zones plus one ghost layer
+__global__ void __launch_bounds__(BLK) k_emf_centre(const Dims d, const Geom m, const double *__restrict__ pv,
+                                                     double *__restrict__ Ec) {
+    const int ni = d.n1 + 2 * d.d1, nj = d.n2 + 2 * d.d2, nz = d.n3 + 2 * d.d3;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)ni * nj * nz) return;
+    const int z = (d.ng3 - d.d3) * d.d3 + (int)(t % nz);
+    const int j = (d.ng2 - d.d2) * d.d2 + (int)((t / nz) % nj);
+    const int i = (d.ng1 - d.d1) * d.d1 + (int)(t / ((long)nz * nj));
+    const long c = cix(d, i, j, z);
+    double pb[NPR];
+#pragma unroll
+    for (int k = 0; k < NPR; k++) pb[k] = __ldg(&pv[k * d.ks + c]);
+    Geo<double> gm;
+    load_geo(d, m, i, j, CENT, gm);
+    double ucon[4], ucov[4], bcon[4];
+    ucon_calc(pb, gm, ucon);
+    lower4(ucon, gm.gcov, ucov);
+    bcon_calc(pb, ucon, ucov, bcon);
+    if (d.ng3 > 0) {
+        Ec[1 * d.ks + c] = -gm.g * (ucon[2] * bcon[3] - ucon[3] * bcon[2]);
+        Ec[2 * d.ks + c] = -gm.g * (ucon[3] * bcon[1] - ucon[1] * bcon[3]);
+    }
+    Ec[3 * d.ks + c] = -gm.g * (ucon[1] * bcon[2] - ucon[2] * bcon[1]);
+}
+
+__device__ __forceinline__ double up(double f) { return (double)(f <= 0.0); }
+__device__ __forceinline__ double dn(double f) { return (double)(f > 0.0); }
+
+// edge EMFs: average of the four face EMFs plus, when ct_upwind, the
+// centre-minus-face corrections from the upwind side of each face, chosen by
+// the sign of its mass flux (consttransport2, GPU_const_trans.h:121-338)
+__global__ void __launch_bounds__(BLK) k_emf_edge(const Dims d, const double *__restrict__ Ec,
+                                                   const double *__restrict__ F1, const double *__restrict__ F2,
+                                                   const double *__restrict__ F3, double *__restrict__ emf) {
+    const int ni = d.n1 + d.d1, nj = d.n2 + d.d2, nz = d.n3 + d.d3;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)ni * nj * nz) return;
+    const int z = d.ng3 * d.d3 + (int)(t % nz);
+    const int j = d.ng2 * d.d2 + (int)((t / nz) % nj);
+    const int i = d.ng1 * d.d1 + (int)(t / ((long)nz * nj));
+    const long c = cix(d, i, j, z);
+    const long ks = d.ks, jsize = d.G3, isize = (long)d.G2 * d.G3;
+    const long D1 = d.d1, D2 = d.d2, D3 = d.d3;
+    const double *Ec1 = Ec + 1 * ks, *Ec2 = Ec + 2 * ks, *Ec3 = Ec + 3 * ks;
+    const double *F1r = F1 + RHO * ks, *F2r = F2 + RHO * ks, *F3r = F3 + RHO * ks;
+    const double w = d.ct_upwind ? 1.0 : 0.0;
+    // in the non-upwind build every correction is an exact 0.0
+#define CORR(expr) (w != 0.0 ? (expr) : 0.0)
+    const double dE_LEFT_13_1 = CORR(Ec1[c] - F3[B2 * ks + c]);
+    const double dE_LEFT_13_2 = CORR(Ec1[c - jsize * D2] - F3[B2 * ks + c - jsize * D2]);
+    const double dE_RIGHT_13_1 = CORR(F3[B2 * ks + c] - Ec1[c - D3]);
+    const double dE_RIGHT_13_2 = CORR(F3[B2 * ks + c - jsize * D2] - Ec1[c - jsize * D2 - D3]);
+    const double dE_LEFT_12_1 = CORR(Ec1[c] + F2[B3 * ks + c]);
+    const double dE_LEFT_12_2 = CORR(Ec1[c - D3] + F2[B3 * ks + c - D3]);
+    const double dE_RIGHT_12_1 = CORR(-F2[B3 * ks + c] - Ec1[c - D2 * jsize]);
+    const double dE_RIGHT_12_2 = CORR(-F2[B3 * ks + c - D3] - Ec1[c - D2 * jsize - D3]);
+    const double dE_LEFT_21_1 = CORR(Ec2[c] - F1[B3 * ks + c]);
+    const double dE_LEFT_21_2 = CORR(Ec2[c - D3] - F1[B3 * ks + c - D3]);
+    const double dE_RIGHT_21_1 = CORR(F1[B3 * ks + c] - Ec2[c - D1 * isize]);
+    const double dE_RIGHT_21_2 = CORR(F1[B3 * ks + c - D3] - Ec2[c - D1 * isize - D3]);
+    const double dE_LEFT_23_1 = CORR(Ec2[c] + F3[B1 * ks + c]);
+    const double dE_LEFT_23_2 = CORR(Ec2[c - D1 * isize] + F3[B1 * ks + c - D1 * isize]);
+    const double dE_RIGHT_23_1 = CORR(-F3[B1 * ks + c] - Ec2[c - D3]);
+    const double dE_RIGHT_23_2 = CORR(-F3[B1 * ks + c - isize * D1] - Ec2[c - isize * D1 - D3]);
+    const double dE_LEFT_31_1 = CORR(Ec3[c] + F1[B2 * ks + c]);
+    const double dE_LEFT_31_2 = CORR(Ec3[c - D2 * jsize] + F1[B2 * ks + c - D2 * jsize]);
+    const double dE_RIGHT_31_1 = CORR(-F1[B2 * ks + c] - Ec3[c - D1 * isize]);
+    const double dE_RIGHT_31_2 = CORR(-F1[B2 * ks + c - D2 * jsize] - Ec3[c - D1 * isize - D2 * jsize]);
+    const double dE_LEFT_32_1 = CORR(Ec3[c] - F2[B1 * ks + c]);
+    const double dE_LEFT_32_2 = CORR(Ec3[c - D1 * isize] - F2[B1 * ks + c - D1 * isize]);
+    const double dE_RIGHT_32_1 = CORR(F2[B1 * ks + c] - Ec3[c - D2 * jsize]);
+    const double dE_RIGHT_32_2 = CORR(F2[B1 * ks + c - D1 * isize] - Ec3[c - D1 * isize - D2 * jsize]);
+#undef CORR
+    double e1 = 0.25 * ((-F2[B3 * ks + c] - (dE_LEFT_13_1 * up(F2r[c]) + dE_LEFT_13_2 * dn(F2r[c])))
+        + (-F2[B3 * ks + c - D3] + (dE_RIGHT_13_1 * up(F2r[c - D3]) + dE_RIGHT_13_2 * dn(F2r[c - D3]))) +
+        +(F3[B2 * ks + c] - (dE_LEFT_12_1 * up(F3r[c]) + dE_LEFT_12_2 * dn(F3r[c])))
+        + (F3[B2 * ks + c - D2 * jsize] + (dE_RIGHT_12_1 * up(F3r[c - D2 * jsize]) + dE_RIGHT_12_2 * dn(F3r[c - D2 * jsize]))));
+    const double e2 = 0.25 * ((-F3[B1 * ks + c] - (dE_LEFT_21_1 * up(F3r[c]) + dE_LEFT_21_2 * dn(F3r[c])))
+        + (-F3[B1 * ks + c - D1 * isize] + (dE_RIGHT_21_1 * up(F3r[c - D1 * isize]) + dE_RIGHT_21_2 * dn(F3r[c - D1 * isize])))
+        + (F1[B3 * ks + c] - (dE_LEFT_23_1 * up(F1r[c]) + dE_LEFT_23_2 * dn(F1r[c])))
+        + (F1[B3 * ks + c - D3] + (dE_RIGHT_23_1 * up(F1r[c - D3]) + dE_RIGHT_23_2 * dn(F1r[c - D3]))));
+    double e3 = 0.25 * ((F2[B1 * ks + c] - (dE_LEFT_31_1 * up(F2r[c]) + dE_LEFT_31_2 * dn(F2r[c])))
+        + (F2[B1 * ks + c - D1 * isize] + (dE_RIGHT_31_1 * up(F2r[c - D1 * isize]) + dE_RIGHT_31_2 * dn(F2r[c - D1 * isize])))
+        + (-F1[B2 * ks + c] - (dE_LEFT_32_1 * up(F1r[c]) + dE_LEFT_32_2 * dn(F1r[c])))
+        + (-F1[B2 * ks + c - D2 * jsize] + (dE_RIGHT_32_1 * up(F1r[c - D2 * jsize]) + dE_RIGHT_32_2 * dn(F1r[c - D2 * jsize]))));
+    if ((d.pole1 && j == d.ng2) || (d.pole2 && j == d.n2 + d.ng2)) {
+        e3 = 0.;
+        e1 = -0.5 * (F2[B3 * ks + c] + F2[B3 * ks + c - D3]);
+    }
+    emf[1 * ks + c] = e1;
+    emf[2 * ks + c] = e2;
+    emf[3 * ks + c] = e3;
+}
+
+// phi-average of the x1-EMF on the polar edges of a block that holds every
+// phi zone (E_average, const_trans.c:268-503): dt-scaled sum over active z,
+// divided by n3, unscaled; x3-EMF zeroed there. One thread per (side, i).
+__global__ void k_pole_average(const Dims d, double *emf, StepSize st) {
+    const int ni = d.n1 + d.ng1;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * ni) return;
+    const int side = t / ni, i = d.ng1 + t % ni;
+    if ((side == 0 && !d.pole1) || (side == 1 && !d.pole2)) return;
+    const int jp = side == 0 ? d.ng2 : d.n2 + d.ng2;
+    const double dt = st.full();
+    double avg = 0.;
+    for (int z = d.ng3; z < d.n3 + d.ng3; z++) avg += dt * emf[1 * d.ks + cix(d, i, jp, z)];
+    avg /= (double)(d.n3);
+    const double avg_new = avg / ((double)1);
+    for (int z = d.ng3; z < d.n3 + 2 * d.ng3; z++) {
+        emf[1 * d.ks + cix(d, i, jp, z)] = avg_new / dt;
+        emf[3 * d.ks + cix(d, i, jp, z)] = 0.;
+    }
+}
+
+// staggered field update from the edge EMFs (consttransport3, GPU_const_trans.h:426-529)
+__global__ void __launch_bounds__(BLK) k_face_update(const Dims d, const Geom m, const double *psi, double *psf,
+                                                      const double *__restrict__ E, StepSize st) {
+    const int ni = d.n1 + d.d1, nj = d.n2 + d.d2, nz = d.n3 + d.d3;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)ni * nj * nz) return;
+    const int z = d.ng3 * d.d3 + (int)(t % nz);
+    const int j = d.ng2 * d.d2 + (int)((t / nz) % nj);
+    const int i = d.ng1 * d.d1 + (int)(t / ((long)nz * nj));
+    const long c = cix(d, i, j, z), gi = gix(d, i, j);
+    const long ks = d.ks, isize = (long)d.G2 * d.G3, jsz = d.G3;
+    const double Dt = st.sub();
+    if (i < d.n1 + d.ng1 + d.d1 && j < d.n2 + d.ng2 && z < d.n3 + d.ng3) {
+        const double gdf = __ldg(&m.gdet[FACE1 * d.gs + gi]);
+        double temp = 0.;
+        temp += 1.0 / ((double)1) * psi[c] * gdf;
+        temp += -Dt / ((double)1 * d.dx2) * (E[3 * ks + c + jsz] - E[3 * ks + c]);
+        if (d.ng3 > 0) temp += Dt / ((double)1 * d.dx3) * (E[2 * ks + c + d.d3] - E[2 * ks + c]);
+        psf[c] = temp / gdf;
+    }
+    if (d.ng3 > 0 && i < d.n1 + d.ng1 && j < d.n2 + d.ng2 && z < d.n3 + d.ng3 + d.d3) {
+        const double gdf = __ldg(&m.gdet[FACE3 * d.gs + gi]);
+        double temp = psi[2 * ks + c] * gdf;
+        temp += -Dt / d.dx1 * (E[2 * ks + c + isize] - E[2 * ks + c]);
+        temp += Dt / d.dx2 * (E[1 * ks + c + jsz] - E[1 * ks + c]);
+        psf[2 * ks + c] = temp / gdf;
+    }
+    if (i < d.n1 + d.ng1 && j < d.n2 + d.ng2 + d.d2 && z < d.n3 + d.ng3) {
+        const double gdf = __ldg(&m.gdet[FACE2 * d.gs + gi]);
+        double temp = 0.;
+        temp += 1.0 / ((double)1) * psi[1 * ks + c] * gdf;
+        temp += Dt / ((double)1 * d.dx1) * (E[3 * ks + c + isize] - E[3 * ks + c]);
+        if (d.ng3 > 0) temp += -Dt / ((double)1 * d.dx3) * (E[1 * ks + c + d.d3] - E[1 * ks + c]);
+        psf[1 * ks + c] = temp / gdf;
+    }
+}
+
+// geometric source gdet T^k_l Gamma^l_{jk} (source, GPU_phys_mhd.h:34-175)
+__device__ __forceinline__ void source(double gam, const double *ph, const Geo<double> &gm, const Dims &d,
+                                       const Geom &m, long gi, double *dU, const State<double> &q) {
+    double mhd[4][4];
+    const long gs = d.gs;
+    const double P = (gam - 1.) * ph[UU];
+    const double u = ph[UU];
+    const double w = P + ph[RHO] + u;
+    const double bsq = dot4(q.bcon, q.bcov);
+    const double eta = w + bsq;
+    const double ptot = P + 0.5 * bsq;
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+            mhd[a][b] = eta * q.ucon[a] * q.ucov[b] + ptot * (a == b ? 1. : 0.) - q.bcon[a] * q.bcov[b];
+#pragma unroll
+    for (int k = 0; k < NPR; k++) dU[k] = 0.;
+#define CONN(s, k) __ldg(&m.conn[(long)((s) * 4 + (k)) * gs + gi])
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        double c;
+        dU[UU] += mhd[0][k] * CONN(0, k);
+        dU[U1] += mhd[1][k] * CONN(4, k);
+        dU[U2] += mhd[2][k] * CONN(7, k);
+        dU[U3] += mhd[3][k] * CONN(9, k);
+        c = CONN(1, k); dU[UU] += mhd[1][k] * c; dU[U1] += mhd[0][k] * c;
+        c = CONN(2, k); dU[UU] += mhd[2][k] * c; dU[U2] += mhd[0][k] * c;
+        c = CONN(3, k); dU[UU] += mhd[3][k] * c; dU[U3] += mhd[0][k] * c;
+        c = CONN(5, k); dU[U1] += mhd[2][k] * c; dU[U2] += mhd[1][k] * c;
+        c = CONN(6, k); dU[U1] += mhd[3][k] * c; dU[U3] += mhd[1][k] * c;
+        c = CONN(8, k); dU[U2] += mhd[3][k] * c; dU[U3] += mhd[2][k] * c;
+    }
+#undef CONN
+    dU[UU] *= gm.g;
+    dU[U1] *= gm.g;
+    dU[U2] *= gm.g;
+    dU[U3] *= gm.g;
+    dU[KTOT] *= gm.g;
+}
+
+// conserved update and inversion of one active zone (fixup, GPU_fixup.h:5-424)
+__global__ void __launch_bounds__(BLK) k_update(const Dims d, const Geom m, const double *__restrict__ pin,
+                                                 const double *__restrict__ pb, double *__restrict__ pout,
+                                                 double *__restrict__ Ucache, const double *__restrict__ psf,
+                                                 const double *__restrict__ F1, const double *__restrict__ F2,
+                                                 const double *__restrict__ F3, int *__restrict__ pflag,
+                                                 int *__restrict__ failimage, int full, StepSize st) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)d.n1 * d.n2 * d.n3) return;
+    const int z = d.ng3 + (int)(t % d.n3);
+    const int j = d.ng2 + (int)((t / d.n3) % d.n2);
+    const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
+    const long c = cix(d, i, j, z), gi = gix(d, i, j);
+    const long ks = d.ks, isize = (long)d.G2 * d.G3;
+    const double Dt = st.sub();
+    Geo<double> gm;
+    load_geo(d, m, i, j, CENT, gm);
+    State<double> q;
+    double pf[NPR], U[NPR], dU[NPR];
+    if (!full) {
+#pragma unroll
+        for (int k = 0; k < NPR; k++) { pf[k] = 0.0; pf[k] += (1.0 / ((double)1)) * pin[k * ks + c]; }
+        get_state(pf, gm, q);
+        double vd;
+        primtoflux(d.gam, pf, q, 0, gm, entropy(d.gam, pf), U, &vd, &vd);
+#pragma unroll
+        for (int k = 0; k < NPR; k++) Ucache[k * ks + c] = U[k];
+    } else {
+#pragma unroll
+        for (int k = 0; k < NPR; k++) U[k] = Ucache[k * ks + c];
+#pragma unroll
+        for (int k = 0; k < NPR; k++) { pf[k] = 0.0; pf[k] += (1.0 / ((double)1)) * pb[k * ks + c]; }
+        get_state(pf, gm, q);
+    }
+#pragma unroll
+    for (int k = 0; k < NPR; k++) {
+        if (d.ng1 > 0) U[k] -= Dt * (F1[k * ks + c + isize] - F1[k * ks + c]) / (d.dx1 * (double)1);
+        if (d.ng2 > 0) U[k] -= Dt * (F2[k * ks + c + d.G3] - F2[k * ks + c]) / (d.dx2 * (double)1);
+        if (d.ng3 > 0) U[k] -= Dt * (F3[k * ks + c + 1] - F3[k * ks + c]) / (d.dx3 * (double)1);
+    }
+    source(d.gam, pf, gm, d, m, gi, dU, q);
+#pragma unroll
+    for (int k = 0; k < NPR; k++) U[k] += Dt * (dU[k]);
+    U[B1] = 0.0;
+    U[B2] = 0.0;
+    U[B1] += (psf[0 * ks + c] * m.gdet[FACE1 * d.gs + gi] + psf[0 * ks + c + isize] * m.gdet[FACE1 * d.gs + gix(d, i + d.d1, j)]) / (2.0 * (double)1);
+    U[B2] += (psf[1 * ks + c] * m.gdet[FACE2 * d.gs + gi] + psf[1 * ks + c + d.G3] * m.gdet[FACE2 * d.gs + gix(d, i, j + d.d2)]) / (2.0 * (double)1);
+    if (d.ng3 > 0)
+        U[B3] = (psf[2 * ks + c] * m.gdet[FACE3 * d.gs + gi] + psf[2 * ks + c + 1 * d.d3] * m.gdet[FACE3 * d.gs + gi]) / 2.0;
+    int flag = utoprim_2d(d.gam, U, gm.gcov, gm.gcon, gm.g, pf);
+    if (flag) {
+        failimage[c]++;
+        flag = utoprim_1dvsq2fix1(d.gam, U, gm.gcov, gm.gcon, gm.g, pf);
+        if (flag) {
+            failimage[1 * ks + c]++;
+            flag = utoprim_1dfix1(d.gam, U, gm.gcov, gm.gcon, gm.g, pf);
+            if (flag) failimage[2 * ks + c]++;
+        }
+    }
+    pflag[c] = flag;
+#pragma unroll
+    for (int k = 0; k < NPR; k++) pout[k * ks + c] = pf[k];
+}
+
+// ------------------------------------------------------------ ghost fills
+// no-inflow check on a ghost zone (inflow_check, GPU_bounds.h:1368-1410)
+__device__ void inflow_check(double *pr, const Geo<double> &gm, int type) {
+    double ucon[4], gamma;
+    ucon_calc(pr, gm, ucon);
+    if (((ucon[1] > 0.) && (type == 0)) || ((ucon[1] < 0.) && (type == 1))) {
+        gamma_calc(pr, gm, &gamma);
+        pr[U1] /= gamma;
+        pr[U2] /= gamma;
+        pr[U3] /= gamma;
+        const double alpha = 1. / sqrt(-gm.gcon[0]);
+        const double beta1 = gm.gcon[1] * alpha * alpha;
+        pr[U1] = beta1 / alpha;
+        double vsq = gm.gcov[4] * pr[U1] * pr[U1];
+        vsq += 2. * gm.gcov[5] * pr[U2] * pr[U1];
+        vsq += 2. * gm.gcov[6] * pr[U3] * pr[U1];
+        vsq += gm.gcov[7] * pr[U2] * pr[U2];
+        vsq += 2 * gm.gcov[8] * pr[U3] * pr[U2];
+        vsq += gm.gcov[9] * pr[U3] * pr[U3];
+        vsq = d_max(1.e-13, vsq);
+        if (vsq >= 1.) vsq = 1. - 1. / (80. * 80.);
+        gamma = 1. / sqrt(1. - vsq);
+        pr[U1] *= gamma;
+        pr[U2] *= gamma;
+        pr[U3] *= gamma;
+    }
+}
+
+__device__ __forceinline__ void copy_cell(const Dims &d, double *pv, long dst, long src) {
+#pragma unroll
+    for (int k = 0; k < NPR; k++) pv[k * d.ks + dst] = pv[k * d.ks + src];
+}
+
+// x1 ghosts over every (j, z): periodic copy, or outflow copy + no-inflow
+__global__ void k_bound_x1(const Dims d, const Geom m, double *pv, double *ps) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)d.ng1 * d.G2 * d.G3) return;
+    const int z = (int)(t % d.G3), j = (int)((t / d.G3) % d.G2), g = (int)(t / ((long)d.G3 * d.G2));
+    const int ilo = g, ihi = d.n1 + d.ng1 + g;
+    const long ks = d.ks;
+    if (d.bc1 == HAMR_BC_PERIODIC) {
+        copy_cell(d, pv, cix(d, ilo, j, z), cix(d, ilo + d.n1, j, z));
+        copy_cell(d, pv, cix(d, ihi, j, z), cix(d, ihi - d.n1, j, z));
+        for (int k = 0; k < 3; k++) {
+            ps[k * ks + cix(d, ilo, j, z)] = ps[k * ks + cix(d, ilo + d.n1, j, z)];
+            ps[k * ks + cix(d, ihi, j, z)] = ps[k * ks + cix(d, ihi - d.n1, j, z)];
+        }
+        return;
+    }
+    double pr[NPR];
+    Geo<double> gm;
+    long src = cix(d, d.ng1, j, z), dst = cix(d, ilo, j, z);
+    for (int k = 0; k < NPR; k++) pr[k] = pv[k * ks + src];
+    load_geo(d, m, ilo, j, CENT, gm);
+    inflow_check(pr, gm, 0);
+    for (int k = 0; k < NPR; k++) pv[k * ks + dst] = pr[k];
+    ps[1 * ks + dst] = ps[1 * ks + src];
+    ps[2 * ks + dst] = ps[2 * ks + src];
+    src = cix(d, d.n1 + d.ng1 - 1, j, z);
+    dst = cix(d, ihi, j, z);
+    for (int k = 0; k < NPR; k++) pr[k] = pv[k * ks + src];
+    load_geo(d, m, ihi, j, CENT, gm);
+    inflow_check(pr, gm, 1);
+    for (int k = 0; k < NPR; k++) pv[k * ks + dst] = pr[k];
+    ps[1 * ks + dst] = ps[1 * ks + src];
+    ps[2 * ks + dst] = ps[2 * ks + src];
+}
+
+// x3 ghosts (periodic) over every (i, j)
+__global__ void k_bound_x3(const Dims d, double *pv, double *ps) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)d.ng3 * d.G1 * d.G2) return;
+    const int g = (int)(t % d.ng3), j = (int)((t / d.ng3) % d.G2), i = (int)(t / ((long)d.ng3 * d.G2));
+    const long lo = cix(d, i, j, g), lo_src = cix(d, i, j, g + d.n3);
+    const long hi = cix(d, i, j, d.n3 + d.ng3 + g), hi_src = cix(d, i, j, d.ng3 + g);
+    copy_cell(d, pv, lo, lo_src);
+    copy_cell(d, pv, hi, hi_src);
+    for (int k = 0; k < 3; k++) {
+        ps[k * d.ks + lo] = ps[k * d.ks + lo_src];
+        ps[k * d.ks + hi] = ps[k * d.ks + hi_src];
+    }
+}
+
+// x2 ghosts over every (i, z): periodic, transmissive or reflective polar
+// axis, or plain outflow copy
+__global__ void k_bound_x2(const Dims d, double *pv, double *ps) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)d.G1 * d.G3) return;
+    const int z = (int)(t % d.G3), i = (int)(t / d.G3);
+    const int n2 = d.n2, ng = d.ng2;
+    const long ks = d.ks;
+    if (d.bc2 == HAMR_BC_PERIODIC) {
+        for (int g = 0; g < ng; g++) {
+            const long lo = cix(d, i, g, z), lo_src = cix(d, i, g + n2, z);
+            const long hi = cix(d, i, n2 + ng + g, z), hi_src = cix(d, i, ng + g, z);
+            copy_cell(d, pv, lo, lo_src);
+            copy_cell(d, pv, hi, hi_src);
+            for (int k = 0; k < 3; k++) {
+                ps[k * ks + lo] = ps[k * ks + lo_src];
+                ps[k * ks + hi] = ps[k * ks + hi_src];
+            }
+        }
+    } else if (d.bc2 == HAMR_BC_POLE_TRANS) {
+        const int zs = d.d3 ? (z - d.ng3 + d.n3 / 2) % d.n3 + d.ng3 : z;
+        if (d.pole1)
+            for (int jj = -ng; jj < 0; jj++) {
+                const long dst = cix(d, i, jj + ng, z), src = cix(d, i, -jj - 1 + ng, zs);
+                copy_cell(d, pv, dst, src);
+                pv[U2 * ks + dst] *= -1.0;
+                pv[U3 * ks + dst] *= -1.0;
+                pv[B2 * ks + dst] *= -1.0;
+                pv[B3 * ks + dst] *= -1.0;
+                ps[0 * ks + dst] = ps[0 * ks + src];
+                ps[2 * ks + dst] = -ps[2 * ks + src];
+            }
+        if (d.pole2)
+            for (int jj = n2; jj < n2 + ng; jj++) {
+                const long dst = cix(d, i, jj + ng, z), src = cix(d, i, 2 * n2 - jj - 1 + ng, zs);
+                copy_cell(d, pv, dst, src);
+                pv[U2 * ks + dst] *= -1.0;
+                pv[U3 * ks + dst] *= -1.0;
+                pv[B2 * ks + dst] *= -1.0;
+                pv[B3 * ks + dst] *= -1.0;
+                ps[0 * ks + dst] = ps[0 * ks + src];
+                ps[2 * ks + dst] = -ps[2 * ks + src];
+            }
+    } else if (d.bc2 == HAMR_BC_POLE_REFL) {
+        const int jref = 2;  // POLEFIX, config.h:490
+        if (d.pole1) {
+            for (int jj = 0; jj < jref; jj++) {
+                const long c = cix(d, i, jj + ng, z), r = cix(d, i, jref + ng, z);
+                pv[U2 * ks + c] = (jj + 0.5) / (jref + 0.5) * pv[U2 * ks + r];
+                pv[RHO * ks + c] = pv[RHO * ks + r];
+                pv[UU * ks + c] = pv[UU * ks + r];
+                pv[U1 * ks + c] = pv[U1 * ks + r];
+                pv[U3 * ks + c] = pv[U3 * ks + r];
+                pv[KTOT * ks + c] = pv[KTOT * ks + r];
+            }
+            for (int g = 1; g <= ng; g++) copy_cell(d, pv, cix(d, i, ng - g, z), cix(d, i, ng + g - 1, z));
+            for (int jj = 0; jj < ng; jj++) {
+                pv[U2 * ks + cix(d, i, jj, z)] *= -1.;
+                pv[B2 * ks + cix(d, i, jj, z)] *= -1.;
+            }
+            for (int g = 1; g <= ng; g++) {
+                ps[0 * ks + cix(d, i, ng - g, z)] = ps[0 * ks + cix(d, i, ng + g - 1, z)];
+                ps[2 * ks + cix(d, i, ng - g, z)] = ps[2 * ks + cix(d, i, ng + g - 1, z)];
+            }
+        }
+        if (d.pole2) {
+            for (int jj = 0; jj < jref; jj++) {
+                const long c = cix(d, i, n2 + ng - 1 - jj, z), r = cix(d, i, n2 + ng - 1 - jref, z);
+                pv[U2 * ks + c] = (jj + 0.5) / (jref + 0.5) * pv[U2 * ks + r];
+                pv[RHO * ks + c] = pv[RHO * ks + r];
+                pv[UU * ks + c] = pv[UU * ks + r];
+                pv[U1 * ks + c] = pv[U1 * ks + r];
+                pv[U3 * ks + c] = pv[U3 * ks + r];
+                pv[KTOT * ks + c] = pv[KTOT * ks + r];
+            }
+            for (int g = 0; g < ng; g++) copy_cell(d, pv, cix(d, i, n2 + ng + g, z), cix(d, i, n2 + ng - 1 - g, z));
+            for (int jj = n2 + ng; jj < n2 + 2 * ng; jj++) {
+                pv[U2 * ks + cix(d, i, jj, z)] *= -1.;
+                pv[B2 * ks + cix(d, i, jj, z)] *= -1.;
+            }
+            for (int g = 0; g < ng; g++) {
+                ps[0 * ks + cix(d, i, n2 + ng + g, z)] = ps[0 * ks + cix(d, i, n2 + ng - 1 - g, z)];
+                ps[2 * ks + cix(d, i, n2 + ng + g, z)] = ps[2 * ks + cix(d, i, n2 + ng - 1 - g, z)];
+            }
+        }
+    } else {
+        for (int g = 0; g < ng; g++) {
+            copy_cell(d, pv, cix(d, i, g, z), cix(d, i, ng, z));
+            copy_cell(d, pv, cix(d, i, n2 + ng + g, z), cix(d, i, n2 + ng - 1, z));
+            ps[0 * ks + cix(d, i, g, z)] = ps[0 * ks + cix(d, i, ng, z)];
+            ps[2 * ks + cix(d, i, g, z)] = ps[2 * ks + cix(d, i, ng, z)];
+            ps[0 * ks + cix(d, i, n2 + ng + g, z)] = ps[0 * ks + cix(d, i, n2 + ng - 1, z)];
+            ps[2 * ks + cix(d, i, n2 + ng + g, z)] = ps[2 * ks + cix(d, i, n2 + ng - 1, z)];
+        }
+    }
+}
+
+// --------------------------------------------------------- step size logic
+constexpr unsigned long long BITS_1E9 = 0x41CDCD6500000000ULL;  // 1.0e9
+
+__global__ void k_dt_reset(unsigned long long *dtbits) {
+    if (threadIdx.x < 4) dtbits[threadIdx.x] = BITS_1E9;
+}
+
+// CFL step 1/(1/dt1 + 1/dt2 + 1/dt3) of the last full sub-step
+// (step_ch.c:1320-1331). In advance mode (dt_state != NULL) the device step
+// size follows min(ndt, 1.3 dt) every `interval` steps (step_ch.c:973-975).
+__global__ void k_dt_finalize(unsigned long long *dtbits, double *ndt_out, double *dt_state, int *counter, int interval) {
+    if (threadIdx.x != 0) return;
+    const double d1 = __longlong_as_double((long long)dtbits[1]);
+    const double d2 = __longlong_as_double((long long)dtbits[2]);
+    const double d3 = __longlong_as_double((long long)dtbits[3]);
+    const double ndt = 1. / (1. / d1 + 1. / d2 + 1. / d3);
+    *ndt_out = ndt;
+    if (dt_state) {
+        const int n = ++(*counter);
+        if (interval <= 1 || n % interval == 0) {
+            double dt = *dt_state;
+            *dt_state = ndt > 1.3 * dt ? 1.3 * dt : ndt;
+        }
+    }
+    dtbits[0] = dtbits[1] = dtbits[2] = dtbits[3] = BITS_1E9;
+}
+
+// |div B| max over active zones (divb_calc, diag.c:153-199)
+__global__ void k_divb(const Dims d, const Geom m, const double *ps, unsigned long long *out) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.;
+    if (t < (long)d.n1 * d.n2 * d.n3) {
+        const int z = d.ng3 + (int)(t % d.n3);
+        const int j = d.ng2 + (int)((t / d.n3) % d.n2);
+        const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
+        const long c = cix(d, i, j, z), ks = d.ks;
+        double divb = 0.;
+        if (d.d1) divb += 0.25 * (ps[0 * ks + c + (long)d.G2 * d.G3] * m.gdet[FACE1 * d.gs + gix(d, i + 1, j)] - ps[0 * ks + c] * m.gdet[FACE1 * d.gs + gix(d, i, j)]) / d.dx1;
+        if (d.d2) divb += 0.25 * (ps[1 * ks + c + d.G3] * m.gdet[FACE2 * d.gs + gix(d, i, j + 1)] - ps[1 * ks + c] * m.gdet[FACE2 * d.gs + gix(d, i, j)]) / d.dx2;
+        if (d.d3) divb += 0.25 * (ps[2 * ks + c + 1] * m.gdet[FACE3 * d.gs + gix(d, i, j)] - ps[2 * ks + c] * m.gdet[FACE3 * d.gs + gix(d, i, j)]) / d.dx3;
+        v = fabs(divb);
+    }
+    for (int o = 16; o > 0; o >>= 1) v = d_max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
+}
+
+inline unsigned nblk(long n) { return (unsigned)((n + BLK - 1) / BLK); }
+
+}  // namespace
+
+// ===========================================================================
+struct hamr_ctx {
+    hamr_params prm;
+    Dims d;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    bool have_geom = false;
+    std::string err;
+    // device state
+    double *p = nullptr, *ph = nullptr, *ps = nullptr, *psh = nullptr, *U = nullptr;
+    double *F1 = nullptr, *F2 = nullptr, *F3 = nullptr, *Ec = nullptr, *emf = nullptr;
+    int *pflag = nullptr, *failimage = nullptr;
+    double *gcov = nullptr, *gcon = nullptr, *gdet = nullptr, *conn = nullptr;
+    unsigned long long *dtbits = nullptr;
+    double *ndt = nullptr, *dt_state = nullptr;
+    int *counter = nullptr;
+    unsigned long long *divb = nullptr;
+    // captured advance graphs
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = -1, graph_interval = -1;
+};
+
+namespace {
+
+int fail_cuda(hamr_ctx *c, cudaError_t e, const char *what) {
+    c->err = std::string(what) + ": " + cudaGetErrorString(e);
+    return HAMR_E_CUDA;
+}
+
+#define CK(call)                                              \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return fail_cuda(ctx, e_, #call); \
+    } while (0)
+
+Geom geom_of(const hamr_ctx *c) { return Geom{c->gcov, c->gcon, c->gdet, c->conn}; }
+
+// kernel groups timed by hamr_profile_step
+enum { PROF_FLUX3, PROF_FLUX2, PROF_FLUX1, PROF_FIXFLUX, PROF_EMF_CENTRE, PROF_EMF_EDGE, PROF_POLE_AVG,
+       PROF_FACE, PROF_UPDATE, PROF_BOUND, PROF_NSLOT };
+
+struct Prof {
+    cudaEvent_t ev[PROF_NSLOT + 1];
+    bool on = false;
+};
+
+inline void prof_mark(Prof *pf, int slot, cudaStream_t s) {
+    if (pf && pf->on) cudaEventRecord(pf->ev[slot + 1], s);
+}
+
+// one sub-step: fluxes, CT, update, ghost fill of the written state
+int launch_stage(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf = nullptr) {
+    const Dims &d = ctx->d;
+    const Geom m = geom_of(ctx);
+    cudaStream_t s = ctx->stream;
+    const double *pin = full ? ctx->ph : ctx->p;
+    const double *psin = full ? ctx->psh : ctx->ps;
+    const int cd = calc_dt ? 1 : 0;
+    if (d.d3) {
+        long n = (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3 - 1);
+        k_flux<3><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, ctx->F3, ctx->dtbits, cd);
+    }
+    prof_mark(pf, PROF_FLUX3, s);
+    {
+        long n = (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2 - 1) * (d.n3 + 2 * d.d3);
+        k_flux<2><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, ctx->F2, ctx->dtbits, cd);
+    }
+    prof_mark(pf, PROF_FLUX2, s);
+    {
+        long n = (long)(d.n1 + 2 * d.d1 - 1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3);
+        k_flux<1><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, ctx->F1, ctx->dtbits, cd);
+    }
+    prof_mark(pf, PROF_FLUX1, s);
+    if (d.bc2 == HAMR_BC_POLE_REFL) {
+        long n = (long)d.G1 * d.G3 + (long)d.G2 * d.G3;
+        k_fix_flux<<<nblk(n), BLK, 0, s>>>(d, ctx->F1, ctx->F2, ctx->F3);
+    }
+    prof_mark(pf, PROF_FIXFLUX, s);
+    {
+        long n = (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3);
+        k_emf_centre<<<nblk(n), BLK, 0, s>>>(d, m, pin, ctx->Ec);
+    }
+    prof_mark(pf, PROF_EMF_CENTRE, s);
+    {
+        long n = (long)(d.n1 + d.d1) * (d.n2 + d.d2) * (d.n3 + d.d3);
+        k_emf_edge<<<nblk(n), BLK, 0, s>>>(d, ctx->Ec, ctx->F1, ctx->F2, ctx->F3, ctx->emf);
+        prof_mark(pf, PROF_EMF_EDGE, s);
+        if (d.bc2 == HAMR_BC_POLE_TRANS)
+            k_pole_average<<<nblk(2L * (d.n1 + d.ng1)), BLK, 0, s>>>(d, ctx->emf, st);
+        prof_mark(pf, PROF_POLE_AVG, s);
+        k_face_update<<<nblk(n), BLK, 0, s>>>(d, m, ctx->ps, full ? ctx->ps : ctx->psh, ctx->emf, st);
+        prof_mark(pf, PROF_FACE, s);
+    }
+    {
+        long n = (long)d.n1 * d.n2 * d.n3;
+        k_update<<<nblk(n), BLK, 0, s>>>(d, m, ctx->p, full ? ctx->ph : ctx->p, full ? ctx->p : ctx->ph, ctx->U,
+                                        full ? ctx->ps : ctx->psh, ctx->F1, ctx->F2, ctx->F3, ctx->pflag,
+                                        ctx->failimage, full, st);
+    }
+    prof_mark(pf, PROF_UPDATE, s);
+    double *pw = full ? ctx->p : ctx->ph;
+    double *psw = full ? ctx->ps : ctx->psh;
+    if (d.d1) k_bound_x1<<<nblk((long)d.ng1 * d.G2 * d.G3), BLK, 0, s>>>(d, m, pw, psw);
+    if (d.d3) k_bound_x3<<<nblk((long)d.ng3 * d.G1 * d.G2), BLK, 0, s>>>(d, pw, psw);
+    if (d.d2) k_bound_x2<<<nblk((long)d.G1 * d.G3), BLK, 0, s>>>(d, pw, psw);
+    prof_mark(pf, PROF_BOUND, s);
+    CK(cudaGetLastError());
+    return HAMR_OK;
+}
+
+int launch_step(hamr_ctx *ctx, StepSize half, StepSize full, double *dt_state, int interval) {
+    int rc = launch_stage(ctx, 0, half, false);
+    if (rc) return rc;
+    rc = launch_stage(ctx, 1, full, true);
+    if (rc) return rc;
+    k_dt_finalize<<<1, 32, 0, ctx->stream>>>(ctx->dtbits, ctx->ndt, dt_state, ctx->counter, interval);
+    CK(cudaGetLastError());
+    return HAMR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
+    if (!prm || !out) return HAMR_E_ARG;
+    *out = nullptr;
+    if (prm->n1 < 2 || prm->n2 < 2 || prm->n3 < 1 || prm->ng != 3) return HAMR_E_ARG;
+    if (prm->precision != HAMR_FP64) return HAMR_E_ARG;
+    if (prm->n3 > 1 && prm->bc3 != HAMR_BC_PERIODIC) return HAMR_E_ARG;
+    if (prm->bc2 == HAMR_BC_POLE_TRANS && (prm->n3 < 2 || prm->n3 % 2)) return HAMR_E_ARG;
+    if (!(prm->gam > 1.0) || !(prm->cour > 0.0) || !(prm->dx1 > 0) || !(prm->dx2 > 0) || !(prm->dx3 > 0)) return HAMR_E_ARG;
+    hamr_ctx *ctx = new hamr_ctx();
+    ctx->prm = *prm;
+    Dims &d = ctx->d;
+    d.n1 = prm->n1; d.n2 = prm->n2; d.n3 = prm->n3;
+    d.d1 = d.n1 > 1; d.d2 = d.n2 > 1; d.d3 = d.n3 > 1;
+    d.ng1 = d.d1 ? prm->ng : 0; d.ng2 = d.d2 ? prm->ng : 0; d.ng3 = d.d3 ? prm->ng : 0;
+    d.G1 = d.n1 + 2 * d.ng1; d.G2 = d.n2 + 2 * d.ng2; d.G3 = d.n3 + 2 * d.ng3;
+    const long ncell = (long)d.G1 * d.G2 * d.G3, ngeo = (long)d.G1 * d.G2;
+    d.ks = prm->ksize ? prm->ksize : ncell + (64 - ncell % 64);
+    d.gs = prm->gsize ? prm->gsize : ngeo + (64 - ngeo % 64);
+    if (d.ks < ncell || d.gs < ngeo) { delete ctx; return HAMR_E_ARG; }
+    d.dx1 = prm->dx1; d.dx2 = prm->dx2; d.dx3 = prm->dx3;
+    d.gam = prm->gam; d.cour = prm->cour;
+    d.pole1 = prm->pole1; d.pole2 = prm->pole2;
+    d.bc1 = prm->bc1; d.bc2 = prm->bc2; d.bc3 = prm->bc3;
+    d.ct_upwind = prm->ct_upwind;
+    if (prm->stream) {
+        ctx->stream = (cudaStream_t)prm->stream;
+    } else {
+        cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { delete ctx; return HAMR_E_CUDA; }
+        ctx->own_stream = true;
+    }
+    const size_t cb = sizeof(double) * d.ks;
+    struct A { void **p; size_t n; } allocs[] = {
+        {(void **)&ctx->p, NPR * cb}, {(void **)&ctx->ph, NPR * cb}, {(void **)&ctx->ps, 3 * cb},
+        {(void **)&ctx->psh, 3 * cb}, {(void **)&ctx->U, NPR * cb}, {(void **)&ctx->F1, NPR * cb},
+        {(void **)&ctx->F2, NPR * cb}, {(void **)&ctx->F3, NPR * cb}, {(void **)&ctx->Ec, 4 * cb},
+        {(void **)&ctx->emf, 4 * cb}, {(void **)&ctx->pflag, sizeof(int) * d.ks},
+        {(void **)&ctx->failimage, 4 * sizeof(int) * d.ks},
+        {(void **)&ctx->gcov, 50 * sizeof(double) * d.gs}, {(void **)&ctx->gcon, 50 * sizeof(double) * d.gs},
+        {(void **)&ctx->gdet, 5 * sizeof(double) * d.gs}, {(void **)&ctx->conn, 40 * sizeof(double) * d.gs},
+        {(void **)&ctx->dtbits, 4 * sizeof(unsigned long long)}, {(void **)&ctx->ndt, sizeof(double)},
+        {(void **)&ctx->dt_state, sizeof(double)}, {(void **)&ctx->counter, sizeof(int)},
+        {(void **)&ctx->divb, sizeof(unsigned long long)}};
+    for (auto &a : allocs) {
+        if (cudaMalloc(a.p, a.n) != cudaSuccess) {
+            hamr_ctx_destroy(ctx);
+            return HAMR_E_NOMEM;
+        }
+        cudaMemsetAsync(*a.p, 0, a.n, ctx->stream);
+    }
+    k_dt_reset<<<1, 32, 0, ctx->stream>>>(ctx->dtbits);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        hamr_ctx_destroy(ctx);
+        return HAMR_E_CUDA;
+    }
+    *out = ctx;
+    return HAMR_OK;
+}
+
+int hamr_ctx_destroy(hamr_ctx *ctx) {
+    if (!ctx) return HAMR_E_ARG;
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
+    void *bufs[] = {ctx->p, ctx->ph, ctx->ps, ctx->psh, ctx->U, ctx->F1, ctx->F2, ctx->F3, ctx->Ec, ctx->emf,
+                    ctx->pflag, ctx->failimage, ctx->gcov, ctx->gcon, ctx->gdet, ctx->conn, ctx->dtbits,
+                    ctx->ndt, ctx->dt_state, ctx->counter, ctx->divb};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return HAMR_OK;
+}
+
+const char *hamr_last_error(const hamr_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int hamr_strides(const hamr_ctx *ctx, long *ksize, long *gsize) {
+    if (!ctx) return HAMR_E_ARG;
+    if (ksize) *ksize = ctx->d.ks;
+    if (gsize) *gsize = ctx->d.gs;
+    return HAMR_OK;
+}
+
+int hamr_set_geometry(hamr_ctx *ctx, const double *gcov, const double *gcon, const double *gdet, const double *conn) {
+    if (!ctx || !gcov || !gcon || !gdet || !conn) return HAMR_E_ARG;
+    const size_t g = sizeof(double) * ctx->d.gs;
+    CK(cudaMemcpyAsync(ctx->gcov, gcov, 50 * g, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->gcon, gcon, 50 * g, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->gdet, gdet, 5 * g, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->conn, conn, 40 * g, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->have_geom = true;
+    return HAMR_OK;
+}
+
+int hamr_upload(hamr_ctx *ctx, const double *p, const double *ps) {
+    if (!ctx || !p || !ps) return HAMR_E_ARG;
+    const size_t cb = sizeof(double) * ctx->d.ks;
+    CK(cudaMemcpyAsync(ctx->p, p, NPR * cb, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->ps, ps, 3 * cb, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return HAMR_OK;
+}
+
+int hamr_download(hamr_ctx *ctx, double *p, double *ps) {
+    if (!ctx) return HAMR_E_ARG;
+    const size_t cb = sizeof(double) * ctx->d.ks;
+    if (p) CK(cudaMemcpyAsync(p, ctx->p, NPR * cb, cudaMemcpyDeviceToHost, ctx->stream));
+    if (ps) CK(cudaMemcpyAsync(ps, ctx->ps, 3 * cb, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return HAMR_OK;
+}
+
+int hamr_download_flags(hamr_ctx *ctx, int *pflag, int *failimage) {
+    if (!ctx) return HAMR_E_ARG;
+    const size_t ib = sizeof(int) * ctx->d.ks;
+    if (pflag) CK(cudaMemcpyAsync(pflag, ctx->pflag, ib, cudaMemcpyDeviceToHost, ctx->stream));
+    if (failimage) CK(cudaMemcpyAsync(failimage, ctx->failimage, 4 * ib, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return HAMR_OK;
+}
+
+int hamr_bound(hamr_ctx *ctx) {
+    if (!ctx) return HAMR_E_ARG;
+    if (!ctx->have_geom) return HAMR_E_STATE;
+    const Dims &d = ctx->d;
+    const Geom m = geom_of(ctx);
+    if (d.d1) k_bound_x1<<<nblk((long)d.ng1 * d.G2 * d.G3), BLK, 0, ctx->stream>>>(d, m, ctx->p, ctx->ps);
+    if (d.d3) k_bound_x3<<<nblk((long)d.ng3 * d.G1 * d.G2), BLK, 0, ctx->stream>>>(d, ctx->p, ctx->ps);
+    if (d.d2) k_bound_x2<<<nblk((long)d.G1 * d.G3), BLK, 0, ctx->stream>>>(d, ctx->p, ctx->ps);
+    CK(cudaGetLastError());
+    return HAMR_OK;
+}
+
+int hamr_stage(hamr_ctx *ctx, int full, double Dt, double dt) {
+    if (!ctx) return HAMR_E_ARG;
+    if (!ctx->have_geom) return HAMR_E_STATE;
+    if (!(Dt > 0) || !(dt > 0)) return HAMR_E_ARG;
+    StepSize st{nullptr, 0., Dt, dt};
+    if (full) k_dt_reset<<<1, 32, 0, ctx->stream>>>(ctx->dtbits);
+    return launch_stage(ctx, full ? 1 : 0, st, full != 0);
+}
+
+int hamr_step(hamr_ctx *ctx, double dt, double *dt_next) {
+    if (!ctx) return HAMR_E_ARG;
+    if (!ctx->have_geom) return HAMR_E_STATE;
+    if (!(dt > 0)) return HAMR_E_ARG;
+    k_dt_reset<<<1, 32, 0, ctx->stream>>>(ctx->dtbits);
+    int rc = launch_step(ctx, StepSize{nullptr, 0.5, 0.5 * dt, dt}, StepSize{nullptr, 1.0, dt, dt}, nullptr, 0);
+    if (rc) return rc;
+    if (dt_next) {
+        CK(cudaMemcpyAsync(dt_next, ctx->ndt, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (!(*dt_next > 0) || !isfinite(*dt_next)) {
+            ctx->err = "non-finite or non-positive CFL step";
+            return HAMR_E_PHYSICS;
+        }
+    }
+    return HAMR_OK;
+}
+
+int hamr_advance(hamr_ctx *ctx, int nsteps, int interval, double *dt_inout) {
+    if (!ctx || !dt_inout || nsteps < 1 || interval < 1) return HAMR_E_ARG;
+    if (!ctx->have_geom) return HAMR_E_STATE;
+    if (!(*dt_inout > 0)) return HAMR_E_ARG;
+    CK(cudaMemcpyAsync(ctx->dt_state, dt_inout, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(ctx->counter, 0, sizeof(int), ctx->stream));
+    k_dt_reset<<<1, 32, 0, ctx->stream>>>(ctx->dtbits);
+    if (!ctx->graph || ctx->graph_steps != nsteps || ctx->graph_interval != interval) {
+        if (ctx->graph) {
+            cudaGraphExecDestroy(ctx->graph);
+            ctx->graph = nullptr;
+        }
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = HAMR_OK;
+        for (int n = 0; n < nsteps && rc == HAMR_OK; n++)
+            rc = launch_step(ctx, StepSize{ctx->dt_state, 0.5, 0., 0.}, StepSize{ctx->dt_state, 1.0, 0., 0.},
+                             ctx->dt_state, interval);
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+        if (rc) return rc;
+        if (e != cudaSuccess) return fail_cuda(ctx, e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&ctx->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail_cuda(ctx, e, "cudaGraphInstantiate");
+        ctx->graph_steps = nsteps;
+        ctx->graph_interval = interval;
+    }
+    CK(cudaGraphLaunch(ctx->graph, ctx->stream));
+    CK(cudaMemcpyAsync(dt_inout, ctx->dt_state, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return HAMR_OK;
+}
+
+int hamr_profile_step(hamr_ctx *ctx, double dt, int reps, double *ms, int nslots) {
+    if (!ctx || !ms || reps < 1 || nslots < PROF_NSLOT) return HAMR_E_ARG;
+    if (!ctx->have_geom) return HAMR_E_STATE;
+    Prof pf;
+    for (auto &e : pf.ev) CK(cudaEventCreate(&e));
+    pf.on = true;
+    for (int k = 0; k < nslots; k++) ms[k] = 0.;
+    int rc = HAMR_OK;
+    for (int r = 0; r < reps && rc == HAMR_OK; r++) {
+        for (int stage = 0; stage < 2 && rc == HAMR_OK; stage++) {
+            k_dt_reset<<<1, 32, 0, ctx->stream>>>(ctx->dtbits);
+            StepSize st{nullptr, 0., stage ? dt : 0.5 * dt, dt};
+            // every group records its end mark, launched or not, so
+            // consecutive marks bracket exactly one group
+            cudaEventRecord(pf.ev[0], ctx->stream);
+            rc = launch_stage(ctx, stage, st, stage == 1, &pf);
+            if (rc) break;
+            if (cudaEventSynchronize(pf.ev[PROF_NSLOT]) != cudaSuccess) { rc = HAMR_E_CUDA; break; }
+            for (int k = 0; k < PROF_NSLOT; k++) {
+                float t = 0.f;
+                cudaEventElapsedTime(&t, pf.ev[k], pf.ev[k + 1]);
+                ms[k] += t / reps;
+            }
+        }
+    }
+    for (auto &e : pf.ev) cudaEventDestroy(e);
+    return rc;
+}
+
+int hamr_device_state(hamr_ctx *ctx, double **p, double **ps, double **ph, double **psh) {
+    if (!ctx) return HAMR_E_ARG;
+    if (p) *p = ctx->p;
+    if (ps) *ps = ctx->ps;
+    if (ph) *ph = ctx->ph;
+    if (psh) *psh = ctx->psh;
+    return HAMR_OK;
+}
+
+int hamr_divb_max(hamr_ctx *ctx, double *out) {
+    if (!ctx || !out) return HAMR_E_ARG;
+    if (!ctx->have_geom) return HAMR_E_STATE;
+    const Dims &d = ctx->d;
+    CK(cudaMemsetAsync(ctx->divb, 0, sizeof(unsigned long long), ctx->stream));
+    k_divb<<<nblk((long)d.n1 * d.n2 * d.n3), BLK, 0, ctx->stream>>>(d, geom_of(ctx), ctx->ps, ctx->divb);
+    CK(cudaGetLastError());
+    unsigned long long bits = 0;
+    CK(cudaMemcpyAsync(&bits, ctx->divb, sizeof(bits), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    memcpy(out, &bits, sizeof(double));
+    return HAMR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,548 @@
+// Per-cell ideal-GRMHD physics for the sm_100a kernels: metric algebra, fluid
+// state, fluxes and fast speeds, PPM reconstruction, geometric source and the
+// primitive-variable inversion chain. Templated on the arithmetic type so the
+// mixed-precision step can run reconstruction/flux/EMF in float.
+//
+// Expression shapes follow the reference device code so that a build without
+// FMA contraction reproduces it to the last bit (apart from pow(), whose CUDA
+// and C-library roundings may differ by one ulp):
+//   lower/raise                    GPU_metric.h:3-34
+//   gamma/ucon/bcon/get_state      GPU_phys_mhd.h:672-761
+//   primtoflux (+ fast speeds)     GPU_phys_mhd.h:432-628
+//   calc_entropy                   GPU_phys_mhd.h:631-670
+//   para (PPM, MC-2 slopes)        GPU_interp.h:60-111
+//   source                         GPU_phys_mhd.h:34-175
+//   Utoprim_2d + Noble Newton      GPU_utoprim_2d.h
+//   Utoprim_1dvsq2fix1             GPU_utoprim_1dvsq2fix1.h
+//   Utoprim_1dfix1                 GPU_utoprim_1dfix1.h
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+namespace hamr {
+
+enum { RHO = 0, UU = 1, U1 = 2, U2 = 3, U3 = 4, B1 = 5, B2 = 6, B3 = 7, KTOT = 8, NPR = 9 };
+enum { FACE1 = 0, FACE2 = 1, CORN = 2, CENT = 3, FACE3 = 4 };
+
+constexpr double SMALL_D = 1.e-20;
+constexpr double NEWT_TOL = 1.0e-10;
+constexpr double MIN_NEWT_TOL = 1.0e-10;
+constexpr int MAX_NEWT_ITER = 30;
+constexpr int EXTRA_NEWT_ITER = 2;
+constexpr double W_TOO_BIG = 1.e20;
+constexpr double UTSQ_TOO_BIG = 1.e20;
+constexpr double FAIL_VAL = 1.e30;
+
+template <typename T>
+struct Geo {
+    T gcov[10], gcon[10], g;
+};
+
+template <typename T>
+struct State {
+    T ucon[4], ucov[4], bcon[4], bcov[4];
+};
+
+template <typename T> __device__ __forceinline__ T d_sqrt(T x);
+template <> __device__ __forceinline__ double d_sqrt<double>(double x) { return sqrt(x); }
+template <> __device__ __forceinline__ float d_sqrt<float>(float x) { return sqrtf(x); }
+template <typename T> __device__ __forceinline__ T d_pow(T x, T y);
+template <> __device__ __forceinline__ double d_pow<double>(double x, double y) { return pow(x, y); }
+template <> __device__ __forceinline__ float d_pow<float>(float x, float y) { return powf(x, y); }
+template <typename T> __device__ __forceinline__ T d_fabs(T x) { return x < T(0) ? -x : x; }
+template <typename T> __device__ __forceinline__ T d_max(T a, T b) { return a > b ? a : b; }
+template <typename T> __device__ __forceinline__ T d_min(T a, T b) { return a < b ? a : b; }
+
+template <typename T>
+__device__ __forceinline__ void lower4(const T *u, const T *g, T *o) {
+    o[0] = g[0] * u[0] + g[1] * u[1] + g[2] * u[2] + g[3] * u[3];
+    o[1] = g[1] * u[0] + g[4] * u[1] + g[5] * u[2] + g[6] * u[3];
+    o[2] = g[2] * u[0] + g[5] * u[1] + g[7] * u[2] + g[8] * u[3];
+    o[3] = g[3] * u[0] + g[6] * u[1] + g[8] * u[2] + g[9] * u[3];
+}
+template <typename T>
+__device__ __forceinline__ void raise4(const T *u, const T *g, T *o) { lower4(u, g, o); }
+
+template <typename T>
+__device__ __forceinline__ T dot4(const T *a, const T *b) {
+    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3];
+}
+
+template <typename T>
+__device__ __forceinline__ void gamma_calc(const T *pr, const Geo<T> &gm, T *gamma) {
+    const T *g = gm.gcov;
+    T qsq = g[4] * pr[U1] * pr[U1] + g[7] * pr[U2] * pr[U2] + g[9] * pr[U3] * pr[U3]
+          + T(2.) * (g[5] * pr[U1] * pr[U2] + g[6] * pr[U1] * pr[U3] + g[8] * pr[U2] * pr[U3]);
+    if (qsq < T(0.)) {
+        if (d_fabs(qsq) > T(1.E-10)) { *gamma = T(1.); return; }
+        qsq = T(1.E-10);
+    }
+    *gamma = d_sqrt(T(1.) + qsq);
+}
+
+template <typename T>
+__device__ __forceinline__ void ucon_calc(const T *pr, const Geo<T> &gm, T *ucon) {
+    T alpha = T(1.) / d_sqrt(-gm.gcon[0]);
+    T beta[4], gamma;
+#pragma unroll
+    for (int j = 1; j < 4; j++) beta[j] = gm.gcon[j] * alpha * alpha;
+    gamma_calc(pr, gm, &gamma);
+    ucon[0] = gamma / alpha;
+#pragma unroll
+    for (int j = 1; j < 4; j++) ucon[j] = pr[U1 + j - 1] - gamma * beta[j] / alpha;
+}
+
+template <typename T>
+__device__ __forceinline__ void bcon_calc(const T *pr, const T *ucon, const T *ucov, T *bcon) {
+    bcon[0] = pr[B1] * ucov[1] + pr[B2] * ucov[2] + pr[B3] * ucov[3];
+#pragma unroll
+    for (int j = 1; j < 4; j++) bcon[j] = (pr[B1 - 1 + j] + bcon[0] * ucon[j]) / ucon[0];
+}
+
+template <typename T>
+__device__ __forceinline__ void get_state(const T *pr, const Geo<T> &gm, State<T> &q) {
+    ucon_calc(pr, gm, q.ucon);
+    lower4(q.ucon, gm.gcov, q.ucov);
+    bcon_calc(pr, q.ucon, q.ucov, q.bcon);
+    lower4(q.bcon, gm.gcov, q.bcov);
+}
+
+template <typename T>
+__device__ __forceinline__ T entropy(T gam, const T *pr) {
+    T P = (gam - T(1.0)) * pr[UU];
+    return P * d_pow(pr[RHO], -gam);
+}
+
+// Fluxes in direction dir (dir == 0: conserved variables); with dir != 0 the
+// fast magnetosonic speeds along dir as well. `ent` is the entropy K of pr,
+// computed once per state by the caller.
+template <typename T>
+__device__ __forceinline__ void primtoflux(T gam, const T *pr, const State<T> &q, int dir, const Geo<T> &gm,
+                                           T ent, T *flux, T *vmax, T *vmin) {
+    T mhd[4];
+    T u = pr[UU];
+    T P = (gam - T(1.)) * u;
+    T w = pr[RHO] + P + u;
+    T bsq = dot4(q.bcon, q.bcov);
+    T eta = w + bsq;
+    T ptot = P + T(0.5) * bsq;
+    flux[RHO] = pr[RHO] * q.ucon[dir];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        mhd[j] = eta * q.ucon[dir] * q.ucov[j] + ptot * (dir == j ? T(1.) : T(0.)) - q.bcon[dir] * q.bcov[j];
+    flux[UU] = mhd[0] + flux[RHO];
+    flux[U1] = mhd[1];
+    flux[U2] = mhd[2];
+    flux[U3] = mhd[3];
+    flux[B1] = q.bcon[1] * q.ucon[dir] - q.bcon[dir] * q.ucon[1];
+    flux[B2] = q.bcon[2] * q.ucon[dir] - q.bcon[dir] * q.ucon[2];
+    flux[B3] = q.bcon[3] * q.ucon[dir] - q.bcon[dir] * q.ucon[3];
+    flux[KTOT] = flux[RHO] * ent;
+#pragma unroll
+    for (int k = 0; k < NPR; k++) flux[k] *= gm.g;
+    if (dir != 0) {
+        T Acon_0, Acon_js;
+        if (dir == 1) { Acon_0 = gm.gcon[1]; Acon_js = gm.gcon[4]; }
+        else if (dir == 2) { Acon_0 = gm.gcon[2]; Acon_js = gm.gcon[7]; }
+        else { Acon_0 = gm.gcon[3]; Acon_js = gm.gcon[9]; }
+        T cs2 = gam * (gam - T(1.)) * pr[UU] / w;
+        T va2 = bsq / eta;
+        T cms2 = cs2 + va2 - cs2 * va2;
+        if (cms2 < T(0.)) cms2 = T(SMALL_D);
+        if (cms2 > T(1.)) cms2 = T(1.);
+        T Asq = Acon_js, Bsq = gm.gcon[0];
+        T Au = q.ucon[dir], Bu = q.ucon[0], AB = Acon_0;
+        T Au2 = Au * Au, Bu2 = Bu * Bu, AuBu = Au * Bu;
+        T A = Bu2 - (Bsq + Bu2) * cms2;
+        T B = T(2.) * (AuBu - (AB + AuBu) * cms2);
+        T C = Au2 - (Asq + Au2) * cms2;
+        T discr = B * B - T(4.) * A * C;
+        if ((discr < T(0.0)) && (discr > T(-1.e-10))) discr = T(0.0);
+        else if (discr < T(-1.e-10)) discr = T(0.);
+        discr = d_sqrt(discr);
+        T vp = -(-B + discr) / (T(2.) * A);
+        T vm = -(-B - discr) / (T(2.) * A);
+        *vmax = d_max(vp, vm);
+        *vmin = d_min(vp, vm);
+    }
+}
+
+// PPM face values of the middle of five zones: l = lower edge, r = upper edge
+template <typename T>
+__device__ __forceinline__ void para(const T *y, T &lout, T &rout) {
+    T dq[5];
+#pragma unroll
+    for (int i = 1; i < 4; i++) {
+        T Dqm = T(2.) * (y[i] - y[i - 1]);
+        T Dqp = T(2.) * (y[i + 1] - y[i]);
+        T Dqc = T(0.5) * (y[i + 1] - y[i - 1]);
+        T aDqm = d_fabs(Dqm), aDqp = d_fabs(Dqp), aDqc = d_fabs(Dqc);
+        T s = Dqm * Dqp;
+        Dqm = d_min(aDqm, aDqp);
+        if (aDqc < Dqm) {
+            if (Dqc > T(0.)) dq[i] = (aDqc) * (T)(s > T(0.));
+            else dq[i] = (-aDqc) * (T)(s > T(0.));
+        } else {
+            if (Dqc > T(0.)) dq[i] = (Dqm) * (T)(s > T(0.));
+            else dq[i] = (-Dqm) * (T)(s > T(0.));
+        }
+    }
+    T l = T(0.5) * (y[2] + y[1]) - (dq[2] - dq[1]) / T(6.0);
+    T r = T(0.5) * (y[3] + y[2]) - (dq[3] - dq[2]) / T(6.0);
+    T qa = (r - y[2]) * (y[2] - l);
+    T qd = (r - l);
+    T qe = T(6.0) * (y[2] - T(0.5) * (l + r));
+    if (qa <= T(0.)) { l = y[2]; r = y[2]; }
+    if (qd * (qd - qe) < T(0.0)) l = T(3.0) * y[2] - T(2.0) * r;
+    else if (qd * (qd + qe) < T(0.0)) r = T(3.0) * y[2] - T(2.0) * l;
+    lout = l;
+    rout = r;
+}
+
+// ---------------------------------------------------------------- inversion
+struct InvQ {
+    double Bcon[4], Qcon[4], ncon[4], Bsq, QdotB, QdotBsq, Qtsq, Qdotn, D;
+};
+
+__device__ __forceinline__ void inv_scalars(const double *U, const double *gcov, const double *gcon, InvQ &s) {
+    double Bcov[4], Qcov[4], Qsq, ncov;
+    s.Bcon[0] = 0.;
+    for (int i = 1; i < 4; i++) s.Bcon[i] = U[B1 + i - 1];
+    lower4(s.Bcon, gcov, Bcov);
+    for (int i = 0; i < 4; i++) Qcov[i] = U[UU + i];
+    raise4(Qcov, gcon, s.Qcon);
+    s.Bsq = 0.;
+    for (int i = 1; i < 4; i++) s.Bsq += s.Bcon[i] * Bcov[i];
+    s.QdotB = 0.;
+    for (int i = 0; i < 4; i++) s.QdotB += Qcov[i] * s.Bcon[i];
+    s.QdotBsq = s.QdotB * s.QdotB;
+    ncov = -sqrt(-1. / gcon[0]);
+    s.ncon[0] = gcon[0] * ncov;
+    s.ncon[1] = gcon[1] * ncov;
+    s.ncon[2] = gcon[2] * ncov;
+    s.ncon[3] = gcon[3] * ncov;
+    s.Qdotn = s.Qcon[0] * ncov;
+    Qsq = 0.;
+    for (int i = 0; i < 4; i++) Qsq += Qcov[i] * s.Qcon[i];
+    s.Qtsq = Qsq + s.Qdotn * s.Qdotn;
+    s.D = U[RHO];
+}
+
+__device__ __forceinline__ int guess_utsq(const double *gcov, const double *prim, double *out) {
+    double utsq = gcov[4] * prim[U1] * prim[U1];
+    utsq += 2. * gcov[5] * prim[U2] * prim[U1];
+    utsq += 2. * gcov[6] * prim[U3] * prim[U1];
+    utsq += gcov[7] * prim[U2] * prim[U2];
+    utsq += 2 * gcov[8] * prim[U3] * prim[U2];
+    utsq += gcov[9] * prim[U3] * prim[U3];
+    if ((utsq < 0.) && (fabs(utsq) < 1.0e-13)) utsq = fabs(utsq);
+    if (utsq < 0. || utsq > UTSQ_TOO_BIG) return 2;
+    *out = utsq;
+    return 0;
+}
+
+__device__ __forceinline__ void set_velocity(const InvQ &s, double gamma, double W, double *prim) {
+    for (int i = 1; i < 4; i++) {
+        double Qtcon = s.Qcon[i] + s.ncon[i] * s.Qdotn;
+        prim[U1 + i - 1] = gamma / (W + s.Bsq) * (Qtcon + s.QdotB * s.Bcon[i] / W);
+    }
+}
+
+__device__ __forceinline__ int inv_prologue(const double *U, double gdet, const double *gcon, double *prim, double *Ut) {
+    if (U[0] <= 0.) return -100;
+    for (int i = B1; i <= B3; i++) prim[i] = U[i] / gdet;
+    double alpha = 1.0 / sqrt(-gcon[0]);
+    Ut[RHO] = alpha * U[RHO] / gdet;
+    Ut[UU] = alpha * (U[UU] - U[RHO]) / gdet;
+    for (int i = U1; i <= U3; i++) Ut[i] = alpha * U[i] / gdet;
+    for (int i = B1; i <= B3; i++) Ut[i] = alpha * U[i] / gdet;
+    return 0;
+}
+
+__device__ __forceinline__ double vsq_of_W(double W, double Bsq, double Qtsq, double QdotBsq) {
+    double Wsq = W * W;
+    double Xsq = (Bsq + W) * (Bsq + W);
+    return (Wsq * Qtsq + QdotBsq * (Bsq + 2. * W)) / (Wsq * Xsq);
+}
+
+// Noble et al. 2006, 2D Newton-Raphson on (W, v^2)
+__device__ __noinline__ int utoprim_2d(double gam, const double *U, const double *gcov, const double *gcon, double gdet, double *prim) {
+    double Ut[NPR], pt[5];
+    int ret = inv_prologue(U, gdet, gcon, prim, Ut);
+    if (ret) return ret;
+    for (int i = 0; i < B1; i++) pt[i] = prim[i];
+    InvQ s;
+    inv_scalars(Ut, gcov, gcon, s);
+    double utsq;
+    if (guess_utsq(gcov, pt, &utsq)) return 2;
+    double gammasq = 1. + utsq;
+    double gamma = sqrt(gammasq);
+    double rho0 = s.D / gamma;
+    double u = pt[UU];
+    double p = (gam - 1.) * u;
+    double w = rho0 + u + p;
+    double W_last = w * gammasq;
+    int i_increase = 0;
+    while (((W_last * W_last * W_last * (W_last + 2. * s.Bsq) - s.QdotBsq * (2. * W_last + s.Bsq)) <= W_last * W_last * (s.Qtsq - s.Bsq * s.Bsq)) && (i_increase < 10)) {
+        W_last *= 10.;
+        i_increase++;
+    }
+    double x0 = fabs(W_last);
+    double vs = fabs(vsq_of_W(W_last, s.Bsq, s.Qtsq, s.QdotBsq));
+    double x1 = (vs > 1.) ? (1.0 - 1.e-15) : vs;
+    // Newton iterations (general_newton_raphson, func_vsq)
+    double f = 1., df = 1., errx = 1.;
+    int n_iter = 0, i_extra = 0, doing_extra = 0, keep = 1;
+    const double Bsq = s.Bsq, Qtsq = s.Qtsq, QdotBsq = s.QdotBsq, Qdotn = s.Qdotn, D = s.D;
+    while (keep) {
+        double Wsq = x0 * x0;
+        double gtmp = 1. - x1;
+        double p_tmp = (gam - 1.) * (fma(x0, gtmp, -D * sqrt(gtmp))) / gam;
+        double dPdW = (gam - 1.) * (1. - x1) / gam;
+        double dPdvsq = (gam - 1.) * (fma(0.5, D / sqrt(1. - x1), -x0)) / gam;
+        double t2 = -0.5 * Bsq + dPdvsq;
+        double t3 = Bsq + x0;
+        double t4 = t3 * t3;
+        double t9 = 1. / Wsq;
+        double t11 = Qtsq - x1 * t4 + QdotBsq * (Bsq + 2.0 * x0) * t9;
+        double t16 = QdotBsq * t9;
+        double t18 = -Qdotn - 0.5 * Bsq * (1.0 + x1) + 0.5 * t16 - x0 + p_tmp;
+        double t21 = 1. / t3;
+        double t23 = 1. / x0;
+        double t24 = t16 * t23;
+        double t25 = -1.0 + dPdW - t24;
+        double t35 = t25 * t3 + (Bsq - 2.0 * dPdvsq) * (QdotBsq + x1 * Wsq * x0) * t9 * t23;
+        double t36 = 1. / t35;
+        double dx0 = -(t2 * t11 + t4 * t18) * t21 * t36;
+        double t40 = (x1 + t24) * t3;
+        double dx1 = -(-t25 * t11 - 2.0 * t40 * t18) * t21 * t36;
+        df = -t11 * t11 - t18 * t18;
+        f = -0.5 * df;
+        double xo0 = x0;
+        x0 += dx0;
+        x1 += dx1;
+        x0 = fabs(x0);
+        x0 = (x0 > W_TOO_BIG) ? xo0 : x0;
+        x1 = (x1 < 0.) ? 0. : x1;
+        x1 = (x1 > 1.) ? (1. - 1.e-15) : x1;
+        errx = (x0 == 0.) ? fabs(x0 - xo0) : fabs((x0 - xo0) / x0);
+        if ((fabs(errx) <= NEWT_TOL) && (doing_extra == 0) && (EXTRA_NEWT_ITER > 0)) doing_extra = 1;
+        if (doing_extra == 1) i_extra++;
+        if (((fabs(errx) <= NEWT_TOL) && (doing_extra == 0)) || (i_extra > EXTRA_NEWT_ITER) || (n_iter >= (MAX_NEWT_ITER - 1)))
+            keep = 0;
+        n_iter++;
+    }
+    int retval = 0;
+    if ((isfinite(f) == 0) || (isfinite(df) == 0)) retval = 2;
+    else if (fabs(errx) > d_min(NEWT_TOL, MIN_NEWT_TOL)) retval = 1;
+    double W = x0, vsq = x1;
+    if ((retval != 0) || (W == FAIL_VAL)) return retval * 100 + 1;
+    if (W <= 0. || W > W_TOO_BIG) return 3;
+    if (vsq >= 1.) return 4;
+    double gtmp = sqrt(1. - vsq);
+    gamma = 1. / gtmp;
+    rho0 = s.D * gtmp;
+    w = W * (1. - vsq);
+    p = (gam - 1.) * (w - rho0) / gam;
+    u = w - (rho0 + p);
+    if (rho0 <= 0.) return 5;
+    if (u <= 0.) return 6;
+    pt[RHO] = rho0;
+    pt[UU] = u;
+    set_velocity(s, gamma, W, pt);
+    for (int i = 0; i < B1; i++) prim[i] = pt[i];
+    return 0;
+}
+
+__device__ __forceinline__ double W_of_vsq2(double gam, double vsq, double *p, double *rho, double *u, double D, double K) {
+    double gtmp = (1. - vsq);
+    *rho = D * sqrt(gtmp);
+    *p = K * pow(*rho, gam);
+    *u = *p / (gam - 1.);
+    return (*rho + *u + *p) / gtmp;
+}
+
+// entropy-based 1D solve in v^2
+__device__ __noinline__ int utoprim_1dvsq2fix1(double gam, const double *U, const double *gcov, const double *gcon, double gdet, double *prim) {
+    double Ut[NPR], pt[5];
+    int ret = inv_prologue(U, gdet, gcon, prim, Ut);
+    if (ret) return ret;
+    for (int i = 0; i < B1; i++) pt[i] = prim[i];
+    double K = U[KTOT] / U[RHO];
+    InvQ s;
+    inv_scalars(Ut, gcov, gcon, s);
+    double utsq, p, rho, u;
+    if (guess_utsq(gcov, pt, &utsq)) return 2;
+    double gammasq = 1. + utsq;
+    double x = 1. - 1. / gammasq;
+    double f = 1., df = 1., errx = 1., W = 0., W_old;
+    int n_iter = 0, i_extra = 0, doing_extra = 0, keep = 1;
+    while (keep) {
+        double Wc = W_of_vsq2(gam, x, &p, &rho, &u, s.D, K);
+        double Wsq = Wc * Wc;
+        double dWdvsq = (gam * (2. - gam) * p + (gam - 1.) * rho) / (2. * (gam - 1.) * (1. - x) * (1. - x));
+        double fact_tmp = (s.Bsq + Wc);
+        double resid = s.Qtsq - x * fact_tmp * fact_tmp + s.QdotBsq * (s.Bsq + 2. * Wc) / Wsq;
+        double jac = -fact_tmp * (fact_tmp + 2. * dWdvsq * (x + s.QdotBsq / (Wc * Wsq)));
+        double dx = -resid / jac;
+        f = 0.5 * resid * resid;
+        df = -2. * f;
+        double xo = x;
+        x += dx;
+        x = (x >= 1.0) ? (0.5 * (xo + 1.)) : x;
+        x = (x < -1.e-10) ? (0.5 * xo) : x;
+        x = fabs(x);
+        W_old = W;
+        W = W_of_vsq2(gam, x, &p, &rho, &u, s.D, K);
+        errx = (W == 0.) ? fabs(W - W_old) : fabs((W - W_old) / W);
+        errx += (x == 0.) ? fabs(x - xo) : fabs((x - xo) / x);
+        if ((fabs(errx) <= NEWT_TOL) && (doing_extra == 0) && (EXTRA_NEWT_ITER > 0)) doing_extra = 1;
+        if (doing_extra == 1) i_extra++;
+        if (((fabs(errx) <= NEWT_TOL) && (doing_extra == 0)) || (i_extra > EXTRA_NEWT_ITER) || (n_iter >= (MAX_NEWT_ITER - 1)))
+            keep = 0;
+        n_iter++;
+    }
+    int retval = 0;
+    if ((isfinite(f) == 0) || (isfinite(df) == 0)) retval = 2;
+    else if (fabs(errx) > d_min(NEWT_TOL, MIN_NEWT_TOL)) retval = 1;
+    if (retval != 0) return retval * 100 + 1;
+    double vsq = x;
+    if ((vsq >= 1.) || (vsq < 0.)) return 4;
+    double rho0;
+    W = W_of_vsq2(gam, vsq, &p, &rho0, &u, s.D, K);
+    double gtmp = sqrt(1. - vsq);
+    double gamma = 1. / gtmp;
+    if (rho0 <= 0.) return 5;
+    if (u <= 0.) return 6;
+    pt[RHO] = rho0;
+    pt[UU] = u;
+    set_velocity(s, gamma, W, pt);
+    for (int i = 0; i < B1; i++) prim[i] = pt[i];
+    return 0;
+}
+
+// inner density solve of the W-based entropy fallback (gnr2 / func_gnr2_rho)
+__device__ __forceinline__ int rho_solve(double gam, double *xr, double D, double K, double W_for) {
+    double f = 1., df = 1., errx = 1.;
+    int n_iter = 0, keep = 1;
+    double x = *xr;
+    while (keep) {
+        double A = D * D;
+        double B0 = A * gam * K;
+        double B = B0 / (gam - 1.);
+        double C = pow(x, gam - 1.);
+        double resid = x * W_for - A - B * C;
+        double jac = W_for - B0 * C / x;
+        double dx = -resid / jac;
+        f = 0.5 * resid * resid;
+        df = -2. * f;
+        double xo = x;
+        x += dx;
+        x = fabs(x);
+        errx = (x == 0.) ? fabs(x - xo) : fabs((x - xo) / x);
+        if ((fabs(errx) <= 1.0e-15) || (n_iter >= (MAX_NEWT_ITER - 1))) keep = 0;
+        n_iter++;
+    }
+    *xr = x;
+    if ((isfinite(f) == 0) || (isfinite(df) == 0) || (isfinite(x) == 0)) return 2;
+    if (fabs(errx) > 1.0e-10) return 1;
+    return 0;
+}
+
+// entropy-based 1D solve in W
+__device__ __noinline__ int utoprim_1dfix1(double gam, const double *U, const double *gcov, const double *gcon, double gdet, double *prim) {
+    double Ut[NPR], pt[5];
+    int ret = inv_prologue(U, gdet, gcon, prim, Ut);
+    if (ret) return ret;
+    for (int i = 0; i < B1; i++) pt[i] = prim[i];
+    double K = U[KTOT] / U[RHO];
+    InvQ s;
+    inv_scalars(Ut, gcov, gcon, s);
+    double utsq;
+    if (guess_utsq(gcov, pt, &utsq)) return 2;
+    const double Bsq = s.Bsq, Qtsq = s.Qtsq, QdotBsq = s.QdotBsq, D = s.D;
+    double gammasq = 1. + utsq;
+    double gamma = sqrt(gammasq);
+    double rho0 = D / gamma;
+    double p = K * pow(rho0, gam);
+    double u = p / (gam - 1.);
+    double w = rho0 + u + p;
+    double W_last = w * gammasq;
+    int i_increase = 0;
+    while (((W_last * W_last * W_last * (W_last + 2. * Bsq) - QdotBsq * (2. * W_last + Bsq)) <= W_last * W_last * (Qtsq - Bsq * Bsq)) && (i_increase < 10)) {
+        W_last *= 10.;
+        i_increase++;
+    }
+    const double rho_for = rho0;
+    double x = W_last;
+    double f = 1., df = 1., errx = 1.;
+    int n_iter = 0, i_extra = 0, doing_extra = 0, keep = 1;
+    while (keep) {
+        // func_1d_orig1
+        double xr = rho_for, rho_g = rho_for;
+        int ntries = 0;
+        while ((rho_solve(gam, &xr, D, K, x)) && (ntries++ < 10)) {
+            rho_g *= 10.;
+            xr = rho_g;
+        }
+        double rho = xr;
+        double t1 = D * D;
+        double t2 = QdotBsq * t1;
+        double t3 = t2 * Bsq;
+        double t5 = Bsq * Bsq;
+        double t8 = t1 * Bsq;
+        double t10 = t1 * x;
+        double t21 = x * x;
+        double t23 = rho * rho;
+        double t26 = 1. / t1;
+        double resid = (t3 + (2.0 * t2 + ((Qtsq - t5) * t1 + (-2.0 * t8 - t10) * x) * x) * x + (t5 + (2.0 * Bsq + x) * x) * t21 * t23) * t26 / t21;
+        double t29 = t1 * t1;
+        double t30 = QdotBsq * t29;
+        double t32 = gam * K;
+        double t33 = pow(rho, 1.0 * gam);
+        double t34 = t32 * t33;
+        double t38 = t23 * t33;
+        double t51 = gam * t1 * K * t33;
+        double t67 = t21 * x;
+        double jac = -2.0 * (t30 * Bsq * t34 + (t30 * t34 + ((-t38 * Bsq * t32 + Bsq * gam * t1 * K * t33) * t1 + (-t38 * gam * K + t51) * t1 * x) * t21) * x + ((-t3 + (-t2 + (-t8 - t10) * t21) * x) * x + (-t5 - Bsq * x) * t67 * t23) * t23) * t26 / (t51 - x * t23) / t67;
+        double dx = -resid / jac;
+        f = 0.5 * resid * resid;
+        df = -2. * f;
+        double xo = x;
+        x += dx;
+        int ii = 0;
+        while (((x * x * x * (x + 2. * Bsq) - QdotBsq * (2. * x + Bsq)) <= x * x * (Qtsq - Bsq * Bsq)) && (ii < 10)) {
+            x -= (1. * ii) * dx / 10.;
+            ii++;
+        }
+        x = fabs(x);
+        errx = (x == 0.) ? fabs(x - xo) : fabs((x - xo) / x);
+        if ((fabs(errx) <= NEWT_TOL) && (doing_extra == 0) && (EXTRA_NEWT_ITER > 0)) doing_extra = 1;
+        if (doing_extra == 1) i_extra++;
+        if (((fabs(errx) <= NEWT_TOL) && (doing_extra == 0)) || (i_extra > EXTRA_NEWT_ITER) || (n_iter >= (MAX_NEWT_ITER - 1)))
+            keep = 0;
+        n_iter++;
+    }
+    int retval = 0;
+    if ((isfinite(f) == 0) || (isfinite(df) == 0) || (isfinite(x) == 0)) retval = 2;
+    else if (fabs(errx) > d_min(NEWT_TOL, MIN_NEWT_TOL)) retval = 1;
+    double W = x;
+    if ((retval != 0) || (W == FAIL_VAL)) return retval * 100 + 1;
+    if (W <= 0. || W > W_TOO_BIG) return 3;
+    double vsq = vsq_of_W(W, Bsq, Qtsq, QdotBsq);
+    if (vsq >= 1.) return 4;
+    double gtmp = sqrt(1. - vsq);
+    gamma = 1. / gtmp;
+    rho0 = D * gtmp;
+    p = K * pow(rho0, gam);
+    u = p / (gam - 1.);
+    if (rho0 <= 0.) return 5;
+    if (u <= 0.) return 6;
+    pt[RHO] = rho0;
+    pt[UU] = u;
+    set_velocity(s, gamma, W, pt);
+    for (int i = 0; i < B1; i++) prim[i] = pt[i];
+    return 0;
+}
+
+}  // namespace hamr

@@ -1,0 +1,159 @@
+/*
+ * hamr_b200.h -- C ABI of the B200 (sm_100a) single-block GRMHD step.
+ *
+ * This is the drop-in boundary for H-AMR's per-block device step. In the
+ * reference the step is driven by advance_GPU() (step_ch.c:997) and
+ * GPU_step_ch() (step_ch.c:916), which launch the per-block launchers
+ * GPU_fluxcalc2D / GPU_fix_flux / GPU_consttransport1-3 / GPU_fixup
+ * (GPU_main.cu:560,1126,1365,1393,1535,1740) on global buffers allocated by
+ * set_arrays_GPU (GPU_mem.h:41) and filled by GPU_write / GPU_write_metric
+ * (GPU_main.cu:309,139). Here the same work sits behind an explicit context:
+ * no globals, plain pointers and sizes, return code 0 or a negative HAMR_E_*.
+ *
+ * Memory layout (identical to the reference device layout, GPU_program1.cu:90-94):
+ *   cell arrays  plane k holds variable k (RHO, UU, U1, U2, U3, B1, B2, B3, KTOT);
+ *                cell (i, j, z) of the ghosted block sits at (i*G2 + j)*G3 + z with
+ *                G1 = n1 + 2*ng, G2 = n2 + 2*ng, G3 = n3 + 2*ng (G3 = 1 when n3 == 1);
+ *                planes are ksize doubles apart.
+ *   face field   3 planes; plane d-1 holds B^d (no sqrt(-g)) on the lower d-face.
+ *   metric       gcov/gcon: plane (s*5 + loc), s the symmetric component
+ *                (00,01,02,03,11,12,13,22,23,33), loc in {FACE1, FACE2, CORN, CENT,
+ *                FACE3}; gdet: plane loc; conn: plane (s*4 + l) holding
+ *                Gamma^l_{s}; every plane indexed (i*G2 + j), gsize doubles apart
+ *                (GPU_main.cu:139-300).
+ * Every entry point is thread-safe per context; contexts are independent.
+ */
+#ifndef HAMR_B200_H
+#define HAMR_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HAMR_NPR 9
+
+enum hamr_status {
+    HAMR_OK = 0,
+    HAMR_E_ARG = -1,       /* invalid argument or size */
+    HAMR_E_CUDA = -2,      /* a CUDA runtime call failed (see hamr_last_error) */
+    HAMR_E_NOMEM = -3,     /* device allocation failed */
+    HAMR_E_STATE = -4,     /* call out of order (e.g. stepping before geometry) */
+    HAMR_E_PHYSICS = -5    /* non-finite or non-positive CFL step */
+};
+
+enum hamr_bc {
+    HAMR_BC_PERIODIC = 0,
+    HAMR_BC_OUTFLOW = 1,    /* copy + no-inflow check (bounds.c:158, GPU_bounds.h:1368) */
+    HAMR_BC_POLE_TRANS = 2, /* transmissive polar axis, 3-D (GPU_bounds.h:510) */
+    HAMR_BC_POLE_REFL = 3   /* reflective polar axis, 2-D (GPU_bounds.h:305) */
+};
+
+enum hamr_precision {
+    HAMR_FP64 = 0,          /* everything in double */
+    HAMR_MIXED = 1          /* reconstruction, Riemann flux and EMF in float; metric,
+                               source, compensated update and inversion in double */
+};
+
+typedef struct hamr_params {
+    int n1, n2, n3;         /* active cells per direction (n3 == 1: 2-D, x1-x2) */
+    int ng;                 /* ghost layers (must be 3: PPM, NG = 2 + PPM, config.h:1280) */
+    long ksize;             /* plane stride of cell arrays; 0: reference rule G + 64 - G%64 */
+    long gsize;             /* plane stride of metric tables; 0: reference rule */
+    double dx1, dx2, dx3;   /* coordinate spacing */
+    double gam;             /* adiabatic index */
+    double cour;            /* Courant factor (COUR, config.h:455) */
+    int pole1, pole2;       /* lower/upper x2 edge is a polar axis (POLE_1/2, GPU_main.cu:566) */
+    int bc1, bc2, bc3;      /* enum hamr_bc per direction */
+    int ct_upwind;          /* 1: upwinded edge EMFs (GR default); 0: face-EMF average
+                               (the reference's CARTESIAN build, GPU_const_trans.h:187) */
+    int precision;          /* enum hamr_precision */
+    void *stream;           /* cudaStream_t to run on; NULL: the context creates one */
+} hamr_params;
+
+typedef struct hamr_ctx hamr_ctx;
+
+/* Create a context on the current CUDA device and allocate its device state.
+ * Replaces set_arrays_GPU (GPU_mem.h:41-). */
+int hamr_ctx_create(const hamr_params *params, hamr_ctx **out);
+int hamr_ctx_destroy(hamr_ctx *ctx);
+/* Text of the last error recorded on ctx (never NULL). */
+const char *hamr_last_error(const hamr_ctx *ctx);
+/* Plane strides chosen at creation. */
+int hamr_strides(const hamr_ctx *ctx, long *ksize, long *gsize);
+
+/* Upload host metric tables (layout above). Replaces GPU_write_metric
+ * (GPU_main.cu:139). */
+int hamr_set_geometry(hamr_ctx *ctx, const double *gcov, const double *gcon,
+                      const double *gdet, const double *conn);
+
+/* Host -> device copy of primitives (NPR planes) and face field (3 planes),
+ * ghost zones included. Replaces GPU_write (GPU_main.cu:309). */
+int hamr_upload(hamr_ctx *ctx, const double *p, const double *ps);
+/* Device -> host copy of the current primitives and face field. Replaces
+ * GPU_read (GPU_main.cu:2646). */
+int hamr_download(hamr_ctx *ctx, double *p, double *ps);
+/* Device -> host copy of the inversion flags (1 int plane) and failure
+ * counters (4 int planes: 2D failed, 1dvsq2fix1 failed, 1dfix1 failed,
+ * floor; GPU_fixup.h:360-382). Either pointer may be NULL. */
+int hamr_download_flags(hamr_ctx *ctx, int *pflag, int *failimage);
+
+/* Ghost fill of the current state (GPU_boundprim, GPU_main.cu:2113). */
+int hamr_bound(hamr_ctx *ctx);
+
+/* One RK2 sub-step on the device, asynchronous on the context stream:
+ * full == 0 advances (p, ps) by Dt into (ph, psh) and caches U(p);
+ * full == 1 advances the cached U by Dt with the fluxes of (ph, psh) into (p, ps).
+ * dt is the step size (polar EMF averaging scales by it, GPU_boundcomE.cu:58).
+ * The written state gets its ghost zones filled. Replaces one advance_GPU()
+ * call plus GPU_boundprim(0) (step_ch.c:926-936). */
+int hamr_stage(hamr_ctx *ctx, int full, double Dt, double dt);
+
+/* Whole RK2 step of size dt (half then full sub-step). When dt_next is not
+ * NULL the call waits for the device and returns the CFL step of the full
+ * sub-step, 1/(1/dt1 + 1/dt2 + 1/dt3) (step_ch.c:1320-1331). */
+int hamr_step(hamr_ctx *ctx, double dt, double *dt_next);
+
+/* nsteps RK2 steps with the step size kept in device memory: every
+ * `interval` steps it becomes min(CFL step, 1.3 * dt) (the SAFE growth limit,
+ * step_ch.c:973-975; interval 16 mirrors AMR_MAXTIMELEVEL). The sequence is
+ * captured once into a CUDA graph per (nsteps, interval) and replayed.
+ * dt_inout: in, the first step size; out, the step size after the last step
+ * (this waits for the device). */
+int hamr_advance(hamr_ctx *ctx, int nsteps, int interval, double *dt_inout);
+
+/* Per-kernel-group device times of `reps` RK2 steps of size dt (the state
+ * advances), averaged per step, from CUDA events recorded between the groups
+ * on the context stream: ms[0..9] = x3 flux, x2 flux, x1 flux, polar flux
+ * fix, centre EMF, edge EMF, polar EMF average, face update, conserved
+ * update + inversion, ghost fill. nslots must be >= 10. */
+int hamr_profile_step(hamr_ctx *ctx, double dt, int reps, double *ms, int nslots);
+
+/* Device pointers of the live state, for zero-copy access (e.g. DLPack or
+ * torch.from_blob in a test harness). Any pointer argument may be NULL. */
+int hamr_device_state(hamr_ctx *ctx, double **p, double **ps, double **ph, double **psh);
+
+/* max over active cells of |div B| of the current face field, definition of
+ * divb_calc (diag.c:153-199); waits for the device. */
+int hamr_divb_max(hamr_ctx *ctx, double *out);
+
+/* ---- host geometry builder (no device needed) ----------------------------
+ * Fills metric tables for a block of n1 x n2 x n3 active cells in the layout
+ * above, following set_grid (main.c:380-455):
+ *   coords == 0: Kerr-Schild metric of spin `spin` in the reference's code
+ *                coordinates (X1 = log r, uniform theta map, X3 = phi;
+ *                vofx_matthewcoords, coord.c:147) with the Jacobian and the
+ *                connection by central differences (metric.c:427-519);
+ *   coords == 1: Minkowski in Cartesian code coordinates (CARTESIAN build).
+ * startx/dx are 4-vectors (index 0 unused). gsize 0: reference rule. */
+int hamr_build_geometry(int coords, double spin, int n1, int n2, int n3, int ng, long gsize,
+                        const double *startx, const double *dx,
+                        double *gcov, double *gcon, double *gdet, double *conn);
+/* Boyer-Lindquist (r, theta, phi) of a code-coordinate point (bl_coord, coord.c:111). */
+int hamr_bl_coord(int coords, double spin, const double *X, double *rthph);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HAMR_B200_H */

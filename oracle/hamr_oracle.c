@@ -235,6 +235,7 @@ static void fluxes(const ho_grid *g, const dims *d, const ho_geom *m, const doub
     int j0 = (d->ng2 - 1) * d->d2 + jdel, j1 = j0 + (d->n2 + 2 * d->d2 - jdel);
     int z0 = (d->ng3 - 1) * d->d3 + zdel, z1 = z0 + (d->n3 + 2 * d->d3 - zdel);
     double best = 1.e9;
+#pragma omp parallel for collapse(2) reduction(min : best) schedule(static)
     for (int i = i0; i < i1; i++)
         for (int j = j0; j < j1; j++)
             for (int z = z0; z < z1; z++) {
@@ -313,6 +314,7 @@ static void fix_flux(const ho_grid *g, const dims *d, double *F1, double *F2, do
 static void emf_centre(const dims *d, const ho_geom *m, const double *pv, double *E_cent) {
     long ks = d->ks;
     int i0 = (d->ng1 - d->d1) * d->d1, j0 = (d->ng2 - d->d2) * d->d2, z0 = (d->ng3 - d->d3) * d->d3;
+#pragma omp parallel for collapse(2) schedule(static)
     for (int i = i0; i < i0 + d->n1 + 2 * d->d1; i++)
         for (int j = j0; j < j0 + d->n2 + 2 * d->d2; j++)
             for (int z = z0; z < z0 + d->n3 + 2 * d->d3; z++) {
@@ -374,6 +376,7 @@ static void emf_edges(const ho_grid *g, const dims *d, const double *E_cent, con
     long D1 = d->d1, D2 = d->d2, D3 = d->d3;
     const double factor = 1.0;
     const double *Ec1 = E_cent + 1 * ks, *Ec2 = E_cent + 2 * ks, *Ec3 = E_cent + 3 * ks;
+#pragma omp parallel for collapse(2) schedule(static)
     for (int i = d->ng1 * d->d1; i < d->ng1 * d->d1 + d->n1 + d->d1; i++)
         for (int j = d->ng2 * d->d2; j < d->ng2 * d->d2 + d->n2 + d->d2; j++)
             for (int z = d->ng3 * d->d3; z < d->ng3 * d->d3 + d->n3 + d->d3; z++) {
@@ -453,6 +456,7 @@ static void face_update(const ho_grid *g, const dims *d, const ho_geom *m, const
                         double *psf, const double *E, double Dt) {
     long ks = d->ks;
     long isize = (long)d->G2 * d->G3, jsz = d->G3;
+#pragma omp parallel for collapse(2) schedule(static)
     for (int i = d->ng1 * d->d1; i < d->ng1 * d->d1 + d->n1 + d->d1; i++)
         for (int j = d->ng2 * d->d2; j < d->ng2 * d->d2 + d->n2 + d->d2; j++)
             for (int z = d->ng3 * d->d3; z < d->ng3 * d->d3 + d->n3 + d->d3; z++) {
@@ -940,6 +944,7 @@ static void update(const ho_grid *g, const dims *d, const ho_geom *m, ho_state *
     const double *pb = full ? s->ph : s->p;
     double *pout = full ? s->p : s->ph;
     const double *psf = full ? s->ps : s->psh;
+#pragma omp parallel for collapse(2) schedule(dynamic, 4)
     for (int i = d->ng1; i < d->ng1 + d->n1; i++)
         for (int j = d->ng2; j < d->ng2 + d->n2; j++)
             for (int z = d->ng3; z < d->ng3 + d->n3; z++) {
