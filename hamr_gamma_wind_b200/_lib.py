@@ -67,6 +67,7 @@ def load(strict: bool = False):
     L.hamr_divb_max.argtypes = [_vp, P(_d)]
     L.hamr_build_geometry.argtypes = [_i, _d, _i, _i, _i, _i, _l, _vp, _vp, _vp, _vp, _vp, _vp]
     L.hamr_bl_coord.argtypes = [_i, _d, _vp, _vp]
+    L.hamr_step_noalloc.argtypes = [P(HamrParams), _vp, _vp, _vp, _vp, _vp, _vp, _d, P(_d)]
     _libs[key] = L
     return L
 
@@ -75,7 +76,8 @@ def load(strict: bool = False):
 SYMBOLS = ["hamr_ctx_create", "hamr_ctx_destroy", "hamr_last_error", "hamr_strides",
            "hamr_set_geometry", "hamr_upload", "hamr_download", "hamr_download_flags",
            "hamr_bound", "hamr_stage", "hamr_step", "hamr_advance", "hamr_device_state", "hamr_profile_step",
-           "hamr_divb_max", "hamr_build_geometry", "hamr_bl_coord"]
+           "hamr_divb_max", "hamr_build_geometry", "hamr_bl_coord", "hamr_step_noalloc"]
+NOALLOC_MAX_CELLS = 32768
 
 PROF_SLOTS = ["flux3", "flux2", "flux1", "fix_flux", "emf_centre", "emf_edge", "pole_average",
               "face_update", "update", "bound"]

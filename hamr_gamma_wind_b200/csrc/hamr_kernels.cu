@@ -18,6 +18,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1032,3 +1033,118 @@ int hamr_divb_max(hamr_ctx *ctx, double *out) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free step (hamr_step_noalloc). All intermediate arrays of one RK2
+// step -- half-step state, cached conserved variables, face fluxes, EMFs,
+// inversion flags, CFL minima -- live in file-scope device arrays sized for at
+// most HAMR_NOALLOC_MAX_CELLS zones per plane. Every GPU that loads the library
+// holds these arrays (about 15 MB) until the process exits; every call shares
+// them, so calls that overlap on the GPU race.
+namespace {
+
+constexpr long NA_DPLANES = 9 + 3 + 9 + 27 + 4 + 4;  // ph, psh, U, F1-F3, E_cent, emf
+constexpr long NA_IPLANES = 1 + 4;                   // pflag, failimage
+static __device__ __align__(256) double na_scratch[NA_DPLANES * HAMR_NOALLOC_MAX_CELLS];
+static __device__ __align__(256) int na_iscratch[NA_IPLANES * HAMR_NOALLOC_MAX_CELLS];
+static __device__ __align__(256) unsigned long long na_dtbits[4];
+static __device__ __align__(256) double na_ndt[1];
+
+constexpr int NA_MAX_DEVICES = 64;
+struct NaPtrs {
+    double *scratch = nullptr;
+    int *iscratch = nullptr;
+    unsigned long long *dtbits = nullptr;
+    double *ndt = nullptr;
+};
+NaPtrs na_ptrs[NA_MAX_DEVICES];
+bool na_ready[NA_MAX_DEVICES];
+std::mutex na_mutex;
+
+// Device addresses of the scratch arrays on the current device, looked up once
+// per device: in host code the array names are host-side stand-ins.
+int na_setup(int dev) {
+    std::lock_guard<std::mutex> lock(na_mutex);
+    if (na_ready[dev]) return HAMR_OK;
+    NaPtrs q;
+    if (cudaGetSymbolAddress((void **)&q.scratch, na_scratch) != cudaSuccess) return HAMR_E_CUDA;
+    if (cudaGetSymbolAddress((void **)&q.iscratch, na_iscratch) != cudaSuccess) return HAMR_E_CUDA;
+    if (cudaGetSymbolAddress((void **)&q.dtbits, na_dtbits) != cudaSuccess) return HAMR_E_CUDA;
+    if (cudaGetSymbolAddress((void **)&q.ndt, na_ndt) != cudaSuccess) return HAMR_E_CUDA;
+    na_ptrs[dev] = q;
+    na_ready[dev] = true;
+    return HAMR_OK;
+}
+
+}  // namespace
+
+extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, const double *gcon,
+                                 const double *gdet, const double *conn, double *p, double *ps,
+                                 double dt, double *dt_next) {
+    if (!prm || !gcov || !gcon || !gdet || !conn || !p || !ps || !(dt > 0)) return HAMR_E_ARG;
+    if (prm->n1 < 2 || prm->n2 < 2 || prm->n3 < 1 || prm->ng != 3 || prm->precision != HAMR_FP64) return HAMR_E_ARG;
+    if (prm->n3 > 1 && prm->bc3 != HAMR_BC_PERIODIC) return HAMR_E_ARG;
+    if (prm->bc2 == HAMR_BC_POLE_TRANS && (prm->n3 < 2 || prm->n3 % 2)) return HAMR_E_ARG;
+    if (!(prm->gam > 1.0) || !(prm->cour > 0.0) || !(prm->dx1 > 0) || !(prm->dx2 > 0) || !(prm->dx3 > 0)) return HAMR_E_ARG;
+    // the same dimension bookkeeping as hamr_ctx_create
+    hamr_ctx c;
+    c.prm = *prm;
+    Dims &d = c.d;
+    d.n1 = prm->n1; d.n2 = prm->n2; d.n3 = prm->n3;
+    d.d1 = d.n1 > 1; d.d2 = d.n2 > 1; d.d3 = d.n3 > 1;
+    d.ng1 = d.d1 ? prm->ng : 0; d.ng2 = d.d2 ? prm->ng : 0; d.ng3 = d.d3 ? prm->ng : 0;
+    d.G1 = d.n1 + 2 * d.ng1; d.G2 = d.n2 + 2 * d.ng2; d.G3 = d.n3 + 2 * d.ng3;
+    const long ncell = (long)d.G1 * d.G2 * d.G3, ngeo = (long)d.G1 * d.G2;
+    d.ks = prm->ksize ? prm->ksize : ncell + (64 - ncell % 64);
+    d.gs = prm->gsize ? prm->gsize : ngeo + (64 - ngeo % 64);
+    if (d.ks < ncell || d.gs < ngeo) return HAMR_E_ARG;
+    if (d.ks > HAMR_NOALLOC_MAX_CELLS) return HAMR_E_ARG;   // beyond the static scratch
+    d.dx1 = prm->dx1; d.dx2 = prm->dx2; d.dx3 = prm->dx3;
+    d.gam = prm->gam; d.cour = prm->cour;
+    d.pole1 = prm->pole1; d.pole2 = prm->pole2;
+    d.bc1 = prm->bc1; d.bc2 = prm->bc2; d.bc3 = prm->bc3;
+    d.ct_upwind = prm->ct_upwind;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES) return HAMR_E_CUDA;
+    if (!na_ready[dev] && na_setup(dev) != HAMR_OK) return HAMR_E_CUDA;
+    const NaPtrs &q = na_ptrs[dev];
+    const long ks = d.ks;
+    c.stream = (cudaStream_t)prm->stream;
+    c.have_geom = true;
+    c.p = p;
+    c.ps = ps;
+    c.ph = q.scratch;
+    c.psh = c.ph + 9 * ks;
+    c.U = c.psh + 3 * ks;
+    c.F1 = c.U + 9 * ks;
+    c.F2 = c.F1 + 9 * ks;
+    c.F3 = c.F2 + 9 * ks;
+    c.Ec = c.F3 + 9 * ks;
+    c.emf = c.Ec + 4 * ks;
+    c.pflag = q.iscratch;
+    c.failimage = q.iscratch + ks;
+    c.gcov = const_cast<double *>(gcov);
+    c.gcon = const_cast<double *>(gcon);
+    c.gdet = const_cast<double *>(gdet);
+    c.conn = const_cast<double *>(conn);
+    c.dtbits = q.dtbits;
+    c.ndt = q.ndt;
+    c.counter = nullptr;
+    // the arrays keep the previous call's contents: zero the failure counters
+    // and, in 2-D, the x3 fluxes and centre EMFs the edge-EMF kernel reads
+    if (cudaMemsetAsync(c.failimage, 0, 4 * sizeof(int) * ks, c.stream) != cudaSuccess) return HAMR_E_CUDA;
+    if (!d.d3) {
+        if (cudaMemsetAsync(c.F3, 0, 9 * sizeof(double) * ks, c.stream) != cudaSuccess) return HAMR_E_CUDA;
+        if (cudaMemsetAsync(c.Ec, 0, 4 * sizeof(double) * ks, c.stream) != cudaSuccess) return HAMR_E_CUDA;
+    }
+    k_dt_reset<<<1, 32, 0, c.stream>>>(c.dtbits);
+    int rc = launch_step(&c, StepSize{nullptr, 0.5, 0.5 * dt, dt}, StepSize{nullptr, 1.0, dt, dt}, nullptr, 0);
+    c.p = c.ps = nullptr;  // caller-owned: not ours to release
+    if (rc) return rc;
+    if (dt_next) {
+        if (cudaMemcpyAsync(dt_next, c.ndt, sizeof(double), cudaMemcpyDeviceToHost, c.stream) != cudaSuccess) return HAMR_E_CUDA;
+        if (cudaStreamSynchronize(c.stream) != cudaSuccess) return HAMR_E_CUDA;
+        if (!(*dt_next > 0) || !isfinite(*dt_next)) return HAMR_E_PHYSICS;
+    }
+    return HAMR_OK;
+}

@@ -134,6 +134,36 @@ int hamr_profile_step(hamr_ctx *ctx, double dt, int reps, double *ms, int nslots
  * torch.from_blob in a test harness). Any pointer argument may be NULL. */
 int hamr_device_state(hamr_ctx *ctx, double **p, double **ps, double **ph, double **psh);
 
+/* ---- allocation-free step --------------------------------------------------
+ * No counterpart in the reference: an extra entry point for callers that may
+ * not allocate device memory at all -- code running inside someone else's
+ * CUDA graph capture (an allocation would break the capture), or a host
+ * framework that owns every byte of HBM through its own pool and forbids
+ * stray cudaMalloc calls. hamr_ctx_create allocates the whole working set, so
+ * those callers use this instead: one RK2 step (half and full sub-step, ghost
+ * fills) of a block whose state and metric tables the caller already holds in
+ * device memory (layout as above; p, ps advanced in place; gcov/gcon/gdet/conn
+ * read only). Every intermediate array lives in static device arrays inside
+ * this library, sized for at most HAMR_NOALLOC_MAX_CELLS zones per plane
+ * (ksize, ghosts and padding included; about 15 MB held on every GPU that
+ * loads the library, until the process exits). Larger blocks are rejected with
+ * HAMR_E_ARG before any device work. Nothing is allocated: no cudaMalloc,
+ * cudaFree, stream or event creation.
+ *   - runs on prm->stream (NULL: the legacy default stream); prm->precision
+ *     must be HAMR_FP64;
+ *   - the first call on a device looks up the device addresses of the static
+ *     arrays (cudaGetSymbolAddress); make that first call outside any stream
+ *     capture;
+ *   - all calls share the same arrays, which keep the previous call's
+ *     contents (the ones read before written are cleared each call): calls
+ *     that overlap on the GPU, from any thread or stream, race;
+ *   - dt_next: when not NULL, the call waits for the device and returns the
+ *     CFL step of the full sub-step, as hamr_step does. */
+#define HAMR_NOALLOC_MAX_CELLS 32768
+int hamr_step_noalloc(const hamr_params *prm, const double *gcov, const double *gcon,
+                      const double *gdet, const double *conn, double *p, double *ps,
+                      double dt, double *dt_next);
+
 /* max over active cells of |div B| of the current face field, definition of
  * divb_calc (diag.c:153-199); waits for the device. */
 int hamr_divb_max(hamr_ctx *ctx, double *out);
