@@ -53,28 +53,47 @@ def algorithmic_bytes_per_cell_update(n3: int) -> float:
     return 59 * 8 + 2 * 1160.0 / n3
 
 
-def kernel_bytes(slot: str, d: dict) -> float:
-    """Algorithmic bytes of one launch of a kernel group (FP64):
+def kernel_bytes(slot: str, d: dict, width: float = 8.0) -> float:
+    """Bytes one launch of a kernel group must move (FP64 storage; with width 4
+    the fluxes and EMFs are float, as in the mixed-precision step):
     flux_d   per face: 9 primitives + 1 normal face field read, 9 fluxes written,
              plus the face metric (21 words) once per (i, j) column;
-    update   per zone: 9 primitives, 27 face fluxes, 3 face fields and 9 cached
-             conserved values read or written, 9 primitives written, plus the
-             centre metric and connection (61 words) per column."""
+    update   (k_cons) per zone: 9 primitives, 9 cached conserved values and 27
+             face fluxes read or written, 7 conserved values written, plus the
+             centre metric and connection (61 words) per column;
+    invert   per zone: 9 primitives (initial guess) + 7 conserved values + 3 face
+             fields read, 9 primitives and 1 int flag written, plus the centre
+             metric and face volumes (23 words) per column."""
     n1, n2, n3 = d["n1"], d["n2"], d["n3"]
     if slot.startswith("flux"):
         k = int(slot[-1])
         nf = (n1 + 2 - (k == 1)) * (n2 + 2 - (k == 2)) * (n3 + 2 - (k == 3))
         ncol = (n1 + 2 - (k == 1)) * (n2 + 2 - (k == 2))
-        return 19 * 8.0 * nf + 21 * 8.0 * ncol
+        return (10 * 8.0 + 9 * width) * nf + 21 * 8.0 * ncol
     if slot == "update":
-        return 57 * 8.0 * n1 * n2 * n3 + 61 * 8.0 * n1 * n2
+        return (25 * 8.0 + 27 * width) * n1 * n2 * n3 + 61 * 8.0 * n1 * n2
+    if slot == "invert":
+        return (28 * 8.0 + 4) * n1 * n2 * n3 + 23 * 8.0 * n1 * n2
     if slot == "emf_centre":
-        return 12 * 8.0 * (n1 + 2) * (n2 + 2) * (n3 + 2)
+        return (9 * 8.0 + 3 * width) * (n1 + 2) * (n2 + 2) * (n3 + 2)
     if slot == "emf_edge":
-        return 15 * 8.0 * (n1 + 1) * (n2 + 1) * (n3 + 1)
+        return 15 * width * (n1 + 1) * (n2 + 1) * (n3 + 1)
     if slot == "face_update":
-        return 9 * 8.0 * (n1 + 1) * (n2 + 1) * (n3 + 1)
+        return (6 * 8.0 + 3 * width) * (n1 + 1) * (n2 + 1) * (n3 + 1)
     return 0.0
+
+
+def launches_per_step(pb) -> int:
+    """Kernels one RK2 step launches (two sub-steps and the step-size
+    finalisation), following the stage sequence of the library."""
+    dims = [n > 1 for n in (pb.n1, pb.n2, pb.n3)]
+    per_stage = sum(dims)                       # face fluxes
+    per_stage += pb.bc[1] == "pole_refl"        # polar flux fix
+    per_stage += 2                              # centre and edge EMFs
+    per_stage += pb.bc[1] == "pole_trans"       # polar EMF average
+    per_stage += 1 + 2                          # face update, conserved update, inversion
+    per_stage += sum(dims)                      # ghost fills
+    return 2 * per_stage + 1
 
 
 class ClockSampler:
@@ -168,25 +187,15 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
-def run_ours(args):
+def _measure(pb, precision, args, stream, world):
+    """Device time of K RK2 steps of one block (after the warm-up) and the
+    per-kernel-group breakdown; returns (ms, dt, blk)."""
     import torch
-    rank, world, local = _dist()
-    torch.cuda.set_device(local)
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    from hamr_gamma_wind_b200 import _lib, problems
     from hamr_gamma_wind_b200.api import Block
-
-    wl = WORKLOADS[args.workload]
-    pb = problems.fm_torus(wl["n1"], wl["n2"], wl["n3"], rout=wl["rout"])
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
-    blk = Block(**pb.block_kwargs(), precision=args.precision, stream=ctypes_stream(stream))
+    blk = Block(**pb.block_kwargs(), precision=precision, stream=ctypes_stream(stream))
     blk.set_geometry(pb.geo)
     blk.upload(pb.p, pb.ps)
     blk.bound()
-    cells = pb.n1 * pb.n2 * pb.n3
     dt = 0.2 * min(pb.dx[:2])
     # warm-up: captures the K-step graph, then W more steps
     dt = blk.step_ch(args.steps, dt, interval=16)
@@ -195,7 +204,7 @@ def run_ours(args):
         torch.distributed.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+    with ClockSampler(torch.cuda.current_device()) as clk:
         e0.record(stream)
         dt = blk.step_ch(args.steps, dt, interval=16)
         e1.record(stream)
@@ -206,33 +215,110 @@ def run_ours(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
         torch.distributed.barrier()
-    value = world * cells * args.steps / (ms * 1e-3)
+    return ms, dt, blk, clk.summary()
+
+
+def _kernel_profile(blk, dt):
+    import ctypes
+    from hamr_gamma_wind_b200 import _lib
+    prof = np.zeros(len(_lib.PROF_SLOTS))
+    blk._check(blk.L.hamr_profile_step(blk.ctx, dt, 2, prof.ctypes.data_as(ctypes.c_void_p), len(prof)),
+               "hamr_profile_step")
+    return dict(zip(_lib.PROF_SLOTS, prof.tolist()))
+
+
+def run_accuracy(args):
+    """Per-field relative L1 difference of the mixed-precision run against the
+    FP64 run after --accuracy steps of the workload (same initial state, same
+    step-size rule)."""
+    import torch
+    from hamr_gamma_wind_b200 import problems
+    wl = WORKLOADS[args.workload]
+    pb = problems.fm_torus(wl["n1"], wl["n2"], wl["n3"], rout=wl["rout"])
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    from hamr_gamma_wind_b200.api import Block
+    out = {}
+    for prec in ("fp64", "mixed"):
+        blk = Block(**pb.block_kwargs(), precision=prec, stream=ctypes_stream(stream))
+        blk.set_geometry(pb.geo)
+        blk.upload(pb.p, pb.ps)
+        blk.bound()
+        dt = 0.2 * min(pb.dx[:2])
+        left = args.accuracy
+        while left > 0:
+            n = min(left, 100)
+            dt = blk.step_ch(n, dt, interval=16)
+            left -= n
+        p, ps = blk.download()
+        out[prec] = (pb.active(p).copy(), pb.active(ps).copy(), dt)
+        blk.close()
+    names = ["rho", "u", "u1", "u2", "u3", "B1", "B2", "B3"]
+    p64, s64, dt64 = out["fp64"]
+    p32, s32, dt32 = out["mixed"]
+    errs = {n: float(np.abs(p32[k] - p64[k]).sum() / max(np.abs(p64[k]).sum(), 1e-300)) for k, n in enumerate(names)}
+    errs.update({f"face_B{k + 1}": float(np.abs(s32[k] - s64[k]).sum() / max(np.abs(s64[k]).sum(), 1e-300))
+                 for k in range(3)})
+    print(json.dumps({"accuracy_steps": args.accuracy, "workload": args.workload,
+                      "l1_rel_mixed_vs_fp64": errs, "dt_fp64": dt64, "dt_mixed": dt32,
+                      "finite": bool(np.isfinite(p32).all() and np.isfinite(p64).all())}), flush=True)
+
+
+def run_ours(args):
+    import ctypes
+    import torch
+    rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    from hamr_gamma_wind_b200 import problems
+
+    wl = WORKLOADS[args.workload]
+    pb = problems.fm_torus(wl["n1"], wl["n2"], wl["n3"], rout=wl["rout"])
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    cells = pb.n1 * pb.n2 * pb.n3
+    precs = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    runs = {}
+    for prec in precs:
+        ms, dt, blk, clocks = _measure(pb, prec, args, stream, world)
+        runs[prec] = dict(ms=ms, value=world * cells * args.steps / (ms * 1e-3), clocks=clocks)
+        if args.kernels_only:
+            blk.close()
+            continue
+        runs[prec]["kernels"] = _kernel_profile(blk, dt)
+        runs[prec]["dt"] = dt
+        if prec == precs[-1]:
+            head_blk = blk
+        else:
+            blk.close()
+    head = precs[-1]
+    value = runs[head]["value"]
     if args.kernels_only:
         if rank == 0:
-            print(json.dumps({"metric": "cell-updates/s", "value": value, "ms_per_step": ms / args.steps,
-                              "zones": cells, "note": "kernels only (profiling run)"}), flush=True)
-        blk.close()
+            print(json.dumps({"metric": "cell-updates/s", "value": value, "ms_per_step": runs[head]["ms"] / args.steps,
+                              "zones": cells, "precision": head, "note": "kernels only (profiling run)",
+                              "runs": {k: {"value": v["value"]} for k, v in runs.items()}}), flush=True)
         if world > 1:
             torch.distributed.destroy_process_group()
         return
-
-    # per-kernel device times (outside the timed region)
-    prof = np.zeros(len(_lib.PROF_SLOTS))
-    blk._check(blk.L.hamr_profile_step(blk.ctx, dt, 2, prof.ctypes.data_as(__import__("ctypes").c_void_p),
-                                       len(prof)), "hamr_profile_step")
-    slots = dict(zip(_lib.PROF_SLOTS, prof.tolist()))
+    blk = head_blk
+    dt = runs[head]["dt"]
+    slots = runs[head]["kernels"]
     top = max(slots, key=slots.get)
     peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
     hbm = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    kb = kernel_bytes(top, wl)
+    width = 4.0 if head == "mixed" else 8.0
+    kb = kernel_bytes(top, wl, width)
     achieved = 2 * kb / (slots[top] * 1e-3) / 1e9 if slots[top] > 0 else 0.0
+    ms = runs[head]["ms"]
     step_gbs = algorithmic_bytes_per_cell_update(pb.n3) * cells / (ms * 1e-3 / args.steps) / 1e9
 
     # end to end through the public API with host buffers: upload from pinned
     # memory, one step, download of the new state, every step
-    import ctypes
     nk = 9 * blk.ksize
     hp = torch.empty(nk, dtype=torch.float64, pin_memory=True).numpy()
     hs = torch.empty(3 * blk.ksize, dtype=torch.float64, pin_memory=True).numpy()
@@ -257,22 +343,25 @@ def run_ours(args):
             "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "mixed f32/f64", "data": "synthetic",
+            "dtype": "f64" if head == "fp64" else "f32 flux/EMF + f64 update/inversion", "data": "synthetic",
             "config": {"workload": f"3-D FM torus {wl['n1']}x{wl['n2']}x{wl['n3']} (a=0.9375, r_in=6, r_max=12, "
-                                   f"gamma=13/9, beta_min=100), {args.precision}",
-                       "zones": cells, "precision": args.precision, "l2": "inputs larger than L2 (no flush)",
+                                   f"gamma=13/9, beta_min=100), {head}",
+                       "zones": cells, "precision": head, "l2": "inputs larger than L2 (no flush)",
                        "dt_update_interval": 16, "parallelism": f"replicas x{world}"},
-            "gpu_launches": args.steps * 23 + 1,
+            "precisions": {k: {"value": v["value"], "ms_per_step": v["ms"] / args.steps,
+                               "kernel_ms_per_step": v.get("kernels")} for k, v in runs.items()},
+            "gpu_launches": args.steps * launches_per_step(pb) + 1,
             "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None, "peak_source": peak_src,
-                         "kernel_ms_per_step": slots},
+                         "frac": achieved / hbm, "traffic": None, "peak_source": peak_src},
             "step_roofline": {"algorithmic_bytes_per_cell_update": algorithmic_bytes_per_cell_update(pb.n3),
                               "achieved_gbs": step_gbs, "frac": step_gbs / hbm},
-            "clocks": clk.summary(),
+            "clocks": runs[head]["clocks"],
             "e2e": {"value": e2e_val, "unit": "cell-updates/s", "h2d_bytes_per_step": bytes_io,
                     "d2h_bytes_per_step": bytes_io, "steps": n_e2e},
             "state_finite": finite,
         }
+        if "fp64" in runs and "mixed" in runs:
+            out["mixed_over_fp64"] = runs["mixed"]["value"] / runs["fp64"]["value"]
         try:
             out["cpu_baseline"] = cpu_baseline(steps=1)
         except Exception as exc:  # the oracle is test infrastructure; report, do not fail the bench
@@ -295,7 +384,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c3", choices=list(WORKLOADS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
+    ap.add_argument("--accuracy", type=int, default=0,
+                    help="instead of timing: per-field L1 difference of mixed vs FP64 after this many steps")
     ap.add_argument("--kernels-only", action="store_true",
                     help="warm-up and timed steps only (for profiler runs)")
     args = ap.parse_args()
@@ -303,6 +394,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.accuracy:
+        run_accuracy(args)
     else:
         run_ours(args)
 

@@ -80,4 +80,4 @@ SYMBOLS = ["hamr_ctx_create", "hamr_ctx_destroy", "hamr_last_error", "hamr_strid
 NOALLOC_MAX_CELLS = 32768
 
 PROF_SLOTS = ["flux3", "flux2", "flux1", "fix_flux", "emf_centre", "emf_edge", "pole_average",
-              "face_update", "update", "bound"]
+              "face_update", "update", "invert", "bound"]

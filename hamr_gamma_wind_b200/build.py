@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 SOURCES = [os.path.join(CSRC, "hamr_kernels.cu"), os.path.join(CSRC, "hamr_geometry.cpp")]
-DEPS = SOURCES + [os.path.join(CSRC, "hamr_physics.cuh"),
+DEPS = SOURCES + [os.path.abspath(__file__), os.path.join(CSRC, "hamr_physics.cuh"),
                   os.path.join(os.path.dirname(HERE), "include", "hamr_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
@@ -37,9 +37,13 @@ def build(force=False, verbose=False):
         outs.append(out)
         if not force and not _stale(out):
             continue
+        # -prec-div/-prec-sqrt=false: single-precision division and square
+        # root use the approximate instructions (the mixed-precision step's
+        # FP32 reconstruction, flux and EMF arithmetic); double precision is
+        # unaffected
         cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
-               "-Xcompiler", "-ffp-contract=off", "-Xptxas", "-v" if verbose else "-O3",
-               *extra, *SOURCES, "-o", out]
+               "-Xcompiler", "-ffp-contract=off", "-prec-div=false", "-prec-sqrt=false",
+               "-Xptxas", "-v" if verbose else "-O3", *extra, *SOURCES, "-o", out]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)

@@ -8,7 +8,7 @@
 //   k_emf_centre, k_emf_edge           cell-centre and edge EMFs (consttransport1/2)
 //   k_pole_average                     phi-averaged polar EMF (E_average, 3-D)
 //   k_face_update                      staggered B update (consttransport3)
-//   k_update                           conserved update, source, inversion (fixup)
+//   k_cons, k_invert                   conserved update + source, inversion (fixup)
 //   k_bound_x1/x3/x2                   ghost fill of the written state
 // All arrays use the reference's structure-of-arrays layout; cell index
 // (i*G2 + j)*G3 + z puts phi (or x3) innermost, so consecutive threads touch
@@ -55,6 +55,18 @@ __device__ __forceinline__ void load_geo(const Dims &d, const Geom &m, int i, in
     o.g = __ldg(&m.gdet[(long)loc * d.gs + idx]);
 }
 
+// metric at one point, stored in double, used in the arithmetic type T
+template <typename T>
+__device__ __forceinline__ void load_geo_t(const Dims &d, const Geom &m, int i, int j, int loc, Geo<T> &o) {
+    long idx = gix(d, i, j);
+#pragma unroll
+    for (int s = 0; s < 10; s++) {
+        o.gcon[s] = (T)__ldg(&m.gcon[(long)(s * 5 + loc) * d.gs + idx]);
+        o.gcov[s] = (T)__ldg(&m.gcov[(long)(s * 5 + loc) * d.gs + idx]);
+    }
+    o.g = (T)__ldg(&m.gdet[(long)loc * d.gs + idx]);
+}
+
 // Sub-step sizes either come by value (hamr_stage) or from device memory
 // (hamr_advance replays a captured graph while the step size evolves).
 struct StepSize {
@@ -68,9 +80,17 @@ struct StepSize {
 // ---------------------------------------------------------------------------
 // Face fluxes of direction DIR over the normal range [ng, n + ng] and one ghost
 // layer either side transversally (fluxcalc2D2's face set).
-template <int DIR>
-__global__ void __launch_bounds__(BLK) k_flux(const Dims d, const Geom m, const double *__restrict__ pv,
-                                               const double *__restrict__ ps, double *__restrict__ F,
+// build options: minimum resident blocks of 128 threads per SM for the
+// double and float flux kernels (caps their registers per thread)
+#ifndef HAMR_FLUX_MINB
+#define HAMR_FLUX_MINB 5
+#endif
+#ifndef HAMR_FLUX_MINB_F
+#define HAMR_FLUX_MINB_F 6
+#endif
+template <int DIR, typename T>
+__global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? HAMR_FLUX_MINB : HAMR_FLUX_MINB_F) k_flux(const Dims d, const Geom m, const double *__restrict__ pv,
+                                               const double *__restrict__ ps, T *__restrict__ F,
                                                unsigned long long *__restrict__ dtbits, int calc_dt) {
     constexpr int idel = DIR == 1, jdel = DIR == 2, zdel = DIR == 3;
     const int i0 = (d.ng1 - 1) * d.d1 + idel, ni = d.n1 + 2 * d.d1 - idel;
@@ -86,47 +106,48 @@ __global__ void __launch_bounds__(BLK) k_flux(const Dims d, const Geom m, const 
         const long c = cix(d, i, j, z);
         const long stride = idel ? (long)d.G2 * d.G3 : (jdel ? (long)d.G3 : 1L);
         const int face = DIR == 1 ? FACE1 : (DIR == 2 ? FACE2 : FACE3);
-        Geo<double> gm;
-        load_geo(d, m, i, j, face, gm);
-        double pl[NPR], pr[NPR];
+        Geo<T> gm;
+        load_geo_t(d, m, i, j, face, gm);
+        T pl[NPR], pr[NPR];
 #pragma unroll
         for (int k = 0; k < NPR; k++) {
             const double *pk = pv + (long)k * d.ks + c;
-            double x[6];
+            T x[6];
 #pragma unroll
-            for (int s = 0; s < 6; s++) x[s] = __ldg(pk + (s - 3) * stride);
-            double lo, hi;
+            for (int s = 0; s < 6; s++) x[s] = (T)__ldg(pk + (s - 3) * stride);
+            T lo, hi;
             para(x, lo, hi);       // zone c-1: upper edge is the left state
             pl[k] = hi;
             para(x + 1, lo, hi);   // zone c: lower edge is the right state
             pr[k] = lo;
         }
-        const double bn = __ldg(&ps[(long)(DIR - 1) * d.ks + c]);
+        const T bn = (T)__ldg(&ps[(long)(DIR - 1) * d.ks + c]);
         pl[B1 + DIR - 1] = bn;
         pr[B1 + DIR - 1] = bn;
         if (DIR == 2 && ((j == d.n2 + d.ng2 && d.pole2) || (j == d.ng2 && d.pole1))) {
-            pl[B1] = 0.;
-            pr[B1] = 0.;
+            pl[B1] = T(0.);
+            pr[B1] = T(0.);
         }
-        State<double> q;
-        double t1[NPR], t2[NPR], t3[NPR], t4[NPR];
-        double cmax_l, cmin_l, cmax_r, cmin_r, vd;
+        const T gam = (T)d.gam;
+        State<T> q;
+        T t1[NPR], t2[NPR], t3[NPR], t4[NPR];
+        T cmax_l, cmin_l, cmax_r, cmin_r, vd;
         get_state(pl, gm, q);
-        double e = entropy(d.gam, pl);
-        primtoflux(d.gam, pl, q, DIR, gm, e, t1, &cmax_l, &cmin_l);
-        primtoflux(d.gam, pl, q, 0, gm, e, t2, &vd, &vd);
+        T e = entropy(gam, pl);
+        primtoflux(gam, pl, q, DIR, gm, e, t1, &cmax_l, &cmin_l);
+        primtoflux(gam, pl, q, 0, gm, e, t2, &vd, &vd);
         get_state(pr, gm, q);
-        e = entropy(d.gam, pr);
-        primtoflux(d.gam, pr, q, DIR, gm, e, t3, &cmax_r, &cmin_r);
-        primtoflux(d.gam, pr, q, 0, gm, e, t4, &vd, &vd);
-        const double cmax = fabs(d_max(d_max(0., cmax_l), cmax_r));
-        const double cmin = fabs(d_max(d_max(0., -cmin_l), -cmin_r));
-        const double ctop = d_max(cmax, cmin);
+        e = entropy(gam, pr);
+        primtoflux(gam, pr, q, DIR, gm, e, t3, &cmax_r, &cmin_r);
+        primtoflux(gam, pr, q, 0, gm, e, t4, &vd, &vd);
+        const T cmax = d_fabs(d_max(d_max(T(0.), cmax_l), cmax_r));
+        const T cmin = d_fabs(d_max(d_max(T(0.), -cmin_l), -cmin_r));
+        const T ctop = d_max(cmax, cmin);
 #pragma unroll
         for (int k = 0; k < NPR; k++)
-            F[(long)k * d.ks + c] = (cmax * t1[k] + cmin * t3[k] - cmax * cmin * (t4[k] - t2[k])) / (cmax + cmin + SMALL_D);
+            F[(long)k * d.ks + c] = (cmax * t1[k] + cmin * t3[k] - cmax * cmin * (t4[k] - t2[k])) / (cmax + cmin + T(SMALL_D));
         const double dxd = DIR == 1 ? d.dx1 : (DIR == 2 ? d.dx2 : d.dx3);
-        const double v = d.cour * dxd / ctop;
+        const double v = d.cour * dxd / (double)ctop;
         if (v > 1.e-6 && v < dtf) dtf = v;
     }
     if (calc_dt) {
@@ -146,7 +167,8 @@ __global__ void __launch_bounds__(BLK) k_flux(const Dims d, const Geom m, const 
 }
 
 // reflective polar axis and no-inflow radial edges (fix_flux, GPU_const_trans.h:3-61)
-__global__ void k_fix_flux(const Dims d, double *F1, double *F2, double *F3) {
+template <typename T>
+__global__ void k_fix_flux(const Dims d, T *F1, T *F2, T *F3) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const long ks = d.ks;
     const long na = (long)d.G1 * d.G3;
@@ -156,12 +178,12 @@ __global__ void k_fix_flux(const Dims d, double *F1, double *F2, double *F3) {
         if (d.pole1) {
             F1[B2 * ks + cix(d, i, d.ng2 - 1, z)] = -F1[B2 * ks + cix(d, i, d.ng2, z)];
             if (d.ng3 > 0) F3[B2 * ks + cix(d, i, d.ng2 - 1, z)] = -F3[B2 * ks + cix(d, i, d.ng2, z)];
-            for (int k = 0; k < NPR; k++) F2[k * ks + cix(d, i, d.ng2, z)] = 0.;
+            for (int k = 0; k < NPR; k++) F2[k * ks + cix(d, i, d.ng2, z)] = T(0.);
         }
         if (d.pole2) {
             F1[B2 * ks + cix(d, i, d.n2 + d.ng2, z)] = -F1[B2 * ks + cix(d, i, d.n2 + d.ng2 - 1, z)];
             if (d.ng3 > 0) F3[B2 * ks + cix(d, i, d.n2 + d.ng2, z)] = -F3[B2 * ks + cix(d, i, d.n2 + d.ng2 - 1, z)];
-            for (int k = 0; k < NPR; k++) F2[k * ks + cix(d, i, d.n2 + d.ng2, z)] = 0.;
+            for (int k = 0; k < NPR; k++) F2[k * ks + cix(d, i, d.n2 + d.ng2, z)] = T(0.);
         }
         return;
     }
@@ -170,14 +192,15 @@ __global__ void k_fix_flux(const Dims d, double *F1, double *F2, double *F3) {
     const int z = (int)(u % d.G3), j = (int)(u / d.G3);
     if (!(j >= d.ng2 - d.d2 && z >= d.ng3 - d.d3 && j < d.n2 + d.ng2 + d.d2 && z < d.n3 + d.ng3 + d.d3)) return;
     const long ci = RHO * ks + cix(d, d.ng1, j, z);
-    if (F1[ci] > 0.) F1[ci] = 0.;
+    if (F1[ci] > T(0.)) F1[ci] = T(0.);
     const long co = RHO * ks + cix(d, d.n1 + d.ng1, j, z);
-    if (F1[co] < 0.) F1[co] = 0.;
+    if (F1[co] < T(0.)) F1[co] = T(0.);
 }
 
 // cell-centre EMF, -gdet (u x b), on the active zones plus one ghost layer
+template <typename T>
 __global__ void __launch_bounds__(BLK) k_emf_centre(const Dims d, const Geom m, const double *__restrict__ pv,
-                                                     double *__restrict__ Ec) {
+                                                     T *__restrict__ Ec) {
     const int ni = d.n1 + 2 * d.d1, nj = d.n2 + 2 * d.d2, nz = d.n3 + 2 * d.d3;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)ni * nj * nz) return;
@@ -185,12 +208,12 @@ __global__ void __launch_bounds__(BLK) k_emf_centre(const Dims d, const Geom m, 
     const int j = (d.ng2 - d.d2) * d.d2 + (int)((t / nz) % nj);
     const int i = (d.ng1 - d.d1) * d.d1 + (int)(t / ((long)nz * nj));
     const long c = cix(d, i, j, z);
-    double pb[NPR];
+    T pb[NPR];
 #pragma unroll
-    for (int k = 0; k < NPR; k++) pb[k] = __ldg(&pv[k * d.ks + c]);
-    Geo<double> gm;
-    load_geo(d, m, i, j, CENT, gm);
-    double ucon[4], ucov[4], bcon[4];
+    for (int k = 0; k < NPR; k++) pb[k] = (T)__ldg(&pv[k * d.ks + c]);
+    Geo<T> gm;
+    load_geo_t(d, m, i, j, CENT, gm);
+    T ucon[4], ucov[4], bcon[4];
     ucon_calc(pb, gm, ucon);
     lower4(ucon, gm.gcov, ucov);
     bcon_calc(pb, ucon, ucov, bcon);
@@ -201,15 +224,16 @@ __global__ void __launch_bounds__(BLK) k_emf_centre(const Dims d, const Geom m, 
     Ec[3 * d.ks + c] = -gm.g * (ucon[1] * bcon[2] - ucon[2] * bcon[1]);
 }
 
-__device__ __forceinline__ double up(double f) { return (double)(f <= 0.0); }
-__device__ __forceinline__ double dn(double f) { return (double)(f > 0.0); }
+template <typename T> __device__ __forceinline__ T up(T f) { return (T)(f <= T(0.0)); }
+template <typename T> __device__ __forceinline__ T dn(T f) { return (T)(f > T(0.0)); }
 
 // edge EMFs: average of the four face EMFs plus, when ct_upwind, the
 // centre-minus-face corrections from the upwind side of each face, chosen by
 // the sign of its mass flux (consttransport2, GPU_const_trans.h:121-338)
-__global__ void __launch_bounds__(BLK) k_emf_edge(const Dims d, const double *__restrict__ Ec,
-                                                   const double *__restrict__ F1, const double *__restrict__ F2,
-                                                   const double *__restrict__ F3, double *__restrict__ emf) {
+template <typename T>
+__global__ void __launch_bounds__(BLK) k_emf_edge(const Dims d, const T *__restrict__ Ec,
+                                                   const T *__restrict__ F1, const T *__restrict__ F2,
+                                                   const T *__restrict__ F3, T *__restrict__ emf) {
     const int ni = d.n1 + d.d1, nj = d.n2 + d.d2, nz = d.n3 + d.d3;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)ni * nj * nz) return;
@@ -219,51 +243,51 @@ __global__ void __launch_bounds__(BLK) k_emf_edge(const Dims d, const double *__
     const long c = cix(d, i, j, z);
     const long ks = d.ks, jsize = d.G3, isize = (long)d.G2 * d.G3;
     const long D1 = d.d1, D2 = d.d2, D3 = d.d3;
-    const double *Ec1 = Ec + 1 * ks, *Ec2 = Ec + 2 * ks, *Ec3 = Ec + 3 * ks;
-    const double *F1r = F1 + RHO * ks, *F2r = F2 + RHO * ks, *F3r = F3 + RHO * ks;
-    const double w = d.ct_upwind ? 1.0 : 0.0;
+    const T *Ec1 = Ec + 1 * ks, *Ec2 = Ec + 2 * ks, *Ec3 = Ec + 3 * ks;
+    const T *F1r = F1 + RHO * ks, *F2r = F2 + RHO * ks, *F3r = F3 + RHO * ks;
+    const bool w = d.ct_upwind != 0;
     // in the non-upwind build every correction is an exact 0.0
-#define CORR(expr) (w != 0.0 ? (expr) : 0.0)
-    const double dE_LEFT_13_1 = CORR(Ec1[c] - F3[B2 * ks + c]);
-    const double dE_LEFT_13_2 = CORR(Ec1[c - jsize * D2] - F3[B2 * ks + c - jsize * D2]);
-    const double dE_RIGHT_13_1 = CORR(F3[B2 * ks + c] - Ec1[c - D3]);
-    const double dE_RIGHT_13_2 = CORR(F3[B2 * ks + c - jsize * D2] - Ec1[c - jsize * D2 - D3]);
-    const double dE_LEFT_12_1 = CORR(Ec1[c] + F2[B3 * ks + c]);
-    const double dE_LEFT_12_2 = CORR(Ec1[c - D3] + F2[B3 * ks + c - D3]);
-    const double dE_RIGHT_12_1 = CORR(-F2[B3 * ks + c] - Ec1[c - D2 * jsize]);
-    const double dE_RIGHT_12_2 = CORR(-F2[B3 * ks + c - D3] - Ec1[c - D2 * jsize - D3]);
-    const double dE_LEFT_21_1 = CORR(Ec2[c] - F1[B3 * ks + c]);
-    const double dE_LEFT_21_2 = CORR(Ec2[c - D3] - F1[B3 * ks + c - D3]);
-    const double dE_RIGHT_21_1 = CORR(F1[B3 * ks + c] - Ec2[c - D1 * isize]);
-    const double dE_RIGHT_21_2 = CORR(F1[B3 * ks + c - D3] - Ec2[c - D1 * isize - D3]);
-    const double dE_LEFT_23_1 = CORR(Ec2[c] + F3[B1 * ks + c]);
-    const double dE_LEFT_23_2 = CORR(Ec2[c - D1 * isize] + F3[B1 * ks + c - D1 * isize]);
-    const double dE_RIGHT_23_1 = CORR(-F3[B1 * ks + c] - Ec2[c - D3]);
-    const double dE_RIGHT_23_2 = CORR(-F3[B1 * ks + c - isize * D1] - Ec2[c - isize * D1 - D3]);
-    const double dE_LEFT_31_1 = CORR(Ec3[c] + F1[B2 * ks + c]);
-    const double dE_LEFT_31_2 = CORR(Ec3[c - D2 * jsize] + F1[B2 * ks + c - D2 * jsize]);
-    const double dE_RIGHT_31_1 = CORR(-F1[B2 * ks + c] - Ec3[c - D1 * isize]);
-    const double dE_RIGHT_31_2 = CORR(-F1[B2 * ks + c - D2 * jsize] - Ec3[c - D1 * isize - D2 * jsize]);
-    const double dE_LEFT_32_1 = CORR(Ec3[c] - F2[B1 * ks + c]);
-    const double dE_LEFT_32_2 = CORR(Ec3[c - D1 * isize] - F2[B1 * ks + c - D1 * isize]);
-    const double dE_RIGHT_32_1 = CORR(F2[B1 * ks + c] - Ec3[c - D2 * jsize]);
-    const double dE_RIGHT_32_2 = CORR(F2[B1 * ks + c - D1 * isize] - Ec3[c - D1 * isize - D2 * jsize]);
+#define CORR(expr) (w ? (expr) : T(0.0))
+    const T dE_LEFT_13_1 = CORR(Ec1[c] - F3[B2 * ks + c]);
+    const T dE_LEFT_13_2 = CORR(Ec1[c - jsize * D2] - F3[B2 * ks + c - jsize * D2]);
+    const T dE_RIGHT_13_1 = CORR(F3[B2 * ks + c] - Ec1[c - D3]);
+    const T dE_RIGHT_13_2 = CORR(F3[B2 * ks + c - jsize * D2] - Ec1[c - jsize * D2 - D3]);
+    const T dE_LEFT_12_1 = CORR(Ec1[c] + F2[B3 * ks + c]);
+    const T dE_LEFT_12_2 = CORR(Ec1[c - D3] + F2[B3 * ks + c - D3]);
+    const T dE_RIGHT_12_1 = CORR(-F2[B3 * ks + c] - Ec1[c - D2 * jsize]);
+    const T dE_RIGHT_12_2 = CORR(-F2[B3 * ks + c - D3] - Ec1[c - D2 * jsize - D3]);
+    const T dE_LEFT_21_1 = CORR(Ec2[c] - F1[B3 * ks + c]);
+    const T dE_LEFT_21_2 = CORR(Ec2[c - D3] - F1[B3 * ks + c - D3]);
+    const T dE_RIGHT_21_1 = CORR(F1[B3 * ks + c] - Ec2[c - D1 * isize]);
+    const T dE_RIGHT_21_2 = CORR(F1[B3 * ks + c - D3] - Ec2[c - D1 * isize - D3]);
+    const T dE_LEFT_23_1 = CORR(Ec2[c] + F3[B1 * ks + c]);
+    const T dE_LEFT_23_2 = CORR(Ec2[c - D1 * isize] + F3[B1 * ks + c - D1 * isize]);
+    const T dE_RIGHT_23_1 = CORR(-F3[B1 * ks + c] - Ec2[c - D3]);
+    const T dE_RIGHT_23_2 = CORR(-F3[B1 * ks + c - isize * D1] - Ec2[c - isize * D1 - D3]);
+    const T dE_LEFT_31_1 = CORR(Ec3[c] + F1[B2 * ks + c]);
+    const T dE_LEFT_31_2 = CORR(Ec3[c - D2 * jsize] + F1[B2 * ks + c - D2 * jsize]);
+    const T dE_RIGHT_31_1 = CORR(-F1[B2 * ks + c] - Ec3[c - D1 * isize]);
+    const T dE_RIGHT_31_2 = CORR(-F1[B2 * ks + c - D2 * jsize] - Ec3[c - D1 * isize - D2 * jsize]);
+    const T dE_LEFT_32_1 = CORR(Ec3[c] - F2[B1 * ks + c]);
+    const T dE_LEFT_32_2 = CORR(Ec3[c - D1 * isize] - F2[B1 * ks + c - D1 * isize]);
+    const T dE_RIGHT_32_1 = CORR(F2[B1 * ks + c] - Ec3[c - D2 * jsize]);
+    const T dE_RIGHT_32_2 = CORR(F2[B1 * ks + c - D1 * isize] - Ec3[c - D1 * isize - D2 * jsize]);
 #undef CORR
-    double e1 = 0.25 * ((-F2[B3 * ks + c] - (dE_LEFT_13_1 * up(F2r[c]) + dE_LEFT_13_2 * dn(F2r[c])))
+    T e1 = T(0.25) * ((-F2[B3 * ks + c] - (dE_LEFT_13_1 * up(F2r[c]) + dE_LEFT_13_2 * dn(F2r[c])))
         + (-F2[B3 * ks + c - D3] + (dE_RIGHT_13_1 * up(F2r[c - D3]) + dE_RIGHT_13_2 * dn(F2r[c - D3]))) +
         +(F3[B2 * ks + c] - (dE_LEFT_12_1 * up(F3r[c]) + dE_LEFT_12_2 * dn(F3r[c])))
         + (F3[B2 * ks + c - D2 * jsize] + (dE_RIGHT_12_1 * up(F3r[c - D2 * jsize]) + dE_RIGHT_12_2 * dn(F3r[c - D2 * jsize]))));
-    const double e2 = 0.25 * ((-F3[B1 * ks + c] - (dE_LEFT_21_1 * up(F3r[c]) + dE_LEFT_21_2 * dn(F3r[c])))
+    const T e2 = T(0.25) * ((-F3[B1 * ks + c] - (dE_LEFT_21_1 * up(F3r[c]) + dE_LEFT_21_2 * dn(F3r[c])))
         + (-F3[B1 * ks + c - D1 * isize] + (dE_RIGHT_21_1 * up(F3r[c - D1 * isize]) + dE_RIGHT_21_2 * dn(F3r[c - D1 * isize])))
         + (F1[B3 * ks + c] - (dE_LEFT_23_1 * up(F1r[c]) + dE_LEFT_23_2 * dn(F1r[c])))
         + (F1[B3 * ks + c - D3] + (dE_RIGHT_23_1 * up(F1r[c - D3]) + dE_RIGHT_23_2 * dn(F1r[c - D3]))));
-    double e3 = 0.25 * ((F2[B1 * ks + c] - (dE_LEFT_31_1 * up(F2r[c]) + dE_LEFT_31_2 * dn(F2r[c])))
+    T e3 = T(0.25) * ((F2[B1 * ks + c] - (dE_LEFT_31_1 * up(F2r[c]) + dE_LEFT_31_2 * dn(F2r[c])))
         + (F2[B1 * ks + c - D1 * isize] + (dE_RIGHT_31_1 * up(F2r[c - D1 * isize]) + dE_RIGHT_31_2 * dn(F2r[c - D1 * isize])))
         + (-F1[B2 * ks + c] - (dE_LEFT_32_1 * up(F1r[c]) + dE_LEFT_32_2 * dn(F1r[c])))
         + (-F1[B2 * ks + c - D2 * jsize] + (dE_RIGHT_32_1 * up(F1r[c - D2 * jsize]) + dE_RIGHT_32_2 * dn(F1r[c - D2 * jsize]))));
     if ((d.pole1 && j == d.ng2) || (d.pole2 && j == d.n2 + d.ng2)) {
-        e3 = 0.;
-        e1 = -0.5 * (F2[B3 * ks + c] + F2[B3 * ks + c - D3]);
+        e3 = T(0.);
+        e1 = T(-0.5) * (F2[B3 * ks + c] + F2[B3 * ks + c - D3]);
     }
     emf[1 * ks + c] = e1;
     emf[2 * ks + c] = e2;
@@ -273,7 +297,8 @@ __global__ void __launch_bounds__(BLK) k_emf_edge(const Dims d, const double *__
 // phi-average of the x1-EMF on the polar edges of a block that holds every
 // phi zone (E_average, const_trans.c:268-503): dt-scaled sum over active z,
 // divided by n3, unscaled; x3-EMF zeroed there. One thread per (side, i).
-__global__ void k_pole_average(const Dims d, double *emf, StepSize st) {
+template <typename T>
+__global__ void k_pole_average(const Dims d, T *emf, StepSize st) {
     const int ni = d.n1 + d.ng1;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 2 * ni) return;
@@ -282,18 +307,19 @@ __global__ void k_pole_average(const Dims d, double *emf, StepSize st) {
     const int jp = side == 0 ? d.ng2 : d.n2 + d.ng2;
     const double dt = st.full();
     double avg = 0.;
-    for (int z = d.ng3; z < d.n3 + d.ng3; z++) avg += dt * emf[1 * d.ks + cix(d, i, jp, z)];
+    for (int z = d.ng3; z < d.n3 + d.ng3; z++) avg += dt * (double)emf[1 * d.ks + cix(d, i, jp, z)];
     avg /= (double)(d.n3);
     const double avg_new = avg / ((double)1);
     for (int z = d.ng3; z < d.n3 + 2 * d.ng3; z++) {
-        emf[1 * d.ks + cix(d, i, jp, z)] = avg_new / dt;
-        emf[3 * d.ks + cix(d, i, jp, z)] = 0.;
+        emf[1 * d.ks + cix(d, i, jp, z)] = (T)(avg_new / dt);
+        emf[3 * d.ks + cix(d, i, jp, z)] = T(0.);
     }
 }
 
 // staggered field update from the edge EMFs (consttransport3, GPU_const_trans.h:426-529)
+template <typename T>
 __global__ void __launch_bounds__(BLK) k_face_update(const Dims d, const Geom m, const double *psi, double *psf,
-                                                      const double *__restrict__ E, StepSize st) {
+                                                      const T *__restrict__ Et, StepSize st) {
     const int ni = d.n1 + d.d1, nj = d.n2 + d.d2, nz = d.n3 + d.d3;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)ni * nj * nz) return;
@@ -303,27 +329,28 @@ __global__ void __launch_bounds__(BLK) k_face_update(const Dims d, const Geom m,
     const long c = cix(d, i, j, z), gi = gix(d, i, j);
     const long ks = d.ks, isize = (long)d.G2 * d.G3, jsz = d.G3;
     const double Dt = st.sub();
+    auto E = [&](long idx) { return (double)Et[idx]; };
     if (i < d.n1 + d.ng1 + d.d1 && j < d.n2 + d.ng2 && z < d.n3 + d.ng3) {
         const double gdf = __ldg(&m.gdet[FACE1 * d.gs + gi]);
         double temp = 0.;
         temp += 1.0 / ((double)1) * psi[c] * gdf;
-        temp += -Dt / ((double)1 * d.dx2) * (E[3 * ks + c + jsz] - E[3 * ks + c]);
-        if (d.ng3 > 0) temp += Dt / ((double)1 * d.dx3) * (E[2 * ks + c + d.d3] - E[2 * ks + c]);
+        temp += -Dt / ((double)1 * d.dx2) * (E(3 * ks + c + jsz) - E(3 * ks + c));
+        if (d.ng3 > 0) temp += Dt / ((double)1 * d.dx3) * (E(2 * ks + c + d.d3) - E(2 * ks + c));
         psf[c] = temp / gdf;
     }
     if (d.ng3 > 0 && i < d.n1 + d.ng1 && j < d.n2 + d.ng2 && z < d.n3 + d.ng3 + d.d3) {
         const double gdf = __ldg(&m.gdet[FACE3 * d.gs + gi]);
         double temp = psi[2 * ks + c] * gdf;
-        temp += -Dt / d.dx1 * (E[2 * ks + c + isize] - E[2 * ks + c]);
-        temp += Dt / d.dx2 * (E[1 * ks + c + jsz] - E[1 * ks + c]);
+        temp += -Dt / d.dx1 * (E(2 * ks + c + isize) - E(2 * ks + c));
+        temp += Dt / d.dx2 * (E(1 * ks + c + jsz) - E(1 * ks + c));
         psf[2 * ks + c] = temp / gdf;
     }
     if (i < d.n1 + d.ng1 && j < d.n2 + d.ng2 + d.d2 && z < d.n3 + d.ng3) {
         const double gdf = __ldg(&m.gdet[FACE2 * d.gs + gi]);
         double temp = 0.;
         temp += 1.0 / ((double)1) * psi[1 * ks + c] * gdf;
-        temp += Dt / ((double)1 * d.dx1) * (E[3 * ks + c + isize] - E[3 * ks + c]);
-        if (d.ng3 > 0) temp += -Dt / ((double)1 * d.dx3) * (E[1 * ks + c + d.d3] - E[1 * ks + c]);
+        temp += Dt / ((double)1 * d.dx1) * (E(3 * ks + c + isize) - E(3 * ks + c));
+        if (d.ng3 > 0) temp += -Dt / ((double)1 * d.dx3) * (E(1 * ks + c + d.d3) - E(1 * ks + c));
         psf[1 * ks + c] = temp / gdf;
     }
 }
@@ -369,25 +396,20 @@ __device__ __forceinline__ void source(double gam, const double *ph, const Geo<d
     dU[KTOT] *= gm.g;
 }
 
-// conserved update and inversion of one active zone (fixup, GPU_fixup.h:5-424)
-__global__ void __launch_bounds__(BLK) k_update(const Dims d, const Geom m, const double *__restrict__ pin,
-                                                 const double *__restrict__ pb, double *__restrict__ pout,
-                                                 double *__restrict__ Ucache, const double *__restrict__ psf,
-                                                 const double *__restrict__ F1, const double *__restrict__ F2,
-                                                 const double *__restrict__ F3, int *__restrict__ pflag,
-                                                 int *__restrict__ failimage, int full, StepSize st) {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)d.n1 * d.n2 * d.n3) return;
-    const int z = d.ng3 + (int)(t % d.n3);
-    const int j = d.ng2 + (int)((t / d.n3) % d.n2);
-    const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
-    const long c = cix(d, i, j, z), gi = gix(d, i, j);
+// Conserved update of one active zone (fixup, GPU_fixup.h:5-424, up to the
+// inversion): U(p^n) computed and cached by the half sub-step or read back by
+// the full one, minus the flux divergence, plus the geometric source at the
+// stage's primitives; U[B] from the face-averaged staggered field. pf returns
+// the stage's primitives (the inversion's initial guess).
+template <typename T>
+__device__ __forceinline__ void cons_update(const Dims &d, const Geom &m, const double *__restrict__ pin,
+                                            const double *__restrict__ pb, double *__restrict__ Ucache,
+                                            const T *__restrict__ F1, const T *__restrict__ F2,
+                                            const T *__restrict__ F3, int full, double Dt, int i, int j,
+                                            long c, long gi, const Geo<double> &gm, double *pf, double *U) {
     const long ks = d.ks, isize = (long)d.G2 * d.G3;
-    const double Dt = st.sub();
-    Geo<double> gm;
-    load_geo(d, m, i, j, CENT, gm);
     State<double> q;
-    double pf[NPR], U[NPR], dU[NPR];
+    double dU[NPR];
     if (!full) {
 #pragma unroll
         for (int k = 0; k < NPR; k++) { pf[k] = 0.0; pf[k] += (1.0 / ((double)1)) * pin[k * ks + c]; }
@@ -403,34 +425,139 @@ __global__ void __launch_bounds__(BLK) k_update(const Dims d, const Geom m, cons
         for (int k = 0; k < NPR; k++) { pf[k] = 0.0; pf[k] += (1.0 / ((double)1)) * pb[k * ks + c]; }
         get_state(pf, gm, q);
     }
+    if constexpr (sizeof(T) == sizeof(double)) {
 #pragma unroll
-    for (int k = 0; k < NPR; k++) {
-        if (d.ng1 > 0) U[k] -= Dt * (F1[k * ks + c + isize] - F1[k * ks + c]) / (d.dx1 * (double)1);
-        if (d.ng2 > 0) U[k] -= Dt * (F2[k * ks + c + d.G3] - F2[k * ks + c]) / (d.dx2 * (double)1);
-        if (d.ng3 > 0) U[k] -= Dt * (F3[k * ks + c + 1] - F3[k * ks + c]) / (d.dx3 * (double)1);
+        for (int k = 0; k < NPR; k++) {
+            if (d.ng1 > 0) U[k] -= Dt * (F1[k * ks + c + isize] - F1[k * ks + c]) / (d.dx1 * (double)1);
+            if (d.ng2 > 0) U[k] -= Dt * (F2[k * ks + c + d.G3] - F2[k * ks + c]) / (d.dx2 * (double)1);
+            if (d.ng3 > 0) U[k] -= Dt * (F3[k * ks + c + 1] - F3[k * ks + c]) / (d.dx3 * (double)1);
+        }
+        source(d.gam, pf, gm, d, m, gi, dU, q);
+#pragma unroll
+        for (int k = 0; k < NPR; k++) U[k] += Dt * (dU[k]);
+    } else {
+        // float fluxes: differences taken in double (exact for two floats of
+        // similar size) and the four increments added to U^n with Neumaier
+        // compensated summation
+        source(d.gam, pf, gm, d, m, gi, dU, q);
+#pragma unroll
+        for (int k = 0; k < NPR; k++) {
+            double sum = U[k], comp = 0.;
+            auto add = [&](double x) {
+                const double tt = sum + x;
+                comp += fabs(sum) >= fabs(x) ? (sum - tt) + x : (x - tt) + sum;
+                sum = tt;
+            };
+            if (d.ng1 > 0) add(-Dt * ((double)F1[k * ks + c + isize] - (double)F1[k * ks + c]) / d.dx1);
+            if (d.ng2 > 0) add(-Dt * ((double)F2[k * ks + c + d.G3] - (double)F2[k * ks + c]) / d.dx2);
+            if (d.ng3 > 0) add(-Dt * ((double)F3[k * ks + c + 1] - (double)F3[k * ks + c]) / d.dx3);
+            add(Dt * dU[k]);
+            U[k] = sum + comp;
+        }
     }
-    source(d.gam, pf, gm, d, m, gi, dU, q);
-#pragma unroll
-    for (int k = 0; k < NPR; k++) U[k] += Dt * (dU[k]);
+}
+
+// U[B] from the face-averaged staggered field (fixup, GPU_fixup.h:330-345)
+__device__ __forceinline__ void face_average_b(const Dims &d, const Geom &m, const double *__restrict__ psf, int i,
+                                               int j, long c, long gi, double *U) {
+    const long ks = d.ks, isize = (long)d.G2 * d.G3;
     U[B1] = 0.0;
     U[B2] = 0.0;
     U[B1] += (psf[0 * ks + c] * m.gdet[FACE1 * d.gs + gi] + psf[0 * ks + c + isize] * m.gdet[FACE1 * d.gs + gix(d, i + d.d1, j)]) / (2.0 * (double)1);
     U[B2] += (psf[1 * ks + c] * m.gdet[FACE2 * d.gs + gi] + psf[1 * ks + c + d.G3] * m.gdet[FACE2 * d.gs + gix(d, i, j + d.d2)]) / (2.0 * (double)1);
     if (d.ng3 > 0)
         U[B3] = (psf[2 * ks + c] * m.gdet[FACE3 * d.gs + gi] + psf[2 * ks + c + 1 * d.d3] * m.gdet[FACE3 * d.gs + gi]) / 2.0;
+}
+
+// Noble 2D inversion with the 1dvsq2fix1 and 1dfix1 fallbacks, recording the
+// outcome in pflag and the failure counters (fixup, GPU_fixup.h:346-382)
+__device__ __forceinline__ void invert_zone(const Dims &d, const Geo<double> &gm, long c, double *U, double *pf,
+                                            double *__restrict__ pout, int *__restrict__ pflag,
+                                            int *__restrict__ failimage) {
+    const long ks = d.ks;
     int flag = utoprim_2d(d.gam, U, gm.gcov, gm.gcon, gm.g, pf);
     if (flag) {
+        // rare path: the fallbacks work on copies so that U and pf can stay
+        // in registers on the common path
+        double Uc[NPR], pc[NPR], gcv[10], gcn[10];
+#pragma unroll
+        for (int k = 0; k < NPR; k++) { Uc[k] = U[k]; pc[k] = pf[k]; }
+#pragma unroll
+        for (int k = 0; k < 10; k++) { gcv[k] = gm.gcov[k]; gcn[k] = gm.gcon[k]; }
         failimage[c]++;
-        flag = utoprim_1dvsq2fix1(d.gam, U, gm.gcov, gm.gcon, gm.g, pf);
+        flag = utoprim_1dvsq2fix1(d.gam, Uc, gcv, gcn, gm.g, pc);
         if (flag) {
             failimage[1 * ks + c]++;
-            flag = utoprim_1dfix1(d.gam, U, gm.gcov, gm.gcon, gm.g, pf);
+            flag = utoprim_1dfix1(d.gam, Uc, gcv, gcn, gm.g, pc);
             if (flag) failimage[2 * ks + c]++;
         }
+#pragma unroll
+        for (int k = 0; k < NPR; k++) pf[k] = pc[k];
     }
     pflag[c] = flag;
 #pragma unroll
     for (int k = 0; k < NPR; k++) pout[k * ks + c] = pf[k];
+}
+
+// build option: minimum resident blocks of 128 threads per SM for the
+// inversion kernel (caps its registers per thread)
+#ifndef HAMR_UPD_MINB
+#define HAMR_UPD_MINB 5
+#endif
+
+// The update in two kernels, so that each holds fewer registers and more
+// zones are in flight: k_cons writes the six non-magnetic conserved variables
+// and U[B3] to seven scratch planes W; k_invert reads them back, sets U[B]
+// from the faces and inverts.
+template <typename T>
+__global__ void __launch_bounds__(BLK) k_cons(const Dims d, const Geom m, const double *__restrict__ pin,
+                                               const double *__restrict__ pb, double *__restrict__ Ucache,
+                                               const T *__restrict__ F1, const T *__restrict__ F2,
+                                               const T *__restrict__ F3, double *__restrict__ W, int full,
+                                               StepSize st) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)d.n1 * d.n2 * d.n3) return;
+    const int z = d.ng3 + (int)(t % d.n3);
+    const int j = d.ng2 + (int)((t / d.n3) % d.n2);
+    const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
+    const long c = cix(d, i, j, z), gi = gix(d, i, j);
+    Geo<double> gm;
+    load_geo(d, m, i, j, CENT, gm);
+    double pf[NPR], U[NPR];
+    cons_update<T>(d, m, pin, pb, Ucache, F1, F2, F3, full, st.sub(), i, j, c, gi, gm, pf, U);
+    W[0 * d.ks + c] = U[RHO];
+    W[1 * d.ks + c] = U[UU];
+    W[2 * d.ks + c] = U[U1];
+    W[3 * d.ks + c] = U[U2];
+    W[4 * d.ks + c] = U[U3];
+    W[5 * d.ks + c] = U[KTOT];
+    W[6 * d.ks + c] = U[B3];   // kept in 2-D, where the faces do not set it
+}
+
+__global__ void __launch_bounds__(BLK, HAMR_UPD_MINB) k_invert(const Dims d, const Geom m, const double *__restrict__ pg,
+                                                 const double *__restrict__ W, const double *__restrict__ psf,
+                                                 double *__restrict__ pout, int *__restrict__ pflag,
+                                                 int *__restrict__ failimage) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)d.n1 * d.n2 * d.n3) return;
+    const int z = d.ng3 + (int)(t % d.n3);
+    const int j = d.ng2 + (int)((t / d.n3) % d.n2);
+    const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
+    const long c = cix(d, i, j, z), gi = gix(d, i, j);
+    Geo<double> gm;
+    load_geo(d, m, i, j, CENT, gm);
+    double pf[NPR], U[NPR];
+#pragma unroll
+    for (int k = 0; k < NPR; k++) pf[k] = pg[k * d.ks + c];
+    U[RHO] = W[0 * d.ks + c];
+    U[UU] = W[1 * d.ks + c];
+    U[U1] = W[2 * d.ks + c];
+    U[U2] = W[3 * d.ks + c];
+    U[U3] = W[4 * d.ks + c];
+    U[KTOT] = W[5 * d.ks + c];
+    U[B3] = W[6 * d.ks + c];
+    face_average_b(d, m, psf, i, j, c, gi, U);
+    invert_zone(d, gm, c, U, pf, pout, pflag, failimage);
 }
 
 // ------------------------------------------------------------ ghost fills
@@ -674,6 +801,7 @@ struct hamr_ctx {
     // device state
     double *p = nullptr, *ph = nullptr, *ps = nullptr, *psh = nullptr, *U = nullptr;
     double *F1 = nullptr, *F2 = nullptr, *F3 = nullptr, *Ec = nullptr, *emf = nullptr;
+    double *W = nullptr;  // updated conserved variables between k_cons and k_invert
     int *pflag = nullptr, *failimage = nullptr;
     double *gcov = nullptr, *gcon = nullptr, *gdet = nullptr, *conn = nullptr;
     unsigned long long *dtbits = nullptr;
@@ -702,7 +830,7 @@ Geom geom_of(const hamr_ctx *c) { return Geom{c->gcov, c->gcon, c->gdet, c->conn
 
 // kernel groups timed by hamr_profile_step
 enum { PROF_FLUX3, PROF_FLUX2, PROF_FLUX1, PROF_FIXFLUX, PROF_EMF_CENTRE, PROF_EMF_EDGE, PROF_POLE_AVG,
-       PROF_FACE, PROF_UPDATE, PROF_BOUND, PROF_NSLOT };
+       PROF_FACE, PROF_UPDATE, PROF_INVERT, PROF_BOUND, PROF_NSLOT };
 
 struct Prof {
     cudaEvent_t ev[PROF_NSLOT + 1];
@@ -713,9 +841,22 @@ inline void prof_mark(Prof *pf, int slot, cudaStream_t s) {
     if (pf && pf->on) cudaEventRecord(pf->ev[slot + 1], s);
 }
 
-// one sub-step: fluxes, CT, update, ghost fill of the written state
-int launch_stage(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf = nullptr) {
+// n faces of direction DIR, one thread per face
+template <int DIR, typename T>
+void launch_flux(long n, cudaStream_t s, const Dims &d, const Geom &m, const double *pin, const double *psin, T *F,
+                 unsigned long long *dtbits, int cd) {
+    k_flux<DIR, T><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd);
+}
+
+// one sub-step: fluxes, CT, update, ghost fill of the written state. T is the
+// type of the fluxes and EMFs (double, or float in the mixed-precision step);
+// the float arrays reuse the double allocations with the same plane stride.
+template <typename T>
+int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf) {
     const Dims &d = ctx->d;
+    T *F1 = reinterpret_cast<T *>(ctx->F1), *F2 = reinterpret_cast<T *>(ctx->F2);
+    T *F3 = reinterpret_cast<T *>(ctx->F3), *Ec = reinterpret_cast<T *>(ctx->Ec);
+    T *emf = reinterpret_cast<T *>(ctx->emf);
     const Geom m = geom_of(ctx);
     cudaStream_t s = ctx->stream;
     const double *pin = full ? ctx->ph : ctx->p;
@@ -723,46 +864,48 @@ int launch_stage(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf = 
     const int cd = calc_dt ? 1 : 0;
     if (d.d3) {
         long n = (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3 - 1);
-        k_flux<3><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, ctx->F3, ctx->dtbits, cd);
+        launch_flux<3, T>(n, s, d, m, pin, psin, F3, ctx->dtbits, cd);
     }
     prof_mark(pf, PROF_FLUX3, s);
     {
         long n = (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2 - 1) * (d.n3 + 2 * d.d3);
-        k_flux<2><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, ctx->F2, ctx->dtbits, cd);
+        launch_flux<2, T>(n, s, d, m, pin, psin, F2, ctx->dtbits, cd);
     }
     prof_mark(pf, PROF_FLUX2, s);
     {
         long n = (long)(d.n1 + 2 * d.d1 - 1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3);
-        k_flux<1><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, ctx->F1, ctx->dtbits, cd);
+        launch_flux<1, T>(n, s, d, m, pin, psin, F1, ctx->dtbits, cd);
     }
     prof_mark(pf, PROF_FLUX1, s);
     if (d.bc2 == HAMR_BC_POLE_REFL) {
         long n = (long)d.G1 * d.G3 + (long)d.G2 * d.G3;
-        k_fix_flux<<<nblk(n), BLK, 0, s>>>(d, ctx->F1, ctx->F2, ctx->F3);
+        k_fix_flux<T><<<nblk(n), BLK, 0, s>>>(d, F1, F2, F3);
     }
     prof_mark(pf, PROF_FIXFLUX, s);
     {
         long n = (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3);
-        k_emf_centre<<<nblk(n), BLK, 0, s>>>(d, m, pin, ctx->Ec);
+        k_emf_centre<T><<<nblk(n), BLK, 0, s>>>(d, m, pin, Ec);
     }
     prof_mark(pf, PROF_EMF_CENTRE, s);
     {
         long n = (long)(d.n1 + d.d1) * (d.n2 + d.d2) * (d.n3 + d.d3);
-        k_emf_edge<<<nblk(n), BLK, 0, s>>>(d, ctx->Ec, ctx->F1, ctx->F2, ctx->F3, ctx->emf);
+        k_emf_edge<T><<<nblk(n), BLK, 0, s>>>(d, Ec, F1, F2, F3, emf);
         prof_mark(pf, PROF_EMF_EDGE, s);
         if (d.bc2 == HAMR_BC_POLE_TRANS)
-            k_pole_average<<<nblk(2L * (d.n1 + d.ng1)), BLK, 0, s>>>(d, ctx->emf, st);
+            k_pole_average<T><<<nblk(2L * (d.n1 + d.ng1)), BLK, 0, s>>>(d, emf, st);
         prof_mark(pf, PROF_POLE_AVG, s);
-        k_face_update<<<nblk(n), BLK, 0, s>>>(d, m, ctx->ps, full ? ctx->ps : ctx->psh, ctx->emf, st);
+        k_face_update<T><<<nblk(n), BLK, 0, s>>>(d, m, ctx->ps, full ? ctx->ps : ctx->psh, emf, st);
         prof_mark(pf, PROF_FACE, s);
     }
     {
         long n = (long)d.n1 * d.n2 * d.n3;
-        k_update<<<nblk(n), BLK, 0, s>>>(d, m, ctx->p, full ? ctx->ph : ctx->p, full ? ctx->p : ctx->ph, ctx->U,
-                                        full ? ctx->ps : ctx->psh, ctx->F1, ctx->F2, ctx->F3, ctx->pflag,
-                                        ctx->failimage, full, st);
+k_cons<T><<<nblk(n), BLK, 0, s>>>(d, m, ctx->p, full ? ctx->ph : ctx->p, ctx->U, F1, F2, F3, ctx->W, full,
+                                         st);
+        prof_mark(pf, PROF_UPDATE, s);
+        k_invert<<<nblk(n), BLK, 0, s>>>(d, m, full ? ctx->ph : ctx->p, ctx->W, full ? ctx->ps : ctx->psh,
+                                         full ? ctx->p : ctx->ph, ctx->pflag, ctx->failimage);
     }
-    prof_mark(pf, PROF_UPDATE, s);
+    prof_mark(pf, PROF_INVERT, s);
     double *pw = full ? ctx->p : ctx->ph;
     double *psw = full ? ctx->ps : ctx->psh;
     if (d.d1) k_bound_x1<<<nblk((long)d.ng1 * d.G2 * d.G3), BLK, 0, s>>>(d, m, pw, psw);
@@ -771,6 +914,11 @@ int launch_stage(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf = 
     prof_mark(pf, PROF_BOUND, s);
     CK(cudaGetLastError());
     return HAMR_OK;
+}
+
+int launch_stage(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf = nullptr) {
+    if (ctx->prm.precision == HAMR_MIXED) return launch_stage_t<float>(ctx, full, st, calc_dt, pf);
+    return launch_stage_t<double>(ctx, full, st, calc_dt, pf);
 }
 
 int launch_step(hamr_ctx *ctx, StepSize half, StepSize full, double *dt_state, int interval) {
@@ -791,7 +939,7 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
     if (!prm || !out) return HAMR_E_ARG;
     *out = nullptr;
     if (prm->n1 < 2 || prm->n2 < 2 || prm->n3 < 1 || prm->ng != 3) return HAMR_E_ARG;
-    if (prm->precision != HAMR_FP64) return HAMR_E_ARG;
+    if (prm->precision != HAMR_FP64 && prm->precision != HAMR_MIXED) return HAMR_E_ARG;
     if (prm->n3 > 1 && prm->bc3 != HAMR_BC_PERIODIC) return HAMR_E_ARG;
     if (prm->bc2 == HAMR_BC_POLE_TRANS && (prm->n3 < 2 || prm->n3 % 2)) return HAMR_E_ARG;
     if (!(prm->gam > 1.0) || !(prm->cour > 0.0) || !(prm->dx1 > 0) || !(prm->dx2 > 0) || !(prm->dx3 > 0)) return HAMR_E_ARG;
@@ -823,7 +971,7 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
         {(void **)&ctx->p, NPR * cb}, {(void **)&ctx->ph, NPR * cb}, {(void **)&ctx->ps, 3 * cb},
         {(void **)&ctx->psh, 3 * cb}, {(void **)&ctx->U, NPR * cb}, {(void **)&ctx->F1, NPR * cb},
         {(void **)&ctx->F2, NPR * cb}, {(void **)&ctx->F3, NPR * cb}, {(void **)&ctx->Ec, 4 * cb},
-        {(void **)&ctx->emf, 4 * cb}, {(void **)&ctx->pflag, sizeof(int) * d.ks},
+        {(void **)&ctx->emf, 4 * cb}, {(void **)&ctx->W, 7 * cb}, {(void **)&ctx->pflag, sizeof(int) * d.ks},
         {(void **)&ctx->failimage, 4 * sizeof(int) * d.ks},
         {(void **)&ctx->gcov, 50 * sizeof(double) * d.gs}, {(void **)&ctx->gcon, 50 * sizeof(double) * d.gs},
         {(void **)&ctx->gdet, 5 * sizeof(double) * d.gs}, {(void **)&ctx->conn, 40 * sizeof(double) * d.gs},
@@ -851,7 +999,7 @@ int hamr_ctx_destroy(hamr_ctx *ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
     void *bufs[] = {ctx->p, ctx->ph, ctx->ps, ctx->psh, ctx->U, ctx->F1, ctx->F2, ctx->F3, ctx->Ec, ctx->emf,
-                    ctx->pflag, ctx->failimage, ctx->gcov, ctx->gcon, ctx->gdet, ctx->conn, ctx->dtbits,
+                    ctx->W, ctx->pflag, ctx->failimage, ctx->gcov, ctx->gcon, ctx->gdet, ctx->conn, ctx->dtbits,
                     ctx->ndt, ctx->dt_state, ctx->counter, ctx->divb};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -1043,7 +1191,7 @@ int hamr_divb_max(hamr_ctx *ctx, double *out) {
 // them, so calls that overlap on the GPU race.
 namespace {
 
-constexpr long NA_DPLANES = 9 + 3 + 9 + 27 + 4 + 4;  // ph, psh, U, F1-F3, E_cent, emf
+constexpr long NA_DPLANES = 9 + 3 + 9 + 27 + 4 + 4 + 7;  // ph, psh, U, F1-F3, E_cent, emf, W
 constexpr long NA_IPLANES = 1 + 4;                   // pflag, failimage
 static __device__ __align__(256) double na_scratch[NA_DPLANES * HAMR_NOALLOC_MAX_CELLS];
 static __device__ __align__(256) int na_iscratch[NA_IPLANES * HAMR_NOALLOC_MAX_CELLS];
@@ -1121,6 +1269,7 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
     c.F3 = c.F2 + 9 * ks;
     c.Ec = c.F3 + 9 * ks;
     c.emf = c.Ec + 4 * ks;
+    c.W = c.emf + 4 * ks;
     c.pflag = q.iscratch;
     c.failimage = q.iscratch + ks;
     c.gcov = const_cast<double *>(gcov);

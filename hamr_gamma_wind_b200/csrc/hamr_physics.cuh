@@ -266,7 +266,7 @@ __device__ __forceinline__ double vsq_of_W(double W, double Bsq, double Qtsq, do
 }
 
 // Noble et al. 2006, 2D Newton-Raphson on (W, v^2)
-__device__ __noinline__ int utoprim_2d(double gam, const double *U, const double *gcov, const double *gcon, double gdet, double *prim) {
+__device__ __forceinline__ int utoprim_2d(double gam, const double *U, const double *gcov, const double *gcon, double gdet, double *prim) {
     double Ut[NPR], pt[5];
     int ret = inv_prologue(U, gdet, gcon, prim, Ut);
     if (ret) return ret;

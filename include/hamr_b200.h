@@ -125,9 +125,9 @@ int hamr_advance(hamr_ctx *ctx, int nsteps, int interval, double *dt_inout);
 
 /* Per-kernel-group device times of `reps` RK2 steps of size dt (the state
  * advances), averaged per step, from CUDA events recorded between the groups
- * on the context stream: ms[0..9] = x3 flux, x2 flux, x1 flux, polar flux
+ * on the context stream: ms[0..10] = x3 flux, x2 flux, x1 flux, polar flux
  * fix, centre EMF, edge EMF, polar EMF average, face update, conserved
- * update + inversion, ghost fill. nslots must be >= 10. */
+ * update, inversion, ghost fill. nslots must be >= 11. */
 int hamr_profile_step(hamr_ctx *ctx, double dt, int reps, double *ms, int nslots);
 
 /* Device pointers of the live state, for zero-copy access (e.g. DLPack or

@@ -931,6 +931,92 @@ int ho_utoprim_1dfix1(double gam, double *U, const double *gcov, const double *g
     return ret;
 }
 
+/* Newman & Hamlin (2014) inversion: fixed point on the pressure with a
+ * closed-form cubic root for W and Aitken acceleration (GPU_utoprim_nm.h).
+ * The reference keeps the pressure history in p_array[3] but indexes it up to
+ * the iteration count (at most 30) when the Aitken step does not trigger;
+ * here the history has room for every iteration, so those writes land in
+ * their own slots instead of the neighbouring stack. */
+static int nm_last_max_index;
+/* largest pressure-history index the last ho_utoprim_nm call used; the
+ * reference's 3-slot history is only well defined when it is <= 2 */
+int ho_utoprim_nm_max_index(void) { return nm_last_max_index; }
+
+int ho_utoprim_nm(double gam, double *U, const double *gcov, const double *gcon, double gdet, double *prim) {
+    double U_tmp[NPR], pt[5];
+    nm_last_max_index = 0;
+    int ret = inv_prologue(U, gdet, gcon, prim, U_tmp);
+    if (ret) return ret;
+    for (int i = 0; i < B1; i++) pt[i] = prim[i];
+    invq s;
+    inv_scalars(U_tmp, gcov, gcon, &s);
+    const double Bsq = s.Bsq, QdotBsq = s.QdotBsq, Qtsq = s.Qtsq, Qdotn = s.Qdotn;
+    double a, d, z = 0., phi, R, Wsq, p_array[32], epsilon, p_old, p_new, vsq, w, gamma = 1., rho0 = 0., u = 0., errx;
+    int iter = 0, iter_tot = 0, set_variables = 0;
+    const double gamma_eos = gam;
+    p_array[0] = (gamma_eos - 1.) * pt[UU];
+    p_new = p_array[0];
+    d = 0.5 * (Qtsq * Bsq - QdotBsq);
+    if (d < 0.0) return 1;
+    do {
+        set_variables = 0;
+        a = -Qdotn + p_new + 0.5 * Bsq;
+        phi = acos(1. / a * sqrt((27. * d) / (4. * a)));
+        epsilon = a / 3. - 2. / 3. * a * cos(2. / 3. * phi + 2. / 3. * 3.14159265358979323846);
+        z = epsilon - Bsq;
+        vsq = (Qtsq * z * z + QdotBsq * (Bsq + 2. * z)) / (z * z * pow(Bsq + z, 2.));
+        if (fabs(vsq) < 1e-15) vsq = 0.0;
+        if (fabs(vsq) >= 1.0) return 1;
+        Wsq = 1. / (1. - vsq);
+        w = z * (1. - vsq);
+        gamma = 1. / sqrt(1. - vsq);
+        rho0 = U_tmp[RHO] / gamma;
+        u = (w - rho0) / gamma_eos;
+        iter++;
+        iter_tot++;
+        if (iter > nm_last_max_index) nm_last_max_index = iter;
+        p_array[iter] = (gamma_eos - 1.) * u;
+        p_old = p_array[iter - 1];
+        p_new = p_array[iter];
+        if (iter >= 2) {
+            R = (p_array[iter] - p_array[iter - 1]) / (p_array[iter - 1] - p_array[iter - 2]);
+            if (R < 1. && R > 0.) {
+                set_variables = 1;
+                p_new = p_array[iter - 1] + (p_array[iter] - p_array[iter - 1]) / (1. - R);
+                p_old = p_array[iter];
+                iter = 0;
+                p_array[iter] = p_new;
+            }
+        }
+        errx = fabs(p_new - p_old) / fabs(p_new + p_old);
+    } while (errx > NEWT_TOL && iter_tot < 30);
+    if (fabs(errx) > MY_MIN(NEWT_TOL, MIN_NEWT_TOL)) return 1;
+    if (set_variables == 1) {
+        a = -Qdotn + p_new + 0.5 * Bsq;
+        phi = acos(1. / a * sqrt((27. * d) / (4. * a)));
+        epsilon = a / 3. - 2. / 3. * a * cos(2. / 3. * phi + 2. / 3. * 3.14159265358979323846);
+        z = epsilon - Bsq;
+        vsq = (Qtsq * z * z + QdotBsq * (Bsq + 2. * z)) / (z * z * pow(Bsq + z, 2.));
+        Wsq = 1. / (1. - vsq);
+        w = z / Wsq;
+        if (vsq >= 1.0 || vsq < 0. || z <= 0. || z > 1.e20 || !isfinite(vsq) || !isfinite(z)) return 4;
+        gamma = sqrt(Wsq);
+        rho0 = U_tmp[RHO] / gamma;
+        u = (w - rho0) / gamma_eos;
+        p_new = (gamma_eos - 1.) * u;
+    }
+    if (rho0 < 0.0) return 5;
+    if (p_new < 0.0) return 6;
+    pt[RHO] = rho0;
+    pt[UU] = u;
+    for (int i = 1; i < 4; i++) {
+        double Qtcon = s.Qcon[i] + s.ncon[i] * s.Qdotn;
+        pt[U1 + i - 1] = gamma / (z + Bsq) * (Qtcon + s.QdotB * s.Bcon[i] / z);
+    }
+    for (int i = 0; i < B1; i++) prim[i] = pt[i];
+    return 0;
+}
+
 /* --------------------------------------------------------------- update -- */
 /* fixup kernel (GPU_fixup.h:5-424): cache U(p^n) on the half step, apply the
  * flux divergence and geometric source, rebuild U[B] from the new face field,
@@ -978,7 +1064,8 @@ static void update(const ho_grid *g, const dims *d, const ho_geom *m, ho_state *
                 U[B2] += (psf[1 * ks + c] * m->gdet[FACE2 * d->gs + gi] + psf[1 * ks + c + d->G3] * m->gdet[FACE2 * d->gs + gix(d, i, j + d->d2)]) / (2.0 * (double)1);
                 if (d->ng3 > 0)
                     U[B3] = (psf[2 * ks + c] * m->gdet[FACE3 * d->gs + gi] + psf[2 * ks + c + 1 * d->d3] * m->gdet[FACE3 * d->gs + gi]) / 2.0;
-                int flag = ho_utoprim_2d(g->gam, U, gm.gcov, gm.gcon, gm.g, pf);
+                int flag = g->inversion == 1 ? ho_utoprim_nm(g->gam, U, gm.gcov, gm.gcon, gm.g, pf)
+                                             : ho_utoprim_2d(g->gam, U, gm.gcov, gm.gcon, gm.g, pf);
                 if (flag) {
                     s->failimage[c]++;
                     flag = ho_utoprim_1dvsq2fix1(g->gam, U, gm.gcov, gm.gcon, gm.g, pf);

@@ -65,6 +65,8 @@ void ho_primtoflux(double gam, const double *pr, const double *gcov10, const dou
 int ho_utoprim_2d(double gam, double *U, const double *gcov10, const double *gcon10, double gdet, double *prim);
 int ho_utoprim_1dvsq2fix1(double gam, double *U, const double *gcov10, const double *gcon10, double gdet, double *prim);
 int ho_utoprim_1dfix1(double gam, double *U, const double *gcov10, const double *gcon10, double gdet, double *prim);
+int ho_utoprim_nm(double gam, double *U, const double *gcov10, const double *gcon10, double gdet, double *prim);
+int ho_utoprim_nm_max_index(void);
 
 /* Diagnostics */
 double ho_divb_max(const ho_grid *g, const ho_geom *m, const double *ps);

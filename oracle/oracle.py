@@ -66,10 +66,11 @@ def lib():
         L.ho_bound.argtypes = [ctypes.POINTER(HoGrid), ctypes.POINTER(HoGeom), _vp, _vp]
         L.ho_para.argtypes = [_vp, _vp, _vp]
         L.ho_primtoflux.argtypes = [_d, _vp, _vp, _vp, _d, _i, _vp, _vp, _vp]
-        for nm in ("ho_utoprim_2d", "ho_utoprim_1dvsq2fix1", "ho_utoprim_1dfix1"):
+        for nm in ("ho_utoprim_2d", "ho_utoprim_1dvsq2fix1", "ho_utoprim_1dfix1", "ho_utoprim_nm"):
             f = getattr(L, nm)
             f.argtypes = [_d, _vp, _vp, _vp, _d, _vp]
             f.restype = _i
+        L.ho_utoprim_nm_max_index.restype = _i
         L.ho_divb_max.argtypes = [ctypes.POINTER(HoGrid), ctypes.POINTER(HoGeom), _vp]
         L.ho_divb_max.restype = _d
         _lib = L

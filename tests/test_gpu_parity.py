@@ -135,3 +135,19 @@ def test_graph_advance_matches_step_loop():
     assert dt_a == dt
     a.close()
     b.close()
+
+
+def test_bench_size_torus_strict():
+    """The 192 x 96 x 64 torus of the benchmark (r_out = 1000), one step of the
+    strict build against the oracle: the kernels' index arithmetic and launch
+    shapes at a production block size, not only at the small test sizes."""
+    pb = problems.fm_torus(192, 96, 64, rout=1000.0)
+    blk, s = make_pair(pb, strict=True)
+    dt = 0.2 * min(pb.dx[:2])
+    dn_gpu = blk.step(dt)
+    dn_orc = oracle_step(s, dt)
+    p, ps = blk.download()
+    assert field_rel_err(blk, p, s, "p").max() <= 1e-14
+    assert field_rel_err(blk, ps, s, "ps").max() <= 1e-14
+    assert abs(dn_gpu - dn_orc) <= 1e-14 * dn_orc
+    blk.close()

@@ -141,7 +141,7 @@ def test_single_cell_pieces(variant):
         np.testing.assert_array_equal(v1, v2)
 
 
-@pytest.mark.parametrize("name", ["2d", "1dvsq2fix1", "1dfix1"])
+@pytest.mark.parametrize("name", ["2d", "1dvsq2fix1", "1dfix1", "nm"])
 def test_inversions_single_cell_bitwise(name):
     """Each inversion of the chain on sampled states whose energy was lowered
     (so that the primary solve is stressed or fails) and whose entropy
@@ -152,6 +152,7 @@ def test_inversions_single_cell_bitwise(name):
     geo, gs, g2 = s.geo, s.blk.gsize, s.blk.g2
     _, gam = O.ref_dims("t3")
     n_ok = n_fail = 0
+    n_skip_nm = [0]
     for trial in range(300):
         i, j = rng.integers(3, 19), rng.integers(3, 11)
         idx = i * g2 + j
@@ -171,10 +172,15 @@ def test_inversions_single_cell_bitwise(name):
         if trial % 3 == 0:
             U[O.KTOT] *= -1.0  # no admissible entropy state: the fallbacks must fail too
         guess = pr * (1 + 0.01 * rng.normal(size=9))
-        r1, p1 = O.ref_utoprim("t3", name, U, gcov, gcon, gdet, guess)
         r2, p2 = O.utoprim(name, gam, U, gcov, gcon, gdet, guess)
+        if name == "nm" and O.lib().ho_utoprim_nm_max_index() > 2:
+            # the reference's 3-slot pressure history overflows here
+            # (GPU_utoprim_nm.h): undefined there, not comparable
+            n_skip_nm[0] += 1
+            continue
+        r1, p1 = O.ref_utoprim("t3", name, U, gcov, gcon, gdet, guess)
         assert r1 == r2, (trial, r1, r2)
         np.testing.assert_array_equal(p1, p2)
         n_ok += r1 == 0
         n_fail += r1 != 0
-    assert n_ok > 20 and n_fail > 20, (n_ok, n_fail)
+    assert n_ok > 20 and n_fail > 20, (n_ok, n_fail, n_skip_nm)
