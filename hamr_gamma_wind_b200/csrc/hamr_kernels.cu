@@ -509,8 +509,14 @@ __device__ __forceinline__ void invert_zone(const Dims &d, const Geo<double> &gm
 // zones are in flight: k_cons writes the six non-magnetic conserved variables
 // and U[B3] to seven scratch planes W; k_invert reads them back, sets U[B]
 // from the faces and inverts.
+// build option: minimum resident blocks of 128 threads per SM for the
+// conserved update (memory-latency bound: more zones in flight pay for the
+// spills of a 64-register cap)
+#ifndef HAMR_CONS_MINB
+#define HAMR_CONS_MINB 8
+#endif
 template <typename T>
-__global__ void __launch_bounds__(BLK) k_cons(const Dims d, const Geom m, const double *__restrict__ pin,
+__global__ void __launch_bounds__(BLK, HAMR_CONS_MINB) k_cons(const Dims d, const Geom m, const double *__restrict__ pin,
                                                const double *__restrict__ pb, double *__restrict__ Ucache,
                                                const T *__restrict__ F1, const T *__restrict__ F2,
                                                const T *__restrict__ F3, double *__restrict__ W, int full,

@@ -40,44 +40,3 @@ def field_rel_err(blk, p_dev, s, name="p"):
         d = np.abs(a[k] - b[k]).max()
         errs.append(0.0 if d == 0 else d / max(scale, 1e-300))
     return np.array(errs)
-
-
-def roundoff_envelope(pb, dt, nsteps=1, seeds=(1, 2), rel=1e-15):
-    """Per-variable spread of the oracle's result when its inputs are
-    perturbed by `rel` (relative, seeded): the round-off sensitivity of the
-    problem itself. Returns (envelope for p, envelope for ps), each the max
-    over seeds of max|perturbed - unperturbed| per variable."""
-    import numpy as np
-    from oracle import oracle as O
-
-    def run(pert_seed):
-        ob = O.Block(pb.n1, pb.n2, pb.n3, pb.ng, pb.ksize, pb.gsize)
-        p = pb.p.copy()
-        if pert_seed is not None:
-            p *= 1.0 + rel * np.random.default_rng(pert_seed).standard_normal(p.size)
-        ob.arrays["p"][:] = p
-        ob.arrays["ps"][:] = pb.ps
-        geo = O.Geometry(pb.geo.gsize, pb.geo.gcov, pb.geo.gcon, pb.geo.gdet, pb.geo.conn)
-        s = O.Setup(ob, geo, pb.dx, pb.gam, pb.cour, pb.poles[0], pb.poles[1],
-                    tuple(BCMAP[b] for b in pb.bc), int(pb.ct_upwind))
-        O.oracle_bound(s)
-        d = dt
-        for _ in range(nsteps):
-            d = min(oracle_step(s, d), 1.3 * d)
-        return s.blk.active("p"), s.blk.active("ps")
-
-    p0, ps0 = run(None)
-    env_p = np.zeros(p0.shape[0])
-    env_s = np.zeros(ps0.shape[0])
-    for sd in seeds:
-        p1, ps1 = run(sd)
-        env_p = np.maximum(env_p, np.abs(p1 - p0).reshape(p0.shape[0], -1).max(axis=1))
-        env_s = np.maximum(env_s, np.abs(ps1 - ps0).reshape(ps0.shape[0], -1).max(axis=1))
-    return env_p, env_s
-
-
-def abs_diff(blk, a_dev, s, name):
-    import numpy as np
-    a = blk.active(a_dev)
-    b = s.blk.active(name)
-    return np.abs(a - b).reshape(a.shape[0], -1).max(axis=1), np.abs(b).reshape(b.shape[0], -1).max(axis=1)

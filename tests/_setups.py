@@ -70,20 +70,34 @@ def fill_synthetic(blk: O.Block, geo: O.Geometry, dx, seed=1, bamp=0.02, stress=
         P[O.RHO][sel] = 1e-5
 
 
-def make_setup(variant, spin=0.9375, rout=40.0, seed=1, stress=False, cour=0.8):
-    """Reference-variant block with the reference's own geometry tables."""
-    dims, gam = O.ref_dims(variant)
+def product_geometry(coords, spin, n1, n2, n3, gsize, startx, dx):
+    """The library's host metric builder (hamr_build_geometry), which the ABI
+    tests pin bit for bit to the reference's metric code, as oracle tables."""
+    from hamr_gamma_wind_b200 import api
+    g = api.build_geometry(coords, spin, n1, n2, n3, startx, dx, gsize=gsize)
+    return O.Geometry(gsize, g.gcov, g.gcon, g.gdet, g.conn)
+
+
+def make_setup(variant, spin=0.9375, rout=40.0, seed=1, stress=False, cour=0.8, dims=None,
+               geometry="reference"):
+    """Reference-variant block with the reference's own geometry tables
+    (geometry="product": the library's geometry builder instead; dims =
+    ((n1, n2, n3, ..., ksize, gsize), gam) when the reference build is absent)."""
+    dims, gam = dims if dims is not None else O.ref_dims(variant)
     n1, n2, n3 = (int(x) for x in dims[:3])
-    blk = O.Block(n1, n2, n3, 3, int(dims[7]), int(dims[8]))
+    ksize, gsize = int(dims[7]), int(dims[8])
+    blk = O.Block(n1, n2, n3, 3, ksize, gsize)
     if variant == "ot":
         startx = [0.0, 0.0, 0.0, 0.0]
         dx = [0.0, 1.0 / n1, 1.0 / n2, 1.0]
-        geo = O.ref_geometry(variant, 0.0, startx, dx)
+        geo = (O.ref_geometry(variant, 0.0, startx, dx) if geometry == "reference"
+               else product_geometry("cartesian", 0.0, n1, n2, n3, gsize, startx, dx))
         bc = (O.BC_PERIODIC, O.BC_PERIODIC, O.BC_PERIODIC)
         poles = (0, 0)
     else:
         startx, dx = mks_grid(n1, n2, n3, spin, rout)
-        geo = O.ref_geometry(variant, spin, startx, dx)
+        geo = (O.ref_geometry(variant, spin, startx, dx) if geometry == "reference"
+               else product_geometry("ks", spin, n1, n2, n3, gsize, startx, dx))
         bc = (O.BC_OUTFLOW, O.BC_POLE_TRANS if n3 > 1 else O.BC_POLE_REFL, O.BC_PERIODIC)
         poles = (1, 1)
     fill_synthetic(blk, geo, dx, seed=seed, stress=stress)

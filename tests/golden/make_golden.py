@@ -1,0 +1,162 @@
+"""Writes the golden fixtures of tests/test_golden.py from the reference's own
+kernel code, built for the host from the reference sources (oracle/Makefile,
+`make -C oracle ref`). Run from the repository root:
+
+    python tests/golden/make_golden.py
+
+Fixtures (numpy .npz, compressed):
+  ref_cells.npz   single-cell known answers: PPM edge values (para), fluxes and
+                  fast speeds (primtoflux), and the four inversions (Noble 2D,
+                  1dvsq2fix1, 1dfix1, Newman) on stressed states, at metric
+                  points of the 3-D torus grid
+  ref_<v>.npz     per compile-time variant (t3: 3-D torus 16x8x8, t2: 2-D
+                  torus 24x24, ot: 2-D Orszag-Tang box 32x32): the half
+                  sub-step's outputs and the state after two RK2 steps of the
+                  reference kernels on a seeded synthetic block, on the
+                  active zones only; plus SHA-256 digests of the metric tables
+                  and of the initial state, so the test can confirm it rebuilt
+                  exactly the same inputs without the reference present.
+"""
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from oracle import oracle as O  # noqa: E402
+from tests._setups import clone, make_setup  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SEED = 13
+DT = {"t3": 0.002, "t2": 0.002, "ot": 0.002}
+
+
+def digest(*arrays):
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a, np.float64).tobytes())
+    return h.hexdigest()
+
+
+def active(blk, name):
+    return blk.active(name).copy()
+
+
+def variant_fixture(v):
+    dims, gam = O.ref_dims(v)
+    s = make_setup(v, seed=SEED)
+    geo = s.geo
+    out = {"dims": np.asarray(dims, np.int64), "gam": gam,
+           "geo_sha": digest(geo.gcov, geo.gcon, geo.gdet, geo.conn),
+           "in_sha": digest(s.blk.arrays["p"], s.blk.arrays["ps"]), "dt": DT[v]}
+    h = clone(s)
+    d = O.ref_stage(v, h, 0, 0.5 * DT[v], DT[v], True)
+    out["half_ph"] = active(h.blk, "ph")
+    out["half_psh"] = active(h.blk, "psh")
+    out["half_dtdir"] = np.asarray(d)
+    st = clone(s)
+    dt = DT[v]
+    stage = lambda s_, f, Dt, dd, c: O.ref_stage(v, s_, f, Dt, dd, c)
+    bound = lambda s_, a, b: O.oracle_bound(s_, a, b)
+    dts = []
+    for _ in range(2):
+        n = O.step(stage, bound, st, dt)
+        dts.append(n)
+        dt = min(n, 1.3 * dt)
+    out["steps_p"] = active(st.blk, "p")
+    out["steps_ps"] = active(st.blk, "ps")
+    out["steps_dt"] = np.asarray(dts)
+    return out
+
+
+def cell_fixture():
+    rng = np.random.default_rng(SEED)
+    L = O.ref("t3")
+    _, gam = O.ref_dims("t3")
+    s = make_setup("t3", seed=2)
+    geo, gs, g2 = s.geo, s.blk.gsize, s.blk.g2
+    out = {"gam": gam}
+    xs = rng.normal(size=(200, 5)) * rng.choice([1e-3, 1.0, 1e3], size=(200, 1))
+    lr = np.zeros((200, 2))
+    for n, x in enumerate(xs):
+        l1, r1 = np.zeros(1), np.zeros(1)
+        L.ref_para(O._ptr(np.ascontiguousarray(x)), O._ptr(l1), O._ptr(r1))
+        lr[n] = l1[0], r1[0]
+    out["para_x"], out["para_lr"] = xs, lr
+
+    def metric(i, j, loc):
+        idx = i * g2 + j
+        gcov = np.array([geo.gcov[(c * 5 + loc) * gs + idx] for c in range(10)])
+        gcon = np.array([geo.gcon[(c * 5 + loc) * gs + idx] for c in range(10)])
+        return gcov, gcon, geo.gdet[loc * gs + idx]
+
+    rows = []
+    for _ in range(100):
+        i, j, d = int(rng.integers(3, 12)), int(rng.integers(3, 10)), int(rng.integers(0, 4))
+        loc = int(rng.choice([O.FACE1, O.FACE2, O.FACE3, O.CENT]))
+        gcov, gcon, gdet = metric(i, j, loc)
+        pr = np.array([1.0, 0.2, 0.1, 0.01, 0.2, 0.3, 0.02, 0.1, 0.01]) * (1 + 0.2 * rng.random(9))
+        f = np.zeros(9)
+        v = np.zeros(2)
+        L.ref_primtoflux(O._ptr(pr.copy()), O._ptr(gcov), O._ptr(gcon), gdet, d, O._ptr(f), O._ptr(v[:1]),
+                         O._ptr(v[1:]))
+        rows.append((pr, gcov, gcon, gdet, d, f, v))
+    out["ptf_pr"] = np.array([r[0] for r in rows])
+    out["ptf_gcov"] = np.array([r[1] for r in rows])
+    out["ptf_gcon"] = np.array([r[2] for r in rows])
+    out["ptf_gdet"] = np.array([r[3] for r in rows])
+    out["ptf_dir"] = np.array([r[4] for r in rows])
+    out["ptf_flux"] = np.array([r[5] for r in rows])
+    out["ptf_v"] = np.array([r[6] for r in rows])
+
+    for name in ("2d", "1dvsq2fix1", "1dfix1", "nm"):
+        keep = []
+        trial = 0
+        while len(keep) < 80:
+            trial += 1
+            i, j = int(rng.integers(3, 19)), int(rng.integers(3, 11))
+            gcov, gcon, gdet = metric(i, j, O.CENT)
+            rho = 10 ** rng.uniform(-6, 0)
+            u = rho * 10 ** rng.uniform(-4, 0)
+            pr = np.array([rho, u, *(rng.normal(size=3) * 10 ** rng.uniform(-2, 0.5)),
+                           *(rng.normal(size=3) * np.sqrt(rho) * 10 ** rng.uniform(-1, 1.5)), 0.0])
+            flux = np.zeros(9)
+            vv = np.zeros(2)
+            O.lib().ho_primtoflux(gam, O._ptr(pr), O._ptr(gcov), O._ptr(gcon), gdet, 0, O._ptr(flux),
+                                  O._ptr(vv[:1]), O._ptr(vv[1:]))
+            U = flux.copy()
+            U[O.UU] += rng.uniform(0, 3.0) * gdet * u
+            if trial % 3 == 0:
+                U[O.KTOT] *= -1.0
+            guess = pr * (1 + 0.01 * rng.normal(size=9))
+            if name == "nm":
+                O.utoprim("nm", gam, U, gcov, gcon, gdet, guess)
+                if O.lib().ho_utoprim_nm_max_index() > 2:
+                    continue  # outside the reference's 3-slot pressure history
+            r, p = O.ref_utoprim("t3", name, U, gcov, gcon, gdet, guess)
+            keep.append((U, gcov, gcon, gdet, guess, r, p))
+        out[f"inv_{name}_U"] = np.array([k[0] for k in keep])
+        out[f"inv_{name}_gcov"] = np.array([k[1] for k in keep])
+        out[f"inv_{name}_gcon"] = np.array([k[2] for k in keep])
+        out[f"inv_{name}_gdet"] = np.array([k[3] for k in keep])
+        out[f"inv_{name}_guess"] = np.array([k[4] for k in keep])
+        out[f"inv_{name}_ret"] = np.array([k[5] for k in keep])
+        out[f"inv_{name}_prim"] = np.array([k[6] for k in keep])
+    return out
+
+
+def main():
+    for v in ("t3", "t2", "ot"):
+        if not O.ref_available(v):
+            raise SystemExit(f"reference host build {v} missing: run `make -C oracle ref` first")
+        np.savez_compressed(os.path.join(HERE, f"ref_{v}.npz"), **variant_fixture(v))
+    np.savez_compressed(os.path.join(HERE, "ref_cells.npz"), **cell_fixture())
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")
+
+
+if __name__ == "__main__":
+    main()
