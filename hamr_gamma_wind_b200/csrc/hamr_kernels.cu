@@ -35,7 +35,7 @@ struct Dims {
     int n1, n2, n3, ng1, ng2, ng3, G1, G2, G3, d1, d2, d3;
     long ks, gs;
     double dx1, dx2, dx3, gam, cour;
-    int pole1, pole2, bc1, bc2, bc3, ct_upwind;
+    int pole1, pole2, bc1, bc2, bc3, ct_upwind, inversion, recon;
 };
 
 struct Geom {
@@ -88,7 +88,7 @@ struct StepSize {
 #ifndef HAMR_FLUX_MINB_F
 #define HAMR_FLUX_MINB_F 6
 #endif
-template <int DIR, typename T>
+template <int DIR, typename T, int REC>
 __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? HAMR_FLUX_MINB : HAMR_FLUX_MINB_F) k_flux(const Dims d, const Geom m, const double *__restrict__ pv,
                                                const double *__restrict__ ps, T *__restrict__ F,
                                                unsigned long long *__restrict__ dtbits, int calc_dt) {
@@ -112,14 +112,25 @@ __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? HAMR_FLUX_MINB : HAMR_FL
 #pragma unroll
         for (int k = 0; k < NPR; k++) {
             const double *pk = pv + (long)k * d.ks + c;
-            T x[6];
+            if constexpr (REC == HAMR_RECON_MC) {
+                // linear MC: the zones' face values y -+ slope/2 (fluxcalcprep, PPM = 0)
+                T x[4];
 #pragma unroll
-            for (int s = 0; s < 6; s++) x[s] = (T)__ldg(pk + (s - 3) * stride);
-            T lo, hi;
-            para(x, lo, hi);       // zone c-1: upper edge is the left state
-            pl[k] = hi;
-            para(x + 1, lo, hi);   // zone c: lower edge is the right state
-            pr[k] = lo;
+                for (int s = 0; s < 4; s++) x[s] = (T)__ldg(pk + (s - 2) * stride);
+                T temp = T(0.5) * slope_lim(x[0], x[1], x[2]);
+                pl[k] = x[1] + temp;
+                temp = T(0.5) * slope_lim(x[1], x[2], x[3]);
+                pr[k] = x[2] - temp;
+            } else {
+                T x[6];
+#pragma unroll
+                for (int s = 0; s < 6; s++) x[s] = (T)__ldg(pk + (s - 3) * stride);
+                T lo, hi;
+                para(x, lo, hi);       // zone c-1: upper edge is the left state
+                pl[k] = hi;
+                para(x + 1, lo, hi);   // zone c: lower edge is the right state
+                pr[k] = lo;
+            }
         }
         const T bn = (T)__ldg(&ps[(long)(DIR - 1) * d.ks + c]);
         pl[B1 + DIR - 1] = bn;
@@ -469,13 +480,16 @@ __device__ __forceinline__ void face_average_b(const Dims &d, const Geom &m, con
         U[B3] = (psf[2 * ks + c] * m.gdet[FACE3 * d.gs + gi] + psf[2 * ks + c + 1 * d.d3] * m.gdet[FACE3 * d.gs + gi]) / 2.0;
 }
 
-// Noble 2D inversion with the 1dvsq2fix1 and 1dfix1 fallbacks, recording the
+// Primary inversion with the 1dvsq2fix1 and 1dfix1 fallbacks, recording the
 // outcome in pflag and the failure counters (fixup, GPU_fixup.h:346-382)
+template <int INV>
 __device__ __forceinline__ void invert_zone(const Dims &d, const Geo<double> &gm, long c, double *U, double *pf,
                                             double *__restrict__ pout, int *__restrict__ pflag,
                                             int *__restrict__ failimage) {
     const long ks = d.ks;
-    int flag = utoprim_2d(d.gam, U, gm.gcov, gm.gcon, gm.g, pf);
+    // primary solver: Noble 2D, or Newman-Hamlin in its place (NEWMAN builds)
+    int flag = INV == HAMR_INV_NM ? utoprim_nm(d.gam, U, gm.gcov, gm.gcon, gm.g, pf)
+                                  : utoprim_2d(d.gam, U, gm.gcov, gm.gcon, gm.g, pf);
     if (flag) {
         // rare path: the fallbacks work on copies so that U and pf can stay
         // in registers on the common path
@@ -540,6 +554,7 @@ __global__ void __launch_bounds__(BLK, HAMR_CONS_MINB) k_cons(const Dims d, cons
     W[6 * d.ks + c] = U[B3];   // kept in 2-D, where the faces do not set it
 }
 
+template <int INV>
 __global__ void __launch_bounds__(BLK, HAMR_UPD_MINB) k_invert(const Dims d, const Geom m, const double *__restrict__ pg,
                                                  const double *__restrict__ W, const double *__restrict__ psf,
                                                  double *__restrict__ pout, int *__restrict__ pflag,
@@ -563,7 +578,7 @@ __global__ void __launch_bounds__(BLK, HAMR_UPD_MINB) k_invert(const Dims d, con
     U[KTOT] = W[5 * d.ks + c];
     U[B3] = W[6 * d.ks + c];
     face_average_b(d, m, psf, i, j, c, gi, U);
-    invert_zone(d, gm, c, U, pf, pout, pflag, failimage);
+    invert_zone<INV>(d, gm, c, U, pf, pout, pflag, failimage);
 }
 
 // ------------------------------------------------------------ ghost fills
@@ -847,11 +862,14 @@ inline void prof_mark(Prof *pf, int slot, cudaStream_t s) {
     if (pf && pf->on) cudaEventRecord(pf->ev[slot + 1], s);
 }
 
-// n faces of direction DIR, one thread per face
+// n faces of direction DIR, one thread per face, with the block's reconstruction
 template <int DIR, typename T>
 void launch_flux(long n, cudaStream_t s, const Dims &d, const Geom &m, const double *pin, const double *psin, T *F,
                  unsigned long long *dtbits, int cd) {
-    k_flux<DIR, T><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd);
+    if (d.recon == HAMR_RECON_MC)
+        k_flux<DIR, T, HAMR_RECON_MC><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd);
+    else
+        k_flux<DIR, T, HAMR_RECON_PPM><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd);
 }
 
 // one sub-step: fluxes, CT, update, ghost fill of the written state. T is the
@@ -908,8 +926,9 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
 k_cons<T><<<nblk(n), BLK, 0, s>>>(d, m, ctx->p, full ? ctx->ph : ctx->p, ctx->U, F1, F2, F3, ctx->W, full,
                                          st);
         prof_mark(pf, PROF_UPDATE, s);
-        k_invert<<<nblk(n), BLK, 0, s>>>(d, m, full ? ctx->ph : ctx->p, ctx->W, full ? ctx->ps : ctx->psh,
-                                         full ? ctx->p : ctx->ph, ctx->pflag, ctx->failimage);
+        auto inv = d.inversion == HAMR_INV_NM ? k_invert<HAMR_INV_NM> : k_invert<HAMR_INV_2D>;
+        inv<<<nblk(n), BLK, 0, s>>>(d, m, full ? ctx->ph : ctx->p, ctx->W, full ? ctx->ps : ctx->psh,
+                                    full ? ctx->p : ctx->ph, ctx->pflag, ctx->failimage);
     }
     prof_mark(pf, PROF_INVERT, s);
     double *pw = full ? ctx->p : ctx->ph;
@@ -944,8 +963,11 @@ extern "C" {
 int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
     if (!prm || !out) return HAMR_E_ARG;
     *out = nullptr;
-    if (prm->n1 < 2 || prm->n2 < 2 || prm->n3 < 1 || prm->ng != 3) return HAMR_E_ARG;
+    if (prm->n1 < 2 || prm->n2 < 2 || prm->n3 < 1) return HAMR_E_ARG;
+    if (prm->recon != HAMR_RECON_PPM && prm->recon != HAMR_RECON_MC) return HAMR_E_ARG;
+    if (!(prm->ng == 3 || (prm->ng == 2 && prm->recon == HAMR_RECON_MC))) return HAMR_E_ARG;
     if (prm->precision != HAMR_FP64 && prm->precision != HAMR_MIXED) return HAMR_E_ARG;
+    if (prm->inversion != HAMR_INV_2D && prm->inversion != HAMR_INV_NM) return HAMR_E_ARG;
     if (prm->n3 > 1 && prm->bc3 != HAMR_BC_PERIODIC) return HAMR_E_ARG;
     if (prm->bc2 == HAMR_BC_POLE_TRANS && (prm->n3 < 2 || prm->n3 % 2)) return HAMR_E_ARG;
     if (!(prm->gam > 1.0) || !(prm->cour > 0.0) || !(prm->dx1 > 0) || !(prm->dx2 > 0) || !(prm->dx3 > 0)) return HAMR_E_ARG;
@@ -965,6 +987,8 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
     d.pole1 = prm->pole1; d.pole2 = prm->pole2;
     d.bc1 = prm->bc1; d.bc2 = prm->bc2; d.bc3 = prm->bc3;
     d.ct_upwind = prm->ct_upwind;
+    d.inversion = prm->inversion;
+    d.recon = prm->recon;
     if (prm->stream) {
         ctx->stream = (cudaStream_t)prm->stream;
     } else {
@@ -1236,7 +1260,10 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
                                  const double *gdet, const double *conn, double *p, double *ps,
                                  double dt, double *dt_next) {
     if (!prm || !gcov || !gcon || !gdet || !conn || !p || !ps || !(dt > 0)) return HAMR_E_ARG;
-    if (prm->n1 < 2 || prm->n2 < 2 || prm->n3 < 1 || prm->ng != 3 || prm->precision != HAMR_FP64) return HAMR_E_ARG;
+    if (prm->n1 < 2 || prm->n2 < 2 || prm->n3 < 1 || prm->precision != HAMR_FP64) return HAMR_E_ARG;
+    if (prm->recon != HAMR_RECON_PPM && prm->recon != HAMR_RECON_MC) return HAMR_E_ARG;
+    if (!(prm->ng == 3 || (prm->ng == 2 && prm->recon == HAMR_RECON_MC))) return HAMR_E_ARG;
+    if (prm->inversion != HAMR_INV_2D && prm->inversion != HAMR_INV_NM) return HAMR_E_ARG;
     if (prm->n3 > 1 && prm->bc3 != HAMR_BC_PERIODIC) return HAMR_E_ARG;
     if (prm->bc2 == HAMR_BC_POLE_TRANS && (prm->n3 < 2 || prm->n3 % 2)) return HAMR_E_ARG;
     if (!(prm->gam > 1.0) || !(prm->cour > 0.0) || !(prm->dx1 > 0) || !(prm->dx2 > 0) || !(prm->dx3 > 0)) return HAMR_E_ARG;
@@ -1258,6 +1285,8 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
     d.pole1 = prm->pole1; d.pole2 = prm->pole2;
     d.bc1 = prm->bc1; d.bc2 = prm->bc2; d.bc3 = prm->bc3;
     d.ct_upwind = prm->ct_upwind;
+    d.inversion = prm->inversion;
+    d.recon = prm->recon;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES) return HAMR_E_CUDA;
     if (!na_ready[dev] && na_setup(dev) != HAMR_OK) return HAMR_E_CUDA;

@@ -167,6 +167,20 @@ __device__ __forceinline__ void primtoflux(T gam, const T *pr, const State<T> &q
     }
 }
 
+// monotonized-central slope with the GPU's steepening factor 2 (slope_lim,
+// GPU_interp.h:2-38); a zone's face values are y -+ slope/2
+template <typename T>
+__device__ __forceinline__ T slope_lim(T y1, T y2, T y3) {
+    const T Dqm = T(2.0) * (y2 - y1);
+    const T Dqp = T(2.0) * (y3 - y2);
+    const T Dqc = T(0.5) * (y3 - y1);
+    const T s = Dqm * Dqp;
+    if (s <= T(0.)) return T(0.);
+    if (d_fabs(Dqm) < d_fabs(Dqp) && d_fabs(Dqm) < d_fabs(Dqc)) return Dqm;
+    if (d_fabs(Dqp) < d_fabs(Dqc)) return Dqp;
+    return Dqc;
+}
+
 // PPM face values of the middle of five zones: l = lower edge, r = upper edge
 template <typename T>
 __device__ __forceinline__ void para(const T *y, T &lout, T &rout) {
@@ -541,6 +555,92 @@ __device__ __noinline__ int utoprim_1dfix1(double gam, const double *U, const do
     pt[RHO] = rho0;
     pt[UU] = u;
     set_velocity(s, gamma, W, pt);
+    for (int i = 0; i < B1; i++) prim[i] = pt[i];
+    return 0;
+}
+
+// Newman & Hamlin 2014: fixed point on the pressure, W from the closed-form
+// root of a cubic, Aitken extrapolation when three successive pressures
+// contract (Utoprim_NM, GPU_utoprim_nm.h). The pressure history is a window
+// of the last three values: the reference's array holds three entries but is
+// indexed up to the iteration count, and only the last three are ever read.
+__device__ __forceinline__ int utoprim_nm(double gam, const double *U, const double *gcov, const double *gcon,
+                                          double gdet, double *prim) {
+    double Ut[NPR], pt[5];
+    int ret = inv_prologue(U, gdet, gcon, prim, Ut);
+    if (ret) return ret;
+    for (int i = 0; i < B1; i++) pt[i] = prim[i];
+    InvQ s;
+    inv_scalars(Ut, gcov, gcon, s);
+    const double Bsq = s.Bsq, QdotBsq = s.QdotBsq, Qtsq = s.Qtsq, Qdotn = s.Qdotn;
+    constexpr double PI_D = 3.14159265358979323846;
+    double a, phi, epsilon, z = 0., vsq, w, gamma = 1., rho0 = 0., u = 0., errx, p_old, p_new;
+    double pm2 = 0., pm1;   // pressures of iterations iter-2 and iter-1
+    int iter = 0, iter_tot = 0, set_variables = 0;
+    pm1 = (gam - 1.) * pt[UU];
+    p_new = pm1;
+    const double d = 0.5 * (Qtsq * Bsq - QdotBsq);
+    if (d < 0.0) return 1;
+    do {
+        set_variables = 0;
+        a = -Qdotn + p_new + 0.5 * Bsq;
+        phi = acos(1. / a * sqrt((27. * d) / (4. * a)));
+        epsilon = a / 3. - 2. / 3. * a * cos(2. / 3. * phi + 2. / 3. * PI_D);
+        z = epsilon - Bsq;
+        vsq = (Qtsq * z * z + QdotBsq * (Bsq + 2. * z)) / (z * z * pow(Bsq + z, 2.));
+        if (fabs(vsq) < 1e-15) vsq = 0.0;
+        if (fabs(vsq) >= 1.0) return 1;
+        w = z * (1. - vsq);
+        gamma = 1. / sqrt(1. - vsq);
+        rho0 = Ut[RHO] / gamma;
+        u = (w - rho0) / gam;
+        iter++;
+        iter_tot++;
+        const double pc = (gam - 1.) * u;
+        p_old = pm1;
+        p_new = pc;
+        bool restart = false;
+        if (iter >= 2) {
+            const double R = (pc - pm1) / (pm1 - pm2);
+            if (R < 1. && R > 0.) {
+                set_variables = 1;
+                p_new = pm1 + (pc - pm1) / (1. - R);
+                p_old = pc;
+                iter = 0;
+                restart = true;
+            }
+        }
+        if (restart) {
+            pm1 = p_new;   // the history restarts from the extrapolated pressure
+        } else {
+            pm2 = pm1;
+            pm1 = pc;
+        }
+        errx = fabs(p_new - p_old) / fabs(p_new + p_old);
+    } while (errx > NEWT_TOL && iter_tot < 30);
+    if (fabs(errx) > d_min(NEWT_TOL, MIN_NEWT_TOL)) return 1;
+    if (set_variables == 1) {
+        a = -Qdotn + p_new + 0.5 * Bsq;
+        phi = acos(1. / a * sqrt((27. * d) / (4. * a)));
+        epsilon = a / 3. - 2. / 3. * a * cos(2. / 3. * phi + 2. / 3. * PI_D);
+        z = epsilon - Bsq;
+        vsq = (Qtsq * z * z + QdotBsq * (Bsq + 2. * z)) / (z * z * pow(Bsq + z, 2.));
+        const double Wsq = 1. / (1. - vsq);
+        w = z / Wsq;
+        if (vsq >= 1.0 || vsq < 0. || z <= 0. || z > 1.e20 || !isfinite(vsq) || !isfinite(z)) return 4;
+        gamma = sqrt(Wsq);
+        rho0 = Ut[RHO] / gamma;
+        u = (w - rho0) / gam;
+        p_new = (gam - 1.) * u;
+    }
+    if (rho0 < 0.0) return 5;
+    if (p_new < 0.0) return 6;
+    pt[RHO] = rho0;
+    pt[UU] = u;
+    for (int i = 1; i < 4; i++) {
+        const double Qtcon = s.Qcon[i] + s.ncon[i] * s.Qdotn;
+        pt[U1 + i - 1] = gamma / (z + Bsq) * (Qtcon + s.QdotB * s.Bcon[i] / z);
+    }
     for (int i = 0; i < B1; i++) prim[i] = pt[i];
     return 0;
 }

@@ -60,7 +60,7 @@ class Problem:
 
     def block_kwargs(self):
         return dict(n1=self.n1, n2=self.n2, n3=self.n3, dx=self.dx, gam=self.gam, cour=self.cour,
-                    bc=self.bc, poles=self.poles, ct_upwind=self.ct_upwind)
+                    bc=self.bc, poles=self.poles, ct_upwind=self.ct_upwind, ng=self.ng)
 
 
 def _alloc(n1, n2, n3, ng):
@@ -177,12 +177,12 @@ def _bsq(P, gcov, gcon):
 
 
 def fm_torus(n1, n2, n3, spin=0.9375, rin=6.0, rmax=12.0, gam=13.0 / 9.0, kappa=1.e-3, beta=100.0,
-             rout=None, seed=12345, noise=0.04, rho_atm=1.e-14, u_atm=1.e-16, cour=0.8) -> Problem:
+             rout=None, seed=12345, noise=0.04, rho_atm=1.e-14, u_atm=1.e-16, cour=0.8, ng=3) -> Problem:
     """Magnetised Fishbone-Moncrief torus around a Kerr hole in the reference's
     code coordinates. n3 > 1: transmissive poles; n3 == 1: axisymmetric with
     reflective poles. The atmosphere is the reference's 1e-7*RHOMIN / 1e-7*UUMIN
-    (init_torus.c:211-212), also divided by the density maximum."""
-    ng = 3
+    (init_torus.c:211-212), also divided by the density maximum. ng: ghost
+    layers (3; 2 suits the linear MC reconstruction)."""
     if rout is None:
         rout = 4.0 * rmax * 2.0
     startx, dx = ks_grid(n1, n2, n3, spin, rout)

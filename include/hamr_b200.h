@@ -56,9 +56,20 @@ enum hamr_precision {
                                source, compensated update and inversion in double */
 };
 
+enum hamr_inversion {
+    HAMR_INV_2D = 0,        /* Noble 2D Newton (Utoprim_2d, the shipped default) */
+    HAMR_INV_NM = 1         /* Newman-Hamlin (Utoprim_NM, GPU_fixup.h:323, NEWMAN builds) */
+};                          /* either way failures fall back to 1dvsq2fix1 then 1dfix1 */
+
+enum hamr_recon {
+    HAMR_RECON_PPM = 0,     /* PPM para (GPU_interp.h:60-111, PPM builds; ng = 3) */
+    HAMR_RECON_MC = 1       /* linear MC slope_lim, factor 2 (GPU_interp.h:2-38, PPM = 0
+                               builds; ng = 2 as there, or 3) */
+};
+
 typedef struct hamr_params {
     int n1, n2, n3;         /* active cells per direction (n3 == 1: 2-D, x1-x2) */
-    int ng;                 /* ghost layers (must be 3: PPM, NG = 2 + PPM, config.h:1280) */
+    int ng;                 /* ghost layers: 3 (NG = 2 + PPM, config.h:1280); 2 allowed with MC */
     long ksize;             /* plane stride of cell arrays; 0: reference rule G + 64 - G%64 */
     long gsize;             /* plane stride of metric tables; 0: reference rule */
     double dx1, dx2, dx3;   /* coordinate spacing */
@@ -70,6 +81,8 @@ typedef struct hamr_params {
                                (the reference's CARTESIAN build, GPU_const_trans.h:187) */
     int precision;          /* enum hamr_precision */
     void *stream;           /* cudaStream_t to run on; NULL: the context creates one */
+    int inversion;          /* enum hamr_inversion (zero-initialised: Noble 2D) */
+    int recon;              /* enum hamr_recon (zero-initialised: PPM) */
 } hamr_params;
 
 typedef struct hamr_ctx hamr_ctx;

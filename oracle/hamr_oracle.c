@@ -204,6 +204,20 @@ void ho_para(const double *x, double *lout, double *rout) {
     *rout = r;
 }
 
+/* slope_lim: monotonized-central slope with the GPU's steepening factor 2
+ * (GPU_interp.h:2-38, the non-NEUTRON_STAR branch); the zone's face values
+ * are y -+ slope/2 (fluxcalcprep with PPM = 0, GPU_program1.cu:178-186) */
+double ho_slope_lim(double y1, double y2, double y3) {
+    double Dqm = (2.0) * (y2 - y1);
+    double Dqp = (2.0) * (y3 - y2);
+    double Dqc = 0.5 * (y3 - y1);
+    double s = Dqm * Dqp;
+    if (s <= 0.) return 0.;
+    if (fabs(Dqm) < fabs(Dqp) && fabs(Dqm) < fabs(Dqc)) return Dqm;
+    if (fabs(Dqp) < fabs(Dqc)) return Dqp;
+    return Dqc;
+}
+
 void ho_primtoflux(double gam, const double *pr, const double *gcov10, const double *gcon10,
                    double gdet, int dir, double *flux, double *vmax, double *vmin) {
     geo gm;
@@ -245,6 +259,14 @@ static void fluxes(const ho_grid *g, const dims *d, const ho_geom *m, const doub
                 double pl[NPR], pr[NPR], lo, hi, x[5];
                 for (int k = 0; k < NPR; k++) {
                     const double *pk = pv + (long)k * d->ks;
+                    if (g->recon == 1) {
+                        double xm = pk[c - stride], temp;
+                        temp = 0.5 * ho_slope_lim(pk[c - 2 * stride], xm, pk[c]);
+                        pl[k] = xm + temp;              /* dq2 of cell c - 1 */
+                        temp = 0.5 * ho_slope_lim(xm, pk[c], pk[c + stride]);
+                        pr[k] = pk[c] - temp;           /* dq1 of cell c */
+                        continue;
+                    }
                     /* upper edge of cell c - 1 */
                     for (int t = 0; t < 5; t++) x[t] = pk[c - stride + (t - 2) * stride];
                     ho_para(x, &lo, &hi);

@@ -34,6 +34,8 @@ typedef struct {
     int ct_upwind;       /* 1: upwinded edge-EMF corrections; 0: plain average of
                             the four face EMFs (the reference's CARTESIAN build,
                             GPU_const_trans.h:187-211) */
+    int recon;           /* 0: PPM (para, PPM builds); 1: MC-limited linear
+                            (slope_lim with factor 2, PPM = 0 builds) */
 } ho_grid;
 
 typedef struct {
@@ -60,6 +62,7 @@ void ho_bound(const ho_grid *g, const ho_geom *m, double *pv, double *ps);
 
 /* Single-cell pieces (pinned one by one against the reference). */
 void ho_para(const double *x, double *l, double *r);
+double ho_slope_lim(double y1, double y2, double y3);
 void ho_primtoflux(double gam, const double *pr, const double *gcov10, const double *gcon10,
                    double gdet, int dir, double *flux, double *vmax, double *vmin);
 int ho_utoprim_2d(double gam, double *U, const double *gcov10, const double *gcon10, double gdet, double *prim);

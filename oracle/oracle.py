@@ -38,7 +38,7 @@ class HoGrid(ctypes.Structure):
                 ("ksize", ctypes.c_long), ("gsize", ctypes.c_long),
                 ("dx1", _d), ("dx2", _d), ("dx3", _d), ("gam", _d), ("cour", _d),
                 ("pole1", _i), ("pole2", _i), ("bc1", _i), ("bc2", _i), ("bc3", _i),
-                ("inversion", _i), ("ct_upwind", _i)]
+                ("inversion", _i), ("ct_upwind", _i), ("recon", _i)]
 
 
 class HoGeom(ctypes.Structure):
@@ -211,12 +211,14 @@ class Setup:
     pole2: int
     bc: tuple  # (bc1, bc2, bc3)
     ct_upwind: int = 1
+    inversion: int = 0  # 0: Noble 2D, 1: Newman-Hamlin
+    recon: int = 0      # 0: PPM, 1: MC-limited linear
 
     def grid(self):
         b = self.blk
         return HoGrid(b.n1, b.n2, b.n3, b.ng, b.ksize, b.gsize, self.dx[0], self.dx[1], self.dx[2],
-                      self.gam, self.cour, self.pole1, self.pole2, self.bc[0], self.bc[1], self.bc[2], 0,
-                      self.ct_upwind)
+                      self.gam, self.cour, self.pole1, self.pole2, self.bc[0], self.bc[1], self.bc[2],
+                      self.inversion, self.ct_upwind, self.recon)
 
 
 def _state(b: Block):

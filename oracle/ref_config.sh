@@ -10,9 +10,10 @@
 # `r < radfix_dens` always passes and return garbage. The configured copy ends
 # the test with `return 0;`, the evident intent: floors off, no failure flag.
 #
-# usage: ref_config.sh <refdir> <outdir> <mode: torus|cart> <BS_1> <BS_2> <BS_3> <gamma-expr>
+# usage: ref_config.sh <refdir> <outdir> <mode: torus|cart> <BS_1> <BS_2> <BS_3> <gamma-expr> [opts]
+#   opts: comma-separated build switches; mc = linear MC reconstruction (PPM 0)
 set -e
-REF="$1"; OUT="$2"; MODE="$3"; B1="$4"; B2="$5"; B3="$6"; GAM="$7"
+REF="$1"; OUT="$2"; MODE="$3"; B1="$4"; B2="$5"; B3="$6"; GAM="$7"; OPTS="${8:-}"
 mkdir -p "$OUT"
 sed -e 's/^#define WHICHPROBLEM .*/#define WHICHPROBLEM TORUS_PROBLEM/' \
     -e "s|^#define GAMMA[[:space:]].*|#define GAMMA ($GAM)|" \
@@ -29,4 +30,7 @@ if [ "$MODE" = "cart" ]; then
   sed -i -e 's/^#define CARTESIAN (0)/#define CARTESIAN (1)/' \
          -e 's/^#define SPHERICAL_GR (1)/#define SPHERICAL_GR (0)/' "$OUT/config.h.tmp"
 fi
+case ",$OPTS," in
+  *,mc,*) sed -i -e 's/^#define PPM (1)/#define PPM (0)/' "$OUT/config.h.tmp" ;;
+esac
 mv "$OUT/config.h.tmp" "$OUT/config.h"

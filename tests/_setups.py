@@ -86,7 +86,7 @@ def make_setup(variant, spin=0.9375, rout=40.0, seed=1, stress=False, cour=0.8, 
     dims, gam = dims if dims is not None else O.ref_dims(variant)
     n1, n2, n3 = (int(x) for x in dims[:3])
     ksize, gsize = int(dims[7]), int(dims[8])
-    blk = O.Block(n1, n2, n3, 3, ksize, gsize)
+    blk = O.Block(n1, n2, n3, int(dims[3]), ksize, gsize)
     if variant == "ot":
         startx = [0.0, 0.0, 0.0, 0.0]
         dx = [0.0, 1.0 / n1, 1.0 / n2, 1.0]
@@ -102,10 +102,11 @@ def make_setup(variant, spin=0.9375, rout=40.0, seed=1, stress=False, cour=0.8, 
         poles = (1, 1)
     fill_synthetic(blk, geo, dx, seed=seed, stress=stress)
     s = O.Setup(blk, geo, tuple(dx[1:]), gam, cour, poles[0], poles[1], bc,
-                ct_upwind=0 if variant == "ot" else 1)
+                ct_upwind=0 if variant == "ot" else 1, recon=1 if variant.endswith("m") else 0)
     O.oracle_bound(s, "p", "ps")
     return s
 
 
 def clone(s: O.Setup) -> O.Setup:
-    return O.Setup(s.blk.copy(), s.geo, s.dx, s.gam, s.cour, s.pole1, s.pole2, s.bc, s.ct_upwind)
+    return O.Setup(s.blk.copy(), s.geo, s.dx, s.gam, s.cour, s.pole1, s.pole2, s.bc, s.ct_upwind, s.inversion,
+                   s.recon)

@@ -34,13 +34,23 @@ def test_create_rejects_bad_parameters_without_device_work():
     L = _lib.load()
     ctx = ctypes.c_void_p()
     prm = _lib.HamrParams(16, 8, 8, 2, 0, 0, 0.1, 0.1, 0.1, 13 / 9, 0.8, 1, 1, 1, 2, 0, 1, 0, None)
-    assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # ng must be 3
+    assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # ng 2 only with MC
+    prm.recon = 7
+    prm.ng = 3
+    assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # no such reconstruction
+    prm.recon = 0
     prm.ng = 3
     prm.gam = 1.0
     assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # gamma <= 1
     prm.gam = 13 / 9
     prm.n3 = 7
     assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # transmissive pole needs even n3
+    prm.n3 = 8
+    prm.inversion = 2
+    assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # no such primary inversion
+    prm.inversion = 0
+    prm.precision = 5
+    assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # no such precision
     assert L.hamr_ctx_create(None, ctypes.byref(ctx)) == -1
     assert L.hamr_stage(None, 0, 0.1, 0.1) == -1
     assert L.hamr_step(None, 0.1, None) == -1

@@ -161,3 +161,41 @@ def test_bench_size_torus_strict():
     assert field_rel_err(blk, ps, s, "ps").max() <= 1e-14
     assert abs(dn_gpu - dn_orc) <= 1e-14 * dn_orc
     blk.close()
+
+
+@pytest.mark.parametrize("case", ["torus3d", "torus2d"])
+def test_newman_hamlin_inversion_strict(case):
+    """Newman-Hamlin as the primary inversion (the reference's NEWMAN builds),
+    fallbacks unchanged: strict build against the oracle over three steps."""
+    pb = CASES[case]()
+    blk, s = make_pair(pb, strict=True, inversion="nm")
+    dt = 0.2 * min(pb.dx[:2])
+    for _ in range(3):
+        dn = blk.step(dt)
+        dn_o = oracle_step(s, dt)
+        assert abs(dn - dn_o) <= 1e-14 * dn_o
+        dt = min(dn, 1.3 * dt)
+    p, ps = blk.download()
+    assert field_rel_err(blk, p, s, "p").max() <= 1e-14
+    assert field_rel_err(blk, ps, s, "ps").max() <= 1e-14
+    blk.close()
+
+
+@pytest.mark.parametrize("ng", [3, 2])
+@pytest.mark.parametrize("case", ["torus3d", "torus2d"])
+def test_mc_reconstruction_strict(case, ng):
+    """Linear MC reconstruction (the reference's PPM = 0 builds, which run with
+    two ghost layers) against the oracle, strict build, three steps."""
+    n1, n2, n3 = (32, 16, 8) if case == "torus3d" else (48, 48, 1)
+    pb = problems.fm_torus(n1, n2, n3, rout=40.0, ng=ng)
+    blk, s = make_pair(pb, strict=True, recon="mc")
+    dt = 0.2 * min(pb.dx[:2])
+    for _ in range(3):
+        dn = blk.step(dt)
+        dn_o = oracle_step(s, dt)
+        assert abs(dn - dn_o) <= 1e-14 * dn_o
+        dt = min(dn, 1.3 * dt)
+    p, ps = blk.download()
+    assert field_rel_err(blk, p, s, "p").max() <= 1e-14
+    assert field_rel_err(blk, ps, s, "ps").max() <= 1e-14
+    blk.close()

@@ -1,6 +1,8 @@
 """Pins the C restatement (oracle/hamr_oracle.c) to the reference's own kernel
 code, built for the host from the reference sources (oracle/Makefile, variants
-t3: 3-D torus 16x8x8, t2: 2-D torus 24x24, ot: 2-D Cartesian 32x32).
+t3: 3-D torus 16x8x8, t2: 2-D torus 24x24, ot: 2-D Cartesian 32x32, t3m: the
+3-D torus with linear MC reconstruction, PPM = 0, which also means two ghost
+layers).
 
 Both sides get identical inputs and identical metric tables (computed by the
 reference's metric.c), and must agree bit for bit.
@@ -11,7 +13,7 @@ import pytest
 from oracle import oracle as O
 from tests._setups import clone, make_setup
 
-VARIANTS = ["t3", "t2", "ot"]
+VARIANTS = ["t3", "t2", "ot", "t3m"]
 
 
 def need_ref(v):
