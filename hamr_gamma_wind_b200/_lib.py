@@ -68,6 +68,14 @@ def load(strict: bool = False):
     L.hamr_build_geometry.argtypes = [_i, _d, _i, _i, _i, _i, _l, _vp, _vp, _vp, _vp, _vp, _vp]
     L.hamr_bl_coord.argtypes = [_i, _d, _vp, _vp]
     L.hamr_step_noalloc.argtypes = [P(HamrParams), _vp, _vp, _vp, _vp, _vp, _vp, _d, P(_d)]
+    L.hamr_batch_create.argtypes = [_vp, _i, _vp, P(_vp)]
+    L.hamr_batch_destroy.argtypes = [_vp]
+    L.hamr_batch_last_error.argtypes = [_vp]
+    L.hamr_batch_last_error.restype = ctypes.c_char_p
+    L.hamr_batch_step.argtypes = [_vp, _vp, _vp]
+    L.hamr_batch_advance.argtypes = [_vp, _i, _i, _vp]
+    L.hamr_batch_autotune.argtypes = [_vp, _vp, _i]
+    L.hamr_batch_tuning.argtypes = [_vp, _vp, _vp, _vp, _vp, _i]
     _libs[key] = L
     return L
 
@@ -76,8 +84,13 @@ def load(strict: bool = False):
 SYMBOLS = ["hamr_ctx_create", "hamr_ctx_destroy", "hamr_last_error", "hamr_strides",
            "hamr_set_geometry", "hamr_upload", "hamr_download", "hamr_download_flags",
            "hamr_bound", "hamr_stage", "hamr_step", "hamr_advance", "hamr_device_state", "hamr_profile_step",
-           "hamr_divb_max", "hamr_build_geometry", "hamr_bl_coord", "hamr_step_noalloc"]
+           "hamr_divb_max", "hamr_build_geometry", "hamr_bl_coord", "hamr_step_noalloc",
+           "hamr_batch_create", "hamr_batch_destroy", "hamr_batch_last_error", "hamr_batch_step",
+           "hamr_batch_advance", "hamr_batch_autotune", "hamr_batch_tuning"]
 NOALLOC_MAX_CELLS = 32768
+
+BATCH_PHASES = ["flux3", "flux2", "flux1", "fix_flux", "emf_centre", "emf_edge", "pole_average",
+                "face_update", "update", "invert", "bound_x1", "bound_x3", "bound_x2"]
 
 PROF_SLOTS = ["flux3", "flux2", "flux1", "fix_flux", "emf_centre", "emf_edge", "pole_average",
               "face_update", "update", "invert", "bound"]

@@ -195,3 +195,78 @@ class Block:
         ptrs = [ctypes.c_void_p() for _ in range(4)]
         self._check(self.L.hamr_device_state(self.ctx, *[ctypes.byref(x) for x in ptrs]), "hamr_device_state")
         return [x.value for x in ptrs]
+
+
+class Batch:
+    """An ensemble of Blocks advanced together (hamr_batch_*): one launch per
+    sub-step phase for all members, per-member step sizes, an optional
+    autotuned launch shape per phase. Members stay owned by the caller and
+    must outlive the batch."""
+
+    def __init__(self, blocks, stream=None):
+        if not blocks:
+            raise ValueError("empty batch")
+        self.blocks = list(blocks)
+        self.L = self.blocks[0].L
+        arr = (ctypes.c_void_p * len(self.blocks))(*[b.ctx.value for b in self.blocks])
+        self._arr = arr
+        h = ctypes.c_void_p()
+        rc = self.L.hamr_batch_create(arr, len(self.blocks), stream, ctypes.byref(h))
+        if rc:
+            raise _lib.HamrError(f"hamr_batch_create: {_lib.ERRORS.get(rc, rc)}")
+        self.h = h
+
+    @property
+    def n(self):
+        return len(self.blocks)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.hamr_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc:
+            msg = self.L.hamr_batch_last_error(self.h).decode()
+            raise _lib.HamrError(f"{what}: {_lib.ERRORS.get(rc, rc)} {msg}")
+
+    def _dts(self, dt):
+        return np.ascontiguousarray(np.broadcast_to(np.asarray(dt, float), (self.n,)), dtype=float)
+
+    def step(self, dt):
+        """One RK2 step of every member (dt: scalar or one per member);
+        returns each member's CFL step."""
+        d = self._dts(dt)
+        out = np.zeros(self.n)
+        self._check(self.L.hamr_batch_step(self.h, d.ctypes.data_as(ctypes.c_void_p),
+                                           out.ctypes.data_as(ctypes.c_void_p)), "hamr_batch_step")
+        return out
+
+    def advance(self, nsteps, dt, interval=16):
+        """nsteps steps with per-member step-size refresh from one captured
+        graph; returns each member's step size afterwards."""
+        d = self._dts(dt).copy()
+        self._check(self.L.hamr_batch_advance(self.h, int(nsteps), int(interval),
+                                              d.ctypes.data_as(ctypes.c_void_p)), "hamr_batch_advance")
+        return d
+
+    def autotune(self, dt, reps=3):
+        d = self._dts(dt)
+        self._check(self.L.hamr_batch_autotune(self.h, d.ctypes.data_as(ctypes.c_void_p), int(reps)),
+                    "hamr_batch_autotune")
+        return self.tuning()
+
+    def tuning(self):
+        n = len(_lib.BATCH_PHASES)
+        tile, grid, order = (np.zeros(n, np.int32) for _ in range(3))
+        ms = np.zeros(n, np.float32)
+        p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        self._check(self.L.hamr_batch_tuning(self.h, p(tile), p(grid), p(order), p(ms), n), "hamr_batch_tuning")
+        return {ph: dict(tile=int(tile[k]), grid=int(grid[k]), order=("largest-first" if order[k] else "given"),
+                         ms=float(ms[k])) for k, ph in enumerate(_lib.BATCH_PHASES)}

@@ -1,0 +1,597 @@
+// Batched ensembles: many independent blocks (different sizes, spins, grids)
+// advanced together, one launch per phase of the sub-step for the whole
+// ensemble. Included at the end of hamr_kernels.cu (same translation unit):
+// the per-item bodies (flux_face, k_cons_at, ...) are the ones the
+// single-block kernels run, so a block advances identically alone or in a
+// batch.
+//
+// Work layout. Each phase has, per block, a count of work items (faces,
+// zones, edges or ghost columns). Items are cut into tiles of `tile` items;
+// the tiles of all blocks form one index space, blocks concatenated in a
+// schedule order. A launch runs `grid` CTAs of BLK threads; CTA b takes tiles
+// b, b + grid, ... (grid == number of tiles: one tile per CTA; smaller grids:
+// persistent CTAs). A tile never straddles two blocks, so the CFL minimum of
+// a tile goes to its own block's slot. Tile size, grid and schedule order are
+// chosen per phase by the autotuner (hamr_batch_autotune) or default to one
+// BLK-item tile per CTA in the caller's order.
+
+namespace {
+
+// everything one block's kernels touch; the step-size slots point into the
+// batch's own contiguous arrays
+struct BEntry {
+    Dims d;
+    Geom m;
+    double *p, *ph, *ps, *psh, *U, *F1, *F2, *F3, *Ec, *emf, *W;
+    int *pflag, *failimage;
+    unsigned long long *dtbits;  // 4 per block
+    double *ndt, *dt_state;      // 1 per block
+    int *counter;                // 1 per block
+};
+
+struct StageArg {
+    int full;      // 0: half sub-step (writes ph, psh), 1: full (writes p, ps)
+    int calc_dt;   // collect the CFL minimum (full sub-step)
+    double frac;   // Dt = frac * dt of each block
+};
+
+__device__ __forceinline__ StepSize entry_step(const BEntry &e, const StageArg &a) {
+    return StepSize{e.dt_state, a.frac, 0., 0.};
+}
+
+// ---- phases: item count per block and the item body ----------------------
+enum { PH_FLUX3, PH_FLUX2, PH_FLUX1, PH_FIXFLUX, PH_EMFC, PH_EMFE, PH_POLE, PH_FACE, PH_CONS, PH_INV,
+       PH_BX1, PH_BX3, PH_BX2, PH_N };
+
+__host__ __device__ inline long phase_items(int ph, const Dims &d) {
+    switch (ph) {
+    case PH_FLUX3: return d.d3 ? n_faces<3>(d) : 0;
+    case PH_FLUX2: return n_faces<2>(d);
+    case PH_FLUX1: return n_faces<1>(d);
+    case PH_FIXFLUX: return d.bc2 == HAMR_BC_POLE_REFL ? n_fix_flux(d) : 0;
+    case PH_EMFC: return (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3);
+    case PH_EMFE:
+    case PH_FACE: return (long)(d.n1 + d.d1) * (d.n2 + d.d2) * (d.n3 + d.d3);
+    case PH_POLE: return d.bc2 == HAMR_BC_POLE_TRANS ? 2L * (d.n1 + d.ng1) : 0;
+    case PH_CONS:
+    case PH_INV: return (long)d.n1 * d.n2 * d.n3;
+    case PH_BX1: return d.d1 ? (long)d.ng1 * d.G2 * d.G3 : 0;
+    case PH_BX3: return d.d3 ? (long)d.ng3 * d.G1 * d.G2 : 0;
+    case PH_BX2: return d.d2 ? (long)d.G1 * d.G3 : 0;
+    }
+    return 0;
+}
+
+template <int DIR, typename T, int REC>
+struct OpFlux {
+    static constexpr int PH = DIR == 3 ? PH_FLUX3 : (DIR == 2 ? PH_FLUX2 : PH_FLUX1);
+    static constexpr int MINB = sizeof(T) == 8 ? HAMR_FLUX_MINB : HAMR_FLUX_MINB_F;
+    static constexpr bool REDUCE = true;
+    static constexpr int SLOT = DIR;
+    __device__ static double run(const BEntry &e, const StageArg &a, long t) {
+        T *F = reinterpret_cast<T *>(DIR == 1 ? e.F1 : (DIR == 2 ? e.F2 : e.F3));
+        return flux_face<DIR, T, REC>(e.d, e.m, a.full ? e.ph : e.p, a.full ? e.psh : e.ps, F, t);
+    }
+};
+
+template <typename T>
+struct OpFixFlux {
+    static constexpr int PH = PH_FIXFLUX, MINB = 1, SLOT = 0;
+    static constexpr bool REDUCE = false;
+    __device__ static double run(const BEntry &e, const StageArg &, long t) {
+        fix_flux_at(e.d, reinterpret_cast<T *>(e.F1), reinterpret_cast<T *>(e.F2), reinterpret_cast<T *>(e.F3), t);
+        return 1.e9;
+    }
+};
+
+template <typename T>
+struct OpEmfCentre {
+    static constexpr int PH = PH_EMFC, MINB = 1, SLOT = 0;
+    static constexpr bool REDUCE = false;
+    __device__ static double run(const BEntry &e, const StageArg &a, long t) {
+        k_emf_centre_at(e.d, e.m, a.full ? e.ph : e.p, reinterpret_cast<T *>(e.Ec), t);
+        return 1.e9;
+    }
+};
+
+template <typename T>
+struct OpEmfEdge {
+    static constexpr int PH = PH_EMFE, MINB = 1, SLOT = 0;
+    static constexpr bool REDUCE = false;
+    __device__ static double run(const BEntry &e, const StageArg &, long t) {
+        k_emf_edge_at(e.d, reinterpret_cast<const T *>(e.Ec), reinterpret_cast<const T *>(e.F1),
+                      reinterpret_cast<const T *>(e.F2), reinterpret_cast<const T *>(e.F3),
+                      reinterpret_cast<T *>(e.emf), t);
+        return 1.e9;
+    }
+};
+
+template <typename T>
+struct OpPole {
+    static constexpr int PH = PH_POLE, MINB = 1, SLOT = 0;
+    static constexpr bool REDUCE = false;
+    __device__ static double run(const BEntry &e, const StageArg &a, long t) {
+        k_pole_average_at(e.d, reinterpret_cast<T *>(e.emf), entry_step(e, a), t);
+        return 1.e9;
+    }
+};
+
+template <typename T>
+struct OpFace {
+    static constexpr int PH = PH_FACE, MINB = 1, SLOT = 0;
+    static constexpr bool REDUCE = false;
+    __device__ static double run(const BEntry &e, const StageArg &a, long t) {
+        k_face_update_at(e.d, e.m, e.ps, a.full ? e.ps : e.psh, reinterpret_cast<const T *>(e.emf),
+                         entry_step(e, a), t);
+        return 1.e9;
+    }
+};
+
+template <typename T>
+struct OpCons {
+    static constexpr int PH = PH_CONS, MINB = HAMR_CONS_MINB, SLOT = 0;
+    static constexpr bool REDUCE = false;
+    __device__ static double run(const BEntry &e, const StageArg &a, long t) {
+        k_cons_at(e.d, e.m, e.p, a.full ? e.ph : e.p, e.U, reinterpret_cast<const T *>(e.F1),
+                  reinterpret_cast<const T *>(e.F2), reinterpret_cast<const T *>(e.F3), e.W, a.full,
+                  entry_step(e, a), t);
+        return 1.e9;
+    }
+};
+
+template <int INV>
+struct OpInvert {
+    static constexpr int PH = PH_INV, MINB = HAMR_UPD_MINB, SLOT = 0;
+    static constexpr bool REDUCE = false;
+    __device__ static double run(const BEntry &e, const StageArg &a, long t) {
+        k_invert_at<INV>(e.d, e.m, a.full ? e.ph : e.p, e.W, a.full ? e.ps : e.psh, a.full ? e.p : e.ph,
+                         e.pflag, e.failimage, t);
+        return 1.e9;
+    }
+};
+
+struct OpBoundX1 {
+    static constexpr int PH = PH_BX1, MINB = 1, SLOT = 0;
+    static constexpr bool REDUCE = false;
+    __device__ static double run(const BEntry &e, const StageArg &a, long t) {
+        k_bound_x1_at(e.d, e.m, a.full ? e.p : e.ph, a.full ? e.ps : e.psh, t);
+        return 1.e9;
+    }
+};
+
+struct OpBoundX3 {
+    static constexpr int PH = PH_BX3, MINB = 1, SLOT = 0;
+    static constexpr bool REDUCE = false;
+    __device__ static double run(const BEntry &e, const StageArg &a, long t) {
+        k_bound_x3_at(e.d, a.full ? e.p : e.ph, a.full ? e.ps : e.psh, t);
+        return 1.e9;
+    }
+};
+
+struct OpBoundX2 {
+    static constexpr int PH = PH_BX2, MINB = 1, SLOT = 0;
+    static constexpr bool REDUCE = false;
+    __device__ static double run(const BEntry &e, const StageArg &a, long t) {
+        k_bound_x2_at(e.d, a.full ? e.p : e.ph, a.full ? e.ps : e.psh, t);
+        return 1.e9;
+    }
+};
+
+}  // namespace
+
+namespace {
+
+// tile space of one phase: start[k] = first tile of the k-th block in the
+// schedule, order[k] = that block's index in the batch
+struct TileMap {
+    const long *start;   // n + 1 entries
+    const int *order;    // n entries
+    int n;
+    int tile;            // items per tile
+};
+
+template <class Op>
+__global__ void __launch_bounds__(BLK, Op::MINB) k_batch(const BEntry *__restrict__ E, const TileMap tm,
+                                                          const StageArg a) {
+    // the tile's block description, staged in shared memory: the bodies read
+    // sizes, strides and pointers from there instead of holding them in registers
+    __shared__ BEntry e;
+    const long ntiles = tm.start[tm.n];
+    for (long w = blockIdx.x; w < ntiles; w += gridDim.x) {
+        int lo = 0, hi = tm.n;   // start[lo] <= w < start[lo + 1]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (tm.start[mid] <= w) lo = mid;
+            else hi = mid;
+        }
+        __syncthreads();   // the previous tile is done with e
+        {
+            static_assert(sizeof(BEntry) % 4 == 0, "BEntry copied as words");
+            const int *src = reinterpret_cast<const int *>(&E[tm.order[lo]]);
+            int *dst = reinterpret_cast<int *>(&e);
+            for (int k = threadIdx.x; k < (int)(sizeof(BEntry) / 4); k += BLK) dst[k] = src[k];
+        }
+        __syncthreads();
+        const long first = (w - tm.start[lo]) * tm.tile;
+        const long cnt = phase_items(Op::PH, e.d);
+        const long last = first + tm.tile < cnt ? first + tm.tile : cnt;
+        double dtf = 1.e9;
+        for (long t = first + threadIdx.x; t < last; t += BLK) dtf = d_min(dtf, Op::run(e, a, t));
+        if (Op::REDUCE && a.calc_dt) cta_min_dt(dtf, &e.dtbits[Op::SLOT]);
+    }
+}
+
+// one thread per block of the batch
+__global__ void k_batch_dt_reset(const BEntry *__restrict__ E, int n) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    for (int k = 0; k < 4; k++) E[b].dtbits[k] = BITS_1E9;
+}
+
+// per block: the CFL step of the full sub-step, and (advance mode) the
+// step-size update min(ndt, 1.3 dt) every `interval` steps, as k_dt_finalize
+__global__ void k_batch_dt_finalize(const BEntry *__restrict__ E, int n, int update, int interval) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    const BEntry &e = E[b];
+    const double d1 = __longlong_as_double((long long)e.dtbits[1]);
+    const double d2 = __longlong_as_double((long long)e.dtbits[2]);
+    const double d3 = __longlong_as_double((long long)e.dtbits[3]);
+    const double ndt = 1. / (1. / d1 + 1. / d2 + 1. / d3);
+    *e.ndt = ndt;
+    if (update) {
+        const int c = ++(*e.counter);
+        if (interval <= 1 || c % interval == 0) {
+            const double dt = *e.dt_state;
+            *e.dt_state = ndt > 1.3 * dt ? 1.3 * dt : ndt;
+        }
+    }
+    for (int k = 0; k < 4; k++) e.dtbits[k] = BITS_1E9;
+}
+
+}  // namespace
+
+// ===========================================================================
+struct hamr_batch {
+    int n = 0;
+    int precision = 0, recon = 0, inversion = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int nsm = 148;
+    std::string err;
+    std::vector<hamr_ctx *> ctx;
+    BEntry *E = nullptr;                    // device, n entries
+    unsigned long long *dtbits = nullptr;   // device, 4n
+    double *dts = nullptr, *ndts = nullptr; // device, n each
+    int *counters = nullptr;                // device, n
+    std::vector<long> items[PH_N];          // host: work items per block and phase
+    long ntiles[PH_N] = {};
+    long *dstart[PH_N] = {};                // device tile maps
+    int *dorder[PH_N] = {};
+    int tile[PH_N], grid[PH_N], order_mode[PH_N];
+    float tuned_ms[PH_N] = {};
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = -1, graph_interval = -1;
+};
+
+namespace {
+
+int bfail(hamr_batch *b, cudaError_t e, const char *what) {
+    b->err = std::string(what) + ": " + cudaGetErrorString(e);
+    return HAMR_E_CUDA;
+}
+
+#define BCK(call)                                               \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return bfail(b, e_, #call);      \
+    } while (0)
+
+// tile map of one phase from its tuning: schedule order (0: as given, 1:
+// largest block first), tiles of `tile` items, prefix over the schedule
+int build_tiles(hamr_batch *b, int ph) {
+    const int n = b->n;
+    std::vector<int> order(n);
+    for (int k = 0; k < n; k++) order[k] = k;
+    if (b->order_mode[ph] == 1)
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int x, int y) { return b->items[ph][x] > b->items[ph][y]; });
+    std::vector<long> start(n + 1, 0);
+    const long tl = b->tile[ph];
+    for (int k = 0; k < n; k++) start[k + 1] = start[k] + (b->items[ph][order[k]] + tl - 1) / tl;
+    b->ntiles[ph] = start[n];
+    BCK(cudaMemcpyAsync(b->dstart[ph], start.data(), sizeof(long) * (n + 1), cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaMemcpyAsync(b->dorder[ph], order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, b->stream));
+    // the host vectors go out of scope: finish the copies first
+    BCK(cudaStreamSynchronize(b->stream));
+    return HAMR_OK;
+}
+
+template <class Op>
+void launch_phase(hamr_batch *b, const StageArg &a) {
+    const int ph = Op::PH;
+    const long nt = b->ntiles[ph];
+    if (nt == 0) return;
+    const long g = b->grid[ph] > 0 && b->grid[ph] < nt ? b->grid[ph] : nt;
+    k_batch<Op><<<(unsigned)g, BLK, 0, b->stream>>>(b->E, TileMap{b->dstart[ph], b->dorder[ph], b->n, b->tile[ph]}, a);
+}
+
+// launches phase `only` (or every phase when only < 0) of one sub-step
+template <typename T, int REC, int INV>
+void batch_stage_t(hamr_batch *b, int full, bool calc_dt, int only) {
+    const StageArg a{full, calc_dt ? 1 : 0, full ? 1.0 : 0.5};
+    auto want = [&](int ph) { return only < 0 || only == ph; };
+    if (want(PH_FLUX3)) launch_phase<OpFlux<3, T, REC>>(b, a);
+    if (want(PH_FLUX2)) launch_phase<OpFlux<2, T, REC>>(b, a);
+    if (want(PH_FLUX1)) launch_phase<OpFlux<1, T, REC>>(b, a);
+    if (want(PH_FIXFLUX)) launch_phase<OpFixFlux<T>>(b, a);
+    if (want(PH_EMFC)) launch_phase<OpEmfCentre<T>>(b, a);
+    if (want(PH_EMFE)) launch_phase<OpEmfEdge<T>>(b, a);
+    if (want(PH_POLE)) launch_phase<OpPole<T>>(b, a);
+    if (want(PH_FACE)) launch_phase<OpFace<T>>(b, a);
+    if (want(PH_CONS)) launch_phase<OpCons<T>>(b, a);
+    if (want(PH_INV)) launch_phase<OpInvert<INV>>(b, a);
+    if (want(PH_BX1)) launch_phase<OpBoundX1>(b, a);
+    if (want(PH_BX3)) launch_phase<OpBoundX3>(b, a);
+    if (want(PH_BX2)) launch_phase<OpBoundX2>(b, a);
+}
+
+template <typename T, int REC>
+void batch_stage_r(hamr_batch *b, int full, bool calc_dt, int only) {
+    if (b->inversion == HAMR_INV_NM) batch_stage_t<T, REC, HAMR_INV_NM>(b, full, calc_dt, only);
+    else batch_stage_t<T, REC, HAMR_INV_2D>(b, full, calc_dt, only);
+}
+
+template <typename T>
+void batch_stage_p(hamr_batch *b, int full, bool calc_dt, int only) {
+    if (b->recon == HAMR_RECON_MC) batch_stage_r<T, HAMR_RECON_MC>(b, full, calc_dt, only);
+    else batch_stage_r<T, HAMR_RECON_PPM>(b, full, calc_dt, only);
+}
+
+void batch_stage(hamr_batch *b, int full, bool calc_dt, int only = -1) {
+    if (b->precision == HAMR_MIXED) batch_stage_p<float>(b, full, calc_dt, only);
+    else batch_stage_p<double>(b, full, calc_dt, only);
+}
+
+unsigned nblk_b(int n) { return (unsigned)((n + 127) / 128); }
+
+// one RK2 step of every block: step sizes from b->dts (frac 1/2, then 1)
+int batch_step_launch(hamr_batch *b, int update, int interval) {
+    batch_stage(b, 0, false);
+    batch_stage(b, 1, true);
+    k_batch_dt_finalize<<<nblk_b(b->n), 128, 0, b->stream>>>(b->E, b->n, update, interval);
+    BCK(cudaGetLastError());
+    return HAMR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hamr_batch_create(hamr_ctx *const *blocks, int n, void *stream, hamr_batch **out) {
+    if (!blocks || !out || n < 1) return HAMR_E_ARG;
+    *out = nullptr;
+    for (int k = 0; k < n; k++) {
+        if (!blocks[k]) return HAMR_E_ARG;
+        if (!blocks[k]->have_geom) return HAMR_E_STATE;
+        const hamr_params &p0 = blocks[0]->prm, &pk = blocks[k]->prm;
+        // one instantiation of every phase kernel serves the whole batch
+        if (pk.precision != p0.precision || pk.recon != p0.recon || pk.inversion != p0.inversion) return HAMR_E_ARG;
+        for (int j = 0; j < k; j++)
+            if (blocks[j] == blocks[k]) return HAMR_E_ARG;
+    }
+    hamr_batch *b = new hamr_batch();
+    b->n = n;
+    b->precision = blocks[0]->prm.precision;
+    b->recon = blocks[0]->prm.recon;
+    b->inversion = blocks[0]->prm.inversion;
+    b->ctx.assign(blocks, blocks + n);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (stream) {
+        b->stream = (cudaStream_t)stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) { delete b; return HAMR_E_CUDA; }
+        b->own_stream = true;
+    }
+    bool ok = cudaMalloc(&b->E, sizeof(BEntry) * n) == cudaSuccess &&
+              cudaMalloc(&b->dtbits, sizeof(unsigned long long) * 4 * n) == cudaSuccess &&
+              cudaMalloc(&b->dts, sizeof(double) * n) == cudaSuccess &&
+              cudaMalloc(&b->ndts, sizeof(double) * n) == cudaSuccess &&
+              cudaMalloc(&b->counters, sizeof(int) * n) == cudaSuccess;
+    for (int ph = 0; ph < PH_N && ok; ph++)
+        ok = cudaMalloc(&b->dstart[ph], sizeof(long) * (n + 1)) == cudaSuccess &&
+             cudaMalloc(&b->dorder[ph], sizeof(int) * n) == cudaSuccess;
+    if (!ok) {
+        hamr_batch_destroy(b);
+        return HAMR_E_NOMEM;
+    }
+    std::vector<BEntry> host(n);
+    for (int k = 0; k < n; k++) {
+        hamr_ctx *c = blocks[k];
+        BEntry &e = host[k];
+        e.d = c->d;
+        e.m = geom_of(c);
+        e.p = c->p; e.ph = c->ph; e.ps = c->ps; e.psh = c->psh; e.U = c->U;
+        e.F1 = c->F1; e.F2 = c->F2; e.F3 = c->F3; e.Ec = c->Ec; e.emf = c->emf; e.W = c->W;
+        e.pflag = c->pflag; e.failimage = c->failimage;
+        e.dtbits = b->dtbits + 4 * k;
+        e.ndt = b->ndts + k;
+        e.dt_state = b->dts + k;
+        e.counter = b->counters + k;
+        for (int ph = 0; ph < PH_N; ph++) b->items[ph].push_back(phase_items(ph, c->d));
+    }
+    int rc = HAMR_OK;
+    // the members' own streams may still be filling their state
+    for (hamr_ctx *c : b->ctx)
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess) rc = HAMR_E_CUDA;
+    if (rc == HAMR_OK &&
+        cudaMemcpyAsync(b->E, host.data(), sizeof(BEntry) * n, cudaMemcpyHostToDevice, b->stream) != cudaSuccess)
+        rc = HAMR_E_CUDA;
+    for (int ph = 0; ph < PH_N && rc == HAMR_OK; ph++) {
+        b->tile[ph] = BLK;      // default: one BLK-item tile per CTA, caller's order
+        b->grid[ph] = 0;
+        b->order_mode[ph] = 0;
+        rc = build_tiles(b, ph);
+    }
+    if (rc == HAMR_OK) {
+        k_batch_dt_reset<<<nblk_b(n), 128, 0, b->stream>>>(b->E, n);
+        if (cudaStreamSynchronize(b->stream) != cudaSuccess) rc = HAMR_E_CUDA;
+    }
+    if (rc) {
+        hamr_batch_destroy(b);
+        return rc;
+    }
+    *out = b;
+    return HAMR_OK;
+}
+
+int hamr_batch_destroy(hamr_batch *b) {
+    if (!b) return HAMR_E_ARG;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    cudaFree(b->E);
+    cudaFree(b->dtbits);
+    cudaFree(b->dts);
+    cudaFree(b->ndts);
+    cudaFree(b->counters);
+    for (int ph = 0; ph < PH_N; ph++) {
+        cudaFree(b->dstart[ph]);
+        cudaFree(b->dorder[ph]);
+    }
+    if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return HAMR_OK;
+}
+
+const char *hamr_batch_last_error(hamr_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+int hamr_batch_step(hamr_batch *b, const double *dt, double *dt_next) {
+    if (!b || !dt) return HAMR_E_ARG;
+    for (int k = 0; k < b->n; k++)
+        if (!(dt[k] > 0)) return HAMR_E_ARG;
+    BCK(cudaMemcpyAsync(b->dts, dt, sizeof(double) * b->n, cudaMemcpyHostToDevice, b->stream));
+    k_batch_dt_reset<<<nblk_b(b->n), 128, 0, b->stream>>>(b->E, b->n);
+    int rc = batch_step_launch(b, 0, 0);
+    if (rc) return rc;
+    if (dt_next) {
+        BCK(cudaMemcpyAsync(dt_next, b->ndts, sizeof(double) * b->n, cudaMemcpyDeviceToHost, b->stream));
+        BCK(cudaStreamSynchronize(b->stream));
+        for (int k = 0; k < b->n; k++)
+            if (!(dt_next[k] > 0) || !isfinite(dt_next[k])) {
+                b->err = "non-finite or non-positive CFL step in block " + std::to_string(k);
+                return HAMR_E_PHYSICS;
+            }
+    }
+    return HAMR_OK;
+}
+
+int hamr_batch_advance(hamr_batch *b, int nsteps, int interval, double *dt_inout) {
+    if (!b || !dt_inout || nsteps < 1 || interval < 1) return HAMR_E_ARG;
+    for (int k = 0; k < b->n; k++)
+        if (!(dt_inout[k] > 0)) return HAMR_E_ARG;
+    BCK(cudaMemcpyAsync(b->dts, dt_inout, sizeof(double) * b->n, cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaMemsetAsync(b->counters, 0, sizeof(int) * b->n, b->stream));
+    k_batch_dt_reset<<<nblk_b(b->n), 128, 0, b->stream>>>(b->E, b->n);
+    if (!b->graph || b->graph_steps != nsteps || b->graph_interval != interval) {
+        if (b->graph) {
+            cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+        }
+        cudaGraph_t g;
+        BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = HAMR_OK;
+        for (int s = 0; s < nsteps && rc == HAMR_OK; s++) rc = batch_step_launch(b, 1, interval);
+        cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        if (rc) return rc;
+        if (e != cudaSuccess) return bfail(b, e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return bfail(b, e, "cudaGraphInstantiate");
+        b->graph_steps = nsteps;
+        b->graph_interval = interval;
+    }
+    BCK(cudaGraphLaunch(b->graph, b->stream));
+    BCK(cudaMemcpyAsync(dt_inout, b->dts, sizeof(double) * b->n, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    return HAMR_OK;
+}
+
+// Picks, phase by phase in stage order, the tile size, grid and schedule
+// order with the shortest device time for this batch: every candidate runs
+// the phase of a half sub-step `reps` times after one warm-up launch, timed
+// with CUDA events on the batch stream. Half sub-steps only write the
+// intermediate arrays (ph, psh, fluxes, EMFs, U cache, scratch), so p and ps
+// are untouched; the inversion failure counters are cleared afterwards.
+int hamr_batch_autotune(hamr_batch *b, const double *dt, int reps) {
+    if (!b || !dt || reps < 1) return HAMR_E_ARG;
+    for (int k = 0; k < b->n; k++)
+        if (!(dt[k] > 0)) return HAMR_E_ARG;
+    BCK(cudaMemcpyAsync(b->dts, dt, sizeof(double) * b->n, cudaMemcpyHostToDevice, b->stream));
+    const int tiles[] = {BLK, 4 * BLK, 16 * BLK, 64 * BLK};
+    const int grids[] = {0, 2 * b->nsm, 4 * b->nsm, 8 * b->nsm, 16 * b->nsm};
+    cudaEvent_t e0, e1;
+    BCK(cudaEventCreate(&e0));
+    BCK(cudaEventCreate(&e1));
+    int rc = HAMR_OK;
+    for (int ph = 0; ph < PH_N && rc == HAMR_OK; ph++) {
+        long work = 0;
+        for (long x : b->items[ph]) work += x;
+        if (work == 0) continue;
+        float best = 1e30f;
+        int bt = b->tile[ph], bg = b->grid[ph], bo = b->order_mode[ph];
+        for (int om = 0; om < 2 && rc == HAMR_OK; om++)
+            for (int tl : tiles)
+                for (int gr : grids) {
+                    b->tile[ph] = tl;
+                    b->grid[ph] = gr;
+                    b->order_mode[ph] = om;
+                    if ((rc = build_tiles(b, ph))) break;
+                    if (gr > 0 && gr >= b->ntiles[ph]) continue;   // same launch as one tile per CTA
+                    batch_stage(b, 0, false, ph);                   // warm-up
+                    cudaEventRecord(e0, b->stream);
+                    for (int r = 0; r < reps; r++) batch_stage(b, 0, false, ph);
+                    cudaEventRecord(e1, b->stream);
+                    if (cudaEventSynchronize(e1) != cudaSuccess) { rc = bfail(b, cudaGetLastError(), "autotune"); break; }
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    ms /= reps;
+                    if (ms < best) { best = ms; bt = tl; bg = gr; bo = om; }
+                }
+        b->tile[ph] = bt;
+        b->grid[ph] = bg;
+        b->order_mode[ph] = bo;
+        b->tuned_ms[ph] = best;
+        if (rc == HAMR_OK) rc = build_tiles(b, ph);
+        if (rc == HAMR_OK) batch_stage(b, 0, false, ph);   // leave this phase's outputs for the next phase
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    for (hamr_ctx *c : b->ctx) BCK(cudaMemsetAsync(c->failimage, 0, 4 * sizeof(int) * c->d.ks, b->stream));
+    k_batch_dt_reset<<<nblk_b(b->n), 128, 0, b->stream>>>(b->E, b->n);
+    BCK(cudaStreamSynchronize(b->stream));
+    if (b->graph) {   // launch shapes changed
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    return HAMR_OK;
+}
+
+// Chosen launch shape of each phase (HAMR_BATCH_PHASES entries each): items
+// per tile, grid (0: one tile per CTA), schedule order (0: as given, 1:
+// largest block first), and the tuned device time of the phase in ms (0 when
+// not tuned). Any output pointer may be NULL.
+int hamr_batch_tuning(hamr_batch *b, int *tile, int *grid, int *order, float *ms, int nphases) {
+    if (!b || nphases < PH_N) return HAMR_E_ARG;
+    for (int ph = 0; ph < PH_N; ph++) {
+        if (tile) tile[ph] = b->tile[ph];
+        if (grid) grid[ph] = b->grid[ph];
+        if (order) order[ph] = b->order_mode[ph];
+        if (ms) ms[ph] = b->tuned_ms[ph];
+    }
+    return HAMR_OK;
+}
+
+}  // extern "C"

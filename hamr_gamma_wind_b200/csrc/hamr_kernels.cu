@@ -18,6 +18,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -88,99 +89,115 @@ struct StepSize {
 #ifndef HAMR_FLUX_MINB_F
 #define HAMR_FLUX_MINB_F 6
 #endif
+// one face of direction DIR (t < n_faces): reconstruction, two states, four
+// flux evaluations, HLL; returns the face's CFL limit, or 1e9 when filtered
 template <int DIR, typename T, int REC>
-__global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? HAMR_FLUX_MINB : HAMR_FLUX_MINB_F) k_flux(const Dims d, const Geom m, const double *__restrict__ pv,
-                                               const double *__restrict__ ps, T *__restrict__ F,
-                                               unsigned long long *__restrict__ dtbits, int calc_dt) {
+__device__ __forceinline__ double flux_face(const Dims &d, const Geom &m, const double *__restrict__ pv,
+                                            const double *__restrict__ ps, T *__restrict__ F, const long t) {
     constexpr int idel = DIR == 1, jdel = DIR == 2, zdel = DIR == 3;
     const int i0 = (d.ng1 - 1) * d.d1 + idel, ni = d.n1 + 2 * d.d1 - idel;
     const int j0 = (d.ng2 - 1) * d.d2 + jdel, nj = d.n2 + 2 * d.d2 - jdel;
     const int z0 = (d.ng3 - 1) * d.d3 + zdel, nz = d.n3 + 2 * d.d3 - zdel;
-    const long nf = (long)ni * nj * nz;
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    (void)ni;
     double dtf = 1.e9;
-    if (t < nf) {
-        const int z = z0 + (int)(t % nz);
-        const int j = j0 + (int)((t / nz) % nj);
-        const int i = i0 + (int)(t / ((long)nz * nj));
-        const long c = cix(d, i, j, z);
-        const long stride = idel ? (long)d.G2 * d.G3 : (jdel ? (long)d.G3 : 1L);
-        const int face = DIR == 1 ? FACE1 : (DIR == 2 ? FACE2 : FACE3);
-        Geo<T> gm;
-        load_geo_t(d, m, i, j, face, gm);
-        T pl[NPR], pr[NPR];
+    const int z = z0 + (int)(t % nz);
+    const int j = j0 + (int)((t / nz) % nj);
+    const int i = i0 + (int)(t / ((long)nz * nj));
+    const long c = cix(d, i, j, z);
+    const long stride = idel ? (long)d.G2 * d.G3 : (jdel ? (long)d.G3 : 1L);
+    const int face = DIR == 1 ? FACE1 : (DIR == 2 ? FACE2 : FACE3);
+    Geo<T> gm;
+    load_geo_t(d, m, i, j, face, gm);
+    T pl[NPR], pr[NPR];
 #pragma unroll
-        for (int k = 0; k < NPR; k++) {
-            const double *pk = pv + (long)k * d.ks + c;
-            if constexpr (REC == HAMR_RECON_MC) {
-                // linear MC: the zones' face values y -+ slope/2 (fluxcalcprep, PPM = 0)
-                T x[4];
+    for (int k = 0; k < NPR; k++) {
+        const double *pk = pv + (long)k * d.ks + c;
+        if constexpr (REC == HAMR_RECON_MC) {
+            // linear MC: the zones' face values y -+ slope/2 (fluxcalcprep, PPM = 0)
+            T x[4];
 #pragma unroll
-                for (int s = 0; s < 4; s++) x[s] = (T)__ldg(pk + (s - 2) * stride);
-                T temp = T(0.5) * slope_lim(x[0], x[1], x[2]);
-                pl[k] = x[1] + temp;
-                temp = T(0.5) * slope_lim(x[1], x[2], x[3]);
-                pr[k] = x[2] - temp;
-            } else {
-                T x[6];
+            for (int s = 0; s < 4; s++) x[s] = (T)__ldg(pk + (s - 2) * stride);
+            T temp = T(0.5) * slope_lim(x[0], x[1], x[2]);
+            pl[k] = x[1] + temp;
+            temp = T(0.5) * slope_lim(x[1], x[2], x[3]);
+            pr[k] = x[2] - temp;
+        } else {
+            T x[6];
 #pragma unroll
-                for (int s = 0; s < 6; s++) x[s] = (T)__ldg(pk + (s - 3) * stride);
-                T lo, hi;
-                para(x, lo, hi);       // zone c-1: upper edge is the left state
-                pl[k] = hi;
-                para(x + 1, lo, hi);   // zone c: lower edge is the right state
-                pr[k] = lo;
-            }
-        }
-        const T bn = (T)__ldg(&ps[(long)(DIR - 1) * d.ks + c]);
-        pl[B1 + DIR - 1] = bn;
-        pr[B1 + DIR - 1] = bn;
-        if (DIR == 2 && ((j == d.n2 + d.ng2 && d.pole2) || (j == d.ng2 && d.pole1))) {
-            pl[B1] = T(0.);
-            pr[B1] = T(0.);
-        }
-        const T gam = (T)d.gam;
-        State<T> q;
-        T t1[NPR], t2[NPR], t3[NPR], t4[NPR];
-        T cmax_l, cmin_l, cmax_r, cmin_r, vd;
-        get_state(pl, gm, q);
-        T e = entropy(gam, pl);
-        primtoflux(gam, pl, q, DIR, gm, e, t1, &cmax_l, &cmin_l);
-        primtoflux(gam, pl, q, 0, gm, e, t2, &vd, &vd);
-        get_state(pr, gm, q);
-        e = entropy(gam, pr);
-        primtoflux(gam, pr, q, DIR, gm, e, t3, &cmax_r, &cmin_r);
-        primtoflux(gam, pr, q, 0, gm, e, t4, &vd, &vd);
-        const T cmax = d_fabs(d_max(d_max(T(0.), cmax_l), cmax_r));
-        const T cmin = d_fabs(d_max(d_max(T(0.), -cmin_l), -cmin_r));
-        const T ctop = d_max(cmax, cmin);
-#pragma unroll
-        for (int k = 0; k < NPR; k++)
-            F[(long)k * d.ks + c] = (cmax * t1[k] + cmin * t3[k] - cmax * cmin * (t4[k] - t2[k])) / (cmax + cmin + T(SMALL_D));
-        const double dxd = DIR == 1 ? d.dx1 : (DIR == 2 ? d.dx2 : d.dx3);
-        const double v = d.cour * dxd / (double)ctop;
-        if (v > 1.e-6 && v < dtf) dtf = v;
-    }
-    if (calc_dt) {
-        // block minimum by warp shuffles, one atomic per block
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) dtf = d_min(dtf, __shfl_xor_sync(0xffffffffu, dtf, o));
-        __shared__ double wmin[BLK / 32];
-        if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = dtf;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double b = wmin[0];
-            for (int w = 1; w < BLK / 32; w++) b = d_min(b, wmin[w]);
-            // positive doubles order like their bit patterns
-            atomicMin(&dtbits[DIR], (unsigned long long)__double_as_longlong(b));
+            for (int s = 0; s < 6; s++) x[s] = (T)__ldg(pk + (s - 3) * stride);
+            T lo, hi;
+            para(x, lo, hi);       // zone c-1: upper edge is the left state
+            pl[k] = hi;
+            para(x + 1, lo, hi);   // zone c: lower edge is the right state
+            pr[k] = lo;
         }
     }
+    const T bn = (T)__ldg(&ps[(long)(DIR - 1) * d.ks + c]);
+    pl[B1 + DIR - 1] = bn;
+    pr[B1 + DIR - 1] = bn;
+    if (DIR == 2 && ((j == d.n2 + d.ng2 && d.pole2) || (j == d.ng2 && d.pole1))) {
+        pl[B1] = T(0.);
+        pr[B1] = T(0.);
+    }
+    const T gam = (T)d.gam;
+    State<T> q;
+    T t1[NPR], t2[NPR], t3[NPR], t4[NPR];
+    T cmax_l, cmin_l, cmax_r, cmin_r, vd;
+    get_state(pl, gm, q);
+    T e = entropy(gam, pl);
+    primtoflux(gam, pl, q, DIR, gm, e, t1, &cmax_l, &cmin_l);
+    primtoflux(gam, pl, q, 0, gm, e, t2, &vd, &vd);
+    get_state(pr, gm, q);
+    e = entropy(gam, pr);
+    primtoflux(gam, pr, q, DIR, gm, e, t3, &cmax_r, &cmin_r);
+    primtoflux(gam, pr, q, 0, gm, e, t4, &vd, &vd);
+    const T cmax = d_fabs(d_max(d_max(T(0.), cmax_l), cmax_r));
+    const T cmin = d_fabs(d_max(d_max(T(0.), -cmin_l), -cmin_r));
+    const T ctop = d_max(cmax, cmin);
+#pragma unroll
+    for (int k = 0; k < NPR; k++)
+        F[(long)k * d.ks + c] = (cmax * t1[k] + cmin * t3[k] - cmax * cmin * (t4[k] - t2[k])) / (cmax + cmin + T(SMALL_D));
+    const double dxd = DIR == 1 ? d.dx1 : (DIR == 2 ? d.dx2 : d.dx3);
+    const double v = d.cour * dxd / (double)ctop;
+    if (v > 1.e-6 && v < dtf) dtf = v;
+    return dtf;
+}
+
+// faces of direction DIR of one block
+template <int DIR>
+__host__ __device__ __forceinline__ long n_faces(const Dims &d) {
+    constexpr int idel = DIR == 1, jdel = DIR == 2, zdel = DIR == 3;
+    return (long)(d.n1 + 2 * d.d1 - idel) * (d.n2 + 2 * d.d2 - jdel) * (d.n3 + 2 * d.d3 - zdel);
+}
+
+// CTA minimum of the threads' CFL limits by warp shuffles, one atomic per CTA
+// (positive doubles order like their bit patterns)
+__device__ __forceinline__ void cta_min_dt(double dtf, unsigned long long *slot) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dtf = d_min(dtf, __shfl_xor_sync(0xffffffffu, dtf, o));
+    __shared__ double wmin[BLK / 32];
+    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = dtf;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = wmin[0];
+        for (int w = 1; w < BLK / 32; w++) b = d_min(b, wmin[w]);
+        atomicMin(slot, (unsigned long long)__double_as_longlong(b));
+    }
+    __syncthreads();   // wmin is reused by the CTA's next tile
+}
+
+template <int DIR, typename T, int REC>
+__global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? HAMR_FLUX_MINB : HAMR_FLUX_MINB_F) k_flux(const Dims d, const Geom m, const double *__restrict__ pv,
+                                               const double *__restrict__ ps, T *__restrict__ F,
+                                               unsigned long long *__restrict__ dtbits, int calc_dt) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const double dtf = t < n_faces<DIR>(d) ? flux_face<DIR, T, REC>(d, m, pv, ps, F, t) : 1.e9;
+    if (calc_dt) cta_min_dt(dtf, &dtbits[DIR]);
 }
 
 // reflective polar axis and no-inflow radial edges (fix_flux, GPU_const_trans.h:3-61)
 template <typename T>
-__global__ void k_fix_flux(const Dims d, T *F1, T *F2, T *F3) {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void fix_flux_at(const Dims &d, T *F1, T *F2, T *F3, const long t) {
     const long ks = d.ks;
     const long na = (long)d.G1 * d.G3;
     if (t < na) {
@@ -208,13 +225,20 @@ __global__ void k_fix_flux(const Dims d, T *F1, T *F2, T *F3) {
     if (F1[co] < T(0.)) F1[co] = T(0.);
 }
 
+// items of fix_flux: (i, z) on the polar rows, then (j, z) on the radial edges
+__host__ __device__ __forceinline__ long n_fix_flux(const Dims &d) { return (long)d.G1 * d.G3 + (long)d.G2 * d.G3; }
+
+template <typename T>
+__global__ void k_fix_flux(const Dims d, T *F1, T *F2, T *F3) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n_fix_flux(d)) fix_flux_at(d, F1, F2, F3, t);
+}
+
 // cell-centre EMF, -gdet (u x b), on the active zones plus one ghost layer
 template <typename T>
-__global__ void __launch_bounds__(BLK) k_emf_centre(const Dims d, const Geom m, const double *__restrict__ pv,
-                                                     T *__restrict__ Ec) {
+__device__ __forceinline__ void k_emf_centre_at(const Dims &d, const Geom &m, const double *__restrict__ pv,
+                                                     T *__restrict__ Ec, const long t) {
     const int ni = d.n1 + 2 * d.d1, nj = d.n2 + 2 * d.d2, nz = d.n3 + 2 * d.d3;
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)ni * nj * nz) return;
     const int z = (d.ng3 - d.d3) * d.d3 + (int)(t % nz);
     const int j = (d.ng2 - d.d2) * d.d2 + (int)((t / nz) % nj);
     const int i = (d.ng1 - d.d1) * d.d1 + (int)(t / ((long)nz * nj));
@@ -235,6 +259,15 @@ __global__ void __launch_bounds__(BLK) k_emf_centre(const Dims d, const Geom m, 
     Ec[3 * d.ks + c] = -gm.g * (ucon[1] * bcon[2] - ucon[2] * bcon[1]);
 }
 
+template <typename T>
+__global__ void __launch_bounds__(BLK) k_emf_centre(const Dims d, const Geom m, const double *__restrict__ pv,
+                                                     T *__restrict__ Ec) {
+    const int ni = d.n1 + 2 * d.d1, nj = d.n2 + 2 * d.d2, nz = d.n3 + 2 * d.d3;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)ni * nj * nz) return;
+    k_emf_centre_at(d, m, pv, Ec, t);
+}
+
 template <typename T> __device__ __forceinline__ T up(T f) { return (T)(f <= T(0.0)); }
 template <typename T> __device__ __forceinline__ T dn(T f) { return (T)(f > T(0.0)); }
 
@@ -242,12 +275,10 @@ template <typename T> __device__ __forceinline__ T dn(T f) { return (T)(f > T(0.
 // centre-minus-face corrections from the upwind side of each face, chosen by
 // the sign of its mass flux (consttransport2, GPU_const_trans.h:121-338)
 template <typename T>
-__global__ void __launch_bounds__(BLK) k_emf_edge(const Dims d, const T *__restrict__ Ec,
+__device__ __forceinline__ void k_emf_edge_at(const Dims &d, const T *__restrict__ Ec,
                                                    const T *__restrict__ F1, const T *__restrict__ F2,
-                                                   const T *__restrict__ F3, T *__restrict__ emf) {
+                                                   const T *__restrict__ F3, T *__restrict__ emf, const long t) {
     const int ni = d.n1 + d.d1, nj = d.n2 + d.d2, nz = d.n3 + d.d3;
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)ni * nj * nz) return;
     const int z = d.ng3 * d.d3 + (int)(t % nz);
     const int j = d.ng2 * d.d2 + (int)((t / nz) % nj);
     const int i = d.ng1 * d.d1 + (int)(t / ((long)nz * nj));
@@ -305,14 +336,22 @@ __global__ void __launch_bounds__(BLK) k_emf_edge(const Dims d, const T *__restr
     emf[3 * ks + c] = e3;
 }
 
+template <typename T>
+__global__ void __launch_bounds__(BLK) k_emf_edge(const Dims d, const T *__restrict__ Ec,
+                                                   const T *__restrict__ F1, const T *__restrict__ F2,
+                                                   const T *__restrict__ F3, T *__restrict__ emf) {
+    const int ni = d.n1 + d.d1, nj = d.n2 + d.d2, nz = d.n3 + d.d3;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)ni * nj * nz) return;
+    k_emf_edge_at(d, Ec, F1, F2, F3, emf, t);
+}
+
 // phi-average of the x1-EMF on the polar edges of a block that holds every
 // phi zone (E_average, const_trans.c:268-503): dt-scaled sum over active z,
 // divided by n3, unscaled; x3-EMF zeroed there. One thread per (side, i).
 template <typename T>
-__global__ void k_pole_average(const Dims d, T *emf, StepSize st) {
+__device__ __forceinline__ void k_pole_average_at(const Dims &d, T *emf, StepSize st, const long t) {
     const int ni = d.n1 + d.ng1;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 2 * ni) return;
     const int side = t / ni, i = d.ng1 + t % ni;
     if ((side == 0 && !d.pole1) || (side == 1 && !d.pole2)) return;
     const int jp = side == 0 ? d.ng2 : d.n2 + d.ng2;
@@ -327,13 +366,19 @@ __global__ void k_pole_average(const Dims d, T *emf, StepSize st) {
     }
 }
 
+template <typename T>
+__global__ void k_pole_average(const Dims d, T *emf, StepSize st) {
+    const int ni = d.n1 + d.ng1;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * ni) return;
+    k_pole_average_at(d, emf, st, t);
+}
+
 // staggered field update from the edge EMFs (consttransport3, GPU_const_trans.h:426-529)
 template <typename T>
-__global__ void __launch_bounds__(BLK) k_face_update(const Dims d, const Geom m, const double *psi, double *psf,
-                                                      const T *__restrict__ Et, StepSize st) {
+__device__ __forceinline__ void k_face_update_at(const Dims &d, const Geom &m, const double *psi, double *psf,
+                                                      const T *__restrict__ Et, StepSize st, const long t) {
     const int ni = d.n1 + d.d1, nj = d.n2 + d.d2, nz = d.n3 + d.d3;
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)ni * nj * nz) return;
     const int z = d.ng3 * d.d3 + (int)(t % nz);
     const int j = d.ng2 * d.d2 + (int)((t / nz) % nj);
     const int i = d.ng1 * d.d1 + (int)(t / ((long)nz * nj));
@@ -364,6 +409,15 @@ __global__ void __launch_bounds__(BLK) k_face_update(const Dims d, const Geom m,
         if (d.ng3 > 0) temp += -Dt / ((double)1 * d.dx3) * (E(1 * ks + c + d.d3) - E(1 * ks + c));
         psf[1 * ks + c] = temp / gdf;
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BLK) k_face_update(const Dims d, const Geom m, const double *psi, double *psf,
+                                                      const T *__restrict__ Et, StepSize st) {
+    const int ni = d.n1 + d.d1, nj = d.n2 + d.d2, nz = d.n3 + d.d3;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)ni * nj * nz) return;
+    k_face_update_at(d, m, psi, psf, Et, st, t);
 }
 
 // geometric source gdet T^k_l Gamma^l_{jk} (source, GPU_phys_mhd.h:34-175)
@@ -530,13 +584,11 @@ __device__ __forceinline__ void invert_zone(const Dims &d, const Geo<double> &gm
 #define HAMR_CONS_MINB 8
 #endif
 template <typename T>
-__global__ void __launch_bounds__(BLK, HAMR_CONS_MINB) k_cons(const Dims d, const Geom m, const double *__restrict__ pin,
+__device__ __forceinline__ void k_cons_at(const Dims &d, const Geom &m, const double *__restrict__ pin,
                                                const double *__restrict__ pb, double *__restrict__ Ucache,
                                                const T *__restrict__ F1, const T *__restrict__ F2,
                                                const T *__restrict__ F3, double *__restrict__ W, int full,
-                                               StepSize st) {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)d.n1 * d.n2 * d.n3) return;
+                                               StepSize st, const long t) {
     const int z = d.ng3 + (int)(t % d.n3);
     const int j = d.ng2 + (int)((t / d.n3) % d.n2);
     const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
@@ -554,13 +606,22 @@ __global__ void __launch_bounds__(BLK, HAMR_CONS_MINB) k_cons(const Dims d, cons
     W[6 * d.ks + c] = U[B3];   // kept in 2-D, where the faces do not set it
 }
 
-template <int INV>
-__global__ void __launch_bounds__(BLK, HAMR_UPD_MINB) k_invert(const Dims d, const Geom m, const double *__restrict__ pg,
-                                                 const double *__restrict__ W, const double *__restrict__ psf,
-                                                 double *__restrict__ pout, int *__restrict__ pflag,
-                                                 int *__restrict__ failimage) {
+template <typename T>
+__global__ void __launch_bounds__(BLK, HAMR_CONS_MINB) k_cons(const Dims d, const Geom m, const double *__restrict__ pin,
+                                               const double *__restrict__ pb, double *__restrict__ Ucache,
+                                               const T *__restrict__ F1, const T *__restrict__ F2,
+                                               const T *__restrict__ F3, double *__restrict__ W, int full,
+                                               StepSize st) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)d.n1 * d.n2 * d.n3) return;
+    k_cons_at(d, m, pin, pb, Ucache, F1, F2, F3, W, full, st, t);
+}
+
+template <int INV>
+__device__ __forceinline__ void k_invert_at(const Dims &d, const Geom &m, const double *__restrict__ pg,
+                                                 const double *__restrict__ W, const double *__restrict__ psf,
+                                                 double *__restrict__ pout, int *__restrict__ pflag,
+                                                 int *__restrict__ failimage, const long t) {
     const int z = d.ng3 + (int)(t % d.n3);
     const int j = d.ng2 + (int)((t / d.n3) % d.n2);
     const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
@@ -579,6 +640,16 @@ __global__ void __launch_bounds__(BLK, HAMR_UPD_MINB) k_invert(const Dims d, con
     U[B3] = W[6 * d.ks + c];
     face_average_b(d, m, psf, i, j, c, gi, U);
     invert_zone<INV>(d, gm, c, U, pf, pout, pflag, failimage);
+}
+
+template <int INV>
+__global__ void __launch_bounds__(BLK, HAMR_UPD_MINB) k_invert(const Dims d, const Geom m, const double *__restrict__ pg,
+                                                 const double *__restrict__ W, const double *__restrict__ psf,
+                                                 double *__restrict__ pout, int *__restrict__ pflag,
+                                                 int *__restrict__ failimage) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)d.n1 * d.n2 * d.n3) return;
+    k_invert_at<INV>(d, m, pg, W, psf, pout, pflag, failimage, t);
 }
 
 // ------------------------------------------------------------ ghost fills
@@ -615,9 +686,7 @@ __device__ __forceinline__ void copy_cell(const Dims &d, double *pv, long dst, l
 }
 
 // x1 ghosts over every (j, z): periodic copy, or outflow copy + no-inflow
-__global__ void k_bound_x1(const Dims d, const Geom m, double *pv, double *ps) {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)d.ng1 * d.G2 * d.G3) return;
+__device__ __forceinline__ void k_bound_x1_at(const Dims &d, const Geom &m, double *pv, double *ps, const long t) {
     const int z = (int)(t % d.G3), j = (int)((t / d.G3) % d.G2), g = (int)(t / ((long)d.G3 * d.G2));
     const int ilo = g, ihi = d.n1 + d.ng1 + g;
     const long ks = d.ks;
@@ -649,10 +718,14 @@ __global__ void k_bound_x1(const Dims d, const Geom m, double *pv, double *ps) {
     ps[2 * ks + dst] = ps[2 * ks + src];
 }
 
-// x3 ghosts (periodic) over every (i, j)
-__global__ void k_bound_x3(const Dims d, double *pv, double *ps) {
+__global__ void k_bound_x1(const Dims d, const Geom m, double *pv, double *ps) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)d.ng3 * d.G1 * d.G2) return;
+    if (t >= (long)d.ng1 * d.G2 * d.G3) return;
+    k_bound_x1_at(d, m, pv, ps, t);
+}
+
+// x3 ghosts (periodic) over every (i, j)
+__device__ __forceinline__ void k_bound_x3_at(const Dims &d, double *pv, double *ps, const long t) {
     const int g = (int)(t % d.ng3), j = (int)((t / d.ng3) % d.G2), i = (int)(t / ((long)d.ng3 * d.G2));
     const long lo = cix(d, i, j, g), lo_src = cix(d, i, j, g + d.n3);
     const long hi = cix(d, i, j, d.n3 + d.ng3 + g), hi_src = cix(d, i, j, d.ng3 + g);
@@ -664,11 +737,15 @@ __global__ void k_bound_x3(const Dims d, double *pv, double *ps) {
     }
 }
 
+__global__ void k_bound_x3(const Dims d, double *pv, double *ps) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)d.ng3 * d.G1 * d.G2) return;
+    k_bound_x3_at(d, pv, ps, t);
+}
+
 // x2 ghosts over every (i, z): periodic, transmissive or reflective polar
 // axis, or plain outflow copy
-__global__ void k_bound_x2(const Dims d, double *pv, double *ps) {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)d.G1 * d.G3) return;
+__device__ __forceinline__ void k_bound_x2_at(const Dims &d, double *pv, double *ps, const long t) {
     const int z = (int)(t % d.G3), i = (int)(t / d.G3);
     const int n2 = d.n2, ng = d.ng2;
     const long ks = d.ks;
@@ -759,6 +836,12 @@ __global__ void k_bound_x2(const Dims d, double *pv, double *ps) {
             ps[2 * ks + cix(d, i, n2 + ng + g, z)] = ps[2 * ks + cix(d, i, n2 + ng - 1, z)];
         }
     }
+}
+
+__global__ void k_bound_x2(const Dims d, double *pv, double *ps) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)d.G1 * d.G3) return;
+    k_bound_x2_at(d, pv, ps, t);
 }
 
 // --------------------------------------------------------- step size logic
@@ -1332,3 +1415,5 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
     }
     return HAMR_OK;
 }
+
+#include "hamr_batch.cuh"

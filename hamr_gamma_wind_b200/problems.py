@@ -287,3 +287,22 @@ def fm_torus(n1, n2, n3, spin=0.9375, rin=6.0, rmax=12.0, gam=13.0 / 9.0, kappa=
     bc = ("outflow", "pole_trans", "periodic") if n3 > 1 else ("outflow", "pole_refl", "periodic")
     return Problem(n1, n2, n3, ng, ks, gs, (dx[1], dx[2], dx[3]), gam, cour, bc, (1, 1), True, geo, p, ps,
                    coords="ks", spin=spin, startx=tuple(startx))
+
+
+def torus_ensemble(count=64, nmin=32, nmax=96, seed=2024, spin_max=0.99, rmax_range=(10.0, 16.0),
+                   rin=6.0, **kw):
+    """Seeded ensemble of magnetised FM tori of uneven sizes: per member, each
+    of n1, n2, n3 drawn uniformly from [nmin, nmax] (n3 even, for the
+    transmissive poles), spin a ~ U[0, spin_max], r_max ~ U[rmax_range], inner
+    edge r_in, outer boundary 8 r_max. Returns (problems, draws)."""
+    rng = np.random.default_rng(seed)
+    out, draws = [], []
+    for k in range(count):
+        n1, n2, n3 = (int(x) for x in rng.integers(nmin, nmax + 1, size=3))
+        n3 += n3 % 2
+        a = float(rng.uniform(0.0, spin_max))
+        rmax = float(rng.uniform(*rmax_range))
+        out.append(fm_torus(n1, n2, n3, spin=a, rin=rin, rmax=rmax, rout=8.0 * rmax,
+                            seed=int(rng.integers(1 << 30)), **kw))
+        draws.append(dict(n=(n1, n2, n3), spin=a, rmax=rmax))
+    return out, draws

@@ -196,6 +196,51 @@ int hamr_build_geometry(int coords, double spin, int n1, int n2, int n3, int ng,
 /* Boyer-Lindquist (r, theta, phi) of a code-coordinate point (bl_coord, coord.c:111). */
 int hamr_bl_coord(int coords, double spin, const double *X, double *rthph);
 
+/* ---- batched ensembles -----------------------------------------------------
+ * A batch advances many independent blocks -- uneven sizes, spins, grids --
+ * together: each phase of a sub-step (three face-flux directions, polar flux
+ * fix, centre and edge EMFs, polar EMF average, face update, conserved update,
+ * inversion, three ghost fills) is ONE launch for the whole ensemble, whose
+ * CTAs walk a tile space covering every block. The reference steps blocks one
+ * after another, a launch sequence per block (GPU_step_ch, step_ch.c:916-990,
+ * looping over n_active blocks); independent problems there are separate
+ * runs. Each block keeps its own step size: arrays of n doubles below are
+ * indexed like `blocks`.
+ *
+ * Members are existing contexts with geometry set; they must share precision,
+ * reconstruction and inversion. The batch runs on its own stream (`stream`, or
+ * one it creates when NULL) and uses the members' device arrays: do not step a
+ * member through its context while the batch is in use. */
+typedef struct hamr_batch hamr_batch;
+
+#define HAMR_BATCH_PHASES 13
+
+int hamr_batch_create(hamr_ctx *const *blocks, int n, void *stream, hamr_batch **out);
+int hamr_batch_destroy(hamr_batch *b);
+const char *hamr_batch_last_error(hamr_batch *b);
+
+/* One RK2 step of every block with its own dt[k]; dt_next[k] (may be NULL)
+ * receives each block's CFL step, as hamr_step. */
+int hamr_batch_step(hamr_batch *b, const double *dt, double *dt_next);
+
+/* nsteps RK2 steps of every block with the per-block step-size refresh of
+ * hamr_advance, replayed from one captured CUDA graph per (nsteps, interval).
+ * dt_inout[k]: in, block k's first step size; out, its step size after the
+ * last step (waits for the device). */
+int hamr_batch_advance(hamr_batch *b, int nsteps, int interval, double *dt_inout);
+
+/* Autotuner: times each phase over candidate launch shapes (items per tile,
+ * persistent grid size or one tile per CTA, schedule order as given or
+ * largest block first) on this batch, probe step sizes dt[k], `reps` timed
+ * launches per candidate, and keeps the fastest. Leaves p and ps untouched. */
+int hamr_batch_autotune(hamr_batch *b, const double *dt, int reps);
+
+/* The launch shape chosen for each of the HAMR_BATCH_PHASES phases (order:
+ * flux x3, x2, x1, polar flux fix, centre EMF, edge EMF, polar EMF average,
+ * face update, conserved update, inversion, ghost fill x1, x3, x2) and its
+ * tuned time in ms. Any output pointer may be NULL. */
+int hamr_batch_tuning(hamr_batch *b, int *tile, int *grid, int *order, float *ms, int nphases);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,6 +54,10 @@ def test_create_rejects_bad_parameters_without_device_work():
     assert L.hamr_ctx_create(None, ctypes.byref(ctx)) == -1
     assert L.hamr_stage(None, 0, 0.1, 0.1) == -1
     assert L.hamr_step(None, 0.1, None) == -1
+    out = ctypes.c_void_p()
+    assert L.hamr_batch_create(None, 0, None, ctypes.byref(out)) == -1
+    assert L.hamr_batch_step(None, None, None) == -1
+    assert L.hamr_batch_advance(None, 1, 1, None) == -1
 
 
 def _compare_tables(a, b):

@@ -1,0 +1,142 @@
+"""Batched ensembles (hamr_batch_*) against the same blocks stepped one by one
+through their own contexts.
+
+The batch launches run the very per-item bodies the single-block kernels run,
+so with the strict build (no multiply-add contraction, identical rounding in
+every inlined copy) the results must be bit for bit the same; the production
+build may contract differently in the batched copies, so it is held to 1e-12
+of each field's scale.
+"""
+import numpy as np
+import pytest
+
+from hamr_gamma_wind_b200 import problems
+from hamr_gamma_wind_b200.api import Batch, Block
+
+pytestmark = pytest.mark.gpu
+
+
+def _members(precision="fp64", strict=True, with_2d=True):
+    pbs, _ = problems.torus_ensemble(4, 16, 26, seed=7)
+    if with_2d:
+        pbs.append(problems.fm_torus(40, 32, 1, rout=40.0))   # reflective poles, 2-D
+    blocks = []
+    for pb in pbs:
+        b = Block(**pb.block_kwargs(), precision=precision, strict=strict)
+        b.set_geometry(pb.geo)
+        b.upload(pb.p, pb.ps)
+        b.bound()
+        blocks.append(b)
+    return pbs, blocks
+
+
+def _rel(a, b):
+    a = a.reshape(a.shape[0], -1)
+    b = b.reshape(b.shape[0], -1)
+    scale = np.maximum(np.abs(b).max(axis=1), 1e-300)
+    return float((np.abs(a - b).max(axis=1) / scale).max())
+
+
+def _close(blocks):
+    for b in blocks:
+        b.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_step_matches_single_blocks_bitwise(precision):
+    pbs, solo = _members(precision)
+    _, mem = _members(precision)
+    batch = Batch(mem)
+    dts = np.array([0.2 * min(pb.dx[:2]) for pb in pbs])
+    for _ in range(3):
+        dn_solo = np.array([b.step(dt) for b, dt in zip(solo, dts)])
+        dn_batch = batch.step(dts)
+        np.testing.assert_array_equal(dn_solo, dn_batch)
+        dts = np.minimum(dn_solo, 1.3 * dts)
+    for a, b in zip(solo, mem):
+        pa, sa = a.download()
+        pb_, sb = b.download()
+        np.testing.assert_array_equal(pa, pb_)
+        np.testing.assert_array_equal(sa, sb)
+    batch.close()
+    _close(solo + mem)
+
+
+def test_batch_production_build_close_to_single_blocks():
+    pbs, solo = _members(strict=False)
+    _, mem = _members(strict=False)
+    batch = Batch(mem)
+    dts = np.array([0.2 * min(pb.dx[:2]) for pb in pbs])
+    for _ in range(2):
+        for b, dt in zip(solo, dts):
+            b.step(dt)
+        batch.step(dts)
+    for a, b in zip(solo, mem):
+        assert _rel(a.active(a.download()[0]), b.active(b.download()[0])) <= 1e-12
+    batch.close()
+    _close(solo + mem)
+
+
+def test_batch_graph_advance_matches_step_loop_and_single_advance():
+    """advance (captured graph, per-member step-size refresh every 2 steps)
+    against the same steps taken through hamr_batch_step, and against each
+    member's own hamr_advance."""
+    pbs, a = _members()
+    _, b = _members()
+    _, solo = _members()
+    ba, bb = Batch(a), Batch(b)
+    dt0 = np.array([0.2 * min(pb.dx[:2]) for pb in pbs])
+    dt_graph = ba.advance(6, dt0, interval=2)
+    dt_solo = np.array([s.step_ch(6, d, interval=2) for s, d in zip(solo, dt0)])
+    np.testing.assert_array_equal(dt_graph, dt_solo)
+    dt = dt0.copy()
+    for n in range(6):
+        dn = bb.step(dt)
+        if (n + 1) % 2 == 0:
+            dt = np.minimum(dn, 1.3 * dt)
+    np.testing.assert_array_equal(dt, dt_graph)
+    for x, y, z in zip(a, b, solo):
+        px, py, pz = x.download()[0], y.download()[0], z.download()[0]
+        np.testing.assert_array_equal(px, py)
+        np.testing.assert_array_equal(px, pz)
+    ba.close()
+    bb.close()
+    _close(a + b + solo)
+
+
+def test_autotuned_batch_gives_identical_results():
+    """The autotuner only changes launch shapes (tiles, grid, schedule order):
+    state after tuning is untouched and the tuned batch steps bit for bit
+    like the untuned one."""
+    pbs, a = _members()
+    _, b = _members()
+    ba, bb = Batch(a), Batch(b)
+    dts = np.array([0.2 * min(pb.dx[:2]) for pb in pbs])
+    p_before = [x.download()[0] for x in a]
+    tun = ba.autotune(dts, reps=1)
+    assert set(tun) == {"flux3", "flux2", "flux1", "fix_flux", "emf_centre", "emf_edge", "pole_average",
+                        "face_update", "update", "invert", "bound_x1", "bound_x3", "bound_x2"}
+    assert tun["flux1"]["ms"] > 0 and tun["flux1"]["tile"] >= 128
+    for x, p0 in zip(a, p_before):
+        np.testing.assert_array_equal(x.download()[0], p0)
+    for _ in range(2):
+        np.testing.assert_array_equal(ba.step(dts), bb.step(dts))
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x.download()[0], y.download()[0])
+        np.testing.assert_array_equal(x.download_flags()[1], y.download_flags()[1])
+    ba.close()
+    bb.close()
+    _close(a + b)
+
+
+def test_batch_rejects_mixed_kinds():
+    pbs, blocks = _members(with_2d=False)
+    pb = pbs[0]
+    other = Block(**pb.block_kwargs(), precision="mixed", strict=True)
+    other.set_geometry(pb.geo)
+    with pytest.raises(Exception):
+        Batch(blocks + [other])
+    with pytest.raises(Exception):
+        Batch([blocks[0], blocks[0]])
+    other.close()
+    _close(blocks)
