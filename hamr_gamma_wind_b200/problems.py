@@ -247,6 +247,8 @@ def fm_torus(n1, n2, n3, spin=0.9375, rin=6.0, rmax=12.0, gam=13.0 / 9.0, kappa=
     u3 = np.broadcast_to(u[:, :, None], shape3).copy()
     pert = 1. + noise * (rng.random(shape3) - 0.5)
     u3 = np.where(inside[:, :, None], u3 * pert, u3)
+    if not inside.any():
+        raise ValueError(f"no bound torus for a={a}, r_in={rin}, r_max={rmax} on this grid")
     rhomax = rho3[np.broadcast_to(inside[:, :, None], shape3)].max()
     rho3 /= rhomax
     u3 /= rhomax
@@ -294,15 +296,19 @@ def torus_ensemble(count=64, nmin=32, nmax=96, seed=2024, spin_max=0.99, rmax_ra
     """Seeded ensemble of magnetised FM tori of uneven sizes: per member, each
     of n1, n2, n3 drawn uniformly from [nmin, nmax] (n3 even, for the
     transmissive poles), spin a ~ U[0, spin_max], r_max ~ U[rmax_range], inner
-    edge r_in, outer boundary 8 r_max. Returns (problems, draws)."""
+    edge r_in, outer boundary 8 r_max; draws that admit no bound torus are
+    redrawn. Returns (problems, draws)."""
     rng = np.random.default_rng(seed)
     out, draws = [], []
-    for k in range(count):
+    while len(out) < count:
         n1, n2, n3 = (int(x) for x in rng.integers(nmin, nmax + 1, size=3))
         n3 += n3 % 2
         a = float(rng.uniform(0.0, spin_max))
         rmax = float(rng.uniform(*rmax_range))
-        out.append(fm_torus(n1, n2, n3, spin=a, rin=rin, rmax=rmax, rout=8.0 * rmax,
-                            seed=int(rng.integers(1 << 30)), **kw))
+        try:
+            out.append(fm_torus(n1, n2, n3, spin=a, rin=rin, rmax=rmax, rout=8.0 * rmax,
+                                seed=int(rng.integers(1 << 30)), **kw))
+        except ValueError:
+            continue   # (a, r_max) admits no bound torus with this inner edge: draw again
         draws.append(dict(n=(n1, n2, n3), spin=a, rmax=rmax))
     return out, draws

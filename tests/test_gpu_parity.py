@@ -191,7 +191,10 @@ def test_mc_reconstruction_strict(case, ng):
     two ghost layers) against the oracle, strict build, three steps. The
     atmosphere is 1e-8 here: with floors off, as shipped, the 1e-14 one next
     to the magnetised torus surface runs away to NaN in the first step under
-    MC, in the oracle exactly as on the GPU."""
+    MC, in the oracle exactly as on the GPU. Tolerance 1e-11: in 3-D more
+    zones reach the entropy fallbacks under MC, whose pow() differs in the
+    last bit between CUDA and the host libm; moving the oracle's pow by one
+    ulp moves these velocities by 5e-12 of their scale (1e-15 with PPM)."""
     n1, n2, n3 = (32, 16, 8) if case == "torus3d" else (48, 48, 1)
     pb = problems.fm_torus(n1, n2, n3, rout=40.0, ng=ng, rho_atm=1e-8, u_atm=1e-10)
     blk, s = make_pair(pb, strict=True, recon="mc")
@@ -199,9 +202,9 @@ def test_mc_reconstruction_strict(case, ng):
     for _ in range(3):
         dn = blk.step(dt)
         dn_o = oracle_step(s, dt)
-        assert abs(dn - dn_o) <= 1e-14 * dn_o
+        assert abs(dn - dn_o) <= 1e-11 * dn_o
         dt = min(dn, 1.3 * dt)
     p, ps = blk.download()
-    assert field_rel_err(blk, p, s, "p").max() <= 1e-14
-    assert field_rel_err(blk, ps, s, "ps").max() <= 1e-14
+    assert field_rel_err(blk, p, s, "p").max() <= 1e-11
+    assert field_rel_err(blk, ps, s, "ps").max() <= 1e-11
     blk.close()
