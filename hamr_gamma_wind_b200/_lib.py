@@ -76,6 +76,15 @@ def load(strict: bool = False):
     L.hamr_batch_advance.argtypes = [_vp, _i, _i, _vp]
     L.hamr_batch_autotune.argtypes = [_vp, _vp, _i]
     L.hamr_batch_tuning.argtypes = [_vp, _vp, _vp, _vp, _vp, _i]
+    L.hamr_adjoint_create.argtypes = [_vp, _i, P(_vp)]
+    L.hamr_adjoint_destroy.argtypes = [_vp]
+    L.hamr_adjoint_last_error.argtypes = [_vp]
+    L.hamr_adjoint_last_error.restype = ctypes.c_char_p
+    L.hamr_adjoint_cotangent.argtypes = [_vp, _vp, _vp, _vp]
+    L.hamr_adjoint_zero.argtypes = [_vp]
+    L.hamr_step_backward.argtypes = [_vp, _d, _d]
+    L.hamr_mdot_forward.argtypes = [_vp, _i, _vp, P(_d)]
+    L.hamr_adjoint_run.argtypes = [_vp, _i, _vp, _i, P(_d), _vp, _vp, P(_d)]
     _libs[key] = L
     return L
 
@@ -86,7 +95,9 @@ SYMBOLS = ["hamr_ctx_create", "hamr_ctx_destroy", "hamr_last_error", "hamr_strid
            "hamr_bound", "hamr_stage", "hamr_step", "hamr_advance", "hamr_device_state", "hamr_profile_step",
            "hamr_divb_max", "hamr_build_geometry", "hamr_bl_coord", "hamr_step_noalloc",
            "hamr_batch_create", "hamr_batch_destroy", "hamr_batch_last_error", "hamr_batch_step",
-           "hamr_batch_advance", "hamr_batch_autotune", "hamr_batch_tuning"]
+           "hamr_batch_advance", "hamr_batch_autotune", "hamr_batch_tuning",
+           "hamr_adjoint_create", "hamr_adjoint_destroy", "hamr_adjoint_last_error", "hamr_adjoint_cotangent",
+           "hamr_adjoint_zero", "hamr_step_backward", "hamr_mdot_forward", "hamr_adjoint_run"]
 NOALLOC_MAX_CELLS = 32768
 
 BATCH_PHASES = ["flux3", "flux2", "flux1", "fix_flux", "emf_centre", "emf_edge", "pole_average",

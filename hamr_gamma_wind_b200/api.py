@@ -270,3 +270,65 @@ class Batch:
         self._check(self.L.hamr_batch_tuning(self.h, p(tile), p(grid), p(order), p(ms), n), "hamr_batch_tuning")
         return {ph: dict(tile=int(tile[k]), grid=int(grid[k]), order=("largest-first" if order[k] else "given"),
                          ms=float(ms[k])) for k, ph in enumerate(_lib.BATCH_PHASES)}
+
+
+class Adjoint:
+    """Reverse mode of the FP64 step of a 2-D torus Block (hamr_adjoint_*):
+    the accretion-rate objective J = sum_n dt_n Mdot_n through x1 face column
+    `mdot_face` and its gradient w.r.t. the initial state and gamma."""
+
+    def __init__(self, block, mdot_face):
+        self.block = block
+        self.L = block.L
+        h = ctypes.c_void_p()
+        rc = self.L.hamr_adjoint_create(block.ctx, int(mdot_face), ctypes.byref(h))
+        if rc:
+            raise _lib.HamrError(f"hamr_adjoint_create: {_lib.ERRORS.get(rc, rc)}")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.hamr_adjoint_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc:
+            msg = self.L.hamr_adjoint_last_error(self.h).decode()
+            raise _lib.HamrError(f"{what}: {_lib.ERRORS.get(rc, rc)} {msg}")
+
+    def forward(self, dts):
+        """Ghost fill and len(dts) steps (the block's state advances); returns J."""
+        d = np.ascontiguousarray(dts, dtype=float)
+        J = ctypes.c_double()
+        self._check(self.L.hamr_mdot_forward(self.h, len(d), d.ctypes.data_as(ctypes.c_void_p), ctypes.byref(J)),
+                    "hamr_mdot_forward")
+        return J.value
+
+    def gradient(self, dts, every=20):
+        """(J, dJ/dp (9 planes), dJ/dps (3 planes), dJ/dgamma); the block's
+        state is left at its initial value."""
+        d = np.ascontiguousarray(dts, dtype=float)
+        gp = np.zeros(9 * self.block.ksize)
+        gs = np.zeros(3 * self.block.ksize)
+        J, gg = ctypes.c_double(), ctypes.c_double()
+        p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        self._check(self.L.hamr_adjoint_run(self.h, len(d), p(d), int(every), ctypes.byref(J), p(gp), p(gs),
+                                            ctypes.byref(gg)), "hamr_adjoint_run")
+        return J.value, gp, gs, gg.value
+
+    def step_backward(self, dt, mdot_weight=0.0):
+        self._check(self.L.hamr_step_backward(self.h, float(dt), float(mdot_weight)), "hamr_step_backward")
+
+    def cotangent_pointers(self):
+        ptrs = [ctypes.c_void_p() for _ in range(3)]
+        self._check(self.L.hamr_adjoint_cotangent(self.h, *[ctypes.byref(x) for x in ptrs]), "hamr_adjoint_cotangent")
+        return [x.value for x in ptrs]
+
+    def zero(self):
+        self._check(self.L.hamr_adjoint_zero(self.h), "hamr_adjoint_zero")

@@ -1,0 +1,978 @@
+// Adjoint (reverse mode) of the FP64 RK2 step for axisymmetric blocks: 2-D
+// (n3 == 1), PPM, HLL, upwinded CT, Noble 2D inversion, outflow x1 with the
+// no-inflow check, reflective polar axis in x2. Included at the end of
+// hamr_kernels.cu.
+//
+// The step is reversed phase by phase. Linear phases (ghost fill copies,
+// flux divergence, face update, edge EMF, polar flux fix) have their
+// transposes written out; nonlinear per-item maps (face flux, centre EMF,
+// geometric source, conserved variables of a state, no-inflow check) get
+// their local derivatives from the forward routines themselves, instantiated
+// with forward-mode dual numbers (hamr_dual.cuh), and their transposes are
+// applied to the incoming cotangents. The inversion is reversed by the
+// implicit-function theorem: U(p) = W at the solution, so
+// W_bar = (dU/dp)^-T p_bar over the five hydrodynamic primitives. Limiter and
+// upwind branches are the ones the forward step took; the CFL step sizes are
+// held fixed.
+#include "hamr_dual.cuh"
+
+namespace {
+
+constexpr int ADJ_NP = 8;   // differentiated primitives: RHO, UU, U1-3, B1-3 (KTOT enters no flux)
+
+// --- templated copies of the double-only forward helpers ------------------
+// (the same operations as inflow_check and source in this file)
+template <typename T>
+__device__ __forceinline__ void inflow_check_t(T *pr, const Geo<double> &g0, int type) {
+    Geo<T> gm;
+    for (int s = 0; s < 10; s++) { gm.gcov[s] = T(g0.gcov[s]); gm.gcon[s] = T(g0.gcon[s]); }
+    gm.g = T(g0.g);
+    T ucon[4], gamma;
+    ucon_calc(pr, gm, ucon);
+    if (((ucon[1] > T(0.)) && (type == 0)) || ((ucon[1] < T(0.)) && (type == 1))) {
+        gamma_calc(pr, gm, &gamma);
+        pr[U1] /= gamma;
+        pr[U2] /= gamma;
+        pr[U3] /= gamma;
+        const double alpha = 1. / sqrt(-g0.gcon[0]);
+        const double beta1 = g0.gcon[1] * alpha * alpha;
+        pr[U1] = T(beta1 / alpha);
+        T vsq = gm.gcov[4] * pr[U1] * pr[U1];
+        vsq += T(2.) * gm.gcov[5] * pr[U2] * pr[U1];
+        vsq += T(2.) * gm.gcov[6] * pr[U3] * pr[U1];
+        vsq += gm.gcov[7] * pr[U2] * pr[U2];
+        vsq += T(2.) * gm.gcov[8] * pr[U3] * pr[U2];
+        vsq += gm.gcov[9] * pr[U3] * pr[U3];
+        vsq = d_max(T(1.e-13), vsq);
+        if (vsq >= T(1.)) vsq = T(1. - 1. / (80. * 80.));
+        gamma = T(1.) / d_sqrt(T(1.) - vsq);
+        pr[U1] *= gamma;
+        pr[U2] *= gamma;
+        pr[U3] *= gamma;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void source_t(T gam, const T *ph, const Geo<T> &gm, const Dims &d, const Geom &m,
+                                         long gi, T *dU, const State<T> &q) {
+    T mhd[4][4];
+    const long gs = d.gs;
+    const T P = (gam - T(1.)) * ph[UU];
+    const T u = ph[UU];
+    const T w = P + ph[RHO] + u;
+    const T bsq = dot4(q.bcon, q.bcov);
+    const T eta = w + bsq;
+    const T ptot = P + T(0.5) * bsq;
+    for (int a = 0; a < 4; a++)
+        for (int b = 0; b < 4; b++)
+            mhd[a][b] = eta * q.ucon[a] * q.ucov[b] + ptot * T(a == b ? 1. : 0.) - q.bcon[a] * q.bcov[b];
+    for (int k = 0; k < NPR; k++) dU[k] = T(0.);
+#define CONN(s, k) __ldg(&m.conn[(long)((s) * 4 + (k)) * gs + gi])
+    for (int k = 0; k < 4; k++) {
+        double c;
+        dU[UU] += mhd[0][k] * CONN(0, k);
+        dU[U1] += mhd[1][k] * CONN(4, k);
+        dU[U2] += mhd[2][k] * CONN(7, k);
+        dU[U3] += mhd[3][k] * CONN(9, k);
+        c = CONN(1, k); dU[UU] += mhd[1][k] * c; dU[U1] += mhd[0][k] * c;
+        c = CONN(2, k); dU[UU] += mhd[2][k] * c; dU[U2] += mhd[0][k] * c;
+        c = CONN(3, k); dU[UU] += mhd[3][k] * c; dU[U3] += mhd[0][k] * c;
+        c = CONN(5, k); dU[U1] += mhd[2][k] * c; dU[U2] += mhd[1][k] * c;
+        c = CONN(6, k); dU[U1] += mhd[3][k] * c; dU[U3] += mhd[1][k] * c;
+        c = CONN(8, k); dU[U2] += mhd[3][k] * c; dU[U3] += mhd[2][k] * c;
+    }
+#undef CONN
+    dU[UU] *= gm.g;
+    dU[U1] *= gm.g;
+    dU[U2] *= gm.g;
+    dU[U3] *= gm.g;
+    dU[KTOT] *= gm.g;
+}
+
+template <int N>
+__device__ __forceinline__ void geo_const(const Geo<double> &g0, Geo<Dual<N>> &g) {
+    for (int s = 0; s < 10; s++) { g.gcov[s] = Dual<N>(g0.gcov[s]); g.gcon[s] = Dual<N>(g0.gcon[s]); }
+    g.g = Dual<N>(g0.g);
+}
+
+// inputs of a state map: the ADJ_NP primitives, then gamma (index ADJ_NP)
+template <int N>
+__device__ __forceinline__ void seed_state(const double *pr, double gam, int pass, Dual<N> *pd, Dual<N> &gd) {
+    for (int k = 0; k < NPR; k++) pd[k] = Dual<N>(pr[k]);
+    for (int q = 0; q < N; q++) {
+        const int in = pass * N + q;
+        if (in < ADJ_NP) pd[in].d[q] = 1.;
+    }
+    gd = Dual<N>(gam);
+    const int qg = ADJ_NP - pass * N;
+    if (qg >= 0 && qg < N) gd.d[qg] = 1.;
+}
+
+__device__ __forceinline__ void block_add(double v, double *target) {
+    // CTA sum by warp shuffles, one atomic per warp
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v != 0.) atomicAdd(target, v);
+}
+
+}  // namespace
+
+namespace {
+
+// one side of a face: (fluxes along DIR, conserved variables, fast speeds) of
+// the reconstructed state ps; returns ps_bar (ADJ_NP) and adds to gam_bar,
+// given the cotangents of those outputs
+template <int DIR>
+__device__ void side_vjp(const double *pside, const Geo<double> &g0, double gam, const double *tfb,
+                         const double *tub, double cmxb, double cmnb, double *pbar, double &gbar) {
+    constexpr int N = 3;
+    Geo<Dual<N>> gm;
+    geo_const(g0, gm);
+    for (int pass = 0; pass * N <= ADJ_NP; pass++) {
+        Dual<N> pd[NPR], gd;
+        seed_state(pside, gam, pass, pd, gd);
+        State<Dual<N>> q;
+        get_state(pd, gm, q);
+        const Dual<N> e = entropy(gd, pd);
+        Dual<N> tf[NPR], tu[NPR], cmx, cmn, vd;
+        primtoflux(gd, pd, q, DIR, gm, e, tf, &cmx, &cmn);
+        primtoflux(gd, pd, q, 0, gm, e, tu, &vd, &vd);
+        for (int qd = 0; qd < N; qd++) {
+            const int in = pass * N + qd;
+            if (in > ADJ_NP) break;
+            double s = cmxb * cmx.d[qd] + cmnb * cmn.d[qd];
+            for (int k = 0; k < NPR; k++) s += tfb[k] * tf[k].d[qd] + tub[k] * tu[k].d[qd];
+            if (in < ADJ_NP) pbar[in] = s;
+            else gbar += s;
+        }
+    }
+}
+
+// face fluxes of direction DIR, reversed: aF (cotangent of the fluxes) ->
+// ap (primitives of the stencil, atomics), aps (normal face field), agam
+template <int DIR>
+__global__ void __launch_bounds__(BLK) k_adj_flux(const Dims d, const Geom m, const double *__restrict__ pv,
+                                                   const double *__restrict__ ps, const double *__restrict__ aF,
+                                                   double *ap, double *aps, double *agam) {
+    constexpr int idel = DIR == 1, jdel = DIR == 2, zdel = DIR == 3;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double gsum = 0.;
+    if (t < n_faces<DIR>(d)) {
+        const int i0 = (d.ng1 - 1) * d.d1 + idel, j0 = (d.ng2 - 1) * d.d2 + jdel, z0 = (d.ng3 - 1) * d.d3 + zdel;
+        const int nj = d.n2 + 2 * d.d2 - jdel, nz = d.n3 + 2 * d.d3 - zdel;
+        const int z = z0 + (int)(t % nz);
+        const int j = j0 + (int)((t / nz) % nj);
+        const int i = i0 + (int)(t / ((long)nz * nj));
+        const long c = cix(d, i, j, z), ks = d.ks;
+        const long stride = idel ? (long)d.G2 * d.G3 : (jdel ? (long)d.G3 : 1L);
+        double Fb[NPR];
+        bool any = false;
+        for (int k = 0; k < NPR; k++) { Fb[k] = aF[k * ks + c]; any |= Fb[k] != 0.; }
+        if (any) {
+            const int face = DIR == 1 ? FACE1 : (DIR == 2 ? FACE2 : FACE3);
+            Geo<double> g0;
+            load_geo(d, m, i, j, face, g0);
+            // PPM edge values and their (branch-local, linear) stencil weights
+            double pl[NPR], pr[NPR], cl[NPR][5], cr[NPR][5];
+            for (int k = 0; k < NPR; k++) {
+                const double *pk = pv + (long)k * ks + c;
+                double x[6];
+                for (int s = 0; s < 6; s++) x[s] = pk[(s - 3) * stride];
+                Dual<5> xl[5], xr[5], lo, hi;
+                for (int s = 0; s < 5; s++) { xl[s] = dual_var<5>(x[s], s); xr[s] = dual_var<5>(x[s + 1], s); }
+                para(xl, lo, hi);
+                pl[k] = hi.v;
+                for (int s = 0; s < 5; s++) cl[k][s] = hi.d[s];
+                para(xr, lo, hi);
+                pr[k] = lo.v;
+                for (int s = 0; s < 5; s++) cr[k][s] = lo.d[s];
+            }
+            const int bn = B1 + DIR - 1;
+            pl[bn] = pr[bn] = ps[(long)(DIR - 1) * ks + c];
+            const bool polefix = DIR == 2 && ((j == d.n2 + d.ng2 && d.pole2) || (j == d.ng2 && d.pole1));
+            if (polefix) pl[B1] = pr[B1] = 0.;
+            const double gam = d.gam;
+            State<double> q;
+            double t1[NPR], t2[NPR], t3[NPR], t4[NPR], cmax_l, cmin_l, cmax_r, cmin_r, vd;
+            get_state(pl, g0, q);
+            double e = entropy(gam, pl);
+            primtoflux(gam, pl, q, DIR, g0, e, t1, &cmax_l, &cmin_l);
+            primtoflux(gam, pl, q, 0, g0, e, t2, &vd, &vd);
+            get_state(pr, g0, q);
+            e = entropy(gam, pr);
+            primtoflux(gam, pr, q, DIR, g0, e, t3, &cmax_r, &cmin_r);
+            primtoflux(gam, pr, q, 0, g0, e, t4, &vd, &vd);
+            // HLL combination reversed (same max/abs selections as the forward)
+            const double in_x = 0. > cmax_l ? 0. : cmax_l;
+            const bool take_r = !(in_x > cmax_r);
+            const double ox = take_r ? cmax_r : in_x;
+            const double cmax = ox < 0. ? -ox : ox;
+            const double in_n = 0. > -cmin_l ? 0. : -cmin_l;
+            const bool take_rn = !(in_n > -cmin_r);
+            const double on = take_rn ? -cmin_r : in_n;
+            const double cmin = on < 0. ? -on : on;
+            const double D = cmax + cmin + SMALL_D;
+            double t1b[NPR], t2b[NPR], t3b[NPR], t4b[NPR], cmaxb = 0., cminb = 0.;
+            for (int k = 0; k < NPR; k++) {
+                const double Fk = (cmax * t1[k] + cmin * t3[k] - cmax * cmin * (t4[k] - t2[k])) / D;
+                t1b[k] = Fb[k] * cmax / D;
+                t3b[k] = Fb[k] * cmin / D;
+                t4b[k] = -Fb[k] * cmax * cmin / D;
+                t2b[k] = Fb[k] * cmax * cmin / D;
+                cmaxb += Fb[k] * ((t1[k] - cmin * (t4[k] - t2[k])) - Fk) / D;
+                cminb += Fb[k] * ((t3[k] - cmax * (t4[k] - t2[k])) - Fk) / D;
+            }
+            const double sx = ox < 0. ? -1. : 1., sn = on < 0. ? -1. : 1.;
+            double cmaxlb = 0., cmaxrb = 0., cminlb = 0., cminrb = 0.;
+            if (take_r) cmaxrb = sx * cmaxb;
+            else if (!(0. > cmax_l)) cmaxlb = sx * cmaxb;
+            if (take_rn) cminrb = -sn * cminb;
+            else if (!(0. > -cmin_l)) cminlb = -sn * cminb;
+            double plb[ADJ_NP], prb[ADJ_NP];
+            side_vjp<DIR>(pl, g0, gam, t1b, t2b, cmaxlb, cminlb, plb, gsum);
+            side_vjp<DIR>(pr, g0, gam, t3b, t4b, cmaxrb, cminrb, prb, gsum);
+            for (int k = 0; k < ADJ_NP; k++) {
+                if (k == bn || (polefix && k == B1)) continue;
+                for (int s = 0; s < 5; s++) {
+                    if (cl[k][s] != 0.) atomicAdd(&ap[k * ks + c + (s - 3) * stride], plb[k] * cl[k][s]);
+                    if (cr[k][s] != 0.) atomicAdd(&ap[k * ks + c + (s - 2) * stride], prb[k] * cr[k][s]);
+                }
+            }
+            atomicAdd(&aps[(long)(DIR - 1) * ks + c], plb[bn] + prb[bn]);
+        }
+    }
+    block_add(gsum, agam);
+}
+
+__device__ __forceinline__ bool active_zone(const Dims &d, int i, int j) {
+    return i >= d.ng1 && i < d.ng1 + d.n1 && j >= d.ng2 && j < d.ng2 + d.n2;
+}
+
+// flux divergence reversed (2-D): aF(f) = Dt/dx (aW(f) - aW(f - s)) for every
+// conserved component the inversion reads from the update (B1, B2 come from
+// the faces instead); plus the accretion-rate objective on x1 face column ih
+template <int DIR>
+__global__ void k_adj_divergence(const Dims d, const double *__restrict__ aW, double *aF, double Dt, int ih,
+                                 double mdot_coef) {
+    constexpr int idel = DIR == 1, jdel = DIR == 2;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_faces<DIR>(d)) return;
+    const int i0 = (d.ng1 - 1) * d.d1 + idel, j0 = (d.ng2 - 1) * d.d2 + jdel;
+    const int nj = d.n2 + 2 * d.d2 - jdel;
+    const int j = j0 + (int)(t % nj);
+    const int i = i0 + (int)(t / nj);
+    const long c = cix(d, i, j, 0), ks = d.ks;
+    const long stride = idel ? (long)d.G2 * d.G3 : (long)d.G3;
+    const double dx = DIR == 1 ? d.dx1 : d.dx2;
+    const bool ac = active_zone(d, i, j), am = active_zone(d, i - idel, j - jdel);
+    for (int k = 0; k < NPR; k++) {
+        if (k == B1 || k == B2) continue;
+        double v = 0.;
+        if (ac) v += Dt * aW[k * ks + c] / dx;
+        if (am) v -= Dt * aW[k * ks + c - stride] / dx;
+        aF[k * ks + c] += v;
+    }
+    if (DIR == 1 && i == ih && j >= d.ng2 && j < d.ng2 + d.n2) aF[RHO * ks + c] += mdot_coef;
+}
+
+// inversion reversed by the implicit-function theorem (active zones).
+// ap: cotangent of the inversion's output (consumed); apg: of its initial
+// guess (KTOT passes through; where no solver converged the hydrodynamic
+// primitives are the guess); aW: of the conserved input (9 planes).
+__global__ void __launch_bounds__(BLK) k_adj_invert(const Dims d, const Geom m, const double *__restrict__ pout,
+                                                     const int *__restrict__ pflag, double *ap, double *apg,
+                                                     double *aW, double *agam) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double gsum = 0.;
+    if (t < (long)d.n1 * d.n2 * d.n3) {
+        const int z = d.ng3 + (int)(t % d.n3);
+        const int j = d.ng2 + (int)((t / d.n3) % d.n2);
+        const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
+        const long c = cix(d, i, j, z), ks = d.ks;
+        double pb[NPR];
+        bool any = false;
+        for (int k = 0; k < NPR; k++) { pb[k] = ap[k * ks + c]; ap[k * ks + c] = 0.; any |= pb[k] != 0.; }
+        if (any) {
+            Geo<double> g0;
+            load_geo(d, m, i, j, CENT, g0);
+            apg[KTOT * ks + c] += pb[KTOT];
+            for (int b = 0; b < 3; b++) aW[(B1 + b) * ks + c] += pb[B1 + b] / g0.g;
+            if (pflag[c] != 0) {
+                for (int k = 0; k < 5; k++) apg[k * ks + c] += pb[k];
+            } else {
+                constexpr int N = ADJ_NP + 1;
+                Geo<Dual<N>> gm;
+                geo_const(g0, gm);
+                double pr[NPR];
+                for (int k = 0; k < NPR; k++) pr[k] = pout[k * ks + c];
+                Dual<N> pd[NPR], gd;
+                seed_state(pr, d.gam, 0, pd, gd);
+                State<Dual<N>> q;
+                get_state(pd, gm, q);
+                Dual<N> Ud[NPR], vd;
+                primtoflux(gd, pd, q, 0, gm, entropy(gd, pd), Ud, &vd, &vd);
+                // solve J5^T x = pb[0..4], J5[r][s] = dU_r/dp_s, by Gaussian
+                // elimination with partial pivoting on A = J5^T
+                double A[5][6];
+                for (int r = 0; r < 5; r++) {
+                    for (int s = 0; s < 5; s++) A[r][s] = Ud[s].d[r];
+                    A[r][5] = pb[r];
+                }
+                bool ok = true;
+                for (int col = 0; col < 5 && ok; col++) {
+                    int piv = col;
+                    for (int r = col + 1; r < 5; r++)
+                        if (fabs(A[r][col]) > fabs(A[piv][col])) piv = r;
+                    if (!(fabs(A[piv][col]) > 0.)) { ok = false; break; }
+                    if (piv != col)
+                        for (int s = 0; s < 6; s++) { const double tmp = A[col][s]; A[col][s] = A[piv][s]; A[piv][s] = tmp; }
+                    for (int r = col + 1; r < 5; r++) {
+                        const double f = A[r][col] / A[col][col];
+                        for (int s = col; s < 6; s++) A[r][s] -= f * A[col][s];
+                    }
+                }
+                if (ok) {
+                    double x[5];
+                    for (int r = 4; r >= 0; r--) {
+                        double v = A[r][5];
+                        for (int s = r + 1; s < 5; s++) v -= A[r][s] * x[s];
+                        x[r] = v / A[r][r];
+                    }
+                    for (int r = 0; r < 5; r++) aW[r * ks + c] += x[r];
+                    // field: p[B] = U[B]/gdet also moves the hydro solution
+                    for (int b = 0; b < 3; b++) {
+                        double v = 0.;
+                        for (int r = 0; r < 5; r++) v += x[r] * Ud[r].d[B1 + b];
+                        aW[(B1 + b) * ks + c] -= v / g0.g;
+                    }
+                    for (int r = 0; r < 5; r++) gsum -= x[r] * Ud[r].d[ADJ_NP];
+                }
+            }
+        }
+    }
+    block_add(gsum, agam);
+}
+
+}  // namespace
+
+namespace {
+
+// source term reversed (active zones): ap += Dt (d dU / d pb)^T aW, agam
+__global__ void __launch_bounds__(BLK) k_adj_source(const Dims d, const Geom m, const double *__restrict__ pb,
+                                                     const double *__restrict__ aW, double *ap, double Dt,
+                                                     double *agam) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double gsum = 0.;
+    if (t < (long)d.n1 * d.n2 * d.n3) {
+        const int z = d.ng3 + (int)(t % d.n3);
+        const int j = d.ng2 + (int)((t / d.n3) % d.n2);
+        const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
+        const long c = cix(d, i, j, z), gi = gix(d, i, j), ks = d.ks;
+        double wb[NPR];
+        bool any = false;
+        for (int k = 0; k < NPR; k++) { wb[k] = aW[k * ks + c]; any |= (k >= UU && k <= U3 && wb[k] != 0.); }
+        if (any) {
+            constexpr int N = 3;
+            Geo<double> g0;
+            load_geo(d, m, i, j, CENT, g0);
+            Geo<Dual<N>> gm;
+            geo_const(g0, gm);
+            double pr[NPR];
+            for (int k = 0; k < NPR; k++) pr[k] = pb[k * ks + c];
+            for (int pass = 0; pass * N <= ADJ_NP; pass++) {
+                Dual<N> pd[NPR], gd, dU[NPR];
+                seed_state(pr, d.gam, pass, pd, gd);
+                State<Dual<N>> q;
+                get_state(pd, gm, q);
+                source_t(gd, pd, gm, d, m, gi, dU, q);
+                for (int qd = 0; qd < N; qd++) {
+                    const int in = pass * N + qd;
+                    if (in > ADJ_NP) break;
+                    double s = 0.;
+                    for (int k = UU; k <= U3; k++) s += wb[k] * dU[k].d[qd];
+                    if (in < ADJ_NP) ap[in * ks + c] += Dt * s;
+                    else gsum += Dt * s;
+                }
+            }
+        }
+    }
+    block_add(gsum, agam);
+}
+
+// conserved variables of a state reversed (U(p^n) cached by the half
+// sub-step, active zones): ap += (dU/dp)^T aU, agam; aU consumed
+__global__ void __launch_bounds__(BLK) k_adj_cons_of_state(const Dims d, const Geom m, const double *__restrict__ pv,
+                                                            double *aU, double *ap, double *agam) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double gsum = 0.;
+    if (t < (long)d.n1 * d.n2 * d.n3) {
+        const int z = d.ng3 + (int)(t % d.n3);
+        const int j = d.ng2 + (int)((t / d.n3) % d.n2);
+        const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
+        const long c = cix(d, i, j, z), ks = d.ks;
+        double ub[NPR];
+        bool any = false;
+        for (int k = 0; k < NPR; k++) { ub[k] = aU[k * ks + c]; aU[k * ks + c] = 0.; any |= ub[k] != 0.; }
+        if (any) {
+            constexpr int N = 3;
+            Geo<double> g0;
+            load_geo(d, m, i, j, CENT, g0);
+            Geo<Dual<N>> gm;
+            geo_const(g0, gm);
+            double pr[NPR];
+            for (int k = 0; k < NPR; k++) pr[k] = pv[k * ks + c];
+            for (int pass = 0; pass * N <= ADJ_NP; pass++) {
+                Dual<N> pd[NPR], gd, U[NPR], vd;
+                seed_state(pr, d.gam, pass, pd, gd);
+                State<Dual<N>> q;
+                get_state(pd, gm, q);
+                primtoflux(gd, pd, q, 0, gm, entropy(gd, pd), U, &vd, &vd);
+                for (int qd = 0; qd < N; qd++) {
+                    const int in = pass * N + qd;
+                    if (in > ADJ_NP) break;
+                    double s = 0.;
+                    for (int k = 0; k < NPR; k++) s += ub[k] * U[k].d[qd];
+                    if (in < ADJ_NP) ap[in * ks + c] += s;
+                    else gsum += s;
+                }
+            }
+        }
+    }
+    block_add(gsum, agam);
+}
+
+// U^n feeds both sub-steps' updates: aU += aW over the components the
+// inversion reads from the update (not B1, B2, which come from the faces)
+__global__ void k_adj_cache_add(const Dims d, const double *__restrict__ aW, double *aU) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)d.n1 * d.n2 * d.n3) return;
+    const int z = d.ng3 + (int)(t % d.n3);
+    const int j = d.ng2 + (int)((t / d.n3) % d.n2);
+    const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
+    const long c = cix(d, i, j, z), ks = d.ks;
+    for (int k = 0; k < NPR; k++)
+        if (k != B1 && k != B2) aU[k * ks + c] += aW[k * ks + c];
+}
+
+// centre EMF reversed (2-D: x3 component only; active zones plus one ring):
+// ap += (d Ec3 / d p)^T aEc3
+__global__ void __launch_bounds__(BLK) k_adj_emf_centre(const Dims d, const Geom m, const double *__restrict__ pv,
+                                                         const double *__restrict__ aEc, double *ap) {
+    const int ni = d.n1 + 2 * d.d1, nj = d.n2 + 2 * d.d2;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)ni * nj) return;
+    const int j = (d.ng2 - d.d2) * d.d2 + (int)(t % nj);
+    const int i = (d.ng1 - d.d1) * d.d1 + (int)(t / nj);
+    const long c = cix(d, i, j, 0), ks = d.ks;
+    const double eb = aEc[3 * ks + c];
+    if (eb == 0.) return;
+    constexpr int N = 6;   // U1, U2, U3, B1, B2, B3
+    Geo<double> g0;
+    load_geo(d, m, i, j, CENT, g0);
+    Geo<Dual<N>> gm;
+    geo_const(g0, gm);
+    Dual<N> pd[NPR];
+    for (int k = 0; k < NPR; k++) pd[k] = Dual<N>(pv[k * ks + c]);
+    for (int q = 0; q < N; q++) pd[U1 + q].d[q] = 1.;
+    Dual<N> ucon[4], ucov[4], bcon[4];
+    ucon_calc(pd, gm, ucon);
+    lower4(ucon, gm.gcov, ucov);
+    bcon_calc(pd, ucon, ucov, bcon);
+    const Dual<N> e3 = -gm.g * (ucon[1] * bcon[2] - ucon[2] * bcon[1]);
+    for (int q = 0; q < N; q++) ap[(U1 + q) * ks + c] += eb * e3.d[q];
+}
+
+// edge EMF reversed (2-D: x3 component, upwind weights from the stage's
+// mass fluxes): aemf3 -> aEc3, aF1[B2], aF2[B1] (atomics)
+__global__ void k_adj_emf_edge(const Dims d, const double *__restrict__ F1, const double *__restrict__ F2,
+                               const double *__restrict__ aemf, double *aEc, double *aF1, double *aF2) {
+    const int ni = d.n1 + d.d1, nj = d.n2 + d.d2;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)ni * nj) return;
+    const int j = d.ng2 * d.d2 + (int)(t % nj);
+    const int i = d.ng1 * d.d1 + (int)(t / nj);
+    const long c = cix(d, i, j, 0), ks = d.ks, is = (long)d.G2 * d.G3, js = d.G3;
+    if ((d.pole1 && j == d.ng2) || (d.pole2 && j == d.n2 + d.ng2)) return;   // e3 = 0 on the axis
+    const double q = 0.25 * aemf[3 * ks + c];
+    if (q == 0.) return;
+    const double *F1r = F1 + RHO * ks, *F2r = F2 + RHO * ks;
+    const double ua = F2r[c] <= 0., da = F2r[c] > 0.;
+    const double ub = F2r[c - is] <= 0., db = F2r[c - is] > 0.;
+    const double uc = F1r[c] <= 0., dc = F1r[c] > 0.;
+    const double ud = F1r[c - js] <= 0., dd = F1r[c - js] > 0.;
+    atomicAdd(&aF2[B1 * ks + c], q * (1. + uc + ud));
+    atomicAdd(&aF2[B1 * ks + c - is], q * (1. + dc + dd));
+    atomicAdd(&aF1[B2 * ks + c], q * (-1. - ua - ub));
+    atomicAdd(&aF1[B2 * ks + c - js], q * (-1. - da - db));
+    atomicAdd(&aEc[3 * ks + c], q * (-ua - uc));
+    atomicAdd(&aEc[3 * ks + c - js], q * (-da - ud));
+    atomicAdd(&aEc[3 * ks + c - is], q * (-ub - dc));
+    atomicAdd(&aEc[3 * ks + c - is - js], q * (-db - dd));
+}
+
+// face update reversed (2-D), per edge: aemf3 from the cotangent of the
+// updated faces apsf
+__global__ void k_adj_face_update_emf(const Dims d, const Geom m, const double *__restrict__ apsf, double *aemf,
+                                      double Dt) {
+    const int ni = d.n1 + d.d1, nj = d.n2 + d.d2;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)ni * nj) return;
+    const int j = d.ng2 + (int)(t % nj);
+    const int i = d.ng1 + (int)(t / nj);
+    const long c = cix(d, i, j, 0), ks = d.ks, is = (long)d.G2 * d.G3, js = d.G3;
+    auto f0 = [&](int ii, int jj) { return ii >= d.ng1 && ii <= d.n1 + d.ng1 && jj >= d.ng2 && jj < d.n2 + d.ng2; };
+    auto f1 = [&](int ii, int jj) { return ii >= d.ng1 && ii < d.n1 + d.ng1 && jj >= d.ng2 && jj <= d.n2 + d.ng2; };
+    auto g1 = [&](int ii, int jj) { return __ldg(&m.gdet[FACE1 * d.gs + gix(d, ii, jj)]); };
+    auto g2 = [&](int ii, int jj) { return __ldg(&m.gdet[FACE2 * d.gs + gix(d, ii, jj)]); };
+    double e = 0.;
+    if (f0(i, j - 1)) e += apsf[c - js] * (-Dt / (d.dx2 * g1(i, j - 1)));
+    if (f0(i, j)) e += apsf[c] * (Dt / (d.dx2 * g1(i, j)));
+    if (f1(i - 1, j)) e += apsf[ks + c - is] * (Dt / (d.dx1 * g2(i - 1, j)));
+    if (f1(i, j)) e += apsf[ks + c] * (-Dt / (d.dx1 * g2(i, j)));
+    aemf[3 * ks + c] = e;
+}
+
+// half sub-step: ps^n -> psh is the identity on the updated faces
+__global__ void k_adj_face_carry(const Dims d, double *apsh, double *aps) {
+    const int ni = d.n1 + d.d1, nj = d.n2 + d.d2;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)ni * nj) return;
+    const int j = d.ng2 + (int)(t % nj);
+    const int i = d.ng1 + (int)(t / nj);
+    const long c = cix(d, i, j, 0), ks = d.ks;
+    if (i <= d.n1 + d.ng1 && j < d.n2 + d.ng2) { aps[c] += apsh[c]; apsh[c] = 0.; }
+    if (i < d.n1 + d.ng1 && j <= d.n2 + d.ng2) { aps[ks + c] += apsh[ks + c]; apsh[ks + c] = 0.; }
+}
+
+// U[B1], U[B2] from the face averages reversed (2-D), per face: aW -> apsf
+__global__ void k_adj_face_average(const Dims d, const Geom m, const double *__restrict__ aW, double *apsf) {
+    const int ni = d.n1 + d.d1, nj = d.n2 + d.d2;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)ni * nj) return;
+    const int j = d.ng2 + (int)(t % nj);
+    const int i = d.ng1 + (int)(t / nj);
+    const long c = cix(d, i, j, 0), ks = d.ks, is = (long)d.G2 * d.G3, js = d.G3;
+    double a = 0., b = 0.;
+    if (active_zone(d, i, j)) { a += aW[B1 * ks + c]; b += aW[B2 * ks + c]; }
+    if (active_zone(d, i - 1, j)) a += aW[B1 * ks + c - is];
+    if (active_zone(d, i, j - 1)) b += aW[B2 * ks + c - js];
+    if (a != 0.) apsf[c] += a * __ldg(&m.gdet[FACE1 * d.gs + gix(d, i, j)]) / 2.0;
+    if (b != 0.) apsf[ks + c] += b * __ldg(&m.gdet[FACE2 * d.gs + gix(d, i, j)]) / 2.0;
+}
+
+// reflective-pole and radial flux fixes reversed (2-D); F holds the fixed fluxes
+__global__ void k_adj_fix_flux(const Dims d, const double *__restrict__ F1, double *aF1, double *aF2) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long ks = d.ks;
+    if (t < d.G1) {
+        const int i = (int)t;
+        if (!(i >= d.ng1 - d.d1 && i < d.n1 + d.ng1 + d.d1)) return;
+        if (d.pole1) {
+            const long g = cix(d, i, d.ng2 - 1, 0), a = cix(d, i, d.ng2, 0);
+            aF1[B2 * ks + a] -= aF1[B2 * ks + g];
+            aF1[B2 * ks + g] = 0.;
+            for (int k = 0; k < NPR; k++) aF2[k * ks + a] = 0.;
+        }
+        if (d.pole2) {
+            const long g = cix(d, i, d.n2 + d.ng2, 0), a = cix(d, i, d.n2 + d.ng2 - 1, 0);
+            aF1[B2 * ks + a] -= aF1[B2 * ks + g];
+            aF1[B2 * ks + g] = 0.;
+            for (int k = 0; k < NPR; k++) aF2[k * ks + g] = 0.;
+        }
+        return;
+    }
+    const long u = t - d.G1;
+    if (u >= d.G2) return;
+    const int j = (int)u;
+    if (!(j >= d.ng2 - d.d2 && j < d.n2 + d.ng2 + d.d2)) return;
+    // clipped mass fluxes (stored as exactly 0) pass no cotangent
+    const long ci = RHO * ks + cix(d, d.ng1, j, 0), co = RHO * ks + cix(d, d.n1 + d.ng1, j, 0);
+    if (F1[ci] == 0.) aF1[ci] = 0.;
+    if (F1[co] == 0.) aF1[co] = 0.;
+}
+
+}  // namespace
+
+namespace {
+
+// x2 reflective-axis ghost fill reversed (2-D), one thread per i: ghost
+// copies (with the sign flips) and the POLEFIX interpolation of the first
+// two rows, in reverse order
+__global__ void k_adj_bound_x2_refl(const Dims d, double *ap, double *aps) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= d.G1) return;
+    const int i = (int)t, n2 = d.n2, ng = d.ng2, jref = 2;
+    const long ks = d.ks;
+    auto C = [&](int j) { return cix(d, i, j, 0); };
+    auto mv = [&](double *a, long dst, long src, double sgn) { a[src] += sgn * a[dst]; a[dst] = 0.; };
+    if (d.pole2) {
+        for (int g = ng - 1; g >= 0; g--) {
+            mv(aps, C(n2 + ng + g), C(n2 + ng - 1 - g), 1.);
+            mv(aps + 2 * ks, C(n2 + ng + g), C(n2 + ng - 1 - g), 1.);
+        }
+        for (int g = ng - 1; g >= 0; g--)
+            for (int k = 0; k < NPR; k++) {
+                const double s = (k == U2 || k == B2) ? -1. : 1.;
+                mv(ap + k * ks, C(n2 + ng + g), C(n2 + ng - 1 - g), s);
+            }
+        for (int jj = jref - 1; jj >= 0; jj--) {
+            const long c = C(n2 + ng - 1 - jj), r = C(n2 + ng - 1 - jref);
+            ap[U2 * ks + r] += (jj + 0.5) / (jref + 0.5) * ap[U2 * ks + c];
+            ap[U2 * ks + c] = 0.;
+            for (int k : {RHO, UU, U1, U3, KTOT}) mv(ap + k * ks, c, r, 1.);
+        }
+    }
+    if (d.pole1) {
+        for (int g = ng; g >= 1; g--) {
+            mv(aps, C(ng - g), C(ng + g - 1), 1.);
+            mv(aps + 2 * ks, C(ng - g), C(ng + g - 1), 1.);
+        }
+        for (int g = ng; g >= 1; g--)
+            for (int k = 0; k < NPR; k++) {
+                const double s = (k == U2 || k == B2) ? -1. : 1.;
+                mv(ap + k * ks, C(ng - g), C(ng + g - 1), s);
+            }
+        for (int jj = jref - 1; jj >= 0; jj--) {
+            const long c = C(jj + ng), r = C(jref + ng);
+            ap[U2 * ks + r] += (jj + 0.5) / (jref + 0.5) * ap[U2 * ks + c];
+            ap[U2 * ks + c] = 0.;
+            for (int k : {RHO, UU, U1, U3, KTOT}) mv(ap + k * ks, c, r, 1.);
+        }
+    }
+}
+
+// x1 outflow ghost fill reversed (2-D), one thread per (side, j): each ghost
+// is the edge zone through the no-inflow check (a map of the velocities)
+__global__ void k_adj_bound_x1_outflow(const Dims d, const Geom m, const double *__restrict__ pv, double *ap,
+                                       double *aps) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2L * d.G2) return;
+    const int side = (int)(t / d.G2), j = (int)(t % d.G2);
+    const long ks = d.ks;
+    const int iedge = side == 0 ? d.ng1 : d.n1 + d.ng1 - 1;
+    const long src = cix(d, iedge, j, 0);
+    double pr[NPR];
+    for (int k = 0; k < NPR; k++) pr[k] = pv[k * ks + src];
+    for (int g = 0; g < d.ng1; g++) {
+        const int ig = side == 0 ? g : d.n1 + d.ng1 + g;
+        const long dst = cix(d, ig, j, 0);
+        double gb[NPR];
+        bool any = false;
+        for (int k = 0; k < NPR; k++) { gb[k] = ap[k * ks + dst]; ap[k * ks + dst] = 0.; any |= gb[k] != 0.; }
+        aps[ks + src] += aps[ks + dst];
+        aps[2 * ks + src] += aps[2 * ks + dst];
+        aps[ks + dst] = aps[2 * ks + dst] = 0.;
+        if (!any) continue;
+        for (int k = 0; k < NPR; k++)
+            if (k < U1 || k > U3) ap[k * ks + src] += gb[k];
+        Geo<double> g0;
+        load_geo(d, m, ig, j, CENT, g0);
+        Dual<3> pd[NPR];
+        for (int k = 0; k < NPR; k++) pd[k] = Dual<3>(pr[k]);
+        for (int q = 0; q < 3; q++) pd[U1 + q].d[q] = 1.;
+        inflow_check_t(pd, g0, side);
+        for (int q = 0; q < 3; q++) {
+            double s = 0.;
+            for (int k = U1; k <= U3; k++) s += gb[k] * pd[k].d[q];
+            ap[(U1 + q) * ks + src] += s;
+        }
+    }
+}
+
+// J contribution of one step: w * Mdot, Mdot = - sum_j F1[RHO](ih, j) dx2 dx3
+__global__ void k_mdot_accum(const Dims d, const double *__restrict__ F1, int ih, double w, double *J) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.;
+    if (t < d.n2) v = -w * F1[RHO * d.ks + cix(d, ih, d.ng2 + (int)t, 0)] * d.dx2 * d.dx3;
+    block_add(v, J);
+}
+
+}  // namespace
+
+// ===========================================================================
+struct hamr_adjoint {
+    hamr_ctx *ctx = nullptr;
+    int ih = 0;                 // x1 face column of the accretion-rate objective
+    std::string err;
+    // cotangents (device): of p, ps (the state), ph, psh, U^n, the conserved
+    // update W (9 planes), fluxes, centre and edge EMFs
+    double *ap = nullptr, *aps = nullptr, *aph = nullptr, *apsh = nullptr, *aU = nullptr, *aW = nullptr;
+    double *aF1 = nullptr, *aF2 = nullptr, *aF3 = nullptr, *aEc = nullptr, *aemf = nullptr;
+    double *agam = nullptr, *J = nullptr;   // 1 double each
+    double *p0 = nullptr, *ps0 = nullptr;   // the step's input state while it is reversed
+    std::vector<double *> store;            // checkpoints and segment states (12 planes each)
+};
+
+namespace {
+
+int afail(hamr_adjoint *a, cudaError_t e, const char *what) {
+    a->err = std::string(what) + ": " + cudaGetErrorString(e);
+    return HAMR_E_CUDA;
+}
+
+#define ACK(call)                                               \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return afail(a, e_, #call);      \
+    } while (0)
+
+// one RK2 step of the context with a fixed dt (no step-size bookkeeping)
+int fixed_step(hamr_ctx *ctx, double dt) {
+    k_dt_reset<<<1, 32, 0, ctx->stream>>>(ctx->dtbits);
+    return launch_step(ctx, StepSize{nullptr, 0.5, 0.5 * dt, dt}, StepSize{nullptr, 1.0, dt, dt}, nullptr, 0);
+}
+
+unsigned nb(long n) { return (unsigned)((n + BLK - 1) / BLK); }
+
+// reverse of one ghost fill (x2 first: the forward fills x1, then x2)
+void adj_bound(hamr_ctx *ctx, const double *pv, double *ap, double *aps) {
+    const Dims &d = ctx->d;
+    cudaStream_t s = ctx->stream;
+    k_adj_bound_x2_refl<<<nb(d.G1), BLK, 0, s>>>(d, ap, aps);
+    k_adj_bound_x1_outflow<<<nb(2L * d.G2), BLK, 0, s>>>(d, geom_of(ctx), pv, ap, aps);
+}
+
+// reverse of one sub-step. pin: the stage's input primitives (p^n or ph);
+// apin/apsin: their cotangents (accumulated); apout: cotangent of the
+// inversion output (consumed); apsout: of the face field it writes.
+int adj_stage(hamr_adjoint *a, int full, double dt, double mdot_coef) {
+    hamr_ctx *ctx = a->ctx;
+    const Dims &d = ctx->d;
+    const Geom m = geom_of(ctx);
+    cudaStream_t s = ctx->stream;
+    const double Dt = full ? dt : 0.5 * dt;
+    const double *pin = full ? ctx->ph : ctx->p;
+    const double *pout = full ? ctx->p : ctx->ph;
+    double *apin = full ? a->aph : a->ap, *apsin = full ? a->apsh : a->aps;
+    double *apout = full ? a->ap : a->aph, *apsout = full ? a->aps : a->apsh;
+    const long ks = d.ks, nz = (long)d.n1 * d.n2, nedge = (long)(d.n1 + 1) * (d.n2 + 1);
+    ACK(cudaMemsetAsync(a->aW, 0, NPR * sizeof(double) * ks, s));
+    ACK(cudaMemsetAsync(a->aF1, 0, NPR * sizeof(double) * ks, s));
+    ACK(cudaMemsetAsync(a->aF2, 0, NPR * sizeof(double) * ks, s));
+    ACK(cudaMemsetAsync(a->aEc, 0, 4 * sizeof(double) * ks, s));
+    // ghost fill of the output, then the inversion (p_out <- W, guess pin)
+    adj_bound(ctx, pout, apout, apsout);
+    k_adj_invert<<<nb(nz), BLK, 0, s>>>(d, m, pout, ctx->pflag, apout, apin, a->aW, a->agam);
+    // U[B1], U[B2] from the updated faces
+    k_adj_face_average<<<nb(nedge), BLK, 0, s>>>(d, m, a->aW, apsout);
+    // update: U^n (cache), source at pin, flux divergence (+ objective)
+    k_adj_cache_add<<<nb(nz), BLK, 0, s>>>(d, a->aW, a->aU);
+    k_adj_source<<<nb(nz), BLK, 0, s>>>(d, m, pin, a->aW, apin, Dt, a->agam);
+    k_adj_divergence<1><<<nb(n_faces<1>(d)), BLK, 0, s>>>(d, a->aW, a->aF1, Dt, a->ih, full ? mdot_coef : 0.);
+    k_adj_divergence<2><<<nb(n_faces<2>(d)), BLK, 0, s>>>(d, a->aW, a->aF2, Dt, -1, 0.);
+    // face update: edge EMFs; ps^n -> psh carries the cotangent over
+    k_adj_face_update_emf<<<nb(nedge), BLK, 0, s>>>(d, m, apsout, a->aemf, Dt);
+    if (!full) k_adj_face_carry<<<nb(nedge), BLK, 0, s>>>(d, a->apsh, a->aps);
+    // edge EMFs -> centre EMFs and fluxes; centre EMFs -> pin
+    k_adj_emf_edge<<<nb(nedge), BLK, 0, s>>>(d, ctx->F1, ctx->F2, a->aemf, a->aEc, a->aF1, a->aF2);
+    k_adj_emf_centre<<<nb((long)(d.n1 + 2) * (d.n2 + 2)), BLK, 0, s>>>(d, m, pin, a->aEc, apin);
+    // flux fixes, then the face fluxes -> pin (and the normal face field)
+    k_adj_fix_flux<<<nb((long)d.G1 + d.G2), BLK, 0, s>>>(d, ctx->F1, a->aF1, a->aF2);
+    k_adj_flux<1><<<nb(n_faces<1>(d)), BLK, 0, s>>>(d, m, pin, full ? ctx->psh : ctx->ps, a->aF1, apin, apsin, a->agam);
+    k_adj_flux<2><<<nb(n_faces<2>(d)), BLK, 0, s>>>(d, m, pin, full ? ctx->psh : ctx->ps, a->aF2, apin, apsin, a->agam);
+    ACK(cudaGetLastError());
+    return HAMR_OK;
+}
+
+}  // namespace
+
+namespace {
+
+int step_backward(hamr_adjoint *a, double dt, double w) {
+    hamr_ctx *ctx = a->ctx;
+    const Dims &d = ctx->d;
+    cudaStream_t s = ctx->stream;
+    const size_t cb = sizeof(double) * d.ks;
+    ACK(cudaMemcpyAsync(a->p0, ctx->p, NPR * cb, cudaMemcpyDeviceToDevice, s));
+    ACK(cudaMemcpyAsync(a->ps0, ctx->ps, 3 * cb, cudaMemcpyDeviceToDevice, s));
+    int rc = fixed_step(ctx, dt);
+    if (rc) return rc;
+    ACK(cudaMemsetAsync(a->aph, 0, NPR * cb, s));
+    ACK(cudaMemsetAsync(a->apsh, 0, 3 * cb, s));
+    if ((rc = adj_stage(a, 1, dt, -w * d.dx2 * d.dx3))) return rc;
+    // back to the step's input; redo its half sub-step for the intermediates
+    ACK(cudaMemcpyAsync(ctx->p, a->p0, NPR * cb, cudaMemcpyDeviceToDevice, s));
+    ACK(cudaMemcpyAsync(ctx->ps, a->ps0, 3 * cb, cudaMemcpyDeviceToDevice, s));
+    if ((rc = launch_stage(ctx, 0, StepSize{nullptr, 0.5, 0.5 * dt, dt}, false))) return rc;
+    if ((rc = adj_stage(a, 0, dt, 0.))) return rc;
+    k_adj_cons_of_state<<<nb((long)d.n1 * d.n2), BLK, 0, s>>>(d, geom_of(ctx), ctx->p, a->aU, a->ap, a->agam);
+    ACK(cudaGetLastError());
+    return HAMR_OK;
+}
+
+int bound_ctx(hamr_ctx *ctx) {
+    const Dims &d = ctx->d;
+    cudaStream_t s = ctx->stream;
+    const Geom m = geom_of(ctx);
+    if (d.d1) k_bound_x1<<<nblk((long)d.ng1 * d.G2 * d.G3), BLK, 0, s>>>(d, m, ctx->p, ctx->ps);
+    if (d.d3) k_bound_x3<<<nblk((long)d.ng3 * d.G1 * d.G2), BLK, 0, s>>>(d, ctx->p, ctx->ps);
+    if (d.d2) k_bound_x2<<<nblk((long)d.G1 * d.G3), BLK, 0, s>>>(d, ctx->p, ctx->ps);
+    return cudaGetLastError() == cudaSuccess ? HAMR_OK : HAMR_E_CUDA;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hamr_adjoint_create(hamr_ctx *ctx, int mdot_face, hamr_adjoint **out) {
+    if (!ctx || !out) return HAMR_E_ARG;
+    *out = nullptr;
+    const hamr_params &p = ctx->prm;
+    const Dims &d = ctx->d;
+    // the configuration the reverse kernels are written for
+    if (p.precision != HAMR_FP64 || p.recon != HAMR_RECON_PPM || p.inversion != HAMR_INV_2D || d.n3 != 1 ||
+        p.ng != 3 || p.bc1 != HAMR_BC_OUTFLOW || p.bc2 != HAMR_BC_POLE_REFL || !p.ct_upwind)
+        return HAMR_E_ARG;
+    if (mdot_face <= d.ng1 || mdot_face >= d.n1 + d.ng1) return HAMR_E_ARG;
+    if (!ctx->have_geom) return HAMR_E_STATE;
+    hamr_adjoint *a = new hamr_adjoint();
+    a->ctx = ctx;
+    a->ih = mdot_face;
+    const size_t cb = sizeof(double) * d.ks;
+    struct A { double **p; size_t n; } al[] = {
+        {&a->ap, NPR * cb}, {&a->aps, 3 * cb}, {&a->aph, NPR * cb}, {&a->apsh, 3 * cb}, {&a->aU, NPR * cb},
+        {&a->aW, NPR * cb}, {&a->aF1, NPR * cb}, {&a->aF2, NPR * cb}, {&a->aF3, NPR * cb}, {&a->aEc, 4 * cb},
+        {&a->aemf, 4 * cb}, {&a->agam, sizeof(double)}, {&a->J, sizeof(double)}, {&a->p0, NPR * cb},
+        {&a->ps0, 3 * cb}};
+    for (auto &x : al) {
+        if (cudaMalloc((void **)x.p, x.n) != cudaSuccess) {
+            hamr_adjoint_destroy(a);
+            return HAMR_E_NOMEM;
+        }
+        cudaMemsetAsync(*x.p, 0, x.n, ctx->stream);
+    }
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        hamr_adjoint_destroy(a);
+        return HAMR_E_CUDA;
+    }
+    *out = a;
+    return HAMR_OK;
+}
+
+int hamr_adjoint_destroy(hamr_adjoint *a) {
+    if (!a) return HAMR_E_ARG;
+    if (a->ctx && a->ctx->stream) cudaStreamSynchronize(a->ctx->stream);
+    for (double *p : {a->ap, a->aps, a->aph, a->apsh, a->aU, a->aW, a->aF1, a->aF2, a->aF3, a->aEc, a->aemf,
+                      a->agam, a->J, a->p0, a->ps0})
+        cudaFree(p);
+    for (double *p : a->store) cudaFree(p);
+    delete a;
+    return HAMR_OK;
+}
+
+const char *hamr_adjoint_last_error(hamr_adjoint *a) { return a ? a->err.c_str() : "null adjoint"; }
+
+int hamr_adjoint_cotangent(hamr_adjoint *a, double **ap, double **aps, double **agam) {
+    if (!a) return HAMR_E_ARG;
+    if (ap) *ap = a->ap;
+    if (aps) *aps = a->aps;
+    if (agam) *agam = a->agam;
+    return HAMR_OK;
+}
+
+int hamr_adjoint_zero(hamr_adjoint *a) {
+    if (!a) return HAMR_E_ARG;
+    const size_t cb = sizeof(double) * a->ctx->d.ks;
+    cudaStream_t s = a->ctx->stream;
+    ACK(cudaMemsetAsync(a->ap, 0, NPR * cb, s));
+    ACK(cudaMemsetAsync(a->aps, 0, 3 * cb, s));
+    ACK(cudaMemsetAsync(a->aU, 0, NPR * cb, s));
+    ACK(cudaMemsetAsync(a->agam, 0, sizeof(double), s));
+    return HAMR_OK;
+}
+
+int hamr_step_backward(hamr_adjoint *a, double dt, double mdot_weight) {
+    if (!a || !(dt > 0)) return HAMR_E_ARG;
+    return step_backward(a, dt, mdot_weight);
+}
+
+int hamr_mdot_forward(hamr_adjoint *a, int nsteps, const double *dt, double *J) {
+    if (!a || !dt || nsteps < 1) return HAMR_E_ARG;
+    hamr_ctx *ctx = a->ctx;
+    cudaStream_t s = ctx->stream;
+    ACK(cudaMemsetAsync(a->J, 0, sizeof(double), s));
+    int rc = bound_ctx(ctx);
+    for (int n = 0; n < nsteps && rc == HAMR_OK; n++) {
+        if (!(dt[n] > 0)) return HAMR_E_ARG;
+        rc = fixed_step(ctx, dt[n]);
+        if (rc == HAMR_OK)
+            k_mdot_accum<<<nb(ctx->d.n2), BLK, 0, s>>>(ctx->d, ctx->F1, a->ih, dt[n], a->J);
+    }
+    if (rc) return rc;
+    if (J) ACK(cudaMemcpyAsync(J, a->J, sizeof(double), cudaMemcpyDeviceToHost, s));
+    ACK(cudaStreamSynchronize(s));
+    return HAMR_OK;
+}
+
+// Gradient of J = sum_n dt[n] Mdot_n over nsteps fixed-size steps with
+// respect to the initial state (active primitives and face field, before
+// the ghost fill) and the adiabatic index. Checkpoints the state every
+// `every` steps on the forward sweep, and reverses segment by segment: each
+// segment is recomputed from its checkpoint, keeping its per-step inputs,
+// then stepped backwards. grad_p (9 planes) / grad_ps (3 planes) are host
+// arrays in the context's layout (NULL: not copied). The context's state is
+// restored to its initial value on return.
+int hamr_adjoint_run(hamr_adjoint *a, int nsteps, const double *dt, int every, double *J, double *grad_p,
+                     double *grad_ps, double *grad_gam) {
+    if (!a || !dt || nsteps < 1 || every < 1) return HAMR_E_ARG;
+    for (int n = 0; n < nsteps; n++)
+        if (!(dt[n] > 0)) return HAMR_E_ARG;
+    hamr_ctx *ctx = a->ctx;
+    const Dims &d = ctx->d;
+    cudaStream_t s = ctx->stream;
+    const size_t cb = sizeof(double) * d.ks, state = 12 * cb;
+    const int nseg = (nsteps + every - 1) / every;
+    const size_t need = (size_t)nseg + 1 + every;   // checkpoints + initial pre-fill copy + segment states
+    while (a->store.size() < need) {
+        double *p = nullptr;
+        if (cudaMalloc((void **)&p, state) != cudaSuccess) return HAMR_E_NOMEM;
+        a->store.push_back(p);
+    }
+    auto save = [&](double *dst) {
+        cudaMemcpyAsync(dst, ctx->p, NPR * cb, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(dst + NPR * d.ks, ctx->ps, 3 * cb, cudaMemcpyDeviceToDevice, s);
+    };
+    auto load = [&](const double *src) {
+        cudaMemcpyAsync(ctx->p, src, NPR * cb, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(ctx->ps, src + NPR * d.ks, 3 * cb, cudaMemcpyDeviceToDevice, s);
+    };
+    double *initial = a->store[nseg];
+    double **seg = a->store.data() + nseg + 1;
+    save(initial);
+    // forward sweep with checkpoints
+    ACK(cudaMemsetAsync(a->J, 0, sizeof(double), s));
+    int rc = bound_ctx(ctx);
+    for (int n = 0; n < nsteps && rc == HAMR_OK; n++) {
+        if (n % every == 0) save(a->store[n / every]);
+        rc = fixed_step(ctx, dt[n]);
+        if (rc == HAMR_OK) k_mdot_accum<<<nb(d.n2), BLK, 0, s>>>(d, ctx->F1, a->ih, dt[n], a->J);
+    }
+    if (rc) return rc;
+    // reverse sweep
+    if ((rc = hamr_adjoint_zero(a))) return rc;
+    for (int sg = nseg - 1; sg >= 0 && rc == HAMR_OK; sg--) {
+        const int n0 = sg * every, n1 = n0 + every < nsteps ? n0 + every : nsteps;
+        load(a->store[sg]);
+        for (int n = n0; n < n1 && rc == HAMR_OK; n++) {
+            save(seg[n - n0]);
+            if (n + 1 < n1) rc = fixed_step(ctx, dt[n]);
+        }
+        for (int n = n1 - 1; n >= n0 && rc == HAMR_OK; n--) {
+            load(seg[n - n0]);
+            rc = step_backward(a, dt[n], dt[n]);
+        }
+    }
+    if (rc) return rc;
+    // the initial ghost fill, reversed, folds ghost cotangents onto the zones
+    load(a->store[0]);
+    adj_bound(ctx, ctx->p, a->ap, a->aps);
+    ACK(cudaGetLastError());
+    if (J) ACK(cudaMemcpyAsync(J, a->J, sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (grad_p) ACK(cudaMemcpyAsync(grad_p, a->ap, NPR * cb, cudaMemcpyDeviceToHost, s));
+    if (grad_ps) ACK(cudaMemcpyAsync(grad_ps, a->aps, 3 * cb, cudaMemcpyDeviceToHost, s));
+    if (grad_gam) ACK(cudaMemcpyAsync(grad_gam, a->agam, sizeof(double), cudaMemcpyDeviceToHost, s));
+    load(initial);
+    ACK(cudaStreamSynchronize(s));
+    return HAMR_OK;
+}
+
+}  // extern "C"

@@ -1417,3 +1417,4 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
 }
 
 #include "hamr_batch.cuh"
+#include "hamr_adjoint.cuh"

@@ -241,6 +241,44 @@ int hamr_batch_autotune(hamr_batch *b, const double *dt, int reps);
  * tuned time in ms. Any output pointer may be NULL. */
 int hamr_batch_tuning(hamr_batch *b, int *tile, int *grid, int *order, float *ms, int nphases);
 
+/* ---- adjoint ---------------------------------------------------------------
+ * Reverse mode of the FP64 RK2 step (no counterpart in the reference, which
+ * has no derivatives), for axisymmetric blocks: n3 == 1, PPM, Noble 2D
+ * inversion, outflow x1, reflective polar axis, upwinded CT -- the 2-D torus
+ * configuration. Step sizes are held fixed (no derivative through the CFL
+ * choice). The objective is J = sum_n w_n Mdot_n with the accretion rate
+ * through x1 face column `mdot_face` of the full sub-step,
+ * Mdot = -sum_j F1[RHO](mdot_face, j) dx2 dx3 (F1 includes gdet; calc_Mdot,
+ * restart.c:864-903, measures the same flux through a sphere).
+ * The adjoint holds its cotangent arrays on the device, in the context's
+ * layout: ap (9 planes), aps (3 planes), and the accumulated d/d gamma. */
+typedef struct hamr_adjoint hamr_adjoint;
+
+int hamr_adjoint_create(hamr_ctx *ctx, int mdot_face, hamr_adjoint **out);
+int hamr_adjoint_destroy(hamr_adjoint *a);
+const char *hamr_adjoint_last_error(hamr_adjoint *a);
+/* device pointers of the state cotangents (any may be NULL) */
+int hamr_adjoint_cotangent(hamr_adjoint *a, double **ap, double **aps, double **agam);
+int hamr_adjoint_zero(hamr_adjoint *a);
+
+/* C-ABI backward of one RK2 step of size dt. On entry the context holds the
+ * step's input state (with ghosts) and ap/aps the cotangent of its output;
+ * on return ap/aps hold the cotangent of the input (ghost entries included:
+ * they belong to the previous ghost fill), d/d gamma is accumulated, and
+ * mdot_weight * Mdot of this step is part of the objective. The context's
+ * state is unchanged; its intermediate arrays are overwritten. */
+int hamr_step_backward(hamr_adjoint *a, double dt, double mdot_weight);
+
+/* Forward sweep for the objective: ghost fill, then nsteps steps of sizes
+ * dt[n] (weights w_n = dt[n]); J receives the objective; the state advances. */
+int hamr_mdot_forward(hamr_adjoint *a, int nsteps, const double *dt, double *J);
+
+/* Objective and its gradient w.r.t. the initial state (host arrays in the
+ * context's layout, NULL to skip) and gamma, with checkpoints every `every`
+ * steps and recompute; the state is left at its initial value. */
+int hamr_adjoint_run(hamr_adjoint *a, int nsteps, const double *dt, int every, double *J, double *grad_p,
+                     double *grad_ps, double *grad_gam);
+
 #ifdef __cplusplus
 }
 #endif
