@@ -450,6 +450,89 @@ def run_ensemble(args):
     print(json.dumps(out), flush=True)
 
 
+ADJOINT = dict(n=256, nsteps=200, every=20, directions=32, spin=0.9375, rout=40.0, generic=1e-3)
+
+
+def run_adjoint(args):
+    """Adjoint workload: 2-D magnetised torus 256 x 256 (a = 0.9375,
+    beta_min = 100, seeded tie-free perturbations), J = accretion rate through
+    the horizon face column integrated over 200 fixed-size steps; gradient
+    w.r.t. the initial pressure field and gamma by hamr_adjoint_run
+    (checkpoint every 20 steps, recompute), timed against the forward sweep
+    (hamr_mdot_forward), and checked against fourth-order central
+    differences on 32 seeded directions."""
+    import torch
+    from hamr_gamma_wind_b200 import problems
+    from hamr_gamma_wind_b200.api import Adjoint, Block
+    rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return
+    A = ADJOINT
+    pb = problems.fm_torus(A["n"], A["n"], 1, spin=A["spin"], rout=A["rout"], generic=A["generic"])
+    rh = 1.0 + np.sqrt(1.0 - A["spin"] ** 2)
+    faces = np.arange(pb.ng + 1, pb.ng + pb.n1)
+    r = np.exp(np.log(0.9 * rh) + (faces - pb.ng) * pb.dx[0])
+    ih = int(faces[np.argmin(np.abs(r - rh))])
+    dts = np.full(A["nsteps"], 0.2 * min(pb.dx[:2]))
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    blk = Block(**pb.block_kwargs(), stream=ctypes_stream(stream))
+    blk.set_geometry(pb.geo)
+    adj = Adjoint(blk, ih)
+
+    def reset(u=None, p=None):
+        q = pb.p.copy() if p is None else p
+        if u is not None:
+            pb.active(q)[1][:, :, 0] = u
+        blk.upload(q, pb.ps)
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(max(1, args.warmup)):
+        reset(); adj.forward(dts)
+    reset()
+    torch.cuda.synchronize()
+    e0.record(stream); J = adj.forward(dts); e1.record(stream); torch.cuda.synchronize()
+    t_fwd = e0.elapsed_time(e1)
+    reset()
+    adj.gradient(dts, A["every"])   # warm-up
+    reset()
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        e0.record(stream); Jg, gp, gs, gg = adj.gradient(dts, A["every"]); e1.record(stream)
+        torch.cuda.synchronize()
+    t_run = e0.elapsed_time(e1)
+    gu = pb.active(gp)[1][:, :, 0].copy()
+    u0 = pb.active(pb.p)[1][:, :, 0].copy()
+
+    def Ju(u):
+        reset(u)
+        return adj.forward(dts)
+    rng = np.random.default_rng(2025)
+    errs = []
+    for _ in range(A["directions"]):
+        v = rng.standard_normal(u0.shape) * u0
+        e = 1e-6
+        fd = (-Ju(u0 + 2 * e * v) + 8 * Ju(u0 + e * v) - 8 * Ju(u0 - e * v) + Ju(u0 - 2 * e * v)) / (12 * e)
+        errs.append(abs(float((gu * v).sum()) - fd) / max(abs(fd), 1e-300))
+    adj.close()
+    blk.close()
+    n = A["nsteps"]
+    out = {"metric": "adjoint/forward time", "value": t_run / t_fwd, "unit": "x", "n_gpus": 1, "steps": n,
+           "warmup": args.warmup, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic",
+           "config": {"workload": f"adjoint: 2-D FM torus {A['n']}x{A['n']} (a={A['spin']}, beta_min=100), "
+                                  f"J = sum_n dt Mdot through x1 face {ih}, {n} steps, checkpoint every {A['every']}",
+                      "zones": A["n"] * A["n"]},
+           "forward_ms_per_step": t_fwd / n, "gradient_ms_per_step": t_run / n,
+           "backward_over_forward": (t_run - t_fwd) / t_fwd,
+           "J": J, "J_from_gradient_run": Jg, "dJ_dgamma": gg,
+           "fd_check": {"directions": A["directions"], "order": 4, "rel_step": 1e-6, "max_rel_err": max(errs),
+                        "median_rel_err": float(np.median(errs))},
+           "clocks": clk.summary(), "gpu_launches": None}
+    print(json.dumps(out), flush=True)
+
+
 def ctypes_stream(stream):
     import ctypes
     return ctypes.c_void_p(stream.cuda_stream)
@@ -461,7 +544,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c3", choices=list(WORKLOADS) + ["c4"])
+    ap.add_argument("--workload", default="c3", choices=list(WORKLOADS) + ["c4", "c5"])
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
     ap.add_argument("--accuracy", type=int, default=0,
                     help="instead of timing: per-field L1 difference of mixed vs FP64 after this many steps")
@@ -476,6 +559,8 @@ def main():
         run_accuracy(args)
     elif args.workload == "c4":
         run_ensemble(args)
+    elif args.workload == "c5":
+        run_adjoint(args)
     else:
         run_ours(args)
 

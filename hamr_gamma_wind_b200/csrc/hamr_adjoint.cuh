@@ -275,19 +275,25 @@ __global__ void k_adj_divergence(const Dims d, const double *__restrict__ aW, do
 }
 
 // inversion reversed by the implicit-function theorem (active zones).
-// ap: cotangent of the inversion's output (consumed); apg: of its initial
-// guess (KTOT passes through; where no solver converged the hydrodynamic
-// primitives are the guess); aW: of the conserved input (9 planes).
+// The solution p of the inversion satisfies G(p; W, B, gamma) = 0 with, over
+// the five hydrodynamic primitives, the rows mass, energy and momenta
+// (U(p) - W, when the Noble 2D solve converged) or the energy row replaced by
+// the entropy relation u = K rho^gamma / (gamma - 1), K = W_KTOT / W_RHO
+// (when an entropy fallback produced p). Then W_bar = -(dG/dW)^T x, with
+// (dG/dp)^T x = p_bar, and likewise for the field and gamma. Where no solver
+// converged, the hydrodynamic primitives are the guess's. ap: cotangent of
+// the output (consumed); apg: of the guess; aW: of the conserved input.
 __global__ void __launch_bounds__(BLK) k_adj_invert(const Dims d, const Geom m, const double *__restrict__ pout,
-                                                     const int *__restrict__ pflag, double *ap, double *apg,
-                                                     double *aW, double *agam) {
+                                                     const double *__restrict__ pg, const double *__restrict__ W7,
+                                                     const double *__restrict__ psf, const int *__restrict__ pflag,
+                                                     double *ap, double *apg, double *aW, double *agam) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     double gsum = 0.;
     if (t < (long)d.n1 * d.n2 * d.n3) {
         const int z = d.ng3 + (int)(t % d.n3);
         const int j = d.ng2 + (int)((t / d.n3) % d.n2);
         const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
-        const long c = cix(d, i, j, z), ks = d.ks;
+        const long c = cix(d, i, j, z), gi = gix(d, i, j), ks = d.ks;
         double pb[NPR];
         bool any = false;
         for (int k = 0; k < NPR; k++) { pb[k] = ap[k * ks + c]; ap[k * ks + c] = 0.; any |= pb[k] != 0.; }
@@ -299,6 +305,18 @@ __global__ void __launch_bounds__(BLK) k_adj_invert(const Dims d, const Geom m, 
             if (pflag[c] != 0) {
                 for (int k = 0; k < 5; k++) apg[k * ks + c] += pb[k];
             } else {
+                // which solver produced p: redo the primary solve on the same input
+                double U[NPR], pf[NPR];
+                U[RHO] = W7[0 * ks + c];
+                U[UU] = W7[1 * ks + c];
+                U[U1] = W7[2 * ks + c];
+                U[U2] = W7[3 * ks + c];
+                U[U3] = W7[4 * ks + c];
+                U[KTOT] = W7[5 * ks + c];
+                U[B3] = W7[6 * ks + c];
+                face_average_b(d, m, psf, i, j, c, gi, U);
+                for (int k = 0; k < NPR; k++) pf[k] = pg[k * ks + c];
+                const bool entropy_row = utoprim_2d(d.gam, U, g0.gcov, g0.gcon, g0.g, pf) != 0;
                 constexpr int N = ADJ_NP + 1;
                 Geo<Dual<N>> gm;
                 geo_const(g0, gm);
@@ -308,13 +326,20 @@ __global__ void __launch_bounds__(BLK) k_adj_invert(const Dims d, const Geom m, 
                 seed_state(pr, d.gam, 0, pd, gd);
                 State<Dual<N>> q;
                 get_state(pd, gm, q);
-                Dual<N> Ud[NPR], vd;
-                primtoflux(gd, pd, q, 0, gm, entropy(gd, pd), Ud, &vd, &vd);
-                // solve J5^T x = pb[0..4], J5[r][s] = dU_r/dp_s, by Gaussian
-                // elimination with partial pivoting on A = J5^T
+                Dual<N> G[NPR], vd;
+                primtoflux(gd, pd, q, 0, gm, entropy(gd, pd), G, &vd, &vd);
+                const double K = U[KTOT] / U[RHO];
+                double rg = 0.;   // rho^gamma / (gamma - 1) at the solution
+                if (entropy_row) {
+                    // u - K rho^gamma / (gamma - 1), K held (it is data)
+                    const Dual<N> rgd = d_pow(pd[RHO], gd) / (gd - 1.);
+                    G[UU] = pd[UU] - K * rgd;
+                    rg = rgd.v;
+                }
+                // (dG/dp5)^T x = pb[0..4], Gaussian elimination with partial pivoting
                 double A[5][6];
                 for (int r = 0; r < 5; r++) {
-                    for (int s = 0; s < 5; s++) A[r][s] = Ud[s].d[r];
+                    for (int s2 = 0; s2 < 5; s2++) A[r][s2] = G[s2].d[r];
                     A[r][5] = pb[r];
                 }
                 bool ok = true;
@@ -324,27 +349,35 @@ __global__ void __launch_bounds__(BLK) k_adj_invert(const Dims d, const Geom m, 
                         if (fabs(A[r][col]) > fabs(A[piv][col])) piv = r;
                     if (!(fabs(A[piv][col]) > 0.)) { ok = false; break; }
                     if (piv != col)
-                        for (int s = 0; s < 6; s++) { const double tmp = A[col][s]; A[col][s] = A[piv][s]; A[piv][s] = tmp; }
+                        for (int s2 = 0; s2 < 6; s2++) { const double tmp = A[col][s2]; A[col][s2] = A[piv][s2]; A[piv][s2] = tmp; }
                     for (int r = col + 1; r < 5; r++) {
                         const double f = A[r][col] / A[col][col];
-                        for (int s = col; s < 6; s++) A[r][s] -= f * A[col][s];
+                        for (int s2 = col; s2 < 6; s2++) A[r][s2] -= f * A[col][s2];
                     }
                 }
                 if (ok) {
                     double x[5];
                     for (int r = 4; r >= 0; r--) {
                         double v = A[r][5];
-                        for (int s = r + 1; s < 5; s++) v -= A[r][s] * x[s];
+                        for (int s2 = r + 1; s2 < 5; s2++) v -= A[r][s2] * x[s2];
                         x[r] = v / A[r][r];
                     }
-                    for (int r = 0; r < 5; r++) aW[r * ks + c] += x[r];
-                    // field: p[B] = U[B]/gdet also moves the hydro solution
+                    // -(dG/dW)^T x
+                    aW[RHO * ks + c] += x[RHO];
+                    for (int r = U1; r <= U3; r++) aW[r * ks + c] += x[r];
+                    if (entropy_row) {
+                        aW[KTOT * ks + c] += x[UU] * rg / U[RHO];
+                        aW[RHO * ks + c] -= x[UU] * rg * U[KTOT] / (U[RHO] * U[RHO]);
+                    } else {
+                        aW[UU * ks + c] += x[UU];
+                    }
+                    // the field: p[B] = U[B]/gdet also moves the hydro solution
                     for (int b = 0; b < 3; b++) {
                         double v = 0.;
-                        for (int r = 0; r < 5; r++) v += x[r] * Ud[r].d[B1 + b];
+                        for (int r = 0; r < 5; r++) v += x[r] * G[r].d[B1 + b];
                         aW[(B1 + b) * ks + c] -= v / g0.g;
                     }
-                    for (int r = 0; r < 5; r++) gsum -= x[r] * Ud[r].d[ADJ_NP];
+                    for (int r = 0; r < 5; r++) gsum -= x[r] * G[r].d[ADJ_NP];
                 }
             }
         }
@@ -751,7 +784,8 @@ int adj_stage(hamr_adjoint *a, int full, double dt, double mdot_coef) {
     ACK(cudaMemsetAsync(a->aEc, 0, 4 * sizeof(double) * ks, s));
     // ghost fill of the output, then the inversion (p_out <- W, guess pin)
     adj_bound(ctx, pout, apout, apsout);
-    k_adj_invert<<<nb(nz), BLK, 0, s>>>(d, m, pout, ctx->pflag, apout, apin, a->aW, a->agam);
+    k_adj_invert<<<nb(nz), BLK, 0, s>>>(d, m, pout, pin, ctx->W, apsout == a->aps ? ctx->ps : ctx->psh,
+                                        ctx->pflag, apout, apin, a->aW, a->agam);
     // U[B1], U[B2] from the updated faces
     k_adj_face_average<<<nb(nedge), BLK, 0, s>>>(d, m, a->aW, apsout);
     // update: U^n (cache), source at pin, flux divergence (+ objective)

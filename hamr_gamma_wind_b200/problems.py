@@ -177,12 +177,18 @@ def _bsq(P, gcov, gcon):
 
 
 def fm_torus(n1, n2, n3, spin=0.9375, rin=6.0, rmax=12.0, gam=13.0 / 9.0, kappa=1.e-3, beta=100.0,
-             rout=None, seed=12345, noise=0.04, rho_atm=1.e-14, u_atm=1.e-16, cour=0.8, ng=3) -> Problem:
+             rout=None, seed=12345, noise=0.04, rho_atm=1.e-14, u_atm=1.e-16, cour=0.8, ng=3,
+             generic=0.0) -> Problem:
     """Magnetised Fishbone-Moncrief torus around a Kerr hole in the reference's
     code coordinates. n3 > 1: transmissive poles; n3 == 1: axisymmetric with
     reflective poles. The atmosphere is the reference's 1e-7*RHOMIN / 1e-7*UUMIN
     (init_torus.c:211-212), also divided by the density maximum. ng: ghost
-    layers (3; 2 suits the linear MC reconstruction)."""
+    layers (3; 2 suits the linear MC reconstruction). generic > 0 removes the
+    exact ties of this state (flat atmosphere, equatorial mirror symmetry,
+    zero velocities and field outside the torus), at which the limiters and
+    upwind switches are not differentiable: seeded relative noise of that size
+    on rho, u and the velocities, a power-law atmosphere, and a weak seeded
+    field everywhere (vector potential scaled with sqrt(rho))."""
     if rout is None:
         rout = 4.0 * rmax * 2.0
     startx, dx = ks_grid(n1, n2, n3, spin, rout)
@@ -219,8 +225,9 @@ def fm_torus(n1, n2, n3, spin=0.9375, rin=6.0, rmax=12.0, gam=13.0 / 9.0, kappa=
     lnh = np.where(r >= rin, lnh, 1.0)
     inside = (lnh >= 0.) & (r >= rin)
     hm1 = np.where(inside, np.exp(np.where(inside, lnh, 0.0)) - 1., 0.)
-    rho = np.where(inside, (np.maximum(hm1, 0.) * (gam - 1.) / (kappa * gam)) ** (1. / (gam - 1.)), rho_atm)
-    u = np.where(inside, kappa * rho ** gam / (gam - 1.), u_atm)
+    ratm, uatm = (rho_atm * (r / rin) ** -1.5, u_atm * (r / rin) ** -2.5) if generic > 0 else (rho_atm, u_atm)
+    rho = np.where(inside, (np.maximum(hm1, 0.) * (gam - 1.) / (kappa * gam)) ** (1. / (gam - 1.)), ratm)
+    u = np.where(inside, kappa * rho ** gam / (gam - 1.), uatm)
     # BL u^phi of the torus, then u^t from normalisation; u^r = u^theta = 0
     with np.errstate(invalid="ignore", divide="ignore"):
         expm2chi = SS * SS * DD / (AA * AA * sth * sth)
@@ -260,12 +267,20 @@ def fm_torus(n1, n2, n3, spin=0.9375, rin=6.0, rmax=12.0, gam=13.0 / 9.0, kappa=
     Pa[U1] = np.where(inside, util1, 0.0)[:, :, None]
     Pa[U2] = np.where(inside, util2, 0.0)[:, :, None]
     Pa[U3] = np.where(inside, util3, 0.0)[:, :, None]
-    Pa[KTOT] = (gam - 1.) * u3 * rho3 ** (-gam)
+    if generic > 0:
+        grng = np.random.default_rng(seed + 1)
+        Pa[RHO] *= 1. + generic * grng.standard_normal(shape3)
+        Pa[UU] *= 1. + generic * grng.standard_normal(shape3)
+        for k in (U1, U2, U3):
+            Pa[k] += generic * 1e-2 * grng.standard_normal(shape3)
+    Pa[KTOT] = (gam - 1.) * Pa[UU] * Pa[RHO] ** (-gam)
     # single poloidal loop: A_phi at zone corners from the corner-averaged density
     rho2 = rho / rhomax
     rpad = np.pad(rho2, 1, mode="edge")
     rho_av = 0.25 * (rpad[1:, 1:] + rpad[:-1, 1:] + rpad[1:, :-1] + rpad[:-1, :-1])   # (n1+1, n2+1)
     A = np.maximum(rho_av - 0.2, 0.0)
+    if generic > 0:
+        A = A + generic * A.max() * np.sqrt(np.maximum(rho_av, 0.)) * grng.standard_normal(A.shape)
     gdf1 = _geo_plane(geo, gs, g1, g2, "gdet", 0, FACE1)[ng:ng + n1 + 1, act2]
     gdf2 = _geo_plane(geo, gs, g1, g2, "gdet", 0, FACE2)[act1, ng:ng + n2 + 1]
     gdc = _geo_plane(geo, gs, g1, g2, "gdet", 0, CENT)[act1, act2]

@@ -20,8 +20,9 @@ def horizon_face(pb, spin):
 
 
 class TorusRun:
-    def __init__(self, n1=48, n2=48, nsteps=10, spin=0.9375, every=4, cfl=0.2, rout=40.0, strict=False):
-        self.pb = problems.fm_torus(n1, n2, 1, spin=spin, rout=rout)
+    def __init__(self, n1=48, n2=48, nsteps=10, spin=0.9375, every=4, cfl=0.2, rout=40.0, strict=False,
+                 generic=1e-3):
+        self.pb = problems.fm_torus(n1, n2, 1, spin=spin, rout=rout, generic=generic)
         self.ih = horizon_face(self.pb, spin)
         self.dts = np.full(nsteps, cfl * min(self.pb.dx[:2]))
         self.every = every
