@@ -459,8 +459,8 @@ def run_adjoint(args):
     the horizon face column integrated over 200 fixed-size steps; gradient
     w.r.t. the initial pressure field and gamma by hamr_adjoint_run
     (checkpoint every 20 steps, recompute), timed against the forward sweep
-    (hamr_mdot_forward), and checked against fourth-order central
-    differences on 32 seeded directions."""
+    (hamr_mdot_forward), and checked against central differences (relative
+    step 1e-8) on 32 seeded directions."""
     import torch
     from hamr_gamma_wind_b200 import problems
     from hamr_gamma_wind_b200.api import Adjoint, Block
@@ -512,8 +512,8 @@ def run_adjoint(args):
     errs = []
     for _ in range(A["directions"]):
         v = rng.standard_normal(u0.shape) * u0
-        e = 1e-6
-        fd = (-Ju(u0 + 2 * e * v) + 8 * Ju(u0 + e * v) - 8 * Ju(u0 - e * v) + Ju(u0 - 2 * e * v)) / (12 * e)
+        e = 1e-8   # the discrete objective has limiter/upwind kinks closer than 1e-6 apart
+        fd = (Ju(u0 + e * v) - Ju(u0 - e * v)) / (2 * e)
         errs.append(abs(float((gu * v).sum()) - fd) / max(abs(fd), 1e-300))
     adj.close()
     blk.close()
@@ -527,7 +527,7 @@ def run_adjoint(args):
            "forward_ms_per_step": t_fwd / n, "gradient_ms_per_step": t_run / n,
            "backward_over_forward": (t_run - t_fwd) / t_fwd,
            "J": J, "J_from_gradient_run": Jg, "dJ_dgamma": gg,
-           "fd_check": {"directions": A["directions"], "order": 4, "rel_step": 1e-6, "max_rel_err": max(errs),
+           "fd_check": {"directions": A["directions"], "order": 2, "rel_step": 1e-8, "max_rel_err": max(errs),
                         "median_rel_err": float(np.median(errs))},
            "clocks": clk.summary(), "gpu_launches": None}
     print(json.dumps(out), flush=True)

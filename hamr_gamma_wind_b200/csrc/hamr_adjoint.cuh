@@ -733,6 +733,9 @@ struct hamr_adjoint {
     double *agam = nullptr, *J = nullptr;   // 1 double each
     double *p0 = nullptr, *ps0 = nullptr;   // the step's input state while it is reversed
     std::vector<double *> store;            // checkpoints and segment states (12 planes each)
+    // captured graphs of one forward step (with the objective) and of one
+    // reversed step, per step size
+    std::map<double, cudaGraphExec_t> fwd_graph, bwd_graph;
 };
 
 namespace {
@@ -833,6 +836,42 @@ int step_backward(hamr_adjoint *a, double dt, double w) {
     return HAMR_OK;
 }
 
+// forward step + objective term, and reversed step, replayed from graphs
+// captured once per step size (the step is launch-bound at these sizes)
+template <class F>
+int graph_run(hamr_adjoint *a, std::map<double, cudaGraphExec_t> &cache, double dt, F body) {
+    cudaStream_t s = a->ctx->stream;
+    auto it = cache.find(dt);
+    if (it == cache.end()) {
+        cudaGraph_t g;
+        ACK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        const int rc = body();
+        cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (rc) return rc;
+        if (e != cudaSuccess) return afail(a, e, "cudaStreamEndCapture");
+        cudaGraphExec_t x;
+        e = cudaGraphInstantiate(&x, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return afail(a, e, "cudaGraphInstantiate");
+        it = cache.emplace(dt, x).first;
+    }
+    ACK(cudaGraphLaunch(it->second, s));
+    return HAMR_OK;
+}
+
+int fwd_step(hamr_adjoint *a, double dt) {
+    return graph_run(a, a->fwd_graph, dt, [&]() -> int {
+        const int rc = fixed_step(a->ctx, dt);
+        if (rc) return rc;
+        k_mdot_accum<<<nb(a->ctx->d.n2), BLK, 0, a->ctx->stream>>>(a->ctx->d, a->ctx->F1, a->ih, dt, a->J);
+        return cudaGetLastError() == cudaSuccess ? HAMR_OK : HAMR_E_CUDA;
+    });
+}
+
+int bwd_step(hamr_adjoint *a, double dt) {
+    return graph_run(a, a->bwd_graph, dt, [&]() -> int { return step_backward(a, dt, dt); });
+}
+
 int bound_ctx(hamr_ctx *ctx) {
     const Dims &d = ctx->d;
     cudaStream_t s = ctx->stream;
@@ -889,6 +928,8 @@ int hamr_adjoint_destroy(hamr_adjoint *a) {
                       a->agam, a->J, a->p0, a->ps0})
         cudaFree(p);
     for (double *p : a->store) cudaFree(p);
+    for (auto &kv : a->fwd_graph) cudaGraphExecDestroy(kv.second);
+    for (auto &kv : a->bwd_graph) cudaGraphExecDestroy(kv.second);
     delete a;
     return HAMR_OK;
 }
@@ -927,9 +968,7 @@ int hamr_mdot_forward(hamr_adjoint *a, int nsteps, const double *dt, double *J) 
     int rc = bound_ctx(ctx);
     for (int n = 0; n < nsteps && rc == HAMR_OK; n++) {
         if (!(dt[n] > 0)) return HAMR_E_ARG;
-        rc = fixed_step(ctx, dt[n]);
-        if (rc == HAMR_OK)
-            k_mdot_accum<<<nb(ctx->d.n2), BLK, 0, s>>>(ctx->d, ctx->F1, a->ih, dt[n], a->J);
+        rc = fwd_step(a, dt[n]);
     }
     if (rc) return rc;
     if (J) ACK(cudaMemcpyAsync(J, a->J, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -977,10 +1016,12 @@ int hamr_adjoint_run(hamr_adjoint *a, int nsteps, const double *dt, int every, d
     int rc = bound_ctx(ctx);
     for (int n = 0; n < nsteps && rc == HAMR_OK; n++) {
         if (n % every == 0) save(a->store[n / every]);
-        rc = fixed_step(ctx, dt[n]);
-        if (rc == HAMR_OK) k_mdot_accum<<<nb(d.n2), BLK, 0, s>>>(d, ctx->F1, a->ih, dt[n], a->J);
+        rc = fwd_step(a, dt[n]);
     }
     if (rc) return rc;
+    double Jval = 0.;
+    ACK(cudaMemcpyAsync(&Jval, a->J, sizeof(double), cudaMemcpyDeviceToHost, s));
+    ACK(cudaStreamSynchronize(s));
     // reverse sweep
     if ((rc = hamr_adjoint_zero(a))) return rc;
     for (int sg = nseg - 1; sg >= 0 && rc == HAMR_OK; sg--) {
@@ -988,11 +1029,11 @@ int hamr_adjoint_run(hamr_adjoint *a, int nsteps, const double *dt, int every, d
         load(a->store[sg]);
         for (int n = n0; n < n1 && rc == HAMR_OK; n++) {
             save(seg[n - n0]);
-            if (n + 1 < n1) rc = fixed_step(ctx, dt[n]);
+            if (n + 1 < n1) rc = fwd_step(a, dt[n]);   // (adds to J's device copy: the value was taken above)
         }
         for (int n = n1 - 1; n >= n0 && rc == HAMR_OK; n--) {
             load(seg[n - n0]);
-            rc = step_backward(a, dt[n], dt[n]);
+            rc = bwd_step(a, dt[n]);
         }
     }
     if (rc) return rc;
@@ -1000,7 +1041,7 @@ int hamr_adjoint_run(hamr_adjoint *a, int nsteps, const double *dt, int every, d
     load(a->store[0]);
     adj_bound(ctx, ctx->p, a->ap, a->aps);
     ACK(cudaGetLastError());
-    if (J) ACK(cudaMemcpyAsync(J, a->J, sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (J) *J = Jval;
     if (grad_p) ACK(cudaMemcpyAsync(grad_p, a->ap, NPR * cb, cudaMemcpyDeviceToHost, s));
     if (grad_ps) ACK(cudaMemcpyAsync(grad_ps, a->aps, 3 * cb, cudaMemcpyDeviceToHost, s));
     if (grad_gam) ACK(cudaMemcpyAsync(grad_gam, a->agam, sizeof(double), cudaMemcpyDeviceToHost, s));
