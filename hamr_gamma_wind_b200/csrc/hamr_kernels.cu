@@ -1301,7 +1301,7 @@ int hamr_divb_max(hamr_ctx *ctx, double *out) {
 // step -- half-step state, cached conserved variables, face fluxes, EMFs,
 // inversion flags, CFL minima -- live in file-scope device arrays sized for at
 // most HAMR_NOALLOC_MAX_CELLS zones per plane. Every GPU that loads the library
-// holds these arrays (about 15 MB) until the process exits; every call shares
+// holds these arrays (about 17 MB) until the process exits; every call shares
 // them, so calls that overlap on the GPU race.
 namespace {
 

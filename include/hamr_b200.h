@@ -158,7 +158,7 @@ int hamr_device_state(hamr_ctx *ctx, double **p, double **ps, double **ph, doubl
  * device memory (layout as above; p, ps advanced in place; gcov/gcon/gdet/conn
  * read only). Every intermediate array lives in static device arrays inside
  * this library, sized for at most HAMR_NOALLOC_MAX_CELLS zones per plane
- * (ksize, ghosts and padding included; about 15 MB held on every GPU that
+ * (ksize, ghosts and padding included; about 17 MB held on every GPU that
  * loads the library, until the process exits). Larger blocks are rejected with
  * HAMR_E_ARG before any device work. Nothing is allocated: no cudaMalloc,
  * cudaFree, stream or event creation.
