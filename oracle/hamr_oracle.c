@@ -229,6 +229,268 @@ void ho_primtoflux(double gam, const double *pr, const double *gcov10, const dou
     primtoflux(gam, pr, &q, dir, &gm, flux, vmax, vmin);
 }
 
+/* ----------------------------------------------------------------- HLLC -- */
+static int sym(int a, int b) {
+    static const int t[4][4] = {{0, 1, 2, 3}, {1, 4, 5, 6}, {2, 5, 7, 8}, {3, 6, 8, 9}};
+    return t[a][b];
+}
+
+/* Orthonormal frame of a face of direction dir (set_Mud, hllc.c:20-164):
+ * Mud[a][b] and its inverse Mi, from the face metric. With (d, e, f) the
+ * cyclic order starting at dir, every entry follows the reference's
+ * expression for that direction. */
+void ho_set_mud(const double *gcov10, const double *gcon10, int dir, double Mud[4][4], double Mi[4][4]) {
+    const int d = dir, e = dir % 3 + 1, f = (dir + 1) % 3 + 1;
+#define GU(a, b) gcon10[sym(a, b)]
+#define GD(a, b) gcov10[sym(a, b)]
+    double A = -pow(-GU(0, 0), -0.5);
+    double B = pow((GU(0, 0)) * (GU(0, 0) * GU(d, d) - GU(0, d) * GU(0, d)), -0.5);
+    double C = pow(GD(f, f), -0.5);
+    double D = pow((GD(f, f)) * (GD(e, e) * GD(f, f) - GD(e, f) * GD(e, f)), -0.5);
+    for (int a = 0; a < 4; a++)
+        for (int b = 0; b < 4; b++) Mud[a][b] = Mi[a][b] = 0.;
+    Mud[0][0] = A * GU(0, 0);
+    Mud[d][0] = A * GU(0, d);
+    Mud[d][d] = B * (GU(0, d) * GU(0, d) - GU(0, 0) * GU(d, d));
+    Mud[e][0] = A * GU(0, e);
+    Mud[e][d] = B * (GU(0, d) * GU(0, e) - GU(0, 0) * GU(d, e));
+    Mud[e][e] = D * GD(f, f);
+    Mud[f][0] = A * GU(0, f);
+    Mud[f][d] = B * (GU(0, d) * GU(0, f) - GU(0, 0) * GU(d, f));
+    Mud[f][e] = -D * GD(e, f);
+    Mud[f][f] = C;
+    double E = GU(0, d) * GU(d, e) - GU(d, d) * GU(0, e);
+    double F = GU(0, d) * GU(0, e) - GU(0, 0) * GU(d, e);
+    double G = GU(0, d) * GU(d, f) - GU(d, d) * GU(0, f);
+    double H = GU(0, d) * GU(0, f) - GU(0, 0) * GU(d, f);
+    Mi[0][0] = -A;
+    Mi[d][0] = B * GU(0, d);
+    Mi[d][d] = -B * GU(0, 0);
+    Mi[e][0] = B * B * E * GU(0, 0) / (D * GD(f, f));
+    Mi[e][d] = B * B * F * GU(0, 0) / (D * GD(f, f));
+    Mi[e][e] = 1. / (D * GD(f, f));
+    Mi[f][0] = (B * B / C) * GU(0, 0) * (G + E * GD(e, f) / GD(f, f));
+    Mi[f][d] = (B * B / C) * GU(0, 0) * (H + F * GD(e, f) / GD(f, f));
+    Mi[f][e] = (1. / C) * GD(e, f) / GD(f, f);
+    Mi[f][f] = 1. / C;
+#undef GU
+#undef GD
+}
+
+/* fluxes in the orthonormal frame (primtoflux_FT, GPU_hllc.h:903-1010) */
+static void primtoflux_ft(double gam, const double *pr, const double *ucon, const double *bcon, int dir,
+                          double *flux) {
+    flux[RHO] = pr[RHO] * ucon[dir];
+    double P = (gam - 1.) * pr[UU];
+    double w = P + pr[RHO] + pr[UU];
+    double bsq = -bcon[0] * bcon[0] + bcon[1] * bcon[1] + bcon[2] * bcon[2] + bcon[3] * bcon[3];
+    double eta = w + bsq;
+    double ptot = P + 0.5 * bsq;
+    flux[UU] = -eta * ucon[dir] * ucon[0] + ptot * (double)(dir == 0) + bcon[dir] * bcon[0];
+    for (int j = 1; j < 4; j++) flux[UU + j] = eta * ucon[dir] * ucon[j] + ptot * (double)(dir == j) - bcon[dir] * bcon[j];
+    for (int k = B1; k <= B3; k++) flux[k] = bcon[k - 4] * ucon[dir] - bcon[dir] * ucon[k - 4];
+    flux[KTOT] = flux[RHO] * P * pow(pr[RHO], -gam);
+}
+
+/* fast speeds in the orthonormal frame (vchar_FT, GPU_hllc.h:1012-1111) */
+static void vchar_ft(double gam, const double *pr, const double *ucon, const double *bcon, int dir, double *vmax,
+                     double *vmin) {
+    double bsq = -bcon[0] * bcon[0] + bcon[1] * bcon[1] + bcon[2] * bcon[2] + bcon[3] * bcon[3];
+    double EF = pr[RHO] + gam * pr[UU];
+    double cs2 = gam * (gam - 1.) * pr[UU] / EF;
+    double EE = bsq + EF;
+    double va2 = bsq / EE;
+    double cms2 = cs2 + va2 - cs2 * va2;
+    if (cms2 < 0.) cms2 = SMALL;
+    if (cms2 > 1.) cms2 = 1.;
+    double Asq = 1., Bsq = -1.;
+    double Au = ucon[dir], Bu = ucon[0];
+    double Au2 = Au * Au, Bu2 = Bu * Bu, AuBu = Au * Bu;
+    double A = Bu2 - (Bsq + Bu2) * cms2;
+    double B = 2. * (AuBu - (AuBu) * cms2);
+    double C = Au2 - (Asq + Au2) * cms2;
+    double discr = B * B - 4. * A * C;
+    if ((discr < 0.0) && (discr > -1.e-10)) discr = 0.0;
+    else if (discr < -1.e-10) discr = 0.;
+    discr = sqrt(discr);
+    double vp = -(-B + discr) / (2. * A);
+    double vm = -(-B - discr) / (2. * A);
+    if (vp > vm) { *vmax = vp; *vmin = vm; }
+    else { *vmax = vm; *vmin = vp; }
+}
+
+/* HLLC star states, hydrodynamic case (calc_HLLC_hydro, GPU_hllc.h:250-315) */
+static void hllc_hydro(int dir, const double *lu, const double *ru, double iv, double cmin, double cmax,
+                       double FT[2][NPR], double FH[2][NPR], const double *Fl, const double *Fr, const double *Ul,
+                       const double *Ur) {
+    const int U_1 = UU + dir, U_2 = UU + dir % 3 + 1, U_3 = UU + (dir + 1) % 3 + 1;
+    const int B_1 = B1 + dir - 1, B_2 = B1 + dir % 3, B_3 = B1 + (dir + 1) % 3;
+    int fail = 0;
+    double A = -FH[1][UU];
+    double B = -FH[1][U_1] + FH[0][UU];
+    double C = FH[0][U_1];
+    double D = B * B - 4. * A * C;
+    double vcon = (-B - sqrt(D)) / (2. * A);
+    double ptot = -(-FH[1][UU]) * vcon + FH[1][U_1];
+    if (!(fabs(ptot) > 0.) || (vcon < cmin) || (vcon > cmax) || !(fabs(vcon) > 0.)) fail = 1;
+    if (cmax > iv && vcon <= iv && fail == 0) {
+        double s = (cmax - ru[dir] / ru[0]) / (cmax - vcon + SMALL);
+        FT[0][RHO] = s * Ur[RHO];
+        FT[0][UU] = (cmax * Ur[UU] + Ur[U_1] - ptot * vcon) / (cmax - vcon + SMALL);
+        FT[0][U_1] = (-FT[0][UU] + ptot) * vcon;
+        FT[0][U_2] = s * Ur[U_2];
+        FT[0][U_3] = s * Ur[U_3];
+        FT[0][B_1] = FH[0][B_1];
+        FT[0][B_2] = s * Ur[B_2];
+        FT[0][B_3] = s * Ur[B_3];
+        FT[0][KTOT] = s * Ur[KTOT];
+        for (int k = 0; k < NPR; k++) FT[1][k] = (Fr[k] + cmax * (FT[0][k] - Ur[k]));
+    } else if (cmin < iv && vcon >= iv && fail == 0) {
+        double s = (cmin - lu[dir] / lu[0]) / (cmin - vcon + SMALL);
+        FT[0][RHO] = s * Ul[RHO];
+        FT[0][UU] = (cmin * Ul[UU] + Ul[U_1] - ptot * vcon) / (cmin - vcon + SMALL);
+        FT[0][U_1] = (-FT[0][UU] + ptot) * vcon;
+        FT[0][U_2] = s * Ul[U_2];
+        FT[0][U_3] = s * Ul[U_3];
+        FT[0][B_1] = FH[0][B_1];
+        FT[0][B_2] = s * Ul[B_2];
+        FT[0][B_3] = s * Ul[B_3];
+        FT[0][KTOT] = s * Ul[KTOT];
+        for (int k = 0; k < NPR; k++) FT[1][k] = (Fl[k] + cmin * (FT[0][k] - Ul[k]));
+    } else {
+        for (int k = 0; k < NPR; k++) { FT[0][k] = FH[0][k]; FT[1][k] = FH[1][k]; }
+    }
+}
+
+/* HLLC star states, magnetised case (calc_HLLC, GPU_hllc.h:317-396) */
+static void hllc_mhd(int dir, const double *lu, const double *ru, double iv, double cmin, double cmax,
+                     double FT[2][NPR], double FH[2][NPR], const double *Fl, const double *Fr, const double *Ul,
+                     const double *Ur) {
+    const int G_1 = dir, G_2 = dir % 3 + 1, G_3 = (dir + 1) % 3 + 1;
+    const int U_1 = UU + G_1, U_2 = UU + G_2, U_3 = UU + G_3;
+    const int B_1 = B1 + G_1 - 1, B_2 = B1 + G_2 - 1, B_3 = B1 + G_3 - 1;
+    double vcon[4];
+    int fail = 0;
+    double A = -FH[1][UU] - (FH[0][B_2] * FH[1][B_2] + FH[0][B_3] * FH[1][B_3]);
+    double B = -FH[1][U_1] + FH[0][UU] + (FH[0][B_2] * FH[0][B_2] + FH[0][B_3] * FH[0][B_3]) +
+               (FH[1][B_2] * FH[1][B_2] + FH[1][B_3] * FH[1][B_3]);
+    double C = FH[0][U_1] - (FH[0][B_2] * FH[1][B_2] + FH[0][B_3] * FH[1][B_3]);
+    double D = B * B - 4. * A * C;
+    vcon[G_1] = (-B - sqrt(D)) / (2. * A);
+    vcon[G_2] = (FH[0][B_2] * vcon[G_1] - FH[1][B_2]) / FH[0][B_1];
+    vcon[G_3] = (FH[0][B_3] * vcon[G_1] - FH[1][B_3]) / FH[0][B_1];
+    double gammasq = 1. / (1. - (vcon[1] * vcon[1] + vcon[2] * vcon[2] + vcon[3] * vcon[3]));
+    double vB = (vcon[1] * FH[0][B1] + vcon[2] * FH[0][B2] + vcon[3] * FH[0][B3]);
+    double ptot = -(-FH[1][UU] - FH[0][B_1] * (vB)) * vcon[dir] + FH[1][U_1] + pow(FH[0][B_1], 2.0) / gammasq;
+    if (!(fabs(ptot) > 0.) || (vcon[G_1] < cmin) || (vcon[G_1] > cmax) || !(fabs(vcon[G_1]) > 0.)) fail = 1;
+    if (cmax > iv && vcon[dir] <= iv && fail == 0) {
+        FT[0][RHO] = (cmax - ru[dir] / ru[0]) / (cmax - vcon[dir] + SMALL) * Ur[RHO];
+        FT[0][UU] = (cmax * Ur[UU] + Ur[U_1] - ptot * vcon[dir] + vB * FH[0][B_1]) / (cmax - vcon[dir] + SMALL);
+        FT[0][U_1] = (-FT[0][UU] + ptot) * vcon[dir] - vB * FH[0][B_1];
+        FT[0][U_2] = (-FH[0][B_1] * (FH[0][B_2] / (gammasq) + vB * vcon[G_2]) + cmax * Ur[U_2] - Fr[U_2]) /
+                     (cmax - vcon[dir] + SMALL);
+        FT[0][U_3] = (-FH[0][B_1] * (FH[0][B_3] / (gammasq) + vB * vcon[G_3]) + cmax * Ur[U_3] - Fr[U_3]) /
+                     (cmax - vcon[dir] + SMALL);
+        FT[0][B_1] = FH[0][B_1];
+        FT[0][B_2] = FH[0][B_2];
+        FT[0][B_3] = FH[0][B_3];
+        FT[0][KTOT] = (cmax - ru[dir] / ru[0]) / (cmax - vcon[dir] + SMALL) * Ur[KTOT];
+        for (int k = 0; k < NPR; k++) FT[1][k] = (Fr[k] + cmax * (FT[0][k] - Ur[k]));
+    } else if (cmin < iv && vcon[dir] >= iv && fail == 0) {
+        FT[0][RHO] = (cmin - lu[dir] / lu[0]) / (cmin - vcon[dir] + SMALL) * Ul[RHO];
+        FT[0][UU] = (cmin * Ul[UU] + Ul[U_1] - ptot * vcon[dir] + vB * FH[0][B_1]) / (cmin - vcon[dir] + SMALL);
+        FT[0][U_1] = (-FT[0][UU] + ptot) * vcon[dir] - vB * FH[0][B_1];
+        FT[0][U_2] = (-FH[0][B_1] * (FH[0][B_2] / (gammasq) + vB * vcon[G_2]) + cmin * Ul[U_2] - Fl[U_2]) /
+                     (cmin - vcon[dir] + SMALL);
+        FT[0][U_3] = (-FH[0][B_1] * (FH[0][B_3] / (gammasq) + vB * vcon[G_3]) + cmin * Ul[U_3] - Fl[U_3]) /
+                     (cmin - vcon[dir] + SMALL);
+        FT[0][B_1] = FH[0][B_1];
+        FT[0][B_2] = FH[0][B_2];
+        FT[0][B_3] = FH[0][B_3];
+        FT[0][KTOT] = (cmin - lu[dir] / lu[0]) / (cmin - vcon[dir] + SMALL) * Ul[KTOT];
+        for (int k = 0; k < NPR; k++) FT[1][k] = (Fl[k] + cmin * (FT[0][k] - Ul[k]));
+    } else {
+        for (int k = 0; k < NPR; k++) { FT[0][k] = FH[0][k]; FT[1][k] = FH[1][k]; }
+    }
+}
+
+/* One face with the HLLC solver in the orthonormal face frame
+ * (fluxcalc2D_FT, GPU_hllc.h:3-248): coordinate-frame fast speeds for the
+ * time step, states transformed with the frame's inverse, HLL or HLLC star
+ * fluxes there (HLLC's hydrodynamic variant where the normal field is
+ * negligible), transformed back; pl/pr already carry the normal field.
+ * Returns the face's ctop. */
+static double hllc_face(double gam, int dir, const double *pl, const double *pr, const geo *gm, double *Fout) {
+    cstate ql, qr;
+    double cmax_l, cmin_l, cmax_r, cmin_r, vd[NPR];
+    get_state(pl, gm, &ql);
+    get_state(pr, gm, &qr);
+    primtoflux(gam, pl, &ql, dir, gm, vd, &cmax_l, &cmin_l);
+    primtoflux(gam, pr, &qr, dir, gm, vd, &cmax_r, &cmin_r);
+    double cmax1 = fabs(MY_MAX(MY_MAX(0., cmax_l), cmax_r));
+    double cmin1 = fabs(MY_MAX(MY_MAX(0., -cmin_l), -cmin_r));
+    double ctop = MY_MAX(cmax1, cmin1);
+    double Mud[4][4], Mi[4][4];
+    ho_set_mud(gm->gcov, gm->gcon, dir, Mud, Mi);
+    double lu[4], lb[4], ru[4], rb[4];
+    for (int a = 0; a < 4; a++) {
+        lu[a] = 0.0; lb[a] = 0.0; ru[a] = 0.0; rb[a] = 0.0;
+        for (int b = 0; b < 4; b++) {
+            lu[a] += ql.ucon[b] * Mi[a][b];
+            lb[a] += ql.bcon[b] * Mi[a][b];
+            ru[a] += qr.ucon[b] * Mi[a][b];
+            rb[a] += qr.bcon[b] * Mi[a][b];
+        }
+    }
+    double Fl[NPR], Fr[NPR], Ul[NPR], Ur[NPR], FT[2][NPR], FH[2][NPR];
+    primtoflux_ft(gam, pl, lu, lb, dir, Fl);
+    primtoflux_ft(gam, pr, ru, rb, dir, Fr);
+    primtoflux_ft(gam, pl, lu, lb, 0, Ul);
+    primtoflux_ft(gam, pr, ru, rb, 0, Ur);
+    vchar_ft(gam, pl, lu, lb, dir, &cmax_l, &cmin_l);
+    vchar_ft(gam, pr, ru, rb, dir, &cmax_r, &cmin_r);
+    double cmax = MY_MAX(cmax_r, cmax_l);
+    double cmin = MY_MIN(cmin_r, cmin_l);
+    const int sdd = dir == 1 ? 4 : (dir == 2 ? 7 : 9);
+    double iv = gm->gcon[dir] / (sqrt(gm->gcon[dir] * gm->gcon[dir] - gm->gcon[0] * gm->gcon[sdd]));
+    if (cmax <= iv) {
+        for (int k = 0; k < NPR; k++) { FT[0][k] = Ur[k]; FT[1][k] = Fr[k]; }
+    } else if (cmin >= iv) {
+        for (int k = 0; k < NPR; k++) { FT[0][k] = Ul[k]; FT[1][k] = Fl[k]; }
+    } else {
+        for (int k = 0; k < NPR; k++) FH[0][k] = (Fl[k] - Fr[k] + cmax * Ur[k] - cmin * Ul[k]) / (cmax - cmin + SMALL);
+        for (int k = 0; k < NPR; k++)
+            FH[1][k] = ((cmax * Fl[k] - cmin * Fr[k] + cmax * cmin * (Ur[k] - Ul[k])) / (cmax - cmin + SMALL));
+        int do_hydro = (fabs(FH[0][dir + B1 - 1] * FH[0][dir + B1 - 1] * lu[0] * ru[0]) < pow(10., -10.) * fabs(FH[0][UU]));
+        if (do_hydro) hllc_hydro(dir, lu, ru, iv, cmin, cmax, FT, FH, Fl, Fr, Ul, Ur);
+        else hllc_mhd(dir, lu, ru, iv, cmin, cmax, FT, FH, Fl, Fr, Ul, Ur);
+    }
+    double F1[NPR];
+    for (int j1 = 0; j1 < 4; j1++) {
+        F1[j1 + UU] = 0.;
+        for (int j2 = 0; j2 < 4; j2++) {
+            F1[j1 + UU] += FT[0][j2 + UU] * Mud[dir][0] * Mi[j2][j1];
+            F1[j1 + UU] += FT[1][j2 + UU] * Mud[dir][dir] * Mi[j2][j1];
+        }
+    }
+    FT[0][U3] = 0.;
+    FT[1][U3] = -FT[0][B1 - 1 + dir];
+    for (int j1 = 1; j1 < 4; j1++) {
+        F1[j1 + U3] = 0.;
+        for (int j2 = 0; j2 < 4; j2++) {
+            F1[j1 + U3] += FT[0][j2 + U3] * Mud[dir][0] * Mud[j1][j2];
+            F1[j1 + U3] += FT[1][j2 + U3] * Mud[dir][dir] * Mud[j1][j2];
+        }
+    }
+    F1[RHO] = FT[0][RHO] * Mud[dir][0];
+    F1[RHO] += FT[1][RHO] * Mud[dir][dir];
+    F1[KTOT] = FT[0][KTOT] * Mud[dir][0];
+    F1[KTOT] += FT[1][KTOT] * Mud[dir][dir];
+    F1[UU] += F1[RHO];
+    for (int k = 0; k < NPR; k++) Fout[k] = gm->g * F1[k];
+    return ctop;
+}
+
 /* ----------------------------------------------------------------- flux -- */
 /*
  * Face fluxes in direction dir (fluxcalcprep + fluxcalc2D2, GPU_program1.cu:78-1068,
@@ -282,6 +544,14 @@ static void fluxes(const ho_grid *g, const dims *d, const ho_geom *m, const doub
                 if (dir == 2 && ((j == d->n2 + d->ng2 && g->pole2) || (j == d->ng2 && g->pole1))) {
                     pl[B1] = 0.;
                     pr[B1] = 0.;
+                }
+                if (g->riemann == 1) {
+                    double Fo[NPR];
+                    double ctop = hllc_face(g->gam, dir, pl, pr, &gm, Fo);
+                    for (int k = 0; k < NPR; k++) F[(long)k * d->ks + c] = Fo[k];
+                    double dtf = factor / ctop;
+                    if (dtf < best && dtf > 1.e-6) best = dtf;
+                    continue;
                 }
                 cstate q;
                 double t1[NPR], t2[NPR], t3[NPR], t4[NPR];

@@ -36,6 +36,8 @@ typedef struct {
                             GPU_const_trans.h:187-211) */
     int recon;           /* 0: PPM (para, PPM builds); 1: MC-limited linear
                             (slope_lim with factor 2, PPM = 0 builds) */
+    int riemann;         /* 0: HLL; 1: HLLC in the orthonormal face frame
+                            (HLLC builds, FRAME_TRANSFORM) */
 } ho_grid;
 
 typedef struct {
@@ -63,6 +65,7 @@ void ho_bound(const ho_grid *g, const ho_geom *m, double *pv, double *ps);
 /* Single-cell pieces (pinned one by one against the reference). */
 void ho_para(const double *x, double *l, double *r);
 double ho_slope_lim(double y1, double y2, double y3);
+void ho_set_mud(const double *gcov10, const double *gcon10, int dir, double Mud[4][4], double Mi[4][4]);
 void ho_primtoflux(double gam, const double *pr, const double *gcov10, const double *gcon10,
                    double gdet, int dir, double *flux, double *vmax, double *vmin);
 int ho_utoprim_2d(double gam, double *U, const double *gcov10, const double *gcon10, double gdet, double *prim);

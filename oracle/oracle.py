@@ -38,7 +38,7 @@ class HoGrid(ctypes.Structure):
                 ("ksize", ctypes.c_long), ("gsize", ctypes.c_long),
                 ("dx1", _d), ("dx2", _d), ("dx3", _d), ("gam", _d), ("cour", _d),
                 ("pole1", _i), ("pole2", _i), ("bc1", _i), ("bc2", _i), ("bc3", _i),
-                ("inversion", _i), ("ct_upwind", _i), ("recon", _i)]
+                ("inversion", _i), ("ct_upwind", _i), ("recon", _i), ("riemann", _i)]
 
 
 class HoGeom(ctypes.Structure):
@@ -73,6 +73,7 @@ def lib():
         L.ho_utoprim_nm_max_index.restype = _i
         L.ho_divb_max.argtypes = [ctypes.POINTER(HoGrid), ctypes.POINTER(HoGeom), _vp]
         L.ho_divb_max.restype = _d
+        L.ho_set_mud.argtypes = [_vp, _vp, _i, _vp, _vp]
         _lib = L
     return _lib
 
@@ -100,6 +101,10 @@ def ref(variant: str):
         L.ref_primtoflux.argtypes = [_vp, _vp, _vp, _d, _i, _vp, _vp, _vp]
         L.ref_para.argtypes = [_vp, _vp, _vp]
         L.ref_bl_coord.argtypes = [_vp, _vp]
+        if hasattr(L, "ref_set_mud"):
+            L.ref_set_mud.argtypes = [_vp, _vp]
+            L.ref_mud_plane.restype = ctypes.c_long
+            L.ref_nsolver.restype = _i
         _refs[variant] = L
     return _refs[variant]
 
@@ -213,12 +218,13 @@ class Setup:
     ct_upwind: int = 1
     inversion: int = 0  # 0: Noble 2D, 1: Newman-Hamlin
     recon: int = 0      # 0: PPM, 1: MC-limited linear
+    riemann: int = 0    # 0: HLL, 1: HLLC
 
     def grid(self):
         b = self.blk
         return HoGrid(b.n1, b.n2, b.n3, b.ng, b.ksize, b.gsize, self.dx[0], self.dx[1], self.dx[2],
                       self.gam, self.cour, self.pole1, self.pole2, self.bc[0], self.bc[1], self.bc[2],
-                      self.inversion, self.ct_upwind, self.recon)
+                      self.inversion, self.ct_upwind, self.recon, self.riemann)
 
 
 def _state(b: Block):
@@ -243,10 +249,54 @@ def oracle_bound(s: Setup, pname="p", psname="ps"):
     lib().ho_bound(ctypes.byref(g), ctypes.byref(m), _ptr(s.blk.arrays[pname]), _ptr(s.blk.arrays[psname]))
 
 
+def set_mud(gcov10, gcon10, d):
+    """Orthonormal face frame of direction d (oracle restatement of set_Mud):
+    (Mud, Mud_inv) as 4x4 arrays."""
+    M = np.zeros(16)
+    Mi = np.zeros(16)
+    lib().ho_set_mud(_ptr(np.ascontiguousarray(gcov10, float)), _ptr(np.ascontiguousarray(gcon10, float)), int(d),
+                     _ptr(M), _ptr(Mi))
+    return M.reshape(4, 4), Mi.reshape(4, 4)
+
+
+_mud_cache: dict = {}
+
+
+def ref_mud_tables(variant, s: Setup):
+    """Frame tables of every (i, j) and face direction in the layout the
+    reference's HLLC kernel reads (get_trans, GPU_hllc.h:878-900)."""
+    key = (variant, id(s.geo))
+    if key in _mud_cache:
+        return _mud_cache[key]
+    L = ref(variant)
+    plane, nsolver = L.ref_mud_plane(), L.ref_nsolver()
+    b, gs = s.blk, s.geo.gsize
+    mud = np.zeros(16 * nsolver * plane)
+    inv = np.zeros(16 * nsolver * plane)
+    loc = {1: FACE1, 2: FACE2, 3: FACE3}
+    for ii in range(b.g1):
+        for jj in range(b.g2):
+            gid = ii * b.g2 + jj
+            for kk in (1, 2, 3):
+                gcov = np.array([s.geo.gcov[(c * 5 + loc[kk]) * gs + gid] for c in range(10)])
+                gcon = np.array([s.geo.gcon[(c * 5 + loc[kk]) * gs + gid] for c in range(10)])
+                M, Mi = set_mud(gcov, gcon, kk)
+                for a in range(4):
+                    for c in range(4):
+                        idx = (a * 4 + c) * nsolver * plane + kk * plane + gid
+                        mud[idx] = M[a, c]
+                        inv[idx] = Mi[a, c]
+    _mud_cache[key] = (mud, inv)
+    return mud, inv
+
+
 def ref_stage(variant, s: Setup, full, Dt, dt, calc_dt=False):
     b = s.blk
     a = b.arrays
     dtdir = np.full(4, 1e9)
+    if s.riemann == 1:
+        mud, inv = ref_mud_tables(variant, s)
+        ref(variant).ref_set_mud(_ptr(mud), _ptr(inv))
     ref(variant).ref_stage(int(full), Dt, dt, s.cour, s.dx[0], s.dx[1], s.dx[2], s.pole1, s.pole2,
                            _ptr(a["p"]), _ptr(a["ph"]), _ptr(a["ps"]), _ptr(a["psh"]), _ptr(a["U"]),
                            _ptr(a["F1"]), _ptr(a["F2"]), _ptr(a["F3"]), _ptr(a["dq1"]), _ptr(a["dq2"]),

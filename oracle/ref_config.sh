@@ -11,7 +11,8 @@
 # the test with `return 0;`, the evident intent: floors off, no failure flag.
 #
 # usage: ref_config.sh <refdir> <outdir> <mode: torus|cart> <BS_1> <BS_2> <BS_3> <gamma-expr> [opts]
-#   opts: comma-separated build switches; mc = linear MC reconstruction (PPM 0)
+#   opts: comma-separated build switches; mc = linear MC reconstruction (PPM 0),
+#         hllc = HLLC Riemann solver (HLLC 1, which turns on FRAME_TRANSFORM)
 set -e
 REF="$1"; OUT="$2"; MODE="$3"; B1="$4"; B2="$5"; B3="$6"; GAM="$7"; OPTS="${8:-}"
 mkdir -p "$OUT"
@@ -32,5 +33,8 @@ if [ "$MODE" = "cart" ]; then
 fi
 case ",$OPTS," in
   *,mc,*) sed -i -e 's/^#define PPM (1)/#define PPM (0)/' "$OUT/config.h.tmp" ;;
+esac
+case ",$OPTS," in
+  *,hllc,*) sed -i -e 's/^#define HLLC (0)/#define HLLC (1)/' "$OUT/config.h.tmp" ;;
 esac
 mv "$OUT/config.h.tmp" "$OUT/config.h"

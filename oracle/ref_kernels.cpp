@@ -78,6 +78,17 @@ static double host_dt_min(const double *dtij, long ngroups) {
  * work arrays (all ksize-planar, zero-initialised by the caller):
  *   F1,F2,F3,dq1,dq2 : NPR planes; E_cent, emf : 4 planes; storage2: NPR planes
  */
+/* HLLC builds (FRAME_TRANSFORM): the orthonormal face frames, in the device
+ * layout get_trans reads (GPU_hllc.h:878-900), are supplied by the caller
+ * (set_Mud, hllc.c:20-164, is host code bound to the reference's globals). */
+static const double *g_mud = nullptr, *g_mudinv = nullptr;
+void ref_set_mud(const double *mud, const double *mudinv) {
+    g_mud = mud;
+    g_mudinv = mudinv;
+}
+long ref_mud_plane(void) { return (long)(BS_2 + 2 * N2G) * (BS_1 + 2 * N1G) + FIX_MEM2; }
+int ref_nsolver(void) { return NSOLVER; }
+
 void ref_stage(int full, double Dt, double dt, double cour,
                double dx1, double dx2, double dx3, int pole1, int pole2,
                double *p, double *ph, double *ps, double *psh, double *storage2,
@@ -102,8 +113,13 @@ void ref_stage(int full, double Dt, double dt, double cour,
         long ngroups = ((LOCAL_WORK_SIZE - nface % LOCAL_WORK_SIZE) + nface) / LOCAL_WORK_SIZE;
         double *dtij = (double *)calloc(ngroups, sizeof(double));
         run_grid(ngroups * LOCAL_WORK_SIZE, LOCAL_WORK_SIZE, [&] {
+#if (FRAME_TRANSFORM)
+            fluxcalc2D_FT(Fd[dir], dq1, dq2, pin, psin, gcov, gcon, gdet, g_mud, g_mudinv, MC, dir, cour, dtij,
+                          pole1, pole2, dxd[dir], calc_dt ? 1 : 0, full);
+#else
             fluxcalc2D2(Fd[dir], dq1, dq2, pin, psin, gcov, gcon, gdet, MC, dir, cour, dtij,
                         pole1, pole2, dxd[dir], calc_dt ? 1 : 0, full);
+#endif
         });
         if (calc_dt) dtdir[dir] = host_dt_min(dtij, ngroups);
         free(dtij);

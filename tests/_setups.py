@@ -102,11 +102,12 @@ def make_setup(variant, spin=0.9375, rout=40.0, seed=1, stress=False, cour=0.8, 
         poles = (1, 1)
     fill_synthetic(blk, geo, dx, seed=seed, stress=stress)
     s = O.Setup(blk, geo, tuple(dx[1:]), gam, cour, poles[0], poles[1], bc,
-                ct_upwind=0 if variant == "ot" else 1, recon=1 if variant.endswith("m") else 0)
+                ct_upwind=0 if variant == "ot" else 1, recon=1 if variant.endswith("m") else 0,
+                riemann=1 if variant.endswith("c") else 0)
     O.oracle_bound(s, "p", "ps")
     return s
 
 
 def clone(s: O.Setup) -> O.Setup:
     return O.Setup(s.blk.copy(), s.geo, s.dx, s.gam, s.cour, s.pole1, s.pole2, s.bc, s.ct_upwind, s.inversion,
-                   s.recon)
+                   s.recon, s.riemann)

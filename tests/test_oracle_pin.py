@@ -2,7 +2,8 @@
 code, built for the host from the reference sources (oracle/Makefile, variants
 t3: 3-D torus 16x8x8, t2: 2-D torus 24x24, ot: 2-D Cartesian 32x32, t3m: the
 3-D torus with linear MC reconstruction, PPM = 0, which also means two ghost
-layers).
+layers; t3c, t2c: the tori with the HLLC solver, HLLC = 1, whose kernel reads
+frame tables the harness builds with the oracle's restatement of set_Mud).
 
 Both sides get identical inputs and identical metric tables (computed by the
 reference's metric.c), and must agree bit for bit.
@@ -13,7 +14,7 @@ import pytest
 from oracle import oracle as O
 from tests._setups import clone, make_setup
 
-VARIANTS = ["t3", "t2", "ot", "t3m"]
+VARIANTS = ["t3", "t2", "ot", "t3m", "t3c", "t2c"]
 
 
 def need_ref(v):
