@@ -21,7 +21,8 @@ class HamrParams(ctypes.Structure):
     _fields_ = [("n1", _i), ("n2", _i), ("n3", _i), ("ng", _i), ("ksize", _l), ("gsize", _l),
                 ("dx1", _d), ("dx2", _d), ("dx3", _d), ("gam", _d), ("cour", _d),
                 ("pole1", _i), ("pole2", _i), ("bc1", _i), ("bc2", _i), ("bc3", _i),
-                ("ct_upwind", _i), ("precision", _i), ("stream", _vp), ("inversion", _i), ("recon", _i)]
+                ("ct_upwind", _i), ("precision", _i), ("stream", _vp), ("inversion", _i), ("recon", _i),
+                ("riemann", _i)]
 
 
 ERRORS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "out of device memory",

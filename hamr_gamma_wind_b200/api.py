@@ -19,6 +19,7 @@ BC = {"periodic": 0, "outflow": 1, "pole_trans": 2, "pole_refl": 3}
 PRECISION = {"fp64": 0, "mixed": 1}
 INVERSION = {"2d": 0, "nm": 1}
 RECON = {"ppm": 0, "mc": 1}
+RIEMANN = {"hll": 0, "hllc": 1}
 RHO, UU, U1, U2, U3, B1, B2, B3, KTOT = range(9)
 FACE1, FACE2, CORN, CENT, FACE3 = range(5)
 NPR = _lib.NPR
@@ -80,7 +81,7 @@ class Block:
 
     def __init__(self, n1, n2, n3, dx, gam, cour=0.8, bc=("outflow", "pole_trans", "periodic"),
                  poles=(1, 1), ct_upwind=True, precision="fp64", strict=False, ng=3, stream=None,
-                 inversion="2d", recon="ppm"):
+                 inversion="2d", recon="ppm", riemann="hll"):
         self.L = _lib.load(strict)
         self.n1, self.n2, self.n3, self.ng = n1, n2, n3, ng
         self.g1 = n1 + 2 * ng
@@ -89,7 +90,7 @@ class Block:
         prm = _lib.HamrParams(n1, n2, n3, ng, 0, 0, float(dx[0]), float(dx[1]), float(dx[2]), float(gam),
                               float(cour), int(poles[0]), int(poles[1]), BC[bc[0]], BC[bc[1]], BC[bc[2]],
                               int(bool(ct_upwind)), PRECISION[precision], stream, INVERSION[inversion],
-                              RECON[recon])
+                              RECON[recon], RIEMANN[riemann])
         ctx = ctypes.c_void_p()
         rc = self.L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx))
         if rc:

@@ -254,7 +254,7 @@ __global__ void k_batch_dt_finalize(const BEntry *__restrict__ E, int n, int upd
 // ===========================================================================
 struct hamr_batch {
     int n = 0;
-    int precision = 0, recon = 0, inversion = 0;
+    int precision = 0, recon = 0, inversion = 0, riemann = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int nsm = 148;
@@ -344,8 +344,12 @@ void batch_stage_r(hamr_batch *b, int full, bool calc_dt, int only) {
 
 template <typename T>
 void batch_stage_p(hamr_batch *b, int full, bool calc_dt, int only) {
-    if (b->recon == HAMR_RECON_MC) batch_stage_r<T, HAMR_RECON_MC>(b, full, calc_dt, only);
-    else batch_stage_r<T, HAMR_RECON_PPM>(b, full, calc_dt, only);
+    switch (b->recon | (b->riemann << 1)) {
+    case 1: batch_stage_r<T, 1>(b, full, calc_dt, only); break;
+    case 2: batch_stage_r<T, 2>(b, full, calc_dt, only); break;
+    case 3: batch_stage_r<T, 3>(b, full, calc_dt, only); break;
+    default: batch_stage_r<T, 0>(b, full, calc_dt, only); break;
+    }
 }
 
 void batch_stage(hamr_batch *b, int full, bool calc_dt, int only = -1) {
@@ -376,7 +380,9 @@ int hamr_batch_create(hamr_ctx *const *blocks, int n, void *stream, hamr_batch *
         if (!blocks[k]->have_geom) return HAMR_E_STATE;
         const hamr_params &p0 = blocks[0]->prm, &pk = blocks[k]->prm;
         // one instantiation of every phase kernel serves the whole batch
-        if (pk.precision != p0.precision || pk.recon != p0.recon || pk.inversion != p0.inversion) return HAMR_E_ARG;
+        if (pk.precision != p0.precision || pk.recon != p0.recon || pk.inversion != p0.inversion ||
+            pk.riemann != p0.riemann)
+            return HAMR_E_ARG;
         for (int j = 0; j < k; j++)
             if (blocks[j] == blocks[k]) return HAMR_E_ARG;
     }
@@ -385,6 +391,7 @@ int hamr_batch_create(hamr_ctx *const *blocks, int n, void *stream, hamr_batch *
     b->precision = blocks[0]->prm.precision;
     b->recon = blocks[0]->prm.recon;
     b->inversion = blocks[0]->prm.inversion;
+    b->riemann = blocks[0]->prm.riemann;
     b->ctx.assign(blocks, blocks + n);
     int dev = 0;
     cudaGetDevice(&dev);

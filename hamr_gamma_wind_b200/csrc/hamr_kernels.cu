@@ -37,7 +37,7 @@ struct Dims {
     int n1, n2, n3, ng1, ng2, ng3, G1, G2, G3, d1, d2, d3;
     long ks, gs;
     double dx1, dx2, dx3, gam, cour;
-    int pole1, pole2, bc1, bc2, bc3, ct_upwind, inversion, recon;
+    int pole1, pole2, bc1, bc2, bc3, ct_upwind, inversion, recon, riemann;
 };
 
 struct Geom {
@@ -91,7 +91,8 @@ struct StepSize {
 #define HAMR_FLUX_MINB_F 6
 #endif
 // one face of direction DIR (t < n_faces): reconstruction, two states, four
-// flux evaluations, HLL; returns the face's CFL limit, or 1e9 when filtered
+// flux evaluations, HLL (or HLLC); returns the face's CFL limit, or 1e9 when
+// filtered. REC: bit 0 MC reconstruction, bit 1 HLLC.
 template <int DIR, typename T, int REC>
 __device__ __forceinline__ double flux_face(const Dims &d, const Geom &m, const double *__restrict__ pv,
                                             const double *__restrict__ ps, T *__restrict__ F, const long t) {
@@ -113,7 +114,7 @@ __device__ __forceinline__ double flux_face(const Dims &d, const Geom &m, const 
 #pragma unroll
     for (int k = 0; k < NPR; k++) {
         const double *pk = pv + (long)k * d.ks + c;
-        if constexpr (REC == HAMR_RECON_MC) {
+        if constexpr ((REC & 1) == HAMR_RECON_MC) {
             // linear MC: the zones' face values y -+ slope/2 (fluxcalcprep, PPM = 0)
             T x[4];
 #pragma unroll
@@ -141,6 +142,17 @@ __device__ __forceinline__ double flux_face(const Dims &d, const Geom &m, const 
         pr[B1] = T(0.);
     }
     const T gam = (T)d.gam;
+    const double dxd = DIR == 1 ? d.dx1 : (DIR == 2 ? d.dx2 : d.dx3);
+    if constexpr ((REC & 2) != 0) {
+        // HLLC in the orthonormal face frame (fluxcalc2D_FT)
+        T Fo[NPR];
+        const T ctop = hllc_face<DIR, T>(gam, pl, pr, gm, Fo);
+#pragma unroll
+        for (int k = 0; k < NPR; k++) F[(long)k * d.ks + c] = Fo[k];
+        const double v = d.cour * dxd / (double)ctop;
+        if (v > 1.e-6 && v < dtf) dtf = v;
+        return dtf;
+    }
     State<T> q;
     T t1[NPR], t2[NPR], t3[NPR], t4[NPR];
     T cmax_l, cmin_l, cmax_r, cmin_r, vd;
@@ -158,7 +170,6 @@ __device__ __forceinline__ double flux_face(const Dims &d, const Geom &m, const 
 #pragma unroll
     for (int k = 0; k < NPR; k++)
         F[(long)k * d.ks + c] = (cmax * t1[k] + cmin * t3[k] - cmax * cmin * (t4[k] - t2[k])) / (cmax + cmin + T(SMALL_D));
-    const double dxd = DIR == 1 ? d.dx1 : (DIR == 2 ? d.dx2 : d.dx3);
     const double v = d.cour * dxd / (double)ctop;
     if (v > 1.e-6 && v < dtf) dtf = v;
     return dtf;
@@ -950,10 +961,12 @@ inline void prof_mark(Prof *pf, int slot, cudaStream_t s) {
 template <int DIR, typename T>
 void launch_flux(long n, cudaStream_t s, const Dims &d, const Geom &m, const double *pin, const double *psin, T *F,
                  unsigned long long *dtbits, int cd) {
-    if (d.recon == HAMR_RECON_MC)
-        k_flux<DIR, T, HAMR_RECON_MC><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd);
-    else
-        k_flux<DIR, T, HAMR_RECON_PPM><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd);
+    switch (d.recon | (d.riemann << 1)) {
+    case 1: k_flux<DIR, T, 1><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+    case 2: k_flux<DIR, T, 2><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+    case 3: k_flux<DIR, T, 3><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+    default: k_flux<DIR, T, 0><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+    }
 }
 
 // one sub-step: fluxes, CT, update, ghost fill of the written state. T is the
@@ -1049,6 +1062,7 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
     *out = nullptr;
     if (prm->n1 < 2 || prm->n2 < 2 || prm->n3 < 1) return HAMR_E_ARG;
     if (prm->recon != HAMR_RECON_PPM && prm->recon != HAMR_RECON_MC) return HAMR_E_ARG;
+    if (prm->riemann != HAMR_RIEMANN_HLL && prm->riemann != HAMR_RIEMANN_HLLC) return HAMR_E_ARG;
     if (!(prm->ng == 3 || (prm->ng == 2 && prm->recon == HAMR_RECON_MC))) return HAMR_E_ARG;
     if (prm->precision != HAMR_FP64 && prm->precision != HAMR_MIXED) return HAMR_E_ARG;
     if (prm->inversion != HAMR_INV_2D && prm->inversion != HAMR_INV_NM) return HAMR_E_ARG;
@@ -1073,6 +1087,7 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
     d.ct_upwind = prm->ct_upwind;
     d.inversion = prm->inversion;
     d.recon = prm->recon;
+    d.riemann = prm->riemann;
     if (prm->stream) {
         ctx->stream = (cudaStream_t)prm->stream;
     } else {
@@ -1346,6 +1361,7 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
     if (!prm || !gcov || !gcon || !gdet || !conn || !p || !ps || !(dt > 0)) return HAMR_E_ARG;
     if (prm->n1 < 2 || prm->n2 < 2 || prm->n3 < 1 || prm->precision != HAMR_FP64) return HAMR_E_ARG;
     if (prm->recon != HAMR_RECON_PPM && prm->recon != HAMR_RECON_MC) return HAMR_E_ARG;
+    if (prm->riemann != HAMR_RIEMANN_HLL && prm->riemann != HAMR_RIEMANN_HLLC) return HAMR_E_ARG;
     if (!(prm->ng == 3 || (prm->ng == 2 && prm->recon == HAMR_RECON_MC))) return HAMR_E_ARG;
     if (prm->inversion != HAMR_INV_2D && prm->inversion != HAMR_INV_NM) return HAMR_E_ARG;
     if (prm->n3 > 1 && prm->bc3 != HAMR_BC_PERIODIC) return HAMR_E_ARG;
@@ -1371,6 +1387,7 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
     d.ct_upwind = prm->ct_upwind;
     d.inversion = prm->inversion;
     d.recon = prm->recon;
+    d.riemann = prm->riemann;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES) return HAMR_E_CUDA;
     if (!na_ready[dev] && na_setup(dev) != HAMR_OK) return HAMR_E_CUDA;

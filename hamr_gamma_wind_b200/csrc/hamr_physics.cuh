@@ -645,4 +645,261 @@ __device__ __forceinline__ int utoprim_nm(double gam, const double *U, const dou
     return 0;
 }
 
+// ---------------------------------------------------------------- HLLC
+// (fluxcalc2D_FT, calc_HLLC, calc_HLLC_hydro, primtoflux_FT, vchar_FT:
+// GPU_hllc.h:3-396, 903-1111; set_Mud: hllc.c:20-164)
+__host__ __device__ __forceinline__ int sym4(int a, int b) {
+    return a == b ? (a == 0 ? 0 : (a == 1 ? 4 : (a == 2 ? 7 : 9)))
+                  : (a + b == 1 ? 1 : (a + b == 2 ? 2 : (a == 0 || b == 0 ? 3 : (a + b == 3 ? 5 : (a + b == 4 ? 6 : 8)))));
+}
+
+// orthonormal frame of a face of direction dir, from the face metric; (d, e, f)
+// is the cyclic order starting at dir
+template <typename T>
+__device__ __forceinline__ void set_mud(const Geo<T> &gm, int dir, T Mud[4][4], T Mi[4][4]) {
+    const int d = dir, e = dir % 3 + 1, f = (dir + 1) % 3 + 1;
+#define GU(a, b) gm.gcon[sym4(a, b)]
+#define GD(a, b) gm.gcov[sym4(a, b)]
+    const T A = -d_pow(-GU(0, 0), T(-0.5));
+    const T B = d_pow((GU(0, 0)) * (GU(0, 0) * GU(d, d) - GU(0, d) * GU(0, d)), T(-0.5));
+    const T C = d_pow(GD(f, f), T(-0.5));
+    const T D = d_pow((GD(f, f)) * (GD(e, e) * GD(f, f) - GD(e, f) * GD(e, f)), T(-0.5));
+    for (int a = 0; a < 4; a++)
+        for (int b = 0; b < 4; b++) Mud[a][b] = Mi[a][b] = T(0.);
+    Mud[0][0] = A * GU(0, 0);
+    Mud[d][0] = A * GU(0, d);
+    Mud[d][d] = B * (GU(0, d) * GU(0, d) - GU(0, 0) * GU(d, d));
+    Mud[e][0] = A * GU(0, e);
+    Mud[e][d] = B * (GU(0, d) * GU(0, e) - GU(0, 0) * GU(d, e));
+    Mud[e][e] = D * GD(f, f);
+    Mud[f][0] = A * GU(0, f);
+    Mud[f][d] = B * (GU(0, d) * GU(0, f) - GU(0, 0) * GU(d, f));
+    Mud[f][e] = -D * GD(e, f);
+    Mud[f][f] = C;
+    const T E = GU(0, d) * GU(d, e) - GU(d, d) * GU(0, e);
+    const T F = GU(0, d) * GU(0, e) - GU(0, 0) * GU(d, e);
+    const T G = GU(0, d) * GU(d, f) - GU(d, d) * GU(0, f);
+    const T H = GU(0, d) * GU(0, f) - GU(0, 0) * GU(d, f);
+    Mi[0][0] = -A;
+    Mi[d][0] = B * GU(0, d);
+    Mi[d][d] = -B * GU(0, 0);
+    Mi[e][0] = B * B * E * GU(0, 0) / (D * GD(f, f));
+    Mi[e][d] = B * B * F * GU(0, 0) / (D * GD(f, f));
+    Mi[e][e] = T(1.) / (D * GD(f, f));
+    Mi[f][0] = (B * B / C) * GU(0, 0) * (G + E * GD(e, f) / GD(f, f));
+    Mi[f][d] = (B * B / C) * GU(0, 0) * (H + F * GD(e, f) / GD(f, f));
+    Mi[f][e] = (T(1.) / C) * GD(e, f) / GD(f, f);
+    Mi[f][f] = T(1.) / C;
+#undef GU
+#undef GD
+}
+
+template <typename T>
+__device__ __forceinline__ void primtoflux_ft(T gam, const T *pr, const T *ucon, const T *bcon, int dir, T *flux) {
+    flux[RHO] = pr[RHO] * ucon[dir];
+    const T P = (gam - T(1.)) * pr[UU];
+    const T w = P + pr[RHO] + pr[UU];
+    const T bsq = -bcon[0] * bcon[0] + bcon[1] * bcon[1] + bcon[2] * bcon[2] + bcon[3] * bcon[3];
+    const T eta = w + bsq;
+    const T ptot = P + T(0.5) * bsq;
+    flux[UU] = -eta * ucon[dir] * ucon[0] + ptot * T(dir == 0 ? 1. : 0.) + bcon[dir] * bcon[0];
+    for (int j = 1; j < 4; j++) flux[UU + j] = eta * ucon[dir] * ucon[j] + ptot * T(dir == j ? 1. : 0.) - bcon[dir] * bcon[j];
+    for (int k = B1; k <= B3; k++) flux[k] = bcon[k - 4] * ucon[dir] - bcon[dir] * ucon[k - 4];
+    flux[KTOT] = flux[RHO] * P * d_pow(pr[RHO], -gam);
+}
+
+template <typename T>
+__device__ __forceinline__ void vchar_ft(T gam, const T *pr, const T *ucon, const T *bcon, int dir, T *vmax, T *vmin) {
+    const T bsq = -bcon[0] * bcon[0] + bcon[1] * bcon[1] + bcon[2] * bcon[2] + bcon[3] * bcon[3];
+    const T EF = pr[RHO] + gam * pr[UU];
+    const T cs2 = gam * (gam - T(1.)) * pr[UU] / EF;
+    const T EE = bsq + EF;
+    const T va2 = bsq / EE;
+    T cms2 = cs2 + va2 - cs2 * va2;
+    if (cms2 < T(0.)) cms2 = T(SMALL_D);
+    if (cms2 > T(1.)) cms2 = T(1.);
+    const T Asq = T(1.), Bsq = T(-1.);
+    const T Au = ucon[dir], Bu = ucon[0];
+    const T Au2 = Au * Au, Bu2 = Bu * Bu, AuBu = Au * Bu;
+    const T A = Bu2 - (Bsq + Bu2) * cms2;
+    const T B = T(2.) * (AuBu - (AuBu) * cms2);
+    const T C = Au2 - (Asq + Au2) * cms2;
+    T discr = B * B - T(4.) * A * C;
+    if ((discr < T(0.0)) && (discr > T(-1.e-10))) discr = T(0.0);
+    else if (discr < T(-1.e-10)) discr = T(0.);
+    discr = d_sqrt(discr);
+    const T vp = -(-B + discr) / (T(2.) * A);
+    const T vm = -(-B - discr) / (T(2.) * A);
+    if (vp > vm) { *vmax = vp; *vmin = vm; }
+    else { *vmax = vm; *vmin = vp; }
+}
+
+template <typename T>
+__device__ __forceinline__ void hllc_hydro(int dir, const T *lu, const T *ru, T iv, T cmin, T cmax, T FT[2][NPR],
+                                           const T FH[2][NPR], const T *Fl, const T *Fr, const T *Ul, const T *Ur) {
+    const int U_1 = UU + dir, U_2 = UU + dir % 3 + 1, U_3 = UU + (dir + 1) % 3 + 1;
+    const int B_1 = B1 + dir - 1, B_2 = B1 + dir % 3, B_3 = B1 + (dir + 1) % 3;
+    bool fail = false;
+    const T A = -FH[1][UU];
+    const T B = -FH[1][U_1] + FH[0][UU];
+    const T C = FH[0][U_1];
+    const T D = B * B - T(4.) * A * C;
+    const T vcon = (-B - d_sqrt(D)) / (T(2.) * A);
+    const T ptot = -(-FH[1][UU]) * vcon + FH[1][U_1];
+    if (!(d_fabs(ptot) > T(0.)) || (vcon < cmin) || (vcon > cmax) || !(d_fabs(vcon) > T(0.))) fail = true;
+    if (cmax > iv && vcon <= iv && !fail) {
+        const T s = (cmax - ru[dir] / ru[0]) / (cmax - vcon + T(SMALL_D));
+        FT[0][RHO] = s * Ur[RHO];
+        FT[0][UU] = (cmax * Ur[UU] + Ur[U_1] - ptot * vcon) / (cmax - vcon + T(SMALL_D));
+        FT[0][U_1] = (-FT[0][UU] + ptot) * vcon;
+        FT[0][U_2] = s * Ur[U_2];
+        FT[0][U_3] = s * Ur[U_3];
+        FT[0][B_1] = FH[0][B_1];
+        FT[0][B_2] = s * Ur[B_2];
+        FT[0][B_3] = s * Ur[B_3];
+        FT[0][KTOT] = s * Ur[KTOT];
+        for (int k = 0; k < NPR; k++) FT[1][k] = (Fr[k] + cmax * (FT[0][k] - Ur[k]));
+    } else if (cmin < iv && vcon >= iv && !fail) {
+        const T s = (cmin - lu[dir] / lu[0]) / (cmin - vcon + T(SMALL_D));
+        FT[0][RHO] = s * Ul[RHO];
+        FT[0][UU] = (cmin * Ul[UU] + Ul[U_1] - ptot * vcon) / (cmin - vcon + T(SMALL_D));
+        FT[0][U_1] = (-FT[0][UU] + ptot) * vcon;
+        FT[0][U_2] = s * Ul[U_2];
+        FT[0][U_3] = s * Ul[U_3];
+        FT[0][B_1] = FH[0][B_1];
+        FT[0][B_2] = s * Ul[B_2];
+        FT[0][B_3] = s * Ul[B_3];
+        FT[0][KTOT] = s * Ul[KTOT];
+        for (int k = 0; k < NPR; k++) FT[1][k] = (Fl[k] + cmin * (FT[0][k] - Ul[k]));
+    } else {
+        for (int k = 0; k < NPR; k++) { FT[0][k] = FH[0][k]; FT[1][k] = FH[1][k]; }
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void hllc_mhd(int dir, const T *lu, const T *ru, T iv, T cmin, T cmax, T FT[2][NPR],
+                                         const T FH[2][NPR], const T *Fl, const T *Fr, const T *Ul, const T *Ur) {
+    const int G_1 = dir, G_2 = dir % 3 + 1, G_3 = (dir + 1) % 3 + 1;
+    const int U_1 = UU + G_1, U_2 = UU + G_2, U_3 = UU + G_3;
+    const int B_1 = B1 + G_1 - 1, B_2 = B1 + G_2 - 1, B_3 = B1 + G_3 - 1;
+    T vcon[4];
+    vcon[0] = T(0.);
+    bool fail = false;
+    const T A = -FH[1][UU] - (FH[0][B_2] * FH[1][B_2] + FH[0][B_3] * FH[1][B_3]);
+    const T B = -FH[1][U_1] + FH[0][UU] + (FH[0][B_2] * FH[0][B_2] + FH[0][B_3] * FH[0][B_3]) +
+                (FH[1][B_2] * FH[1][B_2] + FH[1][B_3] * FH[1][B_3]);
+    const T C = FH[0][U_1] - (FH[0][B_2] * FH[1][B_2] + FH[0][B_3] * FH[1][B_3]);
+    const T D = B * B - T(4.) * A * C;
+    vcon[G_1] = (-B - d_sqrt(D)) / (T(2.) * A);
+    vcon[G_2] = (FH[0][B_2] * vcon[G_1] - FH[1][B_2]) / FH[0][B_1];
+    vcon[G_3] = (FH[0][B_3] * vcon[G_1] - FH[1][B_3]) / FH[0][B_1];
+    const T gammasq = T(1.) / (T(1.) - (vcon[1] * vcon[1] + vcon[2] * vcon[2] + vcon[3] * vcon[3]));
+    const T vB = (vcon[1] * FH[0][B1] + vcon[2] * FH[0][B2] + vcon[3] * FH[0][B3]);
+    const T ptot = -(-FH[1][UU] - FH[0][B_1] * (vB)) * vcon[dir] + FH[1][U_1] + d_pow(FH[0][B_1], T(2.0)) / gammasq;
+    if (!(d_fabs(ptot) > T(0.)) || (vcon[G_1] < cmin) || (vcon[G_1] > cmax) || !(d_fabs(vcon[G_1]) > T(0.))) fail = true;
+    if (cmax > iv && vcon[dir] <= iv && !fail) {
+        FT[0][RHO] = (cmax - ru[dir] / ru[0]) / (cmax - vcon[dir] + T(SMALL_D)) * Ur[RHO];
+        FT[0][UU] = (cmax * Ur[UU] + Ur[U_1] - ptot * vcon[dir] + vB * FH[0][B_1]) / (cmax - vcon[dir] + T(SMALL_D));
+        FT[0][U_1] = (-FT[0][UU] + ptot) * vcon[dir] - vB * FH[0][B_1];
+        FT[0][U_2] = (-FH[0][B_1] * (FH[0][B_2] / (gammasq) + vB * vcon[G_2]) + cmax * Ur[U_2] - Fr[U_2]) /
+                     (cmax - vcon[dir] + T(SMALL_D));
+        FT[0][U_3] = (-FH[0][B_1] * (FH[0][B_3] / (gammasq) + vB * vcon[G_3]) + cmax * Ur[U_3] - Fr[U_3]) /
+                     (cmax - vcon[dir] + T(SMALL_D));
+        FT[0][B_1] = FH[0][B_1];
+        FT[0][B_2] = FH[0][B_2];
+        FT[0][B_3] = FH[0][B_3];
+        FT[0][KTOT] = (cmax - ru[dir] / ru[0]) / (cmax - vcon[dir] + T(SMALL_D)) * Ur[KTOT];
+        for (int k = 0; k < NPR; k++) FT[1][k] = (Fr[k] + cmax * (FT[0][k] - Ur[k]));
+    } else if (cmin < iv && vcon[dir] >= iv && !fail) {
+        FT[0][RHO] = (cmin - lu[dir] / lu[0]) / (cmin - vcon[dir] + T(SMALL_D)) * Ul[RHO];
+        FT[0][UU] = (cmin * Ul[UU] + Ul[U_1] - ptot * vcon[dir] + vB * FH[0][B_1]) / (cmin - vcon[dir] + T(SMALL_D));
+        FT[0][U_1] = (-FT[0][UU] + ptot) * vcon[dir] - vB * FH[0][B_1];
+        FT[0][U_2] = (-FH[0][B_1] * (FH[0][B_2] / (gammasq) + vB * vcon[G_2]) + cmin * Ul[U_2] - Fl[U_2]) /
+                     (cmin - vcon[dir] + T(SMALL_D));
+        FT[0][U_3] = (-FH[0][B_1] * (FH[0][B_3] / (gammasq) + vB * vcon[G_3]) + cmin * Ul[U_3] - Fl[U_3]) /
+                     (cmin - vcon[dir] + T(SMALL_D));
+        FT[0][B_1] = FH[0][B_1];
+        FT[0][B_2] = FH[0][B_2];
+        FT[0][B_3] = FH[0][B_3];
+        FT[0][KTOT] = (cmin - lu[dir] / lu[0]) / (cmin - vcon[dir] + T(SMALL_D)) * Ul[KTOT];
+        for (int k = 0; k < NPR; k++) FT[1][k] = (Fl[k] + cmin * (FT[0][k] - Ul[k]));
+    } else {
+        for (int k = 0; k < NPR; k++) { FT[0][k] = FH[0][k]; FT[1][k] = FH[1][k]; }
+    }
+}
+
+// HLLC flux of one face (states carry the normal field already); returns ctop
+// from the coordinate-frame fast speeds, as the HLL path
+template <int DIR, typename T>
+__device__ __forceinline__ T hllc_face(T gam, const T *pl, const T *pr, const Geo<T> &gm, T *Fout) {
+    State<T> ql, qr;
+    T cmax_l, cmin_l, cmax_r, cmin_r, vd[NPR];
+    get_state(pl, gm, ql);
+    get_state(pr, gm, qr);
+    primtoflux(gam, pl, ql, DIR, gm, T(0.), vd, &cmax_l, &cmin_l);
+    primtoflux(gam, pr, qr, DIR, gm, T(0.), vd, &cmax_r, &cmin_r);
+    const T cmax1 = d_fabs(d_max(d_max(T(0.), cmax_l), cmax_r));
+    const T cmin1 = d_fabs(d_max(d_max(T(0.), -cmin_l), -cmin_r));
+    const T ctop = d_max(cmax1, cmin1);
+    T Mud[4][4], Mi[4][4];
+    set_mud(gm, DIR, Mud, Mi);
+    T lu[4], lb[4], ru[4], rb[4];
+    for (int a = 0; a < 4; a++) {
+        lu[a] = T(0.0); lb[a] = T(0.0); ru[a] = T(0.0); rb[a] = T(0.0);
+        for (int b = 0; b < 4; b++) {
+            lu[a] += ql.ucon[b] * Mi[a][b];
+            lb[a] += ql.bcon[b] * Mi[a][b];
+            ru[a] += qr.ucon[b] * Mi[a][b];
+            rb[a] += qr.bcon[b] * Mi[a][b];
+        }
+    }
+    T Fl[NPR], Fr[NPR], Ul[NPR], Ur[NPR], FT[2][NPR], FH[2][NPR];
+    primtoflux_ft(gam, pl, lu, lb, DIR, Fl);
+    primtoflux_ft(gam, pr, ru, rb, DIR, Fr);
+    primtoflux_ft(gam, pl, lu, lb, 0, Ul);
+    primtoflux_ft(gam, pr, ru, rb, 0, Ur);
+    vchar_ft(gam, pl, lu, lb, DIR, &cmax_l, &cmin_l);
+    vchar_ft(gam, pr, ru, rb, DIR, &cmax_r, &cmin_r);
+    const T cmax = d_max(cmax_r, cmax_l);
+    const T cmin = d_min(cmin_r, cmin_l);
+    constexpr int sdd = DIR == 1 ? 4 : (DIR == 2 ? 7 : 9);
+    const T iv = gm.gcon[DIR] / (d_sqrt(gm.gcon[DIR] * gm.gcon[DIR] - gm.gcon[0] * gm.gcon[sdd]));
+    if (cmax <= iv) {
+        for (int k = 0; k < NPR; k++) { FT[0][k] = Ur[k]; FT[1][k] = Fr[k]; }
+    } else if (cmin >= iv) {
+        for (int k = 0; k < NPR; k++) { FT[0][k] = Ul[k]; FT[1][k] = Fl[k]; }
+    } else {
+        for (int k = 0; k < NPR; k++) FH[0][k] = (Fl[k] - Fr[k] + cmax * Ur[k] - cmin * Ul[k]) / (cmax - cmin + T(SMALL_D));
+        for (int k = 0; k < NPR; k++)
+            FH[1][k] = ((cmax * Fl[k] - cmin * Fr[k] + cmax * cmin * (Ur[k] - Ul[k])) / (cmax - cmin + T(SMALL_D)));
+        const bool do_hydro = d_fabs(FH[0][DIR + B1 - 1] * FH[0][DIR + B1 - 1] * lu[0] * ru[0]) < T(1.e-10) * d_fabs(FH[0][UU]);
+        if (do_hydro) hllc_hydro(DIR, lu, ru, iv, cmin, cmax, FT, FH, Fl, Fr, Ul, Ur);
+        else hllc_mhd(DIR, lu, ru, iv, cmin, cmax, FT, FH, Fl, Fr, Ul, Ur);
+    }
+    T F1[NPR];
+    for (int j1 = 0; j1 < 4; j1++) {
+        F1[j1 + UU] = T(0.);
+        for (int j2 = 0; j2 < 4; j2++) {
+            F1[j1 + UU] += FT[0][j2 + UU] * Mud[DIR][0] * Mi[j2][j1];
+            F1[j1 + UU] += FT[1][j2 + UU] * Mud[DIR][DIR] * Mi[j2][j1];
+        }
+    }
+    FT[0][U3] = T(0.);
+    FT[1][U3] = -FT[0][B1 - 1 + DIR];
+    for (int j1 = 1; j1 < 4; j1++) {
+        F1[j1 + U3] = T(0.);
+        for (int j2 = 0; j2 < 4; j2++) {
+            F1[j1 + U3] += FT[0][j2 + U3] * Mud[DIR][0] * Mud[j1][j2];
+            F1[j1 + U3] += FT[1][j2 + U3] * Mud[DIR][DIR] * Mud[j1][j2];
+        }
+    }
+    F1[RHO] = FT[0][RHO] * Mud[DIR][0];
+    F1[RHO] += FT[1][RHO] * Mud[DIR][DIR];
+    F1[KTOT] = FT[0][KTOT] * Mud[DIR][0];
+    F1[KTOT] += FT[1][KTOT] * Mud[DIR][DIR];
+    F1[UU] += F1[RHO];
+    for (int k = 0; k < NPR; k++) Fout[k] = gm.g * F1[k];
+    return ctop;
+}
+
 }  // namespace hamr

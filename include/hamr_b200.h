@@ -67,6 +67,12 @@ enum hamr_recon {
                                builds; ng = 2 as there, or 3) */
 };
 
+enum hamr_riemann {
+    HAMR_RIEMANN_HLL = 0,   /* HLL (fluxcalc2D2, the shipped default, HLLC 0) */
+    HAMR_RIEMANN_HLLC = 1   /* HLLC in the orthonormal face frame with its HLL fallback
+                               and hydrodynamic sub-case (fluxcalc2D_FT, GPU_hllc.h:3) */
+};
+
 typedef struct hamr_params {
     int n1, n2, n3;         /* active cells per direction (n3 == 1: 2-D, x1-x2) */
     int ng;                 /* ghost layers: 3 (NG = 2 + PPM, config.h:1280); 2 allowed with MC */
@@ -83,6 +89,7 @@ typedef struct hamr_params {
     void *stream;           /* cudaStream_t to run on; NULL: the context creates one */
     int inversion;          /* enum hamr_inversion (zero-initialised: Noble 2D) */
     int recon;              /* enum hamr_recon (zero-initialised: PPM) */
+    int riemann;            /* enum hamr_riemann (zero-initialised: HLL) */
 } hamr_params;
 
 typedef struct hamr_ctx hamr_ctx;
