@@ -1,7 +1,8 @@
 """Throughput of the single-block GRMHD RK2 step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c3|c2] [--precision fp64]
+                    [--workload c3|c2|c4|c5] [--precision fp64|mixed|both]
+                    [--recon ppm|mc] [--riemann hll|hllc]
 
 Workload (default c3): the 3-D Fishbone-Moncrief torus around a Kerr hole,
 a = 0.9375, r_in = 6, r_max = 12, gamma = 13/9, beta_min = 100, 4 % seeded
@@ -192,7 +193,8 @@ def _measure(pb, precision, args, stream, world):
     per-kernel-group breakdown; returns (ms, dt, blk)."""
     import torch
     from hamr_gamma_wind_b200.api import Block
-    blk = Block(**pb.block_kwargs(), precision=precision, stream=ctypes_stream(stream))
+    blk = Block(**pb.block_kwargs(), precision=precision, stream=ctypes_stream(stream), recon=args.recon,
+                riemann=args.riemann)
     blk.set_geometry(pb.geo)
     blk.upload(pb.p, pb.ps)
     blk.bound()
@@ -346,7 +348,8 @@ def run_ours(args):
             "dtype": "f64" if head == "fp64" else "f32 flux/EMF + f64 update/inversion", "data": "synthetic",
             "config": {"workload": f"3-D FM torus {wl['n1']}x{wl['n2']}x{wl['n3']} (a=0.9375, r_in=6, r_max=12, "
                                    f"gamma=13/9, beta_min=100), {head}",
-                       "zones": cells, "precision": head, "l2": "inputs larger than L2 (no flush)",
+                       "zones": cells, "precision": head, "recon": args.recon, "riemann": args.riemann,
+                       "l2": "inputs larger than L2 (no flush)",
                        "dt_update_interval": 16, "parallelism": f"replicas x{world}"},
             "precisions": {k: {"value": v["value"], "ms_per_step": v["ms"] / args.steps,
                                "kernel_ms_per_step": v.get("kernels")} for k, v in runs.items()},
@@ -546,6 +549,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c3", choices=list(WORKLOADS) + ["c4", "c5"])
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
+    ap.add_argument("--recon", default="ppm", choices=["ppm", "mc"],
+                    help="reconstruction of the c3/c2 torus (PPM as shipped, or MC)")
+    ap.add_argument("--riemann", default="hll", choices=["hll", "hllc"],
+                    help="Riemann solver of the c3/c2 torus (HLL as shipped, or HLLC)")
     ap.add_argument("--accuracy", type=int, default=0,
                     help="instead of timing: per-field L1 difference of mixed vs FP64 after this many steps")
     ap.add_argument("--kernels-only", action="store_true",

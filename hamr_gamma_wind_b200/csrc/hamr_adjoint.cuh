@@ -627,48 +627,45 @@ __global__ void k_adj_fix_flux(const Dims d, const double *__restrict__ F1, doub
 
 namespace {
 
-// x2 reflective-axis ghost fill reversed (2-D), one thread per i: ghost
-// copies (with the sign flips) and the POLEFIX interpolation of the first
-// two rows, in reverse order
+// x2 reflective-axis ghost fill reversed (2-D), one item per (component, i)
+// over the NPR primitives and face planes 0 and 2: ghost copies (with the
+// sign flips) and the POLEFIX interpolation of the first two rows, in the
+// reverse of the forward's order
+constexpr int ADJ_X2_COMPS = NPR + 2;
 __global__ void k_adj_bound_x2_refl(const Dims d, double *ap, double *aps) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= d.G1) return;
-    const int i = (int)t, n2 = d.n2, ng = d.ng2, jref = 2;
-    const long ks = d.ks;
+    if (t >= (long)ADJ_X2_COMPS * d.G1) return;
+    const int i = (int)(t % d.G1), comp = (int)(t / d.G1), n2 = d.n2, ng = d.ng2, jref = 2;
+    const bool face = comp >= NPR;
+    const int k = face ? 2 * (comp - NPR) : comp;
+    double *a = (face ? aps : ap) + (long)k * d.ks;
     auto C = [&](int j) { return cix(d, i, j, 0); };
-    auto mv = [&](double *a, long dst, long src, double sgn) { a[src] += sgn * a[dst]; a[dst] = 0.; };
+    auto mv = [&](long dst, long src, double sgn) { a[src] += sgn * a[dst]; a[dst] = 0.; };
+    const double sg = (!face && (k == U2 || k == B2)) ? -1. : 1.;
+    const bool fixrow = !face && (k == RHO || k == UU || k == U1 || k == U3 || k == KTOT);
+    const bool fixu2 = !face && k == U2;
     if (d.pole2) {
-        for (int g = ng - 1; g >= 0; g--) {
-            mv(aps, C(n2 + ng + g), C(n2 + ng - 1 - g), 1.);
-            mv(aps + 2 * ks, C(n2 + ng + g), C(n2 + ng - 1 - g), 1.);
-        }
-        for (int g = ng - 1; g >= 0; g--)
-            for (int k = 0; k < NPR; k++) {
-                const double s = (k == U2 || k == B2) ? -1. : 1.;
-                mv(ap + k * ks, C(n2 + ng + g), C(n2 + ng - 1 - g), s);
-            }
+        for (int g = ng - 1; g >= 0; g--) mv(C(n2 + ng + g), C(n2 + ng - 1 - g), sg);
         for (int jj = jref - 1; jj >= 0; jj--) {
             const long c = C(n2 + ng - 1 - jj), r = C(n2 + ng - 1 - jref);
-            ap[U2 * ks + r] += (jj + 0.5) / (jref + 0.5) * ap[U2 * ks + c];
-            ap[U2 * ks + c] = 0.;
-            for (int k : {RHO, UU, U1, U3, KTOT}) mv(ap + k * ks, c, r, 1.);
+            if (fixu2) {
+                a[r] += (jj + 0.5) / (jref + 0.5) * a[c];
+                a[c] = 0.;
+            } else if (fixrow) {
+                mv(c, r, 1.);
+            }
         }
     }
     if (d.pole1) {
-        for (int g = ng; g >= 1; g--) {
-            mv(aps, C(ng - g), C(ng + g - 1), 1.);
-            mv(aps + 2 * ks, C(ng - g), C(ng + g - 1), 1.);
-        }
-        for (int g = ng; g >= 1; g--)
-            for (int k = 0; k < NPR; k++) {
-                const double s = (k == U2 || k == B2) ? -1. : 1.;
-                mv(ap + k * ks, C(ng - g), C(ng + g - 1), s);
-            }
+        for (int g = ng; g >= 1; g--) mv(C(ng - g), C(ng + g - 1), sg);
         for (int jj = jref - 1; jj >= 0; jj--) {
             const long c = C(jj + ng), r = C(jref + ng);
-            ap[U2 * ks + r] += (jj + 0.5) / (jref + 0.5) * ap[U2 * ks + c];
-            ap[U2 * ks + c] = 0.;
-            for (int k : {RHO, UU, U1, U3, KTOT}) mv(ap + k * ks, c, r, 1.);
+            if (fixu2) {
+                a[r] += (jj + 0.5) / (jref + 0.5) * a[c];
+                a[c] = 0.;
+            } else if (fixrow) {
+                mv(c, r, 1.);
+            }
         }
     }
 }
@@ -732,10 +729,12 @@ struct hamr_adjoint {
     double *aF1 = nullptr, *aF2 = nullptr, *aF3 = nullptr, *aEc = nullptr, *aemf = nullptr;
     double *agam = nullptr, *J = nullptr;   // 1 double each
     double *p0 = nullptr, *ps0 = nullptr;   // the step's input state while it is reversed
-    std::vector<double *> store;            // checkpoints and segment states (12 planes each)
-    // captured graphs of one forward step (with the objective) and of one
-    // reversed step, per step size
-    std::map<double, cudaGraphExec_t> fwd_graph, bwd_graph;
+    std::vector<double *> store;            // checkpoints (12 planes each)
+    std::vector<double *> slots;            // per-step records of a segment (REC_PLANES each)
+    // captured graphs, per step size and record slot: a forward step with the
+    // objective term, a recorded forward step, a reversed step
+    using Key = std::tuple<double, const void *, const void *>;
+    std::map<Key, cudaGraphExec_t> fwd_graph, rec_graph, bwd_graph;
 };
 
 namespace {
@@ -763,21 +762,33 @@ unsigned nb(long n) { return (unsigned)((n + BLK - 1) / BLK); }
 void adj_bound(hamr_ctx *ctx, const double *pv, double *ap, double *aps) {
     const Dims &d = ctx->d;
     cudaStream_t s = ctx->stream;
-    k_adj_bound_x2_refl<<<nb(d.G1), BLK, 0, s>>>(d, ap, aps);
+    k_adj_bound_x2_refl<<<nb((long)ADJ_X2_COMPS * d.G1), BLK, 0, s>>>(d, ap, aps);
     k_adj_bound_x1_outflow<<<nb(2L * d.G2), BLK, 0, s>>>(d, geom_of(ctx), pv, ap, aps);
 }
 
-// reverse of one sub-step. pin: the stage's input primitives (p^n or ph);
-// apin/apsin: their cotangents (accumulated); apout: cotangent of the
-// inversion output (consumed); apsout: of the face field it writes.
-int adj_stage(hamr_adjoint *a, int full, double dt, double mdot_coef) {
+// what the reverse of one sub-step reads of its forward: input and output
+// primitives (ghost-filled) and face fields, the conserved update handed to
+// the inversion, the fixed face fluxes and the inversion's solver flags
+struct StageRec {
+    const double *pin, *pout, *psin, *psout, *W, *F1, *F2;
+    const int *pflag;
+};
+
+// the stage just run by the context, read from its own buffers
+StageRec ctx_stage(const hamr_ctx *ctx, int full) {
+    return full ? StageRec{ctx->ph, ctx->p, ctx->psh, ctx->ps, ctx->W, ctx->F1, ctx->F2, ctx->pflag}
+                : StageRec{ctx->p, ctx->ph, ctx->ps, ctx->psh, ctx->W, ctx->F1, ctx->F2, ctx->pflag};
+}
+
+// reverse of one sub-step. apin/apsin: cotangents of the stage's input
+// primitives and faces (accumulated); apout: of the inversion output
+// (consumed); apsout: of the face field it writes.
+int adj_stage(hamr_adjoint *a, int full, double dt, double mdot_coef, const StageRec &r) {
     hamr_ctx *ctx = a->ctx;
     const Dims &d = ctx->d;
     const Geom m = geom_of(ctx);
     cudaStream_t s = ctx->stream;
     const double Dt = full ? dt : 0.5 * dt;
-    const double *pin = full ? ctx->ph : ctx->p;
-    const double *pout = full ? ctx->p : ctx->ph;
     double *apin = full ? a->aph : a->ap, *apsin = full ? a->apsh : a->aps;
     double *apout = full ? a->ap : a->aph, *apsout = full ? a->aps : a->apsh;
     const long ks = d.ks, nz = (long)d.n1 * d.n2, nedge = (long)(d.n1 + 1) * (d.n2 + 1);
@@ -786,26 +797,83 @@ int adj_stage(hamr_adjoint *a, int full, double dt, double mdot_coef) {
     ACK(cudaMemsetAsync(a->aF2, 0, NPR * sizeof(double) * ks, s));
     ACK(cudaMemsetAsync(a->aEc, 0, 4 * sizeof(double) * ks, s));
     // ghost fill of the output, then the inversion (p_out <- W, guess pin)
-    adj_bound(ctx, pout, apout, apsout);
-    k_adj_invert<<<nb(nz), BLK, 0, s>>>(d, m, pout, pin, ctx->W, apsout == a->aps ? ctx->ps : ctx->psh,
-                                        ctx->pflag, apout, apin, a->aW, a->agam);
+    adj_bound(ctx, r.pout, apout, apsout);
+    k_adj_invert<<<nb(nz), BLK, 0, s>>>(d, m, r.pout, r.pin, r.W, r.psout, r.pflag, apout, apin, a->aW, a->agam);
     // U[B1], U[B2] from the updated faces
     k_adj_face_average<<<nb(nedge), BLK, 0, s>>>(d, m, a->aW, apsout);
     // update: U^n (cache), source at pin, flux divergence (+ objective)
     k_adj_cache_add<<<nb(nz), BLK, 0, s>>>(d, a->aW, a->aU);
-    k_adj_source<<<nb(nz), BLK, 0, s>>>(d, m, pin, a->aW, apin, Dt, a->agam);
+    k_adj_source<<<nb(nz), BLK, 0, s>>>(d, m, r.pin, a->aW, apin, Dt, a->agam);
     k_adj_divergence<1><<<nb(n_faces<1>(d)), BLK, 0, s>>>(d, a->aW, a->aF1, Dt, a->ih, full ? mdot_coef : 0.);
     k_adj_divergence<2><<<nb(n_faces<2>(d)), BLK, 0, s>>>(d, a->aW, a->aF2, Dt, -1, 0.);
     // face update: edge EMFs; ps^n -> psh carries the cotangent over
     k_adj_face_update_emf<<<nb(nedge), BLK, 0, s>>>(d, m, apsout, a->aemf, Dt);
     if (!full) k_adj_face_carry<<<nb(nedge), BLK, 0, s>>>(d, a->apsh, a->aps);
     // edge EMFs -> centre EMFs and fluxes; centre EMFs -> pin
-    k_adj_emf_edge<<<nb(nedge), BLK, 0, s>>>(d, ctx->F1, ctx->F2, a->aemf, a->aEc, a->aF1, a->aF2);
-    k_adj_emf_centre<<<nb((long)(d.n1 + 2) * (d.n2 + 2)), BLK, 0, s>>>(d, m, pin, a->aEc, apin);
+    k_adj_emf_edge<<<nb(nedge), BLK, 0, s>>>(d, r.F1, r.F2, a->aemf, a->aEc, a->aF1, a->aF2);
+    k_adj_emf_centre<<<nb((long)(d.n1 + 2) * (d.n2 + 2)), BLK, 0, s>>>(d, m, r.pin, a->aEc, apin);
     // flux fixes, then the face fluxes -> pin (and the normal face field)
-    k_adj_fix_flux<<<nb((long)d.G1 + d.G2), BLK, 0, s>>>(d, ctx->F1, a->aF1, a->aF2);
-    k_adj_flux<1><<<nb(n_faces<1>(d)), BLK, 0, s>>>(d, m, pin, full ? ctx->psh : ctx->ps, a->aF1, apin, apsin, a->agam);
-    k_adj_flux<2><<<nb(n_faces<2>(d)), BLK, 0, s>>>(d, m, pin, full ? ctx->psh : ctx->ps, a->aF2, apin, apsin, a->agam);
+    k_adj_fix_flux<<<nb((long)d.G1 + d.G2), BLK, 0, s>>>(d, r.F1, a->aF1, a->aF2);
+    k_adj_flux<1><<<nb(n_faces<1>(d)), BLK, 0, s>>>(d, m, r.pin, r.psin, a->aF1, apin, apsin, a->agam);
+    k_adj_flux<2><<<nb(n_faces<2>(d)), BLK, 0, s>>>(d, m, r.pin, r.psin, a->aF2, apin, apsin, a->agam);
+    ACK(cudaGetLastError());
+    return HAMR_OK;
+}
+
+// One step's record, REC_PLANES planes of the block: its input state (p, ps),
+// the half sub-step's output (ph, psh), each sub-step's conserved update,
+// fixed x1/x2 fluxes and solver flags (the two int planes share one).
+constexpr int REC_PLANES = 75;
+struct Slot {
+    double *p, *ps, *ph, *psh, *Wh, *Wf, *F1h, *F2h, *F1f, *F2f;
+    int *flh, *flf;
+};
+Slot slot_of(double *base, long ks) {
+    Slot r;
+    r.p = base; r.ps = base + 9 * ks; r.ph = base + 12 * ks; r.psh = base + 21 * ks;
+    r.Wh = base + 24 * ks; r.Wf = base + 31 * ks;
+    r.F1h = base + 38 * ks; r.F2h = base + 47 * ks; r.F1f = base + 56 * ks; r.F2f = base + 65 * ks;
+    r.flh = reinterpret_cast<int *>(base + 74 * ks); r.flf = r.flh + ks;
+    return r;
+}
+
+// one fixed-size step of the context that leaves its intermediates in the
+// record: the stages write their half-step state, updates, fluxes and flags
+// straight into the slot (the context's buffers are swapped for the slot's
+// while the launches are issued, and put back after)
+int record_step(hamr_adjoint *a, double dt, const Slot &r) {
+    hamr_ctx *ctx = a->ctx;
+    const Dims &d = ctx->d;
+    cudaStream_t s = ctx->stream;
+    const size_t cb = sizeof(double) * d.ks;
+    ACK(cudaMemcpyAsync(r.p, ctx->p, NPR * cb, cudaMemcpyDeviceToDevice, s));
+    ACK(cudaMemcpyAsync(r.ps, ctx->ps, 3 * cb, cudaMemcpyDeviceToDevice, s));
+    struct Swap {
+        hamr_ctx *c;
+        double *ph, *psh, *W, *F1, *F2;
+        int *pflag;
+        ~Swap() { c->ph = ph; c->psh = psh; c->W = W; c->F1 = F1; c->F2 = F2; c->pflag = pflag; }
+    } keep{ctx, ctx->ph, ctx->psh, ctx->W, ctx->F1, ctx->F2, ctx->pflag};
+    ctx->ph = r.ph; ctx->psh = r.psh;
+    ctx->W = r.Wh; ctx->F1 = r.F1h; ctx->F2 = r.F2h; ctx->pflag = r.flh;
+    int rc = launch_stage(ctx, 0, StepSize{nullptr, 0.5, 0.5 * dt, dt}, false);
+    if (rc) return rc;
+    ctx->W = r.Wf; ctx->F1 = r.F1f; ctx->F2 = r.F2f; ctx->pflag = r.flf;
+    return launch_stage(ctx, 1, StepSize{nullptr, 1.0, dt, dt}, false);
+}
+
+// reverse of a whole step from the records of its two sub-steps
+int adj_step(hamr_adjoint *a, double dt, double w, const StageRec &half, const StageRec &full) {
+    hamr_ctx *ctx = a->ctx;
+    const Dims &d = ctx->d;
+    cudaStream_t s = ctx->stream;
+    const size_t cb = sizeof(double) * d.ks;
+    ACK(cudaMemsetAsync(a->aph, 0, NPR * cb, s));
+    ACK(cudaMemsetAsync(a->apsh, 0, 3 * cb, s));
+    int rc = adj_stage(a, 1, dt, -w * d.dx2 * d.dx3, full);
+    if (rc) return rc;
+    if ((rc = adj_stage(a, 0, dt, 0., half))) return rc;
+    k_adj_cons_of_state<<<nb((long)d.n1 * d.n2), BLK, 0, s>>>(d, geom_of(ctx), half.pin, a->aU, a->ap, a->agam);
     ACK(cudaGetLastError());
     return HAMR_OK;
 }
@@ -814,6 +882,9 @@ int adj_stage(hamr_adjoint *a, int full, double dt, double mdot_coef) {
 
 namespace {
 
+// reverse of the step taken from the context's current state, recomputing
+// its forward: the full sub-step is reversed from the context's buffers right
+// after the step, the half sub-step after re-running it from the saved input
 int step_backward(hamr_adjoint *a, double dt, double w) {
     hamr_ctx *ctx = a->ctx;
     const Dims &d = ctx->d;
@@ -825,12 +896,11 @@ int step_backward(hamr_adjoint *a, double dt, double w) {
     if (rc) return rc;
     ACK(cudaMemsetAsync(a->aph, 0, NPR * cb, s));
     ACK(cudaMemsetAsync(a->apsh, 0, 3 * cb, s));
-    if ((rc = adj_stage(a, 1, dt, -w * d.dx2 * d.dx3))) return rc;
-    // back to the step's input; redo its half sub-step for the intermediates
+    if ((rc = adj_stage(a, 1, dt, -w * d.dx2 * d.dx3, ctx_stage(ctx, 1)))) return rc;
     ACK(cudaMemcpyAsync(ctx->p, a->p0, NPR * cb, cudaMemcpyDeviceToDevice, s));
     ACK(cudaMemcpyAsync(ctx->ps, a->ps0, 3 * cb, cudaMemcpyDeviceToDevice, s));
     if ((rc = launch_stage(ctx, 0, StepSize{nullptr, 0.5, 0.5 * dt, dt}, false))) return rc;
-    if ((rc = adj_stage(a, 0, dt, 0.))) return rc;
+    if ((rc = adj_stage(a, 0, dt, 0., ctx_stage(ctx, 0)))) return rc;
     k_adj_cons_of_state<<<nb((long)d.n1 * d.n2), BLK, 0, s>>>(d, geom_of(ctx), ctx->p, a->aU, a->ap, a->agam);
     ACK(cudaGetLastError());
     return HAMR_OK;
@@ -839,9 +909,10 @@ int step_backward(hamr_adjoint *a, double dt, double w) {
 // forward step + objective term, and reversed step, replayed from graphs
 // captured once per step size (the step is launch-bound at these sizes)
 template <class F>
-int graph_run(hamr_adjoint *a, std::map<double, cudaGraphExec_t> &cache, double dt, F body) {
+int graph_run(hamr_adjoint *a, std::map<hamr_adjoint::Key, cudaGraphExec_t> &cache, hamr_adjoint::Key key,
+              F body) {
     cudaStream_t s = a->ctx->stream;
-    auto it = cache.find(dt);
+    auto it = cache.find(key);
     if (it == cache.end()) {
         cudaGraph_t g;
         ACK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -853,14 +924,14 @@ int graph_run(hamr_adjoint *a, std::map<double, cudaGraphExec_t> &cache, double 
         e = cudaGraphInstantiate(&x, g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return afail(a, e, "cudaGraphInstantiate");
-        it = cache.emplace(dt, x).first;
+        it = cache.emplace(key, x).first;
     }
     ACK(cudaGraphLaunch(it->second, s));
     return HAMR_OK;
 }
 
 int fwd_step(hamr_adjoint *a, double dt) {
-    return graph_run(a, a->fwd_graph, dt, [&]() -> int {
+    return graph_run(a, a->fwd_graph, {dt, nullptr, nullptr}, [&]() -> int {
         const int rc = fixed_step(a->ctx, dt);
         if (rc) return rc;
         k_mdot_accum<<<nb(a->ctx->d.n2), BLK, 0, a->ctx->stream>>>(a->ctx->d, a->ctx->F1, a->ih, dt, a->J);
@@ -868,8 +939,19 @@ int fwd_step(hamr_adjoint *a, double dt) {
     });
 }
 
-int bwd_step(hamr_adjoint *a, double dt) {
-    return graph_run(a, a->bwd_graph, dt, [&]() -> int { return step_backward(a, dt, dt); });
+int rec_step(hamr_adjoint *a, double dt, double *slot) {
+    return graph_run(a, a->rec_graph, {dt, slot, nullptr},
+                     [&]() -> int { return record_step(a, dt, slot_of(slot, a->ctx->d.ks)); });
+}
+
+// reversed step from slot's record; next_p/next_ps: the step's output state
+int bwd_step(hamr_adjoint *a, double dt, double *slot, const double *next_p, const double *next_ps) {
+    return graph_run(a, a->bwd_graph, {dt, slot, next_p}, [&]() -> int {
+        const Slot r = slot_of(slot, a->ctx->d.ks);
+        const StageRec half{r.p, r.ph, r.ps, r.psh, r.Wh, r.F1h, r.F2h, r.flh};
+        const StageRec full{r.ph, next_p, r.psh, next_ps, r.Wf, r.F1f, r.F2f, r.flf};
+        return adj_step(a, dt, dt, half, full);
+    });
 }
 
 int bound_ctx(hamr_ctx *ctx) {
@@ -878,7 +960,7 @@ int bound_ctx(hamr_ctx *ctx) {
     const Geom m = geom_of(ctx);
     if (d.d1) k_bound_x1<<<nblk((long)d.ng1 * d.G2 * d.G3), BLK, 0, s>>>(d, m, ctx->p, ctx->ps);
     if (d.d3) k_bound_x3<<<nblk((long)d.ng3 * d.G1 * d.G2), BLK, 0, s>>>(d, ctx->p, ctx->ps);
-    if (d.d2) k_bound_x2<<<nblk((long)d.G1 * d.G3), BLK, 0, s>>>(d, ctx->p, ctx->ps);
+    if (d.d2) k_bound_x2<<<nblk(n_bound_x2(d)), BLK, 0, s>>>(d, ctx->p, ctx->ps);
     return cudaGetLastError() == cudaSuccess ? HAMR_OK : HAMR_E_CUDA;
 }
 
@@ -929,8 +1011,9 @@ int hamr_adjoint_destroy(hamr_adjoint *a) {
                       a->agam, a->J, a->p0, a->ps0})
         cudaFree(p);
     for (double *p : a->store) cudaFree(p);
-    for (auto &kv : a->fwd_graph) cudaGraphExecDestroy(kv.second);
-    for (auto &kv : a->bwd_graph) cudaGraphExecDestroy(kv.second);
+    for (double *p : a->slots) cudaFree(p);
+    for (auto *g : {&a->fwd_graph, &a->rec_graph, &a->bwd_graph})
+        for (auto &kv : *g) cudaGraphExecDestroy(kv.second);
     delete a;
     return HAMR_OK;
 }
@@ -981,8 +1064,9 @@ int hamr_mdot_forward(hamr_adjoint *a, int nsteps, const double *dt, double *J) 
 // respect to the initial state (active primitives and face field, before
 // the ghost fill) and the adiabatic index. Checkpoints the state every
 // `every` steps on the forward sweep, and reverses segment by segment: each
-// segment is recomputed from its checkpoint, keeping its per-step inputs,
-// then stepped backwards. grad_p (9 planes) / grad_ps (3 planes) are host
+// segment is recomputed from its checkpoint, recording every step's
+// intermediates, then its steps are reversed from those records (no forward
+// work in the reverse). grad_p (9 planes) / grad_ps (3 planes) are host
 // arrays in the context's layout (NULL: not copied). The context's state is
 // restored to its initial value on return.
 int hamr_adjoint_run(hamr_adjoint *a, int nsteps, const double *dt, int every, double *J, double *grad_p,
@@ -995,11 +1079,16 @@ int hamr_adjoint_run(hamr_adjoint *a, int nsteps, const double *dt, int every, d
     cudaStream_t s = ctx->stream;
     const size_t cb = sizeof(double) * d.ks, state = 12 * cb;
     const int nseg = (nsteps + every - 1) / every;
-    const size_t need = (size_t)nseg + 1 + every;   // checkpoints + initial pre-fill copy + segment states
-    while (a->store.size() < need) {
+    const int seglen = every < nsteps ? every : nsteps;
+    while (a->store.size() < (size_t)nseg + 1) {   // checkpoints + the initial pre-fill copy
         double *p = nullptr;
         if (cudaMalloc((void **)&p, state) != cudaSuccess) return HAMR_E_NOMEM;
         a->store.push_back(p);
+    }
+    while (a->slots.size() < (size_t)seglen) {
+        double *p = nullptr;
+        if (cudaMalloc((void **)&p, REC_PLANES * cb) != cudaSuccess) return HAMR_E_NOMEM;
+        a->slots.push_back(p);
     }
     auto save = [&](double *dst) {
         cudaMemcpyAsync(dst, ctx->p, NPR * cb, cudaMemcpyDeviceToDevice, s);
@@ -1010,7 +1099,6 @@ int hamr_adjoint_run(hamr_adjoint *a, int nsteps, const double *dt, int every, d
         cudaMemcpyAsync(ctx->ps, src + NPR * d.ks, 3 * cb, cudaMemcpyDeviceToDevice, s);
     };
     double *initial = a->store[nseg];
-    double **seg = a->store.data() + nseg + 1;
     save(initial);
     // forward sweep with checkpoints
     ACK(cudaMemsetAsync(a->J, 0, sizeof(double), s));
@@ -1023,18 +1111,17 @@ int hamr_adjoint_run(hamr_adjoint *a, int nsteps, const double *dt, int every, d
     double Jval = 0.;
     ACK(cudaMemcpyAsync(&Jval, a->J, sizeof(double), cudaMemcpyDeviceToHost, s));
     ACK(cudaStreamSynchronize(s));
-    // reverse sweep
+    // reverse sweep: recompute each segment with records, then reverse it;
+    // the last step of a segment ends in the context's own state
     if ((rc = hamr_adjoint_zero(a))) return rc;
     for (int sg = nseg - 1; sg >= 0 && rc == HAMR_OK; sg--) {
         const int n0 = sg * every, n1 = n0 + every < nsteps ? n0 + every : nsteps;
         load(a->store[sg]);
-        for (int n = n0; n < n1 && rc == HAMR_OK; n++) {
-            save(seg[n - n0]);
-            if (n + 1 < n1) rc = fwd_step(a, dt[n]);   // (adds to J's device copy: the value was taken above)
-        }
+        for (int n = n0; n < n1 && rc == HAMR_OK; n++) rc = rec_step(a, dt[n], a->slots[n - n0]);
         for (int n = n1 - 1; n >= n0 && rc == HAMR_OK; n--) {
-            load(seg[n - n0]);
-            rc = bwd_step(a, dt[n]);
+            const bool last = n == n1 - 1;
+            const Slot nx = slot_of(a->slots[last ? 0 : n + 1 - n0], d.ks);
+            rc = bwd_step(a, dt[n], a->slots[n - n0], last ? ctx->p : nx.p, last ? ctx->ps : nx.ps);
         }
     }
     if (rc) return rc;

@@ -22,6 +22,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/hamr_b200.h"
@@ -755,104 +756,69 @@ __global__ void k_bound_x3(const Dims d, double *pv, double *ps) {
     k_bound_x3_at(d, pv, ps, t);
 }
 
-// x2 ghosts over every (i, z): periodic, transmissive or reflective polar
-// axis, or plain outflow copy
+// x2 ghosts: periodic, transmissive or reflective polar axis, or plain
+// outflow copy. One item per (component, i, z), components being the NPR
+// primitives and then the 3 face-field planes: every rule acts on one
+// component at a time, so the items are independent, and the two poles of a
+// column are filled in order by the same item (with very few rows the
+// reflective-axis rows of one pole feed the other's).
+constexpr int X2_COMPS = NPR + 3;
+__host__ __device__ __forceinline__ long n_bound_x2(const Dims &d) { return (long)X2_COMPS * d.G1 * d.G3; }
+
 __device__ __forceinline__ void k_bound_x2_at(const Dims &d, double *pv, double *ps, const long t) {
-    const int z = (int)(t % d.G3), i = (int)(t / d.G3);
+    const int z = (int)(t % d.G3), i = (int)((t / d.G3) % d.G1), comp = (int)(t / ((long)d.G3 * d.G1));
     const int n2 = d.n2, ng = d.ng2;
-    const long ks = d.ks;
+    const bool face = comp >= NPR;
+    const int k = face ? comp - NPR : comp;
+    double *a = (face ? ps : pv) + (long)k * d.ks;
+    auto C = [&](int j, int zz) { return cix(d, i, j, zz); };
     if (d.bc2 == HAMR_BC_PERIODIC) {
         for (int g = 0; g < ng; g++) {
-            const long lo = cix(d, i, g, z), lo_src = cix(d, i, g + n2, z);
-            const long hi = cix(d, i, n2 + ng + g, z), hi_src = cix(d, i, ng + g, z);
-            copy_cell(d, pv, lo, lo_src);
-            copy_cell(d, pv, hi, hi_src);
-            for (int k = 0; k < 3; k++) {
-                ps[k * ks + lo] = ps[k * ks + lo_src];
-                ps[k * ks + hi] = ps[k * ks + hi_src];
-            }
+            a[C(g, z)] = a[C(g + n2, z)];
+            a[C(n2 + ng + g, z)] = a[C(ng + g, z)];
         }
     } else if (d.bc2 == HAMR_BC_POLE_TRANS) {
+        if (face && k == 1) return;
         const int zs = d.d3 ? (z - d.ng3 + d.n3 / 2) % d.n3 + d.ng3 : z;
+        const double sg = face ? (k == 2 ? -1. : 1.) : ((k == U2 || k == U3 || k == B2 || k == B3) ? -1. : 1.);
         if (d.pole1)
-            for (int jj = -ng; jj < 0; jj++) {
-                const long dst = cix(d, i, jj + ng, z), src = cix(d, i, -jj - 1 + ng, zs);
-                copy_cell(d, pv, dst, src);
-                pv[U2 * ks + dst] *= -1.0;
-                pv[U3 * ks + dst] *= -1.0;
-                pv[B2 * ks + dst] *= -1.0;
-                pv[B3 * ks + dst] *= -1.0;
-                ps[0 * ks + dst] = ps[0 * ks + src];
-                ps[2 * ks + dst] = -ps[2 * ks + src];
-            }
+            for (int jj = -ng; jj < 0; jj++) a[C(jj + ng, z)] = sg * a[C(-jj - 1 + ng, zs)];
         if (d.pole2)
-            for (int jj = n2; jj < n2 + ng; jj++) {
-                const long dst = cix(d, i, jj + ng, z), src = cix(d, i, 2 * n2 - jj - 1 + ng, zs);
-                copy_cell(d, pv, dst, src);
-                pv[U2 * ks + dst] *= -1.0;
-                pv[U3 * ks + dst] *= -1.0;
-                pv[B2 * ks + dst] *= -1.0;
-                pv[B3 * ks + dst] *= -1.0;
-                ps[0 * ks + dst] = ps[0 * ks + src];
-                ps[2 * ks + dst] = -ps[2 * ks + src];
-            }
+            for (int jj = n2; jj < n2 + ng; jj++) a[C(jj + ng, z)] = sg * a[C(2 * n2 - jj - 1 + ng, zs)];
     } else if (d.bc2 == HAMR_BC_POLE_REFL) {
+        if (face && k == 1) return;
         const int jref = 2;  // POLEFIX, config.h:490
+        const bool fixrow = !face && (k == RHO || k == UU || k == U1 || k == U3 || k == KTOT);
+        const bool fixu2 = !face && k == U2;
+        const double sg = (!face && (k == U2 || k == B2)) ? -1. : 1.;
         if (d.pole1) {
+            const double vr = a[C(jref + ng, z)];
             for (int jj = 0; jj < jref; jj++) {
-                const long c = cix(d, i, jj + ng, z), r = cix(d, i, jref + ng, z);
-                pv[U2 * ks + c] = (jj + 0.5) / (jref + 0.5) * pv[U2 * ks + r];
-                pv[RHO * ks + c] = pv[RHO * ks + r];
-                pv[UU * ks + c] = pv[UU * ks + r];
-                pv[U1 * ks + c] = pv[U1 * ks + r];
-                pv[U3 * ks + c] = pv[U3 * ks + r];
-                pv[KTOT * ks + c] = pv[KTOT * ks + r];
+                if (fixu2) a[C(jj + ng, z)] = (jj + 0.5) / (jref + 0.5) * vr;
+                else if (fixrow) a[C(jj + ng, z)] = vr;
             }
-            for (int g = 1; g <= ng; g++) copy_cell(d, pv, cix(d, i, ng - g, z), cix(d, i, ng + g - 1, z));
-            for (int jj = 0; jj < ng; jj++) {
-                pv[U2 * ks + cix(d, i, jj, z)] *= -1.;
-                pv[B2 * ks + cix(d, i, jj, z)] *= -1.;
-            }
-            for (int g = 1; g <= ng; g++) {
-                ps[0 * ks + cix(d, i, ng - g, z)] = ps[0 * ks + cix(d, i, ng + g - 1, z)];
-                ps[2 * ks + cix(d, i, ng - g, z)] = ps[2 * ks + cix(d, i, ng + g - 1, z)];
-            }
+            for (int g = 1; g <= ng; g++) a[C(ng - g, z)] = sg * a[C(ng + g - 1, z)];
         }
         if (d.pole2) {
+            const double vr = a[C(n2 + ng - 1 - jref, z)];
             for (int jj = 0; jj < jref; jj++) {
-                const long c = cix(d, i, n2 + ng - 1 - jj, z), r = cix(d, i, n2 + ng - 1 - jref, z);
-                pv[U2 * ks + c] = (jj + 0.5) / (jref + 0.5) * pv[U2 * ks + r];
-                pv[RHO * ks + c] = pv[RHO * ks + r];
-                pv[UU * ks + c] = pv[UU * ks + r];
-                pv[U1 * ks + c] = pv[U1 * ks + r];
-                pv[U3 * ks + c] = pv[U3 * ks + r];
-                pv[KTOT * ks + c] = pv[KTOT * ks + r];
+                if (fixu2) a[C(n2 + ng - 1 - jj, z)] = (jj + 0.5) / (jref + 0.5) * vr;
+                else if (fixrow) a[C(n2 + ng - 1 - jj, z)] = vr;
             }
-            for (int g = 0; g < ng; g++) copy_cell(d, pv, cix(d, i, n2 + ng + g, z), cix(d, i, n2 + ng - 1 - g, z));
-            for (int jj = n2 + ng; jj < n2 + 2 * ng; jj++) {
-                pv[U2 * ks + cix(d, i, jj, z)] *= -1.;
-                pv[B2 * ks + cix(d, i, jj, z)] *= -1.;
-            }
-            for (int g = 0; g < ng; g++) {
-                ps[0 * ks + cix(d, i, n2 + ng + g, z)] = ps[0 * ks + cix(d, i, n2 + ng - 1 - g, z)];
-                ps[2 * ks + cix(d, i, n2 + ng + g, z)] = ps[2 * ks + cix(d, i, n2 + ng - 1 - g, z)];
-            }
+            for (int g = 0; g < ng; g++) a[C(n2 + ng + g, z)] = sg * a[C(n2 + ng - 1 - g, z)];
         }
     } else {
+        if (face && k == 1) return;
         for (int g = 0; g < ng; g++) {
-            copy_cell(d, pv, cix(d, i, g, z), cix(d, i, ng, z));
-            copy_cell(d, pv, cix(d, i, n2 + ng + g, z), cix(d, i, n2 + ng - 1, z));
-            ps[0 * ks + cix(d, i, g, z)] = ps[0 * ks + cix(d, i, ng, z)];
-            ps[2 * ks + cix(d, i, g, z)] = ps[2 * ks + cix(d, i, ng, z)];
-            ps[0 * ks + cix(d, i, n2 + ng + g, z)] = ps[0 * ks + cix(d, i, n2 + ng - 1, z)];
-            ps[2 * ks + cix(d, i, n2 + ng + g, z)] = ps[2 * ks + cix(d, i, n2 + ng - 1, z)];
+            a[C(g, z)] = a[C(ng, z)];
+            a[C(n2 + ng + g, z)] = a[C(n2 + ng - 1, z)];
         }
     }
 }
 
 __global__ void k_bound_x2(const Dims d, double *pv, double *ps) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)d.G1 * d.G3) return;
+    if (t >= n_bound_x2(d)) return;
     k_bound_x2_at(d, pv, ps, t);
 }
 
@@ -1032,7 +998,7 @@ k_cons<T><<<nblk(n), BLK, 0, s>>>(d, m, ctx->p, full ? ctx->ph : ctx->p, ctx->U,
     double *psw = full ? ctx->ps : ctx->psh;
     if (d.d1) k_bound_x1<<<nblk((long)d.ng1 * d.G2 * d.G3), BLK, 0, s>>>(d, m, pw, psw);
     if (d.d3) k_bound_x3<<<nblk((long)d.ng3 * d.G1 * d.G2), BLK, 0, s>>>(d, pw, psw);
-    if (d.d2) k_bound_x2<<<nblk((long)d.G1 * d.G3), BLK, 0, s>>>(d, pw, psw);
+    if (d.d2) k_bound_x2<<<nblk(n_bound_x2(d)), BLK, 0, s>>>(d, pw, psw);
     prof_mark(pf, PROF_BOUND, s);
     CK(cudaGetLastError());
     return HAMR_OK;
@@ -1192,7 +1158,7 @@ int hamr_bound(hamr_ctx *ctx) {
     const Geom m = geom_of(ctx);
     if (d.d1) k_bound_x1<<<nblk((long)d.ng1 * d.G2 * d.G3), BLK, 0, ctx->stream>>>(d, m, ctx->p, ctx->ps);
     if (d.d3) k_bound_x3<<<nblk((long)d.ng3 * d.G1 * d.G2), BLK, 0, ctx->stream>>>(d, ctx->p, ctx->ps);
-    if (d.d2) k_bound_x2<<<nblk((long)d.G1 * d.G3), BLK, 0, ctx->stream>>>(d, ctx->p, ctx->ps);
+    if (d.d2) k_bound_x2<<<nblk(n_bound_x2(d)), BLK, 0, ctx->stream>>>(d, ctx->p, ctx->ps);
     CK(cudaGetLastError());
     return HAMR_OK;
 }

@@ -50,6 +50,24 @@ template <typename T> __device__ __forceinline__ T d_pow(T x, T y);
 template <> __device__ __forceinline__ double d_pow<double>(double x, double y) { return pow(x, y); }
 template <> __device__ __forceinline__ float d_pow<float>(float x, float y) { return powf(x, y); }
 template <typename T> __device__ __forceinline__ T d_fabs(T x) { return x < T(0) ? -x : x; }
+// x^(-1/2), correctly rounded in all but vanishingly rare near-midpoint cases,
+// so that it agrees with a correctly rounded host pow(x, -0.5): the IEEE
+// quotient 1/sqrt(x) (within about one ulp) takes one Newton step
+// y + y (1 - x y^2) / 2 whose residual is formed exactly with fused
+// multiply-adds (y^2 = h + l split by an fma, then 1 - x h - x l), leaving
+// an error near 2^-104 relative before the final rounding (Newton-Raphson
+// refinement of the reciprocal square root with an fma residual, as in
+// Markstein's IA-64 division and square-root algorithms).
+template <typename T> __device__ __forceinline__ T d_rsqrt(T x);
+template <> __device__ __forceinline__ double d_rsqrt<double>(double x) {
+    if (!(x > 1.0e-300) || x > 1.0e300) return pow(x, -0.5);   // y*y would leave the normal range: the plain pow
+    const double y = 1. / sqrt(x);
+    const double h = y * y;
+    const double l = fma(y, y, -h);
+    const double r = fma(-x, l, fma(-x, h, 1.));
+    return fma(0.5 * y, r, y);
+}
+template <> __device__ __forceinline__ float d_rsqrt<float>(float x) { return powf(x, -0.5f); }
 template <typename T> __device__ __forceinline__ T d_max(T a, T b) { return a > b ? a : b; }
 template <typename T> __device__ __forceinline__ T d_min(T a, T b) { return a < b ? a : b; }
 
@@ -660,10 +678,10 @@ __device__ __forceinline__ void set_mud(const Geo<T> &gm, int dir, T Mud[4][4], 
     const int d = dir, e = dir % 3 + 1, f = (dir + 1) % 3 + 1;
 #define GU(a, b) gm.gcon[sym4(a, b)]
 #define GD(a, b) gm.gcov[sym4(a, b)]
-    const T A = -d_pow(-GU(0, 0), T(-0.5));
-    const T B = d_pow((GU(0, 0)) * (GU(0, 0) * GU(d, d) - GU(0, d) * GU(0, d)), T(-0.5));
-    const T C = d_pow(GD(f, f), T(-0.5));
-    const T D = d_pow((GD(f, f)) * (GD(e, e) * GD(f, f) - GD(e, f) * GD(e, f)), T(-0.5));
+    const T A = -d_rsqrt(-GU(0, 0));
+    const T B = d_rsqrt((GU(0, 0)) * (GU(0, 0) * GU(d, d) - GU(0, d) * GU(0, d)));
+    const T C = d_rsqrt(GD(f, f));
+    const T D = d_rsqrt((GD(f, f)) * (GD(e, e) * GD(f, f) - GD(e, f) * GD(e, f)));
     for (int a = 0; a < 4; a++)
         for (int b = 0; b < 4; b++) Mud[a][b] = Mi[a][b] = T(0.);
     Mud[0][0] = A * GU(0, 0);
@@ -795,7 +813,7 @@ __device__ __forceinline__ void hllc_mhd(int dir, const T *lu, const T *ru, T iv
     vcon[G_3] = (FH[0][B_3] * vcon[G_1] - FH[1][B_3]) / FH[0][B_1];
     const T gammasq = T(1.) / (T(1.) - (vcon[1] * vcon[1] + vcon[2] * vcon[2] + vcon[3] * vcon[3]));
     const T vB = (vcon[1] * FH[0][B1] + vcon[2] * FH[0][B2] + vcon[3] * FH[0][B3]);
-    const T ptot = -(-FH[1][UU] - FH[0][B_1] * (vB)) * vcon[dir] + FH[1][U_1] + d_pow(FH[0][B_1], T(2.0)) / gammasq;
+    const T ptot = -(-FH[1][UU] - FH[0][B_1] * (vB)) * vcon[dir] + FH[1][U_1] + FH[0][B_1] * FH[0][B_1] / gammasq;   // pow(x, 2): x*x is its correctly rounded value
     if (!(d_fabs(ptot) > T(0.)) || (vcon[G_1] < cmin) || (vcon[G_1] > cmax) || !(d_fabs(vcon[G_1]) > T(0.))) fail = true;
     if (cmax > iv && vcon[dir] <= iv && !fail) {
         FT[0][RHO] = (cmax - ru[dir] / ru[0]) / (cmax - vcon[dir] + T(SMALL_D)) * Ur[RHO];

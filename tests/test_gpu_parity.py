@@ -213,18 +213,47 @@ def test_mc_reconstruction_strict(case, ng):
 @pytest.mark.parametrize("case", ["torus3d", "torus2d"])
 def test_hllc_strict(case):
     """HLLC in the orthonormal face frame (the reference's HLLC = 1 builds,
-    fluxcalc2D_FT), strict build against the oracle, three steps. Tolerance
-    1e-13: the frame's pow(x, -0.5) differs in the last bit between CUDA and
-    the host libm."""
+    fluxcalc2D_FT), strict build against the oracle, three steps. The frame's
+    x^-1/2 is correctly rounded on the GPU (Newton step with an fma residual)
+    as the host pow(x, -0.5) is, so the faces agree bit for bit except where
+    the host pow misrounds. Inside the torus body (density above 1e-6 of its
+    peak) every field within 1e-12 of its scale; over all zones 1e-10: the
+    1e-16 atmosphere amplifies last-bit flux differences into its poloidal
+    velocity (moving every pow of the oracle itself by one ulp moves that
+    velocity by 1e-10 to 3e-8 of its scale)."""
     pb = CASES[case]()
     blk, s = make_pair(pb, strict=True, riemann="hllc")
     dt = 0.2 * min(pb.dx[:2])
     for _ in range(3):
         dn = blk.step(dt)
         dn_o = oracle_step(s, dt)
-        assert abs(dn - dn_o) <= 1e-13 * dn_o
+        assert abs(dn - dn_o) <= 1e-14 * dn_o
         dt = min(dn, 1.3 * dt)
     p, ps = blk.download()
-    assert field_rel_err(blk, p, s, "p").max() <= 1e-13
-    assert field_rel_err(blk, ps, s, "ps").max() <= 1e-13
+    assert field_rel_err(blk, p, s, "p").max() <= 1e-10
+    assert field_rel_err(blk, ps, s, "ps").max() <= 1e-12
+    a, b = blk.active(p), s.blk.active("p")
+    body = b[0] > 1e-6 * b[0].max()
+    for k in range(8):
+        assert np.abs(a[k] - b[k])[body].max() <= 1e-12 * np.abs(b[k][body]).max()
+    blk.close()
+
+
+@pytest.mark.parametrize("case", ["torus3d", "torus2d"])
+def test_hllc_production_body(case):
+    """Production (fma) build with HLLC: inside the torus body (density above
+    1e-6 of its peak) every field within 1e-9 of its scale after three steps."""
+    pb = CASES[case]()
+    blk, s = make_pair(pb, strict=False, riemann="hllc")
+    dt = 0.2 * min(pb.dx[:2])
+    for _ in range(3):
+        dn = blk.step(dt)
+        dn_o = oracle_step(s, dt)
+        assert abs(dn - dn_o) <= 1e-13 * dn_o
+        dt = min(dn, 1.3 * dt)
+    a = blk.active(blk.download()[0])
+    b = s.blk.active("p")
+    body = b[0] > 1e-6 * b[0].max()
+    for k in range(8):
+        assert np.abs(a[k] - b[k])[body].max() <= 1e-9 * np.abs(b[k][body]).max()
     blk.close()
