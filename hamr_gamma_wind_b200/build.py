@@ -12,8 +12,10 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 SOURCES = [os.path.join(CSRC, "hamr_kernels.cu"), os.path.join(CSRC, "hamr_geometry.cpp")]
-DEPS = SOURCES + [os.path.abspath(__file__), os.path.join(CSRC, "hamr_physics.cuh"),
-                  os.path.join(os.path.dirname(HERE), "include", "hamr_b200.h")]
+# every source and header the library is compiled from (the .cuh files are
+# included into hamr_kernels.cu)
+DEPS = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".cpp", ".h"))) + [
+    os.path.abspath(__file__), os.path.join(os.path.dirname(HERE), "include", "hamr_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 

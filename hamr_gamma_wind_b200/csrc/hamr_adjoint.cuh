@@ -23,10 +23,7 @@ constexpr int ADJ_NP = 8;   // differentiated primitives: RHO, UU, U1-3, B1-3 (K
 // --- templated copies of the double-only forward helpers ------------------
 // (the same operations as inflow_check and source in this file)
 template <typename T>
-__device__ __forceinline__ void inflow_check_t(T *pr, const Geo<double> &g0, int type) {
-    Geo<T> gm;
-    for (int s = 0; s < 10; s++) { gm.gcov[s] = T(g0.gcov[s]); gm.gcon[s] = T(g0.gcon[s]); }
-    gm.g = T(g0.g);
+__device__ __forceinline__ void inflow_check_t(T *pr, const Geo<double> &gm, int type) {
     T ucon[4], gamma;
     ucon_calc(pr, gm, ucon);
     if (((ucon[1] > T(0.)) && (type == 0)) || ((ucon[1] < T(0.)) && (type == 1))) {
@@ -34,8 +31,8 @@ __device__ __forceinline__ void inflow_check_t(T *pr, const Geo<double> &g0, int
         pr[U1] /= gamma;
         pr[U2] /= gamma;
         pr[U3] /= gamma;
-        const double alpha = 1. / sqrt(-g0.gcon[0]);
-        const double beta1 = g0.gcon[1] * alpha * alpha;
+        const double alpha = 1. / sqrt(-gm.gcon[0]);
+        const double beta1 = gm.gcon[1] * alpha * alpha;
         pr[U1] = T(beta1 / alpha);
         T vsq = gm.gcov[4] * pr[U1] * pr[U1];
         vsq += T(2.) * gm.gcov[5] * pr[U2] * pr[U1];
@@ -52,8 +49,8 @@ __device__ __forceinline__ void inflow_check_t(T *pr, const Geo<double> &g0, int
     }
 }
 
-template <typename T>
-__device__ __forceinline__ void source_t(T gam, const T *ph, const Geo<T> &gm, const Dims &d, const Geom &m,
+template <typename T, typename G>
+__device__ __forceinline__ void source_t(T gam, const T *ph, const Geo<G> &gm, const Dims &d, const Geom &m,
                                          long gi, T *dU, const State<T> &q) {
     T mhd[4][4];
     const long gs = d.gs;
@@ -89,23 +86,19 @@ __device__ __forceinline__ void source_t(T gam, const T *ph, const Geo<T> &gm, c
     dU[KTOT] *= gm.g;
 }
 
-template <int N>
-__device__ __forceinline__ void geo_const(const Geo<double> &g0, Geo<Dual<N>> &g) {
-    for (int s = 0; s < 10; s++) { g.gcov[s] = Dual<N>(g0.gcov[s]); g.gcon[s] = Dual<N>(g0.gcon[s]); }
-    g.g = Dual<N>(g0.g);
-}
-
 // inputs of a state map: the ADJ_NP primitives, then gamma (index ADJ_NP)
+// (every index compile-time after unrolling, so the duals stay in registers)
 template <int N>
 __device__ __forceinline__ void seed_state(const double *pr, double gam, int pass, Dual<N> *pd, Dual<N> &gd) {
-    for (int k = 0; k < NPR; k++) pd[k] = Dual<N>(pr[k]);
-    for (int q = 0; q < N; q++) {
-        const int in = pass * N + q;
-        if (in < ADJ_NP) pd[in].d[q] = 1.;
+#pragma unroll
+    for (int k = 0; k < NPR; k++) {
+        pd[k].v = pr[k];
+#pragma unroll
+        for (int q = 0; q < N; q++) pd[k].d[q] = (k < ADJ_NP && k == pass * N + q) ? 1. : 0.;
     }
-    gd = Dual<N>(gam);
-    const int qg = ADJ_NP - pass * N;
-    if (qg >= 0 && qg < N) gd.d[qg] = 1.;
+    gd.v = gam;
+#pragma unroll
+    for (int q = 0; q < N; q++) gd.d[q] = (ADJ_NP == pass * N + q) ? 1. : 0.;
 }
 
 __device__ __forceinline__ void block_add(double v, double *target) {
@@ -118,43 +111,266 @@ __device__ __forceinline__ void block_add(double v, double *target) {
 
 namespace {
 
-// one side of a face: (fluxes along DIR, conserved variables, fast speeds) of
-// the reconstructed state ps; returns ps_bar (ADJ_NP) and adds to gam_bar,
-// given the cotangents of those outputs
-template <int DIR>
-__device__ void side_vjp(const double *pside, const Geo<double> &g0, double gam, const double *tfb,
-                         const double *tub, double cmxb, double cmnb, double *pbar, double &gbar) {
-    constexpr int N = 3;
-    Geo<Dual<N>> gm;
-    geo_const(g0, gm);
-    for (int pass = 0; pass * N <= ADJ_NP; pass++) {
-        Dual<N> pd[NPR], gd;
-        seed_state(pside, gam, pass, pd, gd);
-        State<Dual<N>> q;
-        get_state(pd, gm, q);
-        const Dual<N> e = entropy(gd, pd);
-        Dual<N> tf[NPR], tu[NPR], cmx, cmn, vd;
-        primtoflux(gd, pd, q, DIR, gm, e, tf, &cmx, &cmn);
-        primtoflux(gd, pd, q, 0, gm, e, tu, &vd, &vd);
-        for (int qd = 0; qd < N; qd++) {
-            const int in = pass * N + qd;
-            if (in > ADJ_NP) break;
-            double s = cmxb * cmx.d[qd] + cmnb * cmn.d[qd];
-            for (int k = 0; k < NPR; k++) s += tfb[k] * tf[k].d[qd] + tub[k] * tu[k].d[qd];
-            if (in < ADJ_NP) pbar[in] = s;
-            else gbar += s;
-        }
+// ---- reverse mode of one state's fluxes, conserved variables and speeds ----
+// Hand-written transpose of get_state + primtoflux (GPU_phys_mhd.h:432-628,
+// 672-761) over a constant metric: the forward values are recomputed, then
+// the cotangents run back through the flux formulas, the magnetosonic
+// quadratic, the scalars (w, P, b^2, eta, ptot, entropy K), b_mu, b^mu, u_mu,
+// u^mu and gamma, in the branch the forward took (clamped speeds and a
+// clamped Lorentz factor pass no derivative).
+struct StateBar {
+    double ucon[4], ucov[4], bcon[4], bcov[4];
+    double rho, u, gam, eta, ptot, w, P, bsq, K;
+};
+
+// flux along D (D == 0: conserved variables) reversed, given the cotangent cb
+template <int D>
+__device__ __forceinline__ void flux_rev(const double *pr, const State<double> &q, double g, double eta, double K,
+                                         const double *cb, StateBar &a) {
+    double c[NPR];
+#pragma unroll
+    for (int k = 0; k < NPR; k++) c[k] = cb[k] * g;
+    const double frb = c[RHO] + c[UU] + c[KTOT] * K;   // F[UU] and F[KTOT] carry F[RHO]
+    a.K += c[KTOT] * (pr[RHO] * q.ucon[D]);
+    a.rho += frb * q.ucon[D];
+    a.ucon[D] += frb * pr[RHO];
+    const double mb[4] = {c[UU], c[U1], c[U2], c[U3]};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        a.eta += mb[j] * q.ucon[D] * q.ucov[j];
+        a.ucon[D] += mb[j] * eta * q.ucov[j];
+        a.ucov[j] += mb[j] * eta * q.ucon[D];
+        a.bcon[D] -= mb[j] * q.bcov[j];
+        a.bcov[j] -= mb[j] * q.bcon[D];
+    }
+    a.ptot += mb[D];
+#pragma unroll
+    for (int i = 1; i < 4; i++) {
+        if (i == D) continue;   // b^D u^D - b^D u^D: identically zero
+        const double cB = c[B1 + i - 1];
+        a.bcon[i] += cB * q.ucon[D];
+        a.ucon[D] += cB * q.bcon[i];
+        a.bcon[D] -= cB * q.ucon[i];
+        a.ucon[i] -= cB * q.bcon[D];
     }
 }
 
+// forward values the reverse needs
+struct StateFwd {
+    State<double> q;
+    double gam_l, P, w, bsq, eta, K;
+    bool gfree;   // the Lorentz factor is sqrt(1 + q^2), not clamped
+};
+
+__device__ __forceinline__ void state_fwd(const double *pr, const Geo<double> &gm, double gam, StateFwd &f) {
+    const double *gc = gm.gcov;
+    get_state(pr, gm, f.q);
+    gamma_calc(pr, gm, &f.gam_l);
+    const double u1 = pr[U1], u2 = pr[U2], u3 = pr[U3];
+    const double qsq = gc[4] * u1 * u1 + gc[7] * u2 * u2 + gc[9] * u3 * u3
+                     + 2. * (gc[5] * u1 * u2 + gc[6] * u1 * u3 + gc[8] * u2 * u3);
+    f.gfree = !(qsq < 0.);
+    f.P = (gam - 1.) * pr[UU];
+    f.w = pr[RHO] + f.P + pr[UU];
+    f.bsq = dot4(f.q.bcon, f.q.bcov);
+    f.eta = f.w + f.bsq;
+    f.K = entropy(gam, pr);
+}
+
+__device__ __forceinline__ void bar_zero(StateBar &a) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) a.ucon[k] = a.ucov[k] = a.bcon[k] = a.bcov[k] = 0.;
+    a.rho = a.u = a.gam = a.eta = a.ptot = a.w = a.P = a.bsq = a.K = 0.;
+}
+
+// from the cotangents of the scalars and of u^mu, u_mu, b^mu, b_mu back to
+// the primitives (pbar, ADJ_NP) and gamma (added to gbar)
+__device__ __forceinline__ void state_back(const double *pr, const Geo<double> &gm, double gam, const StateFwd &f,
+                                           StateBar &a, double *pbar, double &gbar) {
+    const double *gc = gm.gcov, *gn = gm.gcon;
+    const State<double> &q = f.q;
+    const double u = pr[UU], rho = pr[RHO];
+    // eta = w + b^2, ptot = P + b^2/2, w = rho + P + u, P = (gam - 1) u,
+    // K = (gam - 1) u rho^-gam
+    a.w += a.eta;
+    a.bsq += a.eta + 0.5 * a.ptot;
+    a.P += a.ptot + a.w;
+    a.rho += a.w;
+    a.u += a.w + a.P * (gam - 1.);
+    a.gam += a.P * u;
+    if (a.K != 0.) {
+        const double rg = pow(rho, -gam);
+        a.u += a.K * (gam - 1.) * rg;
+        a.gam += a.K * (u * rg - f.K * log(rho));
+        a.rho -= a.K * gam * f.K / rho;
+    }
+    // b^2 = b^mu b_mu; b_mu = g_{mu nu} b^nu
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) {
+        a.bcon[mu] += a.bsq * q.bcov[mu];
+        a.bcov[mu] += a.bsq * q.bcon[mu];
+    }
+    {
+        double t[4];
+        lower4(a.bcov, gc, t);
+#pragma unroll
+        for (int mu = 0; mu < 4; mu++) a.bcon[mu] += t[mu];
+    }
+    // b^j = (B^j + b^0 u^j) / u^0, then b^0 = B^i u_i
+    double Bb[3];
+#pragma unroll
+    for (int j = 1; j < 4; j++) {
+        const double bj = a.bcon[j] / q.ucon[0];
+        Bb[j - 1] = bj;
+        a.bcon[0] += bj * q.ucon[j];
+        a.ucon[j] += bj * q.bcon[0];
+        a.ucon[0] -= bj * q.bcon[j];
+    }
+#pragma unroll
+    for (int i = 1; i < 4; i++) {
+        Bb[i - 1] += a.bcon[0] * q.ucov[i];
+        a.ucov[i] += a.bcon[0] * pr[B1 + i - 1];
+    }
+    // u_mu = g_{mu nu} u^nu
+    {
+        double t[4];
+        lower4(a.ucov, gc, t);
+#pragma unroll
+        for (int mu = 0; mu < 4; mu++) a.ucon[mu] += t[mu];
+    }
+    // u^0 = gamma / alpha, u^j = u~^j - gamma beta^j / alpha, beta^j = g^{0j} alpha^2
+    const double alpha = 1. / d_sqrt(-gn[0]);
+    double gb = a.ucon[0] / alpha;
+#pragma unroll
+    for (int j = 1; j < 4; j++) gb -= a.ucon[j] * (gn[j] * alpha * alpha) / alpha;
+    double ub3[3] = {a.ucon[1], a.ucon[2], a.ucon[3]};
+    if (f.gfree) {
+        const double u1 = pr[U1], u2 = pr[U2], u3 = pr[U3];
+        const double qb = 0.5 * gb / f.gam_l;   // gamma = sqrt(1 + q^2)
+        ub3[0] += 2. * qb * (gc[4] * u1 + gc[5] * u2 + gc[6] * u3);
+        ub3[1] += 2. * qb * (gc[5] * u1 + gc[7] * u2 + gc[8] * u3);
+        ub3[2] += 2. * qb * (gc[6] * u1 + gc[8] * u2 + gc[9] * u3);
+    }
+    pbar[RHO] = a.rho;
+    pbar[UU] = a.u;
+    pbar[U1] = ub3[0];
+    pbar[U2] = ub3[1];
+    pbar[U3] = ub3[2];
+    pbar[B1] = Bb[0];
+    pbar[B2] = Bb[1];
+    pbar[B3] = Bb[2];
+    gbar += a.gam;
+}
+
+// pbar (ADJ_NP) and gbar (added) from the cotangents of the fluxes along DIR
+// (fb), of the conserved variables (ub) and of the fast speeds along DIR
+// (DIR == 0: conserved variables only)
+template <int DIR>
+__device__ void state_vjp(const double *pr, const Geo<double> &gm, double gam, const double *fb, const double *ub,
+                          double cmxb, double cmnb, double *pbar, double &gbar) {
+    const double *gn = gm.gcon;
+    StateFwd f;
+    state_fwd(pr, gm, gam, f);
+    const State<double> &q = f.q;
+    const double u = pr[UU], w = f.w, bsq = f.bsq, eta = f.eta;
+    StateBar a;
+    bar_zero(a);
+    flux_rev<0>(pr, q, gm.g, eta, f.K, ub, a);
+    if (DIR != 0) {
+        flux_rev<DIR>(pr, q, gm.g, eta, f.K, fb, a);
+        // fast speeds: the roots of A v^2 - B v + C = 0 (forward in primtoflux)
+        const double Acon_0 = gn[DIR], Asq = gn[DIR == 1 ? 4 : (DIR == 2 ? 7 : 9)], Bsq = gn[0], AB = Acon_0;
+        const double cs2 = gam * (gam - 1.) * u / w;
+        const double va2 = bsq / eta;
+        double cms2 = cs2 + va2 - cs2 * va2;
+        const bool cfree = !(cms2 < 0.) && !(cms2 > 1.);
+        if (cms2 < 0.) cms2 = SMALL_D;
+        if (cms2 > 1.) cms2 = 1.;
+        const double Au = q.ucon[DIR], Bu = q.ucon[0];
+        const double Au2 = Au * Au, Bu2 = Bu * Bu, AuBu = Au * Bu;
+        const double A = Bu2 - (Bsq + Bu2) * cms2;
+        const double B = 2. * (AuBu - (AB + AuBu) * cms2);
+        const double C = Au2 - (Asq + Au2) * cms2;
+        double discr = B * B - 4. * A * C;
+        const bool dfree = !(discr < 0.);
+        if (!dfree) discr = 0.;
+        const double sq = d_sqrt(discr);
+        const double vp = -(-B + sq) / (2. * A), vm = -(-B - sq) / (2. * A);
+        const double vpb = (vp > vm ? cmxb : 0.) + (vp < vm ? cmnb : 0.);
+        const double vmb = (vp > vm ? 0. : cmxb) + (vp < vm ? 0. : cmnb);
+        double Bb = (vpb + vmb) / (2. * A);
+        const double sb = (vmb - vpb) / (2. * A);
+        double Ab = -(vpb * vp + vmb * vm) / A, Cb = 0.;
+        if (dfree && sq > 0.) {
+            const double Db = 0.5 * sb / sq;
+            Bb += 2. * B * Db;
+            Ab -= 4. * C * Db;
+            Cb = -4. * A * Db;
+        }
+        const double om = 1. - cms2;
+        a.ucon[DIR] += 2. * Bu * om * Bb + 2. * Au * om * Cb;
+        a.ucon[0] += 2. * Bu * om * Ab + 2. * Au * om * Bb;
+        if (cfree) {
+            const double cmsb = -(Bsq + Bu2) * Ab - 2. * (AB + AuBu) * Bb - (Asq + Au2) * Cb;
+            // 1 - va2 = w / eta, without the cancellation where b^2 >> w
+            const double cs2b = cmsb * (w / eta), va2b = cmsb * (1. - cs2);
+            a.bsq += va2b / eta;
+            a.eta -= va2b * va2 / eta;
+            const double numb = cs2b / w;
+            a.w -= cs2b * cs2 / w;
+            a.u += numb * gam * (gam - 1.);
+            a.gam += numb * u * (2. * gam - 1.);
+        }
+    }
+    state_back(pr, gm, gam, f, a, pbar, gbar);
+}
+
+// geometric source of a state reversed (source in hamr_kernels.cu,
+// GPU_phys_mhd.h:34-175): the cotangents wb of dU[UU..U3] give, through the
+// connection, the cotangent of the stress tensor T^a_k = eta u^a u_k +
+// ptot delta^a_k - b^a b_k, and from there the state's
+__device__ void source_vjp(const double *pr, const Geo<double> &gm, double gam, const Dims &d, const Geom &m, long gi,
+                           const double *wb, double *pbar, double &gbar) {
+    StateFwd f;
+    state_fwd(pr, gm, gam, f);
+    const State<double> &q = f.q;
+    StateBar a;
+    bar_zero(a);
+    const long gs = d.gs;
+#pragma unroll
+    for (int al = 0; al < 4; al++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            double tb = 0.;
+#pragma unroll
+            for (int mm = 0; mm < 4; mm++) tb += wb[mm] * __ldg(&m.conn[(long)(sym4(mm, al) * 4 + k) * gs + gi]);
+            tb *= gm.g;
+            a.eta += tb * q.ucon[al] * q.ucov[k];
+            a.ucon[al] += tb * f.eta * q.ucov[k];
+            a.ucov[k] += tb * f.eta * q.ucon[al];
+            if (al == k) a.ptot += tb;
+            a.bcon[al] -= tb * q.bcov[k];
+            a.bcov[k] -= tb * q.bcon[al];
+        }
+    state_back(pr, gm, gam, f, a, pbar, gbar);
+}
+
 // face fluxes of direction DIR, reversed: aF (cotangent of the fluxes) ->
-// ap (primitives of the stencil, atomics), aps (normal face field), agam
+// ap (primitives of the stencil, atomics), aps (normal face field), agam.
+// A lane pair takes one face, one lane per side (s = 0 left, 1 right): each
+// lane reconstructs its side, evaluates it, swaps the result with its
+// partner for the HLL combination, reverses its side's state map by hand
+// (state_vjp) and scatters over its PPM stencil, whose branch-local linear
+// weights it takes from 5-direction dual numbers.
+constexpr int FTEAM = 2;
 template <int DIR>
 __global__ void __launch_bounds__(BLK) k_adj_flux(const Dims d, const Geom m, const double *__restrict__ pv,
                                                    const double *__restrict__ ps, const double *__restrict__ aF,
                                                    double *ap, double *aps, double *agam) {
     constexpr int idel = DIR == 1, jdel = DIR == 2, zdel = DIR == 3;
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, side = lane & 1;
+    const unsigned tm = 3u << (lane & ~1);   // this face's lane pair
+    const long t = ((long)blockIdx.x * blockDim.x + threadIdx.x) / FTEAM;
     double gsum = 0.;
     if (t < n_faces<DIR>(d)) {
         const int i0 = (d.ng1 - 1) * d.d1 + idel, j0 = (d.ng2 - 1) * d.d2 + jdel, z0 = (d.ng3 - 1) * d.d3 + zdel;
@@ -167,40 +383,40 @@ __global__ void __launch_bounds__(BLK) k_adj_flux(const Dims d, const Geom m, co
         double Fb[NPR];
         bool any = false;
         for (int k = 0; k < NPR; k++) { Fb[k] = aF[k * ks + c]; any |= Fb[k] != 0.; }
-        if (any) {
+        if (any) {   // uniform over the pair: same face
             const int face = DIR == 1 ? FACE1 : (DIR == 2 ? FACE2 : FACE3);
+            const int bn = B1 + DIR - 1;
+            const bool polefix = DIR == 2 && ((j == d.n2 + d.ng2 && d.pole2) || (j == d.ng2 && d.pole1));
             Geo<double> g0;
             load_geo(d, m, i, j, face, g0);
-            // PPM edge values and their (branch-local, linear) stencil weights
-            double pl[NPR], pr[NPR], cl[NPR][5], cr[NPR][5];
-            for (int k = 0; k < NPR; k++) {
-                const double *pk = pv + (long)k * ks + c;
-                double x[6];
-                for (int s = 0; s < 6; s++) x[s] = pk[(s - 3) * stride];
-                Dual<5> xl[5], xr[5], lo, hi;
-                for (int s = 0; s < 5; s++) { xl[s] = dual_var<5>(x[s], s); xr[s] = dual_var<5>(x[s + 1], s); }
-                para(xl, lo, hi);
-                pl[k] = hi.v;
-                for (int s = 0; s < 5; s++) cl[k][s] = hi.d[s];
-                para(xr, lo, hi);
-                pr[k] = lo.v;
-                for (int s = 0; s < 5; s++) cr[k][s] = lo.d[s];
+            // this side's reconstructed state: left = upper edge of the zone
+            // below the face (stencil -3..1), right = lower edge of the zone
+            // above it (stencil -2..2)
+            double pme[NPR];
+#pragma unroll
+            for (int k = 0; k < ADJ_NP; k++) {
+                const double *pk = pv + (long)k * ks + c + (side - 3) * stride;
+                double x[5], lo, hi;
+#pragma unroll
+                for (int s = 0; s < 5; s++) x[s] = pk[s * stride];
+                para(x, lo, hi);
+                pme[k] = side ? lo : hi;
             }
-            const int bn = B1 + DIR - 1;
-            pl[bn] = pr[bn] = ps[(long)(DIR - 1) * ks + c];
-            const bool polefix = DIR == 2 && ((j == d.n2 + d.ng2 && d.pole2) || (j == d.ng2 && d.pole1));
-            if (polefix) pl[B1] = pr[B1] = 0.;
+            pme[bn] = ps[(long)(DIR - 1) * ks + c];
+            if (polefix) pme[B1] = 0.;
+            pme[KTOT] = 0.;   // read by no flux
             const double gam = d.gam;
-            State<double> q;
-            double t1[NPR], t2[NPR], t3[NPR], t4[NPR], cmax_l, cmin_l, cmax_r, cmin_r, vd;
-            get_state(pl, g0, q);
-            double e = entropy(gam, pl);
-            primtoflux(gam, pl, q, DIR, g0, e, t1, &cmax_l, &cmin_l);
-            primtoflux(gam, pl, q, 0, g0, e, t2, &vd, &vd);
-            get_state(pr, g0, q);
-            e = entropy(gam, pr);
-            primtoflux(gam, pr, q, DIR, g0, e, t3, &cmax_r, &cmin_r);
-            primtoflux(gam, pr, q, 0, g0, e, t4, &vd, &vd);
+            double ta[NPR], tb[NPR], cmx_me, cmn_me, vd;
+            {
+                State<double> st;
+                get_state(pme, g0, st);
+                const double e = entropy(gam, pme);
+                primtoflux(gam, pme, st, DIR, g0, e, ta, &cmx_me, &cmn_me);
+                primtoflux(gam, pme, st, 0, g0, e, tb, &vd, &vd);
+            }
+            const double cmx_o = __shfl_xor_sync(tm, cmx_me, 1), cmn_o = __shfl_xor_sync(tm, cmn_me, 1);
+            const double cmax_l = side ? cmx_o : cmx_me, cmin_l = side ? cmn_o : cmn_me;
+            const double cmax_r = side ? cmx_me : cmx_o, cmin_r = side ? cmn_me : cmn_o;
             // HLL combination reversed (same max/abs selections as the forward)
             const double in_x = 0. > cmax_l ? 0. : cmax_l;
             const bool take_r = !(in_x > cmax_r);
@@ -211,33 +427,46 @@ __global__ void __launch_bounds__(BLK) k_adj_flux(const Dims d, const Geom m, co
             const double on = take_rn ? -cmin_r : in_n;
             const double cmin = on < 0. ? -on : on;
             const double D = cmax + cmin + SMALL_D;
-            double t1b[NPR], t2b[NPR], t3b[NPR], t4b[NPR], cmaxb = 0., cminb = 0.;
+            // this side's flux and conserved-variable cotangents, and the
+            // speeds' (which need both sides' fluxes)
+            double tfb[NPR], tub[NPR], cmaxb = 0., cminb = 0.;
+#pragma unroll
             for (int k = 0; k < NPR; k++) {
-                const double Fk = (cmax * t1[k] + cmin * t3[k] - cmax * cmin * (t4[k] - t2[k])) / D;
-                t1b[k] = Fb[k] * cmax / D;
-                t3b[k] = Fb[k] * cmin / D;
-                t4b[k] = -Fb[k] * cmax * cmin / D;
-                t2b[k] = Fb[k] * cmax * cmin / D;
-                cmaxb += Fb[k] * ((t1[k] - cmin * (t4[k] - t2[k])) - Fk) / D;
-                cminb += Fb[k] * ((t3[k] - cmax * (t4[k] - t2[k])) - Fk) / D;
+                const double fo = __shfl_xor_sync(tm, ta[k], 1), uo = __shfl_xor_sync(tm, tb[k], 1);
+                const double t1 = side ? fo : ta[k], t2 = side ? uo : tb[k];
+                const double t3 = side ? ta[k] : fo, t4 = side ? tb[k] : uo;
+                const double Fk = (cmax * t1 + cmin * t3 - cmax * cmin * (t4 - t2)) / D;
+                tfb[k] = side ? Fb[k] * cmin / D : Fb[k] * cmax / D;
+                tub[k] = side ? -Fb[k] * cmax * cmin / D : Fb[k] * cmax * cmin / D;
+                cmaxb += Fb[k] * ((t1 - cmin * (t4 - t2)) - Fk) / D;
+                cminb += Fb[k] * ((t3 - cmax * (t4 - t2)) - Fk) / D;
             }
             const double sx = ox < 0. ? -1. : 1., sn = on < 0. ? -1. : 1.;
-            double cmaxlb = 0., cmaxrb = 0., cminlb = 0., cminrb = 0.;
-            if (take_r) cmaxrb = sx * cmaxb;
-            else if (!(0. > cmax_l)) cmaxlb = sx * cmaxb;
-            if (take_rn) cminrb = -sn * cminb;
-            else if (!(0. > -cmin_l)) cminlb = -sn * cminb;
-            double plb[ADJ_NP], prb[ADJ_NP];
-            side_vjp<DIR>(pl, g0, gam, t1b, t2b, cmaxlb, cminlb, plb, gsum);
-            side_vjp<DIR>(pr, g0, gam, t3b, t4b, cmaxrb, cminrb, prb, gsum);
-            for (int k = 0; k < ADJ_NP; k++) {
-                if (k == bn || (polefix && k == B1)) continue;
-                for (int s = 0; s < 5; s++) {
-                    if (cl[k][s] != 0.) atomicAdd(&ap[k * ks + c + (s - 3) * stride], plb[k] * cl[k][s]);
-                    if (cr[k][s] != 0.) atomicAdd(&ap[k * ks + c + (s - 2) * stride], prb[k] * cr[k][s]);
-                }
+            double cmxb = 0., cmnb = 0.;
+            if (side) {
+                if (take_r) cmxb = sx * cmaxb;
+                if (take_rn) cmnb = -sn * cminb;
+            } else {
+                if (!take_r && !(0. > cmax_l)) cmxb = sx * cmaxb;
+                if (!take_rn && !(0. > -cmin_l)) cmnb = -sn * cminb;
             }
-            atomicAdd(&aps[(long)(DIR - 1) * ks + c], plb[bn] + prb[bn]);
+            double pb[ADJ_NP];
+            state_vjp<DIR>(pme, g0, gam, tfb, tub, cmxb, cmnb, pb, gsum);
+            atomicAdd(&aps[(long)(DIR - 1) * ks + c], pb[bn]);
+            // PPM stencil weights of this side, primitive by primitive
+#pragma unroll 1
+            for (int k = 0; k < ADJ_NP; k++) {
+                if (k == bn || (polefix && k == B1) || pb[k] == 0.) continue;
+                const double *pk = pv + (long)k * ks + c + (side - 3) * stride;
+                Dual<5> x[5], lo, hi;
+#pragma unroll
+                for (int s = 0; s < 5; s++) x[s] = dual_var<5>(pk[s * stride], s);
+                para(x, lo, hi);
+                const Dual<5> &e = side ? lo : hi;
+#pragma unroll
+                for (int s = 0; s < 5; s++)
+                    if (e.d[s] != 0.) atomicAdd(&ap[k * ks + c + (side + s - 3) * stride], pb[k] * e.d[s]);
+            }
         }
     }
     block_add(gsum, agam);
@@ -318,8 +547,7 @@ __global__ void __launch_bounds__(BLK) k_adj_invert(const Dims d, const Geom m, 
                 for (int k = 0; k < NPR; k++) pf[k] = pg[k * ks + c];
                 const bool entropy_row = utoprim_2d(d.gam, U, g0.gcov, g0.gcon, g0.g, pf) != 0;
                 constexpr int N = ADJ_NP + 1;
-                Geo<Dual<N>> gm;
-                geo_const(g0, gm);
+                const Geo<double> &gm = g0;   // the metric is data: no derivative parts
                 double pr[NPR];
                 for (int k = 0; k < NPR; k++) pr[k] = pout[k * ks + c];
                 Dual<N> pd[NPR], gd;
@@ -404,28 +632,14 @@ __global__ void __launch_bounds__(BLK) k_adj_source(const Dims d, const Geom m, 
         bool any = false;
         for (int k = 0; k < NPR; k++) { wb[k] = aW[k * ks + c]; any |= (k >= UU && k <= U3 && wb[k] != 0.); }
         if (any) {
-            constexpr int N = 3;
             Geo<double> g0;
             load_geo(d, m, i, j, CENT, g0);
-            Geo<Dual<N>> gm;
-            geo_const(g0, gm);
-            double pr[NPR];
+            double pr[NPR], pbar[ADJ_NP], gb = 0.;
             for (int k = 0; k < NPR; k++) pr[k] = pb[k * ks + c];
-            for (int pass = 0; pass * N <= ADJ_NP; pass++) {
-                Dual<N> pd[NPR], gd, dU[NPR];
-                seed_state(pr, d.gam, pass, pd, gd);
-                State<Dual<N>> q;
-                get_state(pd, gm, q);
-                source_t(gd, pd, gm, d, m, gi, dU, q);
-                for (int qd = 0; qd < N; qd++) {
-                    const int in = pass * N + qd;
-                    if (in > ADJ_NP) break;
-                    double s = 0.;
-                    for (int k = UU; k <= U3; k++) s += wb[k] * dU[k].d[qd];
-                    if (in < ADJ_NP) ap[in * ks + c] += Dt * s;
-                    else gsum += Dt * s;
-                }
-            }
+            const double w4[4] = {wb[UU], wb[U1], wb[U2], wb[U3]};
+            source_vjp(pr, g0, d.gam, d, m, gi, w4, pbar, gb);
+            for (int k = 0; k < ADJ_NP; k++) ap[k * ks + c] += Dt * pbar[k];
+            gsum += Dt * gb;
         }
     }
     block_add(gsum, agam);
@@ -446,28 +660,12 @@ __global__ void __launch_bounds__(BLK) k_adj_cons_of_state(const Dims d, const G
         bool any = false;
         for (int k = 0; k < NPR; k++) { ub[k] = aU[k * ks + c]; aU[k * ks + c] = 0.; any |= ub[k] != 0.; }
         if (any) {
-            constexpr int N = 3;
             Geo<double> g0;
             load_geo(d, m, i, j, CENT, g0);
-            Geo<Dual<N>> gm;
-            geo_const(g0, gm);
-            double pr[NPR];
+            double pr[NPR], pb[ADJ_NP];
             for (int k = 0; k < NPR; k++) pr[k] = pv[k * ks + c];
-            for (int pass = 0; pass * N <= ADJ_NP; pass++) {
-                Dual<N> pd[NPR], gd, U[NPR], vd;
-                seed_state(pr, d.gam, pass, pd, gd);
-                State<Dual<N>> q;
-                get_state(pd, gm, q);
-                primtoflux(gd, pd, q, 0, gm, entropy(gd, pd), U, &vd, &vd);
-                for (int qd = 0; qd < N; qd++) {
-                    const int in = pass * N + qd;
-                    if (in > ADJ_NP) break;
-                    double s = 0.;
-                    for (int k = 0; k < NPR; k++) s += ub[k] * U[k].d[qd];
-                    if (in < ADJ_NP) ap[in * ks + c] += s;
-                    else gsum += s;
-                }
-            }
+            state_vjp<0>(pr, g0, d.gam, ub, ub, 0., 0., pb, gsum);
+            for (int k = 0; k < ADJ_NP; k++) ap[k * ks + c] += pb[k];
         }
     }
     block_add(gsum, agam);
@@ -501,8 +699,7 @@ __global__ void __launch_bounds__(BLK) k_adj_emf_centre(const Dims d, const Geom
     constexpr int N = 6;   // U1, U2, U3, B1, B2, B3
     Geo<double> g0;
     load_geo(d, m, i, j, CENT, g0);
-    Geo<Dual<N>> gm;
-    geo_const(g0, gm);
+    const Geo<double> &gm = g0;   // the metric is data: no derivative parts
     Dual<N> pd[NPR];
     for (int k = 0; k < NPR; k++) pd[k] = Dual<N>(pv[k * ks + c]);
     for (int q = 0; q < N; q++) pd[U1 + q].d[q] = 1.;
@@ -814,8 +1011,8 @@ int adj_stage(hamr_adjoint *a, int full, double dt, double mdot_coef, const Stag
     k_adj_emf_centre<<<nb((long)(d.n1 + 2) * (d.n2 + 2)), BLK, 0, s>>>(d, m, r.pin, a->aEc, apin);
     // flux fixes, then the face fluxes -> pin (and the normal face field)
     k_adj_fix_flux<<<nb((long)d.G1 + d.G2), BLK, 0, s>>>(d, r.F1, a->aF1, a->aF2);
-    k_adj_flux<1><<<nb(n_faces<1>(d)), BLK, 0, s>>>(d, m, r.pin, r.psin, a->aF1, apin, apsin, a->agam);
-    k_adj_flux<2><<<nb(n_faces<2>(d)), BLK, 0, s>>>(d, m, r.pin, r.psin, a->aF2, apin, apsin, a->agam);
+    k_adj_flux<1><<<nb(FTEAM * n_faces<1>(d)), BLK, 0, s>>>(d, m, r.pin, r.psin, a->aF1, apin, apsin, a->agam);
+    k_adj_flux<2><<<nb(FTEAM * n_faces<2>(d)), BLK, 0, s>>>(d, m, r.pin, r.psin, a->aF2, apin, apsin, a->agam);
     ACK(cudaGetLastError());
     return HAMR_OK;
 }

@@ -63,6 +63,7 @@ template <int N> __device__ __forceinline__ Dual<N> &operator+=(Dual<N> &a, cons
 template <int N> __device__ __forceinline__ Dual<N> &operator-=(Dual<N> &a, const Dual<N> &b) { a = a - b; return a; }
 template <int N> __device__ __forceinline__ Dual<N> &operator*=(Dual<N> &a, const Dual<N> &b) { a = a * b; return a; }
 template <int N> __device__ __forceinline__ Dual<N> &operator/=(Dual<N> &a, const Dual<N> &b) { a = a / b; return a; }
+template <int N> __device__ __forceinline__ Dual<N> &operator*=(Dual<N> &a, double b) { a = a * b; return a; }
 
 // comparisons look at the value: the branch the forward code takes
 template <int N> __device__ __forceinline__ bool operator<(const Dual<N> &a, const Dual<N> &b) { return a.v < b.v; }

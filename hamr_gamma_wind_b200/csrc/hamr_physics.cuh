@@ -71,24 +71,26 @@ template <> __device__ __forceinline__ float d_rsqrt<float>(float x) { return po
 template <typename T> __device__ __forceinline__ T d_max(T a, T b) { return a > b ? a : b; }
 template <typename T> __device__ __forceinline__ T d_min(T a, T b) { return a < b ? a : b; }
 
-template <typename T>
-__device__ __forceinline__ void lower4(const T *u, const T *g, T *o) {
+// G, the metric's type, may differ from the state's T: the adjoint runs these
+// routines on dual numbers over a plain-double (constant) metric
+template <typename T, typename G>
+__device__ __forceinline__ void lower4(const T *u, const G *g, T *o) {
     o[0] = g[0] * u[0] + g[1] * u[1] + g[2] * u[2] + g[3] * u[3];
     o[1] = g[1] * u[0] + g[4] * u[1] + g[5] * u[2] + g[6] * u[3];
     o[2] = g[2] * u[0] + g[5] * u[1] + g[7] * u[2] + g[8] * u[3];
     o[3] = g[3] * u[0] + g[6] * u[1] + g[8] * u[2] + g[9] * u[3];
 }
-template <typename T>
-__device__ __forceinline__ void raise4(const T *u, const T *g, T *o) { lower4(u, g, o); }
+template <typename T, typename G>
+__device__ __forceinline__ void raise4(const T *u, const G *g, T *o) { lower4(u, g, o); }
 
 template <typename T>
 __device__ __forceinline__ T dot4(const T *a, const T *b) {
     return a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3];
 }
 
-template <typename T>
-__device__ __forceinline__ void gamma_calc(const T *pr, const Geo<T> &gm, T *gamma) {
-    const T *g = gm.gcov;
+template <typename T, typename G>
+__device__ __forceinline__ void gamma_calc(const T *pr, const Geo<G> &gm, T *gamma) {
+    const G *g = gm.gcov;
     T qsq = g[4] * pr[U1] * pr[U1] + g[7] * pr[U2] * pr[U2] + g[9] * pr[U3] * pr[U3]
           + T(2.) * (g[5] * pr[U1] * pr[U2] + g[6] * pr[U1] * pr[U3] + g[8] * pr[U2] * pr[U3]);
     if (qsq < T(0.)) {
@@ -98,10 +100,11 @@ __device__ __forceinline__ void gamma_calc(const T *pr, const Geo<T> &gm, T *gam
     *gamma = d_sqrt(T(1.) + qsq);
 }
 
-template <typename T>
-__device__ __forceinline__ void ucon_calc(const T *pr, const Geo<T> &gm, T *ucon) {
-    T alpha = T(1.) / d_sqrt(-gm.gcon[0]);
-    T beta[4], gamma;
+template <typename T, typename G>
+__device__ __forceinline__ void ucon_calc(const T *pr, const Geo<G> &gm, T *ucon) {
+    G alpha = G(1.) / d_sqrt(-gm.gcon[0]);
+    G beta[4];
+    T gamma;
 #pragma unroll
     for (int j = 1; j < 4; j++) beta[j] = gm.gcon[j] * alpha * alpha;
     gamma_calc(pr, gm, &gamma);
@@ -117,8 +120,8 @@ __device__ __forceinline__ void bcon_calc(const T *pr, const T *ucon, const T *u
     for (int j = 1; j < 4; j++) bcon[j] = (pr[B1 - 1 + j] + bcon[0] * ucon[j]) / ucon[0];
 }
 
-template <typename T>
-__device__ __forceinline__ void get_state(const T *pr, const Geo<T> &gm, State<T> &q) {
+template <typename T, typename G>
+__device__ __forceinline__ void get_state(const T *pr, const Geo<G> &gm, State<T> &q) {
     ucon_calc(pr, gm, q.ucon);
     lower4(q.ucon, gm.gcov, q.ucov);
     bcon_calc(pr, q.ucon, q.ucov, q.bcon);
@@ -134,8 +137,8 @@ __device__ __forceinline__ T entropy(T gam, const T *pr) {
 // Fluxes in direction dir (dir == 0: conserved variables); with dir != 0 the
 // fast magnetosonic speeds along dir as well. `ent` is the entropy K of pr,
 // computed once per state by the caller.
-template <typename T>
-__device__ __forceinline__ void primtoflux(T gam, const T *pr, const State<T> &q, int dir, const Geo<T> &gm,
+template <typename T, typename G>
+__device__ __forceinline__ void primtoflux(T gam, const T *pr, const State<T> &q, int dir, const Geo<G> &gm,
                                            T ent, T *flux, T *vmax, T *vmin) {
     T mhd[4];
     T u = pr[UU];
@@ -159,7 +162,7 @@ __device__ __forceinline__ void primtoflux(T gam, const T *pr, const State<T> &q
 #pragma unroll
     for (int k = 0; k < NPR; k++) flux[k] *= gm.g;
     if (dir != 0) {
-        T Acon_0, Acon_js;
+        G Acon_0, Acon_js;
         if (dir == 1) { Acon_0 = gm.gcon[1]; Acon_js = gm.gcon[4]; }
         else if (dir == 2) { Acon_0 = gm.gcon[2]; Acon_js = gm.gcon[7]; }
         else { Acon_0 = gm.gcon[3]; Acon_js = gm.gcon[9]; }
@@ -168,8 +171,8 @@ __device__ __forceinline__ void primtoflux(T gam, const T *pr, const State<T> &q
         T cms2 = cs2 + va2 - cs2 * va2;
         if (cms2 < T(0.)) cms2 = T(SMALL_D);
         if (cms2 > T(1.)) cms2 = T(1.);
-        T Asq = Acon_js, Bsq = gm.gcon[0];
-        T Au = q.ucon[dir], Bu = q.ucon[0], AB = Acon_0;
+        const G Asq = Acon_js, Bsq = gm.gcon[0], AB = Acon_0;
+        T Au = q.ucon[dir], Bu = q.ucon[0];
         T Au2 = Au * Au, Bu2 = Bu * Bu, AuBu = Au * Bu;
         T A = Bu2 - (Bsq + Bu2) * cms2;
         T B = T(2.) * (AuBu - (AB + AuBu) * cms2);
