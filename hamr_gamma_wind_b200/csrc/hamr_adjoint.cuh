@@ -364,14 +364,13 @@ __device__ void source_vjp(const double *pr, const Geo<double> &gm, double gam, 
 // weights it takes from 5-direction dual numbers.
 constexpr int FTEAM = 2;
 template <int DIR>
-__global__ void __launch_bounds__(BLK) k_adj_flux(const Dims d, const Geom m, const double *__restrict__ pv,
-                                                   const double *__restrict__ ps, const double *__restrict__ aF,
-                                                   double *ap, double *aps, double *agam) {
+__device__ __forceinline__ void adj_flux_face(const Dims &d, const Geom &m, const double *__restrict__ pv,
+                                              const double *__restrict__ ps, const double *__restrict__ aF,
+                                              double *ap, double *aps, long tt, double &gsum) {
     constexpr int idel = DIR == 1, jdel = DIR == 2, zdel = DIR == 3;
     const int lane = threadIdx.x & 31, side = lane & 1;
     const unsigned tm = 3u << (lane & ~1);   // this face's lane pair
-    const long t = ((long)blockIdx.x * blockDim.x + threadIdx.x) / FTEAM;
-    double gsum = 0.;
+    const long t = tt / FTEAM;
     if (t < n_faces<DIR>(d)) {
         const int i0 = (d.ng1 - 1) * d.d1 + idel, j0 = (d.ng2 - 1) * d.d2 + jdel, z0 = (d.ng3 - 1) * d.d3 + zdel;
         const int nj = d.n2 + 2 * d.d2 - jdel, nz = d.n3 + 2 * d.d3 - zdel;
@@ -469,6 +468,18 @@ __global__ void __launch_bounds__(BLK) k_adj_flux(const Dims d, const Geom m, co
             }
         }
     }
+}
+
+// both directions' faces in one launch (2-D: x1 then x2 faces), so that the
+// two reverses, which only meet in atomics, fill the GPU together
+__global__ void __launch_bounds__(BLK) k_adj_flux12(const Dims d, const Geom m, const double *__restrict__ pv,
+                                                     const double *__restrict__ ps, const double *__restrict__ aF1,
+                                                     const double *__restrict__ aF2, double *ap, double *aps,
+                                                     double *agam) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x, n1 = FTEAM * n_faces<1>(d);
+    double gsum = 0.;
+    if (t < n1) adj_flux_face<1>(d, m, pv, ps, aF1, ap, aps, t, gsum);
+    else adj_flux_face<2>(d, m, pv, ps, aF2, ap, aps, t - n1, gsum);
     block_add(gsum, agam);
 }
 
@@ -480,11 +491,9 @@ __device__ __forceinline__ bool active_zone(const Dims &d, int i, int j) {
 // conserved component the inversion reads from the update (B1, B2 come from
 // the faces instead); plus the accretion-rate objective on x1 face column ih
 template <int DIR>
-__global__ void k_adj_divergence(const Dims d, const double *__restrict__ aW, double *aF, double Dt, int ih,
-                                 double mdot_coef) {
+__device__ __forceinline__ void adj_divergence_face(const Dims &d, const double *__restrict__ aW, double *aF,
+                                                    double Dt, int ih, double mdot_coef, long t) {
     constexpr int idel = DIR == 1, jdel = DIR == 2;
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n_faces<DIR>(d)) return;
     const int i0 = (d.ng1 - 1) * d.d1 + idel, j0 = (d.ng2 - 1) * d.d2 + jdel;
     const int nj = d.n2 + 2 * d.d2 - jdel;
     const int j = j0 + (int)(t % nj);
@@ -503,6 +512,13 @@ __global__ void k_adj_divergence(const Dims d, const double *__restrict__ aW, do
     if (DIR == 1 && i == ih && j >= d.ng2 && j < d.ng2 + d.n2) aF[RHO * ks + c] += mdot_coef;
 }
 
+__global__ void k_adj_divergence12(const Dims d, const double *__restrict__ aW, double *aF1, double *aF2, double Dt,
+                                   int ih, double mdot_coef) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x, n1 = n_faces<1>(d);
+    if (t < n1) adj_divergence_face<1>(d, aW, aF1, Dt, ih, mdot_coef, t);
+    else if (t < n1 + n_faces<2>(d)) adj_divergence_face<2>(d, aW, aF2, Dt, -1, 0., t - n1);
+}
+
 // inversion reversed by the implicit-function theorem (active zones).
 // The solution p of the inversion satisfies G(p; W, B, gamma) = 0 with, over
 // the five hydrodynamic primitives, the rows mass, energy and momenta
@@ -515,7 +531,8 @@ __global__ void k_adj_divergence(const Dims d, const double *__restrict__ aW, do
 __global__ void __launch_bounds__(BLK) k_adj_invert(const Dims d, const Geom m, const double *__restrict__ pout,
                                                      const double *__restrict__ pg, const double *__restrict__ W7,
                                                      const double *__restrict__ psf, const int *__restrict__ pflag,
-                                                     double *ap, double *apg, double *aW, double *agam) {
+                                                     const int *__restrict__ fail0, double *ap, double *apg,
+                                                     double *aW, double *agam) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     double gsum = 0.;
     if (t < (long)d.n1 * d.n2 * d.n3) {
@@ -534,7 +551,9 @@ __global__ void __launch_bounds__(BLK) k_adj_invert(const Dims d, const Geom m, 
             if (pflag[c] != 0) {
                 for (int k = 0; k < 5; k++) apg[k * ks + c] += pb[k];
             } else {
-                // which solver produced p: redo the primary solve on the same input
+                // which solver produced p: the forward's count of primary
+                // failures in this stage when recorded, else redo the primary
+                // solve on the same input
                 double U[NPR], pf[NPR];
                 U[RHO] = W7[0 * ks + c];
                 U[UU] = W7[1 * ks + c];
@@ -544,8 +563,13 @@ __global__ void __launch_bounds__(BLK) k_adj_invert(const Dims d, const Geom m, 
                 U[KTOT] = W7[5 * ks + c];
                 U[B3] = W7[6 * ks + c];
                 face_average_b(d, m, psf, i, j, c, gi, U);
-                for (int k = 0; k < NPR; k++) pf[k] = pg[k * ks + c];
-                const bool entropy_row = utoprim_2d(d.gam, U, g0.gcov, g0.gcon, g0.g, pf) != 0;
+                bool entropy_row;
+                if (fail0) {
+                    entropy_row = fail0[c] != 0;
+                } else {
+                    for (int k = 0; k < NPR; k++) pf[k] = pg[k * ks + c];
+                    entropy_row = utoprim_2d(d.gam, U, g0.gcov, g0.gcon, g0.g, pf) != 0;
+                }
                 constexpr int N = ADJ_NP + 1;
                 const Geo<double> &gm = g0;   // the metric is data: no derivative parts
                 double pr[NPR];
@@ -617,10 +641,11 @@ __global__ void __launch_bounds__(BLK) k_adj_invert(const Dims d, const Geom m, 
 
 namespace {
 
-// source term reversed (active zones): ap += Dt (d dU / d pb)^T aW, agam
+// source term reversed (active zones): ap += Dt (d dU / d pb)^T aW, agam;
+// and the U^n cache: aU += aW
 __global__ void __launch_bounds__(BLK) k_adj_source(const Dims d, const Geom m, const double *__restrict__ pb,
-                                                     const double *__restrict__ aW, double *ap, double Dt,
-                                                     double *agam) {
+                                                     const double *__restrict__ aW, double *ap, double *aU,
+                                                     double Dt, double *agam) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     double gsum = 0.;
     if (t < (long)d.n1 * d.n2 * d.n3) {
@@ -631,6 +656,10 @@ __global__ void __launch_bounds__(BLK) k_adj_source(const Dims d, const Geom m, 
         double wb[NPR];
         bool any = false;
         for (int k = 0; k < NPR; k++) { wb[k] = aW[k * ks + c]; any |= (k >= UU && k <= U3 && wb[k] != 0.); }
+        // U^n feeds both sub-steps' updates: aU += aW over the components the
+        // inversion reads from the update (not B1, B2, which come from the faces)
+        for (int k = 0; k < NPR; k++)
+            if (k != B1 && k != B2) aU[k * ks + c] += wb[k];
         if (any) {
             Geo<double> g0;
             load_geo(d, m, i, j, CENT, g0);
@@ -669,19 +698,6 @@ __global__ void __launch_bounds__(BLK) k_adj_cons_of_state(const Dims d, const G
         }
     }
     block_add(gsum, agam);
-}
-
-// U^n feeds both sub-steps' updates: aU += aW over the components the
-// inversion reads from the update (not B1, B2, which come from the faces)
-__global__ void k_adj_cache_add(const Dims d, const double *__restrict__ aW, double *aU) {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)d.n1 * d.n2 * d.n3) return;
-    const int z = d.ng3 + (int)(t % d.n3);
-    const int j = d.ng2 + (int)((t / d.n3) % d.n2);
-    const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
-    const long c = cix(d, i, j, z), ks = d.ks;
-    for (int k = 0; k < NPR; k++)
-        if (k != B1 && k != B2) aU[k * ks + c] += aW[k * ks + c];
 }
 
 // centre EMF reversed (2-D: x3 component only; active zones plus one ring):
@@ -969,12 +985,13 @@ void adj_bound(hamr_ctx *ctx, const double *pv, double *ap, double *aps) {
 struct StageRec {
     const double *pin, *pout, *psin, *psout, *W, *F1, *F2;
     const int *pflag;
+    const int *fail0;   // primary-solver failures of this stage (nullptr: not recorded)
 };
 
 // the stage just run by the context, read from its own buffers
 StageRec ctx_stage(const hamr_ctx *ctx, int full) {
-    return full ? StageRec{ctx->ph, ctx->p, ctx->psh, ctx->ps, ctx->W, ctx->F1, ctx->F2, ctx->pflag}
-                : StageRec{ctx->p, ctx->ph, ctx->ps, ctx->psh, ctx->W, ctx->F1, ctx->F2, ctx->pflag};
+    return full ? StageRec{ctx->ph, ctx->p, ctx->psh, ctx->ps, ctx->W, ctx->F1, ctx->F2, ctx->pflag, nullptr}
+                : StageRec{ctx->p, ctx->ph, ctx->ps, ctx->psh, ctx->W, ctx->F1, ctx->F2, ctx->pflag, nullptr};
 }
 
 // reverse of one sub-step. apin/apsin: cotangents of the stage's input
@@ -995,14 +1012,14 @@ int adj_stage(hamr_adjoint *a, int full, double dt, double mdot_coef, const Stag
     ACK(cudaMemsetAsync(a->aEc, 0, 4 * sizeof(double) * ks, s));
     // ghost fill of the output, then the inversion (p_out <- W, guess pin)
     adj_bound(ctx, r.pout, apout, apsout);
-    k_adj_invert<<<nb(nz), BLK, 0, s>>>(d, m, r.pout, r.pin, r.W, r.psout, r.pflag, apout, apin, a->aW, a->agam);
+    k_adj_invert<<<nb(nz), BLK, 0, s>>>(d, m, r.pout, r.pin, r.W, r.psout, r.pflag, r.fail0, apout, apin, a->aW,
+                                        a->agam);
     // U[B1], U[B2] from the updated faces
     k_adj_face_average<<<nb(nedge), BLK, 0, s>>>(d, m, a->aW, apsout);
     // update: U^n (cache), source at pin, flux divergence (+ objective)
-    k_adj_cache_add<<<nb(nz), BLK, 0, s>>>(d, a->aW, a->aU);
-    k_adj_source<<<nb(nz), BLK, 0, s>>>(d, m, r.pin, a->aW, apin, Dt, a->agam);
-    k_adj_divergence<1><<<nb(n_faces<1>(d)), BLK, 0, s>>>(d, a->aW, a->aF1, Dt, a->ih, full ? mdot_coef : 0.);
-    k_adj_divergence<2><<<nb(n_faces<2>(d)), BLK, 0, s>>>(d, a->aW, a->aF2, Dt, -1, 0.);
+    k_adj_source<<<nb(nz), BLK, 0, s>>>(d, m, r.pin, a->aW, apin, a->aU, Dt, a->agam);
+    k_adj_divergence12<<<nb(n_faces<1>(d) + n_faces<2>(d)), BLK, 0, s>>>(d, a->aW, a->aF1, a->aF2, Dt, a->ih,
+                                                                        full ? mdot_coef : 0.);
     // face update: edge EMFs; ps^n -> psh carries the cotangent over
     k_adj_face_update_emf<<<nb(nedge), BLK, 0, s>>>(d, m, apsout, a->aemf, Dt);
     if (!full) k_adj_face_carry<<<nb(nedge), BLK, 0, s>>>(d, a->apsh, a->aps);
@@ -1011,19 +1028,20 @@ int adj_stage(hamr_adjoint *a, int full, double dt, double mdot_coef, const Stag
     k_adj_emf_centre<<<nb((long)(d.n1 + 2) * (d.n2 + 2)), BLK, 0, s>>>(d, m, r.pin, a->aEc, apin);
     // flux fixes, then the face fluxes -> pin (and the normal face field)
     k_adj_fix_flux<<<nb((long)d.G1 + d.G2), BLK, 0, s>>>(d, r.F1, a->aF1, a->aF2);
-    k_adj_flux<1><<<nb(FTEAM * n_faces<1>(d)), BLK, 0, s>>>(d, m, r.pin, r.psin, a->aF1, apin, apsin, a->agam);
-    k_adj_flux<2><<<nb(FTEAM * n_faces<2>(d)), BLK, 0, s>>>(d, m, r.pin, r.psin, a->aF2, apin, apsin, a->agam);
+    k_adj_flux12<<<nb(FTEAM * (n_faces<1>(d) + n_faces<2>(d))), BLK, 0, s>>>(d, m, r.pin, r.psin, a->aF1, a->aF2,
+                                                                            apin, apsin, a->agam);
     ACK(cudaGetLastError());
     return HAMR_OK;
 }
 
 // One step's record, REC_PLANES planes of the block: its input state (p, ps),
 // the half sub-step's output (ph, psh), each sub-step's conserved update,
-// fixed x1/x2 fluxes and solver flags (the two int planes share one).
-constexpr int REC_PLANES = 75;
+// fixed x1/x2 fluxes, solver flags (the two int planes share one) and
+// solver-failure counts (4 int planes per sub-step, plane 0 = primary).
+constexpr int REC_PLANES = 79;
 struct Slot {
     double *p, *ps, *ph, *psh, *Wh, *Wf, *F1h, *F2h, *F1f, *F2f;
-    int *flh, *flf;
+    int *flh, *flf, *fih, *fif;
 };
 Slot slot_of(double *base, long ks) {
     Slot r;
@@ -1031,13 +1049,16 @@ Slot slot_of(double *base, long ks) {
     r.Wh = base + 24 * ks; r.Wf = base + 31 * ks;
     r.F1h = base + 38 * ks; r.F2h = base + 47 * ks; r.F1f = base + 56 * ks; r.F2f = base + 65 * ks;
     r.flh = reinterpret_cast<int *>(base + 74 * ks); r.flf = r.flh + ks;
+    r.fih = reinterpret_cast<int *>(base + 75 * ks); r.fif = r.fih + 4 * ks;
     return r;
 }
 
 // one fixed-size step of the context that leaves its intermediates in the
-// record: the stages write their half-step state, updates, fluxes and flags
-// straight into the slot (the context's buffers are swapped for the slot's
-// while the launches are issued, and put back after)
+// record: the stages write their half-step state, updates, fluxes, flags and
+// solver-failure counts straight into the slot (the context's buffers are
+// swapped for the slot's while the launches are issued, and put back after;
+// the context's own failure counts do not see these replays of steps the
+// forward sweep already counted)
 int record_step(hamr_adjoint *a, double dt, const Slot &r) {
     hamr_ctx *ctx = a->ctx;
     const Dims &d = ctx->d;
@@ -1045,17 +1066,20 @@ int record_step(hamr_adjoint *a, double dt, const Slot &r) {
     const size_t cb = sizeof(double) * d.ks;
     ACK(cudaMemcpyAsync(r.p, ctx->p, NPR * cb, cudaMemcpyDeviceToDevice, s));
     ACK(cudaMemcpyAsync(r.ps, ctx->ps, 3 * cb, cudaMemcpyDeviceToDevice, s));
+    ACK(cudaMemsetAsync(r.fih, 0, 8 * sizeof(int) * d.ks, s));
     struct Swap {
         hamr_ctx *c;
         double *ph, *psh, *W, *F1, *F2;
-        int *pflag;
-        ~Swap() { c->ph = ph; c->psh = psh; c->W = W; c->F1 = F1; c->F2 = F2; c->pflag = pflag; }
-    } keep{ctx, ctx->ph, ctx->psh, ctx->W, ctx->F1, ctx->F2, ctx->pflag};
+        int *pflag, *failimage;
+        ~Swap() {
+            c->ph = ph; c->psh = psh; c->W = W; c->F1 = F1; c->F2 = F2; c->pflag = pflag; c->failimage = failimage;
+        }
+    } keep{ctx, ctx->ph, ctx->psh, ctx->W, ctx->F1, ctx->F2, ctx->pflag, ctx->failimage};
     ctx->ph = r.ph; ctx->psh = r.psh;
-    ctx->W = r.Wh; ctx->F1 = r.F1h; ctx->F2 = r.F2h; ctx->pflag = r.flh;
+    ctx->W = r.Wh; ctx->F1 = r.F1h; ctx->F2 = r.F2h; ctx->pflag = r.flh; ctx->failimage = r.fih;
     int rc = launch_stage(ctx, 0, StepSize{nullptr, 0.5, 0.5 * dt, dt}, false);
     if (rc) return rc;
-    ctx->W = r.Wf; ctx->F1 = r.F1f; ctx->F2 = r.F2f; ctx->pflag = r.flf;
+    ctx->W = r.Wf; ctx->F1 = r.F1f; ctx->F2 = r.F2f; ctx->pflag = r.flf; ctx->failimage = r.fif;
     return launch_stage(ctx, 1, StepSize{nullptr, 1.0, dt, dt}, false);
 }
 
@@ -1145,8 +1169,8 @@ int rec_step(hamr_adjoint *a, double dt, double *slot) {
 int bwd_step(hamr_adjoint *a, double dt, double *slot, const double *next_p, const double *next_ps) {
     return graph_run(a, a->bwd_graph, {dt, slot, next_p}, [&]() -> int {
         const Slot r = slot_of(slot, a->ctx->d.ks);
-        const StageRec half{r.p, r.ph, r.ps, r.psh, r.Wh, r.F1h, r.F2h, r.flh};
-        const StageRec full{r.ph, next_p, r.psh, next_ps, r.Wf, r.F1f, r.F2f, r.flf};
+        const StageRec half{r.p, r.ph, r.ps, r.psh, r.Wh, r.F1h, r.F2h, r.flh, r.fih};
+        const StageRec full{r.ph, next_p, r.psh, next_ps, r.Wf, r.F1f, r.F2f, r.flf, r.fif};
         return adj_step(a, dt, dt, half, full);
     });
 }
