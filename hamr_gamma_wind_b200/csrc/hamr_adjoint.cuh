@@ -943,7 +943,13 @@ struct hamr_adjoint {
     double *agam = nullptr, *J = nullptr;   // 1 double each
     double *p0 = nullptr, *ps0 = nullptr;   // the step's input state while it is reversed
     std::vector<double *> store;            // checkpoints (12 planes each)
-    std::vector<double *> slots;            // per-step records of a segment (REC_PLANES each)
+    std::vector<double *> slots;            // two banks of per-step records (REC_PLANES each)
+    double *ends[2] = {nullptr, nullptr};   // per bank: the state a segment ends in (12 planes)
+    int bank_len = 0;                       // records per bank
+    // segments are recomputed on s2 while the previous one is reversed on the
+    // context's stream; events order the two over the banks
+    cudaStream_t s2 = nullptr;
+    cudaEvent_t ev_sweep = nullptr, ev_rec[2] = {nullptr, nullptr}, ev_rev[2] = {nullptr, nullptr};
     // captured graphs, per step size and record slot: a forward step with the
     // objective term, a recorded forward step, a reversed step
     using Key = std::tuple<double, const void *, const void *>;
@@ -1053,32 +1059,36 @@ Slot slot_of(double *base, long ks) {
     return r;
 }
 
-// one fixed-size step of the context that leaves its intermediates in the
-// record: the stages write their half-step state, updates, fluxes, flags and
-// solver-failure counts straight into the slot (the context's buffers are
-// swapped for the slot's while the launches are issued, and put back after;
-// the context's own failure counts do not see these replays of steps the
-// forward sweep already counted)
-int record_step(hamr_adjoint *a, double dt, const Slot &r) {
+// one fixed-size step from the record's input state (r.p, r.ps) to
+// (next_p, next_ps) that leaves its intermediates in the record: the stages
+// write their half-step state, updates, fluxes, flags and solver-failure
+// counts straight into the slot. The context's buffer pointers are swapped
+// for these while the launches are issued and put back after, so the
+// context's own state, and its failure counts, do not see these replays of
+// steps the forward sweep already took. The full sub-step updates the faces
+// in place, so they are copied to next_ps first; it reads no p^n (the half
+// sub-step cached U^n), so p^{n+1} goes straight to next_p.
+int record_step(hamr_adjoint *a, double dt, const Slot &r, double *next_p, double *next_ps) {
     hamr_ctx *ctx = a->ctx;
     const Dims &d = ctx->d;
     cudaStream_t s = ctx->stream;
     const size_t cb = sizeof(double) * d.ks;
-    ACK(cudaMemcpyAsync(r.p, ctx->p, NPR * cb, cudaMemcpyDeviceToDevice, s));
-    ACK(cudaMemcpyAsync(r.ps, ctx->ps, 3 * cb, cudaMemcpyDeviceToDevice, s));
     ACK(cudaMemsetAsync(r.fih, 0, 8 * sizeof(int) * d.ks, s));
+    ACK(cudaMemcpyAsync(next_ps, r.ps, 3 * cb, cudaMemcpyDeviceToDevice, s));
     struct Swap {
         hamr_ctx *c;
-        double *ph, *psh, *W, *F1, *F2;
+        double *p, *ps, *ph, *psh, *W, *F1, *F2;
         int *pflag, *failimage;
         ~Swap() {
-            c->ph = ph; c->psh = psh; c->W = W; c->F1 = F1; c->F2 = F2; c->pflag = pflag; c->failimage = failimage;
+            c->p = p; c->ps = ps; c->ph = ph; c->psh = psh; c->W = W; c->F1 = F1; c->F2 = F2;
+            c->pflag = pflag; c->failimage = failimage;
         }
-    } keep{ctx, ctx->ph, ctx->psh, ctx->W, ctx->F1, ctx->F2, ctx->pflag, ctx->failimage};
-    ctx->ph = r.ph; ctx->psh = r.psh;
+    } keep{ctx, ctx->p, ctx->ps, ctx->ph, ctx->psh, ctx->W, ctx->F1, ctx->F2, ctx->pflag, ctx->failimage};
+    ctx->p = r.p; ctx->ps = r.ps; ctx->ph = r.ph; ctx->psh = r.psh;
     ctx->W = r.Wh; ctx->F1 = r.F1h; ctx->F2 = r.F2h; ctx->pflag = r.flh; ctx->failimage = r.fih;
     int rc = launch_stage(ctx, 0, StepSize{nullptr, 0.5, 0.5 * dt, dt}, false);
     if (rc) return rc;
+    ctx->p = next_p; ctx->ps = next_ps;
     ctx->W = r.Wf; ctx->F1 = r.F1f; ctx->F2 = r.F2f; ctx->pflag = r.flf; ctx->failimage = r.fif;
     return launch_stage(ctx, 1, StepSize{nullptr, 1.0, dt, dt}, false);
 }
@@ -1129,9 +1139,11 @@ int step_backward(hamr_adjoint *a, double dt, double w) {
 
 // forward step + objective term, and reversed step, replayed from graphs
 // captured once per step size (the step is launch-bound at these sizes)
+// (captured on the context's stream, where the body issues its work, and
+// launched on `run`)
 template <class F>
 int graph_run(hamr_adjoint *a, std::map<hamr_adjoint::Key, cudaGraphExec_t> &cache, hamr_adjoint::Key key,
-              F body) {
+              cudaStream_t run, F body) {
     cudaStream_t s = a->ctx->stream;
     auto it = cache.find(key);
     if (it == cache.end()) {
@@ -1147,12 +1159,12 @@ int graph_run(hamr_adjoint *a, std::map<hamr_adjoint::Key, cudaGraphExec_t> &cac
         if (e != cudaSuccess) return afail(a, e, "cudaGraphInstantiate");
         it = cache.emplace(key, x).first;
     }
-    ACK(cudaGraphLaunch(it->second, s));
+    ACK(cudaGraphLaunch(it->second, run));
     return HAMR_OK;
 }
 
 int fwd_step(hamr_adjoint *a, double dt) {
-    return graph_run(a, a->fwd_graph, {dt, nullptr, nullptr}, [&]() -> int {
+    return graph_run(a, a->fwd_graph, {dt, nullptr, nullptr}, a->ctx->stream, [&]() -> int {
         const int rc = fixed_step(a->ctx, dt);
         if (rc) return rc;
         k_mdot_accum<<<nb(a->ctx->d.n2), BLK, 0, a->ctx->stream>>>(a->ctx->d, a->ctx->F1, a->ih, dt, a->J);
@@ -1160,14 +1172,16 @@ int fwd_step(hamr_adjoint *a, double dt) {
     });
 }
 
-int rec_step(hamr_adjoint *a, double dt, double *slot) {
-    return graph_run(a, a->rec_graph, {dt, slot, nullptr},
-                     [&]() -> int { return record_step(a, dt, slot_of(slot, a->ctx->d.ks)); });
+// recorded step on the second stream; next_p/next_ps: where its output goes
+int rec_step(hamr_adjoint *a, double dt, double *slot, double *next_p, double *next_ps) {
+    return graph_run(a, a->rec_graph, {dt, slot, next_p}, a->s2, [&]() -> int {
+        return record_step(a, dt, slot_of(slot, a->ctx->d.ks), next_p, next_ps);
+    });
 }
 
 // reversed step from slot's record; next_p/next_ps: the step's output state
 int bwd_step(hamr_adjoint *a, double dt, double *slot, const double *next_p, const double *next_ps) {
-    return graph_run(a, a->bwd_graph, {dt, slot, next_p}, [&]() -> int {
+    return graph_run(a, a->bwd_graph, {dt, slot, next_p}, a->ctx->stream, [&]() -> int {
         const Slot r = slot_of(slot, a->ctx->d.ks);
         const StageRec half{r.p, r.ph, r.ps, r.psh, r.Wh, r.F1h, r.F2h, r.flh, r.fih};
         const StageRec full{r.ph, next_p, r.psh, next_ps, r.Wf, r.F1f, r.F2f, r.flf, r.fif};
@@ -1217,7 +1231,10 @@ int hamr_adjoint_create(hamr_ctx *ctx, int mdot_face, hamr_adjoint **out) {
         }
         cudaMemsetAsync(*x.p, 0, x.n, ctx->stream);
     }
-    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+    bool ok = cudaStreamCreateWithFlags(&a->s2, cudaStreamNonBlocking) == cudaSuccess;
+    for (cudaEvent_t *e : {&a->ev_sweep, &a->ev_rec[0], &a->ev_rec[1], &a->ev_rev[0], &a->ev_rev[1]})
+        ok = ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok || cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
         hamr_adjoint_destroy(a);
         return HAMR_E_CUDA;
     }
@@ -1231,8 +1248,13 @@ int hamr_adjoint_destroy(hamr_adjoint *a) {
     for (double *p : {a->ap, a->aps, a->aph, a->apsh, a->aU, a->aW, a->aF1, a->aF2, a->aF3, a->aEc, a->aemf,
                       a->agam, a->J, a->p0, a->ps0})
         cudaFree(p);
+    if (a->s2) cudaStreamSynchronize(a->s2);
     for (double *p : a->store) cudaFree(p);
     for (double *p : a->slots) cudaFree(p);
+    for (double *p : a->ends) cudaFree(p);
+    for (cudaEvent_t e : {a->ev_sweep, a->ev_rec[0], a->ev_rec[1], a->ev_rev[0], a->ev_rev[1]})
+        if (e) cudaEventDestroy(e);
+    if (a->s2) cudaStreamDestroy(a->s2);
     for (auto *g : {&a->fwd_graph, &a->rec_graph, &a->bwd_graph})
         for (auto &kv : *g) cudaGraphExecDestroy(kv.second);
     delete a;
@@ -1287,9 +1309,11 @@ int hamr_mdot_forward(hamr_adjoint *a, int nsteps, const double *dt, double *J) 
 // `every` steps on the forward sweep, and reverses segment by segment: each
 // segment is recomputed from its checkpoint, recording every step's
 // intermediates, then its steps are reversed from those records (no forward
-// work in the reverse). grad_p (9 planes) / grad_ps (3 planes) are host
-// arrays in the context's layout (NULL: not copied). The context's state is
-// restored to its initial value on return.
+// work in the reverse). Two banks of records let segment sg-1 be recomputed
+// on a second stream while segment sg is reversed on the context's stream.
+// grad_p (9 planes) / grad_ps (3 planes) are host arrays in the context's
+// layout (NULL: not copied). The context's state is restored to its initial
+// value on return.
 int hamr_adjoint_run(hamr_adjoint *a, int nsteps, const double *dt, int every, double *J, double *grad_p,
                      double *grad_ps, double *grad_gam) {
     if (!a || !dt || nsteps < 1 || every < 1) return HAMR_E_ARG;
@@ -1306,10 +1330,24 @@ int hamr_adjoint_run(hamr_adjoint *a, int nsteps, const double *dt, int every, d
         if (cudaMalloc((void **)&p, state) != cudaSuccess) return HAMR_E_NOMEM;
         a->store.push_back(p);
     }
-    while (a->slots.size() < (size_t)seglen) {
-        double *p = nullptr;
-        if (cudaMalloc((void **)&p, REC_PLANES * cb) != cudaSuccess) return HAMR_E_NOMEM;
-        a->slots.push_back(p);
+    if (a->bank_len < seglen) {   // (re)allocate both banks for the longer segment
+        ACK(cudaStreamSynchronize(s));
+        ACK(cudaStreamSynchronize(a->s2));
+        for (double *p : a->slots) cudaFree(p);
+        a->slots.clear();
+        for (auto *g : {&a->rec_graph, &a->bwd_graph}) {
+            for (auto &kv : *g) cudaGraphExecDestroy(kv.second);
+            g->clear();
+        }
+        a->bank_len = 0;
+        for (int k = 0; k < 2 * seglen; k++) {
+            double *p = nullptr;
+            if (cudaMalloc((void **)&p, REC_PLANES * cb) != cudaSuccess) return HAMR_E_NOMEM;
+            a->slots.push_back(p);
+        }
+        for (double *&e : a->ends)
+            if (!e && cudaMalloc((void **)&e, state) != cudaSuccess) return HAMR_E_NOMEM;
+        a->bank_len = seglen;
     }
     auto save = [&](double *dst) {
         cudaMemcpyAsync(dst, ctx->p, NPR * cb, cudaMemcpyDeviceToDevice, s);
@@ -1331,21 +1369,47 @@ int hamr_adjoint_run(hamr_adjoint *a, int nsteps, const double *dt, int every, d
     if (rc) return rc;
     double Jval = 0.;
     ACK(cudaMemcpyAsync(&Jval, a->J, sizeof(double), cudaMemcpyDeviceToHost, s));
-    ACK(cudaStreamSynchronize(s));
-    // reverse sweep: recompute each segment with records, then reverse it;
-    // the last step of a segment ends in the context's own state
+    ACK(cudaEventRecord(a->ev_sweep, s));
+    ACK(cudaStreamWaitEvent(a->s2, a->ev_sweep, 0));
     if ((rc = hamr_adjoint_zero(a))) return rc;
-    for (int sg = nseg - 1; sg >= 0 && rc == HAMR_OK; sg--) {
-        const int n0 = sg * every, n1 = n0 + every < nsteps ? n0 + every : nsteps;
-        load(a->store[sg]);
-        for (int n = n0; n < n1 && rc == HAMR_OK; n++) rc = rec_step(a, dt[n], a->slots[n - n0]);
-        for (int n = n1 - 1; n >= n0 && rc == HAMR_OK; n--) {
-            const bool last = n == n1 - 1;
-            const Slot nx = slot_of(a->slots[last ? 0 : n + 1 - n0], d.ks);
-            rc = bwd_step(a, dt[n], a->slots[n - n0], last ? ctx->p : nx.p, last ? ctx->ps : nx.ps);
+    // segment sg uses bank sg % 2: record k of the segment is slot k of the
+    // bank, and its last step ends in the bank's `ends` state
+    auto slot = [&](int b, int k) { return a->slots[(size_t)b * a->bank_len + k]; };
+    auto recompute = [&](int sg) -> int {
+        const int b = sg & 1, n0 = sg * every, n1 = n0 + every < nsteps ? n0 + every : nsteps;
+        ACK(cudaStreamWaitEvent(a->s2, a->ev_rev[b], 0));   // the bank's previous segment is reversed
+        const double *src = a->store[sg];
+        ACK(cudaMemcpyAsync(slot(b, 0), src, state, cudaMemcpyDeviceToDevice, a->s2));
+        for (int n = n0; n < n1; n++) {
+            const int k = n - n0;
+            double *nx = n + 1 < n1 ? slot(b, k + 1) : a->ends[b];
+            const int r = rec_step(a, dt[n], slot(b, k), nx, nx + NPR * d.ks);
+            if (r) return r;
         }
+        ACK(cudaEventRecord(a->ev_rec[b], a->s2));
+        return HAMR_OK;
+    };
+    auto reverse = [&](int sg) -> int {
+        const int b = sg & 1, n0 = sg * every, n1 = n0 + every < nsteps ? n0 + every : nsteps;
+        ACK(cudaStreamWaitEvent(s, a->ev_rec[b], 0));
+        for (int n = n1 - 1; n >= n0; n--) {
+            const int k = n - n0;
+            const double *nx = n + 1 < n1 ? slot(b, k + 1) : a->ends[b];
+            const int r = bwd_step(a, dt[n], slot(b, k), nx, nx + NPR * d.ks);
+            if (r) return r;
+        }
+        ACK(cudaEventRecord(a->ev_rev[b], s));
+        return HAMR_OK;
+    };
+    rc = recompute(nseg - 1);
+    for (int sg = nseg - 1; sg >= 0 && rc == HAMR_OK; sg--) {
+        if (sg >= 1 && (rc = recompute(sg - 1))) break;
+        rc = reverse(sg);
     }
-    if (rc) return rc;
+    if (rc) {
+        cudaStreamSynchronize(a->s2);
+        return rc;
+    }
     // the initial ghost fill, reversed, folds ghost cotangents onto the zones
     load(a->store[0]);
     adj_bound(ctx, ctx->p, a->ap, a->aps);
