@@ -22,7 +22,7 @@ class HamrParams(ctypes.Structure):
                 ("dx1", _d), ("dx2", _d), ("dx3", _d), ("gam", _d), ("cour", _d),
                 ("pole1", _i), ("pole2", _i), ("bc1", _i), ("bc2", _i), ("bc3", _i),
                 ("ct_upwind", _i), ("precision", _i), ("stream", _vp), ("inversion", _i), ("recon", _i),
-                ("riemann", _i)]
+                ("riemann", _i), ("halo", _i)]
 
 
 ERRORS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "out of device memory",
@@ -86,6 +86,12 @@ def load(strict: bool = False):
     L.hamr_step_backward.argtypes = [_vp, _d, _d]
     L.hamr_mdot_forward.argtypes = [_vp, _i, _vp, P(_d)]
     L.hamr_adjoint_run.argtypes = [_vp, _i, _vp, _i, P(_d), _vp, _vp, P(_d)]
+    L.hamr_bound_dim.argtypes = [_vp, _i, _i]
+    L.hamr_halo_count.argtypes = [_vp]
+    L.hamr_halo_count.restype = _l
+    L.hamr_halo_pack.argtypes = [_vp, _i, _i, _vp]
+    L.hamr_halo_unpack.argtypes = [_vp, _i, _i, _vp]
+    L.hamr_cfl_dirs.argtypes = [_vp, _vp]
     _libs[key] = L
     return L
 
@@ -98,7 +104,8 @@ SYMBOLS = ["hamr_ctx_create", "hamr_ctx_destroy", "hamr_last_error", "hamr_strid
            "hamr_batch_create", "hamr_batch_destroy", "hamr_batch_last_error", "hamr_batch_step",
            "hamr_batch_advance", "hamr_batch_autotune", "hamr_batch_tuning",
            "hamr_adjoint_create", "hamr_adjoint_destroy", "hamr_adjoint_last_error", "hamr_adjoint_cotangent",
-           "hamr_adjoint_zero", "hamr_step_backward", "hamr_mdot_forward", "hamr_adjoint_run"]
+           "hamr_adjoint_zero", "hamr_step_backward", "hamr_mdot_forward", "hamr_adjoint_run",
+           "hamr_bound_dim", "hamr_halo_count", "hamr_halo_pack", "hamr_halo_unpack", "hamr_cfl_dirs"]
 NOALLOC_MAX_CELLS = 32768
 
 BATCH_PHASES = ["flux3", "flux2", "flux1", "fix_flux", "emf_centre", "emf_edge", "pole_average",

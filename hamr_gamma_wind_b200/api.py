@@ -81,7 +81,7 @@ class Block:
 
     def __init__(self, n1, n2, n3, dx, gam, cour=0.8, bc=("outflow", "pole_trans", "periodic"),
                  poles=(1, 1), ct_upwind=True, precision="fp64", strict=False, ng=3, stream=None,
-                 inversion="2d", recon="ppm", riemann="hll"):
+                 inversion="2d", recon="ppm", riemann="hll", halo=0):
         self.L = _lib.load(strict)
         self.n1, self.n2, self.n3, self.ng = n1, n2, n3, ng
         self.g1 = n1 + 2 * ng
@@ -90,7 +90,7 @@ class Block:
         prm = _lib.HamrParams(n1, n2, n3, ng, 0, 0, float(dx[0]), float(dx[1]), float(dx[2]), float(gam),
                               float(cour), int(poles[0]), int(poles[1]), BC[bc[0]], BC[bc[1]], BC[bc[2]],
                               int(bool(ct_upwind)), PRECISION[precision], stream, INVERSION[inversion],
-                              RECON[recon], RIEMANN[riemann])
+                              RECON[recon], RIEMANN[riemann], int(halo))
         ctx = ctypes.c_void_p()
         rc = self.L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx))
         if rc:
@@ -196,6 +196,30 @@ class Block:
         ptrs = [ctypes.c_void_p() for _ in range(4)]
         self._check(self.L.hamr_device_state(self.ctx, *[ctypes.byref(x) for x in ptrs]), "hamr_device_state")
         return [x.value for x in ptrs]
+
+    # -- a slab of a domain decomposed along x1 (halo != 0) ---------------------
+    def bound_dim(self, full: int, dim: int):
+        """Ghost fill of one direction on the physical sides (hamr_bound_dim)."""
+        self._check(self.L.hamr_bound_dim(self.ctx, int(full), int(dim)), "hamr_bound_dim")
+
+    def halo_count(self) -> int:
+        return int(self.L.hamr_halo_count(self.ctx))
+
+    def halo_pack(self, full: int, side: int, dev_ptr: int):
+        """Active layers next to x1 side `side` into a device buffer."""
+        self._check(self.L.hamr_halo_pack(self.ctx, int(full), int(side), ctypes.c_void_p(dev_ptr)),
+                    "hamr_halo_pack")
+
+    def halo_unpack(self, full: int, side: int, dev_ptr: int):
+        """A device buffer into the ghost layers beyond x1 side `side`."""
+        self._check(self.L.hamr_halo_unpack(self.ctx, int(full), int(side), ctypes.c_void_p(dev_ptr)),
+                    "hamr_halo_unpack")
+
+    def cfl_dirs(self):
+        """Per-direction CFL minima of the last full sub-step (hamr_cfl_dirs)."""
+        out = np.zeros(3)
+        self._check(self.L.hamr_cfl_dirs(self.ctx, out.ctypes.data_as(ctypes.c_void_p)), "hamr_cfl_dirs")
+        return out
 
 
 class Batch:

@@ -111,6 +111,68 @@ __device__ __forceinline__ void block_add(double v, double *target) {
 
 namespace {
 
+// ---- PPM stencil weights -------------------------------------------------
+// para (GPU_interp.h:60-111) is linear in its five inputs on each branch of
+// its limiter and clamps; these are the weights of the lower (upper == false)
+// or upper edge value in the branch the values take, built from the
+// branch-local coefficients of the three MC slopes (the dual-number
+// derivative of para, without carrying five derivatives through every
+// operation)
+__device__ __forceinline__ void para_weights(const double *y, bool upper, double *w) {
+    double dq[4], c[4][3];   // slope i (1..3) = sum_k c[i][k] y[i - 1 + k]
+#pragma unroll
+    for (int i = 1; i < 4; i++) {
+        const double Dqm = 2. * (y[i] - y[i - 1]);
+        const double Dqp = 2. * (y[i + 1] - y[i]);
+        const double Dqc = 0.5 * (y[i + 1] - y[i - 1]);
+        const double aDqm = d_fabs(Dqm), aDqp = d_fabs(Dqp), aDqc = d_fabs(Dqc);
+        const double sm = Dqm * Dqp;
+        const double mn = d_min(aDqm, aDqp);
+        const double on = (double)(sm > 0.);
+        const double sc = Dqc > 0. ? 1. : -1.;   // the sign given to the slope
+        if (aDqc < mn) {
+            dq[i] = (sc * aDqc) * on;
+            const double g = sc * (Dqc < 0. ? -1. : 1.) * on * 0.5;   // d|Dqc| = sign(Dqc) dDqc
+            c[i][0] = -g; c[i][1] = 0.; c[i][2] = g;
+        } else if (aDqm < aDqp) {
+            dq[i] = (sc * mn) * on;
+            const double g = sc * (Dqm < 0. ? -1. : 1.) * on * 2.;
+            c[i][0] = -g; c[i][1] = g; c[i][2] = 0.;
+        } else {
+            dq[i] = (sc * mn) * on;
+            const double g = sc * (Dqp < 0. ? -1. : 1.) * on * 2.;
+            c[i][0] = 0.; c[i][1] = -g; c[i][2] = g;
+        }
+    }
+    double l = 0.5 * (y[2] + y[1]) - (dq[2] - dq[1]) / 6.0;
+    double r = 0.5 * (y[3] + y[2]) - (dq[3] - dq[2]) / 6.0;
+    double wl[5] = {0., 0.5, 0.5, 0., 0.}, wr[5] = {0., 0., 0.5, 0.5, 0.};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        wl[1 + k - 1] += c[1][k] / 6.0;   // - (dq2 - dq1)/6
+        wl[2 + k - 1] -= c[2][k] / 6.0;
+        wr[2 + k - 1] += c[2][k] / 6.0;   // - (dq3 - dq2)/6
+        wr[3 + k - 1] -= c[3][k] / 6.0;
+    }
+    const double qa = (r - y[2]) * (y[2] - l);
+    const double qd = (r - l);
+    const double qe = 6.0 * (y[2] - 0.5 * (l + r));
+    if (qa <= 0.) {
+        l = r = y[2];
+#pragma unroll
+        for (int k = 0; k < 5; k++) wl[k] = wr[k] = k == 2 ? 1. : 0.;
+    }
+    if (qd * (qd - qe) < 0.0) {
+#pragma unroll
+        for (int k = 0; k < 5; k++) wl[k] = (k == 2 ? 3. : 0.) - 2. * wr[k];
+    } else if (qd * (qd + qe) < 0.0) {
+#pragma unroll
+        for (int k = 0; k < 5; k++) wr[k] = (k == 2 ? 3. : 0.) - 2. * wl[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 5; k++) w[k] = upper ? wr[k] : wl[k];
+}
+
 // ---- reverse mode of one state's fluxes, conserved variables and speeds ----
 // Hand-written transpose of get_state + primtoflux (GPU_phys_mhd.h:432-628,
 // 672-761) over a constant metric: the forward values are recomputed, then
@@ -162,7 +224,10 @@ struct StateFwd {
     bool gfree;   // the Lorentz factor is sqrt(1 + q^2), not clamped
 };
 
-__device__ __forceinline__ void state_fwd(const double *pr, const Geo<double> &gm, double gam, StateFwd &f) {
+// need_k: the entropy K = P rho^-gam is wanted (its pow is skipped, K = 0,
+// where no entropy-flux cotangent can reach it)
+__device__ __forceinline__ void state_fwd(const double *pr, const Geo<double> &gm, double gam, StateFwd &f,
+                                          bool need_k = true) {
     const double *gc = gm.gcov;
     get_state(pr, gm, f.q);
     gamma_calc(pr, gm, &f.gam_l);
@@ -174,7 +239,7 @@ __device__ __forceinline__ void state_fwd(const double *pr, const Geo<double> &g
     f.w = pr[RHO] + f.P + pr[UU];
     f.bsq = dot4(f.q.bcon, f.q.bcov);
     f.eta = f.w + f.bsq;
-    f.K = entropy(gam, pr);
+    f.K = need_k ? entropy(gam, pr) : 0.;
 }
 
 __device__ __forceinline__ void bar_zero(StateBar &a) {
@@ -266,11 +331,10 @@ __device__ __forceinline__ void state_back(const double *pr, const Geo<double> &
 // (fb), of the conserved variables (ub) and of the fast speeds along DIR
 // (DIR == 0: conserved variables only)
 template <int DIR>
-__device__ void state_vjp(const double *pr, const Geo<double> &gm, double gam, const double *fb, const double *ub,
-                          double cmxb, double cmnb, double *pbar, double &gbar) {
+__device__ void state_vjp_from(const double *pr, const Geo<double> &gm, double gam, const StateFwd &f,
+                               const double *fb, const double *ub, double cmxb, double cmnb, double *pbar,
+                               double &gbar) {
     const double *gn = gm.gcon;
-    StateFwd f;
-    state_fwd(pr, gm, gam, f);
     const State<double> &q = f.q;
     const double u = pr[UU], w = f.w, bsq = f.bsq, eta = f.eta;
     StateBar a;
@@ -325,6 +389,14 @@ __device__ void state_vjp(const double *pr, const Geo<double> &gm, double gam, c
     state_back(pr, gm, gam, f, a, pbar, gbar);
 }
 
+template <int DIR>
+__device__ __forceinline__ void state_vjp(const double *pr, const Geo<double> &gm, double gam, const double *fb,
+                                          const double *ub, double cmxb, double cmnb, double *pbar, double &gbar) {
+    StateFwd f;
+    state_fwd(pr, gm, gam, f, ub[KTOT] != 0. || (DIR != 0 && fb[KTOT] != 0.));
+    state_vjp_from<DIR>(pr, gm, gam, f, fb, ub, cmxb, cmnb, pbar, gbar);
+}
+
 // geometric source of a state reversed (source in hamr_kernels.cu,
 // GPU_phys_mhd.h:34-175): the cotangents wb of dU[UU..U3] give, through the
 // connection, the cotangent of the stress tensor T^a_k = eta u^a u_k +
@@ -332,7 +404,7 @@ __device__ void state_vjp(const double *pr, const Geo<double> &gm, double gam, c
 __device__ void source_vjp(const double *pr, const Geo<double> &gm, double gam, const Dims &d, const Geom &m, long gi,
                            const double *wb, double *pbar, double &gbar) {
     StateFwd f;
-    state_fwd(pr, gm, gam, f);
+    state_fwd(pr, gm, gam, f, false);   // the source has no entropy row
     const State<double> &q = f.q;
     StateBar a;
     bar_zero(a);
@@ -405,14 +477,13 @@ __device__ __forceinline__ void adj_flux_face(const Dims &d, const Geom &m, cons
             if (polefix) pme[B1] = 0.;
             pme[KTOT] = 0.;   // read by no flux
             const double gam = d.gam;
+            // this side's state, kept for the reverse; the entropy flux only
+            // where its cotangent is nonzero
+            StateFwd f;
+            state_fwd(pme, g0, gam, f, Fb[KTOT] != 0.);
             double ta[NPR], tb[NPR], cmx_me, cmn_me, vd;
-            {
-                State<double> st;
-                get_state(pme, g0, st);
-                const double e = entropy(gam, pme);
-                primtoflux(gam, pme, st, DIR, g0, e, ta, &cmx_me, &cmn_me);
-                primtoflux(gam, pme, st, 0, g0, e, tb, &vd, &vd);
-            }
+            primtoflux(gam, pme, f.q, DIR, g0, f.K, ta, &cmx_me, &cmn_me);
+            primtoflux(gam, pme, f.q, 0, g0, f.K, tb, &vd, &vd);
             const double cmx_o = __shfl_xor_sync(tm, cmx_me, 1), cmn_o = __shfl_xor_sync(tm, cmn_me, 1);
             const double cmax_l = side ? cmx_o : cmx_me, cmin_l = side ? cmn_o : cmn_me;
             const double cmax_r = side ? cmx_me : cmx_o, cmin_r = side ? cmn_me : cmn_o;
@@ -450,21 +521,20 @@ __device__ __forceinline__ void adj_flux_face(const Dims &d, const Geom &m, cons
                 if (!take_rn && !(0. > -cmin_l)) cmnb = -sn * cminb;
             }
             double pb[ADJ_NP];
-            state_vjp<DIR>(pme, g0, gam, tfb, tub, cmxb, cmnb, pb, gsum);
+            state_vjp_from<DIR>(pme, g0, gam, f, tfb, tub, cmxb, cmnb, pb, gsum);
             atomicAdd(&aps[(long)(DIR - 1) * ks + c], pb[bn]);
             // PPM stencil weights of this side, primitive by primitive
 #pragma unroll 1
             for (int k = 0; k < ADJ_NP; k++) {
                 if (k == bn || (polefix && k == B1) || pb[k] == 0.) continue;
                 const double *pk = pv + (long)k * ks + c + (side - 3) * stride;
-                Dual<5> x[5], lo, hi;
+                double x[5], w[5];
 #pragma unroll
-                for (int s = 0; s < 5; s++) x[s] = dual_var<5>(pk[s * stride], s);
-                para(x, lo, hi);
-                const Dual<5> &e = side ? lo : hi;
+                for (int s = 0; s < 5; s++) x[s] = pk[s * stride];
+                para_weights(x, side == 0, w);   // left state: upper edge of the zone below
 #pragma unroll
                 for (int s = 0; s < 5; s++)
-                    if (e.d[s] != 0.) atomicAdd(&ap[k * ks + c + (side + s - 3) * stride], pb[k] * e.d[s]);
+                    if (w[s] != 0.) atomicAdd(&ap[k * ks + c + (side + s - 3) * stride], pb[k] * w[s]);
             }
         }
     }
@@ -1210,7 +1280,7 @@ int hamr_adjoint_create(hamr_ctx *ctx, int mdot_face, hamr_adjoint **out) {
     const Dims &d = ctx->d;
     // the configuration the reverse kernels are written for
     if (p.precision != HAMR_FP64 || p.recon != HAMR_RECON_PPM || p.inversion != HAMR_INV_2D || d.n3 != 1 ||
-        p.riemann != HAMR_RIEMANN_HLL ||
+        p.riemann != HAMR_RIEMANN_HLL || p.halo ||
         p.ng != 3 || p.bc1 != HAMR_BC_OUTFLOW || p.bc2 != HAMR_BC_POLE_REFL || !p.ct_upwind)
         return HAMR_E_ARG;
     if (mdot_face <= d.ng1 || mdot_face >= d.n1 + d.ng1) return HAMR_E_ARG;

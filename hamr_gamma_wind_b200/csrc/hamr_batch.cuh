@@ -383,6 +383,7 @@ int hamr_batch_create(hamr_ctx *const *blocks, int n, void *stream, hamr_batch *
         if (pk.precision != p0.precision || pk.recon != p0.recon || pk.inversion != p0.inversion ||
             pk.riemann != p0.riemann)
             return HAMR_E_ARG;
+        if (pk.halo) return HAMR_E_ARG;   // members are whole problems: no neighbours to exchange with
         for (int j = 0; j < k; j++)
             if (blocks[j] == blocks[k]) return HAMR_E_ARG;
     }

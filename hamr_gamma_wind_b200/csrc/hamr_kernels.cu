@@ -39,6 +39,7 @@ struct Dims {
     long ks, gs;
     double dx1, dx2, dx3, gam, cour;
     int pole1, pole2, bc1, bc2, bc3, ct_upwind, inversion, recon, riemann;
+    int halo;   // x1 sides filled by a neighbouring block (bit 0 lower, bit 1 upper)
 };
 
 struct Geom {
@@ -232,10 +233,12 @@ __device__ __forceinline__ void fix_flux_at(const Dims &d, T *F1, T *F2, T *F3, 
     if (u >= (long)d.G2 * d.G3) return;
     const int z = (int)(u % d.G3), j = (int)(u / d.G3);
     if (!(j >= d.ng2 - d.d2 && z >= d.ng3 - d.d3 && j < d.n2 + d.ng2 + d.d2 && z < d.n3 + d.ng3 + d.d3)) return;
+    // no inflow through the physical radial edges (not through a face shared
+    // with a neighbouring block)
     const long ci = RHO * ks + cix(d, d.ng1, j, z);
-    if (F1[ci] > T(0.)) F1[ci] = T(0.);
+    if (!(d.halo & 1) && F1[ci] > T(0.)) F1[ci] = T(0.);
     const long co = RHO * ks + cix(d, d.n1 + d.ng1, j, z);
-    if (F1[co] < T(0.)) F1[co] = T(0.);
+    if (!(d.halo & 2) && F1[co] < T(0.)) F1[co] = T(0.);
 }
 
 // items of fix_flux: (i, z) on the polar rows, then (j, z) on the radial edges
@@ -714,21 +717,27 @@ __device__ __forceinline__ void k_bound_x1_at(const Dims &d, const Geom &m, doub
     }
     double pr[NPR];
     Geo<double> gm;
-    long src = cix(d, d.ng1, j, z), dst = cix(d, ilo, j, z);
-    for (int k = 0; k < NPR; k++) pr[k] = pv[k * ks + src];
-    load_geo(d, m, ilo, j, CENT, gm);
-    inflow_check(pr, gm, 0);
-    for (int k = 0; k < NPR; k++) pv[k * ks + dst] = pr[k];
-    ps[1 * ks + dst] = ps[1 * ks + src];
-    ps[2 * ks + dst] = ps[2 * ks + src];
-    src = cix(d, d.n1 + d.ng1 - 1, j, z);
-    dst = cix(d, ihi, j, z);
-    for (int k = 0; k < NPR; k++) pr[k] = pv[k * ks + src];
-    load_geo(d, m, ihi, j, CENT, gm);
-    inflow_check(pr, gm, 1);
-    for (int k = 0; k < NPR; k++) pv[k * ks + dst] = pr[k];
-    ps[1 * ks + dst] = ps[1 * ks + src];
-    ps[2 * ks + dst] = ps[2 * ks + src];
+    long src, dst;
+    if (!(d.halo & 1)) {   // a side shared with a neighbouring block is filled by the exchange
+        src = cix(d, d.ng1, j, z);
+        dst = cix(d, ilo, j, z);
+        for (int k = 0; k < NPR; k++) pr[k] = pv[k * ks + src];
+        load_geo(d, m, ilo, j, CENT, gm);
+        inflow_check(pr, gm, 0);
+        for (int k = 0; k < NPR; k++) pv[k * ks + dst] = pr[k];
+        ps[1 * ks + dst] = ps[1 * ks + src];
+        ps[2 * ks + dst] = ps[2 * ks + src];
+    }
+    if (!(d.halo & 2)) {
+        src = cix(d, d.n1 + d.ng1 - 1, j, z);
+        dst = cix(d, ihi, j, z);
+        for (int k = 0; k < NPR; k++) pr[k] = pv[k * ks + src];
+        load_geo(d, m, ihi, j, CENT, gm);
+        inflow_check(pr, gm, 1);
+        for (int k = 0; k < NPR; k++) pv[k * ks + dst] = pr[k];
+        ps[1 * ks + dst] = ps[1 * ks + src];
+        ps[2 * ks + dst] = ps[2 * ks + src];
+    }
 }
 
 __global__ void k_bound_x1(const Dims d, const Geom m, double *pv, double *ps) {
@@ -820,6 +829,32 @@ __global__ void k_bound_x2(const Dims d, double *pv, double *ps) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_bound_x2(d)) return;
     k_bound_x2_at(d, pv, ps, t);
+}
+
+// ------------------------------------------------------------ x1 halos
+// A block of a domain decomposed along x1 exchanges ng layers with each
+// neighbour: the layers next to a shared side (its last ng active layers on
+// the upper side, its first ng on the lower) become the neighbour's ghost
+// layers on the facing side, over the whole ghost-inclusive (x2, x3) cross
+// section, for the NPR primitives and the 3 face-field planes. Buffer layout
+// [component][layer][j][z] (the boundprim slabs of boundcomP.c, one
+// contiguous message per side).
+constexpr int HALO_COMPS = NPR + 3;
+__host__ __device__ __forceinline__ long n_halo(const Dims &d) { return (long)HALO_COMPS * d.ng1 * d.G2 * d.G3; }
+
+template <bool PACK>
+__global__ void k_halo(const Dims d, double *pv, double *ps, int side, double *buf) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_halo(d)) return;
+    const int z = (int)(t % d.G3), j = (int)((t / d.G3) % d.G2);
+    const long r = t / ((long)d.G3 * d.G2);
+    const int g = (int)(r % d.ng1), comp = (int)(r / d.ng1);
+    // packed: active layers next to the side; unpacked: the ghosts beyond it
+    const int i = PACK ? (side ? d.n1 + g : d.ng1 + g) : (side ? d.ng1 + d.n1 + g : g);
+    double *a = comp < NPR ? pv + (long)comp * d.ks : ps + (long)(comp - NPR) * d.ks;
+    const long c = cix(d, i, j, z);
+    if (PACK) buf[t] = a[c];
+    else a[c] = buf[t];
 }
 
 // --------------------------------------------------------- step size logic
@@ -923,6 +958,22 @@ inline void prof_mark(Prof *pf, int slot, cudaStream_t s) {
     if (pf && pf->on) cudaEventRecord(pf->ev[slot + 1], s);
 }
 
+// ghost fill of the state written by a sub-step (full: p, ps; else ph, psh)
+// in direction dim (1, 2, 3), on the block's physical sides; dim 0: all
+// three, in the order x1, x3, x2
+int launch_bound_dim(hamr_ctx *ctx, int full, int dim) {
+    const Dims &d = ctx->d;
+    cudaStream_t s = ctx->stream;
+    double *pw = full ? ctx->p : ctx->ph;
+    double *psw = full ? ctx->ps : ctx->psh;
+    if ((dim == 0 || dim == 1) && d.d1)
+        k_bound_x1<<<nblk((long)d.ng1 * d.G2 * d.G3), BLK, 0, s>>>(d, geom_of(ctx), pw, psw);
+    if ((dim == 0 || dim == 3) && d.d3) k_bound_x3<<<nblk((long)d.ng3 * d.G1 * d.G2), BLK, 0, s>>>(d, pw, psw);
+    if ((dim == 0 || dim == 2) && d.d2) k_bound_x2<<<nblk(n_bound_x2(d)), BLK, 0, s>>>(d, pw, psw);
+    CK(cudaGetLastError());
+    return HAMR_OK;
+}
+
 // n faces of direction DIR, one thread per face, with the block's reconstruction
 template <int DIR, typename T>
 void launch_flux(long n, cudaStream_t s, const Dims &d, const Geom &m, const double *pin, const double *psin, T *F,
@@ -994,11 +1045,9 @@ k_cons<T><<<nblk(n), BLK, 0, s>>>(d, m, ctx->p, full ? ctx->ph : ctx->p, ctx->U,
                                     full ? ctx->p : ctx->ph, ctx->pflag, ctx->failimage);
     }
     prof_mark(pf, PROF_INVERT, s);
-    double *pw = full ? ctx->p : ctx->ph;
-    double *psw = full ? ctx->ps : ctx->psh;
-    if (d.d1) k_bound_x1<<<nblk((long)d.ng1 * d.G2 * d.G3), BLK, 0, s>>>(d, m, pw, psw);
-    if (d.d3) k_bound_x3<<<nblk((long)d.ng3 * d.G1 * d.G2), BLK, 0, s>>>(d, pw, psw);
-    if (d.d2) k_bound_x2<<<nblk(n_bound_x2(d)), BLK, 0, s>>>(d, pw, psw);
+    // ghost fill of the written state; a block of a decomposed domain leaves
+    // it to the caller (hamr_bound_dim around the halo exchange)
+    if (!d.halo) launch_bound_dim(ctx, full, 0);
     prof_mark(pf, PROF_BOUND, s);
     CK(cudaGetLastError());
     return HAMR_OK;
@@ -1031,6 +1080,7 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
     if (prm->riemann != HAMR_RIEMANN_HLL && prm->riemann != HAMR_RIEMANN_HLLC) return HAMR_E_ARG;
     if (!(prm->ng == 3 || (prm->ng == 2 && prm->recon == HAMR_RECON_MC))) return HAMR_E_ARG;
     if (prm->precision != HAMR_FP64 && prm->precision != HAMR_MIXED) return HAMR_E_ARG;
+    if ((prm->halo & ~3) || (prm->halo && (prm->bc1 == HAMR_BC_PERIODIC || prm->n1 < prm->ng))) return HAMR_E_ARG;
     if (prm->inversion != HAMR_INV_2D && prm->inversion != HAMR_INV_NM) return HAMR_E_ARG;
     if (prm->n3 > 1 && prm->bc3 != HAMR_BC_PERIODIC) return HAMR_E_ARG;
     if (prm->bc2 == HAMR_BC_POLE_TRANS && (prm->n3 < 2 || prm->n3 % 2)) return HAMR_E_ARG;
@@ -1054,6 +1104,7 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
     d.inversion = prm->inversion;
     d.recon = prm->recon;
     d.riemann = prm->riemann;
+    d.halo = prm->halo;
     if (prm->stream) {
         ctx->stream = (cudaStream_t)prm->stream;
     } else {
@@ -1154,12 +1205,44 @@ int hamr_download_flags(hamr_ctx *ctx, int *pflag, int *failimage) {
 int hamr_bound(hamr_ctx *ctx) {
     if (!ctx) return HAMR_E_ARG;
     if (!ctx->have_geom) return HAMR_E_STATE;
+    return launch_bound_dim(ctx, 1, 0);
+}
+
+int hamr_bound_dim(hamr_ctx *ctx, int full, int dim) {
+    if (!ctx || dim < 1 || dim > 3) return HAMR_E_ARG;
+    if (!ctx->have_geom) return HAMR_E_STATE;
+    return launch_bound_dim(ctx, full ? 1 : 0, dim);
+}
+
+long hamr_halo_count(const hamr_ctx *ctx) {
+    if (!ctx) return -1;
+    return n_halo(ctx->d);
+}
+
+int hamr_halo_pack(hamr_ctx *ctx, int full, int side, double *buf) {
+    if (!ctx || !buf || (side != 0 && side != 1)) return HAMR_E_ARG;
     const Dims &d = ctx->d;
-    const Geom m = geom_of(ctx);
-    if (d.d1) k_bound_x1<<<nblk((long)d.ng1 * d.G2 * d.G3), BLK, 0, ctx->stream>>>(d, m, ctx->p, ctx->ps);
-    if (d.d3) k_bound_x3<<<nblk((long)d.ng3 * d.G1 * d.G2), BLK, 0, ctx->stream>>>(d, ctx->p, ctx->ps);
-    if (d.d2) k_bound_x2<<<nblk(n_bound_x2(d)), BLK, 0, ctx->stream>>>(d, ctx->p, ctx->ps);
+    k_halo<true><<<nblk(n_halo(d)), BLK, 0, ctx->stream>>>(d, full ? ctx->p : ctx->ph, full ? ctx->ps : ctx->psh,
+                                                           side, buf);
     CK(cudaGetLastError());
+    return HAMR_OK;
+}
+
+int hamr_halo_unpack(hamr_ctx *ctx, int full, int side, const double *buf) {
+    if (!ctx || !buf || (side != 0 && side != 1)) return HAMR_E_ARG;
+    const Dims &d = ctx->d;
+    k_halo<false><<<nblk(n_halo(d)), BLK, 0, ctx->stream>>>(d, full ? ctx->p : ctx->ph, full ? ctx->ps : ctx->psh,
+                                                            side, const_cast<double *>(buf));
+    CK(cudaGetLastError());
+    return HAMR_OK;
+}
+
+int hamr_cfl_dirs(hamr_ctx *ctx, double *dt3) {
+    if (!ctx || !dt3) return HAMR_E_ARG;
+    unsigned long long b[4];
+    CK(cudaMemcpyAsync(b, ctx->dtbits, sizeof(b), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < 3; k++) memcpy(&dt3[k], &b[k + 1], sizeof(double));
     return HAMR_OK;
 }
 
@@ -1175,6 +1258,10 @@ int hamr_stage(hamr_ctx *ctx, int full, double Dt, double dt) {
 int hamr_step(hamr_ctx *ctx, double dt, double *dt_next) {
     if (!ctx) return HAMR_E_ARG;
     if (!ctx->have_geom) return HAMR_E_STATE;
+    if (ctx->d.halo) {   // the halo exchange has to come between the sub-steps
+        ctx->err = "a block with halo sides steps through hamr_stage, hamr_bound_dim and the halo exchange";
+        return HAMR_E_STATE;
+    }
     if (!(dt > 0)) return HAMR_E_ARG;
     k_dt_reset<<<1, 32, 0, ctx->stream>>>(ctx->dtbits);
     int rc = launch_step(ctx, StepSize{nullptr, 0.5, 0.5 * dt, dt}, StepSize{nullptr, 1.0, dt, dt}, nullptr, 0);
@@ -1193,6 +1280,10 @@ int hamr_step(hamr_ctx *ctx, double dt, double *dt_next) {
 int hamr_advance(hamr_ctx *ctx, int nsteps, int interval, double *dt_inout) {
     if (!ctx || !dt_inout || nsteps < 1 || interval < 1) return HAMR_E_ARG;
     if (!ctx->have_geom) return HAMR_E_STATE;
+    if (ctx->d.halo) {   // the halo exchange has to come between the sub-steps
+        ctx->err = "a block with halo sides steps through hamr_stage, hamr_bound_dim and the halo exchange";
+        return HAMR_E_STATE;
+    }
     if (!(*dt_inout > 0)) return HAMR_E_ARG;
     CK(cudaMemcpyAsync(ctx->dt_state, dt_inout, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemsetAsync(ctx->counter, 0, sizeof(int), ctx->stream));
@@ -1226,6 +1317,10 @@ int hamr_advance(hamr_ctx *ctx, int nsteps, int interval, double *dt_inout) {
 int hamr_profile_step(hamr_ctx *ctx, double dt, int reps, double *ms, int nslots) {
     if (!ctx || !ms || reps < 1 || nslots < PROF_NSLOT) return HAMR_E_ARG;
     if (!ctx->have_geom) return HAMR_E_STATE;
+    if (ctx->d.halo) {   // the halo exchange has to come between the sub-steps
+        ctx->err = "a block with halo sides steps through hamr_stage, hamr_bound_dim and the halo exchange";
+        return HAMR_E_STATE;
+    }
     Prof pf;
     for (auto &e : pf.ev) CK(cudaEventCreate(&e));
     pf.on = true;
@@ -1325,7 +1420,7 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
                                  const double *gdet, const double *conn, double *p, double *ps,
                                  double dt, double *dt_next) {
     if (!prm || !gcov || !gcon || !gdet || !conn || !p || !ps || !(dt > 0)) return HAMR_E_ARG;
-    if (prm->n1 < 2 || prm->n2 < 2 || prm->n3 < 1 || prm->precision != HAMR_FP64) return HAMR_E_ARG;
+    if (prm->n1 < 2 || prm->n2 < 2 || prm->n3 < 1 || prm->precision != HAMR_FP64 || prm->halo) return HAMR_E_ARG;
     if (prm->recon != HAMR_RECON_PPM && prm->recon != HAMR_RECON_MC) return HAMR_E_ARG;
     if (prm->riemann != HAMR_RIEMANN_HLL && prm->riemann != HAMR_RIEMANN_HLLC) return HAMR_E_ARG;
     if (!(prm->ng == 3 || (prm->ng == 2 && prm->recon == HAMR_RECON_MC))) return HAMR_E_ARG;
@@ -1334,7 +1429,7 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
     if (prm->bc2 == HAMR_BC_POLE_TRANS && (prm->n3 < 2 || prm->n3 % 2)) return HAMR_E_ARG;
     if (!(prm->gam > 1.0) || !(prm->cour > 0.0) || !(prm->dx1 > 0) || !(prm->dx2 > 0) || !(prm->dx3 > 0)) return HAMR_E_ARG;
     // the same dimension bookkeeping as hamr_ctx_create
-    hamr_ctx c;
+    hamr_ctx c{};   // value-initialised: every field not set below is zero
     c.prm = *prm;
     Dims &d = c.d;
     d.n1 = prm->n1; d.n2 = prm->n2; d.n3 = prm->n3;
@@ -1354,6 +1449,7 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
     d.inversion = prm->inversion;
     d.recon = prm->recon;
     d.riemann = prm->riemann;
+    d.halo = 0;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES) return HAMR_E_CUDA;
     if (!na_ready[dev] && na_setup(dev) != HAMR_OK) return HAMR_E_CUDA;

@@ -90,6 +90,12 @@ typedef struct hamr_params {
     int inversion;          /* enum hamr_inversion (zero-initialised: Noble 2D) */
     int recon;              /* enum hamr_recon (zero-initialised: PPM) */
     int riemann;            /* enum hamr_riemann (zero-initialised: HLL) */
+    int halo;               /* x1 sides shared with a neighbouring block of a domain
+                               decomposed along x1: bit 0 the lower side, bit 1 the
+                               upper (zero-initialised: none). No physical ghost fill
+                               and no radial mass-flux fix there; such a block steps
+                               through hamr_stage, hamr_bound_dim and the hamr_halo_*
+                               exchange (the reference's block exchange, boundcomP.c) */
 } hamr_params;
 
 typedef struct hamr_ctx hamr_ctx;
@@ -121,6 +127,31 @@ int hamr_download_flags(hamr_ctx *ctx, int *pflag, int *failimage);
 
 /* Ghost fill of the current state (GPU_boundprim, GPU_main.cu:2113). */
 int hamr_bound(hamr_ctx *ctx);
+
+/* ---- domains decomposed along x1 (halo != 0) ------------------------------
+ * Such a block's hamr_stage leaves the ghost fill to the caller, which runs,
+ * for the state the sub-step wrote (full: p, ps; else ph, psh):
+ *   hamr_bound_dim(1)  physical x1 sides
+ *   hamr_halo_pack on both neighbours' facing sides, transfer, hamr_halo_unpack
+ *   hamr_bound_dim(3), hamr_bound_dim(2)
+ * the order in which a single block fills x1, x3, x2 ghosts, so that the
+ * decomposed step reproduces the undivided block bit for bit. The step size is
+ * the harmonic combination 1/(1/d1 + 1/d2 + 1/d3) of the per-direction CFL
+ * minima over all blocks (hamr_cfl_dirs after each block's full sub-step).
+ * hamr_step, hamr_advance and hamr_profile_step refuse halo blocks. */
+int hamr_bound_dim(hamr_ctx *ctx, int full, int dim);
+/* Doubles in one side's halo message: (NPR + 3) x ng x G2 x G3, laid out
+ * [component][layer][j][z]. */
+long hamr_halo_count(const hamr_ctx *ctx);
+/* side 0: the lower x1 side, 1: the upper. pack copies the ng active layers
+ * next to that side into buf (device memory, hamr_halo_count doubles);
+ * unpack writes buf into the ghost layers beyond that side. Asynchronous on
+ * the context stream. */
+int hamr_halo_pack(hamr_ctx *ctx, int full, int side, double *buf);
+int hamr_halo_unpack(hamr_ctx *ctx, int full, int side, const double *buf);
+/* Per-direction CFL minima (x1, x2, x3; 1e9 for an inactive direction) of
+ * the last full sub-step run by hamr_stage; waits for the device. */
+int hamr_cfl_dirs(hamr_ctx *ctx, double *dt3);
 
 /* One RK2 sub-step on the device, asynchronous on the context stream:
  * full == 0 advances (p, ps) by Dt into (ph, psh) and caches U(p);

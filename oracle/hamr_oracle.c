@@ -595,9 +595,9 @@ static void fix_flux(const ho_grid *g, const dims *d, double *F1, double *F2, do
         for (int z = 0; z < d->G3; z++) {
             if (!(j >= d->ng2 - d->d2 && z >= d->ng3 - d->d3 && j < d->n2 + d->ng2 + d->d2 && z < d->n3 + d->ng3 + d->d3)) continue;
             long ci = RHO * ks + cix(d, d->ng1, j, z);
-            if (F1[ci] > 0.) F1[ci] = 0.;
+            if (!(g->halo & 1) && F1[ci] > 0.) F1[ci] = 0.;
             long co = RHO * ks + cix(d, d->n1 + d->ng1, j, z);
-            if (F1[co] < 0.) F1[co] = 0.;
+            if (!(g->halo & 2) && F1[co] < 0.) F1[co] = 0.;
         }
 }
 
@@ -1439,11 +1439,11 @@ static void copy_cell(const dims *d, double *pv, long dst, long src) {
  *     flip u^2 and B^2 (boundprim2_reflective, GPU_bounds.h:305-508).
  *  PERIODIC: copy from the opposite edge, all planes and the face field.
  */
-void ho_bound(const ho_grid *g, const ho_geom *m, double *pv, double *ps) {
+void ho_bound_dim(const ho_grid *g, const ho_geom *m, double *pv, double *ps, int dim) {
     dims d = mkdims(g);
     long ks = d.ks;
     /* x1 */
-    if (d.d1) {
+    if (dim == 1 && d.d1) {
         for (int j = 0; j < d.G2; j++)
             for (int z = 0; z < d.G3; z++)
                 for (int t = 0; t < d.ng1; t++) {
@@ -1458,26 +1458,32 @@ void ho_bound(const ho_grid *g, const ho_geom *m, double *pv, double *ps) {
                     } else {
                         geo gm;
                         double pr[NPR];
-                        long src = cix(&d, d.ng1, j, z), dst = cix(&d, ilo, j, z);
-                        for (int k = 0; k < NPR; k++) pr[k] = pv[k * ks + src];
-                        load_geo(&d, m, ilo, j, CENT, &gm);
-                        inflow_check(pr, &gm, 0);
-                        for (int k = 0; k < NPR; k++) pv[k * ks + dst] = pr[k];
-                        ps[1 * ks + dst] = ps[1 * ks + src];
-                        ps[2 * ks + dst] = ps[2 * ks + src];
-                        src = cix(&d, d.n1 + d.ng1 - 1, j, z);
-                        dst = cix(&d, ihi, j, z);
-                        for (int k = 0; k < NPR; k++) pr[k] = pv[k * ks + src];
-                        load_geo(&d, m, ihi, j, CENT, &gm);
-                        inflow_check(pr, &gm, 1);
-                        for (int k = 0; k < NPR; k++) pv[k * ks + dst] = pr[k];
-                        ps[1 * ks + dst] = ps[1 * ks + src];
-                        ps[2 * ks + dst] = ps[2 * ks + src];
+                        long src, dst;
+                        if (!(g->halo & 1)) {
+                            src = cix(&d, d.ng1, j, z);
+                            dst = cix(&d, ilo, j, z);
+                            for (int k = 0; k < NPR; k++) pr[k] = pv[k * ks + src];
+                            load_geo(&d, m, ilo, j, CENT, &gm);
+                            inflow_check(pr, &gm, 0);
+                            for (int k = 0; k < NPR; k++) pv[k * ks + dst] = pr[k];
+                            ps[1 * ks + dst] = ps[1 * ks + src];
+                            ps[2 * ks + dst] = ps[2 * ks + src];
+                        }
+                        if (!(g->halo & 2)) {
+                            src = cix(&d, d.n1 + d.ng1 - 1, j, z);
+                            dst = cix(&d, ihi, j, z);
+                            for (int k = 0; k < NPR; k++) pr[k] = pv[k * ks + src];
+                            load_geo(&d, m, ihi, j, CENT, &gm);
+                            inflow_check(pr, &gm, 1);
+                            for (int k = 0; k < NPR; k++) pv[k * ks + dst] = pr[k];
+                            ps[1 * ks + dst] = ps[1 * ks + src];
+                            ps[2 * ks + dst] = ps[2 * ks + src];
+                        }
                     }
                 }
     }
     /* x3: periodic */
-    if (d.d3) {
+    if (dim == 3 && d.d3) {
         for (int i = 0; i < d.G1; i++)
             for (int j = 0; j < d.G2; j++)
                 for (int t = 0; t < d.ng3; t++) {
@@ -1492,7 +1498,7 @@ void ho_bound(const ho_grid *g, const ho_geom *m, double *pv, double *ps) {
                 }
     }
     /* x2 */
-    if (d.d2) {
+    if (dim == 2 && d.d2) {
         int n2 = d.n2, ng = d.ng2;
         for (int i = 0; i < d.G1; i++)
             for (int z = 0; z < d.G3; z++) {
@@ -1587,6 +1593,12 @@ void ho_bound(const ho_grid *g, const ho_geom *m, double *pv, double *ps) {
                 }
             }
     }
+}
+
+void ho_bound(const ho_grid *g, const ho_geom *m, double *pv, double *ps) {
+    ho_bound_dim(g, m, pv, ps, 1);
+    ho_bound_dim(g, m, pv, ps, 3);
+    ho_bound_dim(g, m, pv, ps, 2);
 }
 
 /* divb_calc (diag.c:153-199), staggered-field definition, max over active cells */

@@ -38,6 +38,11 @@ typedef struct {
                             (slope_lim with factor 2, PPM = 0 builds) */
     int riemann;         /* 0: HLL; 1: HLLC in the orthonormal face frame
                             (HLLC builds, FRAME_TRANSFORM) */
+    int halo;            /* sides interior to a decomposed domain, whose ghosts
+                            come from a neighbouring block: bit 0 the lower x1
+                            side, bit 1 the upper; no physical fill and no
+                            radial mass-flux fix there (the reference fills
+                            them by its block exchange, boundcomP.c) */
 } ho_grid;
 
 typedef struct {
@@ -61,6 +66,10 @@ void ho_stage(const ho_grid *g, const ho_geom *m, ho_state *s, int full,
 
 /* Ghost fill of (pv, ps) for the boundary types in g (direction 1, then 3, then 2). */
 void ho_bound(const ho_grid *g, const ho_geom *m, double *pv, double *ps);
+/* Ghost fill of one direction (1, 2 or 3) on the physical sides; ho_bound is
+ * x1, x3, x2 in that order. A decomposed domain exchanges the x1 halos
+ * between the x1 and x3 fills. */
+void ho_bound_dim(const ho_grid *g, const ho_geom *m, double *pv, double *ps, int dim);
 
 /* Single-cell pieces (pinned one by one against the reference). */
 void ho_para(const double *x, double *l, double *r);

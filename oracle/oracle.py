@@ -38,7 +38,7 @@ class HoGrid(ctypes.Structure):
                 ("ksize", ctypes.c_long), ("gsize", ctypes.c_long),
                 ("dx1", _d), ("dx2", _d), ("dx3", _d), ("gam", _d), ("cour", _d),
                 ("pole1", _i), ("pole2", _i), ("bc1", _i), ("bc2", _i), ("bc3", _i),
-                ("inversion", _i), ("ct_upwind", _i), ("recon", _i), ("riemann", _i)]
+                ("inversion", _i), ("ct_upwind", _i), ("recon", _i), ("riemann", _i), ("halo", _i)]
 
 
 class HoGeom(ctypes.Structure):
@@ -64,6 +64,7 @@ def lib():
         L.ho_stage.argtypes = [ctypes.POINTER(HoGrid), ctypes.POINTER(HoGeom), ctypes.POINTER(HoState),
                                _i, _d, _d, _i, _vp]
         L.ho_bound.argtypes = [ctypes.POINTER(HoGrid), ctypes.POINTER(HoGeom), _vp, _vp]
+        L.ho_bound_dim.argtypes = [ctypes.POINTER(HoGrid), ctypes.POINTER(HoGeom), _vp, _vp, _i]
         L.ho_para.argtypes = [_vp, _vp, _vp]
         L.ho_primtoflux.argtypes = [_d, _vp, _vp, _vp, _d, _i, _vp, _vp, _vp]
         for nm in ("ho_utoprim_2d", "ho_utoprim_1dvsq2fix1", "ho_utoprim_1dfix1", "ho_utoprim_nm"):
@@ -219,12 +220,13 @@ class Setup:
     inversion: int = 0  # 0: Noble 2D, 1: Newman-Hamlin
     recon: int = 0      # 0: PPM, 1: MC-limited linear
     riemann: int = 0    # 0: HLL, 1: HLLC
+    halo: int = 0       # x1 sides filled by a neighbour block: bit 0 lower, bit 1 upper
 
     def grid(self):
         b = self.blk
         return HoGrid(b.n1, b.n2, b.n3, b.ng, b.ksize, b.gsize, self.dx[0], self.dx[1], self.dx[2],
                       self.gam, self.cour, self.pole1, self.pole2, self.bc[0], self.bc[1], self.bc[2],
-                      self.inversion, self.ct_upwind, self.recon, self.riemann)
+                      self.inversion, self.ct_upwind, self.recon, self.riemann, self.halo)
 
 
 def _state(b: Block):
@@ -247,6 +249,14 @@ def oracle_bound(s: Setup, pname="p", psname="ps"):
     g = s.grid()
     m = s.geo.c()
     lib().ho_bound(ctypes.byref(g), ctypes.byref(m), _ptr(s.blk.arrays[pname]), _ptr(s.blk.arrays[psname]))
+
+
+def oracle_bound_dim(s: Setup, dim, pname="p", psname="ps"):
+    """Ghost fill of one direction on the physical sides (halo sides skipped)."""
+    g = s.grid()
+    m = s.geo.c()
+    lib().ho_bound_dim(ctypes.byref(g), ctypes.byref(m), _ptr(s.blk.arrays[pname]), _ptr(s.blk.arrays[psname]),
+                       int(dim))
 
 
 def set_mud(gcov10, gcon10, d):

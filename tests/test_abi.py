@@ -17,7 +17,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     text = open(os.path.join(ROOT, "include", "hamr_b200.h")).read()
-    return sorted(set(re.findall(r"^(?:int|const char \*)\s*(hamr_\w+)\(", text, re.M)))
+    return sorted(set(re.findall(r"^(?:int|long|const char \*)\s*(hamr_\w+)\(", text, re.M)))
 
 
 @pytest.mark.parametrize("strict", [False, True])
@@ -42,6 +42,13 @@ def test_create_rejects_bad_parameters_without_device_work():
     prm.riemann = 4
     assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # no such Riemann solver
     prm.riemann = 0
+    prm.halo = 4
+    assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # halo sides along x1 only
+    prm.halo = 1
+    bc1, prm.bc1 = prm.bc1, 0
+    assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # a periodic x1 has no neighbours
+    prm.bc1 = bc1
+    prm.halo = 0
     prm.ng = 3
     prm.gam = 1.0
     assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # gamma <= 1
