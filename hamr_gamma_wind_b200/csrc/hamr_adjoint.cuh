@@ -119,55 +119,41 @@ namespace {
 // derivative of para, without carrying five derivatives through every
 // operation)
 __device__ __forceinline__ void para_weights(const double *y, bool upper, double *w) {
-    double dq[4], c[4][3];   // slope i (1..3) = sum_k c[i][k] y[i - 1 + k]
+    double dq[4], c0[4], c1[4], c2[4];   // slope i = c0 y[i-1] + c1 y[i] + c2 y[i+1]
 #pragma unroll
     for (int i = 1; i < 4; i++) {
         const double Dqm = 2. * (y[i] - y[i - 1]);
         const double Dqp = 2. * (y[i + 1] - y[i]);
         const double Dqc = 0.5 * (y[i + 1] - y[i - 1]);
         const double aDqm = d_fabs(Dqm), aDqp = d_fabs(Dqp), aDqc = d_fabs(Dqc);
-        const double sm = Dqm * Dqp;
         const double mn = d_min(aDqm, aDqp);
-        const double on = (double)(sm > 0.);
-        const double sc = Dqc > 0. ? 1. : -1.;   // the sign given to the slope
-        if (aDqc < mn) {
-            dq[i] = (sc * aDqc) * on;
-            const double g = sc * (Dqc < 0. ? -1. : 1.) * on * 0.5;   // d|Dqc| = sign(Dqc) dDqc
-            c[i][0] = -g; c[i][1] = 0.; c[i][2] = g;
-        } else if (aDqm < aDqp) {
-            dq[i] = (sc * mn) * on;
-            const double g = sc * (Dqm < 0. ? -1. : 1.) * on * 2.;
-            c[i][0] = -g; c[i][1] = g; c[i][2] = 0.;
-        } else {
-            dq[i] = (sc * mn) * on;
-            const double g = sc * (Dqp < 0. ? -1. : 1.) * on * 2.;
-            c[i][0] = 0.; c[i][1] = -g; c[i][2] = g;
-        }
+        const double on = (double)(Dqm * Dqp > 0.);
+        const double sc = Dqc > 0. ? 1. : -1.;
+        const bool selc = aDqc < mn, selm = aDqm < aDqp;
+        dq[i] = (sc * (selc ? aDqc : mn)) * on;
+        const double gc = sc * (Dqc < 0. ? -1. : 1.) * on * 0.5;
+        const double gm = sc * (Dqm < 0. ? -1. : 1.) * on * 2.;
+        const double gp = sc * (Dqp < 0. ? -1. : 1.) * on * 2.;
+        c0[i] = selc ? -gc : (selm ? -gm : 0.);
+        c1[i] = selc ? 0. : (selm ? gm : -gp);
+        c2[i] = selc ? gc : (selm ? 0. : gp);
     }
     double l = 0.5 * (y[2] + y[1]) - (dq[2] - dq[1]) / 6.0;
     double r = 0.5 * (y[3] + y[2]) - (dq[3] - dq[2]) / 6.0;
-    double wl[5] = {0., 0.5, 0.5, 0., 0.}, wr[5] = {0., 0., 0.5, 0.5, 0.};
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        wl[1 + k - 1] += c[1][k] / 6.0;   // - (dq2 - dq1)/6
-        wl[2 + k - 1] -= c[2][k] / 6.0;
-        wr[2 + k - 1] += c[2][k] / 6.0;   // - (dq3 - dq2)/6
-        wr[3 + k - 1] -= c[3][k] / 6.0;
-    }
+    const double s6 = 1. / 6.0;
+    double wl[5] = {c0[1] * s6, 0.5 + (c1[1] - c0[2]) * s6, 0.5 + (c2[1] - c1[2]) * s6, -c2[2] * s6, 0.};
+    double wr[5] = {0., c0[2] * s6, 0.5 + (c1[2] - c0[3]) * s6, 0.5 + (c2[2] - c1[3]) * s6, -c2[3] * s6};
     const double qa = (r - y[2]) * (y[2] - l);
     const double qd = (r - l);
     const double qe = 6.0 * (y[2] - 0.5 * (l + r));
-    if (qa <= 0.) {
-        l = r = y[2];
+    const bool flat = qa <= 0.;
+    const bool fixl = qd * (qd - qe) < 0.0, fixr = !fixl && qd * (qd + qe) < 0.0;
 #pragma unroll
-        for (int k = 0; k < 5; k++) wl[k] = wr[k] = k == 2 ? 1. : 0.;
-    }
-    if (qd * (qd - qe) < 0.0) {
-#pragma unroll
-        for (int k = 0; k < 5; k++) wl[k] = (k == 2 ? 3. : 0.) - 2. * wr[k];
-    } else if (qd * (qd + qe) < 0.0) {
-#pragma unroll
-        for (int k = 0; k < 5; k++) wr[k] = (k == 2 ? 3. : 0.) - 2. * wl[k];
+    for (int k = 0; k < 5; k++) {
+        const double e2 = k == 2 ? 1. : 0.;
+        const double a = flat ? e2 : wl[k], b = flat ? e2 : wr[k];
+        wl[k] = fixl ? 3. * e2 - 2. * b : a;
+        wr[k] = fixr ? 3. * e2 - 2. * a : b;
     }
 #pragma unroll
     for (int k = 0; k < 5; k++) w[k] = upper ? wr[k] : wl[k];
@@ -542,7 +528,18 @@ __device__ __forceinline__ void adj_flux_face(const Dims &d, const Geom &m, cons
 
 // both directions' faces in one launch (2-D: x1 then x2 faces), so that the
 // two reverses, which only meet in atomics, fill the GPU together
-__global__ void __launch_bounds__(BLK) k_adj_flux12(const Dims d, const Geom m, const double *__restrict__ pv,
+// build options: minimum resident blocks of 128 threads per SM for the
+// reverse kernels, which cap their registers: the 2-D torus gradient is
+// latency bound at low occupancy, and spilling beats it (face reverse at 5
+// blocks: 102 registers with spills against 230 without, 25 % on the whole
+// gradient; the state kernels another 1-2 %)
+#ifndef HAMR_ADJ_FLUX_MINB
+#define HAMR_ADJ_FLUX_MINB 5
+#endif
+#ifndef HAMR_ADJ_ZONE_MINB
+#define HAMR_ADJ_ZONE_MINB 4
+#endif
+__global__ void __launch_bounds__(BLK, HAMR_ADJ_FLUX_MINB) k_adj_flux12(const Dims d, const Geom m, const double *__restrict__ pv,
                                                      const double *__restrict__ ps, const double *__restrict__ aF1,
                                                      const double *__restrict__ aF2, double *ap, double *aps,
                                                      double *agam) {
@@ -598,7 +595,7 @@ __global__ void k_adj_divergence12(const Dims d, const double *__restrict__ aW, 
 // (dG/dp)^T x = p_bar, and likewise for the field and gamma. Where no solver
 // converged, the hydrodynamic primitives are the guess's. ap: cotangent of
 // the output (consumed); apg: of the guess; aW: of the conserved input.
-__global__ void __launch_bounds__(BLK) k_adj_invert(const Dims d, const Geom m, const double *__restrict__ pout,
+__global__ void __launch_bounds__(BLK, HAMR_ADJ_ZONE_MINB - 1) k_adj_invert(const Dims d, const Geom m, const double *__restrict__ pout,
                                                      const double *__restrict__ pg, const double *__restrict__ W7,
                                                      const double *__restrict__ psf, const int *__restrict__ pflag,
                                                      const int *__restrict__ fail0, double *ap, double *apg,
@@ -713,7 +710,7 @@ namespace {
 
 // source term reversed (active zones): ap += Dt (d dU / d pb)^T aW, agam;
 // and the U^n cache: aU += aW
-__global__ void __launch_bounds__(BLK) k_adj_source(const Dims d, const Geom m, const double *__restrict__ pb,
+__global__ void __launch_bounds__(BLK, HAMR_ADJ_ZONE_MINB) k_adj_source(const Dims d, const Geom m, const double *__restrict__ pb,
                                                      const double *__restrict__ aW, double *ap, double *aU,
                                                      double Dt, double *agam) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -746,7 +743,7 @@ __global__ void __launch_bounds__(BLK) k_adj_source(const Dims d, const Geom m, 
 
 // conserved variables of a state reversed (U(p^n) cached by the half
 // sub-step, active zones): ap += (dU/dp)^T aU, agam; aU consumed
-__global__ void __launch_bounds__(BLK) k_adj_cons_of_state(const Dims d, const Geom m, const double *__restrict__ pv,
+__global__ void __launch_bounds__(BLK, HAMR_ADJ_ZONE_MINB) k_adj_cons_of_state(const Dims d, const Geom m, const double *__restrict__ pv,
                                                             double *aU, double *ap, double *agam) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     double gsum = 0.;
