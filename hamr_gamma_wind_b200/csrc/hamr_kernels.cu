@@ -92,6 +92,10 @@ struct StepSize {
 #ifndef HAMR_FLUX_MINB_F
 #define HAMR_FLUX_MINB_F 6
 #endif
+template <int DIR, typename T, int REC>
+__device__ __forceinline__ double flux_eval(const Dims &d, const Geo<T> &gm, const double *__restrict__ ps, T *pl,
+                                            T *pr, T *__restrict__ F, const long c, const int j);
+
 // one face of direction DIR (t < n_faces): reconstruction, two states, four
 // flux evaluations, HLL (or HLLC); returns the face's CFL limit, or 1e9 when
 // filtered. REC: bit 0 MC reconstruction, bit 1 HLLC.
@@ -103,7 +107,6 @@ __device__ __forceinline__ double flux_face(const Dims &d, const Geom &m, const 
     const int j0 = (d.ng2 - 1) * d.d2 + jdel, nj = d.n2 + 2 * d.d2 - jdel;
     const int z0 = (d.ng3 - 1) * d.d3 + zdel, nz = d.n3 + 2 * d.d3 - zdel;
     (void)ni;
-    double dtf = 1.e9;
     const int z = z0 + (int)(t % nz);
     const int j = j0 + (int)((t / nz) % nj);
     const int i = i0 + (int)(t / ((long)nz * nj));
@@ -136,6 +139,16 @@ __device__ __forceinline__ double flux_face(const Dims &d, const Geom &m, const 
             pr[k] = lo;
         }
     }
+    return flux_eval<DIR, T, REC>(d, gm, ps, pl, pr, F, c, j);
+}
+
+// The face flux from the reconstructed states pl, pr (the normal field and
+// the polar B1 fix applied here): two states, four flux evaluations, HLL (or
+// HLLC), the flux written at cell index c; returns the face's CFL limit.
+template <int DIR, typename T, int REC>
+__device__ __forceinline__ double flux_eval(const Dims &d, const Geo<T> &gm, const double *__restrict__ ps, T *pl,
+                                            T *pr, T *__restrict__ F, const long c, const int j) {
+    double dtf = 1.e9;
     const T bn = (T)__ldg(&ps[(long)(DIR - 1) * d.ks + c]);
     pl[B1 + DIR - 1] = bn;
     pr[B1 + DIR - 1] = bn;
@@ -206,6 +219,103 @@ __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? HAMR_FLUX_MINB : HAMR_FL
                                                unsigned long long *__restrict__ dtbits, int calc_dt) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     const double dtf = t < n_faces<DIR>(d) ? flux_face<DIR, T, REC>(d, m, pv, ps, F, t) : 1.e9;
+    if (calc_dt) cta_min_dt(dtf, &dtbits[DIR]);
+}
+
+// Both edge values of one zone, primitive by primitive (the normal field
+// component skipped: the face sets it). PPM (para) or MC.
+template <int DIR, typename T, int REC>
+__device__ __forceinline__ void zone_edges(const Dims &d, const double *__restrict__ pv, long cz, long stride,
+                                           T *lo, T *hi) {
+#pragma unroll
+    for (int k = 0; k < NPR; k++) {
+        if (k == B1 + DIR - 1) continue;
+        const double *pk = pv + (long)k * d.ks + cz;
+        if constexpr ((REC & 1) == HAMR_RECON_MC) {
+            const T y1 = (T)__ldg(pk - stride), y2 = (T)__ldg(pk), y3 = (T)__ldg(pk + stride);
+            const T temp = T(0.5) * slope_lim(y1, y2, y3);
+            lo[k] = y2 - temp;
+            hi[k] = y2 + temp;
+        } else {
+            T x[5];
+#pragma unroll
+            for (int s = 0; s < 5; s++) x[s] = (T)__ldg(pk + (s - 2) * stride);
+            para(x, lo[k], hi[k]);
+        }
+    }
+}
+
+// (x3 faces stay face by face: a warp-shuffle form that reconstructed each
+// zone once, lane l + 1 handing face l its right state, was 6 % slower in
+// FP64 and even in float on the 384 x 192 x 192 torus.)
+// Faces of direction DIR (1 or 2) by rows: a thread walks FLUX_ROW
+// consecutive faces along DIR at fixed transverse indices, reconstructing
+// each zone once (its upper edge is the left state of the next face) where
+// the face-by-face kernel reconstructs every zone twice; neighbouring
+// threads take neighbouring z, so the loads stay coalesced. Same values as
+// k_flux face by face.
+// build options: faces per row, and minimum resident blocks of 128 threads
+// per SM for the row kernels (FP64, float). Measured on the 384 x 192 x 192
+// torus: rows of 12 beat 6, 8, 24 and 48 (shorter rows: more threads in
+// flight, longer: fewer extra reconstructions); 7 float blocks beat 6.
+#ifndef HAMR_FLUX_ROW
+#define HAMR_FLUX_ROW 12
+#endif
+constexpr int FLUX_ROW = HAMR_FLUX_ROW;
+#ifndef HAMR_FLUX_ROWS_MINB
+#define HAMR_FLUX_ROWS_MINB HAMR_FLUX_MINB
+#endif
+#ifndef HAMR_FLUX_ROWS_MINB_F
+#define HAMR_FLUX_ROWS_MINB_F 7
+#endif
+template <int DIR>
+__host__ __device__ __forceinline__ long n_flux_rows(const Dims &d) {
+    static_assert(DIR == 1 || DIR == 2, "rows along x1 or x2");
+    const long nf = DIR == 1 ? d.n1 + 2 * d.d1 - 1 : d.n2 + 2 * d.d2 - 1;
+    const long nt = DIR == 1 ? (long)(d.n2 + 2 * d.d2) : (long)(d.n1 + 2 * d.d1);
+    return ((nf + FLUX_ROW - 1) / FLUX_ROW) * nt * (d.n3 + 2 * d.d3);
+}
+
+template <int DIR, typename T, int REC>
+__global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? HAMR_FLUX_ROWS_MINB : HAMR_FLUX_ROWS_MINB_F)
+    k_flux_rows(const Dims d, const Geom m, const double *__restrict__ pv, const double *__restrict__ ps,
+                T *__restrict__ F, unsigned long long *__restrict__ dtbits, int calc_dt) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double dtf = 1.e9;
+    if (t < n_flux_rows<DIR>(d)) {
+        const int nz = d.n3 + 2 * d.d3, z = (d.ng3 - 1) * d.d3 + (int)(t % nz);
+        const long r = t / nz;
+        const int nt = DIR == 1 ? d.n2 + 2 * d.d2 : d.n1 + 2 * d.d1;
+        const int a = (DIR == 1 ? (d.ng2 - 1) * d.d2 : (d.ng1 - 1) * d.d1) + (int)(r % nt);   // j or i
+        const int seg = (int)(r / nt);
+        const int nf = DIR == 1 ? d.n1 + 2 * d.d1 - 1 : d.n2 + 2 * d.d2 - 1;
+        const int f0 = (DIR == 1 ? d.ng1 : d.ng2) + seg * FLUX_ROW;
+        const int f1 = (DIR == 1 ? d.ng1 : d.ng2) + (seg + 1) * FLUX_ROW < (DIR == 1 ? d.ng1 : d.ng2) + nf
+                           ? (DIR == 1 ? d.ng1 : d.ng2) + (seg + 1) * FLUX_ROW
+                           : (DIR == 1 ? d.ng1 : d.ng2) + nf;
+        const long stride = DIR == 1 ? (long)d.G2 * d.G3 : (long)d.G3;
+        const int face = DIR == 1 ? FACE1 : FACE2;
+        T pl[NPR], lo[NPR], hi[NPR];
+        // the zone below the first face: its upper edge is the first left state
+        const long cf0 = DIR == 1 ? cix(d, f0, a, z) : cix(d, a, f0, z);
+        zone_edges<DIR, T, REC>(d, pv, cf0 - stride, stride, lo, hi);
+#pragma unroll
+        for (int k = 0; k < NPR; k++) pl[k] = hi[k];
+        for (int f = f0; f < f1; f++) {
+            const int i = DIR == 1 ? f : a, j = DIR == 1 ? a : f;
+            const long c = cix(d, i, j, z);
+            zone_edges<DIR, T, REC>(d, pv, c, stride, lo, hi);
+            Geo<T> gm;
+            load_geo_t(d, m, i, j, face, gm);
+            T l[NPR];
+#pragma unroll
+            for (int k = 0; k < NPR; k++) l[k] = pl[k];
+            const double v = flux_eval<DIR, T, REC>(d, gm, ps, l, lo, F, c, j);
+            dtf = v < dtf ? v : dtf;
+#pragma unroll
+            for (int k = 0; k < NPR; k++) pl[k] = hi[k];
+        }
+    }
     if (calc_dt) cta_min_dt(dtf, &dtbits[DIR]);
 }
 
@@ -978,6 +1088,16 @@ int launch_bound_dim(hamr_ctx *ctx, int full, int dim) {
 template <int DIR, typename T>
 void launch_flux(long n, cudaStream_t s, const Dims &d, const Geom &m, const double *pin, const double *psin, T *F,
                  unsigned long long *dtbits, int cd) {
+    if constexpr (DIR != 3) {   // x1 and x2 faces by rows, each zone reconstructed once
+        const long nr = n_flux_rows<DIR>(d);
+        switch (d.recon | (d.riemann << 1)) {
+        case 1: k_flux_rows<DIR, T, 1><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+        case 2: k_flux_rows<DIR, T, 2><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+        case 3: k_flux_rows<DIR, T, 3><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+        default: k_flux_rows<DIR, T, 0><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+        }
+        return;
+    }
     switch (d.recon | (d.riemann << 1)) {
     case 1: k_flux<DIR, T, 1><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
     case 2: k_flux<DIR, T, 2><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
