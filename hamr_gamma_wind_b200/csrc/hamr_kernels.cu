@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -1024,6 +1025,7 @@ struct hamr_ctx {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     bool have_geom = false;
+    long rows_min = 0;   // threads the row flux kernels need before they pay (several waves of the device)
     std::string err;
     // device state
     double *p = nullptr, *ph = nullptr, *ps = nullptr, *psh = nullptr, *U = nullptr;
@@ -1087,14 +1089,18 @@ int launch_bound_dim(hamr_ctx *ctx, int full, int dim) {
 // n faces of direction DIR, one thread per face, with the block's reconstruction
 template <int DIR, typename T>
 void launch_flux(long n, cudaStream_t s, const Dims &d, const Geom &m, const double *pin, const double *psin, T *F,
-                 unsigned long long *dtbits, int cd) {
-    if constexpr (DIR != 3) {   // x1 and x2 faces by rows, each zone reconstructed once
-        const long nr = n_flux_rows<DIR>(d);
+                 unsigned long long *dtbits, int cd, long rows_min) {
+    // x1 and x2 faces by rows, each zone reconstructed once, where the rows
+    // still fill the device several times over; small blocks (2-D, ensemble
+    // members) keep one thread per face
+    if (DIR != 3 && n_flux_rows<DIR == 3 ? 1 : DIR>(d) >= rows_min) {
+        constexpr int RD = DIR == 3 ? 1 : DIR;
+        const long nr = n_flux_rows<RD>(d);
         switch (d.recon | (d.riemann << 1)) {
-        case 1: k_flux_rows<DIR, T, 1><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
-        case 2: k_flux_rows<DIR, T, 2><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
-        case 3: k_flux_rows<DIR, T, 3><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
-        default: k_flux_rows<DIR, T, 0><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+        case 1: k_flux_rows<RD, T, 1><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+        case 2: k_flux_rows<RD, T, 2><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+        case 3: k_flux_rows<RD, T, 3><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+        default: k_flux_rows<RD, T, 0><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
         }
         return;
     }
@@ -1122,17 +1128,17 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
     const int cd = calc_dt ? 1 : 0;
     if (d.d3) {
         long n = (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3 - 1);
-        launch_flux<3, T>(n, s, d, m, pin, psin, F3, ctx->dtbits, cd);
+        launch_flux<3, T>(n, s, d, m, pin, psin, F3, ctx->dtbits, cd, ctx->rows_min);
     }
     prof_mark(pf, PROF_FLUX3, s);
     {
         long n = (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2 - 1) * (d.n3 + 2 * d.d3);
-        launch_flux<2, T>(n, s, d, m, pin, psin, F2, ctx->dtbits, cd);
+        launch_flux<2, T>(n, s, d, m, pin, psin, F2, ctx->dtbits, cd, ctx->rows_min);
     }
     prof_mark(pf, PROF_FLUX2, s);
     {
         long n = (long)(d.n1 + 2 * d.d1 - 1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3);
-        launch_flux<1, T>(n, s, d, m, pin, psin, F1, ctx->dtbits, cd);
+        launch_flux<1, T>(n, s, d, m, pin, psin, F1, ctx->dtbits, cd, ctx->rows_min);
     }
     prof_mark(pf, PROF_FLUX1, s);
     if (d.bc2 == HAMR_BC_POLE_REFL) {
@@ -1231,6 +1237,17 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
         cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) { delete ctx; return HAMR_E_CUDA; }
         ctx->own_stream = true;
+    }
+    {
+        // six waves of the row kernels' residency (blocks of 128 per SM: the
+        // FP64 and float register caps)
+        int dev = 0, nsm = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess)
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        const int per_sm = prm->precision == HAMR_MIXED ? HAMR_FLUX_ROWS_MINB_F : HAMR_FLUX_ROWS_MINB;
+        ctx->rows_min = 6L * nsm * per_sm * BLK;
+        // tuning override (threads; 0: always by rows), read once per context
+        if (const char *e = getenv("HAMR_FLUX_ROWS_MIN")) ctx->rows_min = atol(e);
     }
     const size_t cb = sizeof(double) * d.ks;
     struct A { void **p; size_t n; } allocs[] = {
@@ -1550,6 +1567,7 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
     if (!(prm->gam > 1.0) || !(prm->cour > 0.0) || !(prm->dx1 > 0) || !(prm->dx2 > 0) || !(prm->dx3 > 0)) return HAMR_E_ARG;
     // the same dimension bookkeeping as hamr_ctx_create
     hamr_ctx c{};   // value-initialised: every field not set below is zero
+    c.rows_min = 1L << 60;   // blocks this small keep one thread per face
     c.prm = *prm;
     Dims &d = c.d;
     d.n1 = prm->n1; d.n2 = prm->n2; d.n3 = prm->n3;
