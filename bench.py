@@ -540,6 +540,91 @@ def run_adjoint(args):
     print(json.dumps(out), flush=True)
 
 
+def run_slabs(args):
+    """The c3/c2 torus split along x1 into slabs (hamr_gamma_wind_b200.decomp):
+    with one process, --slabs K slabs on one GPU swapping halos by device
+    copies on one stream; under torchrun, one slab per rank, halos by NCCL
+    point-to-point and the CFL minima by an all-reduce. Times the same K steps
+    of the undivided block on rank 0 beside it (one process only). value =
+    zones x steps / device time, max over ranks."""
+    import torch
+    from hamr_gamma_wind_b200 import decomp, problems
+    from hamr_gamma_wind_b200.api import Block
+    rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    wl = WORKLOADS[args.workload]
+    prec = "mixed" if args.precision == "both" else args.precision
+    pb = problems.fm_torus(wl["n1"], wl["n2"], wl["n3"], rout=wl["rout"])
+    cells = pb.n1 * pb.n2 * pb.n3
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    cs = ctypes_stream(stream).value
+    full = Block(**pb.block_kwargs(), precision=prec, stream=cs)
+    full.set_geometry(pb.geo)
+    full.upload(pb.p, pb.ps)
+    full.bound()
+    p0, ps0 = full.download()
+    from dataclasses import replace
+    pb = replace(pb, p=p0, ps=ps0)
+    k = world if world > 1 else max(2, args.slabs)
+    widths = [pb.n1 // k + (1 if r < pb.n1 % k else 0) for r in range(k)]
+    slabs = decomp.split(pb, widths)
+    mine = [slabs[rank]] if world > 1 else slabs
+    gs = decomp.gpu_slabs(mine, cs, precision=prec)
+    ex = decomp.DistributedExchange(rank, world) if world > 1 else decomp.LocalExchange()
+    st = decomp.SlabStepper(gs, ex)
+    dt = 0.2 * min(pb.dx[:2])
+    for _ in range(args.warmup):
+        dt = min(st.step(dt), 1.3 * dt)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            dt = min(st.step(dt), 1.3 * dt)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    out = None
+    if rank == 0:
+        und = None
+        if world == 1:
+            d2 = 0.2 * min(pb.dx[:2])
+            for _ in range(args.warmup):
+                d2 = min(full.step(d2), 1.3 * d2)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(args.steps):
+                d2 = min(full.step(d2), 1.3 * d2)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            und = cells * args.steps / (e0.elapsed_time(e1) * 1e-3)
+        out = {"metric": "cell-updates/s", "value": cells * args.steps / (ms * 1e-3), "unit": "cell-updates/s",
+               "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+               "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+               "dtype": "f64" if prec == "fp64" else "f32 flux/EMF + f64 update/inversion", "data": "synthetic",
+               "config": {"workload": f"3-D FM torus {wl['n1']}x{wl['n2']}x{wl['n3']} split along x1 into {k} slabs "
+                                      f"{widths}", "zones": cells, "precision": prec,
+                          "exchange": "nccl" if world > 1 else "device copies, one stream",
+                          "parallelism": f"x1 slabs x{k}"},
+               "undivided_value_same_steps": und, "clocks": clk.summary(), "gpu_launches": None}
+        print(json.dumps(out), flush=True)
+    for g in gs:
+        g.block.close()
+    full.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def ctypes_stream(stream):
     import ctypes
     return ctypes.c_void_p(stream.cuda_stream)
@@ -563,6 +648,8 @@ def main():
                     help="instead of timing: per-field L1 difference of mixed vs FP64 after this many steps")
     ap.add_argument("--kernels-only", action="store_true",
                     help="warm-up and timed steps only (for profiler runs)")
+    ap.add_argument("--slabs", type=int, default=0,
+                    help="c3/c2 split along x1: K slabs on one GPU, or one slab per rank under torchrun")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -574,6 +661,8 @@ def main():
         run_ensemble(args)
     elif args.workload == "c5":
         run_adjoint(args)
+    elif args.slabs:
+        run_slabs(args)
     else:
         run_ours(args)
 
