@@ -16,13 +16,13 @@ from hamr_gamma_wind_b200.api import Batch, Block
 pytestmark = pytest.mark.gpu
 
 
-def _members(precision="fp64", strict=True, with_2d=True):
+def _members(precision="fp64", strict=True, with_2d=True, **kw):
     pbs, _ = problems.torus_ensemble(4, 16, 26, seed=7)
     if with_2d:
         pbs.append(problems.fm_torus(40, 32, 1, rout=40.0))   # reflective poles, 2-D
     blocks = []
     for pb in pbs:
-        b = Block(**pb.block_kwargs(), precision=precision, strict=strict)
+        b = Block(**pb.block_kwargs(), precision=precision, strict=strict, **kw)
         b.set_geometry(pb.geo)
         b.upload(pb.p, pb.ps)
         b.bound()
@@ -140,3 +140,20 @@ def test_batch_rejects_mixed_kinds():
         Batch([blocks[0], blocks[0]])
     other.close()
     _close(blocks)
+
+
+@pytest.mark.parametrize("variant", [dict(riemann="hllc"), dict(recon="mc")])
+def test_batch_variants_match_single_blocks_bitwise(variant):
+    """HLLC and MC members run the same per-item bodies in the batch."""
+    pbs, solo = _members(**variant)
+    _, mem = _members(**variant)
+    batch = Batch(mem)
+    dts = np.array([0.2 * min(pb.dx[:2]) for pb in pbs])
+    for _ in range(2):
+        dn_solo = np.array([b.step(dt) for b, dt in zip(solo, dts)])
+        np.testing.assert_array_equal(dn_solo, batch.step(dts))
+        dts = np.minimum(dn_solo, 1.3 * dts)
+    for a, b in zip(solo, mem):
+        np.testing.assert_array_equal(a.download()[0], b.download()[0])
+    batch.close()
+    _close(solo + mem)

@@ -26,8 +26,8 @@ def _stream_handle(stream):
     return ctypes.c_void_p(stream.cuda_stream).value
 
 
-def _undivided(pb, strict, stream):
-    blk = Block(**pb.block_kwargs(), strict=strict, stream=stream)
+def _undivided(pb, strict, stream, **kw):
+    blk = Block(**pb.block_kwargs(), strict=strict, stream=stream, **kw)
     blk.set_geometry(pb.geo)
     blk.upload(pb.p, pb.ps)
     blk.bound()
@@ -36,14 +36,15 @@ def _undivided(pb, strict, stream):
 
 
 @pytest.mark.parametrize("case", list(CASES))
-@pytest.mark.parametrize("strict", [True, False])
-def test_slabs_match_undivided_block(case, strict):
+@pytest.mark.parametrize("strict,kw", [(True, {}), (False, {}), (True, dict(precision="mixed")),
+                                       (True, dict(riemann="hllc"))])
+def test_slabs_match_undivided_block(case, strict, kw):
     make, widths = CASES[case]
     stream = torch.cuda.Stream()
     h = _stream_handle(stream)
-    blk, pb = _undivided(make(), strict, h)
+    blk, pb = _undivided(make(), strict, h, **kw)
     slabs = decomp.split(pb, widths)
-    gs = decomp.gpu_slabs(slabs, h, strict=strict)
+    gs = decomp.gpu_slabs(slabs, h, strict=strict, **kw)
     stepper = decomp.SlabStepper(gs, decomp.LocalExchange())
     dt = 0.2 * min(pb.dx[:2])
     for _ in range(3):
