@@ -548,10 +548,12 @@ __global__ void __launch_bounds__(BLK) k_face_update(const Dims d, const Geom m,
 }
 
 // geometric source gdet T^k_l Gamma^l_{jk} (source, GPU_phys_mhd.h:34-175)
-__device__ __forceinline__ void source(double gam, const double *ph, const Geo<double> &gm, const Dims &d,
-                                       const Geom &m, long gi, double *dU, const State<double> &q) {
+// conn(s, k): the connection coefficient of symmetric pair s and index k at
+// the zone's (i, j) column (from the tables, or staged in shared memory)
+template <class Conn>
+__device__ __forceinline__ void source_c(double gam, const double *ph, const Geo<double> &gm, Conn conn, double *dU,
+                                         const State<double> &q) {
     double mhd[4][4];
-    const long gs = d.gs;
     const double P = (gam - 1.) * ph[UU];
     const double u = ph[UU];
     const double w = P + ph[RHO] + u;
@@ -565,7 +567,7 @@ __device__ __forceinline__ void source(double gam, const double *ph, const Geo<d
             mhd[a][b] = eta * q.ucon[a] * q.ucov[b] + ptot * (a == b ? 1. : 0.) - q.bcon[a] * q.bcov[b];
 #pragma unroll
     for (int k = 0; k < NPR; k++) dU[k] = 0.;
-#define CONN(s, k) __ldg(&m.conn[(long)((s) * 4 + (k)) * gs + gi])
+#define CONN(s, k) conn((s), (k))
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         double c;
@@ -588,17 +590,24 @@ __device__ __forceinline__ void source(double gam, const double *ph, const Geo<d
     dU[KTOT] *= gm.g;
 }
 
+__device__ __forceinline__ void source(double gam, const double *ph, const Geo<double> &gm, const Dims &d,
+                                       const Geom &m, long gi, double *dU, const State<double> &q) {
+    const long gs = d.gs;
+    source_c(gam, ph, gm, [&](int s, int k) { return __ldg(&m.conn[(long)(s * 4 + k) * gs + gi]); }, dU, q);
+}
+
 // Conserved update of one active zone (fixup, GPU_fixup.h:5-424, up to the
 // inversion): U(p^n) computed and cached by the half sub-step or read back by
 // the full one, minus the flux divergence, plus the geometric source at the
 // stage's primitives; U[B] from the face-averaged staggered field. pf returns
 // the stage's primitives (the inversion's initial guess).
-template <typename T>
+template <typename T, class Conn>
 __device__ __forceinline__ void cons_update(const Dims &d, const Geom &m, const double *__restrict__ pin,
                                             const double *__restrict__ pb, double *__restrict__ Ucache,
                                             const T *__restrict__ F1, const T *__restrict__ F2,
                                             const T *__restrict__ F3, int full, double Dt, int i, int j,
-                                            long c, long gi, const Geo<double> &gm, double *pf, double *U) {
+                                            long c, long gi, const Geo<double> &gm, Conn conn, double *pf,
+                                            double *U) {
     const long ks = d.ks, isize = (long)d.G2 * d.G3;
     State<double> q;
     double dU[NPR];
@@ -624,14 +633,14 @@ __device__ __forceinline__ void cons_update(const Dims &d, const Geom &m, const 
             if (d.ng2 > 0) U[k] -= Dt * (F2[k * ks + c + d.G3] - F2[k * ks + c]) / (d.dx2 * (double)1);
             if (d.ng3 > 0) U[k] -= Dt * (F3[k * ks + c + 1] - F3[k * ks + c]) / (d.dx3 * (double)1);
         }
-        source(d.gam, pf, gm, d, m, gi, dU, q);
+        source_c(d.gam, pf, gm, conn, dU, q);
 #pragma unroll
         for (int k = 0; k < NPR; k++) U[k] += Dt * (dU[k]);
     } else {
         // float fluxes: differences taken in double (exact for two floats of
         // similar size) and the four increments added to U^n with Neumaier
         // compensated summation
-        source(d.gam, pf, gm, d, m, gi, dU, q);
+        source_c(d.gam, pf, gm, conn, dU, q);
 #pragma unroll
         for (int k = 0; k < NPR; k++) {
             double sum = U[k], comp = 0.;
@@ -724,7 +733,9 @@ __device__ __forceinline__ void k_cons_at(const Dims &d, const Geom &m, const do
     Geo<double> gm;
     load_geo(d, m, i, j, CENT, gm);
     double pf[NPR], U[NPR];
-    cons_update<T>(d, m, pin, pb, Ucache, F1, F2, F3, full, st.sub(), i, j, c, gi, gm, pf, U);
+    const long gs = d.gs;
+    cons_update<T>(d, m, pin, pb, Ucache, F1, F2, F3, full, st.sub(), i, j, c, gi, gm,
+                   [&](int s, int k) { return __ldg(&m.conn[(long)(s * 4 + k) * gs + gi]); }, pf, U);
     W[0 * d.ks + c] = U[RHO];
     W[1 * d.ks + c] = U[UU];
     W[2 * d.ks + c] = U[U1];
@@ -743,6 +754,58 @@ __global__ void __launch_bounds__(BLK, HAMR_CONS_MINB) k_cons(const Dims d, cons
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)d.n1 * d.n2 * d.n3) return;
     k_cons_at(d, m, pin, pb, Ucache, F1, F2, F3, W, full, st, t);
+}
+
+// The same update with the zones' metric and connection staged in shared
+// memory: the zones of a CTA lie in at most three (i, j) columns when
+// n3 >= 64 (z runs fastest), whose 61 metric and connection values each are
+// loaded once per CTA instead of once per zone.
+constexpr int COL_VALS = 61;   // gcov 10, gcon 10, gdet 1 (centre), conn 40
+template <typename T>
+__global__ void __launch_bounds__(BLK, HAMR_CONS_MINB) k_cons_cols(const Dims d, const Geom m,
+                                               const double *__restrict__ pin, const double *__restrict__ pb,
+                                               double *__restrict__ Ucache, const T *__restrict__ F1,
+                                               const T *__restrict__ F2, const T *__restrict__ F3,
+                                               double *__restrict__ W, int full, StepSize st) {
+    __shared__ double sg[3][COL_VALS];
+    const long nzone = (long)d.n1 * d.n2 * d.n3;
+    const long t0 = (long)blockIdx.x * blockDim.x;
+    const long tl = (t0 + blockDim.x < nzone ? t0 + blockDim.x : nzone) - 1;
+    const long col0 = t0 / d.n3, ncol = tl / d.n3 - col0 + 1;   // <= 3 for n3 >= 64
+    const long gs = d.gs;
+    for (int e = threadIdx.x; e < ncol * COL_VALS; e += blockDim.x) {
+        const long col = col0 + e / COL_VALS;
+        const int v = e % COL_VALS;
+        const long gi = gix(d, d.ng1 + (int)(col / d.n2), d.ng2 + (int)(col % d.n2));
+        double x;
+        if (v < 10) x = m.gcov[(long)(v * 5 + CENT) * gs + gi];
+        else if (v < 20) x = m.gcon[(long)((v - 10) * 5 + CENT) * gs + gi];
+        else if (v == 20) x = m.gdet[(long)CENT * gs + gi];
+        else x = m.conn[(long)(v - 21) * gs + gi];
+        sg[e / COL_VALS][v] = x;
+    }
+    __syncthreads();
+    const long t = t0 + threadIdx.x;
+    if (t >= nzone) return;
+    const int z = d.ng3 + (int)(t % d.n3);
+    const int j = d.ng2 + (int)((t / d.n3) % d.n2);
+    const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
+    const long c = cix(d, i, j, z), gi = gix(d, i, j);
+    const double *g = sg[t / d.n3 - col0];
+    Geo<double> gm;
+#pragma unroll
+    for (int q = 0; q < 10; q++) { gm.gcov[q] = g[q]; gm.gcon[q] = g[10 + q]; }
+    gm.g = g[20];
+    double pf[NPR], U[NPR];
+    cons_update<T>(d, m, pin, pb, Ucache, F1, F2, F3, full, st.sub(), i, j, c, gi, gm,
+                   [&](int s, int k) { return g[21 + s * 4 + k]; }, pf, U);
+    W[0 * d.ks + c] = U[RHO];
+    W[1 * d.ks + c] = U[UU];
+    W[2 * d.ks + c] = U[U1];
+    W[3 * d.ks + c] = U[U2];
+    W[4 * d.ks + c] = U[U3];
+    W[5 * d.ks + c] = U[KTOT];
+    W[6 * d.ks + c] = U[B3];
 }
 
 template <int INV>
@@ -1027,6 +1090,7 @@ struct hamr_ctx {
     bool own_stream = false;
     bool have_geom = false;
     long rows_min = 0;   // threads the row flux kernels need before they pay (several waves of the device)
+    bool cons_cols = true;   // column-staged conserved update where n3 >= 64
     std::string err;
     // device state
     double *p = nullptr, *ph = nullptr, *ps = nullptr, *psh = nullptr, *U = nullptr;
@@ -1164,8 +1228,12 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
     }
     {
         long n = (long)d.n1 * d.n2 * d.n3;
-k_cons<T><<<nblk(n), BLK, 0, s>>>(d, m, ctx->p, full ? ctx->ph : ctx->p, ctx->U, F1, F2, F3, ctx->W, full,
-                                         st);
+        if (d.n3 >= 64 && ctx->cons_cols)   // metric and connection staged per CTA
+            k_cons_cols<T><<<nblk(n), BLK, 0, s>>>(d, m, ctx->p, full ? ctx->ph : ctx->p, ctx->U, F1, F2, F3, ctx->W,
+                                                   full, st);
+        else
+            k_cons<T><<<nblk(n), BLK, 0, s>>>(d, m, ctx->p, full ? ctx->ph : ctx->p, ctx->U, F1, F2, F3, ctx->W, full,
+                                              st);
         prof_mark(pf, PROF_UPDATE, s);
         auto inv = d.inversion == HAMR_INV_NM ? k_invert<HAMR_INV_NM> : k_invert<HAMR_INV_2D>;
         inv<<<nblk(n), BLK, 0, s>>>(d, m, full ? ctx->ph : ctx->p, ctx->W, full ? ctx->ps : ctx->psh,
@@ -1249,6 +1317,7 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
         ctx->rows_min = 6L * nsm * per_sm * BLK;
         // tuning override (threads; 0: always by rows), read once per context
         if (const char *e = getenv("HAMR_FLUX_ROWS_MIN")) ctx->rows_min = atol(e);
+        if (const char *e = getenv("HAMR_CONS_COLS")) ctx->cons_cols = atoi(e) != 0;
     }
     const size_t cb = sizeof(double) * d.ks;
     struct A { void **p; size_t n; } allocs[] = {

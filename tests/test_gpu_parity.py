@@ -281,3 +281,31 @@ def test_row_flux_kernels_strict(case, recon, riemann, monkeypatch):
     np.testing.assert_array_equal(blk_f.active(psf), blk_r.active(psr))
     blk_f.close()
     blk_r.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_column_staged_update_matches(precision, monkeypatch):
+    """The conserved update with the metric and connection staged per CTA
+    (blocks with n3 >= 64) against the zone-by-zone loads: the same values,
+    so bit for bit in either precision (production build)."""
+    from hamr_gamma_wind_b200.api import Block
+    pb = problems.fm_torus(96, 48, 64, rout=1000.0)
+    blks = []
+    for cols in ("0", "1"):
+        monkeypatch.setenv("HAMR_CONS_COLS", cols)
+        b = Block(**pb.block_kwargs(), precision=precision)
+        b.set_geometry(pb.geo)
+        b.upload(pb.p, pb.ps)
+        b.bound()
+        blks.append(b)
+    dt = 0.2 * min(pb.dx[:2])
+    for _ in range(2):
+        d0, d1 = blks[0].step(dt), blks[1].step(dt)
+        assert d0 == d1
+        dt = min(d0, 1.3 * dt)
+    p0, s0 = blks[0].download()
+    p1, s1 = blks[1].download()
+    np.testing.assert_array_equal(p0, p1)
+    np.testing.assert_array_equal(s0, s1)
+    for b in blks:
+        b.close()
