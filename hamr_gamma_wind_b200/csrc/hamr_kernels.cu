@@ -1235,6 +1235,8 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
             k_cons<T><<<nblk(n), BLK, 0, s>>>(d, m, ctx->p, full ? ctx->ph : ctx->p, ctx->U, F1, F2, F3, ctx->W, full,
                                               st);
         prof_mark(pf, PROF_UPDATE, s);
+        // (the inversion gained nothing from the same staging: FP64 Newton work
+        // bounds it, not its 26 metric loads per zone)
         auto inv = d.inversion == HAMR_INV_NM ? k_invert<HAMR_INV_NM> : k_invert<HAMR_INV_2D>;
         inv<<<nblk(n), BLK, 0, s>>>(d, m, full ? ctx->ph : ctx->p, ctx->W, full ? ctx->ps : ctx->psh,
                                     full ? ctx->p : ctx->ph, ctx->pflag, ctx->failimage);
