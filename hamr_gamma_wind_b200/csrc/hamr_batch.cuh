@@ -140,8 +140,10 @@ struct OpCons {
 };
 
 template <int INV>
+// (the batched inversion keeps 5 blocks per SM: its tiles measured slower at
+// the single-block kernel's 6)
 struct OpInvert {
-    static constexpr int PH = PH_INV, MINB = HAMR_UPD_MINB, SLOT = 0;
+    static constexpr int PH = PH_INV, MINB = 5, SLOT = 0;
     static constexpr bool REDUCE = false;
     __device__ static double run(const BEntry &e, const StageArg &a, long t) {
         k_invert_at<INV>(e.d, e.m, a.full ? e.ph : e.p, e.W, a.full ? e.ps : e.psh, a.full ? e.p : e.ph,

@@ -24,6 +24,7 @@
 #include <mutex>
 #include <string>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/hamr_b200.h"
@@ -590,10 +591,60 @@ __device__ __forceinline__ void source_c(double gam, const double *ph, const Geo
     dU[KTOT] *= gm.g;
 }
 
+// connection accessors: from the tables (one (i, j) column: base pointer and
+// plane stride), or from a column staged in shared memory
+struct ConnTable {
+    const double *conn;
+    long gs, gi;
+    __device__ __forceinline__ double operator()(int s, int k) const {
+        return __ldg(&conn[(long)(s * 4 + k) * gs + gi]);
+    }
+};
+struct ConnStaged {
+    const double *g;   // 40 values, (s, k) at s * 4 + k
+    __device__ __forceinline__ double operator()(int s, int k) const { return g[s * 4 + k]; }
+};
+
+// the same with the connection read from the tables (kept as its own body:
+// the batched update spills less with it than through the accessor)
 __device__ __forceinline__ void source(double gam, const double *ph, const Geo<double> &gm, const Dims &d,
                                        const Geom &m, long gi, double *dU, const State<double> &q) {
+    double mhd[4][4];
     const long gs = d.gs;
-    source_c(gam, ph, gm, [&](int s, int k) { return __ldg(&m.conn[(long)(s * 4 + k) * gs + gi]); }, dU, q);
+    const double P = (gam - 1.) * ph[UU];
+    const double u = ph[UU];
+    const double w = P + ph[RHO] + u;
+    const double bsq = dot4(q.bcon, q.bcov);
+    const double eta = w + bsq;
+    const double ptot = P + 0.5 * bsq;
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+            mhd[a][b] = eta * q.ucon[a] * q.ucov[b] + ptot * (a == b ? 1. : 0.) - q.bcon[a] * q.bcov[b];
+#pragma unroll
+    for (int k = 0; k < NPR; k++) dU[k] = 0.;
+#define CONN(s, k) __ldg(&m.conn[(long)((s) * 4 + (k)) * gs + gi])
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        double c;
+        dU[UU] += mhd[0][k] * CONN(0, k);
+        dU[U1] += mhd[1][k] * CONN(4, k);
+        dU[U2] += mhd[2][k] * CONN(7, k);
+        dU[U3] += mhd[3][k] * CONN(9, k);
+        c = CONN(1, k); dU[UU] += mhd[1][k] * c; dU[U1] += mhd[0][k] * c;
+        c = CONN(2, k); dU[UU] += mhd[2][k] * c; dU[U2] += mhd[0][k] * c;
+        c = CONN(3, k); dU[UU] += mhd[3][k] * c; dU[U3] += mhd[0][k] * c;
+        c = CONN(5, k); dU[U1] += mhd[2][k] * c; dU[U2] += mhd[1][k] * c;
+        c = CONN(6, k); dU[U1] += mhd[3][k] * c; dU[U3] += mhd[1][k] * c;
+        c = CONN(8, k); dU[U2] += mhd[3][k] * c; dU[U3] += mhd[2][k] * c;
+    }
+#undef CONN
+    dU[UU] *= gm.g;
+    dU[U1] *= gm.g;
+    dU[U2] *= gm.g;
+    dU[U3] *= gm.g;
+    dU[KTOT] *= gm.g;
 }
 
 // Conserved update of one active zone (fixup, GPU_fixup.h:5-424, up to the
@@ -633,14 +684,16 @@ __device__ __forceinline__ void cons_update(const Dims &d, const Geom &m, const 
             if (d.ng2 > 0) U[k] -= Dt * (F2[k * ks + c + d.G3] - F2[k * ks + c]) / (d.dx2 * (double)1);
             if (d.ng3 > 0) U[k] -= Dt * (F3[k * ks + c + 1] - F3[k * ks + c]) / (d.dx3 * (double)1);
         }
-        source_c(d.gam, pf, gm, conn, dU, q);
+        if constexpr (std::is_same<Conn, ConnTable>::value) source(d.gam, pf, gm, d, m, gi, dU, q);
+        else source_c(d.gam, pf, gm, conn, dU, q);
 #pragma unroll
         for (int k = 0; k < NPR; k++) U[k] += Dt * (dU[k]);
     } else {
         // float fluxes: differences taken in double (exact for two floats of
         // similar size) and the four increments added to U^n with Neumaier
         // compensated summation
-        source_c(d.gam, pf, gm, conn, dU, q);
+        if constexpr (std::is_same<Conn, ConnTable>::value) source(d.gam, pf, gm, d, m, gi, dU, q);
+        else source_c(d.gam, pf, gm, conn, dU, q);
 #pragma unroll
         for (int k = 0; k < NPR; k++) {
             double sum = U[k], comp = 0.;
@@ -733,9 +786,8 @@ __device__ __forceinline__ void k_cons_at(const Dims &d, const Geom &m, const do
     Geo<double> gm;
     load_geo(d, m, i, j, CENT, gm);
     double pf[NPR], U[NPR];
-    const long gs = d.gs;
-    cons_update<T>(d, m, pin, pb, Ucache, F1, F2, F3, full, st.sub(), i, j, c, gi, gm,
-                   [&](int s, int k) { return __ldg(&m.conn[(long)(s * 4 + k) * gs + gi]); }, pf, U);
+    cons_update<T>(d, m, pin, pb, Ucache, F1, F2, F3, full, st.sub(), i, j, c, gi, gm, ConnTable{m.conn, d.gs, gi},
+                   pf, U);
     W[0 * d.ks + c] = U[RHO];
     W[1 * d.ks + c] = U[UU];
     W[2 * d.ks + c] = U[U1];
@@ -797,8 +849,7 @@ __global__ void __launch_bounds__(BLK, HAMR_CONS_MINB) k_cons_cols(const Dims d,
     for (int q = 0; q < 10; q++) { gm.gcov[q] = g[q]; gm.gcon[q] = g[10 + q]; }
     gm.g = g[20];
     double pf[NPR], U[NPR];
-    cons_update<T>(d, m, pin, pb, Ucache, F1, F2, F3, full, st.sub(), i, j, c, gi, gm,
-                   [&](int s, int k) { return g[21 + s * 4 + k]; }, pf, U);
+    cons_update<T>(d, m, pin, pb, Ucache, F1, F2, F3, full, st.sub(), i, j, c, gi, gm, ConnStaged{g + 21}, pf, U);
     W[0 * d.ks + c] = U[RHO];
     W[1 * d.ks + c] = U[UU];
     W[2 * d.ks + c] = U[U1];
