@@ -1309,12 +1309,173 @@ int ho_utoprim_nm(double gam, double *U, const double *gcov, const double *gcon,
     return 0;
 }
 
+/* --------------------------------------------------------------- floors -- */
+/* fixup_cell (GPU_fixup.h:989-1800) with its body as written for an ideal
+ * gas, DRIFT_FLOOR 1, no neutron star, radiation or EOS table. The reference
+ * compiles that body out (#if 0, GPU_fixup.h:1007) and leaves only the
+ * `r < radfix_dens` reset, dead with radfix_dens = 0 (config.h:40); the
+ * product offers the body as an opt-in. Floor constants of the torus build
+ * (config.h:274-287). */
+#define RHOMINLIMIT 1.e-20
+#define UUMINLIMIT 1.e-20
+#define BSQORHOMAX 25.
+#define BSQOUMAX 750.
+#define UORHOMAX 150.
+
+/* ut_calc_3vel (GPU_phys_mhd.h:18-31) */
+static void ut_calc_3vel(const double *vcon, const geo *gm, double *ut) {
+    const double *g = gm->gcov;
+    double AA = g[0];
+    double BB = 2. * (g[1] * vcon[1] + g[2] * vcon[2] + g[3] * vcon[3]);
+    double CC = g[4] * vcon[1] * vcon[1] + g[7] * vcon[2] * vcon[2] + g[9] * vcon[3] * vcon[3]
+              + 2. * (g[5] * vcon[1] * vcon[2] + g[6] * vcon[1] * vcon[3] + g[8] * vcon[2] * vcon[3]);
+    double DD = -1. / (AA + BB + CC);
+    double one_over_alpha_sq = -gm->gcon[0];
+    if (DD < one_over_alpha_sq) DD = one_over_alpha_sq;
+    *ut = sqrt(DD);
+}
+
+/* ucon_to_utcon (GPU_phys_mhd.h:3-15) */
+static void ucon_to_utcon(const double *ucon, const geo *gm, double *utcon) {
+    double alpha = 1. / sqrt(-gm->gcon[0]);
+    double beta[4];
+    for (int j = 1; j < 4; j++) beta[j] = gm->gcon[j] * alpha * alpha;
+    double gamma = alpha * ucon[0];
+    utcon[0] = 0;
+    for (int j = 1; j < 4; j++) utcon[j] = ucon[j] + gamma * beta[j] / alpha;
+}
+
+static int fixup_cell(double gam, double *pf, const geo *gm) {
+    cstate q;
+    double pf_prefloor[NPR], ucondr[4], Bcon[4], Bcov[4], vcon[4], ucon[4], utcon[4];
+    double rhoflr = RHOMINLIMIT, uuflr = UUMINLIMIT;
+    get_state(pf, gm, &q);
+    double bsq = dot4(q.bcon, q.bcov);
+    double u = pf[UU];
+    for (int k = 0; k < NPR; k++) pf_prefloor[k] = pf[k];
+    if (rhoflr < bsq / BSQORHOMAX) rhoflr = bsq / (BSQORHOMAX);
+    if (uuflr < bsq / BSQOUMAX) uuflr = bsq / (BSQOUMAX);
+    if (rhoflr < u / UORHOMAX) rhoflr = u / (UORHOMAX);
+    if (rhoflr < RHOMINLIMIT) rhoflr = RHOMINLIMIT;
+    if (uuflr < UUMINLIMIT) uuflr = UUMINLIMIT;
+    int dofloor = 0;
+    if (pf[RHO] < rhoflr) { pf[RHO] = rhoflr; dofloor = 1; }
+    if (u < uuflr) { pf[UU] = uuflr; u = uuflr; dofloor = 1; }
+    double trans = 10. * bsq / MY_MIN(pf[RHO], u) - 1.;
+    if (dofloor && trans > 0.) {
+        if (trans > 1.) trans = 1.;
+        double betapar = -q.bcon[0] / ((bsq + SMALL) * q.ucon[0]);
+        double betasq = betapar * betapar * bsq;
+        double betasqmax = 1. - 1. / (GAMMAMAX * GAMMAMAX);
+        if (betasq > betasqmax) betasq = betasqmax;
+        double gamma = 1. / sqrt(1 - betasq);
+        for (int m = 0; m < 4; m++) ucondr[m] = gamma * (q.ucon[m] + betapar * q.bcon[m]);
+        Bcon[0] = 0.;
+        for (int m = 1; m < 4; m++) Bcon[m] = pf[B1 - 1 + m];
+        lower4(Bcon, gm->gcov, Bcov);
+        double udotB = dot4(q.ucon, Bcov);
+        double Bsq = dot4(Bcon, Bcov);
+        double B = sqrt(Bsq);
+        double wold = pf_prefloor[RHO] + pf_prefloor[UU] * gam;
+        double QdotB = udotB * wold * q.ucon[0];
+        double wnew = pf[RHO] + pf[UU] * gam;
+        double x = 2. * QdotB / (B * wnew * ucondr[0] + SMALL);
+        double vpar = x / (ucondr[0] * (1. + sqrt(1. + x * x)));
+        double one_over_ucondr_t = 1. / ucondr[0];
+        vcon[0] = 1.;
+        for (int m = 1; m < 4; m++) vcon[m] = vpar * Bcon[m] / (B + SMALL) + ucondr[m] * one_over_ucondr_t;
+        double ut;
+        ut_calc_3vel(vcon, gm, &ut);
+        for (int m = 0; m < 4; m++) ucon[m] = ut * vcon[m];
+        ucon_to_utcon(ucon, gm, utcon);
+        for (int m = 1; m < 4; m++) pf[m + UU] = utcon[m] * trans + pf_prefloor[m + UU] * (1. - trans);
+    }
+    double gamma;
+    if (gamma_calc(pf, gm, &gamma)) return 4;
+    if (gamma > GAMMAMAX) {
+        double f = sqrt((GAMMAMAX * GAMMAMAX - 1.) / (gamma * gamma - 1.));
+        pf[U1] *= f;
+        pf[U2] *= f;
+        pf[U3] *= f;
+    }
+    return 0;
+}
+
+int ho_fixup_cell(double gam, double *pf, const double *gcov10, const double *gcon10, double gdet) {
+    geo gm;
+    for (int k = 0; k < 10; k++) { gm.gcov[k] = gcov10[k]; gm.gcon[k] = gcon10[k]; }
+    gm.g = gdet;
+    return fixup_cell(gam, pf, &gm);
+}
+
+/* fixuputoprim (GPU_fixup.h:735-800) for one failed zone: the floor state
+ * with zero velocity, passed through the floors when they are on */
+static void reset_failed(double gam, double *pf, const geo *gm, int floors) {
+    pf[RHO] = RHOMINLIMIT;
+    pf[UU] = UUMINLIMIT;
+    pf[U1] = 0.0;
+    pf[U2] = 0.0;
+    pf[U3] = 0.0;
+    if (floors) (void)fixup_cell(gam, pf, gm);
+}
+
+/* fixup_utoprim (fixup.c:764-827): each failed active zone, in (i, j, z)
+ * order, takes the average of the first usable stencil of good neighbours
+ * (the 8 neighbours in the x1-x2 plane numbered 1 2 3 / 8 x 4 / 7 6 5 with
+ * 1 at (i-1, j+1), plus 9 = z+1 and 10 = z-1); a repaired zone counts as good
+ * for the zones after it. Only RHO..U3 are set. The two-point x1 and x2
+ * stencils are selected by the flags of the other direction, as written
+ * there (AVG2_X1 when 2 and 6 are good, AVG2_X2 when 4 and 8 are). */
+void ho_fixup_utoprim(const ho_grid *g, double *pv, int *pflag, int *failimage) {
+    dims d = mkdims(g);
+    long ks = d.ks;
+    long sj = d.G3, si = (long)d.G2 * d.G3, sz = d.d3;
+    for (int i = d.ng1; i < d.ng1 + d.n1; i++)
+        for (int j = d.ng2; j < d.ng2 + d.n2; j++)
+            for (int z = d.ng3; z < d.ng3 + d.n3; z++) {
+                long c = cix(&d, i, j, z);
+                if (pflag[c] == 0) continue;
+                int pf[11];
+                pf[1] = !pflag[c - si + sj]; pf[2] = !pflag[c + sj]; pf[3] = !pflag[c + si + sj];
+                pf[8] = !pflag[c - si];                           pf[4] = !pflag[c + si];
+                pf[7] = !pflag[c - si - sj]; pf[6] = !pflag[c - sj]; pf[5] = !pflag[c + si - sj];
+                pf[9] = !pflag[c + sz]; pf[10] = !pflag[c - sz];
+#define P(o) pv[k * ks + c + (o)]
+                if (pf[2] && pf[4] && pf[6] && pf[8] && pf[9] && pf[10]) {
+                    for (int k = 0; k < B1; k++)
+                        P(0) = 1. / 6. * (P(sj) + P(-sj) + P(-si) + P(si) + P(1) + P(-1));
+                } else if (pf[1] && pf[3] && pf[5] && pf[7] && pf[9] && pf[10]) {
+                    for (int k = 0; k < B1; k++)
+                        P(0) = 1. / 6. * (P(si + sj) + P(si - sj) + P(-si + sj) + P(-si - sj) + P(1) + P(-1));
+                } else if (pf[2] && pf[4] && pf[6] && pf[8]) {
+                    for (int k = 0; k < B1; k++) P(0) = 0.25 * (P(sj) + P(-sj) + P(-si) + P(si));
+                } else if (pf[1] && pf[3] && pf[5] && pf[7]) {
+                    for (int k = 0; k < B1; k++) P(0) = 0.25 * (P(si + sj) + P(si - sj) + P(-si + sj) + P(-si - sj));
+                } else if (pf[2] && pf[6]) {
+                    for (int k = 0; k < B1; k++) P(0) = 0.5 * (P(-si) + P(si));
+                } else if (pf[4] && pf[8]) {
+                    for (int k = 0; k < B1; k++) P(0) = 0.5 * (P(-sj) + P(sj));
+                } else if (pf[9] && pf[10]) {
+                    for (int k = 0; k < B1; k++) P(0) = 0.5 * (P(-1) + P(1));
+                } else {
+                    failimage[4 * ks + c]++;
+                    for (int k = RHO; k <= UU; k++)
+                        P(0) = 0.5 * (0.25 * (P(sj) + P(-sj) + P(-si) + P(si))
+                                      + 0.25 * (P(si + sj) + P(si - sj) + P(-si + sj) + P(-si - sj)));
+                    pv[U1 * ks + c] = pv[U2 * ks + c] = pv[U3 * ks + c] = 0.;
+                }
+#undef P
+                pflag[c] = 0;
+            }
+}
+
 /* --------------------------------------------------------------- update -- */
 /* fixup kernel (GPU_fixup.h:5-424): cache U(p^n) on the half step, apply the
  * flux divergence and geometric source, rebuild U[B] from the new face field,
  * invert with the Noble 2D scheme and the entropy fallbacks. The floor routine
- * fixup_cell (GPU_fixup.h:989) is compiled out in the reference, so nothing
- * else touches the primitives. */
+ * fixup_cell (GPU_fixup.h:989) is compiled out in the reference; with
+ * g->floors it runs here as written, and g->repair adds the failed-zone
+ * repair of fixuputoprim (1) or fixup_utoprim (2) after the inversion. */
 static void update(const ho_grid *g, const dims *d, const ho_geom *m, ho_state *s, int full, double Dt) {
     long ks = d->ks;
     long isize = (long)d->G2 * d->G3;
@@ -1367,9 +1528,15 @@ static void update(const ho_grid *g, const dims *d, const ho_geom *m, ho_state *
                         if (flag) s->failimage[2 * ks + c]++;
                     }
                 }
+                if (g->floors && fixup_cell(g->gam, pf, &gm)) {
+                    flag = -333;
+                    s->failimage[3 * ks + c]++;
+                }
+                if (g->repair == 1 && flag != 0) reset_failed(g->gam, pf, &gm, g->floors);
                 s->pflag[c] = flag;
                 for (int k = 0; k < NPR; k++) pout[k * ks + c] = pf[k];
             }
+    if (g->repair == 2) ho_fixup_utoprim(g, pout, s->pflag, s->failimage);
 }
 
 /* ---------------------------------------------------------------- stage -- */

@@ -43,6 +43,12 @@ typedef struct {
                             side, bit 1 the upper; no physical fill and no
                             radial mass-flux fix there (the reference fills
                             them by its block exchange, boundcomP.c) */
+    int floors;          /* 1: drift-frame floors after the inversion (fixup_cell,
+                            GPU_fixup.h:1025-1800, compiled out in the reference) */
+    int repair;          /* zones whose inversion failed (pflag != 0):
+                            1 reset to the floor state (fixuputoprim, GPU_fixup.h:735-852);
+                            2 interpolated from good neighbours (fixup_utoprim,
+                            fixup.c:764-827); 0 left as the solver left them */
 } ho_grid;
 
 typedef struct {
@@ -54,7 +60,7 @@ typedef struct {
     double *U;                   /* conserved U(p^n), NPR planes (storage2) */
     double *F1, *F2, *F3;        /* face fluxes, NPR planes each */
     double *E_cent, *emf;        /* 4 planes each (index 1..3 used) */
-    int *pflag, *failimage;      /* failimage: 4 planes of ksize ints */
+    int *pflag, *failimage;      /* failimage: 5 planes of ksize ints */
 } ho_state;
 
 /* One sub-step: full == 0 advances (p, ps) by Dt into (ph, psh), caching U(p);
@@ -82,6 +88,13 @@ int ho_utoprim_1dvsq2fix1(double gam, double *U, const double *gcov10, const dou
 int ho_utoprim_1dfix1(double gam, double *U, const double *gcov10, const double *gcon10, double gdet, double *prim);
 int ho_utoprim_nm(double gam, double *U, const double *gcov10, const double *gcon10, double gdet, double *prim);
 int ho_utoprim_nm_max_index(void);
+
+/* Floors of one zone (centre metric); returns 4 when the Lorentz factor
+ * cannot be formed, else 0. */
+int ho_fixup_cell(double gam, double *pf, const double *gcov10, const double *gcon10, double gdet);
+/* Neighbour repair of the failed active zones of pv in (i, j, z) order,
+ * clearing their flags (fixup_utoprim, fixup.c:764-827). */
+void ho_fixup_utoprim(const ho_grid *g, double *pv, int *pflag, int *failimage);
 
 /* Diagnostics */
 double ho_divb_max(const ho_grid *g, const ho_geom *m, const double *ps);

@@ -38,7 +38,8 @@ class HoGrid(ctypes.Structure):
                 ("ksize", ctypes.c_long), ("gsize", ctypes.c_long),
                 ("dx1", _d), ("dx2", _d), ("dx3", _d), ("gam", _d), ("cour", _d),
                 ("pole1", _i), ("pole2", _i), ("bc1", _i), ("bc2", _i), ("bc3", _i),
-                ("inversion", _i), ("ct_upwind", _i), ("recon", _i), ("riemann", _i), ("halo", _i)]
+                ("inversion", _i), ("ct_upwind", _i), ("recon", _i), ("riemann", _i), ("halo", _i),
+                ("floors", _i), ("repair", _i)]
 
 
 class HoGeom(ctypes.Structure):
@@ -75,6 +76,9 @@ def lib():
         L.ho_divb_max.argtypes = [ctypes.POINTER(HoGrid), ctypes.POINTER(HoGeom), _vp]
         L.ho_divb_max.restype = _d
         L.ho_set_mud.argtypes = [_vp, _vp, _i, _vp, _vp]
+        L.ho_fixup_cell.argtypes = [_d, _vp, _vp, _vp, _d]
+        L.ho_fixup_cell.restype = _i
+        L.ho_fixup_utoprim.argtypes = [ctypes.POINTER(HoGrid), _vp, _vp, _vp]
         _lib = L
     return _lib
 
@@ -102,6 +106,8 @@ def ref(variant: str):
         L.ref_primtoflux.argtypes = [_vp, _vp, _vp, _d, _i, _vp, _vp, _vp]
         L.ref_para.argtypes = [_vp, _vp, _vp]
         L.ref_bl_coord.argtypes = [_vp, _vp]
+        L.ref_fixuputoprim.argtypes = [_vp] * 7
+        L.ref_fixup_utoprim.argtypes = [_vp, _vp, _vp, ctypes.c_long]
         if hasattr(L, "ref_set_mud"):
             L.ref_set_mud.argtypes = [_vp, _vp]
             L.ref_mud_plane.restype = ctypes.c_long
@@ -221,12 +227,15 @@ class Setup:
     recon: int = 0      # 0: PPM, 1: MC-limited linear
     riemann: int = 0    # 0: HLL, 1: HLLC
     halo: int = 0       # x1 sides filled by a neighbour block: bit 0 lower, bit 1 upper
+    floors: int = 0     # 1: drift-frame floors after the inversion
+    repair: int = 0     # failed zones: 1 reset to the floor state, 2 neighbour interpolation
 
     def grid(self):
         b = self.blk
         return HoGrid(b.n1, b.n2, b.n3, b.ng, b.ksize, b.gsize, self.dx[0], self.dx[1], self.dx[2],
                       self.gam, self.cour, self.pole1, self.pole2, self.bc[0], self.bc[1], self.bc[2],
-                      self.inversion, self.ct_upwind, self.recon, self.riemann, self.halo)
+                      self.inversion, self.ct_upwind, self.recon, self.riemann, self.halo,
+                      self.floors, self.repair)
 
 
 def _state(b: Block):
@@ -325,6 +334,34 @@ def step(stage, bound, s: Setup, dt):
     dtd = stage(s, 1, dt, dt, True)
     bound(s, "p", "ps")
     return 1.0 / (1.0 / dtd[1] + 1.0 / dtd[2] + 1.0 / dtd[3])
+
+
+def fixup_cell(gam, pf, gcov10, gcon10, gdet):
+    """Floors of one zone (oracle restatement of fixup_cell): (flag, prims)."""
+    pf = np.array(pf, float)
+    rc = lib().ho_fixup_cell(gam, _ptr(pf), _ptr(np.ascontiguousarray(gcov10, float)),
+                             _ptr(np.ascontiguousarray(gcon10, float)), gdet)
+    return rc, pf
+
+
+def oracle_fixup_utoprim(s: Setup, pname="p"):
+    """Neighbour repair of the failed zones of one state (fixup_utoprim)."""
+    g = s.grid()
+    a = s.blk.arrays
+    lib().ho_fixup_utoprim(ctypes.byref(g), _ptr(a[pname]), _ptr(a["pflag"]), _ptr(a["failimage"]))
+
+
+def ref_fixup_utoprim(variant, s: Setup, pname="p"):
+    """The reference's CPU fixup_utoprim (fixup.c:764) on one state."""
+    a = s.blk.arrays
+    ref(variant).ref_fixup_utoprim(_ptr(a[pname]), _ptr(a["pflag"]), _ptr(a["failimage"]), s.blk.ksize)
+
+
+def ref_fixuputoprim(variant, s: Setup, pname="p"):
+    """The reference's GPU fixuputoprim kernel (GPU_fixup.h:735), host build."""
+    a = s.blk.arrays
+    ref(variant).ref_fixuputoprim(_ptr(a[pname]), _ptr(a["radius"]), _ptr(s.geo.gcov), _ptr(s.geo.gcon),
+                                  _ptr(s.geo.gdet), _ptr(a["pflag"]), _ptr(a["failimage"]))
 
 
 def divb_max(s: Setup, psname="ps"):

@@ -10,12 +10,18 @@
 # `r < radfix_dens` always passes and return garbage. The configured copy ends
 # the test with `return 0;`, the evident intent: floors off, no failure flag.
 #
+# With PLAIN=1 in the environment the radfix_dens line is left as written:
+# that copy serves the host build of the CPU fixup.c, whose fixup1zone uses
+# the macro as a plain constant.
+#
 # usage: ref_config.sh <refdir> <outdir> <mode: torus|cart> <BS_1> <BS_2> <BS_3> <gamma-expr> [opts]
 #   opts: comma-separated build switches; mc = linear MC reconstruction (PPM 0),
 #         hllc = HLLC Riemann solver (HLLC 1, which turns on FRAME_TRANSFORM)
 set -e
 REF="$1"; OUT="$2"; MODE="$3"; B1="$4"; B2="$5"; B3="$6"; GAM="$7"; OPTS="${8:-}"
 mkdir -p "$OUT"
+RADFIX='s/^#define radfix_dens 0.0[[:space:]]*$/#define radfix_dens 0.0) { pf[RHO] = 1.0; pf[UU] = 0.1; } return 0; if (0/'
+[ -n "${PLAIN:-}" ] && RADFIX='s/^$//'
 sed -e 's/^#define WHICHPROBLEM .*/#define WHICHPROBLEM TORUS_PROBLEM/' \
     -e "s|^#define GAMMA[[:space:]].*|#define GAMMA ($GAM)|" \
     -e 's/^#define NB_1 .*/#define NB_1 1/' \
@@ -25,7 +31,7 @@ sed -e 's/^#define WHICHPROBLEM .*/#define WHICHPROBLEM TORUS_PROBLEM/' \
     -e "s/^#define BS_2 .*/#define BS_2 $B2/" \
     -e "s/^#define BS_3 .*/#define BS_3 $B3/" \
     -e 's/^#define SCUDA .*/#define SCUDA (0)/' \
-    -e 's/^#define radfix_dens 0.0[[:space:]]*$/#define radfix_dens 0.0) { pf[RHO] = 1.0; pf[UU] = 0.1; } return 0; if (0/' \
+    -e "$RADFIX" \
     "$REF/config.h" > "$OUT/config.h.tmp"
 if [ "$MODE" = "cart" ]; then
   sed -i -e 's/^#define CARTESIAN (0)/#define CARTESIAN (1)/' \

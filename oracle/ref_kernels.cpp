@@ -213,4 +213,14 @@ void ref_primtoflux(double *pr, const double *gcov10, const double *gcon10, doub
 /* para (GPU_interp.h:60) on one 5-point stencil. */
 void ref_para(const double *x, double *l, double *r) { para(x[0], x[1], x[2], x[3], x[4], l, r); }
 
+/* fixuputoprim (GPU_fixup.h:735-852) over the active zones: zones with
+ * pflag != 0 are reset to the floor state with zero velocity and passed
+ * through fixup_cell (a no-op as compiled: its floor body is #if 0). Its
+ * call sits commented out after GPU_fixup in advance_GPU (step_ch.c:1281). */
+void ref_fixuputoprim(double *pv, const double *radius, const double *gcov, const double *gcon,
+                      const double *gdet, int *pflag, int *failimage) {
+    long n4 = (long)BS_1 * BS_2 * BS_3;
+    run_grid(n4, LOCAL_WORK_SIZE, [&] { fixuputoprim(pv, radius, gcov, gcon, gdet, pflag, failimage); });
+}
+
 } /* extern "C" */

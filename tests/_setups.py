@@ -6,6 +6,7 @@ every branch of the step (PPM clamps, HLL upwinding, EMF upwind selection,
 Newton inversion) is exercised. ``stress`` adds cells that make the primary
 inversion fail, to walk the entropy fallbacks.
 """
+import dataclasses
 import numpy as np
 
 from oracle import oracle as O
@@ -109,5 +110,21 @@ def make_setup(variant, spin=0.9375, rout=40.0, seed=1, stress=False, cour=0.8, 
 
 
 def clone(s: O.Setup) -> O.Setup:
-    return O.Setup(s.blk.copy(), s.geo, s.dx, s.gam, s.cour, s.pole1, s.pole2, s.bc, s.ct_upwind, s.inversion,
-                   s.recon, s.riemann)
+    return dataclasses.replace(s, blk=s.blk.copy())
+
+
+def plant_failures(s: O.Setup, frac=0.08, seed=11):
+    """Make the inversion fail outright in some zones: a negative internal
+    energy there leaves every solver of the fallback chain without a
+    physical root. A random fraction of the active zones plus a solid 3 x 3
+    (x 3) patch, so that failed zones also border one another."""
+    b = s.blk
+    P = b.active("p")
+    sel = np.random.default_rng(seed).random(P[0].shape) < frac
+    i0, j0 = P.shape[1] // 2, P.shape[2] // 2
+    z0 = P.shape[3] // 2
+    dz = 3 if P.shape[3] > 1 else 1
+    sel[i0:i0 + 3, j0:j0 + 3, z0:z0 + dz] = True
+    P[O.UU][sel] = -1e-2
+    O.oracle_bound(s, "p", "ps")
+    return int(sel.sum())
