@@ -22,7 +22,7 @@ class HamrParams(ctypes.Structure):
                 ("dx1", _d), ("dx2", _d), ("dx3", _d), ("gam", _d), ("cour", _d),
                 ("pole1", _i), ("pole2", _i), ("bc1", _i), ("bc2", _i), ("bc3", _i),
                 ("ct_upwind", _i), ("precision", _i), ("stream", _vp), ("inversion", _i), ("recon", _i),
-                ("riemann", _i), ("halo", _i)]
+                ("riemann", _i), ("halo", _i), ("floors", _i), ("repair", _i)]
 
 
 ERRORS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "out of device memory",

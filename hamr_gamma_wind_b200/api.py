@@ -20,6 +20,7 @@ PRECISION = {"fp64": 0, "mixed": 1}
 INVERSION = {"2d": 0, "nm": 1}
 RECON = {"ppm": 0, "mc": 1}
 RIEMANN = {"hll": 0, "hllc": 1}
+REPAIR = {"none": 0, "reset": 1, "neighbours": 2}
 RHO, UU, U1, U2, U3, B1, B2, B3, KTOT = range(9)
 FACE1, FACE2, CORN, CENT, FACE3 = range(5)
 NPR = _lib.NPR
@@ -81,7 +82,12 @@ class Block:
 
     def __init__(self, n1, n2, n3, dx, gam, cour=0.8, bc=("outflow", "pole_trans", "periodic"),
                  poles=(1, 1), ct_upwind=True, precision="fp64", strict=False, ng=3, stream=None,
-                 inversion="2d", recon="ppm", riemann="hll", halo=0):
+                 inversion="2d", recon="ppm", riemann="hll", halo=0, floors=False, repair="none"):
+        """floors: the drift-frame floors after the inversion (off in the
+        reference's shipped step); repair: what happens to zones whose
+        inversion failed -- "none" (the reference's step), "reset" (floor
+        state, zero velocity: fixuputoprim) or "neighbours" (average of good
+        neighbours: fixup_utoprim)."""
         self.L = _lib.load(strict)
         self.n1, self.n2, self.n3, self.ng = n1, n2, n3, ng
         self.g1 = n1 + 2 * ng
@@ -90,7 +96,7 @@ class Block:
         prm = _lib.HamrParams(n1, n2, n3, ng, 0, 0, float(dx[0]), float(dx[1]), float(dx[2]), float(gam),
                               float(cour), int(poles[0]), int(poles[1]), BC[bc[0]], BC[bc[1]], BC[bc[2]],
                               int(bool(ct_upwind)), PRECISION[precision], stream, INVERSION[inversion],
-                              RECON[recon], RIEMANN[riemann], int(halo))
+                              RECON[recon], RIEMANN[riemann], int(halo), int(bool(floors)), REPAIR[repair])
         ctx = ctypes.c_void_p()
         rc = self.L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx))
         if rc:
@@ -159,7 +165,7 @@ class Block:
 
     def download_flags(self):
         pflag = np.zeros(self.ksize, np.int32)
-        fail = np.zeros(4 * self.ksize, np.int32)
+        fail = np.zeros(5 * self.ksize, np.int32)
         self._check(self.L.hamr_download_flags(self.ctx, pflag.ctypes.data_as(ctypes.c_void_p),
                                                fail.ctypes.data_as(ctypes.c_void_p)), "hamr_download_flags")
         return pflag, fail

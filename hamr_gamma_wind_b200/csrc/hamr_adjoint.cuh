@@ -1277,7 +1277,7 @@ int hamr_adjoint_create(hamr_ctx *ctx, int mdot_face, hamr_adjoint **out) {
     const Dims &d = ctx->d;
     // the configuration the reverse kernels are written for
     if (p.precision != HAMR_FP64 || p.recon != HAMR_RECON_PPM || p.inversion != HAMR_INV_2D || d.n3 != 1 ||
-        p.riemann != HAMR_RIEMANN_HLL || p.halo ||
+        p.riemann != HAMR_RIEMANN_HLL || p.halo || p.floors || p.repair ||
         p.ng != 3 || p.bc1 != HAMR_BC_OUTFLOW || p.bc2 != HAMR_BC_POLE_REFL || !p.ct_upwind)
         return HAMR_E_ARG;
     if (mdot_face <= d.ng1 || mdot_face >= d.n1 + d.ng1) return HAMR_E_ARG;

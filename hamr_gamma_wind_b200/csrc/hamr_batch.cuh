@@ -386,6 +386,7 @@ int hamr_batch_create(hamr_ctx *const *blocks, int n, void *stream, hamr_batch *
             pk.riemann != p0.riemann)
             return HAMR_E_ARG;
         if (pk.halo) return HAMR_E_ARG;   // members are whole problems: no neighbours to exchange with
+        if (pk.floors || pk.repair) return HAMR_E_ARG;   // the opt-in floors and repairs step one block at a time
         for (int j = 0; j < k; j++)
             if (blocks[j] == blocks[k]) return HAMR_E_ARG;
     }

@@ -723,9 +723,18 @@ __device__ __forceinline__ void face_average_b(const Dims &d, const Geom &m, con
         U[B3] = (psf[2 * ks + c] * m.gdet[FACE3 * d.gs + gi] + psf[2 * ks + c + 1 * d.d3] * m.gdet[FACE3 * d.gs + gi]) / 2.0;
 }
 
+// Opt-in work after the inversion (template bits of the inversion kernel):
+// FIX_FLOORS the drift-frame floors (fixup_cell's body, GPU_fixup.h:1025-1800,
+// compiled out in the reference) with the gamma-failure flag -333 and
+// counter 3 of the fixup kernel (GPU_fixup.h:398-415); FIX_RESET the reset of
+// failed zones to the floor state (fixuputoprim, GPU_fixup.h:735-852, whose
+// call is commented out at step_ch.c:1281), fused here because it reads only
+// the zone's own flag and primitives.
+enum { FIX_FLOORS = 1, FIX_RESET = 2 };
+
 // Primary inversion with the 1dvsq2fix1 and 1dfix1 fallbacks, recording the
 // outcome in pflag and the failure counters (fixup, GPU_fixup.h:346-382)
-template <int INV>
+template <int INV, int FIX = 0>
 __device__ __forceinline__ void invert_zone(const Dims &d, const Geo<double> &gm, long c, double *U, double *pf,
                                             double *__restrict__ pout, int *__restrict__ pflag,
                                             int *__restrict__ failimage) {
@@ -750,6 +759,22 @@ __device__ __forceinline__ void invert_zone(const Dims &d, const Geo<double> &gm
         }
 #pragma unroll
         for (int k = 0; k < NPR; k++) pf[k] = pc[k];
+    }
+    if constexpr ((FIX & FIX_FLOORS) != 0) {
+        if (floor_zone(d.gam, pf, gm)) {
+            flag = -333;
+            failimage[3 * ks + c]++;
+        }
+    }
+    if constexpr ((FIX & FIX_RESET) != 0) {
+        if (flag != 0) {
+            pf[RHO] = RHOMINLIMIT;
+            pf[UU] = UUMINLIMIT;
+            pf[U1] = 0.0;
+            pf[U2] = 0.0;
+            pf[U3] = 0.0;
+            if constexpr ((FIX & FIX_FLOORS) != 0) (void)floor_zone(d.gam, pf, gm);
+        }
     }
     pflag[c] = flag;
 #pragma unroll
@@ -859,7 +884,7 @@ __global__ void __launch_bounds__(BLK, HAMR_CONS_MINB) k_cons_cols(const Dims d,
     W[6 * d.ks + c] = U[B3];
 }
 
-template <int INV>
+template <int INV, int FIX = 0>
 __device__ __forceinline__ void k_invert_at(const Dims &d, const Geom &m, const double *__restrict__ pg,
                                                  const double *__restrict__ W, const double *__restrict__ psf,
                                                  double *__restrict__ pout, int *__restrict__ pflag,
@@ -881,17 +906,149 @@ __device__ __forceinline__ void k_invert_at(const Dims &d, const Geom &m, const 
     U[KTOT] = W[5 * d.ks + c];
     U[B3] = W[6 * d.ks + c];
     face_average_b(d, m, psf, i, j, c, gi, U);
-    invert_zone<INV>(d, gm, c, U, pf, pout, pflag, failimage);
+    invert_zone<INV, FIX>(d, gm, c, U, pf, pout, pflag, failimage);
 }
 
-template <int INV>
+template <int INV, int FIX = 0>
 __global__ void __launch_bounds__(BLK, HAMR_UPD_MINB) k_invert(const Dims d, const Geom m, const double *__restrict__ pg,
                                                  const double *__restrict__ W, const double *__restrict__ psf,
                                                  double *__restrict__ pout, int *__restrict__ pflag,
                                                  int *__restrict__ failimage) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)d.n1 * d.n2 * d.n3) return;
-    k_invert_at<INV>(d, m, pg, W, psf, pout, pflag, failimage, t);
+    k_invert_at<INV, FIX>(d, m, pg, W, psf, pout, pflag, failimage, t);
+}
+
+// ------------------------------------------------ neighbour repair (opt-in)
+// fixup_utoprim (fixup.c:764-827): every failed active zone, in (i, j, z)
+// order, takes the average of the first usable stencil of good neighbours
+// (x1-x2 plane numbered 1 2 3 / 8 x 4 / 7 6 5 with 1 at (i-1, j+1); 9 and 10
+// at z+1 and z-1), and then counts as good for the zones after it; only RHO
+// .. U3 change. The two-point x1 and x2 stencils are chosen by the flags of
+// the other direction, as the reference writes them.
+//
+// The order only matters between failed zones within each other's stencil.
+// k_repair_scan repairs at once every failed zone with no failed active zone
+// in its stencil (nothing else reads or writes what it touches) and lists
+// the others; k_repair_chain, one CTA, repairs the listed zones in waves: a
+// zone is ready once no failed active zone with a smaller index is left in
+// its stencil, and ready zones never neighbour each other, so each wave runs
+// in parallel and the result is the sequential one. Every wave repairs at
+// least the smallest pending zone, so at most as many waves as listed zones.
+struct RepairStencil {
+    long si, sj, sz;
+};
+
+__device__ __forceinline__ bool active_zone(const Dims &d, long c) {
+    const int z = (int)(c % d.G3), j = (int)((c / d.G3) % d.G2), i = (int)(c / ((long)d.G3 * d.G2));
+    return i >= d.ng1 && i < d.ng1 + d.n1 && j >= d.ng2 && j < d.ng2 + d.n2 && z >= d.ng3 && z < d.ng3 + d.n3;
+}
+
+// the ten stencil offsets in the reference's numbering 1..10 (index 0 unused)
+__device__ __forceinline__ long stencil_offset(const RepairStencil &o, int q) {
+    switch (q) {
+        case 1: return -o.si + o.sj;
+        case 2: return o.sj;
+        case 3: return o.si + o.sj;
+        case 4: return o.si;
+        case 5: return o.si - o.sj;
+        case 6: return -o.sj;
+        case 7: return -o.si - o.sj;
+        case 8: return -o.si;
+        case 9: return o.sz;
+        default: return -o.sz;
+    }
+}
+
+// a failed active zone among the stencil of c (before c only, when `before`)
+__device__ __forceinline__ bool failed_neighbour(const Dims &d, const RepairStencil &o, const int *pflag, long c,
+                                                 bool before) {
+    for (int q = 1; q <= 10; q++) {
+        const long off = stencil_offset(o, q);
+        if (off == 0 || (before && off > 0)) continue;
+        if (pflag[c + off] != 0 && active_zone(d, c + off)) return true;
+    }
+    return false;
+}
+
+__device__ void repair_zone(const RepairStencil &o, long ks, double *pv, int *pflag, int *failimage, long c) {
+    bool pf[11];
+#pragma unroll
+    for (int q = 1; q <= 10; q++) pf[q] = !pflag[c + stencil_offset(o, q)];
+    const long si = o.si, sj = o.sj;
+#define P(off) pv[k * ks + c + (off)]
+    if (pf[2] && pf[4] && pf[6] && pf[8] && pf[9] && pf[10]) {
+        for (int k = 0; k < B1; k++) P(0) = 1. / 6. * (P(sj) + P(-sj) + P(-si) + P(si) + P(1) + P(-1));
+    } else if (pf[1] && pf[3] && pf[5] && pf[7] && pf[9] && pf[10]) {
+        for (int k = 0; k < B1; k++)
+            P(0) = 1. / 6. * (P(si + sj) + P(si - sj) + P(-si + sj) + P(-si - sj) + P(1) + P(-1));
+    } else if (pf[2] && pf[4] && pf[6] && pf[8]) {
+        for (int k = 0; k < B1; k++) P(0) = 0.25 * (P(sj) + P(-sj) + P(-si) + P(si));
+    } else if (pf[1] && pf[3] && pf[5] && pf[7]) {
+        for (int k = 0; k < B1; k++) P(0) = 0.25 * (P(si + sj) + P(si - sj) + P(-si + sj) + P(-si - sj));
+    } else if (pf[2] && pf[6]) {
+        for (int k = 0; k < B1; k++) P(0) = 0.5 * (P(-si) + P(si));
+    } else if (pf[4] && pf[8]) {
+        for (int k = 0; k < B1; k++) P(0) = 0.5 * (P(-sj) + P(sj));
+    } else if (pf[9] && pf[10]) {
+        for (int k = 0; k < B1; k++) P(0) = 0.5 * (P(-1) + P(1));
+    } else {
+        // no usable stencil: density and energy from both four-point
+        // averages, velocity zero
+        failimage[4 * ks + c]++;
+        for (int k = RHO; k <= UU; k++)
+            P(0) = 0.5 * (0.25 * (P(sj) + P(-sj) + P(-si) + P(si))
+                          + 0.25 * (P(si + sj) + P(si - sj) + P(-si + sj) + P(-si - sj)));
+        pv[U1 * ks + c] = 0.;
+        pv[U2 * ks + c] = 0.;
+        pv[U3 * ks + c] = 0.;
+    }
+#undef P
+    pflag[c] = 0;
+}
+
+__global__ void k_repair_scan(const Dims d, double *__restrict__ pv, int *__restrict__ pflag,
+                              int *__restrict__ failimage, int *__restrict__ list, int *__restrict__ count) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)d.n1 * d.n2 * d.n3) return;
+    const int z = d.ng3 + (int)(t % d.n3);
+    const int j = d.ng2 + (int)((t / d.n3) % d.n2);
+    const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
+    const long c = cix(d, i, j, z);
+    if (pflag[c] == 0) return;
+    const RepairStencil o{(long)d.G2 * d.G3, d.G3, d.d3};
+    if (failed_neighbour(d, o, pflag, c, false))
+        list[atomicAdd(count, 1)] = (int)c;
+    else
+        repair_zone(o, d.ks, pv, pflag, failimage, c);
+}
+
+constexpr int REPAIR_THREADS = 1024;
+__global__ void __launch_bounds__(REPAIR_THREADS) k_repair_chain(const Dims d, double *__restrict__ pv,
+                                                                 int *__restrict__ pflag, int *__restrict__ failimage,
+                                                                 int *__restrict__ list, int *__restrict__ count) {
+    const int n = *count;
+    const RepairStencil o{(long)d.G2 * d.G3, d.G3, d.d3};
+    // entries: c >= 1 pending, ~c (<= -2) ready in this wave, -1 repaired
+    for (int wave = 0; wave <= n; wave++) {
+        int pending = 0;
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            const int e = list[k];
+            if (e < 0) continue;
+            pending = 1;
+            if (!failed_neighbour(d, o, pflag, e, true)) list[k] = ~e;
+        }
+        if (!__syncthreads_or(pending)) break;
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            const int e = list[k];
+            if (e <= -2) {
+                repair_zone(o, d.ks, pv, pflag, failimage, ~e);
+                list[k] = -1;
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *count = 0;
 }
 
 // ------------------------------------------------------------ ghost fills
@@ -1153,6 +1310,7 @@ struct hamr_ctx {
     double *ndt = nullptr, *dt_state = nullptr;
     int *counter = nullptr;
     unsigned long long *divb = nullptr;
+    int *rlist = nullptr, *rcount = nullptr;   // neighbour repair: listed zones and their count
     // captured advance graphs
     cudaGraphExec_t graph = nullptr;
     int graph_steps = -1, graph_interval = -1;
@@ -1288,9 +1446,20 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
         prof_mark(pf, PROF_UPDATE, s);
         // (the inversion gained nothing from the same staging: FP64 Newton work
         // bounds it, not its 26 metric loads per zone)
-        auto inv = d.inversion == HAMR_INV_NM ? k_invert<HAMR_INV_NM> : k_invert<HAMR_INV_2D>;
-        inv<<<nblk(n), BLK, 0, s>>>(d, m, full ? ctx->ph : ctx->p, ctx->W, full ? ctx->ps : ctx->psh,
-                                    full ? ctx->p : ctx->ph, ctx->pflag, ctx->failimage);
+        const int fix = (ctx->prm.floors ? FIX_FLOORS : 0) | (ctx->prm.repair == 1 ? FIX_RESET : 0);
+        using InvK = void (*)(const Dims, const Geom, const double *, const double *, const double *, double *,
+                              int *, int *);
+        static const InvK inv_k[2][4] = {
+            {k_invert<HAMR_INV_2D, 0>, k_invert<HAMR_INV_2D, 1>, k_invert<HAMR_INV_2D, 2>, k_invert<HAMR_INV_2D, 3>},
+            {k_invert<HAMR_INV_NM, 0>, k_invert<HAMR_INV_NM, 1>, k_invert<HAMR_INV_NM, 2>, k_invert<HAMR_INV_NM, 3>}};
+        double *pout = full ? ctx->p : ctx->ph;
+        inv_k[d.inversion == HAMR_INV_NM][fix]<<<nblk(n), BLK, 0, s>>>(
+            d, m, full ? ctx->ph : ctx->p, ctx->W, full ? ctx->ps : ctx->psh, pout, ctx->pflag, ctx->failimage);
+        if (ctx->prm.repair == 2) {
+            k_repair_scan<<<nblk(n), BLK, 0, s>>>(d, pout, ctx->pflag, ctx->failimage, ctx->rlist, ctx->rcount);
+            k_repair_chain<<<1, REPAIR_THREADS, 0, s>>>(d, pout, ctx->pflag, ctx->failimage, ctx->rlist,
+                                                        ctx->rcount);
+        }
     }
     prof_mark(pf, PROF_INVERT, s);
     // ghost fill of the written state; a block of a decomposed domain leaves
@@ -1329,6 +1498,9 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
     if (!(prm->ng == 3 || (prm->ng == 2 && prm->recon == HAMR_RECON_MC))) return HAMR_E_ARG;
     if (prm->precision != HAMR_FP64 && prm->precision != HAMR_MIXED) return HAMR_E_ARG;
     if ((prm->halo & ~3) || (prm->halo && (prm->bc1 == HAMR_BC_PERIODIC || prm->n1 < prm->ng))) return HAMR_E_ARG;
+    if ((prm->floors & ~1) || prm->repair < 0 || prm->repair > 2) return HAMR_E_ARG;
+    // the neighbour repair's order spans the whole domain: not on a slab of one
+    if (prm->repair == 2 && prm->halo) return HAMR_E_ARG;
     if (prm->inversion != HAMR_INV_2D && prm->inversion != HAMR_INV_NM) return HAMR_E_ARG;
     if (prm->n3 > 1 && prm->bc3 != HAMR_BC_PERIODIC) return HAMR_E_ARG;
     if (prm->bc2 == HAMR_BC_POLE_TRANS && (prm->n3 < 2 || prm->n3 % 2)) return HAMR_E_ARG;
@@ -1378,13 +1550,17 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
         {(void **)&ctx->psh, 3 * cb}, {(void **)&ctx->U, NPR * cb}, {(void **)&ctx->F1, NPR * cb},
         {(void **)&ctx->F2, NPR * cb}, {(void **)&ctx->F3, NPR * cb}, {(void **)&ctx->Ec, 4 * cb},
         {(void **)&ctx->emf, 4 * cb}, {(void **)&ctx->W, 7 * cb}, {(void **)&ctx->pflag, sizeof(int) * d.ks},
-        {(void **)&ctx->failimage, 4 * sizeof(int) * d.ks},
+        {(void **)&ctx->failimage, 5 * sizeof(int) * d.ks},
         {(void **)&ctx->gcov, 50 * sizeof(double) * d.gs}, {(void **)&ctx->gcon, 50 * sizeof(double) * d.gs},
         {(void **)&ctx->gdet, 5 * sizeof(double) * d.gs}, {(void **)&ctx->conn, 40 * sizeof(double) * d.gs},
         {(void **)&ctx->dtbits, 4 * sizeof(unsigned long long)}, {(void **)&ctx->ndt, sizeof(double)},
         {(void **)&ctx->dt_state, sizeof(double)}, {(void **)&ctx->counter, sizeof(int)},
-        {(void **)&ctx->divb, sizeof(unsigned long long)}};
+        {(void **)&ctx->divb, sizeof(unsigned long long)},
+        {(void **)&ctx->rlist, prm->repair == 2 ? sizeof(int) * d.n1 * d.n2 * d.n3 : 0},
+        {(void **)&ctx->rcount, prm->repair == 2 ? sizeof(int) : 0}};
+    if (prm->repair == 2 && d.ks > 0x7fffffffL) { hamr_ctx_destroy(ctx); return HAMR_E_ARG; }
     for (auto &a : allocs) {
+        if (a.n == 0) continue;
         if (cudaMalloc(a.p, a.n) != cudaSuccess) {
             hamr_ctx_destroy(ctx);
             return HAMR_E_NOMEM;
@@ -1406,7 +1582,7 @@ int hamr_ctx_destroy(hamr_ctx *ctx) {
     if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
     void *bufs[] = {ctx->p, ctx->ph, ctx->ps, ctx->psh, ctx->U, ctx->F1, ctx->F2, ctx->F3, ctx->Ec, ctx->emf,
                     ctx->W, ctx->pflag, ctx->failimage, ctx->gcov, ctx->gcon, ctx->gdet, ctx->conn, ctx->dtbits,
-                    ctx->ndt, ctx->dt_state, ctx->counter, ctx->divb};
+                    ctx->ndt, ctx->dt_state, ctx->counter, ctx->divb, ctx->rlist, ctx->rcount};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1457,7 +1633,7 @@ int hamr_download_flags(hamr_ctx *ctx, int *pflag, int *failimage) {
     if (!ctx) return HAMR_E_ARG;
     const size_t ib = sizeof(int) * ctx->d.ks;
     if (pflag) CK(cudaMemcpyAsync(pflag, ctx->pflag, ib, cudaMemcpyDeviceToHost, ctx->stream));
-    if (failimage) CK(cudaMemcpyAsync(failimage, ctx->failimage, 4 * ib, cudaMemcpyDeviceToHost, ctx->stream));
+    if (failimage) CK(cudaMemcpyAsync(failimage, ctx->failimage, 5 * ib, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return HAMR_OK;
 }
@@ -1681,6 +1857,7 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
                                  double dt, double *dt_next) {
     if (!prm || !gcov || !gcon || !gdet || !conn || !p || !ps || !(dt > 0)) return HAMR_E_ARG;
     if (prm->n1 < 2 || prm->n2 < 2 || prm->n3 < 1 || prm->precision != HAMR_FP64 || prm->halo) return HAMR_E_ARG;
+    if (prm->floors || prm->repair) return HAMR_E_ARG;
     if (prm->recon != HAMR_RECON_PPM && prm->recon != HAMR_RECON_MC) return HAMR_E_ARG;
     if (prm->riemann != HAMR_RIEMANN_HLL && prm->riemann != HAMR_RIEMANN_HLLC) return HAMR_E_ARG;
     if (!(prm->ng == 3 || (prm->ng == 2 && prm->recon == HAMR_RECON_MC))) return HAMR_E_ARG;

@@ -923,4 +923,117 @@ __device__ __forceinline__ T hllc_face(T gam, const T *pl, const T *pr, const Ge
     return ctop;
 }
 
+// ---------------------------------------------------------------- floors
+// Opt-in floors: the drift-frame floor of fixup_cell for an ideal gas
+// without radiation or a neutron star (GPU_fixup.h:1025-1800; the same
+// algorithm as fixup1zone, fixup.c:57-664). Both bodies are compiled out
+// (#if 0) in the reference, whose shipped step applies no floor. Constants
+// of the torus build (config.h:274-287, 533).
+constexpr double RHOMINLIMIT = 1.e-20;
+constexpr double UUMINLIMIT = 1.e-20;
+constexpr double BSQORHOMAX = 25.;
+constexpr double BSQOUMAX = 750.;
+constexpr double UORHOMAX = 150.;
+constexpr double GAMMAMAX = 80.;
+
+// Lorentz factor w.r.t. the normal observer with its failure flag
+// (gamma_calc, GPU_phys_mhd.h:740-761)
+__device__ __forceinline__ int gamma_calc_flag(const double *pr, const Geo<double> &gm, double *gamma) {
+    const double *g = gm.gcov;
+    double qsq = g[4] * pr[U1] * pr[U1] + g[7] * pr[U2] * pr[U2] + g[9] * pr[U3] * pr[U3]
+               + 2. * (g[5] * pr[U1] * pr[U2] + g[6] * pr[U1] * pr[U3] + g[8] * pr[U2] * pr[U3]);
+    if (qsq < 0.) {
+        if (fabs(qsq) > 1.E-10) { *gamma = 1.; return 1; }
+        qsq = 1.E-10;
+    }
+    *gamma = sqrt(1. + qsq);
+    return 0;
+}
+
+// u^t from the coordinate 3-velocity v^i (ut_calc_3vel, GPU_phys_mhd.h:18-31)
+__device__ __forceinline__ double ut_of_3vel(const double *vcon, const Geo<double> &gm) {
+    const double *g = gm.gcov;
+    const double AA = g[0];
+    const double BB = 2. * (g[1] * vcon[1] + g[2] * vcon[2] + g[3] * vcon[3]);
+    const double CC = g[4] * vcon[1] * vcon[1] + g[7] * vcon[2] * vcon[2] + g[9] * vcon[3] * vcon[3]
+                    + 2. * (g[5] * vcon[1] * vcon[2] + g[6] * vcon[1] * vcon[3] + g[8] * vcon[2] * vcon[3]);
+    double DD = -1. / (AA + BB + CC);
+    const double one_over_alpha_sq = -gm.gcon[0];
+    if (DD < one_over_alpha_sq) DD = one_over_alpha_sq;
+    return sqrt(DD);
+}
+
+// Apply the floors to the primitives pf of one zone (centre metric gm).
+// Returns 4 when the final Lorentz factor cannot be formed (the flag the
+// fixup kernel turns into pflag = -333), else 0.
+__device__ __noinline__ int floor_zone(double gam, double *pf, const Geo<double> &gm) {
+    State<double> q;
+    get_state(pf, gm, q);   // state before the floors
+    const double bsq = dot4(q.bcon, q.bcov);
+    double u = pf[UU];
+    double pre[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) pre[k] = pf[k];
+    double rhoflr = RHOMINLIMIT, uuflr = UUMINLIMIT;
+    // tie the floors to the local field and internal energy
+    if (rhoflr < bsq / BSQORHOMAX) rhoflr = bsq / (BSQORHOMAX);
+    if (uuflr < bsq / BSQOUMAX) uuflr = bsq / (BSQOUMAX);
+    if (rhoflr < u / UORHOMAX) rhoflr = u / (UORHOMAX);
+    if (rhoflr < RHOMINLIMIT) rhoflr = RHOMINLIMIT;
+    if (uuflr < UUMINLIMIT) uuflr = UUMINLIMIT;
+    int dofloor = 0;
+    if (pf[RHO] < rhoflr) { pf[RHO] = rhoflr; dofloor = 1; }
+    if (u < uuflr) { pf[UU] = uuflr; u = uuflr; dofloor = 1; }
+    // drift frame: keep the velocity perpendicular to B, set the parallel
+    // part from B.Q of the state before the floors (Noble et al. 2006, eq. 26)
+    double trans = 10. * bsq / (pf[RHO] < u ? pf[RHO] : u) - 1.;
+    if (dofloor && trans > 0.) {
+        if (trans > 1.) trans = 1.;
+        const double betapar = -q.bcon[0] / ((bsq + SMALL_D) * q.ucon[0]);
+        double betasq = betapar * betapar * bsq;
+        const double betasqmax = 1. - 1. / (GAMMAMAX * GAMMAMAX);
+        if (betasq > betasqmax) betasq = betasqmax;
+        const double gamma = 1. / sqrt(1 - betasq);
+        double ucondr[4], Bcon[4], Bcov[4], vcon[4];
+#pragma unroll
+        for (int m = 0; m < 4; m++) ucondr[m] = gamma * (q.ucon[m] + betapar * q.bcon[m]);
+        Bcon[0] = 0.;
+#pragma unroll
+        for (int m = 1; m < 4; m++) Bcon[m] = pf[B1 - 1 + m];
+        lower4(Bcon, gm.gcov, Bcov);
+        const double udotB = dot4(q.ucon, Bcov);
+        const double Bsq = dot4(Bcon, Bcov);
+        const double B = sqrt(Bsq);
+        const double wold = pre[RHO] + pre[UU] * gam;
+        const double QdotB = udotB * wold * q.ucon[0];
+        const double wnew = pf[RHO] + pf[UU] * gam;
+        const double x = 2. * QdotB / (B * wnew * ucondr[0] + SMALL_D);
+        const double vpar = x / (ucondr[0] * (1. + sqrt(1. + x * x)));
+        const double one_over_ucondr_t = 1. / ucondr[0];
+        vcon[0] = 1.;
+#pragma unroll
+        for (int m = 1; m < 4; m++) vcon[m] = vpar * Bcon[m] / (B + SMALL_D) + ucondr[m] * one_over_ucondr_t;
+        const double ut = ut_of_3vel(vcon, gm);
+        // u^mu = u^t v^mu, then the relative 4-velocity u~^i = u^i + gamma beta^i / alpha
+        // (ucon_to_utcon, GPU_phys_mhd.h:3-15)
+        const double alpha = 1. / sqrt(-gm.gcon[0]);
+        const double gam_n = alpha * (ut * vcon[0]);
+#pragma unroll
+        for (int m = 1; m < 4; m++) {
+            const double utcon = ut * vcon[m] + gam_n * (gm.gcon[m] * alpha * alpha) / alpha;
+            pf[m + UU] = utcon * trans + pre[m + UU] * (1. - trans);
+        }
+    }
+    // limit the Lorentz factor w.r.t. the normal observer
+    double gamma;
+    if (gamma_calc_flag(pf, gm, &gamma)) return 4;
+    if (gamma > GAMMAMAX) {
+        const double f = sqrt((GAMMAMAX * GAMMAMAX - 1.) / (gamma * gamma - 1.));
+        pf[U1] *= f;
+        pf[U2] *= f;
+        pf[U3] *= f;
+    }
+    return 0;
+}
+
 }  // namespace hamr

@@ -96,6 +96,20 @@ typedef struct hamr_params {
                                and no radial mass-flux fix there; such a block steps
                                through hamr_stage, hamr_bound_dim and the hamr_halo_*
                                exchange (the reference's block exchange, boundcomP.c) */
+    int floors;             /* 1: drift-frame floors on rho, u and the velocity after the
+                               inversion, with the Lorentz factor capped at 80 (fixup_cell's
+                               body, GPU_fixup.h:1025-1800, compiled out in the reference;
+                               zero-initialised: off, as the reference ships). A zone
+                               whose Lorentz factor cannot be formed gets pflag -333
+                               and counter 3 (GPU_fixup.h:398-415) */
+    int repair;             /* zones whose inversion failed (pflag != 0) after each sub-step:
+                               0 left as the solvers left them (the reference's step);
+                               1 reset to rho = u = 1e-20 with zero velocity, then floored
+                               when floors is on (fixuputoprim, GPU_fixup.h:735-852);
+                               2 replaced by the average of good neighbours, in (i, j, z)
+                               order, flags cleared (fixup_utoprim, fixup.c:764-827);
+                               no usable stencil: counter 4. Mode 2 is refused for halo
+                               blocks and allocates one int per active zone */
 } hamr_params;
 
 typedef struct hamr_ctx hamr_ctx;
@@ -121,8 +135,10 @@ int hamr_upload(hamr_ctx *ctx, const double *p, const double *ps);
  * GPU_read (GPU_main.cu:2646). */
 int hamr_download(hamr_ctx *ctx, double *p, double *ps);
 /* Device -> host copy of the inversion flags (1 int plane) and failure
- * counters (4 int planes: 2D failed, 1dvsq2fix1 failed, 1dfix1 failed,
- * floor; GPU_fixup.h:360-382). Either pointer may be NULL. */
+ * counters (5 int planes, NFAIL of config.h:1307: 2D failed, 1dvsq2fix1
+ * failed, 1dfix1 failed, floor gamma failure, neighbour repair without a
+ * usable stencil; GPU_fixup.h:360-415, fixup.c:819). Either pointer may be
+ * NULL. */
 int hamr_download_flags(hamr_ctx *ctx, int *pflag, int *failimage);
 
 /* Ghost fill of the current state (GPU_boundprim, GPU_main.cu:2113). */

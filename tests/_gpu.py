@@ -9,9 +9,10 @@ BCMAP = {"periodic": O.BC_PERIODIC, "outflow": O.BC_OUTFLOW, "pole_trans": O.BC_
          "pole_refl": O.BC_POLE_REFL}
 
 
-def make_pair(pb, strict=True, inversion="2d", recon="ppm", riemann="hll"):
+def make_pair(pb, strict=True, inversion="2d", recon="ppm", riemann="hll", floors=False, repair="none"):
     """CUDA block and oracle setup holding the same ghost-filled state."""
-    blk = Block(**pb.block_kwargs(), strict=strict, inversion=inversion, recon=recon, riemann=riemann)
+    blk = Block(**pb.block_kwargs(), strict=strict, inversion=inversion, recon=recon, riemann=riemann,
+                floors=floors, repair=repair)
     blk.set_geometry(pb.geo)
     blk.upload(pb.p, pb.ps)
     blk.bound()
@@ -22,7 +23,8 @@ def make_pair(pb, strict=True, inversion="2d", recon="ppm", riemann="hll"):
     geo = O.Geometry(pb.geo.gsize, pb.geo.gcov, pb.geo.gcon, pb.geo.gdet, pb.geo.conn)
     s = O.Setup(ob, geo, pb.dx, pb.gam, pb.cour, pb.poles[0], pb.poles[1],
                 tuple(BCMAP[b] for b in pb.bc), int(pb.ct_upwind), {"2d": 0, "nm": 1}[inversion],
-                {"ppm": 0, "mc": 1}[recon], {"hll": 0, "hllc": 1}[riemann])
+                {"ppm": 0, "mc": 1}[recon], {"hll": 0, "hllc": 1}[riemann], 0, int(bool(floors)),
+                {"none": 0, "reset": 1, "neighbours": 2}[repair])
     return blk, s
 
 

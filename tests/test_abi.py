@@ -48,7 +48,16 @@ def test_create_rejects_bad_parameters_without_device_work():
     bc1, prm.bc1 = prm.bc1, 0
     assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # a periodic x1 has no neighbours
     prm.bc1 = bc1
+    prm.repair = 2
+    assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # neighbour repair spans the domain
+    prm.repair = 0
     prm.halo = 0
+    prm.floors = 2
+    assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # floors are on or off
+    prm.floors = 0
+    prm.repair = 3
+    assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # no such repair
+    prm.repair = 0
     prm.ng = 3
     prm.gam = 1.0
     assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # gamma <= 1
