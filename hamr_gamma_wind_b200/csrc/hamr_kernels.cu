@@ -761,7 +761,7 @@ __device__ __forceinline__ void invert_zone(const Dims &d, const Geo<double> &gm
         for (int k = 0; k < NPR; k++) pf[k] = pc[k];
     }
     if constexpr ((FIX & FIX_FLOORS) != 0) {
-        if (floor_zone(d.gam, pf, gm)) {
+        if (floor_may_apply(pf, gm) && floor_zone(d.gam, pf, gm)) {
             flag = -333;
             failimage[3 * ks + c]++;
         }
@@ -1007,15 +1007,13 @@ __device__ void repair_zone(const RepairStencil &o, long ks, double *pv, int *pf
     pflag[c] = 0;
 }
 
+// (one thread per cell of the ghosted block: the flag test is one coalesced
+// load, and only a failed zone pays for its (i, j, z))
 __global__ void k_repair_scan(const Dims d, double *__restrict__ pv, int *__restrict__ pflag,
                               int *__restrict__ failimage, int *__restrict__ list, int *__restrict__ count) {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)d.n1 * d.n2 * d.n3) return;
-    const int z = d.ng3 + (int)(t % d.n3);
-    const int j = d.ng2 + (int)((t / d.n3) % d.n2);
-    const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
-    const long c = cix(d, i, j, z);
-    if (pflag[c] == 0) return;
+    const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (long)d.G1 * d.G2 * d.G3) return;
+    if (pflag[c] == 0 || !active_zone(d, c)) return;
     const RepairStencil o{(long)d.G2 * d.G3, d.G3, d.d3};
     if (failed_neighbour(d, o, pflag, c, false))
         list[atomicAdd(count, 1)] = (int)c;
@@ -1456,7 +1454,8 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
         inv_k[d.inversion == HAMR_INV_NM][fix]<<<nblk(n), BLK, 0, s>>>(
             d, m, full ? ctx->ph : ctx->p, ctx->W, full ? ctx->ps : ctx->psh, pout, ctx->pflag, ctx->failimage);
         if (ctx->prm.repair == 2) {
-            k_repair_scan<<<nblk(n), BLK, 0, s>>>(d, pout, ctx->pflag, ctx->failimage, ctx->rlist, ctx->rcount);
+            k_repair_scan<<<nblk((long)d.G1 * d.G2 * d.G3), BLK, 0, s>>>(d, pout, ctx->pflag, ctx->failimage,
+                                                                         ctx->rlist, ctx->rcount);
             k_repair_chain<<<1, REPAIR_THREADS, 0, s>>>(d, pout, ctx->pflag, ctx->failimage, ctx->rlist,
                                                         ctx->rcount);
         }

@@ -963,6 +963,33 @@ __device__ __forceinline__ double ut_of_3vel(const double *vcon, const Geo<doubl
     return sqrt(DD);
 }
 
+// True when the floors may change the zone: false only for a zone clearly
+// above every floor and below the Lorentz cap, where floor_zone changes
+// nothing and returns 0. b^2 = (B^i B_i + (B^i u_i)^2) / (u^t)^2 with
+// u_i = g_ij u~^j and (u^t)^2 = (1 + u~^i u~_i) (-g^tt), all without a
+// division or a square root; every test keeps a relative margin of 1e-6 (far
+// above the rounding of either form of b^2), so a zone near a threshold goes
+// to floor_zone, which decides exactly as the reference does.
+__device__ __forceinline__ bool floor_may_apply(const double *pf, const Geo<double> &gm) {
+    const double *g = gm.gcov;
+    const double v1 = pf[U1], v2 = pf[U2], v3 = pf[U3];
+    const double w1 = g[4] * v1 + g[5] * v2 + g[6] * v3;
+    const double w2 = g[5] * v1 + g[7] * v2 + g[8] * v3;
+    const double w3 = g[6] * v1 + g[8] * v2 + g[9] * v3;
+    const double qsq = v1 * w1 + v2 * w2 + v3 * w3;
+    const double b1 = pf[B1], b2 = pf[B2], b3 = pf[B3];
+    const double BB = b1 * (g[4] * b1 + g[5] * b2 + g[6] * b3) + b2 * (g[5] * b1 + g[7] * b2 + g[8] * b3)
+                    + b3 * (g[6] * b1 + g[8] * b2 + g[9] * b3);
+    const double Bu = b1 * w1 + b2 * w2 + b3 * w3;
+    const double num = (BB + Bu * Bu) * (1. + 1e-6);
+    const double den = (1. + qsq) * -gm.gcon[0];
+    const double rho = pf[RHO], u = pf[UU];
+    if (qsq > -1e-11 && 1. + qsq < 6399. && rho > RHOMINLIMIT * (1. + 1e-6) && u > UUMINLIMIT * (1. + 1e-6) &&
+        BSQORHOMAX * rho * den > num && BSQOUMAX * u * den > num && UORHOMAX * rho > u * (1. + 1e-6))
+        return false;
+    return true;
+}
+
 // Apply the floors to the primitives pf of one zone (centre metric gm).
 // Returns 4 when the final Lorentz factor cannot be formed (the flag the
 // fixup kernel turns into pflag = -333), else 0.
