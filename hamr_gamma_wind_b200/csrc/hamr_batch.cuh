@@ -139,15 +139,15 @@ struct OpCons {
     }
 };
 
-template <int INV>
+template <int INV, int FIX>
 // (the batched inversion keeps 5 blocks per SM: its tiles measured slower at
 // the single-block kernel's 6)
 struct OpInvert {
     static constexpr int PH = PH_INV, MINB = 5, SLOT = 0;
     static constexpr bool REDUCE = false;
     __device__ static double run(const BEntry &e, const StageArg &a, long t) {
-        k_invert_at<INV>(e.d, e.m, a.full ? e.ph : e.p, e.W, a.full ? e.ps : e.psh, a.full ? e.p : e.ph,
-                         e.pflag, e.failimage, t);
+        k_invert_at<INV, FIX>(e.d, e.m, a.full ? e.ph : e.p, e.W, a.full ? e.ps : e.psh, a.full ? e.p : e.ph,
+                              e.pflag, e.failimage, t);
         return 1.e9;
     }
 };
@@ -257,6 +257,7 @@ __global__ void k_batch_dt_finalize(const BEntry *__restrict__ E, int n, int upd
 struct hamr_batch {
     int n = 0;
     int precision = 0, recon = 0, inversion = 0, riemann = 0;
+    int fix = 0;   // FIX_* bits of the inversion phase (opt-in floors, reset of failed zones)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int nsm = 148;
@@ -332,7 +333,14 @@ void batch_stage_t(hamr_batch *b, int full, bool calc_dt, int only) {
     if (want(PH_POLE)) launch_phase<OpPole<T>>(b, a);
     if (want(PH_FACE)) launch_phase<OpFace<T>>(b, a);
     if (want(PH_CONS)) launch_phase<OpCons<T>>(b, a);
-    if (want(PH_INV)) launch_phase<OpInvert<INV>>(b, a);
+    if (want(PH_INV)) {
+        switch (b->fix) {
+            case FIX_FLOORS: launch_phase<OpInvert<INV, FIX_FLOORS>>(b, a); break;
+            case FIX_RESET: launch_phase<OpInvert<INV, FIX_RESET>>(b, a); break;
+            case FIX_FLOORS | FIX_RESET: launch_phase<OpInvert<INV, FIX_FLOORS | FIX_RESET>>(b, a); break;
+            default: launch_phase<OpInvert<INV, 0>>(b, a);
+        }
+    }
     if (want(PH_BX1)) launch_phase<OpBoundX1>(b, a);
     if (want(PH_BX3)) launch_phase<OpBoundX3>(b, a);
     if (want(PH_BX2)) launch_phase<OpBoundX2>(b, a);
@@ -386,7 +394,9 @@ int hamr_batch_create(hamr_ctx *const *blocks, int n, void *stream, hamr_batch *
             pk.riemann != p0.riemann)
             return HAMR_E_ARG;
         if (pk.halo) return HAMR_E_ARG;   // members are whole problems: no neighbours to exchange with
-        if (pk.floors || pk.repair) return HAMR_E_ARG;   // the opt-in floors and repairs step one block at a time
+        // one inversion instantiation for all members; the neighbour repair
+        // (its scan and one-CTA chain per block) steps one block at a time
+        if (pk.floors != p0.floors || pk.repair != p0.repair || pk.repair == 2) return HAMR_E_ARG;
         for (int j = 0; j < k; j++)
             if (blocks[j] == blocks[k]) return HAMR_E_ARG;
     }
@@ -395,6 +405,7 @@ int hamr_batch_create(hamr_ctx *const *blocks, int n, void *stream, hamr_batch *
     b->precision = blocks[0]->prm.precision;
     b->recon = blocks[0]->prm.recon;
     b->inversion = blocks[0]->prm.inversion;
+    b->fix = (blocks[0]->prm.floors ? FIX_FLOORS : 0) | (blocks[0]->prm.repair == 1 ? FIX_RESET : 0);
     b->riemann = blocks[0]->prm.riemann;
     b->ctx.assign(blocks, blocks + n);
     int dev = 0;

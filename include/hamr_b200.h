@@ -109,7 +109,8 @@ typedef struct hamr_params {
                                2 replaced by the average of good neighbours, in (i, j, z)
                                order, flags cleared (fixup_utoprim, fixup.c:764-827);
                                no usable stencil: counter 4. Mode 2 is refused for halo
-                               blocks and allocates one int per active zone */
+                               blocks and in batches, and allocates one int per active
+                               zone. Batch members share floors and repair */
 } hamr_params;
 
 typedef struct hamr_ctx hamr_ctx;

@@ -43,3 +43,18 @@ def field_rel_err(blk, p_dev, s, name="p"):
         d = np.abs(a[k] - b[k]).max()
         errs.append(0.0 if d == 0 else d / max(scale, 1e-300))
     return np.array(errs)
+
+
+def plant(pb, patch=3, frac=0.05, seed=13):
+    """Negative energy (inversion fails) and near-vacuum zones (floors)."""
+    P = pb.active(pb.p)
+    rng = np.random.default_rng(seed)
+    fail = rng.random(P[0].shape) < frac
+    i0, j0 = P.shape[1] // 3, P.shape[2] // 2
+    dz = patch if P.shape[3] > 1 else 1
+    fail[i0:i0 + patch, j0:j0 + patch, :dz] = True
+    P[1][fail] = -1e-2
+    thin = (rng.random(P[0].shape) < frac) & ~fail
+    P[0][thin] = 1e-24
+    P[1][thin] = 1e-26
+    return int(fail.sum()), int(thin.sum())

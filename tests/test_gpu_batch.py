@@ -12,16 +12,19 @@ import pytest
 
 from hamr_gamma_wind_b200 import problems
 from hamr_gamma_wind_b200.api import Batch, Block
+from tests._gpu import plant
 
 pytestmark = pytest.mark.gpu
 
 
-def _members(precision="fp64", strict=True, with_2d=True, **kw):
+def _members(precision="fp64", strict=True, with_2d=True, planted=False, **kw):
     pbs, _ = problems.torus_ensemble(4, 16, 26, seed=7)
     if with_2d:
         pbs.append(problems.fm_torus(40, 32, 1, rout=40.0))   # reflective poles, 2-D
     blocks = []
-    for pb in pbs:
+    for k, pb in enumerate(pbs):
+        if planted:
+            plant(pb, seed=100 + k)
         b = Block(**pb.block_kwargs(), precision=precision, strict=strict, **kw)
         b.set_geometry(pb.geo)
         b.upload(pb.p, pb.ps)
@@ -157,3 +160,44 @@ def test_batch_variants_match_single_blocks_bitwise(variant):
         np.testing.assert_array_equal(a.download()[0], b.download()[0])
     batch.close()
     _close(solo + mem)
+
+
+@pytest.mark.parametrize("floors,repair", [(True, "none"), (False, "reset"), (True, "reset")])
+def test_batch_with_floors_and_reset_matches_single_blocks_bitwise(floors, repair):
+    """Members with planted failed and near-vacuum zones (negative energies,
+    rho = 1e-24): the batched inversion phase with the opt-in floors and the
+    reset of failed zones is the single-block kernel's body, bit for bit,
+    flags and failure counters included."""
+    pbs, solo = _members(planted=True, floors=floors, repair=repair)
+    _, mem = _members(planted=True, floors=floors, repair=repair)
+    batch = Batch(mem)
+    dts = np.array([0.2 * min(pb.dx[:2]) for pb in pbs])
+    for _ in range(2):
+        dn_solo = np.array([b.step(dt) for b, dt in zip(solo, dts)])
+        dn_batch = batch.step(dts)
+        np.testing.assert_array_equal(dn_solo, dn_batch)
+        dts = np.minimum(dn_solo, 1.3 * dts)
+    nflag = 0
+    for a, b in zip(solo, mem):
+        np.testing.assert_array_equal(a.download()[0], b.download()[0])
+        np.testing.assert_array_equal(a.download()[1], b.download()[1])
+        fa, fb = a.download_flags(), b.download_flags()
+        np.testing.assert_array_equal(fa[0], fb[0])
+        np.testing.assert_array_equal(fa[1], fb[1])
+        nflag += int(fa[1].sum())
+    assert nflag > 0
+    batch.close()
+    _close(solo)
+    _close(mem)
+
+
+def test_batch_refuses_mixed_opt_ins_and_the_neighbour_repair():
+    from hamr_gamma_wind_b200 import _lib
+    _, a = _members(with_2d=False, floors=True)
+    _, b = _members(with_2d=False)
+    with pytest.raises(_lib.HamrError):
+        Batch(a[:2] + b[:2])
+    _, c = _members(with_2d=False, repair="neighbours")
+    with pytest.raises(_lib.HamrError):
+        Batch(c)
+    _close(a + b + c)

@@ -20,7 +20,7 @@ import numpy as np
 import pytest
 
 from hamr_gamma_wind_b200 import problems
-from tests._gpu import field_rel_err, make_pair, oracle_step
+from tests._gpu import field_rel_err, make_pair, oracle_step, plant
 
 pytestmark = pytest.mark.gpu
 
@@ -28,21 +28,6 @@ CASES = {
     "torus3d": lambda: problems.fm_torus(32, 16, 8, rout=40.0),
     "torus2d": lambda: problems.fm_torus(48, 48, 1, rout=40.0),
 }
-
-
-def plant(pb, patch=3, frac=0.05, seed=13):
-    """Negative energy (inversion fails) and near-vacuum zones (floors)."""
-    P = pb.active(pb.p)
-    rng = np.random.default_rng(seed)
-    fail = rng.random(P[0].shape) < frac
-    i0, j0 = P.shape[1] // 3, P.shape[2] // 2
-    dz = patch if P.shape[3] > 1 else 1
-    fail[i0:i0 + patch, j0:j0 + patch, :dz] = True
-    P[1][fail] = -1e-2
-    thin = (rng.random(P[0].shape) < frac) & ~fail
-    P[0][thin] = 1e-24
-    P[1][thin] = 1e-26
-    return int(fail.sum()), int(thin.sum())
 
 
 def run_pair(case, floors, repair, steps=2, strict=True, patch=3):
