@@ -16,6 +16,13 @@ Fixtures (numpy .npz, compressed):
                   active zones only; plus SHA-256 digests of the metric tables
                   and of the initial state, so the test can confirm it rebuilt
                   exactly the same inputs without the reference present.
+  ref_repair.npz  the failed-zone repairs (t3, t2): the reference's CPU
+                  fixup_utoprim on seeded random states and flag patterns
+                  (two flag densities), and its fixuputoprim kernel after a
+                  half sub-step of the reference kernels on a seeded block
+                  with planted failed zones; active zones only.
+
+`python tests/golden/make_golden.py repair` writes ref_repair.npz alone.
 """
 import hashlib
 import os
@@ -26,7 +33,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
 from oracle import oracle as O  # noqa: E402
-from tests._setups import clone, make_setup  # noqa: E402
+from tests._setups import clone, make_setup, plant_failures  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SEED = 13
@@ -147,12 +154,56 @@ def cell_fixture():
     return out
 
 
+REPAIR_DENSITIES = (0.35, 0.7)
+
+
+def flag_pattern_setup(dims, gam, density, seed):
+    """Seeded random primitives over the whole ghosted block and random
+    nonzero flags on a fraction `density` of the active zones (fixup_utoprim
+    reads no metric)."""
+    n1, n2, n3, ng = (int(x) for x in dims[:4])
+    blk = O.Block(n1, n2, n3, ng, int(dims[7]), int(dims[8]))
+    rng = np.random.default_rng(seed)
+    blk.arrays["p"][:] = rng.random(blk.arrays["p"].size)
+    act = blk.active("pflag", 1)[0]
+    act[...] = np.where(rng.random(act.shape) < density, rng.integers(1, 7, act.shape), 0)
+    geo = O.Geometry.empty(int(dims[8]))
+    return O.Setup(blk, geo, (1.0, 1.0, 1.0), gam, 0.8, 0, 0, (0, 0, 0))
+
+
+def repair_fixture():
+    out = {}
+    for v in ("t3", "t2"):
+        dims, gam = O.ref_dims(v)
+        out[f"{v}_dims"], out[f"{v}_gam"] = np.asarray(dims, np.int64), gam
+        for k, dens in enumerate(REPAIR_DENSITIES):
+            s = flag_pattern_setup(dims, gam, dens, SEED + k)
+            out[f"{v}_nb{k}_in_sha"] = digest(s.blk.arrays["p"], s.blk.arrays["pflag"])
+            O.ref_fixup_utoprim(v, s, "p")
+            out[f"{v}_nb{k}_p"] = active(s.blk, "p")[:5]   # RHO..U3: the planes the repair sets
+            out[f"{v}_nb{k}_fi4"] = s.blk.active("failimage")[4].copy()
+            assert not s.blk.pflag.any()
+        s = make_setup(v, seed=7)
+        plant_failures(s, frac=0.08, seed=11)
+        out[f"{v}_reset_in_sha"] = digest(s.blk.arrays["p"], s.blk.arrays["ps"])
+        O.ref_stage(v, s, 0, 0.0005, 0.001)
+        O.ref_fixuputoprim(v, s, "ph")
+        out[f"{v}_reset_ph"] = active(s.blk, "ph")[:5]
+        out[f"{v}_reset_pflag"] = s.blk.active("pflag", 1)[0].copy()
+        assert (out[f"{v}_reset_pflag"] != 0).any()
+    return out
+
+
 def main():
+    if sys.argv[1:] == ["repair"]:
+        np.savez_compressed(os.path.join(HERE, "ref_repair.npz"), **repair_fixture())
+        return
     for v in ("t3", "t2", "ot"):
         if not O.ref_available(v):
             raise SystemExit(f"reference host build {v} missing: run `make -C oracle ref` first")
         np.savez_compressed(os.path.join(HERE, f"ref_{v}.npz"), **variant_fixture(v))
     np.savez_compressed(os.path.join(HERE, "ref_cells.npz"), **cell_fixture())
+    np.savez_compressed(os.path.join(HERE, "ref_repair.npz"), **repair_fixture())
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")

@@ -93,3 +93,37 @@ def test_inversions_golden(name):
                          float(f[k + "gdet"][n]), f[k + "guess"][n].copy())
         assert r == rets[n], (n, r, rets[n])
         np.testing.assert_array_equal(p, f[k + "prim"][n])
+
+
+@pytest.mark.parametrize("v", ["t3", "t2"])
+def test_neighbour_repair_golden(v):
+    """The oracle's fixup_utoprim against the reference's CPU routine's
+    output on seeded random states and flag patterns."""
+    from tests.golden.make_golden import REPAIR_DENSITIES, flag_pattern_setup
+    f = load("ref_repair.npz")
+    dims, gam = f[f"{v}_dims"], float(f[f"{v}_gam"])
+    for k, dens in enumerate(REPAIR_DENSITIES):
+        s = flag_pattern_setup(dims, gam, dens, SEED + k)
+        assert digest(s.blk.arrays["p"], s.blk.arrays["pflag"]) == str(f[f"{v}_nb{k}_in_sha"])
+        before = s.blk.active("p").copy()
+        O.oracle_fixup_utoprim(s, "p")
+        np.testing.assert_array_equal(s.blk.active("p")[:5], f[f"{v}_nb{k}_p"])
+        np.testing.assert_array_equal(s.blk.active("p")[5:], before[5:])
+        np.testing.assert_array_equal(s.blk.active("failimage")[4], f[f"{v}_nb{k}_fi4"])
+        assert not s.blk.pflag.any()
+
+
+@pytest.mark.parametrize("v", ["t3", "t2"])
+def test_failed_zone_reset_golden(v):
+    """A half sub-step with planted failed zones and the reset of failed
+    zones (repair 1) against the reference's fixup and fixuputoprim kernels."""
+    from tests._setups import plant_failures
+    f = load("ref_repair.npz")
+    dims, gam = f[f"{v}_dims"], float(f[f"{v}_gam"])
+    s = make_setup(v, seed=7, dims=(dims, gam), geometry="product")
+    plant_failures(s, frac=0.08, seed=11)
+    assert digest(s.blk.arrays["p"], s.blk.arrays["ps"]) == str(f[f"{v}_reset_in_sha"])
+    s.repair = 1
+    O.oracle_stage(s, 0, 0.0005, 0.001)
+    np.testing.assert_array_equal(s.blk.active("ph")[:5], f[f"{v}_reset_ph"])
+    np.testing.assert_array_equal(s.blk.active("pflag", 1)[0], f[f"{v}_reset_pflag"])
