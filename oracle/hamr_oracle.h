@@ -37,7 +37,8 @@ typedef struct {
     int recon;           /* 0: PPM (para, PPM builds); 1: MC-limited linear
                             (slope_lim with factor 2, PPM = 0 builds) */
     int riemann;         /* 0: HLL; 1: HLLC in the orthonormal face frame
-                            (HLLC builds, FRAME_TRANSFORM) */
+                            (HLLC builds, FRAME_TRANSFORM); 2: HLLD there, with
+                            its HLLC and HLL fallbacks (HLLD builds) */
     int halo;            /* sides interior to a decomposed domain, whose ghosts
                             come from a neighbouring block: bit 0 the lower x1
                             side, bit 1 the upper; no physical fill and no

@@ -225,7 +225,7 @@ class Setup:
     ct_upwind: int = 1
     inversion: int = 0  # 0: Noble 2D, 1: Newman-Hamlin
     recon: int = 0      # 0: PPM, 1: MC-limited linear
-    riemann: int = 0    # 0: HLL, 1: HLLC
+    riemann: int = 0    # 0: HLL, 1: HLLC, 2: HLLD
     halo: int = 0       # x1 sides filled by a neighbour block: bit 0 lower, bit 1 upper
     floors: int = 0     # 1: drift-frame floors after the inversion
     repair: int = 0     # failed zones: 1 reset to the floor state, 2 neighbour interpolation
@@ -313,7 +313,7 @@ def ref_stage(variant, s: Setup, full, Dt, dt, calc_dt=False):
     b = s.blk
     a = b.arrays
     dtdir = np.full(4, 1e9)
-    if s.riemann == 1:
+    if s.riemann >= 1:
         mud, inv = ref_mud_tables(variant, s)
         ref(variant).ref_set_mud(_ptr(mud), _ptr(inv))
     ref(variant).ref_stage(int(full), Dt, dt, s.cour, s.dx[0], s.dx[1], s.dx[2], s.pole1, s.pole2,

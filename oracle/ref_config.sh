@@ -16,7 +16,8 @@
 #
 # usage: ref_config.sh <refdir> <outdir> <mode: torus|cart> <BS_1> <BS_2> <BS_3> <gamma-expr> [opts]
 #   opts: comma-separated build switches; mc = linear MC reconstruction (PPM 0),
-#         hllc = HLLC Riemann solver (HLLC 1, which turns on FRAME_TRANSFORM)
+#         hllc = HLLC Riemann solver (HLLC 1, which turns on FRAME_TRANSFORM),
+#         hlld = HLLD Riemann solver (HLLD 1, likewise)
 set -e
 REF="$1"; OUT="$2"; MODE="$3"; B1="$4"; B2="$5"; B3="$6"; GAM="$7"; OPTS="${8:-}"
 mkdir -p "$OUT"
@@ -42,5 +43,8 @@ case ",$OPTS," in
 esac
 case ",$OPTS," in
   *,hllc,*) sed -i -e 's/^#define HLLC (0)/#define HLLC (1)/' "$OUT/config.h.tmp" ;;
+esac
+case ",$OPTS," in
+  *,hlld,*) sed -i -e 's/^#define HLLD (0)/#define HLLD (1)/' "$OUT/config.h.tmp" ;;
 esac
 mv "$OUT/config.h.tmp" "$OUT/config.h"

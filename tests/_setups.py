@@ -104,7 +104,7 @@ def make_setup(variant, spin=0.9375, rout=40.0, seed=1, stress=False, cour=0.8, 
     fill_synthetic(blk, geo, dx, seed=seed, stress=stress)
     s = O.Setup(blk, geo, tuple(dx[1:]), gam, cour, poles[0], poles[1], bc,
                 ct_upwind=0 if variant == "ot" else 1, recon=1 if variant.endswith("m") else 0,
-                riemann=1 if variant.endswith("c") else 0)
+                riemann={"c": 1, "d": 2}.get(variant[-1], 0))
     O.oracle_bound(s, "p", "ps")
     return s
 
