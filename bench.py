@@ -651,8 +651,8 @@ def main():
                     help="c5: finite-difference directions checked after the timing (default 32)")
     ap.add_argument("--recon", default="ppm", choices=["ppm", "mc"],
                     help="reconstruction of the c3/c2 torus (PPM as shipped, or MC)")
-    ap.add_argument("--riemann", default="hll", choices=["hll", "hllc"],
-                    help="Riemann solver of the c3/c2 torus (HLL as shipped, or HLLC)")
+    ap.add_argument("--riemann", default="hll", choices=["hll", "hllc", "hlld"],
+                    help="Riemann solver of the c3/c2 torus (HLL as shipped, HLLC or HLLD)")
     ap.add_argument("--floors", action="store_true",
                     help="c3/c2 torus with the opt-in drift-frame floors (off in the reference's step)")
     ap.add_argument("--repair", default="none", choices=["none", "reset", "neighbours"],

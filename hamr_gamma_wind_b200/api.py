@@ -19,7 +19,7 @@ BC = {"periodic": 0, "outflow": 1, "pole_trans": 2, "pole_refl": 3}
 PRECISION = {"fp64": 0, "mixed": 1}
 INVERSION = {"2d": 0, "nm": 1}
 RECON = {"ppm": 0, "mc": 1}
-RIEMANN = {"hll": 0, "hllc": 1}
+RIEMANN = {"hll": 0, "hllc": 1, "hlld": 2}
 REPAIR = {"none": 0, "reset": 1, "neighbours": 2}
 RHO, UU, U1, U2, U3, B1, B2, B3, KTOT = range(9)
 FACE1, FACE2, CORN, CENT, FACE3 = range(5)

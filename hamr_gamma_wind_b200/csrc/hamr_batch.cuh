@@ -394,6 +394,7 @@ int hamr_batch_create(hamr_ctx *const *blocks, int n, void *stream, hamr_batch *
             pk.riemann != p0.riemann)
             return HAMR_E_ARG;
         if (pk.halo) return HAMR_E_ARG;   // members are whole problems: no neighbours to exchange with
+        if (pk.riemann == HAMR_RIEMANN_HLLD) return HAMR_E_ARG;   // HLLD steps one block at a time
         // one inversion instantiation for all members; the neighbour repair
         // (its scan and one-CTA chain per block) steps one block at a time
         if (pk.floors != p0.floors || pk.repair != p0.repair || pk.repair == 2) return HAMR_E_ARG;

@@ -161,9 +161,9 @@ __device__ __forceinline__ double flux_eval(const Dims &d, const Geo<T> &gm, con
     const T gam = (T)d.gam;
     const double dxd = DIR == 1 ? d.dx1 : (DIR == 2 ? d.dx2 : d.dx3);
     if constexpr ((REC & 2) != 0) {
-        // HLLC in the orthonormal face frame (fluxcalc2D_FT)
+        // HLLC (or, with bit 4, HLLD) in the orthonormal face frame (fluxcalc2D_FT)
         T Fo[NPR];
-        const T ctop = hllc_face<DIR, T>(gam, pl, pr, gm, Fo);
+        const T ctop = hllc_face<DIR, T, (REC & 4) != 0>(gam, pl, pr, gm, Fo);
 #pragma unroll
         for (int k = 0; k < NPR; k++) F[(long)k * d.ks + c] = Fo[k];
         const double v = d.cour * dxd / (double)ctop;
@@ -1359,6 +1359,12 @@ int launch_bound_dim(hamr_ctx *ctx, int full, int dim) {
 }
 
 // n faces of direction DIR, one thread per face, with the block's reconstruction
+// flux kernel variant: bit 0 MC reconstruction, bit 1 the face-frame
+// Riemann solvers (HLLC), bit 2 HLLD there
+inline int rec_key(const Dims &d) {
+    return d.recon | (d.riemann != HAMR_RIEMANN_HLL ? 2 : 0) | (d.riemann == HAMR_RIEMANN_HLLD ? 4 : 0);
+}
+
 template <int DIR, typename T>
 void launch_flux(long n, cudaStream_t s, const Dims &d, const Geom &m, const double *pin, const double *psin, T *F,
                  unsigned long long *dtbits, int cd, long rows_min) {
@@ -1368,18 +1374,22 @@ void launch_flux(long n, cudaStream_t s, const Dims &d, const Geom &m, const dou
     if (DIR != 3 && n_flux_rows<DIR == 3 ? 1 : DIR>(d) >= rows_min) {
         constexpr int RD = DIR == 3 ? 1 : DIR;
         const long nr = n_flux_rows<RD>(d);
-        switch (d.recon | (d.riemann << 1)) {
+        switch (rec_key(d)) {
         case 1: k_flux_rows<RD, T, 1><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
         case 2: k_flux_rows<RD, T, 2><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
         case 3: k_flux_rows<RD, T, 3><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+        case 6: k_flux_rows<RD, T, 6><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+        case 7: k_flux_rows<RD, T, 7><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
         default: k_flux_rows<RD, T, 0><<<nblk(nr), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
         }
         return;
     }
-    switch (d.recon | (d.riemann << 1)) {
+    switch (rec_key(d)) {
     case 1: k_flux<DIR, T, 1><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
     case 2: k_flux<DIR, T, 2><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
     case 3: k_flux<DIR, T, 3><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+    case 6: k_flux<DIR, T, 6><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+    case 7: k_flux<DIR, T, 7><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
     default: k_flux<DIR, T, 0><<<nblk(n), BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
     }
 }
@@ -1493,7 +1503,8 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
     *out = nullptr;
     if (prm->n1 < 2 || prm->n2 < 2 || prm->n3 < 1) return HAMR_E_ARG;
     if (prm->recon != HAMR_RECON_PPM && prm->recon != HAMR_RECON_MC) return HAMR_E_ARG;
-    if (prm->riemann != HAMR_RIEMANN_HLL && prm->riemann != HAMR_RIEMANN_HLLC) return HAMR_E_ARG;
+    if (prm->riemann != HAMR_RIEMANN_HLL && prm->riemann != HAMR_RIEMANN_HLLC && prm->riemann != HAMR_RIEMANN_HLLD)
+        return HAMR_E_ARG;
     if (!(prm->ng == 3 || (prm->ng == 2 && prm->recon == HAMR_RECON_MC))) return HAMR_E_ARG;
     if (prm->precision != HAMR_FP64 && prm->precision != HAMR_MIXED) return HAMR_E_ARG;
     if ((prm->halo & ~3) || (prm->halo && (prm->bc1 == HAMR_BC_PERIODIC || prm->n1 < prm->ng))) return HAMR_E_ARG;

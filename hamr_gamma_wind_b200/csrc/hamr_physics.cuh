@@ -849,9 +849,249 @@ __device__ __forceinline__ void hllc_mhd(int dir, const T *lu, const T *ru, T iv
     }
 }
 
+// HLLD (calc_HLLD and helpers, GPU_hllc.h:398-876; HLLD builds, marked "Does
+// not work yet" in the reference's config.h:482), in the operation order of
+// the reference, including its two slips that shape the result: G adds the
+// second transverse residual instead of its square (GPU_hllc.h:808,822), and
+// the right intermediate speed check takes vcon_ar[3] * vcon_al[3]
+// (GPU_hllc.h:673).
+template <typename T>
+struct HlldFan {
+    T K_al[4], B_al[4], K_ar[4], B_ar[4], v_al[4], v_ar[4], v_cl[4], v_cr[4], B_c[4];
+    T eta_l, eta_r, w_al, w_ar;
+};
+
+// one side's outer intermediate state and Alfven K vector for a total
+// pressure guess (the first half of calc_error_HLLD for side S = cmin or cmax)
+template <typename T>
+__device__ __forceinline__ void hlld_side(int dir, T ptot, T S, T sgn, T BX, const T *R, T *v, T *Bs, T *K, T &w,
+                                          T &eta) {
+    const int G_1 = dir, G_2 = dir % 3 + 1, G_3 = (dir + 1) % 3 + 1;
+    const int U_1 = UU + G_1, U_2 = UU + G_2, U_3 = UU + G_3;
+    const int B_1 = B1 + G_1 - 1, B_2 = B1 + G_2 - 1, B_3 = B1 + G_3 - 1;
+    const T A = R[U_1] + S * R[UU] + ptot * (T(1.) - S * S);
+    const T G = R[B_2] * R[B_2] + R[B_3] + R[B_3];
+    const T C = R[U_2] * R[B_2] + R[U_3] * R[B_3];
+    const T Q = -A - G + (BX * BX) * (T(1.) - S * S);
+    const T X = BX * (A * S * BX + C) - (A + G) * (S * ptot - R[UU]);
+    v[G_1] = (BX * (A * BX + S * C) - (A + G) * (ptot + R[U_1])) / (X);
+    v[G_2] = (Q * R[U_2] + R[B_2] * (C + BX * (S * R[U_1] + R[UU]))) / (X);
+    v[G_3] = (Q * R[U_3] + R[B_3] * (C + BX * (S * R[U_1] + R[UU]))) / (X);
+    w = ptot + (-R[UU] - (v[G_1] * R[U_1] + v[G_2] * R[U_2] + v[G_3] * R[U_3])) / (S - v[G_1] + T(SMALL_D));
+    Bs[G_1] = BX;
+    Bs[G_2] = (R[B_2] - Bs[G_1] * v[G_2]) / (S - v[G_1]);
+    Bs[G_3] = (R[B_3] - Bs[G_1] * v[G_3]) / (S - v[G_1]);
+    eta = sgn * ((T)(BX > T(0.0)) - (T)(BX <= T(0.0))) * d_sqrt(d_fabs(w));
+    const T den = S * ptot - R[UU] + BX * eta;
+    K[G_1] = (R[U_1] + ptot + R[B_1] * eta) / den;
+    K[G_2] = (R[U_2] + R[B_2] * eta) / den;
+    K[G_3] = (R[U_3] + R[B_3] * eta) / den;
+}
+
+// calc_error_HLLD (GPU_hllc.h:685-876, its live second half)
+template <typename T>
+__device__ __forceinline__ T hlld_error(int dir, T ptot, T cmin, T cmax, T BX, const T *R_l, const T *R_r,
+                                        HlldFan<T> &f) {
+    const int G_1 = dir, G_2 = dir % 3 + 1, G_3 = (dir + 1) % 3 + 1;
+    hlld_side(dir, ptot, cmin, T(-1.), BX, R_l, f.v_al, f.B_al, f.K_al, f.w_al, f.eta_l);
+    hlld_side(dir, ptot, cmax, T(1.), BX, R_r, f.v_ar, f.B_ar, f.K_ar, f.w_ar, f.eta_r);
+    f.B_c[G_1] = BX;
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+        const int Gt = t ? G_3 : G_2;
+        f.B_c[Gt] = ((f.B_ar[Gt] * (f.K_ar[G_1] - f.v_ar[dir]) + f.B_ar[dir] * f.v_ar[Gt]) -
+                     (f.B_al[Gt] * (f.K_al[G_1] - f.v_al[dir]) + f.B_al[dir] * f.v_al[Gt])) /
+                    (f.K_ar[dir] - f.K_al[dir] + T(1e-12));
+    }
+    const T delta_Kx = (f.K_ar[dir] - f.K_al[dir]);
+    T B_hat[4];
+    B_hat[1] = delta_Kx * f.B_c[1];
+    B_hat[2] = delta_Kx * f.B_c[2];
+    B_hat[3] = delta_Kx * f.B_c[3];
+    const T kl2 = f.K_al[1] * f.K_al[1] + f.K_al[2] * f.K_al[2] + f.K_al[3] * f.K_al[3];
+    const T kr2 = f.K_ar[1] * f.K_ar[1] + f.K_ar[2] * f.K_ar[2] + f.K_ar[3] * f.K_ar[3];
+    const T Y_l = (T(1.) - kl2) / (f.eta_l * delta_Kx - (f.K_al[1] * B_hat[1] + f.K_al[2] * B_hat[2] + f.K_al[3] * B_hat[3]));
+    const T Y_r = (T(1.) - kr2) / (f.eta_r * delta_Kx - (f.K_ar[1] * B_hat[1] + f.K_ar[2] * B_hat[2] + f.K_ar[3] * B_hat[3]));
+    const T error = delta_Kx * (T(1.) - f.B_ar[dir] * (Y_r - Y_l));
+    const T kbl = f.eta_l - (f.K_al[1] * f.B_c[1] + f.K_al[2] * f.B_c[2] + f.K_al[3] * f.B_c[3]);
+    const T kbr = f.eta_r - (f.K_ar[1] * f.B_c[1] + f.K_ar[2] * f.B_c[2] + f.K_ar[3] * f.B_c[3]);
+#pragma unroll
+    for (int q = 1; q < 4; q++) {
+        f.v_cl[q] = (f.K_al[q] - (f.B_c[q] * (T(1.) - kl2)) / kbl);
+        f.v_cr[q] = (f.K_ar[q] - (f.B_c[q] * (T(1.) - kr2)) / kbr);
+    }
+    f.v_cl[dir] = (f.v_cl[dir] + f.v_cr[dir]) * T(0.5);
+    f.v_cr[dir] = f.v_cl[dir];
+    return error;
+}
+
+// calc_HLLD_pres (GPU_hllc.h:425-531): HLLC estimate of the total pressure,
+// then at most 12 secant-Newton steps on hlld_error
+template <typename T>
+__device__ __noinline__ T hlld_pres(int dir, int &fail_c, int &fail_d, T cmin, T cmax, const T FH[2][NPR], const T *R_l,
+                                    const T *R_r, HlldFan<T> &f) {
+    const int G_1 = dir, G_2 = dir % 3 + 1, G_3 = (dir + 1) % 3 + 1;
+    const int U_1 = UU + G_1;
+    const int B_1 = B1 + G_1 - 1, B_2 = B1 + G_2 - 1, B_3 = B1 + G_3 - 1;
+    T vcon[4];
+    vcon[0] = T(0.);
+    T A = -FH[1][UU] - (FH[0][B_2] * FH[1][B_2] + FH[0][B_3] * FH[1][B_3]);
+    T B = -FH[1][U_1] + FH[0][UU] + (FH[0][B_2] * FH[0][B_2] + FH[0][B_3] * FH[0][B_3]) +
+          (FH[1][B_2] * FH[1][B_2] + FH[1][B_3] * FH[1][B_3]);
+    T C = FH[0][U_1] - (FH[0][B_2] * FH[1][B_2] + FH[0][B_3] * FH[1][B_3]);
+    T D = B * B - T(4.) * A * C;
+    vcon[G_1] = (-B - d_sqrt(d_max(T(0.), D))) / (T(2.) * A);
+    vcon[G_2] = (FH[0][B_2] * vcon[G_1] - FH[1][B_2]) / FH[0][B_1];
+    vcon[G_3] = (FH[0][B_3] * vcon[G_1] - FH[1][B_3]) / FH[0][B_1];
+    const T gammasq = T(1.) / (T(1.) - (vcon[1] * vcon[1] + vcon[2] * vcon[2] + vcon[3] * vcon[3]));
+    if ((vcon[dir] < cmin) || (vcon[dir] > cmax) || !(d_fabs(vcon[dir]) > T(0.))) fail_c = 1;
+    const T v_dot_B = (vcon[1] * FH[0][B1] + vcon[2] * FH[0][B2] + vcon[3] * FH[0][B3]);
+    const T ptot_HLLC =
+        -(-FH[1][UU] - FH[0][B_1] * (v_dot_B)) * vcon[dir] + FH[1][U_1] + FH[0][B_1] * FH[0][B_1] / gammasq;
+    T ptot = ptot_HLLC;
+    if (!(d_fabs(ptot) > T(0.))) {
+        // hydrodynamic estimate
+        fail_c = 1;
+        A = T(1.);
+        B = (-FH[0][UU] - FH[1][U_1]);
+        C = -FH[0][U_1] * FH[1][UU] + FH[1][U_1] * FH[0][UU];
+        D = B * B - T(4.) * A * C;
+        ptot = (-B + d_sqrt(d_max(T(0.), D))) / (T(2.) * A);
+        if (!(d_fabs(ptot) > T(0.))) {
+            fail_d = 1;
+            return T(-10.);
+        }
+    }
+    T ptot_old = ptot, d_ptot = T(0.);
+    T error_1 = hlld_error(dir, ptot, cmin, cmax, FH[0][B_1], R_l, R_r, f);
+    for (int n_iter = 0;; n_iter++) {
+        const T error_2 = hlld_error(dir, ptot + T(1e-10) * d_fabs(ptot), cmin, cmax, FH[0][B_1], R_l, R_r, f);
+        ptot_old = ptot;
+        const T de_dptot = (error_2 - error_1) / (T(1e-10) * d_fabs(ptot));
+        d_ptot = error_1 / de_dptot;
+        ptot = ptot - d_ptot;
+        if (ptot < T(0.)) ptot = T(0.5) * d_fabs(ptot);
+        error_1 = hlld_error(dir, ptot, cmin, cmax, FH[0][B_1], R_l, R_r, f);
+        if ((d_fabs(ptot - ptot_old) <= T(1e-8) * d_fabs(ptot + ptot_old)) || n_iter > 10) break;
+    }
+    if (!(d_fabs(ptot) > T(0.)) || ((d_fabs(d_ptot) > T(1e-8) * d_fabs(ptot + ptot_old)))) {
+        ptot = ptot_HLLC;
+        fail_d = 1;
+    }
+    return ptot;
+}
+
+// check_HLLD_par (GPU_hllc.h:635-683); true to reject the fan
+template <typename T>
+__device__ __forceinline__ bool hlld_check(int dir, T cmin, T cmax, T ptot, HlldFan<T> &f) {
+    const int G_1 = dir;
+    bool fail = false;
+#pragma unroll
+    for (int t = 0; t < 3; t++) {
+        const int Gt = t == 0 ? G_1 : (t == 1 ? dir % 3 + 1 : (dir + 1) % 3 + 1);
+        f.v_cl[Gt] = (f.v_cl[Gt] + f.v_cr[Gt]) * T(0.5);
+        f.v_cr[Gt] = f.v_cl[Gt];
+    }
+    if (f.v_cl[G_1] < f.K_al[G_1] || f.v_cl[G_1] < cmin) fail = true;
+    if (f.v_cl[G_1] > f.K_ar[G_1] || f.v_cl[G_1] > cmax) fail = true;
+    T vsq = (f.v_cl[1] * f.v_cl[1] + f.v_cl[2] * f.v_cl[2] + f.v_cl[3] * f.v_cl[3]);
+    if (!(vsq < T(0.999))) fail = true;
+    if (d_fabs(f.w_al) <= d_fabs(ptot) || f.v_al[G_1] <= cmin || f.K_al[G_1] <= cmin || f.w_al <= T(0.)) fail = true;
+    if (d_fabs(f.w_ar) <= d_fabs(ptot) || f.v_ar[G_1] >= cmax || f.K_ar[G_1] >= cmax || f.w_ar <= T(0.)) fail = true;
+    vsq = (f.v_al[1] * f.v_al[1] + f.v_al[2] * f.v_al[2] + f.v_al[3] * f.v_al[3]);
+    if (!(vsq < T(0.999))) fail = true;
+    vsq = (f.v_ar[1] * f.v_ar[1] + f.v_ar[2] * f.v_ar[2] + f.v_ar[3] * f.v_al[3]);
+    if (!(vsq < T(0.999))) fail = true;
+    vsq = (f.K_al[1] * f.K_al[1] + f.K_al[2] * f.K_al[2] + f.K_al[3] * f.K_al[3]);
+    if (!(vsq < T(0.999))) fail = true;
+    vsq = (f.K_ar[1] * f.K_ar[1] + f.K_ar[2] * f.K_ar[2] + f.K_ar[3] * f.K_ar[3]);
+    if (!(vsq < T(0.999))) fail = true;
+    return fail;
+}
+
+// outer intermediate state (between the fast and Alfven waves) of side S
+template <typename T>
+__device__ __forceinline__ void hlld_outer(int dir, T S, const T *R, T ptot, const T *v, const T *Bs, T BX, T *X) {
+    const int G_1 = dir, G_2 = dir % 3 + 1, G_3 = (dir + 1) % 3 + 1;
+    const T v_dot_B = v[1] * Bs[1] + v[2] * Bs[2] + v[3] * Bs[3];
+    X[RHO] = R[RHO] / (S - v[G_1]);
+    X[UU] = (R[UU] - ptot * v[G_1] + v_dot_B * Bs[G_1]) / (S - v[G_1] + T(SMALL_D));
+    X[UU + G_1] = (-X[UU] + ptot) * v[G_1] - v_dot_B * Bs[G_1];
+    X[UU + G_2] = (-X[UU] + ptot) * v[G_2] - v_dot_B * Bs[G_2];
+    X[UU + G_3] = (-X[UU] + ptot) * v[G_3] - v_dot_B * Bs[G_3];
+    X[B1 + G_1 - 1] = BX;
+    X[B1 + G_2 - 1] = Bs[G_2];
+    X[B1 + G_3 - 1] = Bs[G_3];
+    X[KTOT] = R[KTOT] / (S - v[G_1]);
+}
+
+// inner intermediate state (between the Alfven wave and the contact)
+template <typename T>
+__device__ __forceinline__ void hlld_inner(int dir, const T *Xa, T Ka, const T *va, T ptot, const T *vc, const T *Bc,
+                                           T BX, T *X) {
+    const int G_1 = dir, G_2 = dir % 3 + 1, G_3 = (dir + 1) % 3 + 1;
+    const T v_dot_B = vc[1] * Bc[1] + vc[2] * Bc[2] + vc[3] * Bc[3];
+    X[RHO] = Xa[RHO] * (Ka - va[G_1]) / (Ka - vc[G_1]);
+    X[UU] = -(-Ka * Xa[UU] - Xa[UU + G_1] + ptot * vc[G_1] - v_dot_B * Xa[B1 + G_1 - 1]) / (Ka - vc[G_1]);
+    X[UU + G_1] = (-Xa[UU] + ptot) * vc[G_1] - v_dot_B * Bc[G_1];
+    X[UU + G_2] = (-Xa[UU] + ptot) * vc[G_2] - v_dot_B * Bc[G_2];
+    X[UU + G_3] = (-Xa[UU] + ptot) * vc[G_3] - v_dot_B * Bc[G_3];
+    X[B1 + G_1 - 1] = BX;
+    X[B1 + G_2 - 1] = Bc[G_2];
+    X[B1 + G_3 - 1] = Bc[G_3];
+    X[KTOT] = Xa[KTOT] * (Ka - va[G_1]) / (Ka - vc[G_1]);
+}
+
+// calc_HLLD (GPU_hllc.h:398-423): HLLD star fluxes where the fan passes every
+// check, else HLLC where its estimate held, else HLL. The face at exactly
+// the right Alfven speed (iv == K_ar), where the reference leaves the flux
+// unset, takes HLL.
+template <typename T>
+__device__ __noinline__ void hlld_mhd(int dir, const T *lu, const T *ru, T iv, T cmin, T cmax, T FT[2][NPR],
+                                      const T FH[2][NPR], const T *Fl, const T *Fr, const T *Ul, const T *Ur) {
+    T R_l[NPR], R_r[NPR];
+    HlldFan<T> f;
+    int fail_c = 0, fail_d = 0;
+    for (int k = 0; k < NPR; k++) R_l[k] = (cmin * Ul[k] - Fl[k]);
+    for (int k = 0; k < NPR; k++) R_r[k] = (cmax * Ur[k] - Fr[k]);
+    const T ptot = hlld_pres(dir, fail_c, fail_d, cmin, cmax, FH, R_l, R_r, f);
+    if (fail_d == 0 && hlld_check(dir, cmin, cmax, ptot, f)) fail_d = 1;
+    if (fail_d == 0) {
+        const T BX = FH[0][B1 + dir - 1];
+        T X_a[NPR], X_c[NPR];
+        if ((cmin < iv) && (iv <= f.K_al[dir])) {
+            hlld_outer(dir, cmin, R_l, ptot, f.v_al, f.B_al, BX, X_a);
+            for (int k = 0; k < NPR; k++) { FT[0][k] = X_a[k]; FT[1][k] = Fl[k] + cmin * (X_a[k] - Ul[k]); }
+        } else if ((f.K_al[dir] < iv) && (iv <= f.v_cl[dir])) {
+            hlld_outer(dir, cmin, R_l, ptot, f.v_al, f.B_al, BX, X_a);
+            hlld_inner(dir, X_a, f.K_al[dir], f.v_al, ptot, f.v_cl, f.B_c, BX, X_c);
+            for (int k = 0; k < NPR; k++) {
+                FT[0][k] = X_c[k];
+                FT[1][k] = Fl[k] + cmin * (X_a[k] - Ul[k]) + f.K_al[dir] * (X_c[k] - X_a[k]);
+            }
+        } else if ((f.v_cr[dir] <= iv) && (iv < f.K_ar[dir])) {
+            hlld_outer(dir, cmax, R_r, ptot, f.v_ar, f.B_ar, BX, X_a);
+            hlld_inner(dir, X_a, f.K_ar[dir], f.v_ar, ptot, f.v_cr, f.B_c, BX, X_c);
+            for (int k = 0; k < NPR; k++) {
+                FT[0][k] = X_c[k];
+                FT[1][k] = Fr[k] + cmax * (X_a[k] - Ur[k]) + f.K_ar[dir] * (X_c[k] - X_a[k]);
+            }
+        } else if ((cmax > iv) && (iv > f.K_ar[dir])) {
+            hlld_outer(dir, cmax, R_r, ptot, f.v_ar, f.B_ar, BX, X_a);
+            for (int k = 0; k < NPR; k++) { FT[0][k] = X_a[k]; FT[1][k] = Fr[k] + cmax * (X_a[k] - Ur[k]); }
+        } else {
+            for (int k = 0; k < NPR; k++) { FT[0][k] = FH[0][k]; FT[1][k] = FH[1][k]; }
+        }
+    } else if (fail_c == 0) {
+        hllc_mhd(dir, lu, ru, iv, cmin, cmax, FT, FH, Fl, Fr, Ul, Ur);
+    } else {
+        for (int k = 0; k < NPR; k++) { FT[0][k] = FH[0][k]; FT[1][k] = FH[1][k]; }
+    }
+}
+
 // HLLC flux of one face (states carry the normal field already); returns ctop
 // from the coordinate-frame fast speeds, as the HLL path
-template <int DIR, typename T>
+template <int DIR, typename T, bool HLLD = false>
 __device__ __forceinline__ T hllc_face(T gam, const T *pl, const T *pr, const Geo<T> &gm, T *Fout) {
     State<T> ql, qr;
     T cmax_l, cmin_l, cmax_r, cmin_r, vd[NPR];
@@ -895,6 +1135,7 @@ __device__ __forceinline__ T hllc_face(T gam, const T *pl, const T *pr, const Ge
             FH[1][k] = ((cmax * Fl[k] - cmin * Fr[k] + cmax * cmin * (Ur[k] - Ul[k])) / (cmax - cmin + T(SMALL_D)));
         const bool do_hydro = d_fabs(FH[0][DIR + B1 - 1] * FH[0][DIR + B1 - 1] * lu[0] * ru[0]) < T(1.e-10) * d_fabs(FH[0][UU]);
         if (do_hydro) hllc_hydro(DIR, lu, ru, iv, cmin, cmax, FT, FH, Fl, Fr, Ul, Ur);
+        else if constexpr (HLLD) hlld_mhd(DIR, lu, ru, iv, cmin, cmax, FT, FH, Fl, Fr, Ul, Ur);
         else hllc_mhd(DIR, lu, ru, iv, cmin, cmax, FT, FH, Fl, Fr, Ul, Ur);
     }
     T F1[NPR];

@@ -69,8 +69,12 @@ enum hamr_recon {
 
 enum hamr_riemann {
     HAMR_RIEMANN_HLL = 0,   /* HLL (fluxcalc2D2, the shipped default, HLLC 0) */
-    HAMR_RIEMANN_HLLC = 1   /* HLLC in the orthonormal face frame with its HLL fallback
+    HAMR_RIEMANN_HLLC = 1,  /* HLLC in the orthonormal face frame with its HLL fallback
                                and hydrodynamic sub-case (fluxcalc2D_FT, GPU_hllc.h:3) */
+    HAMR_RIEMANN_HLLD = 2   /* HLLD there (calc_HLLD, GPU_hllc.h:398-876; HLLD builds,
+                               marked "Does not work yet", config.h:482), falling back to
+                               HLLC, then HLL, where its wave fan fails a check; single
+                               blocks only (batches refuse it) */
 };
 
 typedef struct hamr_params {

@@ -23,7 +23,7 @@ def make_pair(pb, strict=True, inversion="2d", recon="ppm", riemann="hll", floor
     geo = O.Geometry(pb.geo.gsize, pb.geo.gcov, pb.geo.gcon, pb.geo.gdet, pb.geo.conn)
     s = O.Setup(ob, geo, pb.dx, pb.gam, pb.cour, pb.poles[0], pb.poles[1],
                 tuple(BCMAP[b] for b in pb.bc), int(pb.ct_upwind), {"2d": 0, "nm": 1}[inversion],
-                {"ppm": 0, "mc": 1}[recon], {"hll": 0, "hllc": 1}[riemann], 0, int(bool(floors)),
+                {"ppm": 0, "mc": 1}[recon], {"hll": 0, "hllc": 1, "hlld": 2}[riemann], 0, int(bool(floors)),
                 {"none": 0, "reset": 1, "neighbours": 2}[repair])
     return blk, s
 
