@@ -94,6 +94,14 @@ struct StepSize {
 #ifndef HAMR_FLUX_MINB_F
 #define HAMR_FLUX_MINB_F 6
 #endif
+// the FP64 x1/x2 row kernels of the face-frame solvers (HLLC, HLLD), which
+// hold both frame states, their fluxes and the HLL state in thread-local
+// arrays, take a looser cap: on the 384 x 192 x 192 torus with HLLC, 3
+// blocks per SM cut those two kernels by 12 % and 9 % against 5; the face
+// kernels and the float kernels measured slower with it
+#ifndef HAMR_FLUX_FT_ROWS_MINB
+#define HAMR_FLUX_FT_ROWS_MINB 3
+#endif
 template <int DIR, typename T, int REC>
 __device__ __forceinline__ double flux_eval(const Dims &d, const Geo<T> &gm, const double *__restrict__ ps, T *pl,
                                             T *pr, T *__restrict__ F, const long c, const int j);
@@ -279,7 +287,8 @@ __host__ __device__ __forceinline__ long n_flux_rows(const Dims &d) {
 }
 
 template <int DIR, typename T, int REC>
-__global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? HAMR_FLUX_ROWS_MINB : HAMR_FLUX_ROWS_MINB_F)
+__global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? ((REC & 2) != 0 ? HAMR_FLUX_FT_ROWS_MINB : HAMR_FLUX_ROWS_MINB)
+                                                         : HAMR_FLUX_ROWS_MINB_F)
     k_flux_rows(const Dims d, const Geom m, const double *__restrict__ pv, const double *__restrict__ ps,
                 T *__restrict__ F, unsigned long long *__restrict__ dtbits, int calc_dt) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
