@@ -39,6 +39,8 @@ def test_create_rejects_bad_parameters_without_device_work():
     prm.ng = 3
     assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # no such reconstruction
     prm.recon = 0
+    prm.riemann = 3
+    assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # no such Riemann solver
     prm.riemann = 4
     assert L.hamr_ctx_create(ctypes.byref(prm), ctypes.byref(ctx)) == -1      # no such Riemann solver
     prm.riemann = 0
