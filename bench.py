@@ -2,7 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload c3|c2|c4|c5] [--precision fp64|mixed|both]
-                    [--recon ppm|mc] [--riemann hll|hllc]
+                    [--recon ppm|mc] [--riemann hll|hllc|hlld] [--no-accuracy]
 
 Workload (default c3): the 3-D Fishbone-Moncrief torus around a Kerr hole,
 a = 0.9375, r_in = 6, r_max = 12, gamma = 13/9, beta_min = 100, 4 % seeded
@@ -14,6 +14,17 @@ value = zones x steps / device time (cell-updates/s, the ZCPS of main.c:225),
 timed with CUDA events on the stream the kernels run on, after W warm-up
 steps, max over ranks. N > 1 runs independent replicas (one block per GPU,
 no exchange): scaling "weak".
+
+The default line also carries, untimed: `accuracy` -- per-field relative L1
+of the mixed step against the FP64 step after 1000 steps of the workload, and
+one FP64 step (production and strict builds) against the oracle's first step
+over every zone; `cpu_baseline` -- the oracle (the reference's step restated
+in C, bit-identical to host builds of the reference kernels) on the host
+cores over the whole workload, a bounded number of steps.
+
+--impl reference times that CPU step on the same workload, set up with the
+oracle's own metric tables, so no code of the CUDA library is loaded; it
+reports the steps it actually ran (at most K, within --cpu-budget seconds).
 """
 from __future__ import annotations
 
@@ -34,8 +45,6 @@ WORKLOADS = {
     "c3": dict(n1=384, n2=192, n3=192, rout=1000.0),
     "c2": dict(n1=192, n2=96, n3=64, rout=1000.0),
 }
-# CPU sample of the same torus (same per-zone work, fewer zones)
-CPU_SAMPLE = dict(n1=64, n2=32, n3=32, rout=1000.0)
 
 
 def _dist():
@@ -148,44 +157,104 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
-def cpu_baseline(steps: int = 1):
-    """The oracle (a C restatement of the reference step, bit-identical to the
-    reference kernels) on the host cores, OpenMP over zones."""
-    from hamr_gamma_wind_b200 import problems
-    from oracle import oracle as O
-    pb = problems.fm_torus(CPU_SAMPLE["n1"], CPU_SAMPLE["n2"], CPU_SAMPLE["n3"], rout=CPU_SAMPLE["rout"])
-    ob = O.Block(pb.n1, pb.n2, pb.n3, pb.ng, pb.ksize, pb.gsize)
-    ob.arrays["p"][:] = pb.p
-    ob.arrays["ps"][:] = pb.ps
-    geo = O.Geometry(pb.geo.gsize, pb.geo.gcov, pb.geo.gcon, pb.geo.gdet, pb.geo.conn)
-    s = O.Setup(ob, geo, pb.dx, pb.gam, pb.cour, 1, 1, (O.BC_OUTFLOW, O.BC_POLE_TRANS, O.BC_PERIODIC), 1)
-    O.oracle_bound(s)
-    stage = lambda s_, f, Dt, d, c: O.oracle_stage(s_, f, Dt, d, c)
-    bound = lambda s_, a, b: O.oracle_bound(s_, a, b)
-    dt = 0.2 * min(pb.dx[:2])
-    dt = min(O.step(stage, bound, s, dt), 1.3 * dt)   # warm-up
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        dt = min(O.step(stage, bound, s, dt), 1.3 * dt)
-    el = time.perf_counter() - t0
+class OracleRun:
+    """The oracle -- the C restatement of the reference step, bit-identical to
+    the reference's own kernels run on the host -- holding one problem, with
+    OpenMP over zones on the host cores. Used only as the CPU baseline and the
+    parity check of the benchmark, never as the thing measured on the GPU."""
+
+    def __init__(self, pb):
+        from oracle import oracle as O
+        self.O, self.pb = O, pb
+        ob = O.Block(pb.n1, pb.n2, pb.n3, pb.ng, pb.ksize, pb.gsize)
+        ob.arrays["p"][:] = pb.p
+        ob.arrays["ps"][:] = pb.ps
+        geo = O.Geometry(pb.geo.gsize, pb.geo.gcov, pb.geo.gcon, pb.geo.gdet, pb.geo.conn)
+        self.s = O.Setup(ob, geo, pb.dx, pb.gam, pb.cour, 1, 1, (O.BC_OUTFLOW, O.BC_POLE_TRANS, O.BC_PERIODIC), 1)
+        O.oracle_bound(self.s)
+        self.threads = O.num_threads()
+
+    def step(self, dt):
+        O = self.O
+        return O.step(lambda s_, f, Dt, d, c: O.oracle_stage(s_, f, Dt, d, c),
+                      lambda s_, a, b: O.oracle_bound(s_, a, b), self.s, dt)
+
+    def run(self, dt, steps, budget_s=None):
+        """Up to `steps` RK2 steps with the CFL step-size rule; stops early
+        once `budget_s` seconds have passed. Returns (steps run, seconds, dt)."""
+        t0 = time.perf_counter()
+        n = 0
+        while n < steps:
+            dt = min(self.step(dt), 1.3 * dt)
+            n += 1
+            if budget_s is not None and time.perf_counter() - t0 > budget_s:
+                break
+        return n, time.perf_counter() - t0, dt
+
+
+def cpu_sample(pb, warmup: int, steps: int, budget_s: float):
+    """Times the oracle on the whole workload: `warmup` untimed RK2 steps, then
+    up to `steps` timed ones within `budget_s` seconds (the count actually run
+    is reported). Returns (baseline dict, oracle run, step-1 state)."""
+    orc = OracleRun(pb)
+    dt0 = 0.2 * min(pb.dx[:2])
+    dt = orc.step(dt0)   # the first step starts from dt0, like the GPU runs
+    first = (orc.s.blk.arrays["p"].copy(), orc.s.blk.arrays["ps"].copy(), dt0)
+    dt = min(dt, 1.3 * dt0)
+    if warmup > 1:
+        _, _, dt = orc.run(dt, warmup - 1)
+    n, el, dt = orc.run(dt, steps, budget_s)
     cells = pb.n1 * pb.n2 * pb.n3
-    return {"value": cells * steps / el, "unit": "cell-updates/s",
-            "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)), "kind": "port",
-            "sample": f"{pb.n1}x{pb.n2}x{pb.n3} torus zones, {steps} RK2 step(s) after 1 warm-up"}
+    cb = {"value": cells * n / el, "unit": "cell-updates/s", "cores": orc.threads, "kind": "port",
+          "sample": f"the whole {pb.n1}x{pb.n2}x{pb.n3} torus, {n} timed RK2 step(s) after {max(1, warmup)} "
+                    f"untimed, OpenMP over zones ({orc.threads} threads)",
+          "steps": n, "ms_per_step": el * 1e3 / n}
+    return cb, orc, first
 
 
 def run_reference(args):
+    """The reference's step on the host cores, on the same workload: the
+    oracle (bit-identical to host builds of the reference kernels) with its
+    own metric tables -- no code of the CUDA library is loaded."""
     rank, world, _ = _dist()
     if rank != 0:
         return
-    cb = cpu_baseline(steps=max(1, args.steps // 10))
+    from hamr_gamma_wind_b200 import problems
+    from oracle import oracle as O
+    wl = WORKLOADS[args.workload]
+    pb = problems.fm_torus(wl["n1"], wl["n2"], wl["n3"], rout=wl["rout"], geometry=O.build_geometry)
+    cb, _, _ = cpu_sample(pb, warmup=1, steps=args.steps, budget_s=args.cpu_budget)
     out = {"metric": "cell-updates/s", "value": cb["value"], "unit": "cell-updates/s", "n_gpus": args.gpus,
-           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
-           "dtype": "f64", "data": "synthetic", "vs_baseline": None,
-           "config": {"workload": f"torus {args.workload} sample", "sample": cb["sample"]},
+           "steps": cb["steps"], "warmup": 1, "requested_steps": args.steps, "requested_warmup": args.warmup,
+           "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "impl": "reference",
+           "dtype": "f64", "data": "synthetic", "vs_baseline": None, "scaling": "weak",
+           "config": _config(wl, "fp64", args, same_config=True),
            "cpu_baseline": cb,
-           "e2e": {"value": cb["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+           "e2e": {"value": cb["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "native_so_loaded": _loaded_native()}
     print(json.dumps(out), flush=True)
+
+
+def _loaded_native():
+    """Shared objects of this repository mapped into the process."""
+    out = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                path = line.split()[-1] if line.strip() else ""
+                if path.endswith(".so") and path.startswith(ROOT):
+                    out.add(os.path.relpath(path, ROOT))
+    except OSError:
+        pass
+    return sorted(out)
+
+
+def _config(wl, precision, args, **extra):
+    return {"workload": f"3-D FM torus {wl['n1']}x{wl['n2']}x{wl['n3']} (a=0.9375, r_in=6, r_max=12, "
+                        f"gamma=13/9, beta_min=100), {precision}",
+            "zones": wl["n1"] * wl["n2"] * wl["n3"], "precision": precision, "recon": args.recon,
+            "riemann": args.riemann, "floors": bool(args.floors), "repair": args.repair,
+            "l2": "inputs larger than L2 (no flush)", "dt_update_interval": 16, **extra}
 
 
 def _measure(pb, precision, args, stream, world):
@@ -229,43 +298,6 @@ def _kernel_profile(blk, dt):
     blk._check(blk.L.hamr_profile_step(blk.ctx, dt, 2, prof.ctypes.data_as(ctypes.c_void_p), len(prof)),
                "hamr_profile_step")
     return dict(zip(_lib.PROF_SLOTS, prof.tolist()))
-
-
-def run_accuracy(args):
-    """Per-field relative L1 difference of the mixed-precision run against the
-    FP64 run after --accuracy steps of the workload (same initial state, same
-    step-size rule)."""
-    import torch
-    from hamr_gamma_wind_b200 import problems
-    wl = WORKLOADS[args.workload]
-    pb = problems.fm_torus(wl["n1"], wl["n2"], wl["n3"], rout=wl["rout"])
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
-    from hamr_gamma_wind_b200.api import Block
-    out = {}
-    for prec in ("fp64", "mixed"):
-        blk = Block(**pb.block_kwargs(), precision=prec, stream=ctypes_stream(stream))
-        blk.set_geometry(pb.geo)
-        blk.upload(pb.p, pb.ps)
-        blk.bound()
-        dt = 0.2 * min(pb.dx[:2])
-        left = args.accuracy
-        while left > 0:
-            n = min(left, 100)
-            dt = blk.step_ch(n, dt, interval=16)
-            left -= n
-        p, ps = blk.download()
-        out[prec] = (pb.active(p).copy(), pb.active(ps).copy(), dt)
-        blk.close()
-    names = ["rho", "u", "u1", "u2", "u3", "B1", "B2", "B3"]
-    p64, s64, dt64 = out["fp64"]
-    p32, s32, dt32 = out["mixed"]
-    errs = {n: float(np.abs(p32[k] - p64[k]).sum() / max(np.abs(p64[k]).sum(), 1e-300)) for k, n in enumerate(names)}
-    errs.update({f"face_B{k + 1}": float(np.abs(s32[k] - s64[k]).sum() / max(np.abs(s64[k]).sum(), 1e-300))
-                 for k in range(3)})
-    print(json.dumps({"accuracy_steps": args.accuracy, "workload": args.workload,
-                      "l1_rel_mixed_vs_fp64": errs, "dt_fp64": dt64, "dt_mixed": dt32,
-                      "finite": bool(np.isfinite(p32).all() and np.isfinite(p64).all())}), flush=True)
 
 
 def run_ours(args):
@@ -345,6 +377,19 @@ def run_ours(args):
     bytes_io = (nk + 3 * blk.ksize) * 8
     p_end, _ = blk.download()
     finite = bool(np.isfinite(blk.active(p_end)).all())
+    blk.close()
+
+    accuracy = None
+    if not args.no_accuracy and rank == 0:
+        accuracy = _accuracy_block(pb, args, stream)
+    cb = None
+    if rank == 0:
+        try:
+            cb, orc, first = cpu_sample(pb, warmup=1, steps=2, budget_s=args.cpu_budget)
+            if accuracy is not None:
+                accuracy.update(_step1_vs_oracle(pb, first, stream))
+        except Exception as exc:  # the oracle is test infrastructure; report, do not fail the bench
+            cb = {"value": None, "error": str(exc)}
 
     if rank == 0:
         out = {
@@ -352,12 +397,7 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if head == "fp64" else "f32 flux/EMF + f64 update/inversion", "data": "synthetic",
-            "config": {"workload": f"3-D FM torus {wl['n1']}x{wl['n2']}x{wl['n3']} (a=0.9375, r_in=6, r_max=12, "
-                                   f"gamma=13/9, beta_min=100), {head}",
-                       "zones": cells, "precision": head, "recon": args.recon, "riemann": args.riemann,
-                       "floors": bool(args.floors), "repair": args.repair,
-                       "l2": "inputs larger than L2 (no flush)",
-                       "dt_update_interval": 16, "parallelism": f"replicas x{world}"},
+            "config": _config(wl, head, args, parallelism=f"replicas x{world}"),
             "precisions": {k: {"value": v["value"], "ms_per_step": v["ms"] / args.steps,
                                "kernel_ms_per_step": v.get("kernels"),
                                **({"failures": v["failures"]} if "failures" in v else {})}
@@ -374,14 +414,81 @@ def run_ours(args):
         }
         if "fp64" in runs and "mixed" in runs:
             out["mixed_over_fp64"] = runs["mixed"]["value"] / runs["fp64"]["value"]
-        try:
-            out["cpu_baseline"] = cpu_baseline(steps=1)
-        except Exception as exc:  # the oracle is test infrastructure; report, do not fail the bench
-            out["cpu_baseline"] = {"value": None, "error": str(exc)}
+        if accuracy is not None:
+            out["accuracy"] = accuracy
+        out["cpu_baseline"] = cb
         print(json.dumps(out), flush=True)
-    blk.close()
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def _rel_errs(a, b, names, l1=True):
+    """Per-field relative L1 (or max) difference of a against b."""
+    out = {}
+    for k, n in enumerate(names):
+        d, r = np.abs(a[k] - b[k]), np.abs(b[k])
+        out[n] = float(d.sum() / max(r.sum(), 1e-300)) if l1 else float(d.max() / max(r.max(), 1e-300))
+    return out
+
+
+PRIM_NAMES = ["rho", "u", "u1", "u2", "u3", "B1", "B2", "B3"]
+FACE_NAMES = ["face_B1", "face_B2", "face_B3"]
+
+
+def _accuracy_block(pb, args, stream):
+    """Per-field relative L1 difference of the mixed-precision step against
+    the FP64 step after `accuracy_steps` steps of the workload from the same
+    initial state with the same step-size rule (device runs, untimed)."""
+    from hamr_gamma_wind_b200.api import Block
+    nsteps = args.accuracy or 1000
+    out = {}
+    for prec in ("fp64", "mixed"):
+        blk = Block(**pb.block_kwargs(), precision=prec, stream=ctypes_stream(stream))
+        blk.set_geometry(pb.geo)
+        blk.upload(pb.p, pb.ps)
+        blk.bound()
+        dt = 0.2 * min(pb.dx[:2])
+        left = nsteps
+        while left > 0:
+            n = min(left, 100)
+            dt = blk.step_ch(n, dt, interval=16)
+            left -= n
+        p, ps = blk.download()
+        out[prec] = (pb.active(p).copy(), pb.active(ps).copy(), dt)
+        blk.close()
+    p64, s64, dt64 = out["fp64"]
+    p32, s32, dt32 = out["mixed"]
+    errs = _rel_errs(p32, p64, PRIM_NAMES)
+    errs.update(_rel_errs(s32, s64, FACE_NAMES))
+    return {"steps": nsteps, "l1_rel_mixed_vs_fp64": errs, "target_rho_l1": 1e-5,
+            "dt_after_fp64": dt64, "dt_after_mixed": dt32,
+            "finite": bool(np.isfinite(p32).all() and np.isfinite(p64).all())}
+
+
+def _step1_vs_oracle(pb, first, stream):
+    """One FP64 step on the GPU from the workload's initial state against the
+    oracle's first step (the reference's step, run on the host): the
+    production build (fused multiply-adds) per field in relative L1 and max
+    over all active zones, and the strict build (no contraction) in max."""
+    from hamr_gamma_wind_b200.api import Block
+    p_o, ps_o, dt0 = first
+    po = pb.active(p_o)
+    so = pb.active(ps_o)
+    res = {}
+    for strict in (False, True):
+        blk = Block(**pb.block_kwargs(), precision="fp64", strict=strict, stream=ctypes_stream(stream))
+        blk.set_geometry(pb.geo)
+        blk.upload(pb.p, pb.ps)
+        blk.bound()
+        blk.step(dt0)
+        p, ps = blk.download()
+        blk.close()
+        pa, sa = pb.active(p), pb.active(ps)
+        key = "strict_fp64_vs_oracle_step1" if strict else "fp64_vs_oracle_step1"
+        res[key] = {"max_rel": {**_rel_errs(pa, po, PRIM_NAMES, l1=False), **_rel_errs(sa, so, FACE_NAMES, l1=False)}}
+        if not strict:
+            res[key]["l1_rel"] = {**_rel_errs(pa, po, PRIM_NAMES), **_rel_errs(sa, so, FACE_NAMES)}
+    return res
 
 
 ENSEMBLE = dict(count=64, nmin=32, nmax=96, seed=2024)
@@ -658,7 +765,11 @@ def main():
     ap.add_argument("--repair", default="none", choices=["none", "reset", "neighbours"],
                     help="c3/c2 torus: repair of failed zones (none, as the reference's step)")
     ap.add_argument("--accuracy", type=int, default=0,
-                    help="instead of timing: per-field L1 difference of mixed vs FP64 after this many steps")
+                    help="steps of the accuracy block (mixed vs FP64 per-field L1; default 1000)")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the accuracy block (mixed vs FP64 after 1000 steps, step 1 vs the oracle)")
+    ap.add_argument("--cpu-budget", type=float, default=120.0,
+                    help="seconds of timed oracle steps at most (CPU baseline and the reference arm)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="warm-up and timed steps only (for profiler runs)")
     ap.add_argument("--slabs", type=int, default=0,
@@ -668,8 +779,6 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
-    elif args.accuracy:
-        run_accuracy(args)
     elif args.workload == "c4":
         run_ensemble(args)
     elif args.workload == "c5":

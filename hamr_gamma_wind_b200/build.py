@@ -33,7 +33,7 @@ def _stale(out):
 
 
 def build(force=False, verbose=False):
-    outs = []
+    outs, jobs = [], []
     for name, extra in TARGETS.items():
         out = os.path.join(HERE, name)
         outs.append(out)
@@ -46,12 +46,18 @@ def build(force=False, verbose=False):
         cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
                "-Xcompiler", "-ffp-contract=off", "-prec-div=false", "-prec-sqrt=false",
                "-Xptxas", "-v" if verbose else "-O3", *extra, *SOURCES, "-o", out]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode != 0:
-            sys.stderr.write(r.stdout + r.stderr)
-            raise RuntimeError(f"nvcc failed building {name}")
-        if verbose:
-            sys.stderr.write(r.stderr)
+        # the builds are independent: compile them side by side
+        jobs.append((name, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+    failed = []
+    for name, proc in jobs:
+        so, se = proc.communicate()
+        if proc.returncode != 0:
+            sys.stderr.write(so + se)
+            failed.append(name)
+        elif verbose:
+            sys.stderr.write(se)
+    if failed:
+        raise RuntimeError(f"nvcc failed building {', '.join(failed)}")
     return outs
 
 

@@ -20,6 +20,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <string>
@@ -1851,21 +1852,23 @@ struct NaPtrs {
     double *ndt = nullptr;
 };
 NaPtrs na_ptrs[NA_MAX_DEVICES];
-bool na_ready[NA_MAX_DEVICES];
+// set (release) after na_ptrs[dev] is written; a reader that sees it set
+// (acquire) also sees the pointers
+std::atomic<bool> na_ready[NA_MAX_DEVICES];
 std::mutex na_mutex;
 
 // Device addresses of the scratch arrays on the current device, looked up once
 // per device: in host code the array names are host-side stand-ins.
 int na_setup(int dev) {
     std::lock_guard<std::mutex> lock(na_mutex);
-    if (na_ready[dev]) return HAMR_OK;
+    if (na_ready[dev].load(std::memory_order_acquire)) return HAMR_OK;
     NaPtrs q;
     if (cudaGetSymbolAddress((void **)&q.scratch, na_scratch) != cudaSuccess) return HAMR_E_CUDA;
     if (cudaGetSymbolAddress((void **)&q.iscratch, na_iscratch) != cudaSuccess) return HAMR_E_CUDA;
     if (cudaGetSymbolAddress((void **)&q.dtbits, na_dtbits) != cudaSuccess) return HAMR_E_CUDA;
     if (cudaGetSymbolAddress((void **)&q.ndt, na_ndt) != cudaSuccess) return HAMR_E_CUDA;
     na_ptrs[dev] = q;
-    na_ready[dev] = true;
+    na_ready[dev].store(true, std::memory_order_release);
     return HAMR_OK;
 }
 
@@ -1909,7 +1912,7 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
     d.halo = 0;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES) return HAMR_E_CUDA;
-    if (!na_ready[dev] && na_setup(dev) != HAMR_OK) return HAMR_E_CUDA;
+    if (!na_ready[dev].load(std::memory_order_acquire) && na_setup(dev) != HAMR_OK) return HAMR_E_CUDA;
     const NaPtrs &q = na_ptrs[dev];
     const long ks = d.ks;
     c.stream = (cudaStream_t)prm->stream;

@@ -178,7 +178,7 @@ def _bsq(P, gcov, gcon):
 
 def fm_torus(n1, n2, n3, spin=0.9375, rin=6.0, rmax=12.0, gam=13.0 / 9.0, kappa=1.e-3, beta=100.0,
              rout=None, seed=12345, noise=0.04, rho_atm=1.e-14, u_atm=1.e-16, cour=0.8, ng=3,
-             generic=0.0) -> Problem:
+             generic=0.0, geometry=None) -> Problem:
     """Magnetised Fishbone-Moncrief torus around a Kerr hole in the reference's
     code coordinates. n3 > 1: transmissive poles; n3 == 1: axisymmetric with
     reflective poles. The atmosphere is the reference's 1e-7*RHOMIN / 1e-7*UUMIN
@@ -188,11 +188,13 @@ def fm_torus(n1, n2, n3, spin=0.9375, rin=6.0, rmax=12.0, gam=13.0 / 9.0, kappa=
     zero velocities and field outside the torus), at which the limiters and
     upwind switches are not differentiable: seeded relative noise of that size
     on rho, u and the velocities, a power-law atmosphere, and a weak seeded
-    field everywhere (vector potential scaled with sqrt(rho))."""
+    field everywhere (vector potential scaled with sqrt(rho)). geometry: the
+    metric-table builder, called like api.build_geometry (default: the
+    library's hamr_build_geometry)."""
     if rout is None:
         rout = 4.0 * rmax * 2.0
     startx, dx = ks_grid(n1, n2, n3, spin, rout)
-    geo = build_geometry("ks", spin, n1, n2, n3, startx, dx, ng)
+    geo = (geometry or build_geometry)("ks", spin, n1, n2, n3, startx, dx, ng)
     ks, p, ps = _alloc(n1, n2, n3, ng)
     g1, g2 = n1 + 2 * ng, n2 + 2 * ng
     g3 = n3 + 2 * ng if n3 > 1 else 1

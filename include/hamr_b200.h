@@ -221,8 +221,12 @@ int hamr_device_state(hamr_ctx *ctx, double **p, double **ps, double **ph, doubl
  * loads the library, until the process exits). Larger blocks are rejected with
  * HAMR_E_ARG before any device work. Nothing is allocated: no cudaMalloc,
  * cudaFree, stream or event creation.
- *   - runs on prm->stream (NULL: the legacy default stream); prm->precision
- *     must be HAMR_FP64;
+ *   - runs on prm->stream (NULL: the legacy default stream);
+ *   - accepts PPM or MC reconstruction, HLL or HLLC, Noble 2D or
+ *     Newman-Hamlin inversion, every boundary kind; refuses with HAMR_E_ARG
+ *     precision other than HAMR_FP64, riemann == HAMR_RIEMANN_HLLD,
+ *     floors != 0, repair != 0 and halo != 0 (those need arrays or passes
+ *     this step does not carry);
  *   - the first call on a device looks up the device addresses of the static
  *     arrays (cudaGetSymbolAddress); make that first call outside any stream
  *     capture;

@@ -100,4 +100,14 @@ void ho_fixup_utoprim(const ho_grid *g, double *pv, int *pflag, int *failimage);
 /* Diagnostics */
 double ho_divb_max(const ho_grid *g, const ho_geom *m, const double *ps);
 
+/* host metric tables of one block (hamr_oracle_geom.c; set_grid, main.c:380-455):
+ * coords 0 Kerr-Schild in the reference's code coordinates, 1 Minkowski;
+ * 0, -1 bad argument, -5 a singular metric */
+int ho_build_geometry(int coords, double spin, int n1, int n2, int n3, int ng, long gsize, const double *startx,
+                      const double *dx, double *gcov, double *gcon, double *gdet, double *conn);
+/* Boyer-Lindquist (r, theta, phi) of a code-coordinate point (bl_coord, coord.c:111) */
+int ho_bl_coord(int coords, double spin, const double *X, double *rthph);
+/* OpenMP threads a parallel loop of the oracle uses (1 without OpenMP) */
+int ho_num_threads(void);
+
 #endif

@@ -79,6 +79,10 @@ def lib():
         L.ho_fixup_cell.argtypes = [_d, _vp, _vp, _vp, _d]
         L.ho_fixup_cell.restype = _i
         L.ho_fixup_utoprim.argtypes = [ctypes.POINTER(HoGrid), _vp, _vp, _vp]
+        L.ho_build_geometry.argtypes = [_i, _d, _i, _i, _i, _i, ctypes.c_long, _vp, _vp, _vp, _vp, _vp, _vp]
+        L.ho_build_geometry.restype = _i
+        L.ho_bl_coord.argtypes = [_i, _d, _vp, _vp]
+        L.ho_num_threads.restype = _i
         _lib = L
     return _lib
 
@@ -210,6 +214,29 @@ def ref_geometry(variant, spin, startx, dx):
     if nfail:
         raise RuntimeError(f"reference geometry reported {nfail} failures")
     return geo
+
+
+def build_geometry(coords: str, spin: float, n1: int, n2: int, n3: int, startx, dx, ng: int = 3,
+                   gsize: int = 0) -> "Geometry":
+    """The oracle's own metric tables (hamr_oracle_geom.c), same call and
+    layout as the product's hamr_gamma_wind_b200.api.build_geometry: lets a
+    problem be set up with no product code loaded."""
+    g1 = n1 + 2 * ng if n1 > 1 else 1
+    g2 = n2 + 2 * ng if n2 > 1 else 1
+    gs = gsize or pad64(g1 * g2)
+    geo = Geometry.empty(gs)
+    sx = np.ascontiguousarray(startx, float)
+    dd = np.ascontiguousarray(dx, float)
+    rc = lib().ho_build_geometry({"ks": 0, "cartesian": 1}[coords], spin, n1, n2, n3, ng, gs, _ptr(sx), _ptr(dd),
+                                 _ptr(geo.gcov), _ptr(geo.gcon), _ptr(geo.gdet), _ptr(geo.conn))
+    if rc:
+        raise RuntimeError(f"ho_build_geometry: {rc}")
+    return geo
+
+
+def num_threads() -> int:
+    """OpenMP threads the oracle's parallel loops use."""
+    return int(lib().ho_num_threads())
 
 
 @dataclass

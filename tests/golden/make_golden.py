@@ -1,6 +1,6 @@
 """Writes the golden fixtures of tests/test_golden.py from the reference's own
 kernel code, built for the host from the reference sources (oracle/Makefile,
-`make -C oracle ref`). Run from the repository root:
+`make -C oracle ref REF=<reference source tree>`). Run from the repository root:
 
     python tests/golden/make_golden.py
 
@@ -200,7 +200,7 @@ def main():
         return
     for v in ("t3", "t2", "ot"):
         if not O.ref_available(v):
-            raise SystemExit(f"reference host build {v} missing: run `make -C oracle ref` first")
+            raise SystemExit(f"reference host build {v} missing: run `make -C oracle ref REF=<reference source tree>` first")
         np.savez_compressed(os.path.join(HERE, f"ref_{v}.npz"), **variant_fixture(v))
     np.savez_compressed(os.path.join(HERE, "ref_cells.npz"), **cell_fixture())
     np.savez_compressed(os.path.join(HERE, "ref_repair.npz"), **repair_fixture())

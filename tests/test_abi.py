@@ -123,3 +123,29 @@ def test_bl_coord_matches_reference():
         L.hamr_bl_coord(0, 0.9375, X.ctypes.data_as(ctypes.c_void_p), a.ctypes.data_as(ctypes.c_void_p))
         R.ref_bl_coord(X.ctypes.data_as(ctypes.c_void_p), b.ctypes.data_as(ctypes.c_void_p))
         assert np.array_equal(a, b), (X, a, b)
+
+
+@pytest.mark.parametrize("variant", ["t3", "t2", "ot"])
+def test_oracle_geometry_matches_reference_bitwise(variant):
+    """The oracle's own metric tables (used to set up the CPU arm with no
+    library code) are the reference's tables bit for bit."""
+    if not O.ref_available(variant):
+        pytest.skip("reference host build not present")
+    dims, _ = O.ref_dims(variant)
+    n1, n2, n3 = (int(x) for x in dims[:3])
+    if variant == "ot":
+        startx, dx, coords, spin = [0, 0, 0, 0], [0, 1 / n1, 1 / n2, 1.0], "cartesian", 0.0
+    else:
+        spin = 0.9375
+        startx, dx = ks_grid(n1, n2, n3, spin, 40.0)
+        coords = "ks"
+    _compare_tables(O.build_geometry(coords, spin, n1, n2, n3, startx, dx), O.ref_geometry(variant, spin, startx, dx))
+
+
+@pytest.mark.parametrize("n", [(24, 16, 8), (96, 48, 32), (64, 64, 1)])
+def test_oracle_geometry_matches_library_bitwise(n):
+    n1, n2, n3 = n
+    spin = 0.9375
+    startx, dx = ks_grid(n1, n2, n3, spin, 1000.0)
+    _compare_tables(O.build_geometry("ks", spin, n1, n2, n3, startx, dx),
+                    build_geometry("ks", spin, n1, n2, n3, startx, dx))

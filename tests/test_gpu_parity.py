@@ -129,6 +129,32 @@ def test_divb_roundoff():
     blk.close()
 
 
+@pytest.mark.parametrize("case", list(CASES))
+def test_divb_matches_oracle(case):
+    """hamr_divb_max against the oracle's divb_calc restatement (diag.c:153-199,
+    with its 0.25 factor) on the same face field: the field after three
+    strict-build steps (div B at round-off, so both sides get the GPU's field
+    bit for bit), then that field with seeded noise, whose divergence is of
+    order noise / dx. Strict build: the same sums in the same order."""
+    pb = CASES[case]()
+    from oracle import oracle as O
+    blk, s = make_pair(pb, strict=True)
+    dt = 0.2 * min(pb.dx[:2])
+    for _ in range(3):
+        dt = min(blk.step(dt), 1.3 * dt)
+    p, ps = blk.download()
+    rng = np.random.default_rng(11)
+    noisy = ps * (1.0 + 1e-3 * rng.standard_normal(ps.shape))
+    for field in (ps, noisy):
+        blk.upload(p, field)
+        s.blk.arrays["ps"][:] = field
+        d_gpu = blk.divb_max()
+        d_orc = O.divb_max(s)
+        assert abs(d_gpu - d_orc) <= 1e-14 * d_orc, (d_gpu, d_orc)
+    assert d_orc > 1e-6 * np.abs(noisy).max() / max(pb.dx)
+    blk.close()
+
+
 def test_graph_advance_matches_step_loop():
     pb = problems.fm_torus(32, 16, 8, rout=40.0)
     a, _ = make_pair(pb, strict=False)

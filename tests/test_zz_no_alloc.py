@@ -5,9 +5,14 @@ buffers using only scratch arrays that live inside the library.
 
 Checked through the C ABI against the context-based step (hamr_step) on the
 same block, on two calls in a row -- the second call runs on scratch that still
-holds the first call's contents. Same kernels in the same order, so the results
-must agree to the parity tests' strict tolerance (1e-14 of each field's scale);
-they are in fact expected to be identical. Collected last on purpose.
+holds the first call's contents -- for every solver combination the entry point
+accepts (PPM and MC with two ghost layers, HLL and HLLC, Noble 2D and
+Newman-Hamlin, transmissive and reflective poles, periodic boxes), and after a
+call on a larger block with a different plane stride, so that a read of stale
+scratch in any kernel would show. Same kernels in the same order, so the
+results must agree to the parity tests' strict tolerance (1e-14 of each
+field's scale); they are in fact expected to be identical. Collected last on
+purpose.
 """
 import ctypes
 
@@ -15,18 +20,19 @@ import numpy as np
 import pytest
 
 from hamr_gamma_wind_b200 import _lib, problems
-from hamr_gamma_wind_b200.api import Block
+from hamr_gamma_wind_b200.api import INVERSION, RECON, RIEMANN, Block
 
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-14
 
 
-def _params(pb, stream):
+def _params(pb, stream, recon="ppm", riemann="hll", inversion="2d"):
     bc = {"periodic": 0, "outflow": 1, "pole_trans": 2, "pole_refl": 3}
     return _lib.HamrParams(pb.n1, pb.n2, pb.n3, pb.ng, pb.ksize, pb.gsize, pb.dx[0], pb.dx[1], pb.dx[2],
                            pb.gam, pb.cour, pb.poles[0], pb.poles[1], bc[pb.bc[0]], bc[pb.bc[1]],
-                           bc[pb.bc[2]], int(pb.ct_upwind), 0, stream)
+                           bc[pb.bc[2]], int(pb.ct_upwind), 0, stream, INVERSION[inversion], RECON[recon],
+                           RIEMANN[riemann])
 
 
 def _rel(a, b):
@@ -36,46 +42,85 @@ def _rel(a, b):
     return (np.abs(a - b).max(axis=1) / scale).max()
 
 
-@pytest.mark.parametrize("case", ["torus3d", "ot"])
-def test_noalloc_step_matches_context_step_twice(case):
-    import torch
-    pb = problems.fm_torus(24, 16, 8, rout=40.0) if case == "torus3d" else problems.orszag_tang(48)
-    assert pb.ksize <= _lib.NOALLOC_MAX_CELLS
-    L = _lib.load()
-    # reference result: the context path
-    blk = Block(**pb.block_kwargs())
+def _context_steps(pb, dt, opts):
+    """Initial state after the ghost fill, and the state and CFL step after
+    each of two hamr_step calls."""
+    blk = Block(**pb.block_kwargs(), **opts)
     blk.set_geometry(pb.geo)
     blk.upload(pb.p, pb.ps)
     blk.bound()
-    p0, ps0 = blk.download()
-    dt = 0.2 * min(pb.dx[:2])
-    dn_ctx = [blk.step(dt)]
-    ref_states = [blk.download()]
-    dn_ctx.append(blk.step(dt))
-    ref_states.append(blk.download())
+    start = blk.download()
+    out = []
+    for _ in range(2):
+        dn = blk.step(dt)
+        out.append((*blk.download(), dn))
     blk.close()
+    return start, out
 
-    # the allocation-free path on caller-owned device buffers
+
+def _noalloc_steps(pb, start, dt, opts, ncalls=2):
+    """The same steps through hamr_step_noalloc on caller-owned device buffers."""
+    import torch
+    L = _lib.load()
     dev = torch.device("cuda")
-    p_d = torch.from_numpy(p0.copy()).to(dev)
-    ps_d = torch.from_numpy(ps0.copy()).to(dev)
+    p_d = torch.from_numpy(start[0].copy()).to(dev)
+    ps_d = torch.from_numpy(start[1].copy()).to(dev)
     tabs = [torch.from_numpy(getattr(pb.geo, n).copy()).to(dev) for n in ("gcov", "gcon", "gdet", "conn")]
     stream = torch.cuda.current_stream()
-    prm = _params(pb, ctypes.c_void_p(stream.cuda_stream))
+    prm = _params(pb, ctypes.c_void_p(stream.cuda_stream), **opts)
     torch.cuda.synchronize()
-    for call in range(2):
+    out = []
+    for call in range(ncalls):
         dn = ctypes.c_double()
         rc = L.hamr_step_noalloc(ctypes.byref(prm), *[ctypes.c_void_p(t.data_ptr()) for t in tabs],
                                  ctypes.c_void_p(p_d.data_ptr()), ctypes.c_void_p(ps_d.data_ptr()), dt,
                                  ctypes.byref(dn))
         assert rc == 0, f"call {call}: rc {rc}"
         torch.cuda.synchronize()
-        p_host = p_d.cpu().numpy()
-        ps_host = ps_d.cpu().numpy()
-        pr, psr = ref_states[call]
-        assert _rel(pb.active(p_host), pb.active(pr)) <= TOL, f"call {call}: primitives differ"
-        assert _rel(pb.active(ps_host), pb.active(psr)) <= TOL, f"call {call}: face field differs"
-        assert abs(dn.value - dn_ctx[call]) <= TOL * dn_ctx[call]
+        out.append((p_d.cpu().numpy(), ps_d.cpu().numpy(), dn.value))
+    return out
+
+
+def _compare(pb, got, ref):
+    for call, ((p, ps, dn), (pr, psr, dr)) in enumerate(zip(got, ref)):
+        assert _rel(pb.active(p), pb.active(pr)) <= TOL, f"call {call}: primitives differ"
+        assert _rel(pb.active(ps), pb.active(psr)) <= TOL, f"call {call}: face field differs"
+        assert abs(dn - dr) <= TOL * dr, f"call {call}: CFL step differs"
+
+
+CASES = {
+    "torus3d": (lambda: problems.fm_torus(24, 16, 8, rout=40.0), {}),
+    "ot": (lambda: problems.orszag_tang(48), {}),
+    "torus3d_hllc": (lambda: problems.fm_torus(24, 16, 8, rout=40.0), {"riemann": "hllc"}),
+    "torus3d_mc_ng2": (lambda: problems.fm_torus(24, 16, 8, rout=40.0, ng=2), {"recon": "mc"}),
+    "torus2d_nm": (lambda: problems.fm_torus(32, 32, 1, rout=40.0), {"inversion": "nm"}),
+}
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_noalloc_step_matches_context_step_twice(case):
+    make, opts = CASES[case]
+    pb = make()
+    assert pb.ksize <= _lib.NOALLOC_MAX_CELLS
+    dt = 0.2 * min(pb.dx[:2])
+    start, ref = _context_steps(pb, dt, opts)
+    _compare(pb, _noalloc_steps(pb, start, dt, opts), ref)
+
+
+def test_noalloc_after_larger_block_with_other_layout():
+    """A large 3-D call first leaves its values all over the scratch; a smaller
+    3-D block with another plane stride (and another ksize / G3 layout) must
+    still reproduce the context step: every scratch location it reads is
+    written or cleared in its own call."""
+    big = problems.fm_torus(28, 20, 12, rout=40.0)
+    small = problems.fm_torus(16, 12, 6, rout=40.0, seed=7)
+    assert small.ksize < big.ksize <= _lib.NOALLOC_MAX_CELLS
+    dt_big = 0.2 * min(big.dx[:2])
+    start_big, _ = _context_steps(big, dt_big, {})
+    _noalloc_steps(big, start_big, dt_big, {"riemann": "hllc"}, ncalls=1)
+    dt = 0.2 * min(small.dx[:2])
+    start, ref = _context_steps(small, dt, {})
+    _compare(small, _noalloc_steps(small, start, dt, {}), ref)
 
 
 def test_noalloc_rejects_oversized_block_before_device_work():
