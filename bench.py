@@ -257,13 +257,15 @@ def _config(wl, precision, args, **extra):
             "l2": "inputs larger than L2 (no flush)", "dt_update_interval": 16, **extra}
 
 
-def _measure(pb, precision, args, stream, world):
+def _measure(pb, precision, args, stream, world, strict=False):
     """Device time of K RK2 steps of one block (after the warm-up) and the
-    per-kernel-group breakdown; returns (ms, dt, blk)."""
+    per-kernel-group breakdown; returns (ms, dt, blk). strict: the library
+    build without multiply-add contraction (the one that reproduces the
+    reference's roundings)."""
     import torch
     from hamr_gamma_wind_b200.api import Block
     blk = Block(**pb.block_kwargs(), precision=precision, stream=ctypes_stream(stream), recon=args.recon,
-                riemann=args.riemann, floors=args.floors, repair=args.repair)
+                riemann=args.riemann, floors=args.floors, repair=args.repair, strict=strict)
     blk.set_geometry(pb.geo)
     blk.upload(pb.p, pb.ps)
     blk.bound()
@@ -315,10 +317,15 @@ def run_ours(args):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     cells = pb.n1 * pb.n2 * pb.n3
-    precs = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    # fp64: the plain drop-in from the build that keeps the reference's
+    # roundings (no multiply-add contraction: matches the oracle to the last
+    # bits); fp64_fma: the same step from the contracted build; mixed: the
+    # mixed-precision step (contracted build)
+    variants = {"fp64": ("fp64", True), "fp64_fma": ("fp64", False), "mixed": ("mixed", False)}
+    precs = ["fp64", "fp64_fma", "mixed"] if args.precision == "both" else [args.precision]
     runs = {}
     for prec in precs:
-        ms, dt, blk, clocks = _measure(pb, prec, args, stream, world)
+        ms, dt, blk, clocks = _measure(pb, variants[prec][0], args, stream, world, strict=variants[prec][1])
         runs[prec] = dict(ms=ms, value=world * cells * args.steps / (ms * 1e-3), clocks=clocks)
         if args.kernels_only:
             blk.close()
@@ -397,7 +404,9 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if head == "fp64" else "f32 flux/EMF + f64 update/inversion", "data": "synthetic",
-            "config": _config(wl, head, args, parallelism=f"replicas x{world}"),
+            "config": _config(wl, head, args, parallelism=f"replicas x{world}",
+                              builds={"fp64": "libhamr_b200_strict.so (no multiply-add contraction)",
+                                      "fp64_fma": "libhamr_b200.so", "mixed": "libhamr_b200.so"}),
             "precisions": {k: {"value": v["value"], "ms_per_step": v["ms"] / args.steps,
                                "kernel_ms_per_step": v.get("kernels"),
                                **({"failures": v["failures"]} if "failures" in v else {})}
@@ -437,13 +446,14 @@ FACE_NAMES = ["face_B1", "face_B2", "face_B3"]
 
 def _accuracy_block(pb, args, stream):
     """Per-field relative L1 difference of the mixed-precision step against
-    the FP64 step after `accuracy_steps` steps of the workload from the same
-    initial state with the same step-size rule (device runs, untimed)."""
+    the FP64 step (the build without contraction, which tracks the oracle)
+    after `accuracy_steps` steps of the workload from the same initial state
+    with the same step-size rule (device runs, untimed)."""
     from hamr_gamma_wind_b200.api import Block
     nsteps = args.accuracy or 1000
     out = {}
     for prec in ("fp64", "mixed"):
-        blk = Block(**pb.block_kwargs(), precision=prec, stream=ctypes_stream(stream))
+        blk = Block(**pb.block_kwargs(), precision=prec, stream=ctypes_stream(stream), strict=prec == "fp64")
         blk.set_geometry(pb.geo)
         blk.upload(pb.p, pb.ps)
         blk.bound()
@@ -515,7 +525,7 @@ def run_ensemble(args):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     cs = ctypes_stream(stream)
-    precs = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    precs = ["fp64", "mixed"] if args.precision == "both" else [args.precision.replace("fp64_fma", "fp64")]
     runs = {}
     for prec in precs:
         blocks = []
@@ -672,7 +682,7 @@ def run_slabs(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     wl = WORKLOADS[args.workload]
-    prec = "mixed" if args.precision == "both" else args.precision
+    prec = "mixed" if args.precision == "both" else args.precision.replace("fp64_fma", "fp64")
     pb = problems.fm_torus(wl["n1"], wl["n2"], wl["n3"], rout=wl["rout"])
     cells = pb.n1 * pb.n2 * pb.n3
     stream = torch.cuda.Stream()
@@ -753,7 +763,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c3", choices=list(WORKLOADS) + ["c4", "c5"])
-    ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"])
+    ap.add_argument("--precision", default="both", choices=["fp64", "fp64_fma", "mixed", "both"])
     ap.add_argument("--fd-directions", type=int, default=None,
                     help="c5: finite-difference directions checked after the timing (default 32)")
     ap.add_argument("--recon", default="ppm", choices=["ppm", "mc"],

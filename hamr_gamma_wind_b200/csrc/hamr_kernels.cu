@@ -36,11 +36,15 @@ using namespace hamr;
 namespace {
 
 constexpr int BLK = 128;
+// CTAs of the inversion's fallback pass (a grid-stride loop over the failed
+// zones, whose count is only known on the device)
+constexpr int FALLBACK_CTAS = 148;
 
 struct Dims {
     int n1, n2, n3, ng1, ng2, ng3, G1, G2, G3, d1, d2, d3;
     long ks, gs;
     double dx1, dx2, dx3, gam, cour;
+    double rdx1, rdx2, rdx3;   // 1/dx, correctly rounded on the host (exact divisions by dx, div_rcp)
     int pole1, pole2, bc1, bc2, bc3, ct_upwind, inversion, recon, riemann;
     int halo;   // x1 sides filled by a neighbouring block (bit 0 lower, bit 1 upper)
 };
@@ -256,9 +260,64 @@ __device__ __forceinline__ void zone_edges(const Dims &d, const double *__restri
     }
 }
 
-// (x3 faces stay face by face: a warp-shuffle form that reconstructed each
-// zone once, lane l + 1 handing face l its right state, was 6 % slower in
-// FP64 and even in float on the 384 x 192 x 192 torus.)
+// x3 faces (phi, the contiguous direction) with each zone reconstructed once.
+// The zones a row of x3 faces touches, z = ng3 - 1 .. ng3 + n3 (n3 + 2 of
+// them for n3 + 1 faces), are numbered row after row as "slots"; CTA b takes
+// slots b (BLK - 1) .. b (BLK - 1) + BLK - 1, one per thread, so consecutive
+// CTAs share one slot. Phase 1: every thread reconstructs its slot's zone and
+// leaves both edges in shared memory. Phase 2: thread l evaluates the face
+// between slots l and l + 1 when both lie in the same row (left state: the
+// upper edge of slot l, right state: the lower edge of slot l + 1). Every
+// thread does the same work in each phase, so the barrier between them costs
+// little. Same values as k_flux<3> face by face: the same para on the same
+// five zones.
+__host__ __device__ __forceinline__ long n_x3_slots(const Dims &d) {
+    return (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3);
+}
+
+template <typename T, int REC>
+__global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? HAMR_FLUX_MINB : HAMR_FLUX_MINB_F)
+    k_flux_x3(const Dims d, const Geom m, const double *__restrict__ pv, const double *__restrict__ ps,
+              T *__restrict__ F, unsigned long long *__restrict__ dtbits, int calc_dt) {
+    __shared__ T slo[NPR - 1][BLK], shi[NPR - 1][BLK];   // zone edges per slot (B3 skipped)
+    const int l = threadIdx.x;
+    const long nslot = n_x3_slots(d);
+    const int rz = d.n3 + 2 * d.d3;   // slots per row
+    const int nj = d.n2 + 2 * d.d2;
+    const long sl = (long)blockIdx.x * (BLK - 1) + l;
+    const int zl = (int)(sl % rz);
+    const long row = sl / rz;
+    const int j = (d.ng2 - 1) * d.d2 + (int)(row % nj);
+    const int i = (d.ng1 - 1) * d.d1 + (int)(row / nj);
+    const long c = cix(d, i, j, d.ng3 - 1 + zl);   // the slot's zone
+    if (sl < nslot) {
+        T lo[NPR], hi[NPR];
+        zone_edges<3, T, REC>(d, pv, c, 1, lo, hi);
+#pragma unroll
+        for (int k = 0, q = 0; k < NPR; k++)
+            if (k != B3) {
+                slo[q][l] = lo[k];
+                shi[q++][l] = hi[k];
+            }
+    }
+    __syncthreads();
+    double dtf = 1.e9;
+    // the face above this slot's zone: zone c + 1 is the next slot of the row
+    if (l < BLK - 1 && sl + 1 < nslot && zl + 1 < rz) {
+        T pl[NPR], pr[NPR];
+#pragma unroll
+        for (int k = 0, q = 0; k < NPR; k++)
+            if (k != B3) {
+                pl[k] = shi[q][l];
+                pr[k] = slo[q++][l + 1];
+            }
+        Geo<T> gm;
+        load_geo_t(d, m, i, j, FACE3, gm);
+        dtf = flux_eval<3, T, REC>(d, gm, ps, pl, pr, F, c + 1, j);
+    }
+    if (calc_dt) cta_min_dt(dtf, &dtbits[3]);
+}
+
 // Faces of direction DIR (1 or 2) by rows: a thread walks FLUX_ROW
 // consecutive faces along DIR at fixed transverse indices, reconstructing
 // each zone once (its upper edge is the left state of the next face) where
@@ -690,9 +749,9 @@ __device__ __forceinline__ void cons_update(const Dims &d, const Geom &m, const 
     if constexpr (sizeof(T) == sizeof(double)) {
 #pragma unroll
         for (int k = 0; k < NPR; k++) {
-            if (d.ng1 > 0) U[k] -= Dt * (F1[k * ks + c + isize] - F1[k * ks + c]) / (d.dx1 * (double)1);
-            if (d.ng2 > 0) U[k] -= Dt * (F2[k * ks + c + d.G3] - F2[k * ks + c]) / (d.dx2 * (double)1);
-            if (d.ng3 > 0) U[k] -= Dt * (F3[k * ks + c + 1] - F3[k * ks + c]) / (d.dx3 * (double)1);
+            if (d.ng1 > 0) U[k] -= div_rcp(Dt * (F1[k * ks + c + isize] - F1[k * ks + c]), d.dx1, d.rdx1);
+            if (d.ng2 > 0) U[k] -= div_rcp(Dt * (F2[k * ks + c + d.G3] - F2[k * ks + c]), d.dx2, d.rdx2);
+            if (d.ng3 > 0) U[k] -= div_rcp(Dt * (F3[k * ks + c + 1] - F3[k * ks + c]), d.dx3, d.rdx3);
         }
         if constexpr (std::is_same<Conn, ConnTable>::value) source(d.gam, pf, gm, d, m, gi, dU, q);
         else source_c(d.gam, pf, gm, conn, dU, q);
@@ -712,9 +771,9 @@ __device__ __forceinline__ void cons_update(const Dims &d, const Geom &m, const 
                 comp += fabs(sum) >= fabs(x) ? (sum - tt) + x : (x - tt) + sum;
                 sum = tt;
             };
-            if (d.ng1 > 0) add(-Dt * ((double)F1[k * ks + c + isize] - (double)F1[k * ks + c]) / d.dx1);
-            if (d.ng2 > 0) add(-Dt * ((double)F2[k * ks + c + d.G3] - (double)F2[k * ks + c]) / d.dx2);
-            if (d.ng3 > 0) add(-Dt * ((double)F3[k * ks + c + 1] - (double)F3[k * ks + c]) / d.dx3);
+            if (d.ng1 > 0) add(div_rcp(-Dt * ((double)F1[k * ks + c + isize] - (double)F1[k * ks + c]), d.dx1, d.rdx1));
+            if (d.ng2 > 0) add(div_rcp(-Dt * ((double)F2[k * ks + c + d.G3] - (double)F2[k * ks + c]), d.dx2, d.rdx2));
+            if (d.ng3 > 0) add(div_rcp(-Dt * ((double)F3[k * ks + c + 1] - (double)F3[k * ks + c]), d.dx3, d.rdx3));
             add(Dt * dU[k]);
             U[k] = sum + comp;
         }
@@ -742,34 +801,37 @@ __device__ __forceinline__ void face_average_b(const Dims &d, const Geom &m, con
 // the zone's own flag and primitives.
 enum { FIX_FLOORS = 1, FIX_RESET = 2 };
 
-// Primary inversion with the 1dvsq2fix1 and 1dfix1 fallbacks, recording the
-// outcome in pflag and the failure counters (fixup, GPU_fixup.h:346-382)
-template <int INV, int FIX = 0>
-__device__ __forceinline__ void invert_zone(const Dims &d, const Geo<double> &gm, long c, double *U, double *pf,
-                                            double *__restrict__ pout, int *__restrict__ pflag,
-                                            int *__restrict__ failimage) {
+// The entropy fallbacks 1dvsq2fix1 then 1dfix1 of a zone whose primary
+// solver failed, counting each failure (fixup, GPU_fixup.h:360-382); returns
+// the final flag. Works on copies so that the caller's U and pf can stay in
+// registers.
+__device__ __forceinline__ int invert_fallbacks(const Dims &d, const Geo<double> &gm, long c, const double *U,
+                                                double *pf, int *__restrict__ failimage) {
     const long ks = d.ks;
-    // primary solver: Noble 2D, or Newman-Hamlin in its place (NEWMAN builds)
-    int flag = INV == HAMR_INV_NM ? utoprim_nm(d.gam, U, gm.gcov, gm.gcon, gm.g, pf)
-                                  : utoprim_2d(d.gam, U, gm.gcov, gm.gcon, gm.g, pf);
+    double Uc[NPR], pc[NPR], gcv[10], gcn[10];
+#pragma unroll
+    for (int k = 0; k < NPR; k++) { Uc[k] = U[k]; pc[k] = pf[k]; }
+#pragma unroll
+    for (int k = 0; k < 10; k++) { gcv[k] = gm.gcov[k]; gcn[k] = gm.gcon[k]; }
+    failimage[c]++;
+    int flag = utoprim_1dvsq2fix1(d.gam, Uc, gcv, gcn, gm.g, pc);
     if (flag) {
-        // rare path: the fallbacks work on copies so that U and pf can stay
-        // in registers on the common path
-        double Uc[NPR], pc[NPR], gcv[10], gcn[10];
-#pragma unroll
-        for (int k = 0; k < NPR; k++) { Uc[k] = U[k]; pc[k] = pf[k]; }
-#pragma unroll
-        for (int k = 0; k < 10; k++) { gcv[k] = gm.gcov[k]; gcn[k] = gm.gcon[k]; }
-        failimage[c]++;
-        flag = utoprim_1dvsq2fix1(d.gam, Uc, gcv, gcn, gm.g, pc);
-        if (flag) {
-            failimage[1 * ks + c]++;
-            flag = utoprim_1dfix1(d.gam, Uc, gcv, gcn, gm.g, pc);
-            if (flag) failimage[2 * ks + c]++;
-        }
-#pragma unroll
-        for (int k = 0; k < NPR; k++) pf[k] = pc[k];
+        failimage[1 * ks + c]++;
+        flag = utoprim_1dfix1(d.gam, Uc, gcv, gcn, gm.g, pc);
+        if (flag) failimage[2 * ks + c]++;
     }
+#pragma unroll
+    for (int k = 0; k < NPR; k++) pf[k] = pc[k];
+    return flag;
+}
+
+// The opt-in floors and reset after the inversion chain, then the zone's
+// flag and primitives written out.
+template <int FIX>
+__device__ __forceinline__ void invert_epilogue(const Dims &d, const Geo<double> &gm, long c, int flag, double *pf,
+                                                double *__restrict__ pout, int *__restrict__ pflag,
+                                                int *__restrict__ failimage) {
+    const long ks = d.ks;
     if constexpr ((FIX & FIX_FLOORS) != 0) {
         if (floor_may_apply(pf, gm) && floor_zone(d.gam, pf, gm)) {
             flag = -333;
@@ -789,6 +851,25 @@ __device__ __forceinline__ void invert_zone(const Dims &d, const Geo<double> &gm
     pflag[c] = flag;
 #pragma unroll
     for (int k = 0; k < NPR; k++) pout[k * ks + c] = pf[k];
+}
+
+// primary solver: Noble 2D, or Newman-Hamlin in its place (NEWMAN builds)
+template <int INV>
+__device__ __forceinline__ int invert_primary(const Dims &d, const Geo<double> &gm, const double *U, double *pf) {
+    return INV == HAMR_INV_NM ? utoprim_nm(d.gam, U, gm.gcov, gm.gcon, gm.g, pf)
+                              : utoprim_2d(d.gam, U, gm.gcov, gm.gcon, gm.g, pf);
+}
+
+// Primary inversion with the 1dvsq2fix1 and 1dfix1 fallbacks, recording the
+// outcome in pflag and the failure counters (fixup, GPU_fixup.h:346-382),
+// all in one pass (the batched inversion's per-item body)
+template <int INV, int FIX = 0>
+__device__ __forceinline__ void invert_zone(const Dims &d, const Geo<double> &gm, long c, double *U, double *pf,
+                                            double *__restrict__ pout, int *__restrict__ pflag,
+                                            int *__restrict__ failimage) {
+    int flag = invert_primary<INV>(d, gm, U, pf);
+    if (flag) flag = invert_fallbacks(d, gm, c, U, pf, failimage);
+    invert_epilogue<FIX>(d, gm, c, flag, pf, pout, pflag, failimage);
 }
 
 // build option: minimum resident blocks of 128 threads per SM for the
@@ -837,8 +918,9 @@ __global__ void __launch_bounds__(BLK, HAMR_CONS_MINB) k_cons(const Dims d, cons
                                                const double *__restrict__ pb, double *__restrict__ Ucache,
                                                const T *__restrict__ F1, const T *__restrict__ F2,
                                                const T *__restrict__ F3, double *__restrict__ W, int full,
-                                               StepSize st) {
+                                               StepSize st, int *__restrict__ nfail) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0) *nfail = 0;   // the inversion's failed-zone list starts empty
     if (t >= (long)d.n1 * d.n2 * d.n3) return;
     k_cons_at(d, m, pin, pb, Ucache, F1, F2, F3, W, full, st, t);
 }
@@ -853,8 +935,10 @@ __global__ void __launch_bounds__(BLK, HAMR_CONS_MINB) k_cons_cols(const Dims d,
                                                const double *__restrict__ pin, const double *__restrict__ pb,
                                                double *__restrict__ Ucache, const T *__restrict__ F1,
                                                const T *__restrict__ F2, const T *__restrict__ F3,
-                                               double *__restrict__ W, int full, StepSize st) {
+                                               double *__restrict__ W, int full, StepSize st,
+                                               int *__restrict__ nfail) {
     __shared__ double sg[3][COL_VALS];
+    if (blockIdx.x == 0 && threadIdx.x == 0) *nfail = 0;   // the inversion's failed-zone list starts empty
     const long nzone = (long)d.n1 * d.n2 * d.n3;
     const long t0 = (long)blockIdx.x * blockDim.x;
     const long tl = (t0 + blockDim.x < nzone ? t0 + blockDim.x : nzone) - 1;
@@ -894,6 +978,23 @@ __global__ void __launch_bounds__(BLK, HAMR_CONS_MINB) k_cons_cols(const Dims d,
     W[6 * d.ks + c] = U[B3];
 }
 
+// the inversion's inputs of one zone: the stage's primitives as the initial
+// guess, the updated conserved variables, U[B] from the faces
+__device__ __forceinline__ void invert_inputs(const Dims &d, const Geom &m, const double *__restrict__ pg,
+                                              const double *__restrict__ W, const double *__restrict__ psf,
+                                              int i, int j, long c, long gi, double *pf, double *U) {
+#pragma unroll
+    for (int k = 0; k < NPR; k++) pf[k] = pg[k * d.ks + c];
+    U[RHO] = W[0 * d.ks + c];
+    U[UU] = W[1 * d.ks + c];
+    U[U1] = W[2 * d.ks + c];
+    U[U2] = W[3 * d.ks + c];
+    U[U3] = W[4 * d.ks + c];
+    U[KTOT] = W[5 * d.ks + c];
+    U[B3] = W[6 * d.ks + c];
+    face_average_b(d, m, psf, i, j, c, gi, U);
+}
+
 template <int INV, int FIX = 0>
 __device__ __forceinline__ void k_invert_at(const Dims &d, const Geom &m, const double *__restrict__ pg,
                                                  const double *__restrict__ W, const double *__restrict__ psf,
@@ -906,27 +1007,65 @@ __device__ __forceinline__ void k_invert_at(const Dims &d, const Geom &m, const 
     Geo<double> gm;
     load_geo(d, m, i, j, CENT, gm);
     double pf[NPR], U[NPR];
-#pragma unroll
-    for (int k = 0; k < NPR; k++) pf[k] = pg[k * d.ks + c];
-    U[RHO] = W[0 * d.ks + c];
-    U[UU] = W[1 * d.ks + c];
-    U[U1] = W[2 * d.ks + c];
-    U[U2] = W[3 * d.ks + c];
-    U[U3] = W[4 * d.ks + c];
-    U[KTOT] = W[5 * d.ks + c];
-    U[B3] = W[6 * d.ks + c];
-    face_average_b(d, m, psf, i, j, c, gi, U);
+    invert_inputs(d, m, pg, W, psf, i, j, c, gi, pf, U);
     invert_zone<INV, FIX>(d, gm, c, U, pf, pout, pflag, failimage);
 }
 
+// The single-block inversion in two passes, so that the common path carries
+// none of the fallbacks' state: k_invert_primary runs the primary solver
+// and, for the zones it solves, the epilogue; a zone it fails goes to a list
+// (its active-zone index) and is finished by k_invert_fallback, which
+// rebuilds the zone's U from the same inputs, restores what the failed
+// primary solver left in pf (U[B]/gdet, written by its prologue unless
+// U[RHO] <= 0) and runs the fallback chain and the epilogue. Same results
+// as the one-pass invert_zone; *nfail must be zero on entry (the conserved
+// update clears it).
 template <int INV, int FIX = 0>
-__global__ void __launch_bounds__(BLK, HAMR_UPD_MINB) k_invert(const Dims d, const Geom m, const double *__restrict__ pg,
-                                                 const double *__restrict__ W, const double *__restrict__ psf,
-                                                 double *__restrict__ pout, int *__restrict__ pflag,
-                                                 int *__restrict__ failimage) {
+__global__ void __launch_bounds__(BLK, HAMR_UPD_MINB)
+    k_invert_primary(const Dims d, const Geom m, const double *__restrict__ pg, const double *__restrict__ W,
+                     const double *__restrict__ psf, double *__restrict__ pout, int *__restrict__ pflag,
+                     int *__restrict__ failimage, int *__restrict__ flist, int *__restrict__ nfail) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)d.n1 * d.n2 * d.n3) return;
-    k_invert_at<INV, FIX>(d, m, pg, W, psf, pout, pflag, failimage, t);
+    const int z = d.ng3 + (int)(t % d.n3);
+    const int j = d.ng2 + (int)((t / d.n3) % d.n2);
+    const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
+    const long c = cix(d, i, j, z), gi = gix(d, i, j);
+    Geo<double> gm;
+    load_geo(d, m, i, j, CENT, gm);
+    double pf[NPR], U[NPR];
+    invert_inputs(d, m, pg, W, psf, i, j, c, gi, pf, U);
+    const int flag = invert_primary<INV>(d, gm, U, pf);
+    if (flag) {
+        flist[atomicAdd(nfail, 1)] = (int)t;
+        return;
+    }
+    invert_epilogue<FIX>(d, gm, c, flag, pf, pout, pflag, failimage);
+}
+
+template <int INV, int FIX = 0>
+__global__ void __launch_bounds__(BLK)
+    k_invert_fallback(const Dims d, const Geom m, const double *__restrict__ pg, const double *__restrict__ W,
+                      const double *__restrict__ psf, double *__restrict__ pout, int *__restrict__ pflag,
+                      int *__restrict__ failimage, const int *__restrict__ flist, const int *__restrict__ nfail) {
+    const int n = *nfail;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const long t = flist[q];
+        const int z = d.ng3 + (int)(t % d.n3);
+        const int j = d.ng2 + (int)((t / d.n3) % d.n2);
+        const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
+        const long c = cix(d, i, j, z), gi = gix(d, i, j);
+        Geo<double> gm;
+        load_geo(d, m, i, j, CENT, gm);
+        double pf[NPR], U[NPR];
+        invert_inputs(d, m, pg, W, psf, i, j, c, gi, pf, U);
+        if (!(U[RHO] <= 0.)) {
+#pragma unroll
+            for (int k = B1; k <= B3; k++) pf[k] = U[k] / gm.g;   // the primary solver's prologue
+        }
+        const int flag = invert_fallbacks(d, gm, c, U, pf, failimage);
+        invert_epilogue<FIX>(d, gm, c, flag, pf, pout, pflag, failimage);
+    }
 }
 
 // ------------------------------------------------ neighbour repair (opt-in)
@@ -1319,6 +1458,7 @@ struct hamr_ctx {
     int *counter = nullptr;
     unsigned long long *divb = nullptr;
     int *rlist = nullptr, *rcount = nullptr;   // neighbour repair: listed zones and their count
+    int *flist = nullptr, *nfail = nullptr;    // zones the primary inversion failed, and their count
     // captured advance graphs
     cudaGraphExec_t graph = nullptr;
     int graph_steps = -1, graph_interval = -1;
@@ -1381,7 +1521,19 @@ void launch_flux(long n, cudaStream_t s, const Dims &d, const Geom &m, const dou
     // x1 and x2 faces by rows, each zone reconstructed once, where the rows
     // still fill the device several times over; small blocks (2-D, ensemble
     // members) keep one thread per face
-    if (DIR != 3 && n_flux_rows<DIR == 3 ? 1 : DIR>(d) >= rows_min) {
+    if (DIR == 3) {   // each zone reconstructed once, edges through shared memory
+        const long nb = (n_x3_slots(d) - 1 + BLK - 2) / (BLK - 1);
+        switch (rec_key(d)) {
+        case 1: k_flux_x3<T, 1><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+        case 2: k_flux_x3<T, 2><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+        case 3: k_flux_x3<T, 3><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+        case 6: k_flux_x3<T, 6><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+        case 7: k_flux_x3<T, 7><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+        default: k_flux_x3<T, 0><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+        }
+        return;
+    }
+    if (n_flux_rows<DIR == 3 ? 1 : DIR>(d) >= rows_min) {
         constexpr int RD = DIR == 3 ? 1 : DIR;
         const long nr = n_flux_rows<RD>(d);
         switch (rec_key(d)) {
@@ -1457,22 +1609,39 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
         long n = (long)d.n1 * d.n2 * d.n3;
         if (d.n3 >= 64 && ctx->cons_cols)   // metric and connection staged per CTA
             k_cons_cols<T><<<nblk(n), BLK, 0, s>>>(d, m, ctx->p, full ? ctx->ph : ctx->p, ctx->U, F1, F2, F3, ctx->W,
-                                                   full, st);
+                                                   full, st, ctx->nfail);
         else
             k_cons<T><<<nblk(n), BLK, 0, s>>>(d, m, ctx->p, full ? ctx->ph : ctx->p, ctx->U, F1, F2, F3, ctx->W, full,
-                                              st);
+                                              st, ctx->nfail);
         prof_mark(pf, PROF_UPDATE, s);
         // (the inversion gained nothing from the same staging: FP64 Newton work
         // bounds it, not its 26 metric loads per zone)
         const int fix = (ctx->prm.floors ? FIX_FLOORS : 0) | (ctx->prm.repair == 1 ? FIX_RESET : 0);
-        using InvK = void (*)(const Dims, const Geom, const double *, const double *, const double *, double *,
-                              int *, int *);
-        static const InvK inv_k[2][4] = {
-            {k_invert<HAMR_INV_2D, 0>, k_invert<HAMR_INV_2D, 1>, k_invert<HAMR_INV_2D, 2>, k_invert<HAMR_INV_2D, 3>},
-            {k_invert<HAMR_INV_NM, 0>, k_invert<HAMR_INV_NM, 1>, k_invert<HAMR_INV_NM, 2>, k_invert<HAMR_INV_NM, 3>}};
+        // primary solver over every zone, then the fallback chain over the
+        // zones it failed (usually none: the second launch reads the count
+        // and returns)
+        using InvP = void (*)(const Dims, const Geom, const double *, const double *, const double *, double *,
+                              int *, int *, int *, int *);
+        using InvF = void (*)(const Dims, const Geom, const double *, const double *, const double *, double *,
+                              int *, int *, const int *, const int *);
+        static const InvP inv_p[2][4] = {
+            {k_invert_primary<HAMR_INV_2D, 0>, k_invert_primary<HAMR_INV_2D, 1>, k_invert_primary<HAMR_INV_2D, 2>,
+             k_invert_primary<HAMR_INV_2D, 3>},
+            {k_invert_primary<HAMR_INV_NM, 0>, k_invert_primary<HAMR_INV_NM, 1>, k_invert_primary<HAMR_INV_NM, 2>,
+             k_invert_primary<HAMR_INV_NM, 3>}};
+        static const InvF inv_f[2][4] = {
+            {k_invert_fallback<HAMR_INV_2D, 0>, k_invert_fallback<HAMR_INV_2D, 1>, k_invert_fallback<HAMR_INV_2D, 2>,
+             k_invert_fallback<HAMR_INV_2D, 3>},
+            {k_invert_fallback<HAMR_INV_NM, 0>, k_invert_fallback<HAMR_INV_NM, 1>, k_invert_fallback<HAMR_INV_NM, 2>,
+             k_invert_fallback<HAMR_INV_NM, 3>}};
         double *pout = full ? ctx->p : ctx->ph;
-        inv_k[d.inversion == HAMR_INV_NM][fix]<<<nblk(n), BLK, 0, s>>>(
-            d, m, full ? ctx->ph : ctx->p, ctx->W, full ? ctx->ps : ctx->psh, pout, ctx->pflag, ctx->failimage);
+        const double *pg = full ? ctx->ph : ctx->p;
+        const double *psf = full ? ctx->ps : ctx->psh;
+        const int nm = d.inversion == HAMR_INV_NM;
+        inv_p[nm][fix]<<<nblk(n), BLK, 0, s>>>(d, m, pg, ctx->W, psf, pout, ctx->pflag, ctx->failimage, ctx->flist,
+                                               ctx->nfail);
+        inv_f[nm][fix]<<<FALLBACK_CTAS, BLK, 0, s>>>(d, m, pg, ctx->W, psf, pout, ctx->pflag, ctx->failimage,
+                                                     ctx->flist, ctx->nfail);
         if (ctx->prm.repair == 2) {
             k_repair_scan<<<nblk((long)d.G1 * d.G2 * d.G3), BLK, 0, s>>>(d, pout, ctx->pflag, ctx->failimage,
                                                                          ctx->rlist, ctx->rcount);
@@ -1537,6 +1706,7 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
     d.gs = prm->gsize ? prm->gsize : ngeo + (64 - ngeo % 64);
     if (d.ks < ncell || d.gs < ngeo) { delete ctx; return HAMR_E_ARG; }
     d.dx1 = prm->dx1; d.dx2 = prm->dx2; d.dx3 = prm->dx3;
+    d.rdx1 = 1.0 / d.dx1; d.rdx2 = 1.0 / d.dx2; d.rdx3 = 1.0 / d.dx3;
     d.gam = prm->gam; d.cour = prm->cour;
     d.pole1 = prm->pole1; d.pole2 = prm->pole2;
     d.bc1 = prm->bc1; d.bc2 = prm->bc2; d.bc3 = prm->bc3;
@@ -1577,7 +1747,8 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
         {(void **)&ctx->dt_state, sizeof(double)}, {(void **)&ctx->counter, sizeof(int)},
         {(void **)&ctx->divb, sizeof(unsigned long long)},
         {(void **)&ctx->rlist, prm->repair == 2 ? sizeof(int) * d.n1 * d.n2 * d.n3 : 0},
-        {(void **)&ctx->rcount, prm->repair == 2 ? sizeof(int) : 0}};
+        {(void **)&ctx->rcount, prm->repair == 2 ? sizeof(int) : 0},
+        {(void **)&ctx->flist, sizeof(int) * d.n1 * d.n2 * d.n3}, {(void **)&ctx->nfail, sizeof(int)}};
     if (prm->repair == 2 && d.ks > 0x7fffffffL) { hamr_ctx_destroy(ctx); return HAMR_E_ARG; }
     for (auto &a : allocs) {
         if (a.n == 0) continue;
@@ -1602,7 +1773,8 @@ int hamr_ctx_destroy(hamr_ctx *ctx) {
     if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
     void *bufs[] = {ctx->p, ctx->ph, ctx->ps, ctx->psh, ctx->U, ctx->F1, ctx->F2, ctx->F3, ctx->Ec, ctx->emf,
                     ctx->W, ctx->pflag, ctx->failimage, ctx->gcov, ctx->gcon, ctx->gdet, ctx->conn, ctx->dtbits,
-                    ctx->ndt, ctx->dt_state, ctx->counter, ctx->divb, ctx->rlist, ctx->rcount};
+                    ctx->ndt, ctx->dt_state, ctx->counter, ctx->divb, ctx->rlist, ctx->rcount,
+                    ctx->flist, ctx->nfail};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1838,11 +2010,12 @@ int hamr_divb_max(hamr_ctx *ctx, double *out) {
 namespace {
 
 constexpr long NA_DPLANES = 9 + 3 + 9 + 27 + 4 + 4 + 7;  // ph, psh, U, F1-F3, E_cent, emf, W
-constexpr long NA_IPLANES = 1 + 4;                   // pflag, failimage
+constexpr long NA_IPLANES = 1 + 4 + 1;               // pflag, failimage, failed-zone list
 static __device__ __align__(256) double na_scratch[NA_DPLANES * HAMR_NOALLOC_MAX_CELLS];
 static __device__ __align__(256) int na_iscratch[NA_IPLANES * HAMR_NOALLOC_MAX_CELLS];
 static __device__ __align__(256) unsigned long long na_dtbits[4];
 static __device__ __align__(256) double na_ndt[1];
+static __device__ __align__(256) int na_nfail[1];
 
 constexpr int NA_MAX_DEVICES = 64;
 struct NaPtrs {
@@ -1850,6 +2023,7 @@ struct NaPtrs {
     int *iscratch = nullptr;
     unsigned long long *dtbits = nullptr;
     double *ndt = nullptr;
+    int *nfail = nullptr;
 };
 NaPtrs na_ptrs[NA_MAX_DEVICES];
 // set (release) after na_ptrs[dev] is written; a reader that sees it set
@@ -1867,6 +2041,7 @@ int na_setup(int dev) {
     if (cudaGetSymbolAddress((void **)&q.iscratch, na_iscratch) != cudaSuccess) return HAMR_E_CUDA;
     if (cudaGetSymbolAddress((void **)&q.dtbits, na_dtbits) != cudaSuccess) return HAMR_E_CUDA;
     if (cudaGetSymbolAddress((void **)&q.ndt, na_ndt) != cudaSuccess) return HAMR_E_CUDA;
+    if (cudaGetSymbolAddress((void **)&q.nfail, na_nfail) != cudaSuccess) return HAMR_E_CUDA;
     na_ptrs[dev] = q;
     na_ready[dev].store(true, std::memory_order_release);
     return HAMR_OK;
@@ -1902,6 +2077,7 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
     if (d.ks < ncell || d.gs < ngeo) return HAMR_E_ARG;
     if (d.ks > HAMR_NOALLOC_MAX_CELLS) return HAMR_E_ARG;   // beyond the static scratch
     d.dx1 = prm->dx1; d.dx2 = prm->dx2; d.dx3 = prm->dx3;
+    d.rdx1 = 1.0 / d.dx1; d.rdx2 = 1.0 / d.dx2; d.rdx3 = 1.0 / d.dx3;
     d.gam = prm->gam; d.cour = prm->cour;
     d.pole1 = prm->pole1; d.pole2 = prm->pole2;
     d.bc1 = prm->bc1; d.bc2 = prm->bc2; d.bc3 = prm->bc3;
@@ -1930,6 +2106,8 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
     c.W = c.emf + 4 * ks;
     c.pflag = q.iscratch;
     c.failimage = q.iscratch + ks;
+    c.flist = q.iscratch + 5 * ks;   // cleared per sub-step by the conserved update
+    c.nfail = q.nfail;
     c.gcov = const_cast<double *>(gcov);
     c.gcon = const_cast<double *>(gcon);
     c.gdet = const_cast<double *>(gdet);

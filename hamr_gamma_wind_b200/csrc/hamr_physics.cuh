@@ -68,6 +68,25 @@ template <> __device__ __forceinline__ double d_rsqrt<double>(double x) {
     return fma(0.5 * y, r, y);
 }
 template <> __device__ __forceinline__ float d_rsqrt<float>(float x) { return powf(x, -0.5f); }
+// a / b correctly rounded, given rb = RN(1/b) (b a per-launch constant whose
+// reciprocal the host rounds once): q0 = RN(a rb), the residual r = a - b q0
+// exactly by one fused multiply-add, then RN(q0 + r rb). This is the final
+// correction step of Newton-Raphson division (P. Markstein, IBM J. Res. Dev.
+// 34 (1990) 111-119): with rb within half an ulp of 1/b and q0 within an ulp
+// of a/b it yields the correctly rounded quotient, barring overflow and
+// underflow of the residual: for b a zone width (2^-100 < b < 2^100) the
+// quotient is the IEEE one bit for bit whenever 2^-900 <= |a| <= 2^900, and
+// for a = +-0 (a zero residual leaves q0, which keeps the sign of a). The
+// step's dividends -- a step size times a difference of fluxes -- are zero
+// or far inside that range (below it, where the residual turns subnormal,
+// the quotient can be one ulp off). Three operations per use instead of a
+// full division with its special-case branch.
+__device__ __forceinline__ double div_rcp(double a, double b, double rb) {
+    const double q0 = a * rb;
+    const double r = fma(-q0, b, a);
+    return r == 0.0 ? q0 : fma(r, rb, q0);
+}
+
 template <typename T> __device__ __forceinline__ T d_max(T a, T b) { return a > b ? a : b; }
 template <typename T> __device__ __forceinline__ T d_min(T a, T b) { return a < b ? a : b; }
 

@@ -109,5 +109,7 @@ int ho_build_geometry(int coords, double spin, int n1, int n2, int n3, int ng, l
 int ho_bl_coord(int coords, double spin, const double *X, double *rthph);
 /* OpenMP threads a parallel loop of the oracle uses (1 without OpenMP) */
 int ho_num_threads(void);
+/* bit-level check of the library's division by a reciprocal (div_rcp) */
+long ho_div_rcp_mismatches(const double *a, long n, const double *b, long m);
 
 #endif

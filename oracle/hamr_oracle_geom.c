@@ -356,3 +356,24 @@ int ho_num_threads(void) { return omp_get_max_threads(); }
 #else
 int ho_num_threads(void) { return 1; }
 #endif
+
+/* Check of the exact-division method the CUDA library uses for divisions by
+ * the constant zone widths (div_rcp): q0 = a*rb, r = fma(-q0, b, a),
+ * q = r == 0 ? q0 : fma(r, rb, q0) with rb = 1/b correctly rounded. Returns how
+ * many of the n*m quotients a[i]/b[j] it does not reproduce bit for bit
+ * (compared as bit patterns; both sides are IEEE binary64 round-to-nearest). */
+long ho_div_rcp_mismatches(const double *a, long n, const double *b, long m) {
+    long bad = 0;
+#pragma omp parallel for reduction(+ : bad) schedule(static)
+    for (long j = 0; j < m; j++) {
+        const double rb = 1.0 / b[j];
+        for (long i = 0; i < n; i++) {
+            const double q0 = a[i] * rb;
+            const double r = fma(-q0, b[j], a[i]);
+            const double q = r == 0.0 ? q0 : fma(r, rb, q0);
+            const double e = a[i] / b[j];
+            if (memcmp(&q, &e, sizeof(double)) != 0) bad++;
+        }
+    }
+    return bad;
+}

@@ -2,7 +2,11 @@
 
 ctypes bindings for
   * ``liboracle.so``        the C restatement of the single-block RK2 sub-step
-                            (oracle/hamr_oracle.c), and
+                            (oracle/hamr_oracle.c),
+  * ``liboracle_fma.so``    the same sources compiled with fused multiply-add
+                            contraction (selected inside ``contracted()``): how
+                            far the step moves when its roundings change, the
+                            envelope a contracted GPU build is held to, and
   * ``_ref/libref_<v>.so``  host builds of the reference's own kernels for the
                             compile-time variants listed in oracle/Makefile
                             (only present where the reference sources were).
@@ -12,6 +16,7 @@ use this module.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import os
 from dataclasses import dataclass, field
@@ -51,16 +56,29 @@ class HoState(ctypes.Structure):
                                    "E_cent", "emf", "pflag", "failimage")]
 
 
-_lib = None
+_libs: dict = {}
+_variant = "liboracle.so"
+
+
+@contextlib.contextmanager
+def contracted():
+    """Inside the block every oracle call runs the build with fused
+    multiply-add contraction (liboracle_fma.so)."""
+    global _variant
+    old, _variant = _variant, "liboracle_fma.so"
+    try:
+        yield
+    finally:
+        _variant = old
 
 
 def lib():
     """The restatement library (built by ``make -C oracle``)."""
-    global _lib
-    if _lib is None:
-        path = os.path.join(HERE, "liboracle.so")
+    name = _variant
+    if name not in _libs:
+        path = os.path.join(HERE, name)
         if not os.path.exists(path):
-            raise RuntimeError("oracle/liboracle.so missing: run `make -C oracle`")
+            raise RuntimeError(f"oracle/{name} missing: run `make -C oracle`")
         L = ctypes.CDLL(path)
         L.ho_stage.argtypes = [ctypes.POINTER(HoGrid), ctypes.POINTER(HoGeom), ctypes.POINTER(HoState),
                                _i, _d, _d, _i, _vp]
@@ -83,8 +101,10 @@ def lib():
         L.ho_build_geometry.restype = _i
         L.ho_bl_coord.argtypes = [_i, _d, _vp, _vp]
         L.ho_num_threads.restype = _i
-        _lib = L
-    return _lib
+        L.ho_div_rcp_mismatches.argtypes = [_vp, ctypes.c_long, _vp, ctypes.c_long]
+        L.ho_div_rcp_mismatches.restype = ctypes.c_long
+        _libs[name] = L
+    return _libs[name]
 
 
 def ref_available(variant: str) -> bool:
