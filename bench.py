@@ -15,7 +15,10 @@ timed with CUDA events on the stream the kernels run on, after W warm-up
 steps, max over ranks. N > 1 runs independent replicas (one block per GPU,
 no exchange): scaling "weak".
 
-The default line also carries, untimed: `accuracy` -- per-field relative L1
+The default line also carries, untimed: `adjoint` -- the adjoint workload
+(2-D torus 256 x 256, 200 steps): gradient over forward time, and the
+gradient checked against the FP64 tangent-linear oracle and central
+differences; `accuracy` -- per-field relative L1
 of the mixed step against the FP64 step after 1000 steps of the workload, and
 one FP64 step (production and strict builds) against the oracle's first step
 over every zone; `cpu_baseline` -- the oracle (the reference's step restated
@@ -389,6 +392,10 @@ def run_ours(args):
     accuracy = None
     if not args.no_accuracy and rank == 0:
         accuracy = _accuracy_block(pb, args, stream)
+    adjoint = None
+    if not args.no_adjoint and rank == 0:
+        adjoint = _adjoint_block(args, fd_directions=8, tlm_directions=7)
+        torch.cuda.set_stream(stream)
     cb = None
     if rank == 0:
         try:
@@ -425,6 +432,8 @@ def run_ours(args):
             out["mixed_over_fp64"] = runs["mixed"]["value"] / runs["fp64"]["value"]
         if accuracy is not None:
             out["accuracy"] = accuracy
+        if adjoint is not None:
+            out["adjoint"] = adjoint
         out["cpu_baseline"] = cb
         print(json.dumps(out), flush=True)
     if world > 1:
@@ -579,39 +588,35 @@ def run_ensemble(args):
     print(json.dumps(out), flush=True)
 
 
-ADJOINT = dict(n=256, nsteps=200, every=20, directions=32, spin=0.9375, rout=40.0, generic=1e-3)
+ADJOINT = dict(n=256, nsteps=200, every=20, directions=32, spin=0.9375, rout=40.0, generic=1e-3, radius=12.0)
 
 
-def run_adjoint(args):
-    """Adjoint workload: 2-D magnetised torus 256 x 256 (a = 0.9375,
-    beta_min = 100, seeded tie-free perturbations), J = accretion rate through
-    the horizon face column integrated over 200 fixed-size steps; gradient
-    w.r.t. the initial pressure field and gamma by hamr_adjoint_run
-    (checkpoint every 20 steps, recompute), timed against the forward sweep
-    (hamr_mdot_forward), and checked against central differences (relative
-    step 1e-8) on 32 seeded directions."""
+def _adjoint_block(args, fd_directions, tlm_directions):
+    """The adjoint workload: 2-D magnetised torus 256 x 256 (a = 0.9375,
+    beta_min = 100, seeded tie-free perturbations), J = sum_n dt Mdot_n, the
+    mass inflow through the sphere at the torus's pressure maximum r = 12
+    integrated over 200 fixed-size steps; gradient w.r.t. the initial
+    internal-energy field and gamma by hamr_adjoint_run (checkpoint every 20
+    steps, recompute), timed against the forward sweep (hamr_mdot_forward),
+    both on the build without contraction. Checked against the FP64
+    tangent-linear oracle (the reference step on dual numbers, on the host)
+    along `tlm_directions` seeded directions and gamma, and against central
+    differences (relative step 1e-8) along `fd_directions`."""
     import torch
-    from hamr_gamma_wind_b200 import problems
     from hamr_gamma_wind_b200.api import Adjoint, Block
-    rank, world, local = _dist()
-    torch.cuda.set_device(local)
-    if rank != 0:
-        return
+    from tests._adjoint import TorusRun, tangent_errors
     A = ADJOINT
-    pb = problems.fm_torus(A["n"], A["n"], 1, spin=A["spin"], rout=A["rout"], generic=A["generic"])
-    rh = 1.0 + np.sqrt(1.0 - A["spin"] ** 2)
-    faces = np.arange(pb.ng + 1, pb.ng + pb.n1)
-    r = np.exp(np.log(0.9 * rh) + (faces - pb.ng) * pb.dx[0])
-    ih = int(faces[np.argmin(np.abs(r - rh))])
-    dts = np.full(A["nsteps"], 0.2 * min(pb.dx[:2]))
+    run = TorusRun(A["n"], A["n"], nsteps=A["nsteps"], every=A["every"], spin=A["spin"], rout=A["rout"],
+                   strict=True, generic=A["generic"], radius=A["radius"])
+    pb, dts = run.pb, run.dts
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    blk = Block(**pb.block_kwargs(), stream=ctypes_stream(stream))
+    blk = Block(**pb.block_kwargs(), stream=ctypes_stream(stream), strict=True)
     blk.set_geometry(pb.geo)
-    adj = Adjoint(blk, ih)
+    adj = Adjoint(blk, run.ih)
 
-    def reset(u=None, p=None):
-        q = pb.p.copy() if p is None else p
+    def reset(u=None):
+        q = pb.p.copy()
         if u is not None:
             pb.active(q)[1][:, :, 0] = u
         blk.upload(q, pb.ps)
@@ -628,10 +633,8 @@ def run_adjoint(args):
     reset()
     torch.cuda.synchronize()
     with ClockSampler(torch.cuda.current_device()) as clk:
-        torch.cuda.profiler.start()   # a profiler started with profiling off captures this region only
         e0.record(stream); Jg, gp, gs, gg = adj.gradient(dts, A["every"]); e1.record(stream)
         torch.cuda.synchronize()
-        torch.cuda.profiler.stop()
     t_run = e0.elapsed_time(e1)
     gu = pb.active(gp)[1][:, :, 0].copy()
     u0 = pb.active(pb.p)[1][:, :, 0].copy()
@@ -640,29 +643,46 @@ def run_adjoint(args):
         reset(u)
         return adj.forward(dts)
     rng = np.random.default_rng(2025)
-    errs = []
-    ndir = A["directions"] if args.fd_directions is None else args.fd_directions
-    for _ in range(ndir):
+    fd_errs = []
+    for _ in range(fd_directions):
         v = rng.standard_normal(u0.shape) * u0
-        e = 1e-8   # the discrete objective has limiter/upwind kinks closer than 1e-6 apart
+        e = 1e-8
         fd = (Ju(u0 + e * v) - Ju(u0 - e * v)) / (2 * e)
-        errs.append(abs(float((gu * v).sum()) - fd) / max(abs(fd), 1e-300))
+        fd_errs.append(abs(float((gu * v).sum()) - fd) / max(abs(fd), 1e-300))
     adj.close()
     blk.close()
+    t0 = time.perf_counter()
+    tlm, tlm_g = tangent_errors(run, u0, pb.gam, gu, gg, ndir=tlm_directions) if tlm_directions else ([], None)
+    t_tlm = time.perf_counter() - t0
     n = A["nsteps"]
-    out = {"metric": "adjoint/forward time", "value": t_run / t_fwd, "unit": "x", "n_gpus": 1, "steps": n,
-           "warmup": args.warmup, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-           "data": "synthetic",
-           "config": {"workload": f"adjoint: 2-D FM torus {A['n']}x{A['n']} (a={A['spin']}, beta_min=100), "
-                                  f"J = sum_n dt Mdot through x1 face {ih}, {n} steps, checkpoint every {A['every']}",
-                      "zones": A["n"] * A["n"]},
-           "forward_ms_per_step": t_fwd / n, "gradient_ms_per_step": t_run / n,
-           "backward_over_forward": (t_run - t_fwd) / t_fwd,
-           "J": J, "J_from_gradient_run": Jg, "dJ_dgamma": gg,
-           "fd_check": {"directions": ndir, "order": 2, "rel_step": 1e-8,
-                        "max_rel_err": max(errs) if errs else None,
-                        "median_rel_err": float(np.median(errs)) if errs else None},
-           "clocks": clk.summary(), "gpu_launches": None}
+    return {"workload": f"adjoint: 2-D FM torus {A['n']}x{A['n']} (a={A['spin']}, beta_min=100), J = sum_n dt Mdot "
+                        f"through x1 face {run.ih} (r = {A['radius']}, the pressure maximum), {n} steps, "
+                        f"checkpoint every {A['every']}",
+            "adjoint_over_forward": t_run / t_fwd, "forward_ms_per_step": t_fwd / n,
+            "gradient_ms_per_step": t_run / n, "J": J, "J_from_gradient_run": Jg, "dJ_dgamma": gg,
+            "tangent_linear_check": {"directions": len(tlm), "reference": "oracle on forward-mode dual numbers (FP64)",
+                                     "max_rel_err": float(np.max(tlm)) if len(tlm) else None,
+                                     "median_rel_err": float(np.median(tlm)) if len(tlm) else None,
+                                     "gamma_rel_err": tlm_g, "host_seconds": t_tlm},
+            "fd_check": {"directions": fd_directions, "order": 2, "rel_step": 1e-8,
+                         "max_rel_err": max(fd_errs) if fd_errs else None,
+                         "median_rel_err": float(np.median(fd_errs)) if fd_errs else None},
+            "clocks": clk.summary()}
+
+
+def run_adjoint(args):
+    """The adjoint workload on its own line: metric adjoint/forward time."""
+    import torch
+    rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return
+    ndir = ADJOINT["directions"] if args.fd_directions is None else args.fd_directions
+    r = _adjoint_block(args, ndir, tlm_directions=ndir)
+    out = {"metric": "adjoint/forward time", "value": r["adjoint_over_forward"], "unit": "x", "n_gpus": 1,
+           "steps": ADJOINT["nsteps"], "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": r["workload"], "zones": ADJOINT["n"] ** 2}, **r, "gpu_launches": None}
     print(json.dumps(out), flush=True)
 
 
@@ -778,6 +798,8 @@ def main():
                     help="steps of the accuracy block (mixed vs FP64 per-field L1; default 1000)")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the accuracy block (mixed vs FP64 after 1000 steps, step 1 vs the oracle)")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the adjoint block (C5 adjoint/forward time, tangent-linear and FD checks)")
     ap.add_argument("--cpu-budget", type=float, default=120.0,
                     help="seconds of timed oracle steps at most (CPU baseline and the reference arm)")
     ap.add_argument("--kernels-only", action="store_true",
