@@ -431,15 +431,11 @@ __global__ void k_fix_flux(const Dims d, T *F1, T *F2, T *F3) {
     if (t < n_fix_flux(d)) fix_flux_at(d, F1, F2, F3, t);
 }
 
-// cell-centre EMF, -gdet (u x b), on the active zones plus one ghost layer
+// cell-centre EMF, -gdet (u x b), of zone (i, j, z): e[0..2] = E1, E2, E3
+// (E1, E2 only in 3-D)
 template <typename T>
-__device__ __forceinline__ void k_emf_centre_at(const Dims &d, const Geom &m, const double *__restrict__ pv,
-                                                     T *__restrict__ Ec, const long t) {
-    const int ni = d.n1 + 2 * d.d1, nj = d.n2 + 2 * d.d2, nz = d.n3 + 2 * d.d3;
-    const int z = (d.ng3 - d.d3) * d.d3 + (int)(t % nz);
-    const int j = (d.ng2 - d.d2) * d.d2 + (int)((t / nz) % nj);
-    const int i = (d.ng1 - d.d1) * d.d1 + (int)(t / ((long)nz * nj));
-    const long c = cix(d, i, j, z);
+__device__ __forceinline__ void emf_centre_eval(const Dims &d, const Geom &m, const double *__restrict__ pv, int i,
+                                                int j, long c, T *e) {
     T pb[NPR];
 #pragma unroll
     for (int k = 0; k < NPR; k++) pb[k] = (T)__ldg(&pv[k * d.ks + c]);
@@ -450,10 +446,29 @@ __device__ __forceinline__ void k_emf_centre_at(const Dims &d, const Geom &m, co
     lower4(ucon, gm.gcov, ucov);
     bcon_calc(pb, ucon, ucov, bcon);
     if (d.ng3 > 0) {
-        Ec[1 * d.ks + c] = -gm.g * (ucon[2] * bcon[3] - ucon[3] * bcon[2]);
-        Ec[2 * d.ks + c] = -gm.g * (ucon[3] * bcon[1] - ucon[1] * bcon[3]);
+        e[0] = -gm.g * (ucon[2] * bcon[3] - ucon[3] * bcon[2]);
+        e[1] = -gm.g * (ucon[3] * bcon[1] - ucon[1] * bcon[3]);
     }
-    Ec[3 * d.ks + c] = -gm.g * (ucon[1] * bcon[2] - ucon[2] * bcon[1]);
+    e[2] = -gm.g * (ucon[1] * bcon[2] - ucon[2] * bcon[1]);
+}
+
+// on the active zones plus one ghost layer
+template <typename T>
+__device__ __forceinline__ void k_emf_centre_at(const Dims &d, const Geom &m, const double *__restrict__ pv,
+                                                     T *__restrict__ Ec, const long t) {
+    const int ni = d.n1 + 2 * d.d1, nj = d.n2 + 2 * d.d2, nz = d.n3 + 2 * d.d3;
+    const int z = (d.ng3 - d.d3) * d.d3 + (int)(t % nz);
+    const int j = (d.ng2 - d.d2) * d.d2 + (int)((t / nz) % nj);
+    const int i = (d.ng1 - d.d1) * d.d1 + (int)(t / ((long)nz * nj));
+    (void)ni;
+    const long c = cix(d, i, j, z);
+    T e[3];
+    emf_centre_eval(d, m, pv, i, j, c, e);
+    if (d.ng3 > 0) {
+        Ec[1 * d.ks + c] = e[0];
+        Ec[2 * d.ks + c] = e[1];
+    }
+    Ec[3 * d.ks + c] = e[2];
 }
 
 template <typename T>
@@ -470,47 +485,44 @@ template <typename T> __device__ __forceinline__ T dn(T f) { return (T)(f > T(0.
 
 // edge EMFs: average of the four face EMFs plus, when ct_upwind, the
 // centre-minus-face corrections from the upwind side of each face, chosen by
-// the sign of its mass flux (consttransport2, GPU_const_trans.h:121-338)
-template <typename T>
-__device__ __forceinline__ void k_emf_edge_at(const Dims &d, const T *__restrict__ Ec,
-                                                   const T *__restrict__ F1, const T *__restrict__ F2,
-                                                   const T *__restrict__ F3, T *__restrict__ emf, const long t) {
-    const int ni = d.n1 + d.d1, nj = d.n2 + d.d2, nz = d.n3 + d.d3;
-    const int z = d.ng3 * d.d3 + (int)(t % nz);
-    const int j = d.ng2 * d.d2 + (int)((t / nz) % nj);
-    const int i = d.ng1 * d.d1 + (int)(t / ((long)nz * nj));
-    const long c = cix(d, i, j, z);
+// the sign of its mass flux (consttransport2, GPU_const_trans.h:121-338), for
+// the edge at cell index c (row j): ec(k, di, dj, dz) is centre EMF k (1..3)
+// of the zone offset by (di, dj, dz) in {-1, 0}^3 from the edge's cell
+// (times the direction flags d1..d3); e[0..2] = E1, E2, E3
+template <typename T, class EC>
+__device__ __forceinline__ void emf_edge_eval(const Dims &d, EC ec, const T *__restrict__ F1,
+                                              const T *__restrict__ F2, const T *__restrict__ F3, long c, int j,
+                                              T *e) {
     const long ks = d.ks, jsize = d.G3, isize = (long)d.G2 * d.G3;
     const long D1 = d.d1, D2 = d.d2, D3 = d.d3;
-    const T *Ec1 = Ec + 1 * ks, *Ec2 = Ec + 2 * ks, *Ec3 = Ec + 3 * ks;
     const T *F1r = F1 + RHO * ks, *F2r = F2 + RHO * ks, *F3r = F3 + RHO * ks;
     const bool w = d.ct_upwind != 0;
     // in the non-upwind build every correction is an exact 0.0
 #define CORR(expr) (w ? (expr) : T(0.0))
-    const T dE_LEFT_13_1 = CORR(Ec1[c] - F3[B2 * ks + c]);
-    const T dE_LEFT_13_2 = CORR(Ec1[c - jsize * D2] - F3[B2 * ks + c - jsize * D2]);
-    const T dE_RIGHT_13_1 = CORR(F3[B2 * ks + c] - Ec1[c - D3]);
-    const T dE_RIGHT_13_2 = CORR(F3[B2 * ks + c - jsize * D2] - Ec1[c - jsize * D2 - D3]);
-    const T dE_LEFT_12_1 = CORR(Ec1[c] + F2[B3 * ks + c]);
-    const T dE_LEFT_12_2 = CORR(Ec1[c - D3] + F2[B3 * ks + c - D3]);
-    const T dE_RIGHT_12_1 = CORR(-F2[B3 * ks + c] - Ec1[c - D2 * jsize]);
-    const T dE_RIGHT_12_2 = CORR(-F2[B3 * ks + c - D3] - Ec1[c - D2 * jsize - D3]);
-    const T dE_LEFT_21_1 = CORR(Ec2[c] - F1[B3 * ks + c]);
-    const T dE_LEFT_21_2 = CORR(Ec2[c - D3] - F1[B3 * ks + c - D3]);
-    const T dE_RIGHT_21_1 = CORR(F1[B3 * ks + c] - Ec2[c - D1 * isize]);
-    const T dE_RIGHT_21_2 = CORR(F1[B3 * ks + c - D3] - Ec2[c - D1 * isize - D3]);
-    const T dE_LEFT_23_1 = CORR(Ec2[c] + F3[B1 * ks + c]);
-    const T dE_LEFT_23_2 = CORR(Ec2[c - D1 * isize] + F3[B1 * ks + c - D1 * isize]);
-    const T dE_RIGHT_23_1 = CORR(-F3[B1 * ks + c] - Ec2[c - D3]);
-    const T dE_RIGHT_23_2 = CORR(-F3[B1 * ks + c - isize * D1] - Ec2[c - isize * D1 - D3]);
-    const T dE_LEFT_31_1 = CORR(Ec3[c] + F1[B2 * ks + c]);
-    const T dE_LEFT_31_2 = CORR(Ec3[c - D2 * jsize] + F1[B2 * ks + c - D2 * jsize]);
-    const T dE_RIGHT_31_1 = CORR(-F1[B2 * ks + c] - Ec3[c - D1 * isize]);
-    const T dE_RIGHT_31_2 = CORR(-F1[B2 * ks + c - D2 * jsize] - Ec3[c - D1 * isize - D2 * jsize]);
-    const T dE_LEFT_32_1 = CORR(Ec3[c] - F2[B1 * ks + c]);
-    const T dE_LEFT_32_2 = CORR(Ec3[c - D1 * isize] - F2[B1 * ks + c - D1 * isize]);
-    const T dE_RIGHT_32_1 = CORR(F2[B1 * ks + c] - Ec3[c - D2 * jsize]);
-    const T dE_RIGHT_32_2 = CORR(F2[B1 * ks + c - D1 * isize] - Ec3[c - D1 * isize - D2 * jsize]);
+    const T dE_LEFT_13_1 = CORR(ec(1, 0, 0, 0) - F3[B2 * ks + c]);
+    const T dE_LEFT_13_2 = CORR(ec(1, 0, -1, 0) - F3[B2 * ks + c - jsize * D2]);
+    const T dE_RIGHT_13_1 = CORR(F3[B2 * ks + c] - ec(1, 0, 0, -1));
+    const T dE_RIGHT_13_2 = CORR(F3[B2 * ks + c - jsize * D2] - ec(1, 0, -1, -1));
+    const T dE_LEFT_12_1 = CORR(ec(1, 0, 0, 0) + F2[B3 * ks + c]);
+    const T dE_LEFT_12_2 = CORR(ec(1, 0, 0, -1) + F2[B3 * ks + c - D3]);
+    const T dE_RIGHT_12_1 = CORR(-F2[B3 * ks + c] - ec(1, 0, -1, 0));
+    const T dE_RIGHT_12_2 = CORR(-F2[B3 * ks + c - D3] - ec(1, 0, -1, -1));
+    const T dE_LEFT_21_1 = CORR(ec(2, 0, 0, 0) - F1[B3 * ks + c]);
+    const T dE_LEFT_21_2 = CORR(ec(2, 0, 0, -1) - F1[B3 * ks + c - D3]);
+    const T dE_RIGHT_21_1 = CORR(F1[B3 * ks + c] - ec(2, -1, 0, 0));
+    const T dE_RIGHT_21_2 = CORR(F1[B3 * ks + c - D3] - ec(2, -1, 0, -1));
+    const T dE_LEFT_23_1 = CORR(ec(2, 0, 0, 0) + F3[B1 * ks + c]);
+    const T dE_LEFT_23_2 = CORR(ec(2, -1, 0, 0) + F3[B1 * ks + c - D1 * isize]);
+    const T dE_RIGHT_23_1 = CORR(-F3[B1 * ks + c] - ec(2, 0, 0, -1));
+    const T dE_RIGHT_23_2 = CORR(-F3[B1 * ks + c - isize * D1] - ec(2, -1, 0, -1));
+    const T dE_LEFT_31_1 = CORR(ec(3, 0, 0, 0) + F1[B2 * ks + c]);
+    const T dE_LEFT_31_2 = CORR(ec(3, 0, -1, 0) + F1[B2 * ks + c - D2 * jsize]);
+    const T dE_RIGHT_31_1 = CORR(-F1[B2 * ks + c] - ec(3, -1, 0, 0));
+    const T dE_RIGHT_31_2 = CORR(-F1[B2 * ks + c - D2 * jsize] - ec(3, -1, -1, 0));
+    const T dE_LEFT_32_1 = CORR(ec(3, 0, 0, 0) - F2[B1 * ks + c]);
+    const T dE_LEFT_32_2 = CORR(ec(3, -1, 0, 0) - F2[B1 * ks + c - D1 * isize]);
+    const T dE_RIGHT_32_1 = CORR(F2[B1 * ks + c] - ec(3, 0, -1, 0));
+    const T dE_RIGHT_32_2 = CORR(F2[B1 * ks + c - D1 * isize] - ec(3, -1, -1, 0));
 #undef CORR
     T e1 = T(0.25) * ((-F2[B3 * ks + c] - (dE_LEFT_13_1 * up(F2r[c]) + dE_LEFT_13_2 * dn(F2r[c])))
         + (-F2[B3 * ks + c - D3] + (dE_RIGHT_13_1 * up(F2r[c - D3]) + dE_RIGHT_13_2 * dn(F2r[c - D3]))) +
@@ -528,9 +540,30 @@ __device__ __forceinline__ void k_emf_edge_at(const Dims &d, const T *__restrict
         e3 = T(0.);
         e1 = T(-0.5) * (F2[B3 * ks + c] + F2[B3 * ks + c - D3]);
     }
-    emf[1 * ks + c] = e1;
-    emf[2 * ks + c] = e2;
-    emf[3 * ks + c] = e3;
+    e[0] = e1;
+    e[1] = e2;
+    e[2] = e3;
+}
+
+template <typename T>
+__device__ __forceinline__ void k_emf_edge_at(const Dims &d, const T *__restrict__ Ec,
+                                                   const T *__restrict__ F1, const T *__restrict__ F2,
+                                                   const T *__restrict__ F3, T *__restrict__ emf, const long t) {
+    const int ni = d.n1 + d.d1, nj = d.n2 + d.d2, nz = d.n3 + d.d3;
+    const int z = d.ng3 * d.d3 + (int)(t % nz);
+    const int j = d.ng2 * d.d2 + (int)((t / nz) % nj);
+    const int i = d.ng1 * d.d1 + (int)(t / ((long)nz * nj));
+    (void)ni;
+    const long c = cix(d, i, j, z);
+    const long ks = d.ks, jsize = d.G3, isize = (long)d.G2 * d.G3;
+    auto ec = [&](int k, int di, int dj, int dz) {
+        return Ec[k * ks + c + di * d.d1 * isize + dj * d.d2 * jsize + dz * d.d3];
+    };
+    T e[3];
+    emf_edge_eval<T>(d, ec, F1, F2, F3, c, j, e);
+    emf[1 * ks + c] = e[0];
+    emf[2 * ks + c] = e[1];
+    emf[3 * ks + c] = e[2];
 }
 
 template <typename T>
@@ -571,7 +604,40 @@ __global__ void k_pole_average(const Dims d, T *emf, StepSize st) {
     k_pole_average_at(d, emf, st, t);
 }
 
-// staggered field update from the edge EMFs (consttransport3, GPU_const_trans.h:426-529)
+// staggered field update from the edge EMFs (consttransport3,
+// GPU_const_trans.h:426-529) of the face triple at cell (i, j, z): E(k, di,
+// dj, dz) is edge EMF k (1..3) at the offset (di, dj, dz) in {0, 1}^3 (times
+// the direction flags); `rows` selects which faces to write (bit 0: x1, bit 1:
+// x2, bit 2: x3) on top of the range checks.
+template <class EF>
+__device__ __forceinline__ void face_update_eval(const Dims &d, const Geom &m, const double *psi, double *psf,
+                                                 EF E, double Dt, int i, int j, int z, long c, long gi, int faces) {
+    const long ks = d.ks;
+    if ((faces & 1) && i < d.n1 + d.ng1 + d.d1 && j < d.n2 + d.ng2 && z < d.n3 + d.ng3) {
+        const double gdf = __ldg(&m.gdet[FACE1 * d.gs + gi]);
+        double temp = 0.;
+        temp += 1.0 / ((double)1) * psi[c] * gdf;
+        temp += -Dt / ((double)1 * d.dx2) * (E(3, 0, 1, 0) - E(3, 0, 0, 0));
+        if (d.ng3 > 0) temp += Dt / ((double)1 * d.dx3) * (E(2, 0, 0, 1) - E(2, 0, 0, 0));
+        psf[c] = temp / gdf;
+    }
+    if ((faces & 4) && d.ng3 > 0 && i < d.n1 + d.ng1 && j < d.n2 + d.ng2 && z < d.n3 + d.ng3 + d.d3) {
+        const double gdf = __ldg(&m.gdet[FACE3 * d.gs + gi]);
+        double temp = psi[2 * ks + c] * gdf;
+        temp += -Dt / d.dx1 * (E(2, 1, 0, 0) - E(2, 0, 0, 0));
+        temp += Dt / d.dx2 * (E(1, 0, 1, 0) - E(1, 0, 0, 0));
+        psf[2 * ks + c] = temp / gdf;
+    }
+    if ((faces & 2) && i < d.n1 + d.ng1 && j < d.n2 + d.ng2 + d.d2 && z < d.n3 + d.ng3) {
+        const double gdf = __ldg(&m.gdet[FACE2 * d.gs + gi]);
+        double temp = 0.;
+        temp += 1.0 / ((double)1) * psi[1 * ks + c] * gdf;
+        temp += Dt / ((double)1 * d.dx1) * (E(3, 1, 0, 0) - E(3, 0, 0, 0));
+        if (d.ng3 > 0) temp += -Dt / ((double)1 * d.dx3) * (E(1, 0, 0, 1) - E(1, 0, 0, 0));
+        psf[1 * ks + c] = temp / gdf;
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ void k_face_update_at(const Dims &d, const Geom &m, const double *psi, double *psf,
                                                       const T *__restrict__ Et, StepSize st, const long t) {
@@ -579,33 +645,13 @@ __device__ __forceinline__ void k_face_update_at(const Dims &d, const Geom &m, c
     const int z = d.ng3 * d.d3 + (int)(t % nz);
     const int j = d.ng2 * d.d2 + (int)((t / nz) % nj);
     const int i = d.ng1 * d.d1 + (int)(t / ((long)nz * nj));
+    (void)ni;
     const long c = cix(d, i, j, z), gi = gix(d, i, j);
     const long ks = d.ks, isize = (long)d.G2 * d.G3, jsz = d.G3;
-    const double Dt = st.sub();
-    auto E = [&](long idx) { return (double)Et[idx]; };
-    if (i < d.n1 + d.ng1 + d.d1 && j < d.n2 + d.ng2 && z < d.n3 + d.ng3) {
-        const double gdf = __ldg(&m.gdet[FACE1 * d.gs + gi]);
-        double temp = 0.;
-        temp += 1.0 / ((double)1) * psi[c] * gdf;
-        temp += -Dt / ((double)1 * d.dx2) * (E(3 * ks + c + jsz) - E(3 * ks + c));
-        if (d.ng3 > 0) temp += Dt / ((double)1 * d.dx3) * (E(2 * ks + c + d.d3) - E(2 * ks + c));
-        psf[c] = temp / gdf;
-    }
-    if (d.ng3 > 0 && i < d.n1 + d.ng1 && j < d.n2 + d.ng2 && z < d.n3 + d.ng3 + d.d3) {
-        const double gdf = __ldg(&m.gdet[FACE3 * d.gs + gi]);
-        double temp = psi[2 * ks + c] * gdf;
-        temp += -Dt / d.dx1 * (E(2 * ks + c + isize) - E(2 * ks + c));
-        temp += Dt / d.dx2 * (E(1 * ks + c + jsz) - E(1 * ks + c));
-        psf[2 * ks + c] = temp / gdf;
-    }
-    if (i < d.n1 + d.ng1 && j < d.n2 + d.ng2 + d.d2 && z < d.n3 + d.ng3) {
-        const double gdf = __ldg(&m.gdet[FACE2 * d.gs + gi]);
-        double temp = 0.;
-        temp += 1.0 / ((double)1) * psi[1 * ks + c] * gdf;
-        temp += Dt / ((double)1 * d.dx1) * (E(3 * ks + c + isize) - E(3 * ks + c));
-        if (d.ng3 > 0) temp += -Dt / ((double)1 * d.dx3) * (E(1 * ks + c + d.d3) - E(1 * ks + c));
-        psf[1 * ks + c] = temp / gdf;
-    }
+    auto E = [&](int k, int di, int dj, int dz) {
+        return (double)Et[k * ks + c + di * isize + dj * jsz + dz * d.d3];
+    };
+    face_update_eval(d, m, psi, psf, E, st.sub(), i, j, z, c, gi, 7);
 }
 
 template <typename T>
@@ -615,6 +661,135 @@ __global__ void __launch_bounds__(BLK) k_face_update(const Dims d, const Geom m,
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)ni * nj * nz) return;
     k_face_update_at(d, m, psi, psf, Et, st, t);
+}
+
+// ---------------------------------------------------------------- fused CT
+// Constrained transport of a 3-D block in one kernel: centre EMFs, edge EMFs
+// and the face update, with the centre and edge EMFs kept in shared memory
+// instead of two HBM round trips. A CTA owns a tile of CT_TJ x CT_TZ (j, z)
+// columns and marches along i over a chunk of planes, with two-plane rings:
+// for plane i it builds the centre EMFs of plane i (tile plus a one-zone halo
+// on the low j and z sides, which the edges need), then the edge EMFs of
+// plane i (tile plus one edge on the high sides, which the faces need), then
+// updates the faces of plane i - 1 (their upper edges lie in plane i). A
+// chunk recomputes the centre and edge EMFs of the plane before it. Same
+// expressions as k_emf_centre, k_emf_edge and k_face_update (the shared
+// evaluators above), so the same values.
+//
+// With transmissive poles the polar x1-EMFs are replaced by their phi average
+// over the whole ring (k_pole_average) before the faces next to the poles
+// are updated: the kernel writes the edge EMFs of the two rows at each pole
+// to the global array and leaves the faces of rows ng2, n2 + ng2 - 1 and
+// n2 + ng2 to k_face_update_polar, which runs after the average.
+//
+// Measured on the 384 x 192 x 192 torus, per step: 4.0-5.0 ms (FP64) and
+// 2.2-3.2 ms (float) over chunks of 4-24 planes and 2-4 CTAs per SM, against
+// 2.7 and 1.9 ms for the three separate kernels: CTAs marching plane by plane
+// with two barriers per plane keep too few loads in flight. The stage
+// therefore runs the three kernels; HAMR_CT_FUSED=1 selects this one.
+constexpr int CT_TZ = 32, CT_TJ = 8, CT_THREADS = CT_TZ * CT_TJ;
+// build option: x1 planes per CTA of the fused CT kernel (more planes: less
+// recomputed plane per chunk, fewer CTAs in flight)
+#ifndef HAMR_CT_CHUNK
+#define HAMR_CT_CHUNK 24
+#endif
+
+__device__ __forceinline__ bool ct_polar_row(const Dims &d, int j) {
+    return d.bc2 == HAMR_BC_POLE_TRANS && (j == d.ng2 || j == d.n2 + d.ng2 - 1 || j == d.n2 + d.ng2);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(CT_THREADS, 2)
+    k_ct_fused(const Dims d, const Geom m, const double *__restrict__ pv, const T *__restrict__ F1,
+               const T *__restrict__ F2, const T *__restrict__ F3, const double *psi, double *psf,
+               T *__restrict__ emf_g, StepSize st) {
+    constexpr int EJ = CT_TJ + 2, EZ = CT_TZ + 2;   // centre-EMF tile with its low-side halo
+    constexpr int GJ = CT_TJ + 1, GZ = CT_TZ + 1;   // edge tile with its high-side edge
+    __shared__ T sEc[2][3][EJ][EZ];
+    __shared__ T sE[2][3][GJ][GZ];
+    const int tid = threadIdx.x;
+    const int j0 = d.ng2 + blockIdx.y * CT_TJ, z0 = d.ng3 + blockIdx.x * CT_TZ;
+    const int ia = d.ng1 + blockIdx.z * HAMR_CT_CHUNK;
+    const int ib = min(ia + HAMR_CT_CHUNK, d.n1 + d.ng1 + 1);   // face planes [ia, ib)
+    const int ie = min(ib, d.n1 + d.ng1);                        // last edge plane
+    const long ks = d.ks, isize = (long)d.G2 * d.G3, jsz = d.G3;
+    const double Dt = st.sub();
+    const bool polar = d.bc2 == HAMR_BC_POLE_TRANS;
+    // the faces of plane i from the edge rings (plane i in slot i & 1)
+    auto faces = [&](int i) {
+        const int jj = tid / CT_TZ, zz = tid % CT_TZ;
+        const int j = j0 + jj, z = z0 + zz;
+        if (j > d.n2 + d.ng2 || z > d.n3 + d.ng3 || ct_polar_row(d, j)) return;
+        auto E = [&](int k, int di, int dj, int dz) { return (double)sE[(i + di) & 1][k - 1][jj + dj][zz + dz]; };
+        face_update_eval(d, m, psi, psf, E, Dt, i, j, z, cix(d, i, j, z), gix(d, i, j), 7);
+    };
+    for (int i = ia - 1; i <= ie; i++) {
+        // centre EMFs of plane i: zones j0-1 .. j0+CT_TJ, z0-1 .. z0+CT_TZ
+        for (int e = tid; e < EJ * EZ; e += CT_THREADS) {
+            const int jj = e / EZ, zz = e % EZ;
+            const int j = j0 - 1 + jj, z = z0 - 1 + zz;
+            if (j <= d.n2 + d.ng2 && z <= d.n3 + d.ng3) {
+                T ec[3];
+                emf_centre_eval(d, m, pv, i, j, cix(d, i, j, z), ec);
+                sEc[i & 1][0][jj][zz] = ec[0];
+                sEc[i & 1][1][jj][zz] = ec[1];
+                sEc[i & 1][2][jj][zz] = ec[2];
+            }
+        }
+        __syncthreads();
+        if (i < ia) continue;
+        // edge EMFs of plane i: edges j0 .. j0+CT_TJ, z0 .. z0+CT_TZ
+        for (int e = tid; e < GJ * GZ; e += CT_THREADS) {
+            const int jj = e / GZ, zz = e % GZ;
+            const int j = j0 + jj, z = z0 + zz;
+            if (j <= d.n2 + d.ng2 && z <= d.n3 + d.ng3) {
+                const long c = cix(d, i, j, z);
+                auto ec = [&](int k, int di, int dj, int dz) { return sEc[(i + di) & 1][k - 1][jj + 1 + dj][zz + 1 + dz]; };
+                T ed[3];
+                emf_edge_eval<T>(d, ec, F1, F2, F3, c, j, ed);
+                sE[i & 1][0][jj][zz] = ed[0];
+                sE[i & 1][1][jj][zz] = ed[1];
+                sE[i & 1][2][jj][zz] = ed[2];
+                if (polar && (j == d.ng2 || j == d.ng2 + 1 || j == d.n2 + d.ng2 - 1 || j == d.n2 + d.ng2)) {
+                    emf_g[1 * ks + c] = ed[0];
+                    emf_g[2 * ks + c] = ed[1];
+                    emf_g[3 * ks + c] = ed[2];
+                }
+            }
+        }
+        __syncthreads();
+        if (i - 1 >= ia) faces(i - 1);
+    }
+    // the last x1-face plane has no edge plane above it (x1 faces only)
+    if (ib == d.n1 + d.ng1 + 1) {
+        const int i = d.n1 + d.ng1;
+        const int jj = tid / CT_TZ, zz = tid % CT_TZ;
+        const int j = j0 + jj, z = z0 + zz;
+        if (j <= d.n2 + d.ng2 && z <= d.n3 + d.ng3 && !ct_polar_row(d, j)) {
+            auto E = [&](int k, int di, int dj, int dz) { return (double)sE[(i + di) & 1][k - 1][jj + dj][zz + dz]; };
+            face_update_eval(d, m, psi, psf, E, Dt, i, j, z, cix(d, i, j, z), gix(d, i, j), 1);
+        }
+    }
+    (void)isize;
+    (void)jsz;
+}
+
+// the faces k_ct_fused leaves for after the polar average: rows ng2,
+// n2 + ng2 - 1 and n2 + ng2, from the global edge EMFs
+template <typename T>
+__global__ void k_face_update_polar(const Dims d, const Geom m, const double *psi, double *psf,
+                                    const T *__restrict__ Et, StepSize st) {
+    const int ni = d.n1 + 1, nz = d.n3 + 1;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3L * ni * nz) return;
+    const int z = d.ng3 + (int)(t % nz);
+    const int i = d.ng1 + (int)((t / nz) % ni);
+    const int r = (int)(t / ((long)nz * ni));
+    const int j = r == 0 ? d.ng2 : (r == 1 ? d.n2 + d.ng2 - 1 : d.n2 + d.ng2);
+    const long c = cix(d, i, j, z);
+    const long ks = d.ks, isize = (long)d.G2 * d.G3, jsz = d.G3;
+    auto E = [&](int k, int di, int dj, int dz) { return (double)Et[k * ks + c + di * isize + dj * jsz + dz]; };
+    face_update_eval(d, m, psi, psf, E, st.sub(), i, j, z, c, gix(d, i, j), 7);
 }
 
 // geometric source gdet T^k_l Gamma^l_{jk} (source, GPU_phys_mhd.h:34-175)
@@ -721,14 +896,14 @@ __device__ __forceinline__ void source(double gam, const double *ph, const Geo<d
 // the full one, minus the flux divergence, plus the geometric source at the
 // stage's primitives; U[B] from the face-averaged staggered field. pf returns
 // the stage's primitives (the inversion's initial guess).
-template <typename T, class Conn>
-__device__ __forceinline__ void cons_update(const Dims &d, const Geom &m, const double *__restrict__ pin,
-                                            const double *__restrict__ pb, double *__restrict__ Ucache,
-                                            const T *__restrict__ F1, const T *__restrict__ F2,
-                                            const T *__restrict__ F3, int full, double Dt, int i, int j,
-                                            long c, long gi, const Geo<double> &gm, Conn conn, double *pf,
-                                            double *U) {
-    const long ks = d.ks, isize = (long)d.G2 * d.G3;
+// FX(dir, k, up): flux k of direction dir on the zone's lower face (up = 0)
+// or upper face (up = 1).
+template <typename T, class Conn, class FX>
+__device__ __forceinline__ void cons_update_fx(const Dims &d, const Geom &m, const double *__restrict__ pin,
+                                               const double *__restrict__ pb, double *__restrict__ Ucache, FX FX_,
+                                               int full, double Dt, int i, int j, long c, long gi,
+                                               const Geo<double> &gm, Conn conn, double *pf, double *U) {
+    const long ks = d.ks;
     State<double> q;
     double dU[NPR];
     if (!full) {
@@ -749,9 +924,9 @@ __device__ __forceinline__ void cons_update(const Dims &d, const Geom &m, const 
     if constexpr (sizeof(T) == sizeof(double)) {
 #pragma unroll
         for (int k = 0; k < NPR; k++) {
-            if (d.ng1 > 0) U[k] -= div_rcp(Dt * (F1[k * ks + c + isize] - F1[k * ks + c]), d.dx1, d.rdx1);
-            if (d.ng2 > 0) U[k] -= div_rcp(Dt * (F2[k * ks + c + d.G3] - F2[k * ks + c]), d.dx2, d.rdx2);
-            if (d.ng3 > 0) U[k] -= div_rcp(Dt * (F3[k * ks + c + 1] - F3[k * ks + c]), d.dx3, d.rdx3);
+            if (d.ng1 > 0) U[k] -= div_rcp(Dt * (FX_(1, k, 1) - FX_(1, k, 0)), d.dx1, d.rdx1);
+            if (d.ng2 > 0) U[k] -= div_rcp(Dt * (FX_(2, k, 1) - FX_(2, k, 0)), d.dx2, d.rdx2);
+            if (d.ng3 > 0) U[k] -= div_rcp(Dt * (FX_(3, k, 1) - FX_(3, k, 0)), d.dx3, d.rdx3);
         }
         if constexpr (std::is_same<Conn, ConnTable>::value) source(d.gam, pf, gm, d, m, gi, dU, q);
         else source_c(d.gam, pf, gm, conn, dU, q);
@@ -771,13 +946,28 @@ __device__ __forceinline__ void cons_update(const Dims &d, const Geom &m, const 
                 comp += fabs(sum) >= fabs(x) ? (sum - tt) + x : (x - tt) + sum;
                 sum = tt;
             };
-            if (d.ng1 > 0) add(div_rcp(-Dt * ((double)F1[k * ks + c + isize] - (double)F1[k * ks + c]), d.dx1, d.rdx1));
-            if (d.ng2 > 0) add(div_rcp(-Dt * ((double)F2[k * ks + c + d.G3] - (double)F2[k * ks + c]), d.dx2, d.rdx2));
-            if (d.ng3 > 0) add(div_rcp(-Dt * ((double)F3[k * ks + c + 1] - (double)F3[k * ks + c]), d.dx3, d.rdx3));
+            if (d.ng1 > 0) add(div_rcp(-Dt * ((double)FX_(1, k, 1) - (double)FX_(1, k, 0)), d.dx1, d.rdx1));
+            if (d.ng2 > 0) add(div_rcp(-Dt * ((double)FX_(2, k, 1) - (double)FX_(2, k, 0)), d.dx2, d.rdx2));
+            if (d.ng3 > 0) add(div_rcp(-Dt * ((double)FX_(3, k, 1) - (double)FX_(3, k, 0)), d.dx3, d.rdx3));
             add(Dt * dU[k]);
             U[k] = sum + comp;
         }
     }
+}
+
+// the same with the fluxes read from the global arrays
+template <typename T, class Conn>
+__device__ __forceinline__ void cons_update(const Dims &d, const Geom &m, const double *__restrict__ pin,
+                                            const double *__restrict__ pb, double *__restrict__ Ucache,
+                                            const T *__restrict__ F1, const T *__restrict__ F2,
+                                            const T *__restrict__ F3, int full, double Dt, int i, int j,
+                                            long c, long gi, const Geo<double> &gm, Conn conn, double *pf,
+                                            double *U) {
+    const long ks = d.ks, isize = (long)d.G2 * d.G3;
+    auto fx = [&](int dir, int k, int up) -> T {
+        return dir == 1 ? F1[k * ks + c + up * isize] : (dir == 2 ? F2[k * ks + c + up * d.G3] : F3[k * ks + c + up]);
+    };
+    cons_update_fx<T>(d, m, pin, pb, Ucache, fx, full, Dt, i, j, c, gi, gm, conn, pf, U);
 }
 
 // U[B] from the face-averaged staggered field (fixup, GPU_fixup.h:330-345)
@@ -993,6 +1183,170 @@ __device__ __forceinline__ void invert_inputs(const Dims &d, const Geom &m, cons
     U[KTOT] = W[5 * d.ks + c];
     U[B3] = W[6 * d.ks + c];
     face_average_b(d, m, psf, i, j, c, gi, U);
+}
+
+// ------------------------------------------- TMA-staged conserved update
+// The conserved update of one (i, j) row of zones (or an equal piece of it)
+// per CTA, with the 45 flux operands of every zone -- the x1 fluxes on both
+// faces, the x2 fluxes on both faces, the x3 fluxes of the row and one more
+// -- brought into shared memory by bulk asynchronous copies (TMA,
+// cp.async.bulk) before any arithmetic: 45 copies per row, completion
+// counted on one mbarrier, all in flight at once, where a thread of the
+// one-zone-per-thread kernel can only keep as many loads in flight as its
+// registers hold. A bulk copy must start and end on 16-byte boundaries: each
+// copied segment is widened to them and indexed from its offset. Same
+// expressions as k_cons / k_cons_cols (cons_update_fx), so the same values.
+//
+// The wait on the barrier is bounded: a CTA that gives up sets *kerr and
+// waits again, also bounded, for its copies before it returns without
+// computing; the host reports the flag as an error.
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait; false when it gave up
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+    for (int it = 0; it < (1 << 20); it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+// global -> shared bulk copy of `bytes` (multiple of 16, both addresses
+// 16-byte aligned), completion counted on the barrier
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned bytes, unsigned bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// shared-memory layout of one CTA of k_cons_tma, in bytes
+struct ConsTmaLayout {
+    int cap;       // elements per staged segment (a piece of lpiece zones, widened)
+    int seg_bytes; // cap * sizeof(T), a multiple of 16
+    int f_off;     // first segment (after the barrier and the metric column)
+    int total;
+};
+template <typename T>
+__host__ __device__ __forceinline__ ConsTmaLayout cons_tma_layout(int lpiece) {
+    constexpr int A = 16 / (int)sizeof(T);
+    ConsTmaLayout L;
+    L.cap = ((lpiece + 1 + 2 * (A - 1)) + A - 1) / A * A;
+    L.seg_bytes = L.cap * (int)sizeof(T);
+    L.f_off = 16 + ((COL_VALS * 8 + 15) / 16) * 16;
+    L.total = L.f_off + 5 * NPR * L.seg_bytes;
+    return L;
+}
+
+// build option: resident CTAs per SM of the TMA-staged update (caps its
+// registers; measured on the 384 x 192 x 192 torus, per step: float 3 (2.86
+// ms; 2: 4.05, 4: 2.88), double 4 (3.67 ms; 2: 4.05, 3: 3.86))
+#ifndef HAMR_CONS_TMA_MINB_F
+#define HAMR_CONS_TMA_MINB_F 3
+#endif
+#ifndef HAMR_CONS_TMA_MINB
+#define HAMR_CONS_TMA_MINB 4
+#endif
+template <typename T>
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? HAMR_CONS_TMA_MINB : HAMR_CONS_TMA_MINB_F)
+    k_cons_tma(const Dims d, const Geom m, const double *__restrict__ pin, const double *__restrict__ pb,
+               double *__restrict__ Ucache, const T *__restrict__ F1, const T *__restrict__ F2,
+               const T *__restrict__ F3, double *__restrict__ W, int full, StepSize st, int *__restrict__ nfail,
+               int *__restrict__ kerr, int npiece, int lpiece) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int A = 16 / (int)sizeof(T);
+    const ConsTmaLayout lay = cons_tma_layout<T>(lpiece);
+    unsigned long long *bar = reinterpret_cast<unsigned long long *>(smem);
+    double *sg = reinterpret_cast<double *>(smem + 16);
+    T *sf = reinterpret_cast<T *>(smem + lay.f_off);   // [kind][plane][cap]
+    const unsigned bar_a = smem_addr(bar);
+    const int row = blockIdx.x / npiece, piece = blockIdx.x % npiece;
+    const int i = d.ng1 + row / d.n2, j = d.ng2 + row % d.n2;
+    const int za = d.ng3 + piece * lpiece;
+    const int L = min(lpiece, d.n3 - piece * lpiece);
+    const long ks = d.ks, isize = (long)d.G2 * d.G3;
+    const long c0 = cix(d, i, j, za), gi = gix(d, i, j);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *nfail = 0;   // the inversion's failed-zone list starts empty
+    // the five segment kinds: start cell, length, source array
+    auto seg_start = [&](int q) -> long { return q == 1 ? c0 + isize : (q == 3 ? c0 + d.G3 : c0); };
+    auto seg_len = [&](int q) -> int { return q == 4 ? L + 1 : L; };
+    auto seg_src = [&](int q) -> const T * { return q < 2 ? F1 : (q < 4 ? F2 : F3); };
+    if (threadIdx.x == 0) mbar_init(bar_a, 1);
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        unsigned total = 0;
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            const long s0 = seg_start(q), sa = s0 & ~(long)(A - 1);
+            const long se = (s0 + seg_len(q) + A - 1) & ~(long)(A - 1);
+            total += (unsigned)((se - sa) * (long)sizeof(T)) * NPR;
+        }
+        if (threadIdx.x == 0) mbar_expect_tx(bar_a, total);
+        __syncwarp();
+        for (int e = threadIdx.x; e < 5 * NPR; e += 32) {
+            const int q = e / NPR, k = e % NPR;
+            const long s0 = seg_start(q), sa = s0 & ~(long)(A - 1);
+            const long se = (s0 + seg_len(q) + A - 1) & ~(long)(A - 1);
+            bulk_g2s(smem_addr(sf + (long)e * lay.cap), seg_src(q) + (long)k * ks + sa,
+                     (unsigned)((se - sa) * (long)sizeof(T)), bar_a);
+        }
+    }
+    // the row's metric and connection column, while the copies fly
+    for (int v = threadIdx.x; v < COL_VALS; v += blockDim.x) {
+        double x;
+        if (v < 10) x = m.gcov[(long)(v * 5 + CENT) * d.gs + gi];
+        else if (v < 20) x = m.gcon[(long)((v - 10) * 5 + CENT) * d.gs + gi];
+        else if (v == 20) x = m.gdet[(long)CENT * d.gs + gi];
+        else x = m.conn[(long)(v - 21) * d.gs + gi];
+        sg[v] = x;
+    }
+    __syncthreads();
+    if (!mbar_wait(bar_a, 0)) {
+        atomicExch(kerr, 1);
+        (void)mbar_wait(bar_a, 0);   // let the copies land before the CTA's shared memory goes
+        return;
+    }
+    const int l = threadIdx.x;
+    if (l >= L) return;
+    const long c = c0 + l;
+    int off[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+        const long s0 = seg_start(q);
+        off[q] = (int)(s0 - (s0 & ~(long)(A - 1))) + l;
+    }
+    auto fx = [&](int dir, int k, int up) -> T {
+        const int q = dir == 1 ? up : (dir == 2 ? 2 + up : 4);
+        return sf[(long)(q * NPR + k) * lay.cap + off[q] + (dir == 3 ? up : 0)];
+    };
+    Geo<double> gm;
+#pragma unroll
+    for (int q = 0; q < 10; q++) { gm.gcov[q] = sg[q]; gm.gcon[q] = sg[10 + q]; }
+    gm.g = sg[20];
+    double pf[NPR], U[NPR];
+    cons_update_fx<T>(d, m, pin, pb, Ucache, fx, full, st.sub(), i, j, c, gi, gm, ConnStaged{sg + 21}, pf, U);
+    W[0 * d.ks + c] = U[RHO];
+    W[1 * d.ks + c] = U[UU];
+    W[2 * d.ks + c] = U[U1];
+    W[3 * d.ks + c] = U[U2];
+    W[4 * d.ks + c] = U[U3];
+    W[5 * d.ks + c] = U[KTOT];
+    W[6 * d.ks + c] = U[B3];
 }
 
 template <int INV, int FIX = 0>
@@ -1446,6 +1800,9 @@ struct hamr_ctx {
     bool have_geom = false;
     long rows_min = 0;   // threads the row flux kernels need before they pay (several waves of the device)
     bool cons_cols = true;   // column-staged conserved update where n3 >= 64
+    bool ct_fused = false;   // one constrained-transport kernel for 3-D blocks (slower: off)
+    bool cons_tma = true;    // conserved update with TMA-staged fluxes (3-D, n3 >= 32, aligned planes)
+    int *kerr = nullptr;     // set by kernels whose bounded waits gave up
     std::string err;
     // device state
     double *p = nullptr, *ph = nullptr, *ps = nullptr, *psh = nullptr, *U = nullptr;
@@ -1478,6 +1835,19 @@ int fail_cuda(hamr_ctx *c, cudaError_t e, const char *what) {
     } while (0)
 
 Geom geom_of(const hamr_ctx *c) { return Geom{c->gcov, c->gcon, c->gdet, c->conn}; }
+
+// the error word kernels set when a bounded wait gave up (read after a
+// synchronisation the caller already makes; cleared once reported)
+int check_kerr(hamr_ctx *ctx) {
+    if (!ctx->kerr) return HAMR_OK;
+    int v = 0;
+    CK(cudaMemcpyAsync(&v, ctx->kerr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (!v) return HAMR_OK;
+    CK(cudaMemsetAsync(ctx->kerr, 0, sizeof(int), ctx->stream));
+    ctx->err = "a kernel's wait for its bulk copies timed out (the step's results are invalid)";
+    return HAMR_E_CUDA;
+}
 
 // kernel groups timed by hamr_profile_step
 enum { PROF_FLUX3, PROF_FLUX2, PROF_FLUX1, PROF_FIXFLUX, PROF_EMF_CENTRE, PROF_EMF_EDGE, PROF_POLE_AVG,
@@ -1556,6 +1926,13 @@ void launch_flux(long n, cudaStream_t s, const Dims &d, const Geom &m, const dou
     }
 }
 
+// the bulk copies of k_cons_tma need 16-byte aligned flux planes
+template <typename T>
+bool cons_tma_aligned(const hamr_ctx *ctx, const Dims &d, const T *F1, const T *F2, const T *F3) {
+    auto al = [](const void *p) { return ((uintptr_t)p & 15) == 0; };
+    return ctx->kerr && (d.ks * (long)sizeof(T)) % 16 == 0 && al(F1) && al(F2) && al(F3);
+}
+
 // one sub-step: fluxes, CT, update, ghost fill of the written state. T is the
 // type of the fluxes and EMFs (double, or float in the mixed-precision step);
 // the float arrays reuse the double allocations with the same plane stride.
@@ -1590,6 +1967,24 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
         k_fix_flux<T><<<nblk(n), BLK, 0, s>>>(d, F1, F2, F3);
     }
     prof_mark(pf, PROF_FIXFLUX, s);
+    if (d.d3 && ctx->ct_fused) {
+        // centre EMFs, edge EMFs and the face update in one kernel (polar
+        // rows of transmissive poles after the phi average); timed as the
+        // edge-EMF group
+        prof_mark(pf, PROF_EMF_CENTRE, s);
+        const dim3 grid((d.n3 + CT_TZ) / CT_TZ, (d.n2 + CT_TJ) / CT_TJ, (d.n1 + HAMR_CT_CHUNK) / HAMR_CT_CHUNK);
+        k_ct_fused<T><<<grid, CT_THREADS, 0, s>>>(d, m, pin, F1, F2, F3, ctx->ps, full ? ctx->ps : ctx->psh, emf, st);
+        prof_mark(pf, PROF_EMF_EDGE, s);
+        if (d.bc2 == HAMR_BC_POLE_TRANS) {
+            k_pole_average<T><<<nblk(2L * (d.n1 + d.ng1)), BLK, 0, s>>>(d, emf, st);
+            prof_mark(pf, PROF_POLE_AVG, s);
+            k_face_update_polar<T><<<nblk(3L * (d.n1 + 1) * (d.n3 + 1)), BLK, 0, s>>>(
+                d, m, ctx->ps, full ? ctx->ps : ctx->psh, emf, st);
+        } else {
+            prof_mark(pf, PROF_POLE_AVG, s);
+        }
+        prof_mark(pf, PROF_FACE, s);
+    } else {
     {
         long n = (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3);
         k_emf_centre<T><<<nblk(n), BLK, 0, s>>>(d, m, pin, Ec);
@@ -1605,9 +2000,16 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
         k_face_update<T><<<nblk(n), BLK, 0, s>>>(d, m, ctx->ps, full ? ctx->ps : ctx->psh, emf, st);
         prof_mark(pf, PROF_FACE, s);
     }
+    }
     {
         long n = (long)d.n1 * d.n2 * d.n3;
-        if (d.n3 >= 64 && ctx->cons_cols)   // metric and connection staged per CTA
+        const bool tma = ctx->cons_tma && d.d3 && d.n3 >= 32 && cons_tma_aligned<T>(ctx, d, F1, F2, F3);
+        if (tma) {   // one row of zones per CTA, flux operands staged by bulk copies
+            const int npiece = (d.n3 + 255) / 256, lpiece = (d.n3 + npiece - 1) / npiece;
+            k_cons_tma<T><<<d.n1 * d.n2 * npiece, (lpiece + 31) / 32 * 32, cons_tma_layout<T>(lpiece).total, s>>>(
+                d, m, ctx->p, full ? ctx->ph : ctx->p, ctx->U, F1, F2, F3, ctx->W, full, st, ctx->nfail, ctx->kerr,
+                npiece, lpiece);
+        } else if (d.n3 >= 64 && ctx->cons_cols)   // metric and connection staged per CTA
             k_cons_cols<T><<<nblk(n), BLK, 0, s>>>(d, m, ctx->p, full ? ctx->ph : ctx->p, ctx->U, F1, F2, F3, ctx->W,
                                                    full, st, ctx->nfail);
         else
@@ -1733,6 +2135,8 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
         // tuning override (threads; 0: always by rows), read once per context
         if (const char *e = getenv("HAMR_FLUX_ROWS_MIN")) ctx->rows_min = atol(e);
         if (const char *e = getenv("HAMR_CONS_COLS")) ctx->cons_cols = atoi(e) != 0;
+        if (const char *e = getenv("HAMR_CT_FUSED")) ctx->ct_fused = atoi(e) != 0;
+        if (const char *e = getenv("HAMR_CONS_TMA")) ctx->cons_tma = atoi(e) != 0;
     }
     const size_t cb = sizeof(double) * d.ks;
     struct A { void **p; size_t n; } allocs[] = {
@@ -1748,7 +2152,8 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
         {(void **)&ctx->divb, sizeof(unsigned long long)},
         {(void **)&ctx->rlist, prm->repair == 2 ? sizeof(int) * d.n1 * d.n2 * d.n3 : 0},
         {(void **)&ctx->rcount, prm->repair == 2 ? sizeof(int) : 0},
-        {(void **)&ctx->flist, sizeof(int) * d.n1 * d.n2 * d.n3}, {(void **)&ctx->nfail, sizeof(int)}};
+        {(void **)&ctx->flist, sizeof(int) * d.n1 * d.n2 * d.n3}, {(void **)&ctx->nfail, sizeof(int)},
+        {(void **)&ctx->kerr, sizeof(int)}};
     if (prm->repair == 2 && d.ks > 0x7fffffffL) { hamr_ctx_destroy(ctx); return HAMR_E_ARG; }
     for (auto &a : allocs) {
         if (a.n == 0) continue;
@@ -1759,6 +2164,11 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
         cudaMemsetAsync(*a.p, 0, a.n, ctx->stream);
     }
     k_dt_reset<<<1, 32, 0, ctx->stream>>>(ctx->dtbits);
+    // the TMA-staged update's shared memory for rows of up to 256 zones
+    cudaFuncSetAttribute(k_cons_tma<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         cons_tma_layout<double>(256).total);
+    cudaFuncSetAttribute(k_cons_tma<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         cons_tma_layout<float>(256).total);
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
         hamr_ctx_destroy(ctx);
         return HAMR_E_CUDA;
@@ -1774,7 +2184,7 @@ int hamr_ctx_destroy(hamr_ctx *ctx) {
     void *bufs[] = {ctx->p, ctx->ph, ctx->ps, ctx->psh, ctx->U, ctx->F1, ctx->F2, ctx->F3, ctx->Ec, ctx->emf,
                     ctx->W, ctx->pflag, ctx->failimage, ctx->gcov, ctx->gcon, ctx->gdet, ctx->conn, ctx->dtbits,
                     ctx->ndt, ctx->dt_state, ctx->counter, ctx->divb, ctx->rlist, ctx->rcount,
-                    ctx->flist, ctx->nfail};
+                    ctx->flist, ctx->nfail, ctx->kerr};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1897,6 +2307,7 @@ int hamr_step(hamr_ctx *ctx, double dt, double *dt_next) {
     if (dt_next) {
         CK(cudaMemcpyAsync(dt_next, ctx->ndt, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
+        if (int rc2 = check_kerr(ctx)) return rc2;
         if (!(*dt_next > 0) || !isfinite(*dt_next)) {
             ctx->err = "non-finite or non-positive CFL step";
             return HAMR_E_PHYSICS;
@@ -1939,7 +2350,7 @@ int hamr_advance(hamr_ctx *ctx, int nsteps, int interval, double *dt_inout) {
     CK(cudaGraphLaunch(ctx->graph, ctx->stream));
     CK(cudaMemcpyAsync(dt_inout, ctx->dt_state, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    return HAMR_OK;
+    return check_kerr(ctx);
 }
 
 int hamr_profile_step(hamr_ctx *ctx, double dt, int reps, double *ms, int nslots) {
@@ -2065,6 +2476,7 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
     // the same dimension bookkeeping as hamr_ctx_create
     hamr_ctx c{};   // value-initialised: every field not set below is zero
     c.rows_min = 1L << 60;   // blocks this small keep one thread per face
+    c.cons_tma = false;      // the update without the bulk-copy staging (no error word here)
     c.prm = *prm;
     Dims &d = c.d;
     d.n1 = prm->n1; d.n2 = prm->n2; d.n3 = prm->n3;

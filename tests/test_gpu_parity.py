@@ -436,3 +436,56 @@ def test_benchmark_size_strict_c3_one_step():
     assert field_rel_err(blk, ps, s, "ps").max() <= 1e-14
     assert abs(dn_gpu - dn_orc) <= 1e-14 * dn_orc
     blk.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("shape", [(24, 16, 8), (64, 40, 48), (50, 18, 70)])
+def test_fused_ct_matches_separate_kernels(precision, shape, monkeypatch):
+    """The fused constrained-transport kernel (centre EMFs, edge EMFs and the
+    face update in one pass, polar rows after the phi average; selected with
+    HAMR_CT_FUSED=1) against the three separate kernels: bit for bit, over
+    blocks that span several (j, z) tiles and x1 chunks, with ragged tile
+    edges. Strict build: with multiply-add contraction the compiler may fuse
+    the same expression differently in two kernels, so only the build without
+    it is bitwise comparable."""
+    from hamr_gamma_wind_b200.api import Block
+    pb = problems.fm_torus(*shape, rout=40.0)
+    out = {}
+    for fused in ("1", "0"):
+        monkeypatch.setenv("HAMR_CT_FUSED", fused)
+        blk = Block(**pb.block_kwargs(), precision=precision, strict=True)
+        blk.set_geometry(pb.geo)
+        blk.upload(pb.p, pb.ps)
+        blk.bound()
+        dt = 0.2 * min(pb.dx[:2])
+        for _ in range(3):
+            dt = min(blk.step(dt), 1.3 * dt)
+        out[fused] = blk.download()
+        blk.close()
+    assert np.array_equal(out["1"][0], out["0"][0])
+    assert np.array_equal(out["1"][1], out["0"][1])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("shape", [(24, 16, 32), (20, 12, 300), (16, 10, 37)])
+def test_tma_staged_update_matches_direct_loads(precision, shape, monkeypatch):
+    """The conserved update with its flux operands staged by bulk copies (one
+    row of zones per CTA, rows longer than 256 zones in equal pieces, ragged
+    16-byte windows) against the update that loads them directly: bit for
+    bit over three steps (strict build, as above)."""
+    from hamr_gamma_wind_b200.api import Block
+    pb = problems.fm_torus(*shape, rout=40.0)
+    out = {}
+    for tma in ("1", "0"):
+        monkeypatch.setenv("HAMR_CONS_TMA", tma)
+        blk = Block(**pb.block_kwargs(), precision=precision, strict=True)
+        blk.set_geometry(pb.geo)
+        blk.upload(pb.p, pb.ps)
+        blk.bound()
+        dt = 0.2 * min(pb.dx[:2])
+        for _ in range(3):
+            dt = min(blk.step(dt), 1.3 * dt)
+        out[tma] = blk.download()
+        blk.close()
+    assert np.array_equal(out["1"][0], out["0"][0])
+    assert np.array_equal(out["1"][1], out["0"][1])
