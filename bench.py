@@ -389,18 +389,25 @@ def run_ours(args):
     finite = bool(np.isfinite(blk.active(p_end)).all())
     blk.close()
 
+    # untimed blocks: a failure in one is reported in the line, not fatal
     accuracy = None
     if not args.no_accuracy and rank == 0:
-        accuracy = _accuracy_block(pb, args, stream)
+        try:
+            accuracy = _accuracy_block(pb, args, stream)
+        except Exception as exc:
+            accuracy = {"error": f"{type(exc).__name__}: {exc}"}
     adjoint = None
     if not args.no_adjoint and rank == 0:
-        adjoint = _adjoint_block(args, fd_directions=8, tlm_directions=7)
+        try:
+            adjoint = _adjoint_block(args, fd_directions=8, tlm_directions=7)
+        except Exception as exc:
+            adjoint = {"error": f"{type(exc).__name__}: {exc}"}
         torch.cuda.set_stream(stream)
     cb = None
     if rank == 0:
         try:
             cb, orc, first = cpu_sample(pb, warmup=1, steps=2, budget_s=args.cpu_budget)
-            if accuracy is not None:
+            if accuracy is not None and "error" not in accuracy:
                 accuracy.update(_step1_vs_oracle(pb, first, stream))
         except Exception as exc:  # the oracle is test infrastructure; report, do not fail the bench
             cb = {"value": None, "error": str(exc)}

@@ -11,11 +11,12 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); runs the CUDA path")
-    # the oracle restatement is plain C and is rebuilt here when missing
-    lib = os.path.join(ROOT, "oracle", "liboracle.so")
-    if not os.path.exists(lib):
-        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "liboracle.so"], check=True,
-                       stdout=subprocess.DEVNULL)
+    # the oracle restatement (plain C, and its FMA and dual-number builds) is
+    # rebuilt here when missing
+    for name in ("liboracle.so", "liboracle_fma.so", "liboracle_dual.so"):
+        if not os.path.exists(os.path.join(ROOT, "oracle", name)):
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), name], check=True,
+                           stdout=subprocess.DEVNULL)
 
 
 def pytest_collection_modifyitems(config, items):
