@@ -617,23 +617,23 @@ __device__ __forceinline__ void face_update_eval(const Dims &d, const Geom &m, c
         const double gdf = __ldg(&m.gdet[FACE1 * d.gs + gi]);
         double temp = 0.;
         temp += 1.0 / ((double)1) * psi[c] * gdf;
-        temp += -Dt / ((double)1 * d.dx2) * (E(3, 0, 1, 0) - E(3, 0, 0, 0));
-        if (d.ng3 > 0) temp += Dt / ((double)1 * d.dx3) * (E(2, 0, 0, 1) - E(2, 0, 0, 0));
+        temp += div_rcp(-Dt, d.dx2, d.rdx2) * (E(3, 0, 1, 0) - E(3, 0, 0, 0));
+        if (d.ng3 > 0) temp += div_rcp(Dt, d.dx3, d.rdx3) * (E(2, 0, 0, 1) - E(2, 0, 0, 0));
         psf[c] = temp / gdf;
     }
     if ((faces & 4) && d.ng3 > 0 && i < d.n1 + d.ng1 && j < d.n2 + d.ng2 && z < d.n3 + d.ng3 + d.d3) {
         const double gdf = __ldg(&m.gdet[FACE3 * d.gs + gi]);
         double temp = psi[2 * ks + c] * gdf;
-        temp += -Dt / d.dx1 * (E(2, 1, 0, 0) - E(2, 0, 0, 0));
-        temp += Dt / d.dx2 * (E(1, 0, 1, 0) - E(1, 0, 0, 0));
+        temp += div_rcp(-Dt, d.dx1, d.rdx1) * (E(2, 1, 0, 0) - E(2, 0, 0, 0));
+        temp += div_rcp(Dt, d.dx2, d.rdx2) * (E(1, 0, 1, 0) - E(1, 0, 0, 0));
         psf[2 * ks + c] = temp / gdf;
     }
     if ((faces & 2) && i < d.n1 + d.ng1 && j < d.n2 + d.ng2 + d.d2 && z < d.n3 + d.ng3) {
         const double gdf = __ldg(&m.gdet[FACE2 * d.gs + gi]);
         double temp = 0.;
         temp += 1.0 / ((double)1) * psi[1 * ks + c] * gdf;
-        temp += Dt / ((double)1 * d.dx1) * (E(3, 1, 0, 0) - E(3, 0, 0, 0));
-        if (d.ng3 > 0) temp += -Dt / ((double)1 * d.dx3) * (E(1, 0, 0, 1) - E(1, 0, 0, 0));
+        temp += div_rcp(Dt, d.dx1, d.rdx1) * (E(3, 1, 0, 0) - E(3, 0, 0, 0));
+        if (d.ng3 > 0) temp += div_rcp(-Dt, d.dx3, d.rdx3) * (E(1, 0, 0, 1) - E(1, 0, 0, 0));
         psf[1 * ks + c] = temp / gdf;
     }
 }
@@ -1063,10 +1063,11 @@ __device__ __forceinline__ void invert_zone(const Dims &d, const Geo<double> &gm
 }
 
 // build option: minimum resident blocks of 128 threads per SM for the
-// inversion kernel (caps its registers per thread; on the 384 x 192 x 192
-// torus 6 blocks beat 5 by 6 % and 4 by 8 %)
+// inversion kernels (caps their registers per thread; on the 384 x 192 x 192
+// torus, per step, for the primary-solver kernel: 8 blocks 3.18 ms (mixed
+// step) / 3.07 ms (FP64), 7: 3.34 / 3.21, 6: 3.36 / 3.21)
 #ifndef HAMR_UPD_MINB
-#define HAMR_UPD_MINB 6
+#define HAMR_UPD_MINB 8
 #endif
 
 // The update in two kernels, so that each holds fewer registers and more

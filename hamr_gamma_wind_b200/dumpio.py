@@ -68,13 +68,14 @@ class Params:
     Rin: float = 0.0
     Rout: float = 0.0
     R0: float = 0.0            # mdot in CALC_MDOT builds
-    density: float = 1.0       # MASS_DENSITY_SCALE
+    # MASS_DENSITY_SCALE of the torus build (config.h:804, the M87 scaling)
+    density: float = 0.001 * 0.00001 * 0.0000000002 * 3.1 * 0.000001 * 0.1 / 30.0
     lim: int = 0
     stag: int = 1              # STAGGERED
     dump_cnt_reduced: int = 0
-    f1: int = 1
-    f2: int = 1
-    f3: int = 1
+    f1: int = 2                # REDUCE_FACTOR1-3 (config.h:578-580)
+    f2: int = 2
+    f3: int = 2
     r1: int = 1
     r2: int = 1
     r3: int = 1
@@ -207,6 +208,10 @@ def restart_state(pb_like, arr, geo):
 
 def params_for(pb_like, t=0.0, nstep=0, dt=0.0, spin=0.0, rin=0.0, rout=0.0, tf=0.0, startx=None, **kw) -> Params:
     sx = startx if startx is not None else getattr(pb_like, "startx", (0.0, 0.0, 0.0, 0.0))
+    # REF_d is 0 for a direction of one zone (config.h:373-387)
+    kw.setdefault("r1", int(pb_like.n1 > 1))
+    kw.setdefault("r2", int(pb_like.n2 > 1))
+    kw.setdefault("r3", int(pb_like.n3 > 1))
     return Params(t=t, nstep=nstep, dt=dt, BS1=pb_like.n1, BS2=pb_like.n2, BS3=pb_like.n3,
                   startx1=float(sx[1]), startx2=float(sx[2]), startx3=float(sx[3]),
                   dx1=float(pb_like.dx[0]), dx2=float(pb_like.dx[1]), dx3=float(pb_like.dx[2]),

@@ -138,6 +138,56 @@ def entropy_wave(n: int, amp: float = 1e-3, v0: float = 0.5, gam: float = 5.0 / 
                    False, geo, p, ps, coords="cartesian")
 
 
+# ------------------------------------------------------- linear MHD modes
+# 3-D (1,1,1) plane waves on the uniform state rho = 1, u = 1, B = (1, 0, 0):
+# frequency and eigenvector (drho, du, du1, du2, du3, dB1, dB2, dB3) per mode
+# (init_entwave, init_tests.c:1054-1156). The frequencies are those of
+# gamma = 4/3 (the Alfven one is 2 pi sqrt(3) v_A with v_A^2 = (1/3) /
+# (rho + gamma u + b^2)); the reference's config.h sets GAMMA = 5/3, for which
+# these vectors are not eigenmodes, so linear_mode uses 4/3.
+LINEAR_MODES = {
+    "entropy": (2. * np.pi / 5., (1., 0., 0., 0., 0., 0., 0., 0.)),
+    "slow": (2.35896379113, (0.556500332363, 0.742000443151, -0.282334999306, 0.0367010491491, 0.0367010491491,
+                             -0.195509141461, 0.0977545707307, 0.0977545707307)),
+    "alfven": (-3.44144232573, (0., 0., 0., -0.339683110243, 0.339683110243, 0., 0.620173672946, -0.620173672946)),
+    "fast": (6.92915162882, (0.481846076323, 0.642461435098, -0.0832240462505, -0.224080007379, -0.224080007379,
+                             0.406380545676, -0.203190272838, -0.203190272838)),
+}
+
+
+def linear_mode(n: int, mode: str = "fast", amp: float = 1.e-5, gam: float = 4.0 / 3.0, cour: float = 0.4,
+                ng: int = 3) -> Problem:
+    """Linear MHD eigenmode on the periodic unit cube in Minkowski space, n^3
+    zones, wavevector 2 pi (1, 1, 1): primitives rho0 + drho cos(k.X), ... at
+    zone centres, the face field at the faces (init_entwave,
+    init_tests.c:1253-1289). After one period 2 pi / |omega| (the reference's
+    tf) the exact solution is the initial state again."""
+    omega, vec = LINEAR_MODES[mode]
+    ks, p, ps = _alloc(n, n, n, ng)
+    dx = (1.0 / n, 1.0 / n, 1.0 / n)
+    geo = build_geometry("cartesian", 0.0, n, n, n, [0.0, 0.0, 0.0, 0.0], [0.0, *dx], ng)
+    g = n + 2 * ng
+    c = (np.arange(g) - ng + 0.5) / n
+    f = (np.arange(g) - ng) / n
+    k1 = k2 = k3 = 2.0 * np.pi
+
+    def cosk(x1, x2, x3):
+        return amp * np.cos(k1 * x1[:, None, None] + k2 * x2[None, :, None] + k3 * x3[None, None, :])
+
+    P = p.reshape(NPR, ks)[:, :g ** 3].reshape(NPR, g, g, g)
+    S = ps.reshape(3, ks)[:, :g ** 3].reshape(3, g, g, g)
+    m = cosk(c, c, c)
+    base = (1.0, 1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0)
+    for k in range(8):
+        P[k] = base[k] + vec[k] * m
+    P[KTOT] = (gam - 1.0) * P[UU] * P[RHO] ** (-gam)
+    S[0] = base[5] + vec[5] * cosk(f, c, c)
+    S[1] = base[6] + vec[6] * cosk(c, f, c)
+    S[2] = base[7] + vec[7] * cosk(c, c, f)
+    return Problem(n, n, n, ng, ks, geo.gsize, dx, gam, cour, ("periodic", "periodic", "periodic"), (0, 0), False,
+                   geo, p, ps, coords="cartesian")
+
+
 # ---------------------------------------------------------------- FM torus
 def lfish(a, r):
     """Specific angular momentum of the Fishbone-Moncrief torus with pressure

@@ -438,3 +438,24 @@ def ref_utoprim(variant, name, U, gcov10, gcon10, gdet, prim):
     rc = getattr(ref(variant), "ref_utoprim_" + name)(_ptr(U), _ptr(np.asarray(gcov10, float)),
                                                      _ptr(np.asarray(gcon10, float)), gdet, _ptr(prim))
     return rc, prim
+
+
+def ref_dump_available(variant: str) -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", f"libref_dump_{variant}.so"))
+
+
+def ref_dump_files(variant, p, ps, ksize, geo, prm_d, prm_i, param_path, dump_path, rdump_path):
+    """The reference's own writers (dump_params, dump_block,
+    rdump_block_write; oracle/ref_dumpio.c) on one block of a compile-time
+    variant: state (p, ps) and metric tables in the device layout; prm_d = (t,
+    dt, DTd, DTl, startx1-3, dx1-3, tf, a, gam, cour, Rin, Rout, R0), prm_i =
+    (nstep, dump_cnt, rdump_cnt, failed, lim, dump_cnt_reduced)."""
+    L = ctypes.CDLL(os.path.join(HERE, "_ref", f"libref_dump_{variant}.so"))
+    L.ref_dump_files.restype = _i
+    d = np.ascontiguousarray(prm_d, dtype=np.float64)
+    i = np.ascontiguousarray(prm_i, dtype=np.int32)
+    rc = L.ref_dump_files(_ptr(np.ascontiguousarray(p)), _ptr(np.ascontiguousarray(ps)), ctypes.c_long(ksize),
+                          _ptr(geo.gcov), _ptr(geo.gcon), _ptr(geo.gdet), ctypes.c_long(geo.gsize), _ptr(d), _ptr(i),
+                          param_path.encode(), dump_path.encode(), rdump_path.encode())
+    if rc:
+        raise RuntimeError(f"ref_dump_files: {rc}")

@@ -6,4 +6,8 @@
 typedef void *gpuStream_t;
 typedef void *gpuEvent_t;
 typedef int gpuError_t;
+/* copy kinds named by the reference's restart.c (its device paths are never
+ * called in the host builds) */
+#define gpuMemcpyHostToDevice 1
+#define gpuMemcpyDeviceToHost 2
 #endif

@@ -22,7 +22,12 @@ Fixtures (numpy .npz, compressed):
                   half sub-step of the reference kernels on a seeded block
                   with planted failed zones; active zones only.
 
-`python tests/golden/make_golden.py repair` writes ref_repair.npz alone.
+  ref_dump_t2.npz the parameter header, float dump and double restart files the
+                  reference's own writers (dump_params, dump_block,
+                  rdump_block_write; oracle/ref_dumpio.c) produce for the 2-D
+                  variant's block with a seeded generic state (dump_case)
+`python tests/golden/make_golden.py repair` writes ref_repair.npz alone,
+`... dump` ref_dump_t2.npz alone.
 """
 import hashlib
 import os
@@ -194,9 +199,48 @@ def repair_fixture():
     return out
 
 
+def dump_case(v):
+    """The block of variant v with a generic state (torus, seeded 1e-3 relative
+    perturbation of every entry, ghosts included) and run parameters for the
+    dump and restart comparison; returns (problem, Params, prm_d, prm_i)."""
+    from hamr_gamma_wind_b200 import dumpio, problems
+    dims, _ = O.ref_dims(v) if O.ref_available(v) else (DUMP_DIMS[v], None)
+    n1, n2, n3 = (int(x) for x in dims[:3])
+    pb = problems.fm_torus(n1, n2, n3, rout=40.0)
+    rng = np.random.default_rng(3)
+    pb.p[:] *= 1.0 + 1e-3 * rng.standard_normal(pb.p.shape)
+    pb.ps[:] *= 1.0 + 1e-3 * rng.standard_normal(pb.ps.shape)
+    prm = dumpio.params_for(pb, t=12.5, nstep=40, dt=0.01, spin=0.9375, rin=1.2, rout=40.0, tf=2000.0)
+    prm.dump_cnt, prm.rdump_cnt, prm.lim = 3, 7, 1
+    prm_d = [prm.t, prm.dt, prm.DTd, prm.DTl, prm.startx1, prm.startx2, prm.startx3, prm.dx1, prm.dx2, prm.dx3,
+             prm.tf, prm.a, prm.gam, prm.cour, prm.Rin, prm.Rout, prm.R0]
+    prm_i = [prm.nstep, prm.dump_cnt, prm.rdump_cnt, prm.failed, prm.lim, prm.dump_cnt_reduced]
+    return pb, prm, prm_d, prm_i
+
+
+DUMP_DIMS = {"t3": (16, 8, 8), "t2": (24, 24, 1)}
+
+
+def dump_fixture(v):
+    """The reference writers' files (dump_params, dump_block,
+    rdump_block_write) for dump_case(v), as byte arrays, and a digest of the
+    inputs."""
+    import tempfile
+    pb, prm, prm_d, prm_i = dump_case(v)
+    d = tempfile.mkdtemp()
+    paths = [os.path.join(d, f) for f in ("parameters", "new_dump0", "rdump0")]
+    O.ref_dump_files(v, pb.p, pb.ps, pb.ksize, pb.geo, prm_d, prm_i, *paths)
+    out = {k: np.frombuffer(open(pth, "rb").read(), np.uint8) for k, pth in zip(("params", "dump", "rdump"), paths)}
+    out["inputs"] = np.array(digest(pb.p, pb.ps, pb.geo.gcov, pb.geo.gcon, pb.geo.gdet))
+    return out
+
+
 def main():
     if sys.argv[1:] == ["repair"]:
         np.savez_compressed(os.path.join(HERE, "ref_repair.npz"), **repair_fixture())
+        return
+    if sys.argv[1:] == ["dump"]:
+        np.savez_compressed(os.path.join(HERE, "ref_dump_t2.npz"), **dump_fixture("t2"))
         return
     for v in ("t3", "t2", "ot"):
         if not O.ref_available(v):
@@ -204,6 +248,7 @@ def main():
         np.savez_compressed(os.path.join(HERE, f"ref_{v}.npz"), **variant_fixture(v))
     np.savez_compressed(os.path.join(HERE, "ref_cells.npz"), **cell_fixture())
     np.savez_compressed(os.path.join(HERE, "ref_repair.npz"), **repair_fixture())
+    np.savez_compressed(os.path.join(HERE, "ref_dump_t2.npz"), **dump_fixture("t2"))
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")

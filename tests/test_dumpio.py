@@ -3,10 +3,12 @@ on the host: the parameter header's byte layout follows dump_params field by
 field, the restart array carries the primitives and the face field times the
 face sqrt(-g) over the ghost-inclusive block, the dump the active zones'
 rho, u, u^mu, B^i in float32."""
+import os
 import struct
 import tempfile
 
 import numpy as np
+import pytest
 
 from hamr_gamma_wind_b200 import dumpio, problems
 
@@ -80,3 +82,51 @@ def test_dump_variables_and_normalisation():
     np.testing.assert_allclose(norm[ng:ng + pb.n1, ng:ng + pb.n2, ng:ng + pb.n3], -1.0, atol=1e-12)
     np.testing.assert_array_equal(arr[..., 2:6], np.moveaxis(uc[:, ng:ng + pb.n1, ng:ng + pb.n2, ng:ng + pb.n3],
                                                              0, -1).astype(np.float32))
+
+
+def _ours(tmp_path, pb, prm):
+    ours = tmp_path / "ours"
+    ddir = dumpio.write_dump(str(ours), pb, pb.p, pb.geo, prm)
+    rdir = dumpio.write_restart(str(ours), pb, pb.p, pb.ps, pb.geo, prm)
+    return (open(f"{ddir}/parameters", "rb").read(), open(f"{ddir}/new_dump0", "rb").read(),
+            open(f"{rdir}/rdump0", "rb").read())
+
+
+def _same_files(ref, ours):
+    """byte for byte, except the 8 bytes of DTr in the header: dump_params
+    writes sizeof(double) bytes from the int DTr (dump.c:216, decs.h:855), so
+    its upper four bytes are whatever follows it in memory"""
+    a, b = ref[0], ours[0]
+    assert len(a) == len(b)
+    dtr = struct.calcsize("<diiidd")   # offset of DTr
+    assert a[:dtr + 4] == b[:dtr + 4] and a[dtr + 8:] == b[dtr + 8:]
+    assert ref[1] == ours[1], "float dump differs"
+    assert ref[2] == ours[2], "restart differs"
+
+
+@pytest.mark.parametrize("variant", ["t3", "t2"])
+def test_files_match_the_reference_writers(variant, tmp_path):
+    """dumpio's parameter header, dump and restart files against the ones the
+    reference's own writers produce (dump_params, dump_block,
+    rdump_block_write from dump.c and restart.c, host-built for the block of
+    the variant, oracle/ref_dumpio.c) for the same state and metric."""
+    from oracle import oracle as O
+    from tests.golden.make_golden import dump_case
+    if not O.ref_dump_available(variant):
+        pytest.skip("reference host build not present")
+    pb, prm, prm_d, prm_i = dump_case(variant)
+    ref = tmp_path / "ref"
+    ref.mkdir()
+    paths = [str(ref / f) for f in ("parameters", "new_dump0", "rdump0")]
+    O.ref_dump_files(variant, pb.p, pb.ps, pb.ksize, pb.geo, prm_d, prm_i, *paths)
+    _same_files([open(pth, "rb").read() for pth in paths], _ours(tmp_path, pb, prm))
+
+
+def test_files_match_the_reference_golden_files(tmp_path):
+    """The same against the committed output of the reference's writers
+    (tests/golden/ref_dump_t2.npz), where the reference is absent."""
+    from tests.golden.make_golden import digest, dump_case
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_dump_t2.npz"))
+    pb, prm, _, _ = dump_case("t2")
+    assert str(g["inputs"]) == digest(pb.p, pb.ps, pb.geo.gcov, pb.geo.gcon, pb.geo.gdet)
+    _same_files([g[k].tobytes() for k in ("params", "dump", "rdump")], _ours(tmp_path, pb, prm))

@@ -1,0 +1,82 @@
+"""Known-answer tests of the reference (init_tests.c): linear MHD eigenmodes
+return to their initial state after one period, with second-order
+convergence of the L1 error; and the Orszag-Tang configuration of the
+benchmark set (128 x 128, 500 steps) against the oracle.
+
+Modes: 3-D (1,1,1) plane waves on rho = 1, u = 1, B = (1, 0, 0) in a periodic
+Minkowski cube, amplitude 1e-5, run for one period 2 pi / |omega| with fixed
+steps of about 0.4 dx (the reference's tf, init_tests.c:1257). The error is the
+mean absolute deviation of the eight primitives from the initial state over
+the amplitude. Measured on the oracle (N = 8, 16, 32): ratios 3.1-4.7 per
+doubling; PPM's extremum clipping at the cosine's crests keeps the order a
+little under two at coarse N."""
+import numpy as np
+import pytest
+
+from hamr_gamma_wind_b200 import problems
+from hamr_gamma_wind_b200.api import Block
+from tests._gpu import field_rel_err, make_pair, oracle_step
+
+pytestmark = pytest.mark.gpu
+
+
+def _period_steps(pb, mode):
+    omega, _ = problems.LINEAR_MODES[mode]
+    tf = 2 * np.pi / abs(omega)
+    nst = int(np.ceil(tf / (0.4 * pb.dx[0])))
+    return nst, tf / nst
+
+
+def _mode_error(n, mode):
+    pb = problems.linear_mode(n, mode)
+    nst, dt = _period_steps(pb, mode)
+    blk = Block(**pb.block_kwargs(), strict=True)
+    blk.set_geometry(pb.geo)
+    blk.upload(pb.p, pb.ps)
+    blk.bound()
+    for _ in range(nst):
+        blk.step(dt)
+    p, _ = blk.download()
+    blk.close()
+    return np.abs(pb.active(p)[:8] - pb.active(pb.p)[:8]).mean() / 1e-5
+
+
+@pytest.mark.parametrize("mode", ["slow", "alfven", "fast"])
+def test_linear_mode_second_order(mode):
+    e16, e32, e64 = (_mode_error(n, mode) for n in (16, 32, 64))
+    r1, r2 = e16 / e32, e32 / e64
+    assert e64 < 2e-3, (e16, e32, e64)
+    assert r1 >= 2.9 and r2 >= 3.4, (mode, e16, e32, e64, r1, r2)
+
+
+@pytest.mark.parametrize("mode", ["slow", "alfven", "fast"])
+def test_linear_mode_matches_oracle(mode):
+    """One full period at 16^3 against the oracle, strict build."""
+    pb = problems.linear_mode(16, mode)
+    nst, dt = _period_steps(pb, mode)
+    blk, s = make_pair(pb, strict=True)
+    for _ in range(nst):
+        blk.step(dt)
+        oracle_step(s, dt)
+    p, ps = blk.download()
+    assert field_rel_err(blk, p, s, "p").max() <= 1e-13
+    assert field_rel_err(blk, ps, s, "ps").max() <= 1e-13
+    blk.close()
+
+
+def test_orszag_tang_128_500_steps_against_oracle():
+    """The benchmark set's 2-D configuration: Orszag-Tang 128 x 128, CFL 0.5,
+    500 steps with the CFL step-size rule, strict build against the oracle."""
+    pb = problems.orszag_tang(128)
+    blk, s = make_pair(pb, strict=True)
+    dt = 0.2 * min(pb.dx[:2])
+    for _ in range(500):
+        dn = blk.step(dt)
+        dn_o = oracle_step(s, dt)
+        assert abs(dn - dn_o) <= 1e-9 * dn_o
+        dt = min(dn_o, 1.3 * dt)
+    p, ps = blk.download()
+    e, eb = field_rel_err(blk, p, s, "p"), field_rel_err(blk, ps, s, "ps")
+    assert e.max() <= 1e-9 and eb.max() <= 1e-9, (e, eb)
+    assert np.isfinite(p).all()
+    blk.close()
