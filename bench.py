@@ -76,7 +76,11 @@ def kernel_bytes(slot: str, d: dict, width: float = 8.0) -> float:
              centre metric and connection (61 words) per column;
     invert   per zone: 9 primitives (initial guess) + 7 conserved values + 3 face
              fields read, 9 primitives and 1 int flag written, plus the centre
-             metric and face volumes (23 words) per column."""
+             metric and face volumes (23 words) per column;
+    emf_centre per zone (one ghost layer around): 3 velocities and 3 face
+             fields read, 3 centre EMFs written;
+    emf_edge   per edge: 3 centre EMFs and 9 face fluxes read, 3 EMFs written;
+    face_update per face triple: 3 EMFs read, old and new face fields."""
     n1, n2, n3 = d["n1"], d["n2"], d["n3"]
     if slot.startswith("flux"):
         k = int(slot[-1])
@@ -88,12 +92,57 @@ def kernel_bytes(slot: str, d: dict, width: float = 8.0) -> float:
     if slot == "invert":
         return (28 * 8.0 + 4) * n1 * n2 * n3 + 23 * 8.0 * n1 * n2
     if slot == "emf_centre":
-        return (9 * 8.0 + 3 * width) * (n1 + 2) * (n2 + 2) * (n3 + 2)
+        return (6 * 8.0 + 3 * width) * (n1 + 2) * (n2 + 2) * (n3 + 2)
     if slot == "emf_edge":
         return 15 * width * (n1 + 1) * (n2 + 1) * (n3 + 1)
     if slot == "face_update":
         return (6 * 8.0 + 3 * width) * (n1 + 1) * (n2 + 1) * (n3 + 1)
     return 0.0
+
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per active zone of
+# one launch, from single-launch ncu captures of each kernel on the 3-D torus
+# 192 x 96 x 64 (profiles/k_*_torus_192x96x64.md; inputs larger than L2, caches
+# flushed before the launch). Every kernel's traffic grows with the number of
+# zones (plus a per-column metric term under 1 %), so a launch on another block
+# moves these figures times its zones. flux1 and flux2 share the row kernel.
+NCU_DRAM_BYTES_PER_ZONE = {
+    "fp64": {"flux1": 205.0, "flux2": 205.0, "flux3": 158.3, "update": 458.5, "invert": 191.5,
+             "emf_centre": 62.5, "emf_edge": 125.6, "face_update": 54.2},
+    "mixed": {"flux1": 125.2, "flux2": 125.2, "flux3": 105.1, "update": 317.2, "invert": 191.1,
+              "emf_centre": 58.1, "emf_edge": 57.3, "face_update": 40.2},
+}
+
+# what limits each kernel group, read from the same captures
+KERNEL_LIMITER = {
+    "flux1": "latency: PPM stencil loads (long scoreboard) and dependent FP chains",
+    "flux2": "latency: PPM stencil loads (long scoreboard) and dependent FP chains",
+    "flux3": "latency: dependent FP64/FP32 chains of the four flux evaluations per face",
+    "update": "FP64 fixed-latency chains after TMA-staged operand loads",
+    "invert": "FP64 dependent Newton iterations (FP64 pipe 45 % active)",
+    "emf_centre": "memory latency (long scoreboard)",
+    "emf_edge": "memory latency (long scoreboard)",
+    "face_update": "memory latency (long scoreboard)",
+}
+
+
+def kernel_rooflines(slots: dict, d: dict, prec: str, hbm: float) -> dict:
+    """Per kernel group, per launch: algorithmic bytes, achieved GB/s over its
+    live CUDA-event time (two launches per step), fraction of the HBM peak,
+    DRAM traffic from the ncu capture scaled to this block, and the limiter."""
+    width = 4.0 if prec == "mixed" else 8.0
+    zones = d["n1"] * d["n2"] * d["n3"]
+    tab = NCU_DRAM_BYTES_PER_ZONE.get("mixed" if prec == "mixed" else "fp64", {})
+    out = {}
+    for slot, ms in slots.items():
+        kb = kernel_bytes(slot, d, width)
+        if kb <= 0 or ms <= 0:
+            continue
+        gbs = 2 * kb / (ms * 1e-3) / 1e9
+        out[slot] = {"ms_per_step": ms, "algorithmic_bytes": kb, "achieved_gbs": gbs, "frac": gbs / hbm,
+                     "traffic": tab[slot] * zones if slot in tab else None,
+                     "limiter": KERNEL_LIMITER.get(slot)}
+    return out
 
 
 def launches_per_step(pb) -> int:
@@ -364,6 +413,7 @@ def run_ours(args):
     width = 4.0 if head == "mixed" else 8.0
     kb = kernel_bytes(top, wl, width)
     achieved = 2 * kb / (slots[top] * 1e-3) / 1e9 if slots[top] > 0 else 0.0
+    kroof = kernel_rooflines(slots, wl, head, hbm)
     ms = runs[head]["ms"]
     step_gbs = algorithmic_bytes_per_cell_update(pb.n3) * cells / (ms * 1e-3 / args.steps) / 1e9
 
@@ -427,7 +477,11 @@ def run_ours(args):
                            for k, v in runs.items()},
             "gpu_launches": args.steps * launches_per_step(pb) + 1,
             "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None, "peak_source": peak_src},
+                         "frac": achieved / hbm, "traffic": kroof.get(top, {}).get("traffic"),
+                         "algorithmic_bytes": kb, "limiter": KERNEL_LIMITER.get(top),
+                         "traffic_source": "ncu DRAM bytes per zone, torus 192x96x64 capture, times zones",
+                         "peak_source": peak_src},
+            "kernel_rooflines": kroof,
             "step_roofline": {"algorithmic_bytes_per_cell_update": algorithmic_bytes_per_cell_update(pb.n3),
                               "achieved_gbs": step_gbs, "frac": step_gbs / hbm},
             "clocks": runs[head]["clocks"],
