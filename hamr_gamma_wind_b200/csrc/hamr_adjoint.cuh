@@ -138,8 +138,8 @@ __device__ __forceinline__ void para_weights(const double *y, bool upper, double
         c1[i] = selc ? 0. : (selm ? gm : -gp);
         c2[i] = selc ? gc : (selm ? 0. : gp);
     }
-    double l = 0.5 * (y[2] + y[1]) - (dq[2] - dq[1]) / 6.0;
-    double r = 0.5 * (y[3] + y[2]) - (dq[3] - dq[2]) / 6.0;
+    double l = 0.5 * (y[2] + y[1]) - div6(dq[2] - dq[1]);   // the forward's edges, bit for bit
+    double r = 0.5 * (y[3] + y[2]) - div6(dq[3] - dq[2]);
     const double s6 = 1. / 6.0;
     double wl[5] = {c0[1] * s6, 0.5 + (c1[1] - c0[2]) * s6, 0.5 + (c2[1] - c1[2]) * s6, -c2[2] * s6, 0.};
     double wr[5] = {0., c0[2] * s6, 0.5 + (c1[2] - c0[3]) * s6, 0.5 + (c2[2] - c1[3]) * s6, -c2[3] * s6};
@@ -269,9 +269,10 @@ __device__ __forceinline__ void state_back(const double *pr, const Geo<double> &
     }
     // b^j = (B^j + b^0 u^j) / u^0, then b^0 = B^i u_i
     double Bb[3];
+    const double ru0 = 1. / q.ucon[0];
 #pragma unroll
     for (int j = 1; j < 4; j++) {
-        const double bj = a.bcon[j] / q.ucon[0];
+        const double bj = a.bcon[j] * ru0;
         Bb[j - 1] = bj;
         a.bcon[0] += bj * q.ucon[j];
         a.ucon[j] += bj * q.bcon[0];
@@ -290,10 +291,11 @@ __device__ __forceinline__ void state_back(const double *pr, const Geo<double> &
         for (int mu = 0; mu < 4; mu++) a.ucon[mu] += t[mu];
     }
     // u^0 = gamma / alpha, u^j = u~^j - gamma beta^j / alpha, beta^j = g^{0j} alpha^2
-    const double alpha = 1. / d_sqrt(-gn[0]);
-    double gb = a.ucon[0] / alpha;
+    // (1/alpha = sqrt(-g^tt); beta^j / alpha = g^{0j} alpha)
+    const double sg = d_sqrt(-gn[0]), alpha = 1. / sg;
+    double gb = a.ucon[0] * sg;
 #pragma unroll
-    for (int j = 1; j < 4; j++) gb -= a.ucon[j] * (gn[j] * alpha * alpha) / alpha;
+    for (int j = 1; j < 4; j++) gb -= a.ucon[j] * (gn[j] * alpha);
     double ub3[3] = {a.ucon[1], a.ucon[2], a.ucon[3]};
     if (f.gfree) {
         const double u1 = pr[U1], u2 = pr[U2], u3 = pr[U3];
@@ -330,8 +332,9 @@ __device__ void state_vjp_from(const double *pr, const Geo<double> &gm, double g
         flux_rev<DIR>(pr, q, gm.g, eta, f.K, fb, a);
         // fast speeds: the roots of A v^2 - B v + C = 0 (forward in primtoflux)
         const double Acon_0 = gn[DIR], Asq = gn[DIR == 1 ? 4 : (DIR == 2 ? 7 : 9)], Bsq = gn[0], AB = Acon_0;
-        const double cs2 = gam * (gam - 1.) * u / w;
-        const double va2 = bsq / eta;
+        const double rw = 1. / w, reta = 1. / eta;
+        const double cs2 = gam * (gam - 1.) * u * rw;
+        const double va2 = bsq * reta;
         double cms2 = cs2 + va2 - cs2 * va2;
         const bool cfree = !(cms2 < 0.) && !(cms2 > 1.);
         if (cms2 < 0.) cms2 = SMALL_D;
@@ -345,12 +348,13 @@ __device__ void state_vjp_from(const double *pr, const Geo<double> &gm, double g
         const bool dfree = !(discr < 0.);
         if (!dfree) discr = 0.;
         const double sq = d_sqrt(discr);
-        const double vp = -(-B + sq) / (2. * A), vm = -(-B - sq) / (2. * A);
+        const double rA = 1. / A, r2A = 0.5 * rA;
+        const double vp = -(-B + sq) * r2A, vm = -(-B - sq) * r2A;
         const double vpb = (vp > vm ? cmxb : 0.) + (vp < vm ? cmnb : 0.);
         const double vmb = (vp > vm ? 0. : cmxb) + (vp < vm ? 0. : cmnb);
-        double Bb = (vpb + vmb) / (2. * A);
-        const double sb = (vmb - vpb) / (2. * A);
-        double Ab = -(vpb * vp + vmb * vm) / A, Cb = 0.;
+        double Bb = (vpb + vmb) * r2A;
+        const double sb = (vmb - vpb) * r2A;
+        double Ab = -(vpb * vp + vmb * vm) * rA, Cb = 0.;
         if (dfree && sq > 0.) {
             const double Db = 0.5 * sb / sq;
             Bb += 2. * B * Db;
@@ -363,11 +367,11 @@ __device__ void state_vjp_from(const double *pr, const Geo<double> &gm, double g
         if (cfree) {
             const double cmsb = -(Bsq + Bu2) * Ab - 2. * (AB + AuBu) * Bb - (Asq + Au2) * Cb;
             // 1 - va2 = w / eta, without the cancellation where b^2 >> w
-            const double cs2b = cmsb * (w / eta), va2b = cmsb * (1. - cs2);
-            a.bsq += va2b / eta;
-            a.eta -= va2b * va2 / eta;
-            const double numb = cs2b / w;
-            a.w -= cs2b * cs2 / w;
+            const double cs2b = cmsb * (w * reta), va2b = cmsb * (1. - cs2);
+            a.bsq += va2b * reta;
+            a.eta -= va2b * va2 * reta;
+            const double numb = cs2b * rw;
+            a.w -= cs2b * cs2 * rw;
             a.u += numb * gam * (gam - 1.);
             a.gam += numb * u * (2. * gam - 1.);
         }
@@ -482,7 +486,9 @@ __device__ __forceinline__ void adj_flux_face(const Dims &d, const Geom &m, cons
             const bool take_rn = !(in_n > -cmin_r);
             const double on = take_rn ? -cmin_r : in_n;
             const double cmin = on < 0. ? -on : on;
-            const double D = cmax + cmin + SMALL_D;
+            // (the cotangents need no bit-level agreement with a reference:
+            // one reciprocal of the HLL denominator for all 45 quotients)
+            const double rD = 1. / (cmax + cmin + SMALL_D);
             // this side's flux and conserved-variable cotangents, and the
             // speeds' (which need both sides' fluxes)
             double tfb[NPR], tub[NPR], cmaxb = 0., cminb = 0.;
@@ -491,11 +497,12 @@ __device__ __forceinline__ void adj_flux_face(const Dims &d, const Geom &m, cons
                 const double fo = __shfl_xor_sync(tm, ta[k], 1), uo = __shfl_xor_sync(tm, tb[k], 1);
                 const double t1 = side ? fo : ta[k], t2 = side ? uo : tb[k];
                 const double t3 = side ? ta[k] : fo, t4 = side ? tb[k] : uo;
-                const double Fk = (cmax * t1 + cmin * t3 - cmax * cmin * (t4 - t2)) / D;
-                tfb[k] = side ? Fb[k] * cmin / D : Fb[k] * cmax / D;
-                tub[k] = side ? -Fb[k] * cmax * cmin / D : Fb[k] * cmax * cmin / D;
-                cmaxb += Fb[k] * ((t1 - cmin * (t4 - t2)) - Fk) / D;
-                cminb += Fb[k] * ((t3 - cmax * (t4 - t2)) - Fk) / D;
+                const double Fk = (cmax * t1 + cmin * t3 - cmax * cmin * (t4 - t2)) * rD;
+                const double Fbr = Fb[k] * rD;
+                tfb[k] = side ? Fbr * cmin : Fbr * cmax;
+                tub[k] = side ? -Fbr * cmax * cmin : Fbr * cmax * cmin;
+                cmaxb += Fbr * ((t1 - cmin * (t4 - t2)) - Fk);
+                cminb += Fbr * ((t3 - cmax * (t4 - t2)) - Fk);
             }
             const double sx = ox < 0. ? -1. : 1., sn = on < 0. ? -1. : 1.;
             double cmxb = 0., cmnb = 0.;

@@ -45,12 +45,17 @@ struct Dims {
     long ks, gs;
     double dx1, dx2, dx3, gam, cour;
     double rdx1, rdx2, rdx3;   // 1/dx, correctly rounded on the host (exact divisions by dx, div_rcp)
+    double rgam;               // 1/gam, likewise (the inversion's divisions by gamma)
     int pole1, pole2, bc1, bc2, bc3, ct_upwind, inversion, recon, riemann;
     int halo;   // x1 sides filled by a neighbouring block (bit 0 lower, bit 1 upper)
 };
 
 struct Geom {
     const double *gcov, *gcon, *gdet, *conn;
+    // per (i, j) column at the zone centre, when tabulated (else null): 1/gdet,
+    // the lapse 1/sqrt(-g^tt) and n_t = -sqrt(-1/g^tt), each computed with the
+    // inversion's own operations (k_inv_tab), planes of gs
+    const double *itab = nullptr;
 };
 
 __device__ __forceinline__ long cix(const Dims &d, int i, int j, int z) { return ((long)i * d.G2 + j) * d.G3 + z; }
@@ -197,9 +202,10 @@ __device__ __forceinline__ double flux_eval(const Dims &d, const Geo<T> &gm, con
     const T cmax = d_fabs(d_max(d_max(T(0.), cmax_l), cmax_r));
     const T cmin = d_fabs(d_max(d_max(T(0.), -cmin_l), -cmin_r));
     const T ctop = d_max(cmax, cmin);
+    const Divisor<T> dh(cmax + cmin + T(SMALL_D));   // the nine HLL quotients share it
 #pragma unroll
     for (int k = 0; k < NPR; k++)
-        F[(long)k * d.ks + c] = (cmax * t1[k] + cmin * t3[k] - cmax * cmin * (t4[k] - t2[k])) / (cmax + cmin + T(SMALL_D));
+        F[(long)k * d.ks + c] = dh.div(cmax * t1[k] + cmin * t3[k] - cmax * cmin * (t4[k] - t2[k]));
     const double v = d.cour * dxd / (double)ctop;
     if (v > 1.e-6 && v < dtf) dtf = v;
     return dtf;
@@ -275,8 +281,19 @@ __host__ __device__ __forceinline__ long n_x3_slots(const Dims &d) {
     return (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3);
 }
 
+// build options: resident blocks per SM for the double and float x3 slot
+// kernels. Measured per 384 x 192 x 192 step: float 10 blocks (48 registers)
+// 2.04 ms, 12: 2.09, 8: 2.14, 6 (80 registers, no spills): 2.54; double 6
+// blocks 8.10 ms, 5: 8.16, 4: 8.16
+#ifndef HAMR_FLUX_X3_MINB
+#define HAMR_FLUX_X3_MINB 6
+#endif
+#ifndef HAMR_FLUX_X3_MINB_F
+#define HAMR_FLUX_X3_MINB_F 10
+#endif
+
 template <typename T, int REC>
-__global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? HAMR_FLUX_MINB : HAMR_FLUX_MINB_F)
+__global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? HAMR_FLUX_X3_MINB : HAMR_FLUX_X3_MINB_F)
     k_flux_x3(const Dims d, const Geom m, const double *__restrict__ pv, const double *__restrict__ ps,
               T *__restrict__ F, unsigned long long *__restrict__ dtbits, int calc_dt) {
     __shared__ T slo[NPR - 1][BLK], shi[NPR - 1][BLK];   // zone edges per slot (B3 skipped)
@@ -327,7 +344,9 @@ __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? HAMR_FLUX_MINB : HAMR_FL
 // build options: faces per row, and minimum resident blocks of 128 threads
 // per SM for the row kernels (FP64, float). Measured on the 384 x 192 x 192
 // torus: rows of 12 beat 6, 8, 24 and 48 (shorter rows: more threads in
-// flight, longer: fewer extra reconstructions); 7 float blocks beat 6.
+// flight, longer: fewer extra reconstructions); 7 float blocks beat 6 and 8,
+// 5 double blocks beat 4. The stencil window (RowWindow) took the float x1 +
+// x2 fluxes from 4.48 to 3.77 ms per step (FP64 13.49 -> 13.36).
 #ifndef HAMR_FLUX_ROW
 #define HAMR_FLUX_ROW 12
 #endif
@@ -346,11 +365,61 @@ __host__ __device__ __forceinline__ long n_flux_rows(const Dims &d) {
     return ((nf + FLUX_ROW - 1) / FLUX_ROW) * nt * (d.n3 + 2 * d.d3);
 }
 
+// A thread's stencil window along its row, in shared memory: the NW zones
+// (5 for PPM, 3 for MC) around the zone being reconstructed, each as its
+// NPR - 1 reconstructed primitives (the normal field component is not
+// reconstructed), converted to T once when loaded. Slot of zone index q along
+// the row: q mod NW. Each thread touches only its own column (threadIdx.x), so
+// no barrier is needed, and consecutive threads hit consecutive banks. Moving
+// to the next face loads one new zone (NPR - 1 values) instead of the whole
+// stencil (NW (NPR - 1) values); the reconstruction sees the same values as
+// zone_edges.
+template <int DIR, typename T, int REC>
+struct RowWindow {
+    static constexpr int NW = (REC & 1) == HAMR_RECON_MC ? 3 : 5;
+    static constexpr int H = NW / 2;
+    static constexpr int NK = NPR - 1;
+    T *w;
+    __device__ __forceinline__ T &at(int slot, int kk) const { return w[(slot * NK + kk) * BLK]; }
+    __device__ __forceinline__ void load(const Dims &d, const double *__restrict__ pv, long cz, int slot) const {
+        int kk = 0;
+#pragma unroll
+        for (int k = 0; k < NPR; k++) {
+            if (k == B1 + DIR - 1) continue;
+            at(slot, kk++) = (T)__ldg(pv + (long)k * d.ks + cz);
+        }
+    }
+    // edges of the zone whose stencil starts in slot s0 (the zone q - H)
+    __device__ __forceinline__ void edges(int s0, T *lo, T *hi) const {
+        int kk = 0;
+#pragma unroll
+        for (int k = 0; k < NPR; k++) {
+            if (k == B1 + DIR - 1) continue;
+            T x[NW];
+#pragma unroll
+            for (int s = 0; s < NW; s++) {
+                const int sl = s0 + s;
+                x[s] = at(sl >= NW ? sl - NW : sl, kk);
+            }
+            if constexpr (NW == 3) {
+                const T temp = T(0.5) * slope_lim(x[0], x[1], x[2]);
+                lo[k] = x[1] - temp;
+                hi[k] = x[1] + temp;
+            } else {
+                para(x, lo[k], hi[k]);
+            }
+            kk++;
+        }
+    }
+};
+
 template <int DIR, typename T, int REC>
 __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? ((REC & 2) != 0 ? HAMR_FLUX_FT_ROWS_MINB : HAMR_FLUX_ROWS_MINB)
                                                          : HAMR_FLUX_ROWS_MINB_F)
     k_flux_rows(const Dims d, const Geom m, const double *__restrict__ pv, const double *__restrict__ ps,
                 T *__restrict__ F, unsigned long long *__restrict__ dtbits, int calc_dt) {
+    using Win = RowWindow<DIR, T, REC>;
+    __shared__ T wbuf[Win::NW * Win::NK * BLK];
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     double dtf = 1.e9;
     if (t < n_flux_rows<DIR>(d)) {
@@ -360,22 +429,30 @@ __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? ((REC & 2) != 0 ? HAMR_F
         const int a = (DIR == 1 ? (d.ng2 - 1) * d.d2 : (d.ng1 - 1) * d.d1) + (int)(r % nt);   // j or i
         const int seg = (int)(r / nt);
         const int nf = DIR == 1 ? d.n1 + 2 * d.d1 - 1 : d.n2 + 2 * d.d2 - 1;
-        const int f0 = (DIR == 1 ? d.ng1 : d.ng2) + seg * FLUX_ROW;
-        const int f1 = (DIR == 1 ? d.ng1 : d.ng2) + (seg + 1) * FLUX_ROW < (DIR == 1 ? d.ng1 : d.ng2) + nf
-                           ? (DIR == 1 ? d.ng1 : d.ng2) + (seg + 1) * FLUX_ROW
-                           : (DIR == 1 ? d.ng1 : d.ng2) + nf;
+        const int ng = DIR == 1 ? d.ng1 : d.ng2;
+        const int f0 = ng + seg * FLUX_ROW;
+        const int f1 = min(f0 + FLUX_ROW, ng + nf);
         const long stride = DIR == 1 ? (long)d.G2 * d.G3 : (long)d.G3;
         const int face = DIR == 1 ? FACE1 : FACE2;
+        const Win win{wbuf + threadIdx.x};
+        constexpr int NW = Win::NW, H = Win::H;
         T pl[NPR], lo[NPR], hi[NPR];
-        // the zone below the first face: its upper edge is the first left state
+        // the stencil of the zone below the first face, zones f0 - 1 - H ..
+        // f0 - 1 + H (f0 >= ng > H), then its upper edge: the first left state
         const long cf0 = DIR == 1 ? cix(d, f0, a, z) : cix(d, a, f0, z);
-        zone_edges<DIR, T, REC>(d, pv, cf0 - stride, stride, lo, hi);
+#pragma unroll
+        for (int s = 0; s < NW; s++) win.load(d, pv, cf0 + (s - 1 - H) * stride, (f0 - 1 - H + s) % NW);
+        win.edges((f0 - 1 - H) % NW, lo, hi);
 #pragma unroll
         for (int k = 0; k < NPR; k++) pl[k] = hi[k];
+        int s0 = (f0 - H) % NW;   // slot of zone f - H
         for (int f = f0; f < f1; f++) {
             const int i = DIR == 1 ? f : a, j = DIR == 1 ? a : f;
             const long c = cix(d, i, j, z);
-            zone_edges<DIR, T, REC>(d, pv, c, stride, lo, hi);
+            // zone f + H replaces zone f - H - 1 (slot s0 + 2H, mod NW)
+            win.load(d, pv, c + H * stride, s0 == 0 ? NW - 1 : s0 - 1);
+            win.edges(s0, lo, hi);
+            s0 = s0 == NW - 1 ? 0 : s0 + 1;
             Geo<T> gm;
             load_geo_t(d, m, i, j, face, gm);
             T l[NPR];
@@ -1043,21 +1120,44 @@ __device__ __forceinline__ void invert_epilogue(const Dims &d, const Geo<double>
     for (int k = 0; k < NPR; k++) pout[k * ks + c] = pf[k];
 }
 
+// the inversion's per-zone constants, from the column table when there is one
+__device__ __forceinline__ InvK inv_k(const Dims &d, const Geom &m, long gi, const Geo<double> &gm) {
+    if (m.itab)
+        return InvK{d.gam, d.rgam, gm.g, __ldg(&m.itab[gi]), __ldg(&m.itab[d.gs + gi]),
+                    __ldg(&m.itab[2 * d.gs + gi])};
+    return inv_consts(d.gam, d.rgam, gm.g, gm.gcon);
+}
+
+// the column table: at the zone centre of every (i, j), with the operations
+// of inv_consts, so that a tabulated value equals the one computed in place
+__global__ void k_inv_tab(const Dims d, const double *__restrict__ gcon, const double *__restrict__ gdet,
+                          double *__restrict__ itab) {
+    const long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= d.gs) return;
+    const double g = gdet[(long)CENT * d.gs + idx];
+    const double g00 = gcon[(long)CENT * d.gs + idx];   // component 0, location CENT
+    itab[idx] = 1.0 / g;
+    itab[d.gs + idx] = 1.0 / sqrt(-g00);
+    itab[2 * d.gs + idx] = -sqrt(-1. / g00);
+}
+
 // primary solver: Noble 2D, or Newman-Hamlin in its place (NEWMAN builds)
 template <int INV>
-__device__ __forceinline__ int invert_primary(const Dims &d, const Geo<double> &gm, const double *U, double *pf) {
+__device__ __forceinline__ int invert_primary(const Dims &d, const InvK &k, const Geo<double> &gm, const double *U,
+                                              double *pf) {
     return INV == HAMR_INV_NM ? utoprim_nm(d.gam, U, gm.gcov, gm.gcon, gm.g, pf)
-                              : utoprim_2d(d.gam, U, gm.gcov, gm.gcon, gm.g, pf);
+                              : utoprim_2d_k(k, U, gm.gcov, gm.gcon, pf);
 }
 
 // Primary inversion with the 1dvsq2fix1 and 1dfix1 fallbacks, recording the
 // outcome in pflag and the failure counters (fixup, GPU_fixup.h:346-382),
 // all in one pass (the batched inversion's per-item body)
 template <int INV, int FIX = 0>
-__device__ __forceinline__ void invert_zone(const Dims &d, const Geo<double> &gm, long c, double *U, double *pf,
+__device__ __forceinline__ void invert_zone(const Dims &d, const InvK &k, const Geo<double> &gm, long c, double *U,
+                                            double *pf,
                                             double *__restrict__ pout, int *__restrict__ pflag,
                                             int *__restrict__ failimage) {
-    int flag = invert_primary<INV>(d, gm, U, pf);
+    int flag = invert_primary<INV>(d, k, gm, U, pf);
     if (flag) flag = invert_fallbacks(d, gm, c, U, pf, failimage);
     invert_epilogue<FIX>(d, gm, c, flag, pf, pout, pflag, failimage);
 }
@@ -1363,7 +1463,7 @@ __device__ __forceinline__ void k_invert_at(const Dims &d, const Geom &m, const 
     load_geo(d, m, i, j, CENT, gm);
     double pf[NPR], U[NPR];
     invert_inputs(d, m, pg, W, psf, i, j, c, gi, pf, U);
-    invert_zone<INV, FIX>(d, gm, c, U, pf, pout, pflag, failimage);
+    invert_zone<INV, FIX>(d, inv_k(d, m, gi, gm), gm, c, U, pf, pout, pflag, failimage);
 }
 
 // The single-block inversion in two passes, so that the common path carries
@@ -1390,7 +1490,7 @@ __global__ void __launch_bounds__(BLK, HAMR_UPD_MINB)
     load_geo(d, m, i, j, CENT, gm);
     double pf[NPR], U[NPR];
     invert_inputs(d, m, pg, W, psf, i, j, c, gi, pf, U);
-    const int flag = invert_primary<INV>(d, gm, U, pf);
+    const int flag = invert_primary<INV>(d, inv_k(d, m, gi, gm), gm, U, pf);
     if (flag) {
         flist[atomicAdd(nfail, 1)] = (int)t;
         return;
@@ -1804,6 +1904,16 @@ struct hamr_ctx {
     bool ct_fused = false;   // one constrained-transport kernel for 3-D blocks (slower: off)
     bool cons_tma = true;    // conserved update with TMA-staged fluxes (3-D, n3 >= 32, aligned planes)
     int *kerr = nullptr;     // set by kernels whose bounded waits gave up
+    // independent kernels of a sub-step on two side streams, forked from and
+    // joined back into `stream` by events (the x1/x2 fluxes and the centre
+    // EMFs beside the x3 fluxes; the rest of the CT chain beside the conserved
+    // update); off for the per-kernel profile and the allocation-free step.
+    // Measured on the 384 x 192 x 192 torus: 14.44 ms per mixed step with the
+    // side streams, 14.35 without (FP64 31.40, 31.32): off by default,
+    // HAMR_CONCURRENT=1 turns it on
+    bool concurrent = false;
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t ev[5] = {};
     std::string err;
     // device state
     double *p = nullptr, *ph = nullptr, *ps = nullptr, *psh = nullptr, *U = nullptr;
@@ -1811,6 +1921,7 @@ struct hamr_ctx {
     double *W = nullptr;  // updated conserved variables between k_cons and k_invert
     int *pflag = nullptr, *failimage = nullptr;
     double *gcov = nullptr, *gcon = nullptr, *gdet = nullptr, *conn = nullptr;
+    double *itab = nullptr;   // the inversion's column table (k_inv_tab), 3 planes of gs
     unsigned long long *dtbits = nullptr;
     double *ndt = nullptr, *dt_state = nullptr;
     int *counter = nullptr;
@@ -1835,7 +1946,7 @@ int fail_cuda(hamr_ctx *c, cudaError_t e, const char *what) {
         if (e_ != cudaSuccess) return fail_cuda(ctx, e_, #call); \
     } while (0)
 
-Geom geom_of(const hamr_ctx *c) { return Geom{c->gcov, c->gcon, c->gdet, c->conn}; }
+Geom geom_of(const hamr_ctx *c) { return Geom{c->gcov, c->gcon, c->gdet, c->conn, c->itab}; }
 
 // the error word kernels set when a bounded wait gave up (read after a
 // synchronisation the caller already makes; cleared once reported)
@@ -1948,6 +2059,16 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
     const double *pin = full ? ctx->ph : ctx->p;
     const double *psin = full ? ctx->psh : ctx->ps;
     const int cd = calc_dt ? 1 : 0;
+    // the fluxes of the three directions (each with its own step-size slot)
+    // and the centre EMFs read only the sub-step's input state: x3 on the
+    // stage stream, x2 and x1 + centre EMFs on the side streams
+    const bool conc = ctx->concurrent && !(pf && pf->on) && !(d.d3 && ctx->ct_fused);
+    cudaStream_t s2 = conc ? ctx->side[0] : s, s3 = conc ? ctx->side[1] : s;
+    if (conc) {
+        CK(cudaEventRecord(ctx->ev[0], s));
+        CK(cudaStreamWaitEvent(s2, ctx->ev[0], 0));
+        CK(cudaStreamWaitEvent(s3, ctx->ev[0], 0));
+    }
     if (d.d3) {
         long n = (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3 - 1);
         launch_flux<3, T>(n, s, d, m, pin, psin, F3, ctx->dtbits, cd, ctx->rows_min);
@@ -1955,19 +2076,34 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
     prof_mark(pf, PROF_FLUX3, s);
     {
         long n = (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2 - 1) * (d.n3 + 2 * d.d3);
-        launch_flux<2, T>(n, s, d, m, pin, psin, F2, ctx->dtbits, cd, ctx->rows_min);
+        launch_flux<2, T>(n, s2, d, m, pin, psin, F2, ctx->dtbits, cd, ctx->rows_min);
     }
     prof_mark(pf, PROF_FLUX2, s);
     {
         long n = (long)(d.n1 + 2 * d.d1 - 1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3);
-        launch_flux<1, T>(n, s, d, m, pin, psin, F1, ctx->dtbits, cd, ctx->rows_min);
+        launch_flux<1, T>(n, s3, d, m, pin, psin, F1, ctx->dtbits, cd, ctx->rows_min);
     }
     prof_mark(pf, PROF_FLUX1, s);
+    if (conc) {
+        long n = (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3);
+        k_emf_centre<T><<<nblk(n), BLK, 0, s3>>>(d, m, pin, Ec);
+        CK(cudaEventRecord(ctx->ev[1], s2));
+        CK(cudaEventRecord(ctx->ev[2], s3));
+        CK(cudaStreamWaitEvent(s, ctx->ev[1], 0));
+        CK(cudaStreamWaitEvent(s, ctx->ev[2], 0));
+    }
     if (d.bc2 == HAMR_BC_POLE_REFL) {
         long n = (long)d.G1 * d.G3 + (long)d.G2 * d.G3;
         k_fix_flux<T><<<nblk(n), BLK, 0, s>>>(d, F1, F2, F3);
     }
     prof_mark(pf, PROF_FIXFLUX, s);
+    // the rest of the CT chain (edge EMFs, polar average, face update) writes
+    // only EMFs and the face field, which the conserved update does not read:
+    // on a side stream beside it, joined before the inversion
+    if (conc) {
+        CK(cudaEventRecord(ctx->ev[3], s));
+        CK(cudaStreamWaitEvent(s2, ctx->ev[3], 0));
+    }
     if (d.d3 && ctx->ct_fused) {
         // centre EMFs, edge EMFs and the face update in one kernel (polar
         // rows of transmissive poles after the phi average); timed as the
@@ -1986,19 +2122,19 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
         }
         prof_mark(pf, PROF_FACE, s);
     } else {
-    {
+    if (!conc) {
         long n = (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3);
         k_emf_centre<T><<<nblk(n), BLK, 0, s>>>(d, m, pin, Ec);
     }
     prof_mark(pf, PROF_EMF_CENTRE, s);
     {
         long n = (long)(d.n1 + d.d1) * (d.n2 + d.d2) * (d.n3 + d.d3);
-        k_emf_edge<T><<<nblk(n), BLK, 0, s>>>(d, Ec, F1, F2, F3, emf);
+        k_emf_edge<T><<<nblk(n), BLK, 0, s2>>>(d, Ec, F1, F2, F3, emf);
         prof_mark(pf, PROF_EMF_EDGE, s);
         if (d.bc2 == HAMR_BC_POLE_TRANS)
-            k_pole_average<T><<<nblk(2L * (d.n1 + d.ng1)), BLK, 0, s>>>(d, emf, st);
+            k_pole_average<T><<<nblk(2L * (d.n1 + d.ng1)), BLK, 0, s2>>>(d, emf, st);
         prof_mark(pf, PROF_POLE_AVG, s);
-        k_face_update<T><<<nblk(n), BLK, 0, s>>>(d, m, ctx->ps, full ? ctx->ps : ctx->psh, emf, st);
+        k_face_update<T><<<nblk(n), BLK, 0, s2>>>(d, m, ctx->ps, full ? ctx->ps : ctx->psh, emf, st);
         prof_mark(pf, PROF_FACE, s);
     }
     }
@@ -2017,6 +2153,10 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
             k_cons<T><<<nblk(n), BLK, 0, s>>>(d, m, ctx->p, full ? ctx->ph : ctx->p, ctx->U, F1, F2, F3, ctx->W, full,
                                               st, ctx->nfail);
         prof_mark(pf, PROF_UPDATE, s);
+        if (conc) {
+            CK(cudaEventRecord(ctx->ev[4], s2));
+            CK(cudaStreamWaitEvent(s, ctx->ev[4], 0));
+        }
         // (the inversion gained nothing from the same staging: FP64 Newton work
         // bounds it, not its 26 metric loads per zone)
         const int fix = (ctx->prm.floors ? FIX_FLOORS : 0) | (ctx->prm.repair == 1 ? FIX_RESET : 0);
@@ -2110,6 +2250,7 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
     if (d.ks < ncell || d.gs < ngeo) { delete ctx; return HAMR_E_ARG; }
     d.dx1 = prm->dx1; d.dx2 = prm->dx2; d.dx3 = prm->dx3;
     d.rdx1 = 1.0 / d.dx1; d.rdx2 = 1.0 / d.dx2; d.rdx3 = 1.0 / d.dx3;
+    d.rgam = 1.0 / prm->gam;
     d.gam = prm->gam; d.cour = prm->cour;
     d.pole1 = prm->pole1; d.pole2 = prm->pole2;
     d.bc1 = prm->bc1; d.bc2 = prm->bc2; d.bc3 = prm->bc3;
@@ -2138,6 +2279,13 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
         if (const char *e = getenv("HAMR_CONS_COLS")) ctx->cons_cols = atoi(e) != 0;
         if (const char *e = getenv("HAMR_CT_FUSED")) ctx->ct_fused = atoi(e) != 0;
         if (const char *e = getenv("HAMR_CONS_TMA")) ctx->cons_tma = atoi(e) != 0;
+        if (const char *e = getenv("HAMR_CONCURRENT")) ctx->concurrent = atoi(e) != 0;
+    }
+    if (ctx->concurrent) {
+        for (auto &st : ctx->side)
+            if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) ctx->concurrent = false;
+        for (auto &ev : ctx->ev)
+            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) ctx->concurrent = false;
     }
     const size_t cb = sizeof(double) * d.ks;
     struct A { void **p; size_t n; } allocs[] = {
@@ -2148,6 +2296,7 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
         {(void **)&ctx->failimage, 5 * sizeof(int) * d.ks},
         {(void **)&ctx->gcov, 50 * sizeof(double) * d.gs}, {(void **)&ctx->gcon, 50 * sizeof(double) * d.gs},
         {(void **)&ctx->gdet, 5 * sizeof(double) * d.gs}, {(void **)&ctx->conn, 40 * sizeof(double) * d.gs},
+        {(void **)&ctx->itab, 3 * sizeof(double) * d.gs},
         {(void **)&ctx->dtbits, 4 * sizeof(unsigned long long)}, {(void **)&ctx->ndt, sizeof(double)},
         {(void **)&ctx->dt_state, sizeof(double)}, {(void **)&ctx->counter, sizeof(int)},
         {(void **)&ctx->divb, sizeof(unsigned long long)},
@@ -2183,11 +2332,16 @@ int hamr_ctx_destroy(hamr_ctx *ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->graph) cudaGraphExecDestroy(ctx->graph);
     void *bufs[] = {ctx->p, ctx->ph, ctx->ps, ctx->psh, ctx->U, ctx->F1, ctx->F2, ctx->F3, ctx->Ec, ctx->emf,
-                    ctx->W, ctx->pflag, ctx->failimage, ctx->gcov, ctx->gcon, ctx->gdet, ctx->conn, ctx->dtbits,
+                    ctx->W, ctx->pflag, ctx->failimage, ctx->gcov, ctx->gcon, ctx->gdet, ctx->conn, ctx->itab,
+                    ctx->dtbits,
                     ctx->ndt, ctx->dt_state, ctx->counter, ctx->divb, ctx->rlist, ctx->rcount,
                     ctx->flist, ctx->nfail, ctx->kerr};
     for (void *b : bufs)
         if (b) cudaFree(b);
+    for (auto st : ctx->side)
+        if (st) cudaStreamDestroy(st);
+    for (auto ev : ctx->ev)
+        if (ev) cudaEventDestroy(ev);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return HAMR_OK;
@@ -2209,6 +2363,8 @@ int hamr_set_geometry(hamr_ctx *ctx, const double *gcov, const double *gcon, con
     CK(cudaMemcpyAsync(ctx->gcon, gcon, 50 * g, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->gdet, gdet, 5 * g, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->conn, conn, 40 * g, cudaMemcpyHostToDevice, ctx->stream));
+    k_inv_tab<<<nblk(ctx->d.gs), BLK, 0, ctx->stream>>>(ctx->d, ctx->gcon, ctx->gdet, ctx->itab);
+    CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->have_geom = true;
     return HAMR_OK;
@@ -2478,6 +2634,7 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
     hamr_ctx c{};   // value-initialised: every field not set below is zero
     c.rows_min = 1L << 60;   // blocks this small keep one thread per face
     c.cons_tma = false;      // the update without the bulk-copy staging (no error word here)
+    c.concurrent = false;    // no side streams
     c.prm = *prm;
     Dims &d = c.d;
     d.n1 = prm->n1; d.n2 = prm->n2; d.n3 = prm->n3;
@@ -2491,6 +2648,7 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
     if (d.ks > HAMR_NOALLOC_MAX_CELLS) return HAMR_E_ARG;   // beyond the static scratch
     d.dx1 = prm->dx1; d.dx2 = prm->dx2; d.dx3 = prm->dx3;
     d.rdx1 = 1.0 / d.dx1; d.rdx2 = 1.0 / d.dx2; d.rdx3 = 1.0 / d.dx3;
+    d.rgam = 1.0 / prm->gam;
     d.gam = prm->gam; d.cour = prm->cour;
     d.pole1 = prm->pole1; d.pole2 = prm->pole2;
     d.bc1 = prm->bc1; d.bc2 = prm->bc2; d.bc3 = prm->bc3;

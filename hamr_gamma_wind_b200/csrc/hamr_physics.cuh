@@ -19,6 +19,8 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include <type_traits>
+
 namespace hamr {
 
 enum { RHO = 0, UU = 1, U1 = 2, U2 = 3, U3 = 4, B1 = 5, B2 = 6, B3 = 7, KTOT = 8, NPR = 9 };
@@ -87,6 +89,33 @@ __device__ __forceinline__ double div_rcp(double a, double b, double rb) {
     return r == 0.0 ? q0 : fma(r, rb, q0);
 }
 
+// div_rcp that also returns the IEEE quotient for an infinite dividend (the
+// residual of an infinite q0 is NaN): for the inversion, which may meet an
+// overflowed state before it reports the failure
+__device__ __forceinline__ double div_rcp_inf(double a, double b, double rb) {
+    const double q0 = a * rb;
+    const double r = fma(-q0, b, a);
+    return (r == 0.0 || isinf(q0)) ? q0 : fma(r, rb, q0);
+}
+
+// Quotients a_k / b that share one divisor. In double precision: one IEEE
+// reciprocal of b, then the exact form per quotient (div_rcp_inf: the IEEE
+// quotient bit for bit for 2^-900 <= |a| <= 2^900, zeros and infinities),
+// which replaces all but one full division by three operations. Other types
+// (float, whose division is already the approximate one in the mixed step,
+// and the adjoint's dual numbers) divide as written.
+template <typename T>
+struct Divisor {
+    T b, rb;
+    __device__ __forceinline__ explicit Divisor(T b_) : b(b_), rb(b_) {
+        if constexpr (std::is_same<T, double>::value) rb = 1.0 / b_;
+    }
+    __device__ __forceinline__ T div(T a) const {
+        if constexpr (std::is_same<T, double>::value) return div_rcp_inf(a, b, rb);
+        else return a / b;
+    }
+};
+
 template <typename T> __device__ __forceinline__ T d_max(T a, T b) { return a > b ? a : b; }
 template <typename T> __device__ __forceinline__ T d_min(T a, T b) { return a < b ? a : b; }
 
@@ -127,16 +156,24 @@ __device__ __forceinline__ void ucon_calc(const T *pr, const Geo<G> &gm, T *ucon
 #pragma unroll
     for (int j = 1; j < 4; j++) beta[j] = gm.gcon[j] * alpha * alpha;
     gamma_calc(pr, gm, &gamma);
-    ucon[0] = gamma / alpha;
+    if constexpr (std::is_same<T, G>::value) {
+        const Divisor<T> da(alpha);   // four quotients by the lapse
+        ucon[0] = da.div(gamma);
 #pragma unroll
-    for (int j = 1; j < 4; j++) ucon[j] = pr[U1 + j - 1] - gamma * beta[j] / alpha;
+        for (int j = 1; j < 4; j++) ucon[j] = pr[U1 + j - 1] - da.div(gamma * beta[j]);
+    } else {
+        ucon[0] = gamma / alpha;
+#pragma unroll
+        for (int j = 1; j < 4; j++) ucon[j] = pr[U1 + j - 1] - gamma * beta[j] / alpha;
+    }
 }
 
 template <typename T>
 __device__ __forceinline__ void bcon_calc(const T *pr, const T *ucon, const T *ucov, T *bcon) {
     bcon[0] = pr[B1] * ucov[1] + pr[B2] * ucov[2] + pr[B3] * ucov[3];
+    const Divisor<T> du(ucon[0]);
 #pragma unroll
-    for (int j = 1; j < 4; j++) bcon[j] = (pr[B1 - 1 + j] + bcon[0] * ucon[j]) / ucon[0];
+    for (int j = 1; j < 4; j++) bcon[j] = du.div(pr[B1 - 1 + j] + bcon[0] * ucon[j]);
 }
 
 template <typename T, typename G>
@@ -200,8 +237,9 @@ __device__ __forceinline__ void primtoflux(T gam, const T *pr, const State<T> &q
         if ((discr < T(0.0)) && (discr > T(-1.e-10))) discr = T(0.0);
         else if (discr < T(-1.e-10)) discr = T(0.);
         discr = d_sqrt(discr);
-        T vp = -(-B + discr) / (T(2.) * A);
-        T vm = -(-B - discr) / (T(2.) * A);
+        const Divisor<T> d2a(T(2.) * A);
+        T vp = d2a.div(-(-B + discr));
+        T vm = d2a.div(-(-B - discr));
         *vmax = d_max(vp, vm);
         *vmin = d_min(vp, vm);
     }
@@ -219,6 +257,19 @@ __device__ __forceinline__ T slope_lim(T y1, T y2, T y3) {
     if (d_fabs(Dqm) < d_fabs(Dqp) && d_fabs(Dqm) < d_fabs(Dqc)) return Dqm;
     if (d_fabs(Dqp) < d_fabs(Dqc)) return Dqp;
     return Dqc;
+}
+
+// a / 6 for PPM's edge correction: in double precision by the exact
+// reciprocal form (div_rcp; the IEEE quotient bit for bit for
+// 2^-900 <= |a| <= 2^900 and zeros, the range of differences of limited
+// slopes of the state), else the type's own division
+template <typename T>
+__device__ __forceinline__ T div6(T a) {
+    if constexpr (std::is_same<T, double>::value) {
+        return div_rcp(a, 6.0, 1.0 / 6.0);
+    } else {
+        return a / T(6.0);
+    }
 }
 
 // PPM face values of the middle of five zones: l = lower edge, r = upper edge
@@ -241,8 +292,8 @@ __device__ __forceinline__ void para(const T *y, T &lout, T &rout) {
             else dq[i] = (-Dqm) * (T)(s > T(0.));
         }
     }
-    T l = T(0.5) * (y[2] + y[1]) - (dq[2] - dq[1]) / T(6.0);
-    T r = T(0.5) * (y[3] + y[2]) - (dq[3] - dq[2]) / T(6.0);
+    T l = T(0.5) * (y[2] + y[1]) - div6(dq[2] - dq[1]);
+    T r = T(0.5) * (y[3] + y[2]) - div6(dq[3] - dq[2]);
     T qa = (r - y[2]) * (y[2] - l);
     T qd = (r - l);
     T qe = T(6.0) * (y[2] - T(0.5) * (l + r));
@@ -258,8 +309,21 @@ struct InvQ {
     double Bcon[4], Qcon[4], ncon[4], Bsq, QdotB, QdotBsq, Qtsq, Qdotn, D;
 };
 
-__device__ __forceinline__ void inv_scalars(const double *U, const double *gcov, const double *gcon, InvQ &s) {
-    double Bcov[4], Qcov[4], Qsq, ncov;
+// per-zone constants of the inversion: gamma and the metric values it
+// divides by, with their reciprocals rounded once (exact divisions, div_rcp),
+// and the lapse and the normal observer's n_t. Either tabulated per (i, j)
+// column or computed in place (inv_consts), with the same operations.
+struct InvK {
+    double gam, rgam, gdet, rgdet, alpha, ncov;
+};
+
+__device__ __forceinline__ InvK inv_consts(double gam, double rgam, double gdet, const double *gcon) {
+    return InvK{gam, rgam, gdet, 1.0 / gdet, 1.0 / sqrt(-gcon[0]), -sqrt(-1. / gcon[0])};
+}
+
+__device__ __forceinline__ void inv_scalars_n(const double *U, const double *gcov, const double *gcon, double ncov,
+                                              InvQ &s) {
+    double Bcov[4], Qcov[4], Qsq;
     s.Bcon[0] = 0.;
     for (int i = 1; i < 4; i++) s.Bcon[i] = U[B1 + i - 1];
     lower4(s.Bcon, gcov, Bcov);
@@ -270,7 +334,6 @@ __device__ __forceinline__ void inv_scalars(const double *U, const double *gcov,
     s.QdotB = 0.;
     for (int i = 0; i < 4; i++) s.QdotB += Qcov[i] * s.Bcon[i];
     s.QdotBsq = s.QdotB * s.QdotB;
-    ncov = -sqrt(-1. / gcon[0]);
     s.ncon[0] = gcon[0] * ncov;
     s.ncon[1] = gcon[1] * ncov;
     s.ncon[2] = gcon[2] * ncov;
@@ -280,6 +343,10 @@ __device__ __forceinline__ void inv_scalars(const double *U, const double *gcov,
     for (int i = 0; i < 4; i++) Qsq += Qcov[i] * s.Qcon[i];
     s.Qtsq = Qsq + s.Qdotn * s.Qdotn;
     s.D = U[RHO];
+}
+
+__device__ __forceinline__ void inv_scalars(const double *U, const double *gcov, const double *gcon, InvQ &s) {
+    inv_scalars_n(U, gcov, gcon, -sqrt(-1. / gcon[0]), s);
 }
 
 __device__ __forceinline__ int guess_utsq(const double *gcov, const double *prim, double *out) {
@@ -302,6 +369,17 @@ __device__ __forceinline__ void set_velocity(const InvQ &s, double gamma, double
     }
 }
 
+// the same with the divisions by gdet in the exact reciprocal form
+__device__ __forceinline__ int inv_prologue_k(const double *U, const InvK &k, double *prim, double *Ut) {
+    if (U[0] <= 0.) return -100;
+    for (int i = B1; i <= B3; i++) prim[i] = div_rcp_inf(U[i], k.gdet, k.rgdet);
+    Ut[RHO] = div_rcp_inf(k.alpha * U[RHO], k.gdet, k.rgdet);
+    Ut[UU] = div_rcp_inf(k.alpha * (U[UU] - U[RHO]), k.gdet, k.rgdet);
+    for (int i = U1; i <= U3; i++) Ut[i] = div_rcp_inf(k.alpha * U[i], k.gdet, k.rgdet);
+    for (int i = B1; i <= B3; i++) Ut[i] = div_rcp_inf(k.alpha * U[i], k.gdet, k.rgdet);
+    return 0;
+}
+
 __device__ __forceinline__ int inv_prologue(const double *U, double gdet, const double *gcon, double *prim, double *Ut) {
     if (U[0] <= 0.) return -100;
     for (int i = B1; i <= B3; i++) prim[i] = U[i] / gdet;
@@ -319,14 +397,20 @@ __device__ __forceinline__ double vsq_of_W(double W, double Bsq, double Qtsq, do
     return (Wsq * Qtsq + QdotBsq * (Bsq + 2. * W)) / (Wsq * Xsq);
 }
 
-// Noble et al. 2006, 2D Newton-Raphson on (W, v^2)
-__device__ __forceinline__ int utoprim_2d(double gam, const double *U, const double *gcov, const double *gcon, double gdet, double *prim) {
+// Noble et al. 2006, 2D Newton-Raphson on (W, v^2). The divisions by gamma
+// and gdet use their reciprocals in the exact form (div_rcp_inf): the same
+// quotients, bit for bit, for the dividends this solver meets (an energy
+// density or a conserved variable, between 2^-900 and 2^900, zero, or
+// non-finite).
+__device__ __forceinline__ int utoprim_2d_k(const InvK &k, const double *U, const double *gcov, const double *gcon,
+                                            double *prim) {
+    const double gam = k.gam, rgam = k.rgam;
     double Ut[NPR], pt[5];
-    int ret = inv_prologue(U, gdet, gcon, prim, Ut);
+    int ret = inv_prologue_k(U, k, prim, Ut);
     if (ret) return ret;
     for (int i = 0; i < B1; i++) pt[i] = prim[i];
     InvQ s;
-    inv_scalars(Ut, gcov, gcon, s);
+    inv_scalars_n(Ut, gcov, gcon, k.ncov, s);
     double utsq;
     if (guess_utsq(gcov, pt, &utsq)) return 2;
     double gammasq = 1. + utsq;
@@ -351,9 +435,9 @@ __device__ __forceinline__ int utoprim_2d(double gam, const double *U, const dou
     while (keep) {
         double Wsq = x0 * x0;
         double gtmp = 1. - x1;
-        double p_tmp = (gam - 1.) * (fma(x0, gtmp, -D * sqrt(gtmp))) / gam;
-        double dPdW = (gam - 1.) * (1. - x1) / gam;
-        double dPdvsq = (gam - 1.) * (fma(0.5, D / sqrt(1. - x1), -x0)) / gam;
+        double p_tmp = div_rcp_inf((gam - 1.) * (fma(x0, gtmp, -D * sqrt(gtmp))), gam, rgam);
+        double dPdW = div_rcp_inf((gam - 1.) * (1. - x1), gam, rgam);
+        double dPdvsq = div_rcp_inf((gam - 1.) * (fma(0.5, D / sqrt(1. - x1), -x0)), gam, rgam);
         double t2 = -0.5 * Bsq + dPdvsq;
         double t3 = Bsq + x0;
         double t4 = t3 * t3;
@@ -397,7 +481,7 @@ __device__ __forceinline__ int utoprim_2d(double gam, const double *U, const dou
     gamma = 1. / gtmp;
     rho0 = s.D * gtmp;
     w = W * (1. - vsq);
-    p = (gam - 1.) * (w - rho0) / gam;
+    p = div_rcp_inf((gam - 1.) * (w - rho0), gam, rgam);
     u = w - (rho0 + p);
     if (rho0 <= 0.) return 5;
     if (u <= 0.) return 6;
@@ -406,6 +490,11 @@ __device__ __forceinline__ int utoprim_2d(double gam, const double *U, const dou
     set_velocity(s, gamma, W, pt);
     for (int i = 0; i < B1; i++) prim[i] = pt[i];
     return 0;
+}
+
+__device__ __forceinline__ int utoprim_2d(double gam, const double *U, const double *gcov, const double *gcon,
+                                          double gdet, double *prim) {
+    return utoprim_2d_k(inv_consts(gam, 1.0 / gam, gdet, gcon), U, gcov, gcon, prim);
 }
 
 __device__ __forceinline__ double W_of_vsq2(double gam, double vsq, double *p, double *rho, double *u, double D, double K) {

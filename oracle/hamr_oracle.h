@@ -111,5 +111,6 @@ int ho_bl_coord(int coords, double spin, const double *X, double *rthph);
 int ho_num_threads(void);
 /* bit-level check of the library's division by a reciprocal (div_rcp) */
 long ho_div_rcp_mismatches(const double *a, long n, const double *b, long m);
+long ho_div_rcp_mismatches_g(const double *a, long n, const double *b, long m, int guard);
 
 #endif

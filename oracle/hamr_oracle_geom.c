@@ -363,6 +363,12 @@ int ho_num_threads(void) { return 1; }
  * many of the n*m quotients a[i]/b[j] it does not reproduce bit for bit
  * (compared as bit patterns; both sides are IEEE binary64 round-to-nearest). */
 long ho_div_rcp_mismatches(const double *a, long n, const double *b, long m) {
+    return ho_div_rcp_mismatches_g(a, n, b, m, 0);
+}
+
+/* The same with the infinite-dividend guard of the inversion's form (guard =
+ * 1): q = (r == 0 || isinf(q0)) ? q0 : fma(r, rb, q0). */
+long ho_div_rcp_mismatches_g(const double *a, long n, const double *b, long m, int guard) {
     long bad = 0;
 #pragma omp parallel for reduction(+ : bad) schedule(static)
     for (long j = 0; j < m; j++) {
@@ -370,7 +376,7 @@ long ho_div_rcp_mismatches(const double *a, long n, const double *b, long m) {
         for (long i = 0; i < n; i++) {
             const double q0 = a[i] * rb;
             const double r = fma(-q0, b[j], a[i]);
-            const double q = r == 0.0 ? q0 : fma(r, rb, q0);
+            const double q = (r == 0.0 || (guard && isinf(q0))) ? q0 : fma(r, rb, q0);
             const double e = a[i] / b[j];
             if (memcmp(&q, &e, sizeof(double)) != 0) bad++;
         }

@@ -103,6 +103,8 @@ def lib():
         L.ho_num_threads.restype = _i
         L.ho_div_rcp_mismatches.argtypes = [_vp, ctypes.c_long, _vp, ctypes.c_long]
         L.ho_div_rcp_mismatches.restype = ctypes.c_long
+        L.ho_div_rcp_mismatches_g.argtypes = [_vp, ctypes.c_long, _vp, ctypes.c_long, ctypes.c_int]
+        L.ho_div_rcp_mismatches_g.restype = ctypes.c_long
         _libs[name] = L
     return _libs[name]
 

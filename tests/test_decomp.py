@@ -72,6 +72,9 @@ def test_oracle_slabs_match_undivided_block(case):
     np.testing.assert_array_equal(pb.active(ps), s_full.blk.active("ps"))
 
 
+WIDTHS = {2: [14, 18], 3: [10, 9, 13]}
+
+
 def _rank(rank, world, path, port):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
@@ -79,7 +82,7 @@ def _rank(rank, world, path, port):
                             timeout=__import__("datetime").timedelta(seconds=60))
     try:
         pb, _ = bound_problem(problems.fm_torus(32, 16, 8, rout=40.0))
-        slabs = decomp.split(pb, [14, 18])
+        slabs = decomp.split(pb, WIDTHS[world])
         me = OracleSlab(slabs[rank])
         stepper = decomp.SlabStepper([me], decomp.DistributedExchange(rank, world))
         dt = 0.2 * min(pb.dx[:2])
@@ -94,19 +97,23 @@ def _rank(rank, world, path, port):
         dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_match_undivided_block():
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_match_undivided_block(world):
+    """One slab per rank (the middle rank of three exchanges with both
+    neighbours), halos and the CFL minimum over gloo: bit for bit the
+    undivided block, step sizes included."""
     with tempfile.TemporaryDirectory() as path:
-        port = 29500 + os.getpid() % 2000
-        mp.spawn(_rank, args=(2, path, port), nprocs=2, join=True)
+        port = 29500 + (os.getpid() + 97 * world) % 2000
+        mp.spawn(_rank, args=(world, path, port), nprocs=world, join=True)
         pb, s_full = bound_problem(problems.fm_torus(32, 16, 8, rout=40.0))
-        slabs = decomp.split(pb, [14, 18])
+        slabs = decomp.split(pb, WIDTHS[world])
         dt = 0.2 * min(pb.dx[:2])
         dts = []
         for _ in range(2):
             dn = oracle_step(s_full, dt)
             dts.append(dn)
             dt = min(dn, 1.3 * dt)
-        res = [np.load(os.path.join(path, f"rank{r}.npz")) for r in range(2)]
+        res = [np.load(os.path.join(path, f"rank{r}.npz")) for r in range(world)]
         for r in res:
             np.testing.assert_array_equal(r["dts"], np.array(dts))
         p, ps = decomp.join(pb, slabs, [(r["p"], r["ps"]) for r in res])

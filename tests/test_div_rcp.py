@@ -43,3 +43,22 @@ def test_div_rcp_matches_ieee_division():
     # outside the range: residuals below the normal range can misround
     tiny = np.array([9.332636185032189e-302, 5.696189077778436e-306])
     assert _check(tiny, np.array([np.nextafter(2.0, 1.0)])) == 2
+
+
+def test_div_rcp_inversion_divisors():
+    """The inversion's form (div_rcp_inf) divides by gamma and by the metric
+    determinant of the zone: adiabatic indices and sqrt(-g) over the range of
+    the torus grids (log-uniform from 1e-4 to 1e7), dividends over the exact
+    range, and infinite dividends (an overflowed state), which the guard
+    returns as the IEEE quotient does."""
+    rng = np.random.default_rng(77)
+    b = np.concatenate([[13 / 9, 4 / 3, 5 / 3, 1.4, 2.0],
+                        np.exp(rng.uniform(np.log(1e-4), np.log(1e7), 120))])
+    a = np.exp2(rng.uniform(-899.0, 899.0, 300_000)) * rng.choice([-1.0, 1.0], 300_000)
+    a[:6] = [0.0, -0.0, np.inf, -np.inf, 1.0, -1.0]
+    a = np.ascontiguousarray(a)
+    b = np.ascontiguousarray(b)
+    args = (a.ctypes.data_as(ctypes.c_void_p), a.size, b.ctypes.data_as(ctypes.c_void_p), b.size)
+    assert O.lib().ho_div_rcp_mismatches_g(*args, 1) == 0
+    # without the guard only the infinite dividends differ (NaN for +-inf)
+    assert O.lib().ho_div_rcp_mismatches_g(*args, 0) == 2 * b.size
