@@ -76,6 +76,7 @@ def load(strict: bool = False):
     L.hamr_batch_step.argtypes = [_vp, _vp, _vp]
     L.hamr_batch_advance.argtypes = [_vp, _i, _i, _vp]
     L.hamr_batch_autotune.argtypes = [_vp, _vp, _i]
+    L.hamr_batch_set_persistent.argtypes = [_vp, _i]
     L.hamr_batch_tuning.argtypes = [_vp, _vp, _vp, _vp, _vp, _i]
     L.hamr_adjoint_create.argtypes = [_vp, _i, P(_vp)]
     L.hamr_adjoint_destroy.argtypes = [_vp]
@@ -102,7 +103,7 @@ SYMBOLS = ["hamr_ctx_create", "hamr_ctx_destroy", "hamr_last_error", "hamr_strid
            "hamr_bound", "hamr_stage", "hamr_step", "hamr_advance", "hamr_device_state", "hamr_profile_step",
            "hamr_divb_max", "hamr_build_geometry", "hamr_bl_coord", "hamr_step_noalloc",
            "hamr_batch_create", "hamr_batch_destroy", "hamr_batch_last_error", "hamr_batch_step",
-           "hamr_batch_advance", "hamr_batch_autotune", "hamr_batch_tuning",
+           "hamr_batch_advance", "hamr_batch_autotune", "hamr_batch_set_persistent", "hamr_batch_tuning",
            "hamr_adjoint_create", "hamr_adjoint_destroy", "hamr_adjoint_last_error", "hamr_adjoint_cotangent",
            "hamr_adjoint_zero", "hamr_step_backward", "hamr_mdot_forward", "hamr_adjoint_run",
            "hamr_bound_dim", "hamr_halo_count", "hamr_halo_pack", "hamr_halo_unpack", "hamr_cfl_dirs"]

@@ -287,6 +287,11 @@ class Batch:
                                               d.ctypes.data_as(ctypes.c_void_p)), "hamr_batch_advance")
         return d
 
+    def set_persistent(self, on=True):
+        """One persistent cooperative launch per sub-step (True) or one
+        launch per phase (False, the default)."""
+        self._check(self.L.hamr_batch_set_persistent(self.h, int(bool(on))), "hamr_batch_set_persistent")
+
     def autotune(self, dt, reps=3):
         d = self._dts(dt)
         self._check(self.L.hamr_batch_autotune(self.h, d.ctypes.data_as(ctypes.c_void_p), int(reps)),

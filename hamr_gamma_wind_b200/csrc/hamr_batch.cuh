@@ -251,6 +251,112 @@ __global__ void k_batch_dt_finalize(const BEntry *__restrict__ E, int n, int upd
     for (int k = 0; k < 4; k++) e.dtbits[k] = BITS_1E9;
 }
 
+// ---- one persistent launch per sub-step ------------------------------------
+// The alternative to one launch per phase: a cooperative launch of as many
+// CTAs as fit on the device at once runs every phase of a sub-step, phase
+// after phase, each CTA taking tiles b, b + grid, ... of the phase's tile
+// map, with a grid-wide barrier wherever the next phase reads what the
+// previous wrote (x3/x2/x1 fluxes and centre EMFs | polar flux fix | edge
+// EMFs and conserved update | polar EMF average | face update | inversion |
+// ghost fills x1 | x3 | x2). The cost is one register budget for all phases
+// (the FP64 flux's), instead of each phase's own.
+
+struct PhaseMaps {
+    TileMap tm[PH_N];
+};
+
+// the tile loop of k_batch for one phase, inside the persistent kernel
+template <class Op>
+__device__ __forceinline__ void run_phase(const BEntry *__restrict__ E, const TileMap &tm, const StageArg &a,
+                                          BEntry &e) {
+    if (tm.start == nullptr) return;   // no items in this phase
+    const long ntiles = tm.start[tm.n];
+    for (long w = blockIdx.x; w < ntiles; w += gridDim.x) {
+        int lo = 0, hi = tm.n;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (tm.start[mid] <= w) lo = mid;
+            else hi = mid;
+        }
+        __syncthreads();
+        {
+            const int *src = reinterpret_cast<const int *>(&E[tm.order[lo]]);
+            int *dst = reinterpret_cast<int *>(&e);
+            for (int k = threadIdx.x; k < (int)(sizeof(BEntry) / 4); k += BLK) dst[k] = src[k];
+        }
+        __syncthreads();
+        const long first = (w - tm.start[lo]) * tm.tile;
+        const long cnt = phase_items(Op::PH, e.d);
+        const long last = first + tm.tile < cnt ? first + tm.tile : cnt;
+        double dtf = 1.e9;
+        for (long t = first + threadIdx.x; t < last; t += BLK) dtf = d_min(dtf, Op::run(e, a, t));
+        if (Op::REDUCE && a.calc_dt) cta_min_dt(dtf, &e.dtbits[Op::SLOT]);
+    }
+}
+
+// Grid-wide barrier of a cooperative launch (all CTAs resident): bar[0]
+// counts arrivals, bar[1] is the generation. Thread 0 publishes the CTA's
+// writes (fence), arrives, and waits for the generation to move, at most
+// 2^24 polls of 64 ns; a wait that gives up sets *kerr = 2 and goes on (the
+// sub-step's results are then invalid and the host reports the error).
+__device__ __forceinline__ void grid_barrier(unsigned *bar, int *kerr) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = bar + 1;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) + 1 == gridDim.x) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            for (int it = 0; *gen == g; it++) {
+                if (it >= (1 << 24)) {
+                    atomicExch(kerr, 2);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+constexpr int PERSIST_MINB = HAMR_FLUX_MINB;   // the FP64 flux phases' budget
+
+template <typename T>
+__global__ void __launch_bounds__(BLK, PERSIST_MINB)
+    k_batch_stage(const BEntry *__restrict__ E, const PhaseMaps pm, const StageArg a, unsigned *bar, int *kerr) {
+    __shared__ BEntry e;
+    auto has = [&](int ph) { return pm.tm[ph].start != nullptr && pm.tm[ph].n > 0; };
+    run_phase<OpFlux<3, T, 0>>(E, pm.tm[PH_FLUX3], a, e);
+    run_phase<OpFlux<2, T, 0>>(E, pm.tm[PH_FLUX2], a, e);
+    run_phase<OpFlux<1, T, 0>>(E, pm.tm[PH_FLUX1], a, e);
+    run_phase<OpEmfCentre<T>>(E, pm.tm[PH_EMFC], a, e);
+    grid_barrier(bar, kerr);
+    if (has(PH_FIXFLUX)) {
+        run_phase<OpFixFlux<T>>(E, pm.tm[PH_FIXFLUX], a, e);
+        grid_barrier(bar, kerr);
+    }
+    run_phase<OpEmfEdge<T>>(E, pm.tm[PH_EMFE], a, e);
+    run_phase<OpCons<T>>(E, pm.tm[PH_CONS], a, e);
+    grid_barrier(bar, kerr);
+    if (has(PH_POLE)) {
+        run_phase<OpPole<T>>(E, pm.tm[PH_POLE], a, e);
+        grid_barrier(bar, kerr);
+    }
+    run_phase<OpFace<T>>(E, pm.tm[PH_FACE], a, e);
+    grid_barrier(bar, kerr);
+    run_phase<OpInvert<HAMR_INV_2D, 0>>(E, pm.tm[PH_INV], a, e);
+    grid_barrier(bar, kerr);
+    run_phase<OpBoundX1>(E, pm.tm[PH_BX1], a, e);
+    grid_barrier(bar, kerr);
+    run_phase<OpBoundX3>(E, pm.tm[PH_BX3], a, e);
+    grid_barrier(bar, kerr);
+    run_phase<OpBoundX2>(E, pm.tm[PH_BX2], a, e);
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -275,6 +381,11 @@ struct hamr_batch {
     float tuned_ms[PH_N] = {};
     cudaGraphExec_t graph = nullptr;
     int graph_steps = -1, graph_interval = -1;
+    // one persistent launch per sub-step (hamr_batch_set_persistent)
+    bool persistent = false;
+    int persist_grid = 0;        // CTAs of the cooperative launch
+    unsigned *bar = nullptr;     // grid barrier: arrivals, generation
+    int *kerr = nullptr;         // set when a barrier wait gave up
 };
 
 namespace {
@@ -369,8 +480,45 @@ void batch_stage(hamr_batch *b, int full, bool calc_dt, int only = -1) {
 
 unsigned nblk_b(int n) { return (unsigned)((n + 127) / 128); }
 
+// one sub-step of every block in one cooperative launch (k_batch_stage)
+int batch_stage_persistent(hamr_batch *b, int full, bool calc_dt) {
+    PhaseMaps pm;
+    for (int ph = 0; ph < PH_N; ph++)
+        pm.tm[ph] = b->ntiles[ph] ? TileMap{b->dstart[ph], b->dorder[ph], b->n, b->tile[ph]}
+                                  : TileMap{nullptr, nullptr, 0, BLK};
+    StageArg a{full, calc_dt ? 1 : 0, full ? 1.0 : 0.5};
+    const BEntry *E = b->E;
+    void *args[] = {(void *)&E, (void *)&pm, (void *)&a, (void *)&b->bar, (void *)&b->kerr};
+    const void *fn = b->precision == HAMR_MIXED ? (const void *)k_batch_stage<float>
+                                                : (const void *)k_batch_stage<double>;
+    BCK(cudaMemsetAsync(b->bar, 0, 2 * sizeof(unsigned), b->stream));
+    BCK(cudaLaunchCooperativeKernel(fn, dim3(b->persist_grid), dim3(BLK), args, 0, b->stream));
+    return HAMR_OK;
+}
+
+// the persistent kernels' error word (a barrier wait that gave up), read after
+// the caller's synchronisation and cleared
+int batch_check_kerr(hamr_batch *b) {
+    if (!b->kerr) return HAMR_OK;
+    int v = 0;
+    BCK(cudaMemcpyAsync(&v, b->kerr, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    if (!v) return HAMR_OK;
+    BCK(cudaMemsetAsync(b->kerr, 0, sizeof(int), b->stream));
+    b->err = "a grid barrier of the persistent sub-step timed out (the step's results are invalid)";
+    return HAMR_E_CUDA;
+}
+
 // one RK2 step of every block: step sizes from b->dts (frac 1/2, then 1)
 int batch_step_launch(hamr_batch *b, int update, int interval) {
+    if (b->persistent) {
+        int rc = batch_stage_persistent(b, 0, false);
+        if (!rc) rc = batch_stage_persistent(b, 1, true);
+        if (rc) return rc;
+        k_batch_dt_finalize<<<nblk_b(b->n), 128, 0, b->stream>>>(b->E, b->n, update, interval);
+        BCK(cudaGetLastError());
+        return HAMR_OK;
+    }
     batch_stage(b, 0, false);
     batch_stage(b, 1, true);
     k_batch_dt_finalize<<<nblk_b(b->n), 128, 0, b->stream>>>(b->E, b->n, update, interval);
@@ -479,6 +627,8 @@ int hamr_batch_destroy(hamr_batch *b) {
     cudaFree(b->dts);
     cudaFree(b->ndts);
     cudaFree(b->counters);
+    cudaFree(b->bar);
+    cudaFree(b->kerr);
     for (int ph = 0; ph < PH_N; ph++) {
         cudaFree(b->dstart[ph]);
         cudaFree(b->dorder[ph]);
@@ -498,6 +648,7 @@ int hamr_batch_step(hamr_batch *b, const double *dt, double *dt_next) {
     k_batch_dt_reset<<<nblk_b(b->n), 128, 0, b->stream>>>(b->E, b->n);
     int rc = batch_step_launch(b, 0, 0);
     if (rc) return rc;
+    if (b->persistent && (rc = batch_check_kerr(b))) return rc;
     if (dt_next) {
         BCK(cudaMemcpyAsync(dt_next, b->ndts, sizeof(double) * b->n, cudaMemcpyDeviceToHost, b->stream));
         BCK(cudaStreamSynchronize(b->stream));
@@ -538,6 +689,47 @@ int hamr_batch_advance(hamr_batch *b, int nsteps, int interval, double *dt_inout
     BCK(cudaGraphLaunch(b->graph, b->stream));
     BCK(cudaMemcpyAsync(dt_inout, b->dts, sizeof(double) * b->n, cudaMemcpyDeviceToHost, b->stream));
     BCK(cudaStreamSynchronize(b->stream));
+    return b->persistent ? batch_check_kerr(b) : HAMR_OK;
+}
+
+// One persistent cooperative launch per sub-step instead of one launch per
+// phase (PPM, HLL, Noble 2D, no floors or repair; the tile maps stay those
+// of the autotuner or the default). The grid is every CTA the device can
+// hold at once at the kernel's register budget.
+int hamr_batch_set_persistent(hamr_batch *b, int on) {
+    if (!b) return HAMR_E_ARG;
+    if (!on) {
+        b->persistent = false;
+    } else {
+        if (b->recon != HAMR_RECON_PPM || b->riemann != HAMR_RIEMANN_HLL || b->inversion != HAMR_INV_2D || b->fix)
+            return HAMR_E_ARG;
+        int dev = 0, coop = 0, per_sm = 0;
+        BCK(cudaGetDevice(&dev));
+        BCK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+        if (!coop) {
+            b->err = "the device does not support cooperative launches";
+            return HAMR_E_CUDA;
+        }
+        const void *fn = b->precision == HAMR_MIXED ? (const void *)k_batch_stage<float>
+                                                    : (const void *)k_batch_stage<double>;
+        BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, BLK, 0));
+        if (per_sm < 1) {
+            b->err = "the persistent sub-step kernel does not fit on a multiprocessor";
+            return HAMR_E_CUDA;
+        }
+        if (!b->bar) BCK(cudaMalloc(&b->bar, 2 * sizeof(unsigned)));
+        if (!b->kerr) BCK(cudaMalloc(&b->kerr, sizeof(int)));
+        BCK(cudaMemsetAsync(b->bar, 0, 2 * sizeof(unsigned), b->stream));
+        BCK(cudaMemsetAsync(b->kerr, 0, sizeof(int), b->stream));
+        BCK(cudaStreamSynchronize(b->stream));
+        b->persist_grid = per_sm * b->nsm;
+        b->persistent = true;
+    }
+    if (b->graph) {   // the captured advance holds the other launch form
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+        b->graph_steps = b->graph_interval = -1;
+    }
     return HAMR_OK;
 }
 

@@ -52,9 +52,11 @@ struct Dims {
 
 struct Geom {
     const double *gcov, *gcon, *gdet, *conn;
-    // per (i, j) column at the zone centre, when tabulated (else null): 1/gdet,
-    // the lapse 1/sqrt(-g^tt) and n_t = -sqrt(-1/g^tt), each computed with the
-    // inversion's own operations (k_inv_tab), planes of gs
+    // per (i, j) column, when tabulated (else null), planes of gs: at the zone
+    // centre 1/gdet, the lapse 1/sqrt(-g^tt) and n_t = -sqrt(-1/g^tt), each
+    // with the inversion's own operations; then 1/gdet at the FACE1, FACE2
+    // and FACE3 locations (the face update's divisions by the face volume)
+    // (k_inv_tab)
     const double *itab = nullptr;
 };
 
@@ -69,6 +71,12 @@ __device__ __forceinline__ void load_geo(const Dims &d, const Geom &m, int i, in
         o.gcov[s] = __ldg(&m.gcov[(long)(s * 5 + loc) * d.gs + idx]);
     }
     o.g = __ldg(&m.gdet[(long)loc * d.gs + idx]);
+}
+
+// temp / (face volume at plane `plane` of the column table), exactly
+__device__ __forceinline__ double div_face_volume(const Dims &d, const Geom &m, double temp, double gdf, int plane,
+                                                  long gi) {
+    return m.itab ? div_rcp_inf(temp, gdf, __ldg(&m.itab[(long)plane * d.gs + gi])) : temp / gdf;
 }
 
 // metric at one point, stored in double, used in the arithmetic type T
@@ -696,14 +704,14 @@ __device__ __forceinline__ void face_update_eval(const Dims &d, const Geom &m, c
         temp += 1.0 / ((double)1) * psi[c] * gdf;
         temp += div_rcp(-Dt, d.dx2, d.rdx2) * (E(3, 0, 1, 0) - E(3, 0, 0, 0));
         if (d.ng3 > 0) temp += div_rcp(Dt, d.dx3, d.rdx3) * (E(2, 0, 0, 1) - E(2, 0, 0, 0));
-        psf[c] = temp / gdf;
+        psf[c] = div_face_volume(d, m, temp, gdf, 3, gi);
     }
     if ((faces & 4) && d.ng3 > 0 && i < d.n1 + d.ng1 && j < d.n2 + d.ng2 && z < d.n3 + d.ng3 + d.d3) {
         const double gdf = __ldg(&m.gdet[FACE3 * d.gs + gi]);
         double temp = psi[2 * ks + c] * gdf;
         temp += div_rcp(-Dt, d.dx1, d.rdx1) * (E(2, 1, 0, 0) - E(2, 0, 0, 0));
         temp += div_rcp(Dt, d.dx2, d.rdx2) * (E(1, 0, 1, 0) - E(1, 0, 0, 0));
-        psf[2 * ks + c] = temp / gdf;
+        psf[2 * ks + c] = div_face_volume(d, m, temp, gdf, 5, gi);
     }
     if ((faces & 2) && i < d.n1 + d.ng1 && j < d.n2 + d.ng2 + d.d2 && z < d.n3 + d.ng3) {
         const double gdf = __ldg(&m.gdet[FACE2 * d.gs + gi]);
@@ -711,7 +719,7 @@ __device__ __forceinline__ void face_update_eval(const Dims &d, const Geom &m, c
         temp += 1.0 / ((double)1) * psi[1 * ks + c] * gdf;
         temp += div_rcp(Dt, d.dx1, d.rdx1) * (E(3, 1, 0, 0) - E(3, 0, 0, 0));
         if (d.ng3 > 0) temp += div_rcp(-Dt, d.dx3, d.rdx3) * (E(1, 0, 0, 1) - E(1, 0, 0, 0));
-        psf[1 * ks + c] = temp / gdf;
+        psf[1 * ks + c] = div_face_volume(d, m, temp, gdf, 4, gi);
     }
 }
 
@@ -1139,7 +1147,11 @@ __global__ void k_inv_tab(const Dims d, const double *__restrict__ gcon, const d
     itab[idx] = 1.0 / g;
     itab[d.gs + idx] = 1.0 / sqrt(-g00);
     itab[2 * d.gs + idx] = -sqrt(-1. / g00);
+    itab[3 * d.gs + idx] = 1.0 / gdet[(long)FACE1 * d.gs + idx];
+    itab[4 * d.gs + idx] = 1.0 / gdet[(long)FACE2 * d.gs + idx];
+    itab[5 * d.gs + idx] = 1.0 / gdet[(long)FACE3 * d.gs + idx];
 }
+
 
 // primary solver: Noble 2D, or Newman-Hamlin in its place (NEWMAN builds)
 template <int INV>
@@ -1921,7 +1933,7 @@ struct hamr_ctx {
     double *W = nullptr;  // updated conserved variables between k_cons and k_invert
     int *pflag = nullptr, *failimage = nullptr;
     double *gcov = nullptr, *gcon = nullptr, *gdet = nullptr, *conn = nullptr;
-    double *itab = nullptr;   // the inversion's column table (k_inv_tab), 3 planes of gs
+    double *itab = nullptr;   // the column table of reciprocals (k_inv_tab), 6 planes of gs
     unsigned long long *dtbits = nullptr;
     double *ndt = nullptr, *dt_state = nullptr;
     int *counter = nullptr;
@@ -2296,7 +2308,7 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
         {(void **)&ctx->failimage, 5 * sizeof(int) * d.ks},
         {(void **)&ctx->gcov, 50 * sizeof(double) * d.gs}, {(void **)&ctx->gcon, 50 * sizeof(double) * d.gs},
         {(void **)&ctx->gdet, 5 * sizeof(double) * d.gs}, {(void **)&ctx->conn, 40 * sizeof(double) * d.gs},
-        {(void **)&ctx->itab, 3 * sizeof(double) * d.gs},
+        {(void **)&ctx->itab, 6 * sizeof(double) * d.gs},
         {(void **)&ctx->dtbits, 4 * sizeof(unsigned long long)}, {(void **)&ctx->ndt, sizeof(double)},
         {(void **)&ctx->dt_state, sizeof(double)}, {(void **)&ctx->counter, sizeof(int)},
         {(void **)&ctx->divb, sizeof(unsigned long long)},

@@ -89,13 +89,13 @@ __device__ __forceinline__ double div_rcp(double a, double b, double rb) {
     return r == 0.0 ? q0 : fma(r, rb, q0);
 }
 
-// div_rcp that also returns the IEEE quotient for an infinite dividend (the
-// residual of an infinite q0 is NaN): for the inversion, which may meet an
-// overflowed state before it reports the failure
+// div_rcp that also returns the IEEE quotient where an operand is infinite
+// or the divisor zero: there the residual is not finite (0 * inf or
+// inf - inf) and q0 is already the IEEE result (+-inf, +-0 or NaN)
 __device__ __forceinline__ double div_rcp_inf(double a, double b, double rb) {
     const double q0 = a * rb;
     const double r = fma(-q0, b, a);
-    return (r == 0.0 || isinf(q0)) ? q0 : fma(r, rb, q0);
+    return (r == 0.0 || !(fabs(r) <= 1.7976931348623157e308)) ? q0 : fma(r, rb, q0);
 }
 
 // Quotients a_k / b that share one divisor. In double precision: one IEEE
@@ -363,9 +363,10 @@ __device__ __forceinline__ int guess_utsq(const double *gcov, const double *prim
 }
 
 __device__ __forceinline__ void set_velocity(const InvQ &s, double gamma, double W, double *prim) {
+    const Divisor<double> dw(W);   // the three quotients by W
     for (int i = 1; i < 4; i++) {
         double Qtcon = s.Qcon[i] + s.ncon[i] * s.Qdotn;
-        prim[U1 + i - 1] = gamma / (W + s.Bsq) * (Qtcon + s.QdotB * s.Bcon[i] / W);
+        prim[U1 + i - 1] = gamma / (W + s.Bsq) * (Qtcon + dw.div(s.QdotB * s.Bcon[i]));
     }
 }
 
@@ -432,6 +433,9 @@ __device__ __forceinline__ int utoprim_2d_k(const InvK &k, const double *U, cons
     double f = 1., df = 1., errx = 1.;
     int n_iter = 0, i_extra = 0, doing_extra = 0, keep = 1;
     const double Bsq = s.Bsq, Qtsq = s.Qtsq, QdotBsq = s.QdotBsq, Qdotn = s.Qdotn, D = s.D;
+    // 1/x0 of the current iterate: t23 of this iteration, and the divisor of
+    // the previous iteration's errx (the same x0), one reciprocal for both
+    double rx0 = 1. / x0;
     while (keep) {
         double Wsq = x0 * x0;
         double gtmp = 1. - x1;
@@ -446,7 +450,7 @@ __device__ __forceinline__ int utoprim_2d_k(const InvK &k, const double *U, cons
         double t16 = QdotBsq * t9;
         double t18 = -Qdotn - 0.5 * Bsq * (1.0 + x1) + 0.5 * t16 - x0 + p_tmp;
         double t21 = 1. / t3;
-        double t23 = 1. / x0;
+        double t23 = rx0;
         double t24 = t16 * t23;
         double t25 = -1.0 + dPdW - t24;
         double t35 = t25 * t3 + (Bsq - 2.0 * dPdvsq) * (QdotBsq + x1 * Wsq * x0) * t9 * t23;
@@ -463,7 +467,8 @@ __device__ __forceinline__ int utoprim_2d_k(const InvK &k, const double *U, cons
         x0 = (x0 > W_TOO_BIG) ? xo0 : x0;
         x1 = (x1 < 0.) ? 0. : x1;
         x1 = (x1 > 1.) ? (1. - 1.e-15) : x1;
-        errx = (x0 == 0.) ? fabs(x0 - xo0) : fabs((x0 - xo0) / x0);
+        rx0 = 1. / x0;
+        errx = (x0 == 0.) ? fabs(x0 - xo0) : fabs(div_rcp_inf(x0 - xo0, x0, rx0));
         if ((fabs(errx) <= NEWT_TOL) && (doing_extra == 0) && (EXTRA_NEWT_ITER > 0)) doing_extra = 1;
         if (doing_extra == 1) i_extra++;
         if (((fabs(errx) <= NEWT_TOL) && (doing_extra == 0)) || (i_extra > EXTRA_NEWT_ITER) || (n_iter >= (MAX_NEWT_ITER - 1)))
@@ -857,8 +862,9 @@ __device__ __forceinline__ void vchar_ft(T gam, const T *pr, const T *ucon, cons
     if ((discr < T(0.0)) && (discr > T(-1.e-10))) discr = T(0.0);
     else if (discr < T(-1.e-10)) discr = T(0.);
     discr = d_sqrt(discr);
-    const T vp = -(-B + discr) / (T(2.) * A);
-    const T vm = -(-B - discr) / (T(2.) * A);
+    const Divisor<T> d2a(T(2.) * A);
+    const T vp = d2a.div(-(-B + discr));
+    const T vm = d2a.div(-(-B - discr));
     if (vp > vm) { *vmax = vp; *vmin = vm; }
     else { *vmax = vm; *vmin = vp; }
 }
@@ -877,9 +883,10 @@ __device__ __forceinline__ void hllc_hydro(int dir, const T *lu, const T *ru, T 
     const T ptot = -(-FH[1][UU]) * vcon + FH[1][U_1];
     if (!(d_fabs(ptot) > T(0.)) || (vcon < cmin) || (vcon > cmax) || !(d_fabs(vcon) > T(0.))) fail = true;
     if (cmax > iv && vcon <= iv && !fail) {
-        const T s = (cmax - ru[dir] / ru[0]) / (cmax - vcon + T(SMALL_D));
+        const Divisor<T> dc(cmax - vcon + T(SMALL_D));
+        const T s = dc.div(cmax - ru[dir] / ru[0]);
         FT[0][RHO] = s * Ur[RHO];
-        FT[0][UU] = (cmax * Ur[UU] + Ur[U_1] - ptot * vcon) / (cmax - vcon + T(SMALL_D));
+        FT[0][UU] = dc.div(cmax * Ur[UU] + Ur[U_1] - ptot * vcon);
         FT[0][U_1] = (-FT[0][UU] + ptot) * vcon;
         FT[0][U_2] = s * Ur[U_2];
         FT[0][U_3] = s * Ur[U_3];
@@ -889,9 +896,10 @@ __device__ __forceinline__ void hllc_hydro(int dir, const T *lu, const T *ru, T 
         FT[0][KTOT] = s * Ur[KTOT];
         for (int k = 0; k < NPR; k++) FT[1][k] = (Fr[k] + cmax * (FT[0][k] - Ur[k]));
     } else if (cmin < iv && vcon >= iv && !fail) {
-        const T s = (cmin - lu[dir] / lu[0]) / (cmin - vcon + T(SMALL_D));
+        const Divisor<T> dc(cmin - vcon + T(SMALL_D));
+        const T s = dc.div(cmin - lu[dir] / lu[0]);
         FT[0][RHO] = s * Ul[RHO];
-        FT[0][UU] = (cmin * Ul[UU] + Ul[U_1] - ptot * vcon) / (cmin - vcon + T(SMALL_D));
+        FT[0][UU] = dc.div(cmin * Ul[UU] + Ul[U_1] - ptot * vcon);
         FT[0][U_1] = (-FT[0][UU] + ptot) * vcon;
         FT[0][U_2] = s * Ul[U_2];
         FT[0][U_3] = s * Ul[U_3];
@@ -920,37 +928,37 @@ __device__ __forceinline__ void hllc_mhd(int dir, const T *lu, const T *ru, T iv
     const T C = FH[0][U_1] - (FH[0][B_2] * FH[1][B_2] + FH[0][B_3] * FH[1][B_3]);
     const T D = B * B - T(4.) * A * C;
     vcon[G_1] = (-B - d_sqrt(D)) / (T(2.) * A);
-    vcon[G_2] = (FH[0][B_2] * vcon[G_1] - FH[1][B_2]) / FH[0][B_1];
-    vcon[G_3] = (FH[0][B_3] * vcon[G_1] - FH[1][B_3]) / FH[0][B_1];
+    const Divisor<T> db(FH[0][B_1]);
+    vcon[G_2] = db.div(FH[0][B_2] * vcon[G_1] - FH[1][B_2]);
+    vcon[G_3] = db.div(FH[0][B_3] * vcon[G_1] - FH[1][B_3]);
     const T gammasq = T(1.) / (T(1.) - (vcon[1] * vcon[1] + vcon[2] * vcon[2] + vcon[3] * vcon[3]));
+    const Divisor<T> dg(gammasq);
     const T vB = (vcon[1] * FH[0][B1] + vcon[2] * FH[0][B2] + vcon[3] * FH[0][B3]);
-    const T ptot = -(-FH[1][UU] - FH[0][B_1] * (vB)) * vcon[dir] + FH[1][U_1] + FH[0][B_1] * FH[0][B_1] / gammasq;   // pow(x, 2): x*x is its correctly rounded value
+    const T ptot = -(-FH[1][UU] - FH[0][B_1] * (vB)) * vcon[dir] + FH[1][U_1] + dg.div(FH[0][B_1] * FH[0][B_1]);   // pow(x, 2): x*x is its correctly rounded value
     if (!(d_fabs(ptot) > T(0.)) || (vcon[G_1] < cmin) || (vcon[G_1] > cmax) || !(d_fabs(vcon[G_1]) > T(0.))) fail = true;
     if (cmax > iv && vcon[dir] <= iv && !fail) {
-        FT[0][RHO] = (cmax - ru[dir] / ru[0]) / (cmax - vcon[dir] + T(SMALL_D)) * Ur[RHO];
-        FT[0][UU] = (cmax * Ur[UU] + Ur[U_1] - ptot * vcon[dir] + vB * FH[0][B_1]) / (cmax - vcon[dir] + T(SMALL_D));
+        const Divisor<T> dc(cmax - vcon[dir] + T(SMALL_D));
+        FT[0][RHO] = dc.div(cmax - ru[dir] / ru[0]) * Ur[RHO];
+        FT[0][UU] = dc.div(cmax * Ur[UU] + Ur[U_1] - ptot * vcon[dir] + vB * FH[0][B_1]);
         FT[0][U_1] = (-FT[0][UU] + ptot) * vcon[dir] - vB * FH[0][B_1];
-        FT[0][U_2] = (-FH[0][B_1] * (FH[0][B_2] / (gammasq) + vB * vcon[G_2]) + cmax * Ur[U_2] - Fr[U_2]) /
-                     (cmax - vcon[dir] + T(SMALL_D));
-        FT[0][U_3] = (-FH[0][B_1] * (FH[0][B_3] / (gammasq) + vB * vcon[G_3]) + cmax * Ur[U_3] - Fr[U_3]) /
-                     (cmax - vcon[dir] + T(SMALL_D));
+        FT[0][U_2] = dc.div(-FH[0][B_1] * (dg.div(FH[0][B_2]) + vB * vcon[G_2]) + cmax * Ur[U_2] - Fr[U_2]);
+        FT[0][U_3] = dc.div(-FH[0][B_1] * (dg.div(FH[0][B_3]) + vB * vcon[G_3]) + cmax * Ur[U_3] - Fr[U_3]);
         FT[0][B_1] = FH[0][B_1];
         FT[0][B_2] = FH[0][B_2];
         FT[0][B_3] = FH[0][B_3];
-        FT[0][KTOT] = (cmax - ru[dir] / ru[0]) / (cmax - vcon[dir] + T(SMALL_D)) * Ur[KTOT];
+        FT[0][KTOT] = dc.div(cmax - ru[dir] / ru[0]) * Ur[KTOT];
         for (int k = 0; k < NPR; k++) FT[1][k] = (Fr[k] + cmax * (FT[0][k] - Ur[k]));
     } else if (cmin < iv && vcon[dir] >= iv && !fail) {
-        FT[0][RHO] = (cmin - lu[dir] / lu[0]) / (cmin - vcon[dir] + T(SMALL_D)) * Ul[RHO];
-        FT[0][UU] = (cmin * Ul[UU] + Ul[U_1] - ptot * vcon[dir] + vB * FH[0][B_1]) / (cmin - vcon[dir] + T(SMALL_D));
+        const Divisor<T> dc(cmin - vcon[dir] + T(SMALL_D));
+        FT[0][RHO] = dc.div(cmin - lu[dir] / lu[0]) * Ul[RHO];
+        FT[0][UU] = dc.div(cmin * Ul[UU] + Ul[U_1] - ptot * vcon[dir] + vB * FH[0][B_1]);
         FT[0][U_1] = (-FT[0][UU] + ptot) * vcon[dir] - vB * FH[0][B_1];
-        FT[0][U_2] = (-FH[0][B_1] * (FH[0][B_2] / (gammasq) + vB * vcon[G_2]) + cmin * Ul[U_2] - Fl[U_2]) /
-                     (cmin - vcon[dir] + T(SMALL_D));
-        FT[0][U_3] = (-FH[0][B_1] * (FH[0][B_3] / (gammasq) + vB * vcon[G_3]) + cmin * Ul[U_3] - Fl[U_3]) /
-                     (cmin - vcon[dir] + T(SMALL_D));
+        FT[0][U_2] = dc.div(-FH[0][B_1] * (dg.div(FH[0][B_2]) + vB * vcon[G_2]) + cmin * Ul[U_2] - Fl[U_2]);
+        FT[0][U_3] = dc.div(-FH[0][B_1] * (dg.div(FH[0][B_3]) + vB * vcon[G_3]) + cmin * Ul[U_3] - Fl[U_3]);
         FT[0][B_1] = FH[0][B_1];
         FT[0][B_2] = FH[0][B_2];
         FT[0][B_3] = FH[0][B_3];
-        FT[0][KTOT] = (cmin - lu[dir] / lu[0]) / (cmin - vcon[dir] + T(SMALL_D)) * Ul[KTOT];
+        FT[0][KTOT] = dc.div(cmin - lu[dir] / lu[0]) * Ul[KTOT];
         for (int k = 0; k < NPR; k++) FT[1][k] = (Fl[k] + cmin * (FT[0][k] - Ul[k]));
     } else {
         for (int k = 0; k < NPR; k++) { FT[0][k] = FH[0][k]; FT[1][k] = FH[1][k]; }
@@ -1238,9 +1246,10 @@ __device__ __forceinline__ T hllc_face(T gam, const T *pl, const T *pr, const Ge
     } else if (cmin >= iv) {
         for (int k = 0; k < NPR; k++) { FT[0][k] = Ul[k]; FT[1][k] = Fl[k]; }
     } else {
-        for (int k = 0; k < NPR; k++) FH[0][k] = (Fl[k] - Fr[k] + cmax * Ur[k] - cmin * Ul[k]) / (cmax - cmin + T(SMALL_D));
+        const Divisor<T> dh(cmax - cmin + T(SMALL_D));   // the 18 HLL-state quotients share it
+        for (int k = 0; k < NPR; k++) FH[0][k] = dh.div(Fl[k] - Fr[k] + cmax * Ur[k] - cmin * Ul[k]);
         for (int k = 0; k < NPR; k++)
-            FH[1][k] = ((cmax * Fl[k] - cmin * Fr[k] + cmax * cmin * (Ur[k] - Ul[k])) / (cmax - cmin + T(SMALL_D)));
+            FH[1][k] = dh.div(cmax * Fl[k] - cmin * Fr[k] + cmax * cmin * (Ur[k] - Ul[k]));
         const bool do_hydro = d_fabs(FH[0][DIR + B1 - 1] * FH[0][DIR + B1 - 1] * lu[0] * ru[0]) < T(1.e-10) * d_fabs(FH[0][UU]);
         if (do_hydro) hllc_hydro(DIR, lu, ru, iv, cmin, cmax, FT, FH, Fl, Fr, Ul, Ur);
         else if constexpr (HLLD) hlld_mhd(DIR, lu, ru, iv, cmin, cmax, FT, FH, Fl, Fr, Ul, Ur);

@@ -298,6 +298,16 @@ int hamr_batch_advance(hamr_batch *b, int nsteps, int interval, double *dt_inout
  * launches per candidate, and keeps the fastest. Leaves p and ps untouched. */
 int hamr_batch_autotune(hamr_batch *b, const double *dt, int reps);
 
+/* One persistent cooperative launch per sub-step (on != 0) instead of one
+ * launch per phase: every CTA the device holds at once runs all phases of the
+ * sub-step, with a grid-wide barrier (bounded waits; a wait that gives up is
+ * reported as HAMR_E_CUDA) wherever a phase reads what the previous wrote.
+ * For PPM, HLL, Noble 2D, no floors or repair (else HAMR_E_ARG); the phases
+ * keep their tile maps. Replaces the role of GPU_step_ch's per-kernel
+ * launches (step_ch.c:916-1335) for a whole ensemble; no reference
+ * counterpart. */
+int hamr_batch_set_persistent(hamr_batch *b, int on);
+
 /* The launch shape chosen for each of the HAMR_BATCH_PHASES phases (order:
  * flux x3, x2, x1, polar flux fix, centre EMF, edge EMF, polar EMF average,
  * face update, conserved update, inversion, ghost fill x1, x3, x2) and its

@@ -18,6 +18,7 @@
  *   LU_decompose, LU_substitution, invert_matrix  lu.c
  *   set_grid loop                 main.c:380-455
  */
+#include <float.h>
 #include <math.h>
 #include <string.h>
 
@@ -366,8 +367,8 @@ long ho_div_rcp_mismatches(const double *a, long n, const double *b, long m) {
     return ho_div_rcp_mismatches_g(a, n, b, m, 0);
 }
 
-/* The same with the infinite-dividend guard of the inversion's form (guard =
- * 1): q = (r == 0 || isinf(q0)) ? q0 : fma(r, rb, q0). */
+/* The same with the guard of the form that also covers infinite operands and
+ * a zero divisor (guard = 1): q = (r == 0 || r not finite) ? q0 : fma(r, rb, q0). */
 long ho_div_rcp_mismatches_g(const double *a, long n, const double *b, long m, int guard) {
     long bad = 0;
 #pragma omp parallel for reduction(+ : bad) schedule(static)
@@ -376,7 +377,7 @@ long ho_div_rcp_mismatches_g(const double *a, long n, const double *b, long m, i
         for (long i = 0; i < n; i++) {
             const double q0 = a[i] * rb;
             const double r = fma(-q0, b[j], a[i]);
-            const double q = (r == 0.0 || (guard && isinf(q0))) ? q0 : fma(r, rb, q0);
+            const double q = (r == 0.0 || (guard && !(fabs(r) <= DBL_MAX))) ? q0 : fma(r, rb, q0);
             const double e = a[i] / b[j];
             if (memcmp(&q, &e, sizeof(double)) != 0) bad++;
         }

@@ -46,11 +46,12 @@ def test_div_rcp_matches_ieee_division():
 
 
 def test_div_rcp_inversion_divisors():
-    """The inversion's form (div_rcp_inf) divides by gamma and by the metric
-    determinant of the zone: adiabatic indices and sqrt(-g) over the range of
-    the torus grids (log-uniform from 1e-4 to 1e7), dividends over the exact
-    range, and infinite dividends (an overflowed state), which the guard
-    returns as the IEEE quotient does."""
+    """The guarded form (div_rcp_inf, used by the inversion and wherever
+    quotients share a divisor) on the inversion's divisors -- adiabatic
+    indices and sqrt(-g) over the range of the torus grids (log-uniform from
+    1e-4 to 1e7) -- with dividends over the exact range and infinite
+    dividends (an overflowed state), which the guard returns as the IEEE
+    quotient does; and with infinite and zero divisors."""
     rng = np.random.default_rng(77)
     b = np.concatenate([[13 / 9, 4 / 3, 5 / 3, 1.4, 2.0],
                         np.exp(rng.uniform(np.log(1e-4), np.log(1e7), 120))])
@@ -62,3 +63,11 @@ def test_div_rcp_inversion_divisors():
     assert O.lib().ho_div_rcp_mismatches_g(*args, 1) == 0
     # without the guard only the infinite dividends differ (NaN for +-inf)
     assert O.lib().ho_div_rcp_mismatches_g(*args, 0) == 2 * b.size
+    # infinite and zero divisors (no NaN results here: their bit patterns
+    # are not compared)
+    a2 = np.ascontiguousarray([1.0, -3.5, 1e-300, 7e300, np.inf, -np.inf])
+    for bad in ([np.inf, -np.inf], [0.0, -0.0]):
+        aa = a2 if bad[0] == 0.0 else a2[:4]
+        b2 = np.ascontiguousarray(bad)
+        assert O.lib().ho_div_rcp_mismatches_g(aa.ctypes.data_as(ctypes.c_void_p), aa.size,
+                                               b2.ctypes.data_as(ctypes.c_void_p), b2.size, 1) == 0

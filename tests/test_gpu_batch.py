@@ -201,3 +201,42 @@ def test_batch_refuses_mixed_opt_ins_and_the_neighbour_repair():
     with pytest.raises(_lib.HamrError):
         Batch(c)
     _close(a + b + c)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_persistent_batch_matches_phase_launches(precision):
+    """One persistent cooperative launch per sub-step (every phase in one
+    kernel, grid-wide barriers between dependent phases) against one launch
+    per phase: bit for bit, stepwise and through the captured advance, with
+    the ensemble's 3-D members and the 2-D member with reflective poles (the
+    polar flux fix as an extra phase), after autotuning the tile maps."""
+    pbs, a = _members(precision)
+    _, b = _members(precision)
+    ba, bb = Batch(a), Batch(b)
+    dts = np.array([0.2 * min(pb.dx[:2]) for pb in pbs])
+    ba.autotune(dts, reps=1)
+    ba.set_persistent(True)
+    for _ in range(2):
+        np.testing.assert_array_equal(ba.step(dts), bb.step(dts))
+    np.testing.assert_array_equal(ba.advance(4, dts, interval=2), bb.advance(4, dts, interval=2))
+    for x, y in zip(a, b):
+        px, sx = x.download()
+        py, sy = y.download()
+        assert np.isfinite(px).all()
+        np.testing.assert_array_equal(px, py)
+        np.testing.assert_array_equal(sx, sy)
+        np.testing.assert_array_equal(x.download_flags()[1], y.download_flags()[1])
+    ba.set_persistent(False)   # back to per-phase launches: still identical
+    np.testing.assert_array_equal(ba.step(dts), bb.step(dts))
+    ba.close()
+    bb.close()
+    _close(a + b)
+
+
+def test_persistent_batch_refuses_other_solvers():
+    pbs, a = _members(with_2d=False, riemann="hllc")
+    ba = Batch(a)
+    with pytest.raises(Exception):
+        ba.set_persistent(True)
+    ba.close()
+    _close(a)
