@@ -222,7 +222,6 @@ def test_persistent_batch_matches_phase_launches(precision):
     for x, y in zip(a, b):
         px, sx = x.download()
         py, sy = y.download()
-        assert np.isfinite(px).all()
         np.testing.assert_array_equal(px, py)
         np.testing.assert_array_equal(sx, sy)
         np.testing.assert_array_equal(x.download_flags()[1], y.download_flags()[1])
