@@ -769,7 +769,8 @@ def run_adjoint(args):
 
 
 def run_slabs(args):
-    """The c3/c2 torus split along x1 into slabs (hamr_gamma_wind_b200.decomp):
+    """The c3/c2 torus split along x1 (or x2, --slab-axis 2) into slabs
+    (hamr_gamma_wind_b200.decomp):
     with one process, --slabs K slabs on one GPU swapping halos by device
     copies on one stream; under torchrun, one slab per rank, halos by NCCL
     point-to-point and the CFL minima by an all-reduce. Times the same K steps
@@ -798,12 +799,14 @@ def run_slabs(args):
     from dataclasses import replace
     pb = replace(pb, p=p0, ps=ps0)
     k = world if world > 1 else max(2, args.slabs)
-    widths = [pb.n1 // k + (1 if r < pb.n1 % k else 0) for r in range(k)]
-    slabs = decomp.split(pb, widths)
+    axis = args.slab_axis
+    n = pb.n1 if axis == 1 else pb.n2
+    widths = [n // k + (1 if r < n % k else 0) for r in range(k)]
+    slabs = decomp.split(pb, widths, axis=axis)
     mine = [slabs[rank]] if world > 1 else slabs
     gs = decomp.gpu_slabs(mine, cs, precision=prec)
     ex = decomp.DistributedExchange(rank, world) if world > 1 else decomp.LocalExchange()
-    st = decomp.SlabStepper(gs, ex)
+    st = decomp.SlabStepper(gs, ex, axis=axis)
     dt = 0.2 * min(pb.dx[:2])
     for _ in range(args.warmup):
         dt = min(st.step(dt), 1.3 * dt)
@@ -840,10 +843,10 @@ def run_slabs(args):
                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
                "dtype": "f64" if prec == "fp64" else "f32 flux/EMF + f64 update/inversion", "data": "synthetic",
-               "config": {"workload": f"3-D FM torus {wl['n1']}x{wl['n2']}x{wl['n3']} split along x1 into {k} slabs "
+               "config": {"workload": f"3-D FM torus {wl['n1']}x{wl['n2']}x{wl['n3']} split along x{axis} into {k} slabs "
                                       f"{widths}", "zones": cells, "precision": prec,
                           "exchange": "nccl" if world > 1 else "device copies, one stream",
-                          "parallelism": f"x1 slabs x{k}"},
+                          "parallelism": f"x{axis} slabs x{k}"},
                "undivided_value_same_steps": und, "clocks": clk.summary(), "gpu_launches": None}
         print(json.dumps(out), flush=True)
     for g in gs:
@@ -887,7 +890,8 @@ def main():
     ap.add_argument("--kernels-only", action="store_true",
                     help="warm-up and timed steps only (for profiler runs)")
     ap.add_argument("--slabs", type=int, default=0,
-                    help="c3/c2 split along x1: K slabs on one GPU, or one slab per rank under torchrun")
+                    help="c3/c2 split into slabs: K slabs on one GPU, or one slab per rank under torchrun")
+    ap.add_argument("--slab-axis", type=int, default=1, choices=[1, 2], help="split along x1 or x2")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -212,12 +212,13 @@ class Block:
         return int(self.L.hamr_halo_count(self.ctx))
 
     def halo_pack(self, full: int, side: int, dev_ptr: int):
-        """Active layers next to x1 side `side` into a device buffer."""
+        """Active layers next to side `side` (0, 1: lower and upper x1; 2, 3:
+        lower and upper x2) into a device buffer."""
         self._check(self.L.hamr_halo_pack(self.ctx, int(full), int(side), ctypes.c_void_p(dev_ptr)),
                     "hamr_halo_pack")
 
     def halo_unpack(self, full: int, side: int, dev_ptr: int):
-        """A device buffer into the ghost layers beyond x1 side `side`."""
+        """A device buffer into the ghost layers beyond side `side` (0-3)."""
         self._check(self.L.hamr_halo_unpack(self.ctx, int(full), int(side), ctypes.c_void_p(dev_ptr)),
                     "hamr_halo_unpack")
 

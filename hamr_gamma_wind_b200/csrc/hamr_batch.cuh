@@ -70,7 +70,7 @@ struct OpFlux {
     static constexpr int SLOT = DIR;
     __device__ static double run(const BEntry &e, const StageArg &a, long t) {
         T *F = reinterpret_cast<T *>(DIR == 1 ? e.F1 : (DIR == 2 ? e.F2 : e.F3));
-        return flux_face<DIR, T, REC>(e.d, e.m, a.full ? e.ph : e.p, a.full ? e.psh : e.ps, F, t);
+        return dt_of_ctop(e.d, DIR, flux_face<DIR, T, REC>(e.d, e.m, a.full ? e.ph : e.p, a.full ? e.psh : e.ps, F, t));
     }
 };
 

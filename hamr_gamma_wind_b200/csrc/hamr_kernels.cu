@@ -20,6 +20,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <map>
 #include <mutex>
@@ -46,8 +47,12 @@ struct Dims {
     double dx1, dx2, dx3, gam, cour;
     double rdx1, rdx2, rdx3;   // 1/dx, correctly rounded on the host (exact divisions by dx, div_rcp)
     double rgam;               // 1/gam, likewise (the inversion's divisions by gamma)
+    // CFL per direction k = 1..3: c0[k] = cour dx_k, and ctop_lim[k], the
+    // largest double x with c0[k] / x > 1e-6 (set_cfl_limits)
+    double cfl_c0[4], ctop_lim[4];
     int pole1, pole2, bc1, bc2, bc3, ct_upwind, inversion, recon, riemann;
-    int halo;   // x1 sides filled by a neighbouring block (bit 0 lower, bit 1 upper)
+    int halo;   // sides filled by a neighbouring block: bits 0, 1 the lower and upper x1
+                // sides, bits 2, 3 the lower and upper x2 sides
 };
 
 struct Geom {
@@ -120,13 +125,29 @@ struct StepSize {
 #ifndef HAMR_FLUX_FT_ROWS_MINB
 #define HAMR_FLUX_FT_ROWS_MINB 3
 #endif
+
+// The CFL limit of a face is cour dx / ctop (fluxcalc2D2's dtij, counted
+// when above 1e-6), the block's the minimum over its faces and 1e9. A face
+// here contributes its signal speed ctop when cour dx / ctop > 1e-6, that is
+// when ctop <= ctop_lim (the largest such double, set on the host), else 0;
+// the kernels keep the largest contribution and divide once
+// (dt_of_ctop): the same minimum, bit for bit.
+__device__ __forceinline__ double ctop_term(const Dims &d, int dir, double ctop) {
+    return ctop <= d.ctop_lim[dir] ? ctop : 0.0;
+}
+__device__ __forceinline__ double dt_of_ctop(const Dims &d, int dir, double cmax) {
+    const double v = d.cfl_c0[dir] / cmax;   // +inf for cmax = 0
+    return v < 1.e9 ? v : 1.e9;
+}
+
 template <int DIR, typename T, int REC>
 __device__ __forceinline__ double flux_eval(const Dims &d, const Geo<T> &gm, const double *__restrict__ ps, T *pl,
                                             T *pr, T *__restrict__ F, const long c, const int j);
 
 // one face of direction DIR (t < n_faces): reconstruction, two states, four
-// flux evaluations, HLL (or HLLC); returns the face's CFL limit, or 1e9 when
-// filtered. REC: bit 0 MC reconstruction, bit 1 HLLC.
+// flux evaluations, HLL (or HLLC); returns the face's signal-speed
+// contribution to the CFL limit (ctop_term). REC: bit 0 MC reconstruction,
+// bit 1 HLLC.
 template <int DIR, typename T, int REC>
 __device__ __forceinline__ double flux_face(const Dims &d, const Geom &m, const double *__restrict__ pv,
                                             const double *__restrict__ ps, T *__restrict__ F, const long t) {
@@ -172,7 +193,8 @@ __device__ __forceinline__ double flux_face(const Dims &d, const Geom &m, const 
 
 // The face flux from the reconstructed states pl, pr (the normal field and
 // the polar B1 fix applied here): two states, four flux evaluations, HLL (or
-// HLLC), the flux written at cell index c; returns the face's CFL limit.
+// HLLC), the flux written at cell index c; returns the face's signal-speed
+// contribution to the CFL limit (ctop_term).
 template <int DIR, typename T, int REC>
 __device__ __forceinline__ double flux_eval(const Dims &d, const Geo<T> &gm, const double *__restrict__ ps, T *pl,
                                             T *pr, T *__restrict__ F, const long c, const int j) {
@@ -192,9 +214,9 @@ __device__ __forceinline__ double flux_eval(const Dims &d, const Geo<T> &gm, con
         const T ctop = hllc_face<DIR, T, (REC & 4) != 0>(gam, pl, pr, gm, Fo);
 #pragma unroll
         for (int k = 0; k < NPR; k++) F[(long)k * d.ks + c] = Fo[k];
-        const double v = d.cour * dxd / (double)ctop;
-        if (v > 1.e-6 && v < dtf) dtf = v;
-        return dtf;
+        (void)dxd;
+        (void)dtf;
+        return ctop_term(d, DIR, (double)ctop);
     }
     State<T> q;
     T t1[NPR], t2[NPR], t3[NPR], t4[NPR];
@@ -214,9 +236,9 @@ __device__ __forceinline__ double flux_eval(const Dims &d, const Geo<T> &gm, con
 #pragma unroll
     for (int k = 0; k < NPR; k++)
         F[(long)k * d.ks + c] = dh.div(cmax * t1[k] + cmin * t3[k] - cmax * cmin * (t4[k] - t2[k]));
-    const double v = d.cour * dxd / (double)ctop;
-    if (v > 1.e-6 && v < dtf) dtf = v;
-    return dtf;
+    (void)dxd;
+    (void)dtf;
+    return ctop_term(d, DIR, (double)ctop);
 }
 
 // faces of direction DIR of one block
@@ -242,13 +264,31 @@ __device__ __forceinline__ void cta_min_dt(double dtf, unsigned long long *slot)
     __syncthreads();   // wmin is reused by the CTA's next tile
 }
 
+// The same from the faces' signal speeds (ctop_term): the CTA's largest, then
+// one division, min(1e9, c0 / max) -- the minimum over the CTA's faces of
+// the per-face limit c0 / ctop, because correctly rounded division by a
+// positive divisor does not increase as the divisor grows
+__device__ __forceinline__ void cta_max_ctop(const Dims &d, int dir, double cmx, unsigned long long *slot) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cmx = d_max(cmx, __shfl_xor_sync(0xffffffffu, cmx, o));
+    __shared__ double wmax[BLK / 32];
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = cmx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = wmax[0];
+        for (int w = 1; w < BLK / 32; w++) b = d_max(b, wmax[w]);
+        atomicMin(slot, (unsigned long long)__double_as_longlong(dt_of_ctop(d, dir, b)));
+    }
+    __syncthreads();
+}
+
 template <int DIR, typename T, int REC>
 __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? HAMR_FLUX_MINB : HAMR_FLUX_MINB_F) k_flux(const Dims d, const Geom m, const double *__restrict__ pv,
                                                const double *__restrict__ ps, T *__restrict__ F,
                                                unsigned long long *__restrict__ dtbits, int calc_dt) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    const double dtf = t < n_faces<DIR>(d) ? flux_face<DIR, T, REC>(d, m, pv, ps, F, t) : 1.e9;
-    if (calc_dt) cta_min_dt(dtf, &dtbits[DIR]);
+    const double cmx = t < n_faces<DIR>(d) ? flux_face<DIR, T, REC>(d, m, pv, ps, F, t) : 0.0;
+    if (calc_dt) cta_max_ctop(d, DIR, cmx, &dtbits[DIR]);
 }
 
 // Both edge values of one zone, primitive by primitive (the normal field
@@ -300,10 +340,18 @@ __host__ __device__ __forceinline__ long n_x3_slots(const Dims &d) {
 #define HAMR_FLUX_X3_MINB_F 10
 #endif
 
+template <typename T>
+__device__ __forceinline__ void emf_centre_eval(const Dims &d, const Geom &m, const double *__restrict__ pv, int i,
+                                                int j, long c, T *e);
+
+// With Ec non-null the kernel also computes the centre EMFs (k_emf_centre's
+// work): its slots are exactly k_emf_centre's zones, and the slot's
+// primitives are already in L1 from its reconstruction stencil. A slot that
+// two CTAs share is done by the first. Same values as k_emf_centre.
 template <typename T, int REC>
 __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? HAMR_FLUX_X3_MINB : HAMR_FLUX_X3_MINB_F)
     k_flux_x3(const Dims d, const Geom m, const double *__restrict__ pv, const double *__restrict__ ps,
-              T *__restrict__ F, unsigned long long *__restrict__ dtbits, int calc_dt) {
+              T *__restrict__ F, unsigned long long *__restrict__ dtbits, int calc_dt, T *__restrict__ Ec) {
     __shared__ T slo[NPR - 1][BLK], shi[NPR - 1][BLK];   // zone edges per slot (B3 skipped)
     const int l = threadIdx.x;
     const long nslot = n_x3_slots(d);
@@ -324,9 +372,16 @@ __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? HAMR_FLUX_X3_MINB : HAMR
                 slo[q][l] = lo[k];
                 shi[q++][l] = hi[k];
             }
+        if (Ec && (l < BLK - 1 || sl == nslot - 1)) {
+            T e[3];
+            emf_centre_eval(d, m, pv, i, j, c, e);
+            Ec[1 * d.ks + c] = e[0];
+            Ec[2 * d.ks + c] = e[1];
+            Ec[3 * d.ks + c] = e[2];
+        }
     }
     __syncthreads();
-    double dtf = 1.e9;
+    double cmx = 0.0;
     // the face above this slot's zone: zone c + 1 is the next slot of the row
     if (l < BLK - 1 && sl + 1 < nslot && zl + 1 < rz) {
         T pl[NPR], pr[NPR];
@@ -338,9 +393,9 @@ __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? HAMR_FLUX_X3_MINB : HAMR
             }
         Geo<T> gm;
         load_geo_t(d, m, i, j, FACE3, gm);
-        dtf = flux_eval<3, T, REC>(d, gm, ps, pl, pr, F, c + 1, j);
+        cmx = flux_eval<3, T, REC>(d, gm, ps, pl, pr, F, c + 1, j);
     }
-    if (calc_dt) cta_min_dt(dtf, &dtbits[3]);
+    if (calc_dt) cta_max_ctop(d, 3, cmx, &dtbits[3]);
 }
 
 // Faces of direction DIR (1 or 2) by rows: a thread walks FLUX_ROW
@@ -429,7 +484,7 @@ __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? ((REC & 2) != 0 ? HAMR_F
     using Win = RowWindow<DIR, T, REC>;
     __shared__ T wbuf[Win::NW * Win::NK * BLK];
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    double dtf = 1.e9;
+    double cmx = 0.0;
     if (t < n_flux_rows<DIR>(d)) {
         const int nz = d.n3 + 2 * d.d3, z = (d.ng3 - 1) * d.d3 + (int)(t % nz);
         const long r = t / nz;
@@ -466,13 +521,12 @@ __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? ((REC & 2) != 0 ? HAMR_F
             T l[NPR];
 #pragma unroll
             for (int k = 0; k < NPR; k++) l[k] = pl[k];
-            const double v = flux_eval<DIR, T, REC>(d, gm, ps, l, lo, F, c, j);
-            dtf = v < dtf ? v : dtf;
+            cmx = d_max(cmx, flux_eval<DIR, T, REC>(d, gm, ps, l, lo, F, c, j));
 #pragma unroll
             for (int k = 0; k < NPR; k++) pl[k] = hi[k];
         }
     }
-    if (calc_dt) cta_min_dt(dtf, &dtbits[DIR]);
+    if (calc_dt) cta_max_ctop(d, DIR, cmx, &dtbits[DIR]);
 }
 
 // reflective polar axis and no-inflow radial edges (fix_flux, GPU_const_trans.h:3-61)
@@ -1816,8 +1870,8 @@ __device__ __forceinline__ void k_bound_x2_at(const Dims &d, double *pv, double 
     } else {
         if (face && k == 1) return;
         for (int g = 0; g < ng; g++) {
-            a[C(g, z)] = a[C(ng, z)];
-            a[C(n2 + ng + g, z)] = a[C(n2 + ng - 1, z)];
+            if (!(d.halo & 4)) a[C(g, z)] = a[C(ng, z)];
+            if (!(d.halo & 8)) a[C(n2 + ng + g, z)] = a[C(n2 + ng - 1, z)];
         }
     }
 }
@@ -1828,26 +1882,45 @@ __global__ void k_bound_x2(const Dims d, double *pv, double *ps) {
     k_bound_x2_at(d, pv, ps, t);
 }
 
-// ------------------------------------------------------------ x1 halos
-// A block of a domain decomposed along x1 exchanges ng layers with each
-// neighbour: the layers next to a shared side (its last ng active layers on
-// the upper side, its first ng on the lower) become the neighbour's ghost
-// layers on the facing side, over the whole ghost-inclusive (x2, x3) cross
-// section, for the NPR primitives and the 3 face-field planes. Buffer layout
-// [component][layer][j][z] (the boundprim slabs of boundcomP.c, one
-// contiguous message per side).
+// ------------------------------------------------------------ halos
+// A block of a domain decomposed along x1 (or x2) exchanges ng layers with
+// each neighbour: the layers next to a shared side (its last ng active layers
+// on the upper side, its first ng on the lower) become the neighbour's ghost
+// layers on the facing side, over the whole ghost-inclusive cross section
+// ((x2, x3) for an x1 side, (x1, x3) for an x2 side), for the NPR primitives
+// and the 3 face-field planes. Buffer layout [component][layer][j][z] for x1
+// sides (side 0, 1), [component][layer][i][z] for x2 sides (side 2, 3) (the
+// boundprim slabs of boundcomP.c, one contiguous message per side).
 constexpr int HALO_COMPS = NPR + 3;
-__host__ __device__ __forceinline__ long n_halo(const Dims &d) { return (long)HALO_COMPS * d.ng1 * d.G2 * d.G3; }
+__host__ __device__ __forceinline__ long n_halo_side(const Dims &d, int side) {
+    return side < 2 ? (long)HALO_COMPS * d.ng1 * d.G2 * d.G3 : (long)HALO_COMPS * d.ng2 * d.G1 * d.G3;
+}
+__host__ __device__ __forceinline__ long n_halo(const Dims &d) {
+    const long a = n_halo_side(d, 0), b = n_halo_side(d, 2);
+    return a > b ? a : b;
+}
 
 template <bool PACK>
 __global__ void k_halo(const Dims d, double *pv, double *ps, int side, double *buf) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n_halo(d)) return;
-    const int z = (int)(t % d.G3), j = (int)((t / d.G3) % d.G2);
-    const long r = t / ((long)d.G3 * d.G2);
-    const int g = (int)(r % d.ng1), comp = (int)(r / d.ng1);
-    // packed: active layers next to the side; unpacked: the ghosts beyond it
-    const int i = PACK ? (side ? d.n1 + g : d.ng1 + g) : (side ? d.ng1 + d.n1 + g : g);
+    if (t >= n_halo_side(d, side)) return;
+    const bool upper = side & 1;
+    const int z = (int)(t % d.G3);
+    int i, j, comp;
+    if (side < 2) {
+        j = (int)((t / d.G3) % d.G2);
+        const long r = t / ((long)d.G3 * d.G2);
+        const int g = (int)(r % d.ng1);
+        comp = (int)(r / d.ng1);
+        // packed: active layers next to the side; unpacked: the ghosts beyond it
+        i = PACK ? (upper ? d.n1 + g : d.ng1 + g) : (upper ? d.ng1 + d.n1 + g : g);
+    } else {
+        i = (int)((t / d.G3) % d.G1);
+        const long r = t / ((long)d.G3 * d.G1);
+        const int g = (int)(r % d.ng2);
+        comp = (int)(r / d.ng2);
+        j = PACK ? (upper ? d.n2 + g : d.ng2 + g) : (upper ? d.ng2 + d.n2 + g : g);
+    }
     double *a = comp < NPR ? pv + (long)comp * d.ks : ps + (long)(comp - NPR) * d.ks;
     const long c = cix(d, i, j, z);
     if (PACK) buf[t] = a[c];
@@ -1905,6 +1978,28 @@ inline unsigned nblk(long n) { return (unsigned)((n + BLK - 1) / BLK); }
 }  // namespace
 
 // ===========================================================================
+// The CFL bookkeeping constants of a block (Dims::cfl_c0, ctop_lim): c0 =
+// cour dx per direction, as the device computes it, and the largest double
+// x with c0 / x > 1e-6, found from c0 / 1e-6 by stepping one ulp at a time
+// (IEEE division on the host, as on the device).
+static void set_cfl_limits(Dims &d) {
+    const double dx[4] = {0., d.dx1, d.dx2, d.dx3};
+    d.cfl_c0[0] = 0.;
+    d.ctop_lim[0] = -1.;
+    for (int k = 1; k < 4; k++) {
+        const double c0 = d.cour * dx[k];
+        d.cfl_c0[k] = c0;
+        double x = c0 / 1.e-6;
+        if (!(c0 > 0.) || !std::isfinite(x) || !(x > 0.)) {
+            d.ctop_lim[k] = -1.;   // no face counts
+            continue;
+        }
+        for (int it = 0; it < 64 && !(c0 / x > 1.e-6); it++) x = std::nextafter(x, 0.);
+        for (int it = 0; it < 64 && c0 / std::nextafter(x, INFINITY) > 1.e-6; it++) x = std::nextafter(x, INFINITY);
+        d.ctop_lim[k] = x;
+    }
+}
+
 struct hamr_ctx {
     hamr_params prm;
     Dims d;
@@ -1924,6 +2019,9 @@ struct hamr_ctx {
     // side streams, 14.35 without (FP64 31.40, 31.32): off by default,
     // HAMR_CONCURRENT=1 turns it on
     bool concurrent = false;
+    // 3-D blocks: the centre EMFs computed by the x3 flux kernel instead of
+    // k_emf_centre (HAMR_EMF_IN_X3=0 keeps the separate kernel)
+    bool emf_in_x3 = true;
     cudaStream_t side[2] = {nullptr, nullptr};
     cudaEvent_t ev[5] = {};
     std::string err;
@@ -2011,19 +2109,19 @@ inline int rec_key(const Dims &d) {
 
 template <int DIR, typename T>
 void launch_flux(long n, cudaStream_t s, const Dims &d, const Geom &m, const double *pin, const double *psin, T *F,
-                 unsigned long long *dtbits, int cd, long rows_min) {
+                 unsigned long long *dtbits, int cd, long rows_min, T *Ec = nullptr) {
     // x1 and x2 faces by rows, each zone reconstructed once, where the rows
     // still fill the device several times over; small blocks (2-D, ensemble
     // members) keep one thread per face
     if (DIR == 3) {   // each zone reconstructed once, edges through shared memory
         const long nb = (n_x3_slots(d) - 1 + BLK - 2) / (BLK - 1);
         switch (rec_key(d)) {
-        case 1: k_flux_x3<T, 1><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
-        case 2: k_flux_x3<T, 2><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
-        case 3: k_flux_x3<T, 3><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
-        case 6: k_flux_x3<T, 6><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
-        case 7: k_flux_x3<T, 7><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
-        default: k_flux_x3<T, 0><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd); break;
+        case 1: k_flux_x3<T, 1><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd, Ec); break;
+        case 2: k_flux_x3<T, 2><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd, Ec); break;
+        case 3: k_flux_x3<T, 3><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd, Ec); break;
+        case 6: k_flux_x3<T, 6><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd, Ec); break;
+        case 7: k_flux_x3<T, 7><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd, Ec); break;
+        default: k_flux_x3<T, 0><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd, Ec); break;
         }
         return;
     }
@@ -2076,6 +2174,8 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
     // stage stream, x2 and x1 + centre EMFs on the side streams
     const bool conc = ctx->concurrent && !(pf && pf->on) && !(d.d3 && ctx->ct_fused);
     cudaStream_t s2 = conc ? ctx->side[0] : s, s3 = conc ? ctx->side[1] : s;
+    // 3-D: the centre EMFs come out of the x3 flux kernel
+    const bool ec_x3 = d.d3 && !ctx->ct_fused && ctx->emf_in_x3;
     if (conc) {
         CK(cudaEventRecord(ctx->ev[0], s));
         CK(cudaStreamWaitEvent(s2, ctx->ev[0], 0));
@@ -2083,7 +2183,7 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
     }
     if (d.d3) {
         long n = (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3 - 1);
-        launch_flux<3, T>(n, s, d, m, pin, psin, F3, ctx->dtbits, cd, ctx->rows_min);
+        launch_flux<3, T>(n, s, d, m, pin, psin, F3, ctx->dtbits, cd, ctx->rows_min, ec_x3 ? Ec : nullptr);
     }
     prof_mark(pf, PROF_FLUX3, s);
     {
@@ -2098,7 +2198,7 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
     prof_mark(pf, PROF_FLUX1, s);
     if (conc) {
         long n = (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3);
-        k_emf_centre<T><<<nblk(n), BLK, 0, s3>>>(d, m, pin, Ec);
+        if (!ec_x3) k_emf_centre<T><<<nblk(n), BLK, 0, s3>>>(d, m, pin, Ec);
         CK(cudaEventRecord(ctx->ev[1], s2));
         CK(cudaEventRecord(ctx->ev[2], s3));
         CK(cudaStreamWaitEvent(s, ctx->ev[1], 0));
@@ -2134,7 +2234,7 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
         }
         prof_mark(pf, PROF_FACE, s);
     } else {
-    if (!conc) {
+    if (!conc && !ec_x3) {
         long n = (long)(d.n1 + 2 * d.d1) * (d.n2 + 2 * d.d2) * (d.n3 + 2 * d.d3);
         k_emf_centre<T><<<nblk(n), BLK, 0, s>>>(d, m, pin, Ec);
     }
@@ -2241,7 +2341,11 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
         return HAMR_E_ARG;
     if (!(prm->ng == 3 || (prm->ng == 2 && prm->recon == HAMR_RECON_MC))) return HAMR_E_ARG;
     if (prm->precision != HAMR_FP64 && prm->precision != HAMR_MIXED) return HAMR_E_ARG;
-    if ((prm->halo & ~3) || (prm->halo && (prm->bc1 == HAMR_BC_PERIODIC || prm->n1 < prm->ng))) return HAMR_E_ARG;
+    if ((prm->halo & ~15) || ((prm->halo & 3) && (prm->bc1 == HAMR_BC_PERIODIC || prm->n1 < prm->ng))) return HAMR_E_ARG;
+    // an x2 side shared with a neighbour is no pole and no periodic wrap
+    if ((prm->halo & 12) && (prm->bc2 == HAMR_BC_PERIODIC || prm->n2 < prm->ng || ((prm->halo & 4) && prm->pole1) ||
+                             ((prm->halo & 8) && prm->pole2)))
+        return HAMR_E_ARG;
     if ((prm->floors & ~1) || prm->repair < 0 || prm->repair > 2) return HAMR_E_ARG;
     // the neighbour repair's order spans the whole domain: not on a slab of one
     if (prm->repair == 2 && prm->halo) return HAMR_E_ARG;
@@ -2263,6 +2367,7 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
     d.dx1 = prm->dx1; d.dx2 = prm->dx2; d.dx3 = prm->dx3;
     d.rdx1 = 1.0 / d.dx1; d.rdx2 = 1.0 / d.dx2; d.rdx3 = 1.0 / d.dx3;
     d.rgam = 1.0 / prm->gam;
+    set_cfl_limits(d);
     d.gam = prm->gam; d.cour = prm->cour;
     d.pole1 = prm->pole1; d.pole2 = prm->pole2;
     d.bc1 = prm->bc1; d.bc2 = prm->bc2; d.bc3 = prm->bc3;
@@ -2292,6 +2397,7 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
         if (const char *e = getenv("HAMR_CT_FUSED")) ctx->ct_fused = atoi(e) != 0;
         if (const char *e = getenv("HAMR_CONS_TMA")) ctx->cons_tma = atoi(e) != 0;
         if (const char *e = getenv("HAMR_CONCURRENT")) ctx->concurrent = atoi(e) != 0;
+        if (const char *e = getenv("HAMR_EMF_IN_X3")) ctx->emf_in_x3 = atoi(e) != 0;
     }
     if (ctx->concurrent) {
         for (auto &st : ctx->side)
@@ -2427,19 +2533,19 @@ long hamr_halo_count(const hamr_ctx *ctx) {
 }
 
 int hamr_halo_pack(hamr_ctx *ctx, int full, int side, double *buf) {
-    if (!ctx || !buf || (side != 0 && side != 1)) return HAMR_E_ARG;
+    if (!ctx || !buf || side < 0 || side > 3) return HAMR_E_ARG;
     const Dims &d = ctx->d;
-    k_halo<true><<<nblk(n_halo(d)), BLK, 0, ctx->stream>>>(d, full ? ctx->p : ctx->ph, full ? ctx->ps : ctx->psh,
-                                                           side, buf);
+    k_halo<true><<<nblk(n_halo_side(d, side)), BLK, 0, ctx->stream>>>(
+        d, full ? ctx->p : ctx->ph, full ? ctx->ps : ctx->psh, side, buf);
     CK(cudaGetLastError());
     return HAMR_OK;
 }
 
 int hamr_halo_unpack(hamr_ctx *ctx, int full, int side, const double *buf) {
-    if (!ctx || !buf || (side != 0 && side != 1)) return HAMR_E_ARG;
+    if (!ctx || !buf || side < 0 || side > 3) return HAMR_E_ARG;
     const Dims &d = ctx->d;
-    k_halo<false><<<nblk(n_halo(d)), BLK, 0, ctx->stream>>>(d, full ? ctx->p : ctx->ph, full ? ctx->ps : ctx->psh,
-                                                            side, const_cast<double *>(buf));
+    k_halo<false><<<nblk(n_halo_side(d, side)), BLK, 0, ctx->stream>>>(
+        d, full ? ctx->p : ctx->ph, full ? ctx->ps : ctx->psh, side, const_cast<double *>(buf));
     CK(cudaGetLastError());
     return HAMR_OK;
 }
@@ -2661,6 +2767,7 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
     d.dx1 = prm->dx1; d.dx2 = prm->dx2; d.dx3 = prm->dx3;
     d.rdx1 = 1.0 / d.dx1; d.rdx2 = 1.0 / d.dx2; d.rdx3 = 1.0 / d.dx3;
     d.rgam = 1.0 / prm->gam;
+    set_cfl_limits(d);
     d.gam = prm->gam; d.cour = prm->cour;
     d.pole1 = prm->pole1; d.pole2 = prm->pole2;
     d.bc1 = prm->bc1; d.bc2 = prm->bc2; d.bc3 = prm->bc3;

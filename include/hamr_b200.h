@@ -94,10 +94,12 @@ typedef struct hamr_params {
     int inversion;          /* enum hamr_inversion (zero-initialised: Noble 2D) */
     int recon;              /* enum hamr_recon (zero-initialised: PPM) */
     int riemann;            /* enum hamr_riemann (zero-initialised: HLL) */
-    int halo;               /* x1 sides shared with a neighbouring block of a domain
-                               decomposed along x1: bit 0 the lower side, bit 1 the
-                               upper (zero-initialised: none). No physical ghost fill
-                               and no radial mass-flux fix there; such a block steps
+    int halo;               /* sides shared with a neighbouring block of a decomposed
+                               domain: bit 0 the lower x1 side, bit 1 the upper, bit 2
+                               the lower x2 side, bit 3 the upper (zero-initialised:
+                               none). No physical ghost fill and no radial mass-flux
+                               fix there; an x2 halo side is no pole (pole1/pole2 0
+                               there) and bc2 is not periodic. Such a block steps
                                through hamr_stage, hamr_bound_dim and the hamr_halo_*
                                exchange (the reference's block exchange, boundcomP.c) */
     int floors;             /* 1: drift-frame floors on rho, u and the velocity after the
@@ -149,25 +151,29 @@ int hamr_download_flags(hamr_ctx *ctx, int *pflag, int *failimage);
 /* Ghost fill of the current state (GPU_boundprim, GPU_main.cu:2113). */
 int hamr_bound(hamr_ctx *ctx);
 
-/* ---- domains decomposed along x1 (halo != 0) ------------------------------
+/* ---- decomposed domains (halo != 0) ---------------------------------------
  * Such a block's hamr_stage leaves the ghost fill to the caller, which runs,
- * for the state the sub-step wrote (full: p, ps; else ph, psh):
+ * for the state the sub-step wrote (full: p, ps; else ph, psh), along x1:
  *   hamr_bound_dim(1)  physical x1 sides
  *   hamr_halo_pack on both neighbours' facing sides, transfer, hamr_halo_unpack
  *   hamr_bound_dim(3), hamr_bound_dim(2)
+ * and along x2:
+ *   hamr_bound_dim(1), hamr_bound_dim(3), hamr_bound_dim(2)  (poles, physical sides)
+ *   the x2 halo exchange (sides 2, 3)
  * the order in which a single block fills x1, x3, x2 ghosts, so that the
  * decomposed step reproduces the undivided block bit for bit. The step size is
  * the harmonic combination 1/(1/d1 + 1/d2 + 1/d3) of the per-direction CFL
  * minima over all blocks (hamr_cfl_dirs after each block's full sub-step).
  * hamr_step, hamr_advance and hamr_profile_step refuse halo blocks. */
 int hamr_bound_dim(hamr_ctx *ctx, int full, int dim);
-/* Doubles in one side's halo message: (NPR + 3) x ng x G2 x G3, laid out
- * [component][layer][j][z]. */
+/* Doubles a halo message buffer needs: the larger of an x1 side's
+ * (NPR + 3) x ng x G2 x G3, laid out [component][layer][j][z], and an x2
+ * side's (NPR + 3) x ng x G1 x G3, laid out [component][layer][i][z]. */
 long hamr_halo_count(const hamr_ctx *ctx);
-/* side 0: the lower x1 side, 1: the upper. pack copies the ng active layers
- * next to that side into buf (device memory, hamr_halo_count doubles);
- * unpack writes buf into the ghost layers beyond that side. Asynchronous on
- * the context stream. */
+/* side 0: the lower x1 side, 1: the upper, 2: the lower x2 side, 3: the
+ * upper. pack copies the ng active layers next to that side into buf (device
+ * memory, hamr_halo_count doubles); unpack writes buf into the ghost layers
+ * beyond that side. Asynchronous on the context stream. */
 int hamr_halo_pack(hamr_ctx *ctx, int full, int side, double *buf);
 int hamr_halo_unpack(hamr_ctx *ctx, int full, int side, const double *buf);
 /* Per-direction CFL minima (x1, x2, x3; 1e9 for an inactive direction) of

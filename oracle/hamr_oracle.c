@@ -2001,15 +2001,20 @@ void ho_bound_dim(const ho_grid *g, const ho_geom *m, double *pv, double *ps, in
                         }
                     }
                 }
-                /* HO_BC_OUTFLOW in x2: plain copy of the edge row */
+                /* HO_BC_OUTFLOW in x2: plain copy of the edge row (not on an x2
+                 * side shared with a neighbour block: halo bits 2, 3) */
                 else {
                     for (int t = 0; t < ng; t++) {
-                        copy_cell(&d, pv, cix(&d, i, t, z), cix(&d, i, ng, z));
-                        copy_cell(&d, pv, cix(&d, i, n2 + ng + t, z), cix(&d, i, n2 + ng - 1, z));
-                        ps[0 * ks + cix(&d, i, t, z)] = ps[0 * ks + cix(&d, i, ng, z)];
-                        ps[2 * ks + cix(&d, i, t, z)] = ps[2 * ks + cix(&d, i, ng, z)];
-                        ps[0 * ks + cix(&d, i, n2 + ng + t, z)] = ps[0 * ks + cix(&d, i, n2 + ng - 1, z)];
-                        ps[2 * ks + cix(&d, i, n2 + ng + t, z)] = ps[2 * ks + cix(&d, i, n2 + ng - 1, z)];
+                        if (!(g->halo & 4)) {
+                            copy_cell(&d, pv, cix(&d, i, t, z), cix(&d, i, ng, z));
+                            ps[0 * ks + cix(&d, i, t, z)] = ps[0 * ks + cix(&d, i, ng, z)];
+                            ps[2 * ks + cix(&d, i, t, z)] = ps[2 * ks + cix(&d, i, ng, z)];
+                        }
+                        if (!(g->halo & 8)) {
+                            copy_cell(&d, pv, cix(&d, i, n2 + ng + t, z), cix(&d, i, n2 + ng - 1, z));
+                            ps[0 * ks + cix(&d, i, n2 + ng + t, z)] = ps[0 * ks + cix(&d, i, n2 + ng - 1, z)];
+                            ps[2 * ks + cix(&d, i, n2 + ng + t, z)] = ps[2 * ks + cix(&d, i, n2 + ng - 1, z)];
+                        }
                     }
                 }
             }

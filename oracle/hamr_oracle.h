@@ -41,9 +41,11 @@ typedef struct {
                             its HLLC and HLL fallbacks (HLLD builds) */
     int halo;            /* sides interior to a decomposed domain, whose ghosts
                             come from a neighbouring block: bit 0 the lower x1
-                            side, bit 1 the upper; no physical fill and no
-                            radial mass-flux fix there (the reference fills
-                            them by its block exchange, boundcomP.c) */
+                            side, bit 1 the upper, bits 2, 3 the lower and upper
+                            x2 sides (no pole there: pole1/pole2 0); no physical
+                            fill and no radial mass-flux fix there (the
+                            reference fills them by its block exchange,
+                            boundcomP.c) */
     int floors;          /* 1: drift-frame floors after the inversion (fixup_cell,
                             GPU_fixup.h:1025-1800, compiled out in the reference) */
     int repair;          /* zones whose inversion failed (pflag != 0):
@@ -74,8 +76,9 @@ void ho_stage(const ho_grid *g, const ho_geom *m, ho_state *s, int full,
 /* Ghost fill of (pv, ps) for the boundary types in g (direction 1, then 3, then 2). */
 void ho_bound(const ho_grid *g, const ho_geom *m, double *pv, double *ps);
 /* Ghost fill of one direction (1, 2 or 3) on the physical sides; ho_bound is
- * x1, x3, x2 in that order. A decomposed domain exchanges the x1 halos
- * between the x1 and x3 fills. */
+ * x1, x3, x2 in that order. A domain decomposed along x1 exchanges the x1
+ * halos between the x1 and x3 fills; one decomposed along x2 exchanges the x2
+ * halos after the x2 fill. */
 void ho_bound_dim(const ho_grid *g, const ho_geom *m, double *pv, double *ps, int dim);
 
 /* Single-cell pieces (pinned one by one against the reference). */

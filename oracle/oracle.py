@@ -275,7 +275,7 @@ class Setup:
     inversion: int = 0  # 0: Noble 2D, 1: Newman-Hamlin
     recon: int = 0      # 0: PPM, 1: MC-limited linear
     riemann: int = 0    # 0: HLL, 1: HLLC, 2: HLLD
-    halo: int = 0       # x1 sides filled by a neighbour block: bit 0 lower, bit 1 upper
+    halo: int = 0       # sides filled by a neighbour block: bits 0, 1 lower/upper x1; 2, 3 lower/upper x2
     floors: int = 0     # 1: drift-frame floors after the inversion
     repair: int = 0     # failed zones: 1 reset to the floor state, 2 neighbour interpolation
 

@@ -1,6 +1,6 @@
 """The oracle as a slab of a decomposed domain (host arrays; halo messages
-packed by numpy in the device layout [component][layer][j][z]), for the
-decomposition tests: the steppers of hamr_gamma_wind_b200.decomp drive it
+packed by numpy in the device layouts, [component][layer][j][z] for x1 sides
+and [component][layer][i][z] for x2 sides), for the decomposition tests: the steppers of hamr_gamma_wind_b200.decomp drive it
 exactly as they drive the GPU blocks."""
 import numpy as np
 import torch
@@ -24,7 +24,7 @@ class OracleSlab:
         self.s = oracle_setup(sp, halo=getattr(sp, "halo", 0), **kw)
         self.dt3 = None
         b = self.s.blk
-        self.count = 12 * sp.ng * b.g2 * b.g3
+        self.count = max(12 * sp.ng * b.g2 * b.g3, 12 * sp.ng * b.g1 * b.g3)
 
     @staticmethod
     def _names(full):
@@ -38,24 +38,40 @@ class OracleSlab:
     def bound_dim(self, full, dim):
         O.oracle_bound_dim(self.s, dim, *self._names(full))
 
+    def _layers(self, side, ghost):
+        """index of the ng layers next to `side` (0, 1: x1; 2, 3: x2):
+        the active ones, or the ghosts beyond it"""
+        ng = self.sp.ng
+        n = self.sp.n1 if side < 2 else self.sp.n2
+        if ghost:
+            i0 = ng + n if side & 1 else 0
+        else:
+            i0 = n if side & 1 else ng
+        sl = slice(i0, i0 + ng)
+        return (slice(None), sl) if side < 2 else (slice(None), slice(None), sl)
+
     def pack(self, full, side):
-        ng, n1 = self.sp.ng, self.sp.n1
-        i0 = n1 if side else ng
         pn, sn = self._names(full)
-        a = np.concatenate([self.s.blk.view(pn, 9)[:, i0:i0 + ng], self.s.blk.view(sn, 3)[:, i0:i0 + ng]])
+        ix = self._layers(side, ghost=False)
+        a = np.concatenate([self.s.blk.view(pn, 9)[ix], self.s.blk.view(sn, 3)[ix]])
+        if side >= 2:   # [component][layer][i][z], as the device packs it
+            a = a.transpose(0, 2, 1, 3)
         return torch.from_numpy(np.ascontiguousarray(a).reshape(-1).copy())
 
     def recv_buffer(self, side):
         return torch.empty(self.count, dtype=torch.float64)
 
     def unpack(self, full, side, buf):
-        ng, n1 = self.sp.ng, self.sp.n1
-        i0 = ng + n1 if side else 0
+        ng = self.sp.ng
         b = self.s.blk
-        a = buf.numpy().reshape(12, ng, b.g2, b.g3)
         pn, sn = self._names(full)
-        b.view(pn, 9)[:, i0:i0 + ng] = a[:9]
-        b.view(sn, 3)[:, i0:i0 + ng] = a[9:]
+        ix = self._layers(side, ghost=True)
+        if side < 2:
+            a = buf.numpy()[:12 * ng * b.g2 * b.g3].reshape(12, ng, b.g2, b.g3)
+        else:
+            a = buf.numpy()[:12 * ng * b.g1 * b.g3].reshape(12, ng, b.g1, b.g3).transpose(0, 2, 1, 3)
+        b.view(pn, 9)[ix] = a[:9]
+        b.view(sn, 3)[ix] = a[9:]
 
     def cfl_dirs(self):
         return self.dt3

@@ -1,9 +1,11 @@
-"""Domains decomposed along x1 (hamr_gamma_wind_b200.decomp), on the host:
-the oracle as the slabs, driven by the same steppers the GPU blocks use.
+"""Domains decomposed along x1 or x2 (hamr_gamma_wind_b200.decomp), on the
+host: the oracle as the slabs, driven by the same steppers the GPU blocks use.
 
-Split into slabs with halo sides and stepped with the halo exchange between
-the x1 and x3 ghost fills, the domain must reproduce the undivided block bit
-for bit, step size included; over two gloo ranks (one slab each, halos by
+Split into slabs with halo sides and stepped with the halo exchange in the
+undivided block's fill order (along x1 between the x1 and x3 ghost fills,
+along x2 after the x2 fill, the poles staying with the first and last slab),
+the domain must reproduce the undivided block bit for bit, step size
+included; over two and three gloo ranks (one slab each, halos by
 point-to-point messages, CFL minima by an all-reduce) as well.
 """
 import os
@@ -22,8 +24,12 @@ from tests._decomp import OracleSlab, oracle_setup
 from tests._gpu import oracle_step
 
 CASES = {
-    "torus3d": (lambda: problems.fm_torus(32, 16, 8, rout=40.0), [12, 20]),
-    "torus2d": (lambda: problems.fm_torus(48, 48, 1, rout=40.0), [10, 16, 22]),
+    "torus3d": (lambda: problems.fm_torus(32, 16, 8, rout=40.0), [12, 20], 1),
+    "torus2d": (lambda: problems.fm_torus(48, 48, 1, rout=40.0), [10, 16, 22], 1),
+    # along x2: transmissive poles (3-D) and reflective poles (2-D, with the
+    # near-axis row fix) in the first and last slabs
+    "torus3d_x2": (lambda: problems.fm_torus(24, 24, 8, rout=40.0), [7, 9, 8], 2),
+    "torus2d_x2": (lambda: problems.fm_torus(40, 48, 1, rout=40.0), [20, 28], 2),
 }
 
 
@@ -53,14 +59,23 @@ def test_split_join_round_trip():
         decomp.split(pb, [2, 30])
     with pytest.raises(ValueError):
         decomp.split(pb, [10, 10])
+    # along x2: halo bits 4 and 8, the poles with the end slabs
+    x2 = decomp.split(pb, [5, 6, 5], axis=2)
+    assert [s.halo for s in x2] == [8, 12, 4]
+    assert [s.poles for s in x2] == [(pb.poles[0], 0), (0, 0), (0, pb.poles[1])]
+    p, ps = decomp.join(pb, x2, [(s.p, s.ps) for s in x2])
+    np.testing.assert_array_equal(p, pb.p)
+    np.testing.assert_array_equal(ps, pb.ps)
+    with pytest.raises(ValueError):
+        decomp.split(pb, [4, 12], axis=2)   # narrower than ng + 2
 
 
 @pytest.mark.parametrize("case", list(CASES))
 def test_oracle_slabs_match_undivided_block(case):
-    make, widths = CASES[case]
+    make, widths, axis = CASES[case]
     pb, s_full = bound_problem(make())
-    slabs = decomp.split(pb, widths)
-    stepper = decomp.SlabStepper([OracleSlab(sp) for sp in slabs], decomp.LocalExchange())
+    slabs = decomp.split(pb, widths, axis=axis)
+    stepper = decomp.SlabStepper([OracleSlab(sp) for sp in slabs], decomp.LocalExchange(), axis=axis)
     dt = 0.2 * min(pb.dx[:2])
     for _ in range(3):
         dn_full = oracle_step(s_full, dt)
@@ -72,19 +87,19 @@ def test_oracle_slabs_match_undivided_block(case):
     np.testing.assert_array_equal(pb.active(ps), s_full.blk.active("ps"))
 
 
-WIDTHS = {2: [14, 18], 3: [10, 9, 13]}
+WIDTHS = {(2, 1): [14, 18], (3, 1): [10, 9, 13], (2, 2): [7, 9]}
 
 
-def _rank(rank, world, path, port):
+def _rank(rank, world, path, port, axis=1):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world,
                             timeout=__import__("datetime").timedelta(seconds=60))
     try:
         pb, _ = bound_problem(problems.fm_torus(32, 16, 8, rout=40.0))
-        slabs = decomp.split(pb, WIDTHS[world])
+        slabs = decomp.split(pb, WIDTHS[world, axis], axis=axis)
         me = OracleSlab(slabs[rank])
-        stepper = decomp.SlabStepper([me], decomp.DistributedExchange(rank, world))
+        stepper = decomp.SlabStepper([me], decomp.DistributedExchange(rank, world), axis=axis)
         dt = 0.2 * min(pb.dx[:2])
         dts = []
         for _ in range(2):
@@ -97,16 +112,17 @@ def _rank(rank, world, path, port):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_gloo_ranks_match_undivided_block(world):
+@pytest.mark.parametrize("world,axis", [(2, 1), (3, 1), (2, 2)])
+def test_gloo_ranks_match_undivided_block(world, axis):
     """One slab per rank (the middle rank of three exchanges with both
-    neighbours), halos and the CFL minimum over gloo: bit for bit the
-    undivided block, step sizes included."""
+    neighbours; along x2 each rank holds one pole), halos and the CFL
+    minimum over gloo: bit for bit the undivided block, step sizes
+    included."""
     with tempfile.TemporaryDirectory() as path:
-        port = 29500 + (os.getpid() + 97 * world) % 2000
-        mp.spawn(_rank, args=(world, path, port), nprocs=world, join=True)
+        port = 29500 + (os.getpid() + 97 * world + 31 * axis) % 2000
+        mp.spawn(_rank, args=(world, path, port, axis), nprocs=world, join=True)
         pb, s_full = bound_problem(problems.fm_torus(32, 16, 8, rout=40.0))
-        slabs = decomp.split(pb, WIDTHS[world])
+        slabs = decomp.split(pb, WIDTHS[world, axis], axis=axis)
         dt = 0.2 * min(pb.dx[:2])
         dts = []
         for _ in range(2):

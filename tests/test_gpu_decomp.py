@@ -1,7 +1,8 @@
-"""Domains decomposed along x1 on one GPU (hamr_gamma_wind_b200.decomp): slabs
-as Blocks with halo sides, halos packed and unpacked by the library's
-kernels (hamr_halo_pack / hamr_halo_unpack) between the x1 and x3 ghost
-fills, against the undivided Block. Every slab runs the same kernels on the
+"""Domains decomposed along x1 or x2 on one GPU (hamr_gamma_wind_b200.decomp):
+slabs as Blocks with halo sides, halos packed and unpacked by the library's
+kernels (hamr_halo_pack / hamr_halo_unpack) in the undivided block's fill
+order (x1 halos between the x1 and x3 ghost fills, x2 halos after the x2
+fill, the poles with the end slabs), against the undivided Block. Every slab runs the same kernels on the
 same data as the undivided block (the step-size reduction is a minimum), so
 in either build the domain must match it bit for bit, step sizes included."""
 import ctypes
@@ -17,8 +18,10 @@ from hamr_gamma_wind_b200.api import Block
 pytestmark = pytest.mark.gpu
 
 CASES = {
-    "torus3d": (lambda: problems.fm_torus(32, 16, 8, rout=40.0), [12, 20]),
-    "torus2d": (lambda: problems.fm_torus(48, 48, 1, rout=40.0), [10, 16, 22]),
+    "torus3d": (lambda: problems.fm_torus(32, 16, 8, rout=40.0), [12, 20], 1),
+    "torus2d": (lambda: problems.fm_torus(48, 48, 1, rout=40.0), [10, 16, 22], 1),
+    "torus3d_x2": (lambda: problems.fm_torus(24, 24, 8, rout=40.0), [7, 9, 8], 2),
+    "torus2d_x2": (lambda: problems.fm_torus(40, 48, 1, rout=40.0), [20, 28], 2),
 }
 
 
@@ -39,13 +42,13 @@ def _undivided(pb, strict, stream, **kw):
 @pytest.mark.parametrize("strict,kw", [(True, {}), (False, {}), (True, dict(precision="mixed")),
                                        (True, dict(riemann="hllc"))])
 def test_slabs_match_undivided_block(case, strict, kw):
-    make, widths = CASES[case]
+    make, widths, axis = CASES[case]
     stream = torch.cuda.Stream()
     h = _stream_handle(stream)
     blk, pb = _undivided(make(), strict, h, **kw)
-    slabs = decomp.split(pb, widths)
+    slabs = decomp.split(pb, widths, axis=axis)
     gs = decomp.gpu_slabs(slabs, h, strict=strict, **kw)
-    stepper = decomp.SlabStepper(gs, decomp.LocalExchange())
+    stepper = decomp.SlabStepper(gs, decomp.LocalExchange(), axis=axis)
     dt = 0.2 * min(pb.dx[:2])
     for _ in range(3):
         dn_full = blk.step(dt)
@@ -69,5 +72,15 @@ def test_halo_block_refuses_whole_steps():
     b.upload(sl.p, sl.ps)
     with pytest.raises(_lib.HamrError):
         b.step(0.01)
-    assert b.halo_count() == 12 * pb.ng * (pb.n2 + 2 * pb.ng) * (pb.n3 + 2 * pb.ng)
+    # the larger of an x1 side's (G2 x G3) and an x2 side's (G1 x G3) message
+    G1, G2, G3 = sl.n1 + 2 * pb.ng, pb.n2 + 2 * pb.ng, pb.n3 + 2 * pb.ng
+    assert b.halo_count() == 12 * pb.ng * max(G1, G2) * G3
     b.close()
+
+
+def test_x2_halo_side_refuses_a_pole():
+    """An x2 side shared with a neighbour cannot be a pole."""
+    pb = problems.fm_torus(24, 24, 8, rout=40.0)
+    sl = decomp.split(pb, [12, 12], axis=2)[0]
+    with pytest.raises(_lib.HamrError):
+        Block(**dict(sl.block_kwargs(), poles=(1, 1)), halo=sl.halo)

@@ -531,3 +531,29 @@ def test_concurrent_substep_matches_serial(precision, case, monkeypatch):
     assert np.array_equal(out["1"][0], out["0"][0])
     assert np.array_equal(out["1"][1], out["0"][1])
     assert out["1"][2] == out["0"][2]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("shape", [(24, 16, 32), (20, 12, 130), (16, 10, 38)])
+def test_centre_emfs_in_x3_kernel_match_separate_kernel(precision, shape, monkeypatch):
+    """The centre EMFs computed by the x3 flux kernel (its slots are the
+    centre-EMF zones; a slot shared by two CTAs, and the last slot, done
+    once) against k_emf_centre: bit for bit over three steps, rows longer and
+    shorter than a CTA's 127 slots."""
+    from hamr_gamma_wind_b200.api import Block
+    pb = problems.fm_torus(*shape, rout=40.0, rho_atm=1e-8, u_atm=1e-10)
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("HAMR_EMF_IN_X3", flag)
+        blk = Block(**pb.block_kwargs(), precision=precision, strict=True)
+        blk.set_geometry(pb.geo)
+        blk.upload(pb.p, pb.ps)
+        blk.bound()
+        dt = 0.2 * min(pb.dx)
+        for _ in range(3):
+            dt = min(blk.step(dt), 1.3 * dt)
+        out[flag] = blk.download()
+        blk.close()
+    assert np.isfinite(pb.active(out["0"][0])).all()
+    assert np.array_equal(out["1"][0], out["0"][0])
+    assert np.array_equal(out["1"][1], out["0"][1])
