@@ -996,11 +996,21 @@ __global__ void k_adj_bound_x1_outflow(const Dims d, const Geom m, const double 
 }
 
 // J contribution of one step: w * Mdot, Mdot = - sum_j F1[RHO](ih, j) dx2 dx3
+// one CTA of BLK threads: the column's terms summed in a fixed order (strided
+// partial sums, then a tree in shared memory), so that the objective does not
+// depend on the order in which atomics land
 __global__ void k_mdot_accum(const Dims d, const double *__restrict__ F1, int ih, double w, double *J) {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ double part[BLK];
     double v = 0.;
-    if (t < d.n2) v = -w * F1[RHO * d.ks + cix(d, ih, d.ng2 + (int)t, 0)] * d.dx2 * d.dx3;
-    block_add(v, J);
+    for (int t = threadIdx.x; t < d.n2; t += BLK)
+        v += -w * F1[RHO * d.ks + cix(d, ih, d.ng2 + t, 0)] * d.dx2 * d.dx3;
+    part[threadIdx.x] = v;
+    __syncthreads();
+    for (int s = BLK / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) part[threadIdx.x] += part[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *J += part[0];
 }
 
 }  // namespace
@@ -1241,7 +1251,7 @@ int fwd_step(hamr_adjoint *a, double dt) {
     return graph_run(a, a->fwd_graph, {dt, nullptr, nullptr}, a->ctx->stream, [&]() -> int {
         const int rc = fixed_step(a->ctx, dt);
         if (rc) return rc;
-        k_mdot_accum<<<nb(a->ctx->d.n2), BLK, 0, a->ctx->stream>>>(a->ctx->d, a->ctx->F1, a->ih, dt, a->J);
+        k_mdot_accum<<<1, BLK, 0, a->ctx->stream>>>(a->ctx->d, a->ctx->F1, a->ih, dt, a->J);
         return cudaGetLastError() == cudaSuccess ? HAMR_OK : HAMR_E_CUDA;
     });
 }

@@ -60,8 +60,9 @@ struct Geom {
     // per (i, j) column, when tabulated (else null), planes of gs: at the zone
     // centre 1/gdet, the lapse 1/sqrt(-g^tt) and n_t = -sqrt(-1/g^tt), each
     // with the inversion's own operations; then 1/gdet at the FACE1, FACE2
-    // and FACE3 locations (the face update's divisions by the face volume)
-    // (k_inv_tab)
+    // and FACE3 locations (the face update's divisions by the face volume);
+    // then the lapse at each of the 5 locations (planes 6-10) and its
+    // reciprocal (11-15), with geo_lapse's operations (k_inv_tab)
     const double *itab = nullptr;
 };
 
@@ -76,6 +77,12 @@ __device__ __forceinline__ void load_geo(const Dims &d, const Geom &m, int i, in
         o.gcov[s] = __ldg(&m.gcov[(long)(s * 5 + loc) * d.gs + idx]);
     }
     o.g = __ldg(&m.gdet[(long)loc * d.gs + idx]);
+    if (m.itab) {
+        o.lapse = __ldg(&m.itab[(long)(6 + loc) * d.gs + idx]);
+        o.rlapse = __ldg(&m.itab[(long)(11 + loc) * d.gs + idx]);
+    } else {
+        geo_lapse(o);
+    }
 }
 
 // temp / (face volume at plane `plane` of the column table), exactly
@@ -94,6 +101,12 @@ __device__ __forceinline__ void load_geo_t(const Dims &d, const Geom &m, int i, 
         o.gcov[s] = (T)__ldg(&m.gcov[(long)(s * 5 + loc) * d.gs + idx]);
     }
     o.g = (T)__ldg(&m.gdet[(long)loc * d.gs + idx]);
+    if (std::is_same<T, double>::value && m.itab) {
+        o.lapse = (T)__ldg(&m.itab[(long)(6 + loc) * d.gs + idx]);
+        o.rlapse = (T)__ldg(&m.itab[(long)(11 + loc) * d.gs + idx]);
+    } else {
+        geo_lapse(o);   // float: the lapse of the float metric, as before
+    }
 }
 
 // Sub-step sizes either come by value (hamr_stage) or from device memory
@@ -1204,6 +1217,11 @@ __global__ void k_inv_tab(const Dims d, const double *__restrict__ gcon, const d
     itab[3 * d.gs + idx] = 1.0 / gdet[(long)FACE1 * d.gs + idx];
     itab[4 * d.gs + idx] = 1.0 / gdet[(long)FACE2 * d.gs + idx];
     itab[5 * d.gs + idx] = 1.0 / gdet[(long)FACE3 * d.gs + idx];
+    for (int loc = 0; loc < 5; loc++) {
+        const double a = 1. / sqrt(-gcon[(long)loc * d.gs + idx]);   // g^tt at loc (component 0)
+        itab[(long)(6 + loc) * d.gs + idx] = a;
+        itab[(long)(11 + loc) * d.gs + idx] = 1. / a;
+    }
 }
 
 
@@ -1324,6 +1342,7 @@ __global__ void __launch_bounds__(BLK, HAMR_CONS_MINB) k_cons_cols(const Dims d,
 #pragma unroll
     for (int q = 0; q < 10; q++) { gm.gcov[q] = g[q]; gm.gcon[q] = g[10 + q]; }
     gm.g = g[20];
+    geo_lapse(gm);
     double pf[NPR], U[NPR];
     cons_update<T>(d, m, pin, pb, Ucache, F1, F2, F3, full, st.sub(), i, j, c, gi, gm, ConnStaged{g + 21}, pf, U);
     W[0 * d.ks + c] = U[RHO];
@@ -1505,6 +1524,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? HAMR_CONS_TMA_MINB : HAM
 #pragma unroll
     for (int q = 0; q < 10; q++) { gm.gcov[q] = sg[q]; gm.gcon[q] = sg[10 + q]; }
     gm.g = sg[20];
+    geo_lapse(gm);
     double pf[NPR], U[NPR];
     cons_update_fx<T>(d, m, pin, pb, Ucache, fx, full, st.sub(), i, j, c, gi, gm, ConnStaged{sg + 21}, pf, U);
     W[0 * d.ks + c] = U[RHO];
@@ -2031,7 +2051,7 @@ struct hamr_ctx {
     double *W = nullptr;  // updated conserved variables between k_cons and k_invert
     int *pflag = nullptr, *failimage = nullptr;
     double *gcov = nullptr, *gcon = nullptr, *gdet = nullptr, *conn = nullptr;
-    double *itab = nullptr;   // the column table of reciprocals (k_inv_tab), 6 planes of gs
+    double *itab = nullptr;   // the column table of reciprocals (k_inv_tab), 16 planes of gs
     unsigned long long *dtbits = nullptr;
     double *ndt = nullptr, *dt_state = nullptr;
     int *counter = nullptr;
@@ -2367,8 +2387,8 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
     d.dx1 = prm->dx1; d.dx2 = prm->dx2; d.dx3 = prm->dx3;
     d.rdx1 = 1.0 / d.dx1; d.rdx2 = 1.0 / d.dx2; d.rdx3 = 1.0 / d.dx3;
     d.rgam = 1.0 / prm->gam;
-    set_cfl_limits(d);
     d.gam = prm->gam; d.cour = prm->cour;
+    set_cfl_limits(d);   // after dx and cour
     d.pole1 = prm->pole1; d.pole2 = prm->pole2;
     d.bc1 = prm->bc1; d.bc2 = prm->bc2; d.bc3 = prm->bc3;
     d.ct_upwind = prm->ct_upwind;
@@ -2414,7 +2434,7 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
         {(void **)&ctx->failimage, 5 * sizeof(int) * d.ks},
         {(void **)&ctx->gcov, 50 * sizeof(double) * d.gs}, {(void **)&ctx->gcon, 50 * sizeof(double) * d.gs},
         {(void **)&ctx->gdet, 5 * sizeof(double) * d.gs}, {(void **)&ctx->conn, 40 * sizeof(double) * d.gs},
-        {(void **)&ctx->itab, 6 * sizeof(double) * d.gs},
+        {(void **)&ctx->itab, 16 * sizeof(double) * d.gs},
         {(void **)&ctx->dtbits, 4 * sizeof(unsigned long long)}, {(void **)&ctx->ndt, sizeof(double)},
         {(void **)&ctx->dt_state, sizeof(double)}, {(void **)&ctx->counter, sizeof(int)},
         {(void **)&ctx->divb, sizeof(unsigned long long)},
@@ -2767,8 +2787,8 @@ extern "C" int hamr_step_noalloc(const hamr_params *prm, const double *gcov, con
     d.dx1 = prm->dx1; d.dx2 = prm->dx2; d.dx3 = prm->dx3;
     d.rdx1 = 1.0 / d.dx1; d.rdx2 = 1.0 / d.dx2; d.rdx3 = 1.0 / d.dx3;
     d.rgam = 1.0 / prm->gam;
-    set_cfl_limits(d);
     d.gam = prm->gam; d.cour = prm->cour;
+    set_cfl_limits(d);   // after dx and cour
     d.pole1 = prm->pole1; d.pole2 = prm->pole2;
     d.bc1 = prm->bc1; d.bc2 = prm->bc2; d.bc3 = prm->bc3;
     d.ct_upwind = prm->ct_upwind;

@@ -38,7 +38,12 @@ constexpr double FAIL_VAL = 1.e30;
 template <typename T>
 struct Geo {
     T gcov[10], gcon[10], g;
+    T lapse, rlapse;   // 1/sqrt(-g^tt) and its reciprocal, each rounded once
 };
+
+// the lapse of a filled Geo, computed in place (ucon_calc's operations)
+template <typename T>
+__device__ __forceinline__ void geo_lapse(Geo<T> &o);
 
 template <typename T>
 struct State {
@@ -98,6 +103,12 @@ __device__ __forceinline__ double div_rcp_inf(double a, double b, double rb) {
     return (r == 0.0 || !(fabs(r) <= 1.7976931348623157e308)) ? q0 : fma(r, rb, q0);
 }
 
+template <typename T>
+__device__ __forceinline__ void geo_lapse(Geo<T> &o) {
+    o.lapse = T(1.) / d_sqrt(-o.gcon[0]);
+    o.rlapse = T(1.) / o.lapse;   // read by the double-precision quotients only
+}
+
 // Quotients a_k / b that share one divisor. In double precision: one IEEE
 // reciprocal of b, then the exact form per quotient (div_rcp_inf: the IEEE
 // quotient bit for bit for 2^-900 <= |a| <= 2^900, zeros and infinities),
@@ -110,6 +121,8 @@ struct Divisor {
     __device__ __forceinline__ explicit Divisor(T b_) : b(b_), rb(b_) {
         if constexpr (std::is_same<T, double>::value) rb = 1.0 / b_;
     }
+    // with the divisor's reciprocal already at hand (rounded once, 1/b)
+    __device__ __forceinline__ Divisor(T b_, T rb_) : b(b_), rb(rb_) {}
     __device__ __forceinline__ T div(T a) const {
         if constexpr (std::is_same<T, double>::value) return div_rcp_inf(a, b, rb);
         else return a / b;
@@ -150,14 +163,14 @@ __device__ __forceinline__ void gamma_calc(const T *pr, const Geo<G> &gm, T *gam
 
 template <typename T, typename G>
 __device__ __forceinline__ void ucon_calc(const T *pr, const Geo<G> &gm, T *ucon) {
-    G alpha = G(1.) / d_sqrt(-gm.gcon[0]);
+    const G alpha = gm.lapse;   // 1/sqrt(-g^tt), from the Geo (tabulated or geo_lapse)
     G beta[4];
     T gamma;
 #pragma unroll
     for (int j = 1; j < 4; j++) beta[j] = gm.gcon[j] * alpha * alpha;
     gamma_calc(pr, gm, &gamma);
     if constexpr (std::is_same<T, G>::value) {
-        const Divisor<T> da(alpha);   // four quotients by the lapse
+        const Divisor<T> da(alpha, gm.rlapse);   // four quotients by the lapse
         ucon[0] = da.div(gamma);
 #pragma unroll
         for (int j = 1; j < 4; j++) ucon[j] = pr[U1 + j - 1] - da.div(gamma * beta[j]);
