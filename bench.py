@@ -105,19 +105,21 @@ def kernel_bytes(slot: str, d: dict, width: float = 8.0) -> float:
 # 192 x 96 x 64 (profiles/k_*_torus_192x96x64.md; inputs larger than L2, caches
 # flushed before the launch). Every kernel's traffic grows with the number of
 # zones (plus a per-column metric term under 1 %), so a launch on another block
-# moves these figures times its zones. flux1 and flux2 share the row kernel.
+# moves these figures times its zones. flux1 and flux2 share the row kernel;
+# flux3 includes the centre EMFs (computed by the x3 kernel on 3-D blocks);
+# invert adds the fallback pass's 2.9 B.
 NCU_DRAM_BYTES_PER_ZONE = {
-    "fp64": {"flux1": 205.0, "flux2": 205.0, "flux3": 158.3, "update": 458.5, "invert": 191.5,
-             "emf_centre": 62.5, "emf_edge": 125.6, "face_update": 54.2},
-    "mixed": {"flux1": 125.2, "flux2": 125.2, "flux3": 105.1, "update": 317.2, "invert": 191.1,
-              "emf_centre": 58.1, "emf_edge": 57.3, "face_update": 40.2},
+    "fp64": {"flux1": 219.3, "flux2": 219.3, "flux3": 296.5, "update": 457.1, "invert": 223.6,
+             "emf_edge": 123.7, "face_update": 54.7},
+    "mixed": {"flux1": 134.2, "flux2": 134.2, "flux3": 136.7, "update": 315.4, "invert": 223.4,
+              "emf_edge": 58.6, "face_update": 40.6},
 }
 
 # what limits each kernel group, read from the same captures
 KERNEL_LIMITER = {
     "flux1": "latency: PPM stencil loads (long scoreboard) and dependent FP chains",
     "flux2": "latency: PPM stencil loads (long scoreboard) and dependent FP chains",
-    "flux3": "latency: dependent FP64/FP32 chains of the four flux evaluations per face",
+    "flux3": "latency: dependent FP64/FP32 chains of the four flux evaluations per face (and the centre EMFs)",
     "update": "FP64 fixed-latency chains after TMA-staged operand loads",
     "invert": "FP64 dependent Newton iterations (FP64 pipe 45 % active)",
     "emf_centre": "memory latency (long scoreboard)",
@@ -133,9 +135,16 @@ def kernel_rooflines(slots: dict, d: dict, prec: str, hbm: float) -> dict:
     width = 4.0 if prec == "mixed" else 8.0
     zones = d["n1"] * d["n2"] * d["n3"]
     tab = NCU_DRAM_BYTES_PER_ZONE.get("mixed" if prec == "mixed" else "fp64", {})
+    # 3-D blocks: the centre EMFs come out of the x3 flux kernel (their slot
+    # then times only its event pair)
+    fused_ec = d["n3"] > 1 and slots.get("emf_centre", 0.0) < 0.05
     out = {}
     for slot, ms in slots.items():
+        if fused_ec and slot == "emf_centre":
+            continue
         kb = kernel_bytes(slot, d, width)
+        if fused_ec and slot == "flux3":
+            kb += kernel_bytes("emf_centre", d, width)
         if kb <= 0 or ms <= 0:
             continue
         gbs = 2 * kb / (ms * 1e-3) / 1e9
@@ -411,9 +420,9 @@ def run_ours(args):
     hbm = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     width = 4.0 if head == "mixed" else 8.0
-    kb = kernel_bytes(top, wl, width)
-    achieved = 2 * kb / (slots[top] * 1e-3) / 1e9 if slots[top] > 0 else 0.0
     kroof = kernel_rooflines(slots, wl, head, hbm)
+    kb = kroof[top]["algorithmic_bytes"] if top in kroof else kernel_bytes(top, wl, width)
+    achieved = kroof[top]["achieved_gbs"] if top in kroof else 0.0
     ms = runs[head]["ms"]
     step_gbs = algorithmic_bytes_per_cell_update(pb.n3) * cells / (ms * 1e-3 / args.steps) / 1e9
 

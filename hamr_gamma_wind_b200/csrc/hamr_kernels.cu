@@ -346,6 +346,9 @@ __host__ __device__ __forceinline__ long n_x3_slots(const Dims &d) {
 // kernels. Measured per 384 x 192 x 192 step: float 10 blocks (48 registers)
 // 2.04 ms, 12: 2.09, 8: 2.14, 6 (80 registers, no spills): 2.54; double 6
 // blocks 8.10 ms, 5: 8.16, 4: 8.16
+#ifndef HAMR_FLUX_FT_X3_MINB   // the FP64 face-frame solvers (HLLC, HLLD) in the x3 slot kernel
+#define HAMR_FLUX_FT_X3_MINB 6
+#endif
 #ifndef HAMR_FLUX_X3_MINB
 #define HAMR_FLUX_X3_MINB 6
 #endif
@@ -362,7 +365,8 @@ __device__ __forceinline__ void emf_centre_eval(const Dims &d, const Geom &m, co
 // primitives are already in L1 from its reconstruction stencil. A slot that
 // two CTAs share is done by the first. Same values as k_emf_centre.
 template <typename T, int REC>
-__global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? HAMR_FLUX_X3_MINB : HAMR_FLUX_X3_MINB_F)
+__global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? ((REC & 2) != 0 ? HAMR_FLUX_FT_X3_MINB : HAMR_FLUX_X3_MINB)
+                                                         : HAMR_FLUX_X3_MINB_F)
     k_flux_x3(const Dims d, const Geom m, const double *__restrict__ pv, const double *__restrict__ ps,
               T *__restrict__ F, unsigned long long *__restrict__ dtbits, int calc_dt, T *__restrict__ Ec) {
     __shared__ T slo[NPR - 1][BLK], shi[NPR - 1][BLK];   // zone edges per slot (B3 skipped)
