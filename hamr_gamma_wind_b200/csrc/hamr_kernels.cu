@@ -138,6 +138,9 @@ struct StepSize {
 #ifndef HAMR_FLUX_FT_ROWS_MINB
 #define HAMR_FLUX_FT_ROWS_MINB 3
 #endif
+#ifndef HAMR_FLUX_FT_ROWS_MINB_F   // the same in the float step
+#define HAMR_FLUX_FT_ROWS_MINB_F HAMR_FLUX_ROWS_MINB_F
+#endif
 
 // The CFL limit of a face is cour dx / ctop (fluxcalc2D2's dtij, counted
 // when above 1e-6), the block's the minimum over its faces and 1e9. A face
@@ -344,13 +347,22 @@ __host__ __device__ __forceinline__ long n_x3_slots(const Dims &d) {
 
 // build options: resident blocks per SM for the double and float x3 slot
 // kernels. Measured per 384 x 192 x 192 step: float 10 blocks (48 registers)
-// 2.04 ms, 12: 2.09, 8: 2.14, 6 (80 registers, no spills): 2.54; double 6
-// blocks 8.10 ms, 5: 8.16, 4: 8.16
-#ifndef HAMR_FLUX_FT_X3_MINB   // the FP64 face-frame solvers (HLLC, HLLD) in the x3 slot kernel
-#define HAMR_FLUX_FT_X3_MINB 6
+// 2.04 ms, 12: 2.09, 8: 2.14, 6 (80 registers, no spills): 2.54; double (with
+// the shared-divisor quotients and the centre EMFs) 5 blocks 5.48 ms, 4:
+// 5.52, 6: 5.62.
+// The face-frame solvers (HLLC, HLLD) in the x3 slot kernel, which hold both
+// frame states, their fluxes and (HLLD) the wave fan in thread-local arrays:
+// on the 384 x 192 x 192 torus, FP64, per step, 4 blocks per SM (128
+// registers) HLLC 8.63 ms / HLLD 9.68 ms, 5: 8.66 / 11.98, 6: 9.80 / 14.91,
+// 3: 9.50 / 9.87
+#ifndef HAMR_FLUX_FT_X3_MINB
+#define HAMR_FLUX_FT_X3_MINB 4
+#endif
+#ifndef HAMR_FLUX_FT_X3_MINB_F   // float: 7 blocks, HLLC 3.83 -> 3.69 ms, HLLD 6.19 -> 3.96 (5: 4.01 / 4.22)
+#define HAMR_FLUX_FT_X3_MINB_F 7
 #endif
 #ifndef HAMR_FLUX_X3_MINB
-#define HAMR_FLUX_X3_MINB 6
+#define HAMR_FLUX_X3_MINB 5
 #endif
 #ifndef HAMR_FLUX_X3_MINB_F
 #define HAMR_FLUX_X3_MINB_F 10
@@ -366,7 +378,7 @@ __device__ __forceinline__ void emf_centre_eval(const Dims &d, const Geom &m, co
 // two CTAs share is done by the first. Same values as k_emf_centre.
 template <typename T, int REC>
 __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? ((REC & 2) != 0 ? HAMR_FLUX_FT_X3_MINB : HAMR_FLUX_X3_MINB)
-                                                         : HAMR_FLUX_X3_MINB_F)
+                                                         : ((REC & 2) != 0 ? HAMR_FLUX_FT_X3_MINB_F : HAMR_FLUX_X3_MINB_F))
     k_flux_x3(const Dims d, const Geom m, const double *__restrict__ pv, const double *__restrict__ ps,
               T *__restrict__ F, unsigned long long *__restrict__ dtbits, int calc_dt, T *__restrict__ Ec) {
     __shared__ T slo[NPR - 1][BLK], shi[NPR - 1][BLK];   // zone edges per slot (B3 skipped)
@@ -431,8 +443,8 @@ __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? ((REC & 2) != 0 ? HAMR_F
 #define HAMR_FLUX_ROW 12
 #endif
 constexpr int FLUX_ROW = HAMR_FLUX_ROW;
-#ifndef HAMR_FLUX_ROWS_MINB
-#define HAMR_FLUX_ROWS_MINB HAMR_FLUX_MINB
+#ifndef HAMR_FLUX_ROWS_MINB   // FP64: 4 blocks (128 registers) x2 + x1 9.18 -> 8.79 ms per step (5: 96)
+#define HAMR_FLUX_ROWS_MINB 4
 #endif
 #ifndef HAMR_FLUX_ROWS_MINB_F
 #define HAMR_FLUX_ROWS_MINB_F 7
@@ -495,7 +507,7 @@ struct RowWindow {
 
 template <int DIR, typename T, int REC>
 __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? ((REC & 2) != 0 ? HAMR_FLUX_FT_ROWS_MINB : HAMR_FLUX_ROWS_MINB)
-                                                         : HAMR_FLUX_ROWS_MINB_F)
+                                                         : ((REC & 2) != 0 ? HAMR_FLUX_FT_ROWS_MINB_F : HAMR_FLUX_ROWS_MINB_F))
     k_flux_rows(const Dims d, const Geom m, const double *__restrict__ pv, const double *__restrict__ ps,
                 T *__restrict__ F, unsigned long long *__restrict__ dtbits, int calc_dt) {
     using Win = RowWindow<DIR, T, REC>;

@@ -1003,18 +1003,20 @@ __device__ __forceinline__ void hlld_side(int dir, T ptot, T S, T sgn, T BX, con
     const T C = R[U_2] * R[B_2] + R[U_3] * R[B_3];
     const T Q = -A - G + (BX * BX) * (T(1.) - S * S);
     const T X = BX * (A * S * BX + C) - (A + G) * (S * ptot - R[UU]);
-    v[G_1] = (BX * (A * BX + S * C) - (A + G) * (ptot + R[U_1])) / (X);
-    v[G_2] = (Q * R[U_2] + R[B_2] * (C + BX * (S * R[U_1] + R[UU]))) / (X);
-    v[G_3] = (Q * R[U_3] + R[B_3] * (C + BX * (S * R[U_1] + R[UU]))) / (X);
+    const Divisor<T> dX(X);   // quotients sharing a divisor (exact form in FP64)
+    v[G_1] = dX.div(BX * (A * BX + S * C) - (A + G) * (ptot + R[U_1]));
+    v[G_2] = dX.div(Q * R[U_2] + R[B_2] * (C + BX * (S * R[U_1] + R[UU])));
+    v[G_3] = dX.div(Q * R[U_3] + R[B_3] * (C + BX * (S * R[U_1] + R[UU])));
     w = ptot + (-R[UU] - (v[G_1] * R[U_1] + v[G_2] * R[U_2] + v[G_3] * R[U_3])) / (S - v[G_1] + T(SMALL_D));
     Bs[G_1] = BX;
-    Bs[G_2] = (R[B_2] - Bs[G_1] * v[G_2]) / (S - v[G_1]);
-    Bs[G_3] = (R[B_3] - Bs[G_1] * v[G_3]) / (S - v[G_1]);
+    const Divisor<T> dS(S - v[G_1]);
+    Bs[G_2] = dS.div(R[B_2] - Bs[G_1] * v[G_2]);
+    Bs[G_3] = dS.div(R[B_3] - Bs[G_1] * v[G_3]);
     eta = sgn * ((T)(BX > T(0.0)) - (T)(BX <= T(0.0))) * d_sqrt(d_fabs(w));
-    const T den = S * ptot - R[UU] + BX * eta;
-    K[G_1] = (R[U_1] + ptot + R[B_1] * eta) / den;
-    K[G_2] = (R[U_2] + R[B_2] * eta) / den;
-    K[G_3] = (R[U_3] + R[B_3] * eta) / den;
+    const Divisor<T> dden(S * ptot - R[UU] + BX * eta);
+    K[G_1] = dden.div(R[U_1] + ptot + R[B_1] * eta);
+    K[G_2] = dden.div(R[U_2] + R[B_2] * eta);
+    K[G_3] = dden.div(R[U_3] + R[B_3] * eta);
 }
 
 // calc_error_HLLD (GPU_hllc.h:685-876, its live second half)
@@ -1025,12 +1027,12 @@ __device__ __forceinline__ T hlld_error(int dir, T ptot, T cmin, T cmax, T BX, c
     hlld_side(dir, ptot, cmin, T(-1.), BX, R_l, f.v_al, f.B_al, f.K_al, f.w_al, f.eta_l);
     hlld_side(dir, ptot, cmax, T(1.), BX, R_r, f.v_ar, f.B_ar, f.K_ar, f.w_ar, f.eta_r);
     f.B_c[G_1] = BX;
+    const Divisor<T> dK(f.K_ar[dir] - f.K_al[dir] + T(1e-12));
 #pragma unroll
     for (int t = 0; t < 2; t++) {
         const int Gt = t ? G_3 : G_2;
-        f.B_c[Gt] = ((f.B_ar[Gt] * (f.K_ar[G_1] - f.v_ar[dir]) + f.B_ar[dir] * f.v_ar[Gt]) -
-                     (f.B_al[Gt] * (f.K_al[G_1] - f.v_al[dir]) + f.B_al[dir] * f.v_al[Gt])) /
-                    (f.K_ar[dir] - f.K_al[dir] + T(1e-12));
+        f.B_c[Gt] = dK.div((f.B_ar[Gt] * (f.K_ar[G_1] - f.v_ar[dir]) + f.B_ar[dir] * f.v_ar[Gt]) -
+                           (f.B_al[Gt] * (f.K_al[G_1] - f.v_al[dir]) + f.B_al[dir] * f.v_al[Gt]));
     }
     const T delta_Kx = (f.K_ar[dir] - f.K_al[dir]);
     T B_hat[4];
@@ -1044,10 +1046,11 @@ __device__ __forceinline__ T hlld_error(int dir, T ptot, T cmin, T cmax, T BX, c
     const T error = delta_Kx * (T(1.) - f.B_ar[dir] * (Y_r - Y_l));
     const T kbl = f.eta_l - (f.K_al[1] * f.B_c[1] + f.K_al[2] * f.B_c[2] + f.K_al[3] * f.B_c[3]);
     const T kbr = f.eta_r - (f.K_ar[1] * f.B_c[1] + f.K_ar[2] * f.B_c[2] + f.K_ar[3] * f.B_c[3]);
+    const Divisor<T> dkl(kbl), dkr(kbr);
 #pragma unroll
     for (int q = 1; q < 4; q++) {
-        f.v_cl[q] = (f.K_al[q] - (f.B_c[q] * (T(1.) - kl2)) / kbl);
-        f.v_cr[q] = (f.K_ar[q] - (f.B_c[q] * (T(1.) - kr2)) / kbr);
+        f.v_cl[q] = (f.K_al[q] - dkl.div(f.B_c[q] * (T(1.) - kl2)));
+        f.v_cr[q] = (f.K_ar[q] - dkr.div(f.B_c[q] * (T(1.) - kr2)));
     }
     f.v_cl[dir] = (f.v_cl[dir] + f.v_cr[dir]) * T(0.5);
     f.v_cr[dir] = f.v_cl[dir];
@@ -1143,7 +1146,8 @@ template <typename T>
 __device__ __forceinline__ void hlld_outer(int dir, T S, const T *R, T ptot, const T *v, const T *Bs, T BX, T *X) {
     const int G_1 = dir, G_2 = dir % 3 + 1, G_3 = (dir + 1) % 3 + 1;
     const T v_dot_B = v[1] * Bs[1] + v[2] * Bs[2] + v[3] * Bs[3];
-    X[RHO] = R[RHO] / (S - v[G_1]);
+    const Divisor<T> dS(S - v[G_1]);
+    X[RHO] = dS.div(R[RHO]);
     X[UU] = (R[UU] - ptot * v[G_1] + v_dot_B * Bs[G_1]) / (S - v[G_1] + T(SMALL_D));
     X[UU + G_1] = (-X[UU] + ptot) * v[G_1] - v_dot_B * Bs[G_1];
     X[UU + G_2] = (-X[UU] + ptot) * v[G_2] - v_dot_B * Bs[G_2];
@@ -1151,7 +1155,7 @@ __device__ __forceinline__ void hlld_outer(int dir, T S, const T *R, T ptot, con
     X[B1 + G_1 - 1] = BX;
     X[B1 + G_2 - 1] = Bs[G_2];
     X[B1 + G_3 - 1] = Bs[G_3];
-    X[KTOT] = R[KTOT] / (S - v[G_1]);
+    X[KTOT] = dS.div(R[KTOT]);
 }
 
 // inner intermediate state (between the Alfven wave and the contact)
@@ -1160,15 +1164,16 @@ __device__ __forceinline__ void hlld_inner(int dir, const T *Xa, T Ka, const T *
                                            T BX, T *X) {
     const int G_1 = dir, G_2 = dir % 3 + 1, G_3 = (dir + 1) % 3 + 1;
     const T v_dot_B = vc[1] * Bc[1] + vc[2] * Bc[2] + vc[3] * Bc[3];
-    X[RHO] = Xa[RHO] * (Ka - va[G_1]) / (Ka - vc[G_1]);
-    X[UU] = -(-Ka * Xa[UU] - Xa[UU + G_1] + ptot * vc[G_1] - v_dot_B * Xa[B1 + G_1 - 1]) / (Ka - vc[G_1]);
+    const Divisor<T> dK(Ka - vc[G_1]);
+    X[RHO] = dK.div(Xa[RHO] * (Ka - va[G_1]));
+    X[UU] = dK.div(-(-Ka * Xa[UU] - Xa[UU + G_1] + ptot * vc[G_1] - v_dot_B * Xa[B1 + G_1 - 1]));
     X[UU + G_1] = (-Xa[UU] + ptot) * vc[G_1] - v_dot_B * Bc[G_1];
     X[UU + G_2] = (-Xa[UU] + ptot) * vc[G_2] - v_dot_B * Bc[G_2];
     X[UU + G_3] = (-Xa[UU] + ptot) * vc[G_3] - v_dot_B * Bc[G_3];
     X[B1 + G_1 - 1] = BX;
     X[B1 + G_2 - 1] = Bc[G_2];
     X[B1 + G_3 - 1] = Bc[G_3];
-    X[KTOT] = Xa[KTOT] * (Ka - va[G_1]) / (Ka - vc[G_1]);
+    X[KTOT] = dK.div(Xa[KTOT] * (Ka - va[G_1]));
 }
 
 // calc_HLLD (GPU_hllc.h:398-423): HLLD star fluxes where the fan passes every
