@@ -62,8 +62,9 @@ struct Geom {
     // with the inversion's own operations; then 1/gdet at the FACE1, FACE2
     // and FACE3 locations (the face update's divisions by the face volume);
     // then the lapse at each of the 5 locations (planes 6-10) and its
-    // reciprocal (11-15), with geo_lapse's operations (k_inv_tab)
-    const double *itab = nullptr;
+    // reciprocal (11-15), with geo_lapse's operations (k_inv_tab). Brace
+    // initialisation with the four metric tables leaves it null.
+    const double *itab;
 };
 
 __device__ __forceinline__ long cix(const Dims &d, int i, int j, int z) { return ((long)i * d.G2 + j) * d.G3 + z; }
@@ -505,6 +506,57 @@ struct RowWindow {
     }
 };
 
+// One row of FLUX_ROW faces along DIR (row t < n_flux_rows), reconstructed
+// through the thread's stencil window in `wbuf` (a CTA's NW * NK * BLK
+// values; column threadIdx.x); returns the row's largest signal-speed
+// contribution (ctop_term)
+template <int DIR, typename T, int REC>
+__device__ __forceinline__ double flux_row(const Dims &d, const Geom &m, const double *__restrict__ pv,
+                                           const double *__restrict__ ps, T *__restrict__ F, T *wbuf, const long t) {
+    using Win = RowWindow<DIR, T, REC>;
+    double cmx = 0.0;
+    const int nz = d.n3 + 2 * d.d3, z = (d.ng3 - 1) * d.d3 + (int)(t % nz);
+    const long r = t / nz;
+    const int nt = DIR == 1 ? d.n2 + 2 * d.d2 : d.n1 + 2 * d.d1;
+    const int a = (DIR == 1 ? (d.ng2 - 1) * d.d2 : (d.ng1 - 1) * d.d1) + (int)(r % nt);   // j or i
+    const int seg = (int)(r / nt);
+    const int nf = DIR == 1 ? d.n1 + 2 * d.d1 - 1 : d.n2 + 2 * d.d2 - 1;
+    const int ng = DIR == 1 ? d.ng1 : d.ng2;
+    const int f0 = ng + seg * FLUX_ROW;
+    const int f1 = min(f0 + FLUX_ROW, ng + nf);
+    const long stride = DIR == 1 ? (long)d.G2 * d.G3 : (long)d.G3;
+    const int face = DIR == 1 ? FACE1 : FACE2;
+    const Win win{wbuf + threadIdx.x};
+    constexpr int NW = Win::NW, H = Win::H;
+    T pl[NPR], lo[NPR], hi[NPR];
+    // the stencil of the zone below the first face, zones f0 - 1 - H ..
+    // f0 - 1 + H (f0 >= ng > H), then its upper edge: the first left state
+    const long cf0 = DIR == 1 ? cix(d, f0, a, z) : cix(d, a, f0, z);
+#pragma unroll
+    for (int s = 0; s < NW; s++) win.load(d, pv, cf0 + (s - 1 - H) * stride, (f0 - 1 - H + s) % NW);
+    win.edges((f0 - 1 - H) % NW, lo, hi);
+#pragma unroll
+    for (int k = 0; k < NPR; k++) pl[k] = hi[k];
+    int s0 = (f0 - H) % NW;   // slot of zone f - H
+    for (int f = f0; f < f1; f++) {
+        const int i = DIR == 1 ? f : a, j = DIR == 1 ? a : f;
+        const long c = cix(d, i, j, z);
+        // zone f + H replaces zone f - H - 1 (slot s0 + 2H, mod NW)
+        win.load(d, pv, c + H * stride, s0 == 0 ? NW - 1 : s0 - 1);
+        win.edges(s0, lo, hi);
+        s0 = s0 == NW - 1 ? 0 : s0 + 1;
+        Geo<T> gm;
+        load_geo_t(d, m, i, j, face, gm);
+        T l[NPR];
+#pragma unroll
+        for (int k = 0; k < NPR; k++) l[k] = pl[k];
+        cmx = d_max(cmx, flux_eval<DIR, T, REC>(d, gm, ps, l, lo, F, c, j));
+#pragma unroll
+        for (int k = 0; k < NPR; k++) pl[k] = hi[k];
+    }
+    return cmx;
+}
+
 template <int DIR, typename T, int REC>
 __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? ((REC & 2) != 0 ? HAMR_FLUX_FT_ROWS_MINB : HAMR_FLUX_ROWS_MINB)
                                                          : ((REC & 2) != 0 ? HAMR_FLUX_FT_ROWS_MINB_F : HAMR_FLUX_ROWS_MINB_F))
@@ -513,48 +565,7 @@ __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? ((REC & 2) != 0 ? HAMR_F
     using Win = RowWindow<DIR, T, REC>;
     __shared__ T wbuf[Win::NW * Win::NK * BLK];
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    double cmx = 0.0;
-    if (t < n_flux_rows<DIR>(d)) {
-        const int nz = d.n3 + 2 * d.d3, z = (d.ng3 - 1) * d.d3 + (int)(t % nz);
-        const long r = t / nz;
-        const int nt = DIR == 1 ? d.n2 + 2 * d.d2 : d.n1 + 2 * d.d1;
-        const int a = (DIR == 1 ? (d.ng2 - 1) * d.d2 : (d.ng1 - 1) * d.d1) + (int)(r % nt);   // j or i
-        const int seg = (int)(r / nt);
-        const int nf = DIR == 1 ? d.n1 + 2 * d.d1 - 1 : d.n2 + 2 * d.d2 - 1;
-        const int ng = DIR == 1 ? d.ng1 : d.ng2;
-        const int f0 = ng + seg * FLUX_ROW;
-        const int f1 = min(f0 + FLUX_ROW, ng + nf);
-        const long stride = DIR == 1 ? (long)d.G2 * d.G3 : (long)d.G3;
-        const int face = DIR == 1 ? FACE1 : FACE2;
-        const Win win{wbuf + threadIdx.x};
-        constexpr int NW = Win::NW, H = Win::H;
-        T pl[NPR], lo[NPR], hi[NPR];
-        // the stencil of the zone below the first face, zones f0 - 1 - H ..
-        // f0 - 1 + H (f0 >= ng > H), then its upper edge: the first left state
-        const long cf0 = DIR == 1 ? cix(d, f0, a, z) : cix(d, a, f0, z);
-#pragma unroll
-        for (int s = 0; s < NW; s++) win.load(d, pv, cf0 + (s - 1 - H) * stride, (f0 - 1 - H + s) % NW);
-        win.edges((f0 - 1 - H) % NW, lo, hi);
-#pragma unroll
-        for (int k = 0; k < NPR; k++) pl[k] = hi[k];
-        int s0 = (f0 - H) % NW;   // slot of zone f - H
-        for (int f = f0; f < f1; f++) {
-            const int i = DIR == 1 ? f : a, j = DIR == 1 ? a : f;
-            const long c = cix(d, i, j, z);
-            // zone f + H replaces zone f - H - 1 (slot s0 + 2H, mod NW)
-            win.load(d, pv, c + H * stride, s0 == 0 ? NW - 1 : s0 - 1);
-            win.edges(s0, lo, hi);
-            s0 = s0 == NW - 1 ? 0 : s0 + 1;
-            Geo<T> gm;
-            load_geo_t(d, m, i, j, face, gm);
-            T l[NPR];
-#pragma unroll
-            for (int k = 0; k < NPR; k++) l[k] = pl[k];
-            cmx = d_max(cmx, flux_eval<DIR, T, REC>(d, gm, ps, l, lo, F, c, j));
-#pragma unroll
-            for (int k = 0; k < NPR; k++) pl[k] = hi[k];
-        }
-    }
+    const double cmx = t < n_flux_rows<DIR>(d) ? flux_row<DIR, T, REC>(d, m, pv, ps, F, wbuf, t) : 0.0;
     if (calc_dt) cta_max_ctop(d, DIR, cmx, &dtbits[DIR]);
 }
 
