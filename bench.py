@@ -160,9 +160,9 @@ def launches_per_step(pb) -> int:
     dims = [n > 1 for n in (pb.n1, pb.n2, pb.n3)]
     per_stage = sum(dims)                       # face fluxes
     per_stage += pb.bc[1] == "pole_refl"        # polar flux fix
-    per_stage += 2                              # centre and edge EMFs
+    per_stage += 1 if pb.n3 > 1 else 2          # edge EMFs (+ centre EMFs; in 3-D the x3 flux kernel makes them)
     per_stage += pb.bc[1] == "pole_trans"       # polar EMF average
-    per_stage += 1 + 2                          # face update, conserved update, inversion
+    per_stage += 1 + 1 + 2                      # face update, conserved update, inversion (two passes)
     per_stage += sum(dims)                      # ghost fills
     return 2 * per_stage + 1
 
