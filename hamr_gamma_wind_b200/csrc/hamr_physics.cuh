@@ -55,7 +55,12 @@ template <> __device__ __forceinline__ double d_sqrt<double>(double x) { return 
 template <> __device__ __forceinline__ float d_sqrt<float>(float x) { return sqrtf(x); }
 template <typename T> __device__ __forceinline__ T d_pow(T x, T y);
 template <> __device__ __forceinline__ double d_pow<double>(double x, double y) { return pow(x, y); }
-template <> __device__ __forceinline__ float d_pow<float>(float x, float y) { return powf(x, y); }
+// float (the mixed step's entropy K = P rho^-gam of the face states, which
+// only the entropy flux carries): the fast exp2(y log2 x) intrinsic, relative
+// error a few 1e-6 at the atmosphere's densities against powf's ulp; measured
+// on the 384 x 192 x 192 torus: the three float flux kernels 6.05 -> 5.59 ms
+// per step, L1 of every field against FP64 after 1000 steps unchanged
+template <> __device__ __forceinline__ float d_pow<float>(float x, float y) { return __powf(x, y); }
 template <typename T> __device__ __forceinline__ T d_fabs(T x) { return x < T(0) ? -x : x; }
 // x^(-1/2), correctly rounded in all but vanishingly rare near-midpoint cases,
 // so that it agrees with a correctly rounded host pow(x, -0.5): the IEEE
