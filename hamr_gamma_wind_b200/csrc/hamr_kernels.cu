@@ -1475,12 +1475,29 @@ __host__ __device__ __forceinline__ ConsTmaLayout cons_tma_layout(int lpiece) {
 #ifndef HAMR_CONS_TMA_MINB
 #define HAMR_CONS_TMA_MINB 4
 #endif
-template <typename T>
-__global__ void __launch_bounds__(256, sizeof(T) == 8 ? HAMR_CONS_TMA_MINB : HAMR_CONS_TMA_MINB_F)
+// FUSE: 0 writes the seven planes of W for the inversion kernels; HAMR_INV_2D
+// + 1 or HAMR_INV_NM + 1 runs the primary inversion of each zone right after
+// its update (no floors or repair): the guess is pb (the state the update
+// read), the face field psf, the output pout, and only a zone whose primary
+// solver fails writes W and goes to the list for k_invert_fallback (*nfail
+// cleared before the launch). The W round trip and the inversion's reload of
+// the guess disappear; same values as the update followed by
+// k_invert_primary.
+#ifndef HAMR_CONS_INV_TMA_MINB   // the same kernel with the primary inversion inside (FUSE != 0);
+#define HAMR_CONS_INV_TMA_MINB 3    // FP64 at 4 blocks spills 0.6 KB a thread (measured C3 update+inversion
+#endif                              // 5.35 ms at 3 blocks, 6.0 at 4, 5.43 at 2)
+#ifndef HAMR_CONS_INV_TMA_MINB_F
+#define HAMR_CONS_INV_TMA_MINB_F HAMR_CONS_TMA_MINB_F
+#endif
+template <typename T, int FUSE = 0>
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? (FUSE ? HAMR_CONS_INV_TMA_MINB : HAMR_CONS_TMA_MINB)
+                                                       : (FUSE ? HAMR_CONS_INV_TMA_MINB_F : HAMR_CONS_TMA_MINB_F))
     k_cons_tma(const Dims d, const Geom m, const double *__restrict__ pin, const double *__restrict__ pb,
                double *__restrict__ Ucache, const T *__restrict__ F1, const T *__restrict__ F2,
                const T *__restrict__ F3, double *__restrict__ W, int full, StepSize st, int *__restrict__ nfail,
-               int *__restrict__ kerr, int npiece, int lpiece) {
+               int *__restrict__ kerr, int npiece, int lpiece, const double *__restrict__ psf = nullptr,
+               double *__restrict__ pout = nullptr, int *__restrict__ pflag = nullptr,
+               int *__restrict__ failimage = nullptr, int *__restrict__ flist = nullptr) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int A = 16 / (int)sizeof(T);
     const ConsTmaLayout lay = cons_tma_layout<T>(lpiece);
@@ -1494,7 +1511,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? HAMR_CONS_TMA_MINB : HAM
     const int L = min(lpiece, d.n3 - piece * lpiece);
     const long ks = d.ks, isize = (long)d.G2 * d.G3;
     const long c0 = cix(d, i, j, za), gi = gix(d, i, j);
-    if (blockIdx.x == 0 && threadIdx.x == 0) *nfail = 0;   // the inversion's failed-zone list starts empty
+    if (!FUSE && blockIdx.x == 0 && threadIdx.x == 0) *nfail = 0;   // the inversion's failed-zone list starts empty
     // the five segment kinds: start cell, length, source array
     auto seg_start = [&](int q) -> long { return q == 1 ? c0 + isize : (q == 3 ? c0 + d.G3 : c0); };
     auto seg_len = [&](int q) -> int { return q == 4 ? L + 1 : L; };
@@ -1554,13 +1571,36 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? HAMR_CONS_TMA_MINB : HAM
     geo_lapse(gm);
     double pf[NPR], U[NPR];
     cons_update_fx<T>(d, m, pin, pb, Ucache, fx, full, st.sub(), i, j, c, gi, gm, ConnStaged{sg + 21}, pf, U);
-    W[0 * d.ks + c] = U[RHO];
-    W[1 * d.ks + c] = U[UU];
-    W[2 * d.ks + c] = U[U1];
-    W[3 * d.ks + c] = U[U2];
-    W[4 * d.ks + c] = U[U3];
-    W[5 * d.ks + c] = U[KTOT];
-    W[6 * d.ks + c] = U[B3];
+    auto write_w = [&]() {
+        W[0 * d.ks + c] = U[RHO];
+        W[1 * d.ks + c] = U[UU];
+        W[2 * d.ks + c] = U[U1];
+        W[3 * d.ks + c] = U[U2];
+        W[4 * d.ks + c] = U[U3];
+        W[5 * d.ks + c] = U[KTOT];
+        W[6 * d.ks + c] = U[B3];
+    };
+    if constexpr (FUSE == 0) {
+        write_w();
+    } else {
+        constexpr int INV = FUSE - 1;
+        const double Uw[7] = {U[RHO], U[UU], U[U1], U[U2], U[U3], U[KTOT], U[B3]};
+        // the inversion's inputs as k_invert_primary reads them: the guess
+        // straight from pb, U[B] from the updated faces
+#pragma unroll
+        for (int k = 0; k < NPR; k++) pf[k] = pb[k * ks + c];
+        face_average_b(d, m, psf, i, j, c, gi, U);
+        const int flag = invert_primary<INV>(d, inv_k(d, m, gi, gm), gm, U, pf);
+        if (flag) {
+            U[RHO] = Uw[0]; U[UU] = Uw[1]; U[U1] = Uw[2]; U[U2] = Uw[3]; U[U3] = Uw[4]; U[KTOT] = Uw[5];
+            U[B3] = Uw[6];
+            write_w();
+            const long t = ((long)(i - d.ng1) * d.n2 + (j - d.ng2)) * d.n3 + (za - d.ng3 + l);
+            flist[atomicAdd(nfail, 1)] = (int)t;
+            return;
+        }
+        invert_epilogue<0>(d, gm, c, flag, pf, pout, pflag, failimage);
+    }
 }
 
 template <int INV, int FIX = 0>
@@ -2069,6 +2109,9 @@ struct hamr_ctx {
     // 3-D blocks: the centre EMFs computed by the x3 flux kernel instead of
     // k_emf_centre (HAMR_EMF_IN_X3=0 keeps the separate kernel)
     bool emf_in_x3 = true;
+    // the primary inversion inside the TMA-staged update kernel (no floors or
+    // repair; HAMR_FUSE_INV=0 keeps the separate inversion kernel)
+    bool fuse_inv = true;
     cudaStream_t side[2] = {nullptr, nullptr};
     cudaEvent_t ev[5] = {};
     std::string err;
@@ -2300,11 +2343,28 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
     {
         long n = (long)d.n1 * d.n2 * d.n3;
         const bool tma = ctx->cons_tma && d.d3 && d.n3 >= 32 && cons_tma_aligned<T>(ctx, d, F1, F2, F3);
+        const int fix = (ctx->prm.floors ? FIX_FLOORS : 0) | (ctx->prm.repair == 1 ? FIX_RESET : 0);
+        double *pout = full ? ctx->p : ctx->ph;
+        const double *pg = full ? ctx->ph : ctx->p;
+        const double *psf = full ? ctx->ps : ctx->psh;
+        const int nm = d.inversion == HAMR_INV_NM;
+        // the primary inversion inside the update kernel (the face update, which
+        // it reads, has run in this stream)
+        const bool fuse = tma && ctx->fuse_inv && fix == 0 && ctx->prm.repair != 2 && !conc;
         if (tma) {   // one row of zones per CTA, flux operands staged by bulk copies
             const int npiece = (d.n3 + 255) / 256, lpiece = (d.n3 + npiece - 1) / npiece;
-            k_cons_tma<T><<<d.n1 * d.n2 * npiece, (lpiece + 31) / 32 * 32, cons_tma_layout<T>(lpiece).total, s>>>(
-                d, m, ctx->p, full ? ctx->ph : ctx->p, ctx->U, F1, F2, F3, ctx->W, full, st, ctx->nfail, ctx->kerr,
-                npiece, lpiece);
+            const dim3 grid(d.n1 * d.n2 * npiece), block((lpiece + 31) / 32 * 32);
+            const size_t sm = cons_tma_layout<T>(lpiece).total;
+            if (fuse) {
+                CK(cudaMemsetAsync(ctx->nfail, 0, sizeof(int), s));
+                auto kf = nm ? k_cons_tma<T, HAMR_INV_NM + 1> : k_cons_tma<T, HAMR_INV_2D + 1>;
+                kf<<<grid, block, sm, s>>>(d, m, ctx->p, pg, ctx->U, F1, F2, F3, ctx->W, full, st, ctx->nfail,
+                                           ctx->kerr, npiece, lpiece, psf, pout, ctx->pflag, ctx->failimage,
+                                           ctx->flist);
+            } else {
+                k_cons_tma<T><<<grid, block, sm, s>>>(d, m, ctx->p, pg, ctx->U, F1, F2, F3, ctx->W, full, st,
+                                                      ctx->nfail, ctx->kerr, npiece, lpiece);
+            }
         } else if (d.n3 >= 64 && ctx->cons_cols)   // metric and connection staged per CTA
             k_cons_cols<T><<<nblk(n), BLK, 0, s>>>(d, m, ctx->p, full ? ctx->ph : ctx->p, ctx->U, F1, F2, F3, ctx->W,
                                                    full, st, ctx->nfail);
@@ -2316,9 +2376,6 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
             CK(cudaEventRecord(ctx->ev[4], s2));
             CK(cudaStreamWaitEvent(s, ctx->ev[4], 0));
         }
-        // (the inversion gained nothing from the same staging: FP64 Newton work
-        // bounds it, not its 26 metric loads per zone)
-        const int fix = (ctx->prm.floors ? FIX_FLOORS : 0) | (ctx->prm.repair == 1 ? FIX_RESET : 0);
         // primary solver over every zone, then the fallback chain over the
         // zones it failed (usually none: the second launch reads the count
         // and returns)
@@ -2336,12 +2393,9 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
              k_invert_fallback<HAMR_INV_2D, 3>},
             {k_invert_fallback<HAMR_INV_NM, 0>, k_invert_fallback<HAMR_INV_NM, 1>, k_invert_fallback<HAMR_INV_NM, 2>,
              k_invert_fallback<HAMR_INV_NM, 3>}};
-        double *pout = full ? ctx->p : ctx->ph;
-        const double *pg = full ? ctx->ph : ctx->p;
-        const double *psf = full ? ctx->ps : ctx->psh;
-        const int nm = d.inversion == HAMR_INV_NM;
-        inv_p[nm][fix]<<<nblk(n), BLK, 0, s>>>(d, m, pg, ctx->W, psf, pout, ctx->pflag, ctx->failimage, ctx->flist,
-                                               ctx->nfail);
+        if (!fuse)
+            inv_p[nm][fix]<<<nblk(n), BLK, 0, s>>>(d, m, pg, ctx->W, psf, pout, ctx->pflag, ctx->failimage,
+                                                   ctx->flist, ctx->nfail);
         inv_f[nm][fix]<<<FALLBACK_CTAS, BLK, 0, s>>>(d, m, pg, ctx->W, psf, pout, ctx->pflag, ctx->failimage,
                                                      ctx->flist, ctx->nfail);
         if (ctx->prm.repair == 2) {
@@ -2445,6 +2499,7 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
         if (const char *e = getenv("HAMR_CONS_TMA")) ctx->cons_tma = atoi(e) != 0;
         if (const char *e = getenv("HAMR_CONCURRENT")) ctx->concurrent = atoi(e) != 0;
         if (const char *e = getenv("HAMR_EMF_IN_X3")) ctx->emf_in_x3 = atoi(e) != 0;
+        if (const char *e = getenv("HAMR_FUSE_INV")) ctx->fuse_inv = atoi(e) != 0;
     }
     if (ctx->concurrent) {
         for (auto &st : ctx->side)
@@ -2483,6 +2538,14 @@ int hamr_ctx_create(const hamr_params *prm, hamr_ctx **out) {
     cudaFuncSetAttribute(k_cons_tma<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          cons_tma_layout<double>(256).total);
     cudaFuncSetAttribute(k_cons_tma<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         cons_tma_layout<float>(256).total);
+    cudaFuncSetAttribute(k_cons_tma<double, HAMR_INV_2D + 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         cons_tma_layout<double>(256).total);
+    cudaFuncSetAttribute(k_cons_tma<double, HAMR_INV_NM + 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         cons_tma_layout<double>(256).total);
+    cudaFuncSetAttribute(k_cons_tma<float, HAMR_INV_2D + 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         cons_tma_layout<float>(256).total);
+    cudaFuncSetAttribute(k_cons_tma<float, HAMR_INV_NM + 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          cons_tma_layout<float>(256).total);
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
         hamr_ctx_destroy(ctx);

@@ -557,3 +557,35 @@ def test_centre_emfs_in_x3_kernel_match_separate_kernel(precision, shape, monkey
     assert np.isfinite(pb.active(out["0"][0])).all()
     assert np.array_equal(out["1"][0], out["0"][0])
     assert np.array_equal(out["1"][1], out["0"][1])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("inversion", ["2d", "nm"])
+def test_inversion_inside_update_matches_separate_kernels(precision, inversion, monkeypatch):
+    """The primary inversion run inside the TMA-staged update kernel (the
+    guess from the state the update read, W written only for zones whose
+    primary solver fails, which then take the fallback pass) against the
+    update kernel followed by k_invert_primary: bit for bit over three steps
+    of fixed size, flags and failure counters included, on a torus with
+    planted failed and near-vacuum zones so that the fallback list is used."""
+    from hamr_gamma_wind_b200.api import Block
+    from tests._gpu import plant
+    pb = problems.fm_torus(24, 16, 40, rout=40.0, rho_atm=1e-8, u_atm=1e-10)
+    nfail, _ = plant(pb)
+    assert nfail > 0
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("HAMR_FUSE_INV", flag)
+        blk = Block(**pb.block_kwargs(), precision=precision, strict=True, inversion=inversion)
+        blk.set_geometry(pb.geo)
+        blk.upload(pb.p, pb.ps)
+        blk.bound()
+        dt = 0.2 * min(pb.dx)
+        for _ in range(3):   # fixed sub-steps: a failed zone without floors may stay unphysical
+            blk.advance_stage(0, 0.5 * dt, dt)
+            blk.advance_stage(1, dt, dt)
+        out[flag] = (*blk.download(), *blk.download_flags())
+        blk.close()
+    assert out["0"][3].any()   # the fallback pass had zones to count
+    for a, b in zip(out["1"], out["0"]):
+        assert np.array_equal(a, b, equal_nan=True)
