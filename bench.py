@@ -114,12 +114,14 @@ def kernel_bytes(slot: str, d: dict, width: float = 8.0) -> float:
 # zones (plus a per-column metric term under 1 %), so a launch on another block
 # moves these figures times its zones. flux1 and flux2 share the row kernel;
 # flux3 includes the centre EMFs (computed by the x3 kernel on 3-D blocks);
-# invert adds the fallback pass's 2.9 B.
+# invert adds the fallback pass's 2.9 B; update_invert is the update kernel
+# with the primary inversion inside (the default on 3-D blocks with
+# n3 >= 32 and no floors or repair).
 NCU_DRAM_BYTES_PER_ZONE = {
     "fp64": {"flux1": 219.3, "flux2": 219.3, "flux3": 296.5, "update": 457.1, "invert": 223.6,
-             "emf_edge": 123.7, "face_update": 54.7},
+             "update_invert": 509.2, "emf_edge": 123.7, "face_update": 54.7},
     "mixed": {"flux1": 134.2, "flux2": 134.2, "flux3": 136.7, "update": 315.4, "invert": 223.4,
-              "emf_edge": 58.6, "face_update": 40.6},
+              "update_invert": 388.6, "emf_edge": 58.6, "face_update": 40.6},
 }
 
 # what limits each kernel group, read from the same captures
@@ -129,6 +131,8 @@ KERNEL_LIMITER = {
     "flux3": "latency: dependent FP64/FP32 chains of the four flux evaluations per face (and the centre EMFs)",
     "update": "FP64 fixed-latency chains after TMA-staged operand loads",
     "invert": "FP64 dependent Newton iterations (FP64 pipe 45 % active)",
+    "update_invert": "FP64 fixed-latency chains of the update's sums and the Newton iterations "
+                     "(FP64 pipe 35-45 % active)",
     "emf_centre": "memory latency (long scoreboard)",
     "emf_edge": "memory latency (long scoreboard)",
     "face_update": "memory latency (long scoreboard)",
@@ -167,7 +171,7 @@ def kernel_rooflines(slots: dict, d: dict, prec: str, hbm: float) -> dict:
         gbs = 2 * kb / (ms * 1e-3) / 1e9
         out[slot] = {"ms_per_step": ms, "algorithmic_bytes": kb, "achieved_gbs": gbs, "frac": gbs / hbm,
                      "traffic": tab[key] * zones if key in tab else None,
-                     "limiter": KERNEL_LIMITER.get(slot)}
+                     "limiter": KERNEL_LIMITER.get(key)}
     return out
 
 
@@ -503,9 +507,11 @@ def run_ours(args):
                                **({"failures": v["failures"]} if "failures" in v else {})}
                            for k, v in runs.items()},
             "gpu_launches": args.steps * launches_per_step(pb, inversion_fused(slots, wl)) + 1,
-            "roofline": {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "roofline": {"bound": "hbm", "kernel": ("update+invert" if top == "update" and inversion_fused(slots, wl)
+                                                    else top),
+                         "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": kroof.get(top, {}).get("traffic"),
-                         "algorithmic_bytes": kb, "limiter": KERNEL_LIMITER.get(top),
+                         "algorithmic_bytes": kb, "limiter": kroof.get(top, {}).get("limiter"),
                          "traffic_source": "ncu DRAM bytes per zone, torus 192x96x64 capture, times zones",
                          "peak_source": peak_src},
             "kernel_rooflines": kroof,
