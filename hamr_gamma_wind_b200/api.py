@@ -305,6 +305,7 @@ class Batch:
         ms = np.zeros(n, np.float32)
         p = lambda a: a.ctypes.data_as(ctypes.c_void_p)
         self._check(self.L.hamr_batch_tuning(self.h, p(tile), p(grid), p(order), p(ms), n), "hamr_batch_tuning")
+        # tile 0: the conserved update's row kernel with bulk-copy staging
         return {ph: dict(tile=int(tile[k]), grid=int(grid[k]), order=("largest-first" if order[k] else "given"),
                          ms=float(ms[k])) for k, ph in enumerate(_lib.BATCH_PHASES)}
 

@@ -24,6 +24,7 @@ struct BEntry {
     Geom m;
     double *p, *ph, *ps, *psh, *U, *F1, *F2, *F3, *Ec, *emf, *W;
     int *pflag, *failimage;
+    int *nfail, *kerr;           // the block's failed-zone count; the batch's error word
     unsigned long long *dtbits;  // 4 per block
     double *ndt, *dt_state;      // 1 per block
     int *counter;                // 1 per block
@@ -151,6 +152,35 @@ struct OpInvert {
         return 1.e9;
     }
 };
+
+// The conserved update phase with the single-block kernel's bulk-copy
+// staging (cons_tma_row): one CTA per row piece of a block, rstart[k] the
+// first CTA of block k (every block 3-D with n3 >= 32 and aligned flux
+// planes). Same values as OpCons. (The primary inversion inside, as the
+// single-block kernel runs it, measured slower here: rows of 32-96 zones.)
+template <typename T>
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? HAMR_CONS_TMA_MINB : HAMR_CONS_TMA_MINB_F)
+    k_batch_cons_tma(const BEntry *__restrict__ E, const long *__restrict__ rstart, int n, const StageArg a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ BEntry e;
+    int lo = 0, hi = n;   // rstart[lo] <= blockIdx.x < rstart[lo + 1]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (rstart[mid] <= (long)blockIdx.x) lo = mid;
+        else hi = mid;
+    }
+    {
+        const int *src = reinterpret_cast<const int *>(&E[lo]);
+        int *dst = reinterpret_cast<int *>(&e);
+        for (int k = threadIdx.x; k < (int)(sizeof(BEntry) / 4); k += blockDim.x) dst[k] = src[k];
+    }
+    __syncthreads();
+    const int npiece = (e.d.n3 + 255) / 256, lpiece = (e.d.n3 + npiece - 1) / npiece;
+    cons_tma_row<T, 0>(e.d, e.m, e.p, a.full ? e.ph : e.p, e.U, reinterpret_cast<const T *>(e.F1),
+                       reinterpret_cast<const T *>(e.F2), reinterpret_cast<const T *>(e.F3), e.W, a.full,
+                       entry_step(e, a), e.nfail, e.kerr, npiece, lpiece, (int)(blockIdx.x - rstart[lo]), smem,
+                       nullptr, nullptr, nullptr, nullptr, nullptr);
+}
 
 struct OpBoundX1 {
     static constexpr int PH = PH_BX1, MINB = 1, SLOT = 0;
@@ -382,6 +412,14 @@ struct hamr_batch {
     cudaGraphExec_t graph = nullptr;
     int graph_steps = -1, graph_interval = -1;
     // one persistent launch per sub-step (hamr_batch_set_persistent)
+    // conserved update phase with bulk-copy staging (k_batch_cons_tma): every
+    // block allows it (cons_tma_ok) and it is in use (cons_tma: by default in
+    // the mixed step; the autotuner times it against the tiled update)
+    bool cons_tma_ok = false, cons_tma = false;
+    long *rstart = nullptr;      // device, n + 1: first CTA of each block
+    long ncons_ctas = 0;
+    int cons_block = 0;          // threads per CTA: the longest row piece, in warps
+    size_t cons_smem = 0;        // dynamic shared memory: the longest piece's layout
     bool persistent = false;
     int persist_grid = 0;        // CTAs of the cooperative launch
     unsigned *bar = nullptr;     // grid barrier: arrivals, generation
@@ -430,6 +468,8 @@ void launch_phase(hamr_batch *b, const StageArg &a) {
     k_batch<Op><<<(unsigned)g, BLK, 0, b->stream>>>(b->E, TileMap{b->dstart[ph], b->dorder[ph], b->n, b->tile[ph]}, a);
 }
 
+unsigned nblk_b(int n) { return (unsigned)((n + 127) / 128); }
+
 // launches phase `only` (or every phase when only < 0) of one sub-step
 template <typename T, int REC, int INV>
 void batch_stage_t(hamr_batch *b, int full, bool calc_dt, int only) {
@@ -443,7 +483,13 @@ void batch_stage_t(hamr_batch *b, int full, bool calc_dt, int only) {
     if (want(PH_EMFE)) launch_phase<OpEmfEdge<T>>(b, a);
     if (want(PH_POLE)) launch_phase<OpPole<T>>(b, a);
     if (want(PH_FACE)) launch_phase<OpFace<T>>(b, a);
-    if (want(PH_CONS)) launch_phase<OpCons<T>>(b, a);
+    if (want(PH_CONS)) {
+        if (b->cons_tma)
+            k_batch_cons_tma<T><<<(unsigned)b->ncons_ctas, b->cons_block, b->cons_smem, b->stream>>>(b->E, b->rstart,
+                                                                                                 b->n, a);
+        else
+            launch_phase<OpCons<T>>(b, a);
+    }
     if (want(PH_INV)) {
         switch (b->fix) {
             case FIX_FLOORS: launch_phase<OpInvert<INV, FIX_FLOORS>>(b, a); break;
@@ -478,7 +524,6 @@ void batch_stage(hamr_batch *b, int full, bool calc_dt, int only = -1) {
     else batch_stage_p<double>(b, full, calc_dt, only);
 }
 
-unsigned nblk_b(int n) { return (unsigned)((n + 127) / 128); }
 
 // one sub-step of every block in one cooperative launch (k_batch_stage)
 int batch_stage_persistent(hamr_batch *b, int full, bool calc_dt) {
@@ -526,6 +571,44 @@ int batch_step_launch(hamr_batch *b, int update, int interval) {
     return HAMR_OK;
 }
 
+// The bulk-copy update phase (k_batch_cons_tma) when every block allows it,
+// as a single block decides for itself: 3-D, n3 >= 32, flux planes 16-byte
+// aligned, the block's own switch on (HAMR_CONS_TMA). CTAs per block: its
+// row pieces; block size and shared memory: the longest piece's.
+template <typename T>
+int batch_setup_cons_tma(hamr_batch *b) {
+    b->cons_tma_ok = b->cons_tma = false;
+    std::vector<long> rs(b->n + 1, 0);
+    int block = 0;
+    int sm = 0;
+    for (int k = 0; k < b->n; k++) {
+        hamr_ctx *c = b->ctx[k];
+        const Dims &d = c->d;
+        if (!(c->cons_tma && d.d3 && d.n3 >= 32 &&
+              cons_tma_aligned<T>(c, d, reinterpret_cast<const T *>(c->F1), reinterpret_cast<const T *>(c->F2),
+                                  reinterpret_cast<const T *>(c->F3))))
+            return HAMR_OK;
+        const int npiece = (d.n3 + 255) / 256, lpiece = (d.n3 + npiece - 1) / npiece;
+        rs[k + 1] = rs[k] + (long)d.n1 * d.n2 * npiece;
+        block = std::max(block, (lpiece + 31) / 32 * 32);
+        sm = std::max(sm, cons_tma_layout<T>(lpiece).total);
+    }
+    if (rs[b->n] > 0x7fffffffL) return HAMR_OK;   // more CTAs than one launch's grid holds
+    BCK(cudaFuncSetAttribute(k_batch_cons_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    BCK(cudaMemcpyAsync(b->rstart, rs.data(), sizeof(long) * (b->n + 1), cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));   // rs goes out of scope
+    b->ncons_ctas = rs[b->n];
+    b->cons_block = block;
+    b->cons_smem = (size_t)sm;
+    b->cons_tma_ok = true;
+    // measured on the 64-torus ensemble (rows of 32-96 zones), per sub-step:
+    // float fluxes 2.37 ms against 2.69 for the tiled update; FP64 3.20
+    // against 2.59 (the FP64 staging holds 6 CTAs of at most 96 threads per SM)
+    b->cons_tma = sizeof(T) == 4;
+    if (const char *e = getenv("HAMR_BATCH_CONS_TMA")) b->cons_tma = atoi(e) != 0;   // 1: also FP64; 0: off
+    return HAMR_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -570,7 +653,9 @@ int hamr_batch_create(hamr_ctx *const *blocks, int n, void *stream, hamr_batch *
               cudaMalloc(&b->dtbits, sizeof(unsigned long long) * 4 * n) == cudaSuccess &&
               cudaMalloc(&b->dts, sizeof(double) * n) == cudaSuccess &&
               cudaMalloc(&b->ndts, sizeof(double) * n) == cudaSuccess &&
-              cudaMalloc(&b->counters, sizeof(int) * n) == cudaSuccess;
+              cudaMalloc(&b->counters, sizeof(int) * n) == cudaSuccess &&
+              cudaMalloc(&b->kerr, sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&b->rstart, sizeof(long) * (n + 1)) == cudaSuccess;
     for (int ph = 0; ph < PH_N && ok; ph++)
         ok = cudaMalloc(&b->dstart[ph], sizeof(long) * (n + 1)) == cudaSuccess &&
              cudaMalloc(&b->dorder[ph], sizeof(int) * n) == cudaSuccess;
@@ -591,6 +676,8 @@ int hamr_batch_create(hamr_ctx *const *blocks, int n, void *stream, hamr_batch *
         e.ndt = b->ndts + k;
         e.dt_state = b->dts + k;
         e.counter = b->counters + k;
+        e.nfail = c->nfail;
+        e.kerr = b->kerr;
         for (int ph = 0; ph < PH_N; ph++) b->items[ph].push_back(phase_items(ph, c->d));
     }
     int rc = HAMR_OK;
@@ -606,6 +693,9 @@ int hamr_batch_create(hamr_ctx *const *blocks, int n, void *stream, hamr_batch *
         b->order_mode[ph] = 0;
         rc = build_tiles(b, ph);
     }
+    if (rc == HAMR_OK && cudaMemsetAsync(b->kerr, 0, sizeof(int), b->stream) != cudaSuccess) rc = HAMR_E_CUDA;
+    if (rc == HAMR_OK)
+        rc = b->precision == HAMR_MIXED ? batch_setup_cons_tma<float>(b) : batch_setup_cons_tma<double>(b);
     if (rc == HAMR_OK) {
         k_batch_dt_reset<<<nblk_b(n), 128, 0, b->stream>>>(b->E, n);
         if (cudaStreamSynchronize(b->stream) != cudaSuccess) rc = HAMR_E_CUDA;
@@ -629,6 +719,7 @@ int hamr_batch_destroy(hamr_batch *b) {
     cudaFree(b->counters);
     cudaFree(b->bar);
     cudaFree(b->kerr);
+    cudaFree(b->rstart);
     for (int ph = 0; ph < PH_N; ph++) {
         cudaFree(b->dstart[ph]);
         cudaFree(b->dorder[ph]);
@@ -648,7 +739,7 @@ int hamr_batch_step(hamr_batch *b, const double *dt, double *dt_next) {
     k_batch_dt_reset<<<nblk_b(b->n), 128, 0, b->stream>>>(b->E, b->n);
     int rc = batch_step_launch(b, 0, 0);
     if (rc) return rc;
-    if (b->persistent && (rc = batch_check_kerr(b))) return rc;
+    if ((b->persistent || b->cons_tma_ok) && (rc = batch_check_kerr(b))) return rc;
     if (dt_next) {
         BCK(cudaMemcpyAsync(dt_next, b->ndts, sizeof(double) * b->n, cudaMemcpyDeviceToHost, b->stream));
         BCK(cudaStreamSynchronize(b->stream));
@@ -689,7 +780,7 @@ int hamr_batch_advance(hamr_batch *b, int nsteps, int interval, double *dt_inout
     BCK(cudaGraphLaunch(b->graph, b->stream));
     BCK(cudaMemcpyAsync(dt_inout, b->dts, sizeof(double) * b->n, cudaMemcpyDeviceToHost, b->stream));
     BCK(cudaStreamSynchronize(b->stream));
-    return b->persistent ? batch_check_kerr(b) : HAMR_OK;
+    return b->persistent || b->cons_tma_ok ? batch_check_kerr(b) : HAMR_OK;
 }
 
 // One persistent cooperative launch per sub-step instead of one launch per
@@ -756,6 +847,27 @@ int hamr_batch_autotune(hamr_batch *b, const double *dt, int reps) {
         if (work == 0) continue;
         float best = 1e30f;
         int bt = b->tile[ph], bg = b->grid[ph], bo = b->order_mode[ph];
+        // device ms of the phase's current launch form, < 0 on a CUDA error
+        auto time_phase = [&]() -> float {
+            batch_stage(b, 0, false, ph);   // warm-up
+            cudaEventRecord(e0, b->stream);
+            for (int r = 0; r < reps; r++) batch_stage(b, 0, false, ph);
+            cudaEventRecord(e1, b->stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) return -1.f;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            return ms / reps;
+        };
+        // the conserved update's bulk-copy kernel is one more candidate (its
+        // launch shape is fixed)
+        bool tma_best = false;
+        if (ph == PH_CONS && b->cons_tma_ok) {
+            b->cons_tma = true;
+            const float ms = time_phase();
+            if (ms < 0) rc = bfail(b, cudaGetLastError(), "autotune");
+            else { best = ms; tma_best = true; }
+            b->cons_tma = false;
+        }
         for (int om = 0; om < 2 && rc == HAMR_OK; om++)
             for (int tl : tiles)
                 for (int gr : grids) {
@@ -764,16 +876,11 @@ int hamr_batch_autotune(hamr_batch *b, const double *dt, int reps) {
                     b->order_mode[ph] = om;
                     if ((rc = build_tiles(b, ph))) break;
                     if (gr > 0 && gr >= b->ntiles[ph]) continue;   // same launch as one tile per CTA
-                    batch_stage(b, 0, false, ph);                   // warm-up
-                    cudaEventRecord(e0, b->stream);
-                    for (int r = 0; r < reps; r++) batch_stage(b, 0, false, ph);
-                    cudaEventRecord(e1, b->stream);
-                    if (cudaEventSynchronize(e1) != cudaSuccess) { rc = bfail(b, cudaGetLastError(), "autotune"); break; }
-                    float ms = 0.f;
-                    cudaEventElapsedTime(&ms, e0, e1);
-                    ms /= reps;
-                    if (ms < best) { best = ms; bt = tl; bg = gr; bo = om; }
+                    const float ms = time_phase();
+                    if (ms < 0) { rc = bfail(b, cudaGetLastError(), "autotune"); break; }
+                    if (ms < best) { best = ms; bt = tl; bg = gr; bo = om; tma_best = false; }
                 }
+        if (ph == PH_CONS) b->cons_tma = tma_best;
         b->tile[ph] = bt;
         b->grid[ph] = bg;
         b->order_mode[ph] = bo;
@@ -801,7 +908,7 @@ int hamr_batch_autotune(hamr_batch *b, const double *dt, int reps) {
 int hamr_batch_tuning(hamr_batch *b, int *tile, int *grid, int *order, float *ms, int nphases) {
     if (!b || nphases < PH_N) return HAMR_E_ARG;
     for (int ph = 0; ph < PH_N; ph++) {
-        if (tile) tile[ph] = b->tile[ph];
+        if (tile) tile[ph] = ph == PH_CONS && b->cons_tma ? 0 : b->tile[ph];
         if (grid) grid[ph] = b->grid[ph];
         if (order) order[ph] = b->order_mode[ph];
         if (ms) ms[ph] = b->tuned_ms[ph];

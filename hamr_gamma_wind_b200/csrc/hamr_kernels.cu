@@ -1489,29 +1489,31 @@ __host__ __device__ __forceinline__ ConsTmaLayout cons_tma_layout(int lpiece) {
 #ifndef HAMR_CONS_INV_TMA_MINB_F
 #define HAMR_CONS_INV_TMA_MINB_F HAMR_CONS_TMA_MINB_F
 #endif
-template <typename T, int FUSE = 0>
-__global__ void __launch_bounds__(256, sizeof(T) == 8 ? (FUSE ? HAMR_CONS_INV_TMA_MINB : HAMR_CONS_TMA_MINB)
-                                                       : (FUSE ? HAMR_CONS_INV_TMA_MINB_F : HAMR_CONS_TMA_MINB_F))
-    k_cons_tma(const Dims d, const Geom m, const double *__restrict__ pin, const double *__restrict__ pb,
-               double *__restrict__ Ucache, const T *__restrict__ F1, const T *__restrict__ F2,
-               const T *__restrict__ F3, double *__restrict__ W, int full, StepSize st, int *__restrict__ nfail,
-               int *__restrict__ kerr, int npiece, int lpiece, const double *__restrict__ psf = nullptr,
-               double *__restrict__ pout = nullptr, int *__restrict__ pflag = nullptr,
-               int *__restrict__ failimage = nullptr, int *__restrict__ flist = nullptr) {
-    extern __shared__ __align__(16) unsigned char smem[];
+// The body of one CTA: row piece `blk` (row * npiece + piece) of the block,
+// `smem` the CTA's dynamic shared memory (cons_tma_layout(lpiece).total bytes).
+template <typename T, int FUSE>
+__device__ __forceinline__ void cons_tma_row(const Dims &d, const Geom &m, const double *__restrict__ pin,
+                                             const double *__restrict__ pb, double *__restrict__ Ucache,
+                                             const T *__restrict__ F1, const T *__restrict__ F2,
+                                             const T *__restrict__ F3, double *__restrict__ W, int full,
+                                             const StepSize &st, int *__restrict__ nfail, int *__restrict__ kerr,
+                                             int npiece, int lpiece, int blk, unsigned char *smem,
+                                             const double *__restrict__ psf, double *__restrict__ pout,
+                                             int *__restrict__ pflag, int *__restrict__ failimage,
+                                             int *__restrict__ flist) {
     constexpr int A = 16 / (int)sizeof(T);
     const ConsTmaLayout lay = cons_tma_layout<T>(lpiece);
     unsigned long long *bar = reinterpret_cast<unsigned long long *>(smem);
     double *sg = reinterpret_cast<double *>(smem + 16);
     T *sf = reinterpret_cast<T *>(smem + lay.f_off);   // [kind][plane][cap]
     const unsigned bar_a = smem_addr(bar);
-    const int row = blockIdx.x / npiece, piece = blockIdx.x % npiece;
+    const int row = blk / npiece, piece = blk % npiece;
     const int i = d.ng1 + row / d.n2, j = d.ng2 + row % d.n2;
     const int za = d.ng3 + piece * lpiece;
     const int L = min(lpiece, d.n3 - piece * lpiece);
     const long ks = d.ks, isize = (long)d.G2 * d.G3;
     const long c0 = cix(d, i, j, za), gi = gix(d, i, j);
-    if (!FUSE && blockIdx.x == 0 && threadIdx.x == 0) *nfail = 0;   // the inversion's failed-zone list starts empty
+    if (!FUSE && blk == 0 && threadIdx.x == 0) *nfail = 0;   // the inversion's failed-zone list starts empty
     // the five segment kinds: start cell, length, source array
     auto seg_start = [&](int q) -> long { return q == 1 ? c0 + isize : (q == 3 ? c0 + d.G3 : c0); };
     auto seg_len = [&](int q) -> int { return q == 4 ? L + 1 : L; };
@@ -1603,6 +1605,20 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? (FUSE ? HAMR_CONS_INV_TM
     }
 }
 
+template <typename T, int FUSE = 0>
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? (FUSE ? HAMR_CONS_INV_TMA_MINB : HAMR_CONS_TMA_MINB)
+                                                       : (FUSE ? HAMR_CONS_INV_TMA_MINB_F : HAMR_CONS_TMA_MINB_F))
+    k_cons_tma(const Dims d, const Geom m, const double *__restrict__ pin, const double *__restrict__ pb,
+               double *__restrict__ Ucache, const T *__restrict__ F1, const T *__restrict__ F2,
+               const T *__restrict__ F3, double *__restrict__ W, int full, StepSize st, int *__restrict__ nfail,
+               int *__restrict__ kerr, int npiece, int lpiece, const double *__restrict__ psf = nullptr,
+               double *__restrict__ pout = nullptr, int *__restrict__ pflag = nullptr,
+               int *__restrict__ failimage = nullptr, int *__restrict__ flist = nullptr) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    cons_tma_row<T, FUSE>(d, m, pin, pb, Ucache, F1, F2, F3, W, full, st, nfail, kerr, npiece, lpiece, blockIdx.x,
+                          smem, psf, pout, pflag, failimage, flist);
+}
+
 template <int INV, int FIX = 0>
 __device__ __forceinline__ void k_invert_at(const Dims &d, const Geom &m, const double *__restrict__ pg,
                                                  const double *__restrict__ W, const double *__restrict__ psf,
@@ -1651,29 +1667,36 @@ __global__ void __launch_bounds__(BLK, HAMR_UPD_MINB)
     invert_epilogue<FIX>(d, gm, c, flag, pf, pout, pflag, failimage);
 }
 
+// the fallback chain and epilogue of one listed zone (active-zone index t)
+template <int FIX>
+__device__ __forceinline__ void invert_fallback_at(const Dims &d, const Geom &m, const double *__restrict__ pg,
+                                                   const double *__restrict__ W, const double *__restrict__ psf,
+                                                   double *__restrict__ pout, int *__restrict__ pflag,
+                                                   int *__restrict__ failimage, const long t) {
+    const int z = d.ng3 + (int)(t % d.n3);
+    const int j = d.ng2 + (int)((t / d.n3) % d.n2);
+    const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
+    const long c = cix(d, i, j, z), gi = gix(d, i, j);
+    Geo<double> gm;
+    load_geo(d, m, i, j, CENT, gm);
+    double pf[NPR], U[NPR];
+    invert_inputs(d, m, pg, W, psf, i, j, c, gi, pf, U);
+    if (!(U[RHO] <= 0.)) {
+#pragma unroll
+        for (int k = B1; k <= B3; k++) pf[k] = U[k] / gm.g;   // the primary solver's prologue
+    }
+    const int flag = invert_fallbacks(d, gm, c, U, pf, failimage);
+    invert_epilogue<FIX>(d, gm, c, flag, pf, pout, pflag, failimage);
+}
+
 template <int INV, int FIX = 0>
 __global__ void __launch_bounds__(BLK)
     k_invert_fallback(const Dims d, const Geom m, const double *__restrict__ pg, const double *__restrict__ W,
                       const double *__restrict__ psf, double *__restrict__ pout, int *__restrict__ pflag,
                       int *__restrict__ failimage, const int *__restrict__ flist, const int *__restrict__ nfail) {
     const int n = *nfail;
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        const long t = flist[q];
-        const int z = d.ng3 + (int)(t % d.n3);
-        const int j = d.ng2 + (int)((t / d.n3) % d.n2);
-        const int i = d.ng1 + (int)(t / ((long)d.n3 * d.n2));
-        const long c = cix(d, i, j, z), gi = gix(d, i, j);
-        Geo<double> gm;
-        load_geo(d, m, i, j, CENT, gm);
-        double pf[NPR], U[NPR];
-        invert_inputs(d, m, pg, W, psf, i, j, c, gi, pf, U);
-        if (!(U[RHO] <= 0.)) {
-#pragma unroll
-            for (int k = B1; k <= B3; k++) pf[k] = U[k] / gm.g;   // the primary solver's prologue
-        }
-        const int flag = invert_fallbacks(d, gm, c, U, pf, failimage);
-        invert_epilogue<FIX>(d, gm, c, flag, pf, pout, pflag, failimage);
-    }
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+        invert_fallback_at<FIX>(d, m, pg, W, psf, pout, pflag, failimage, flist[q]);
 }
 
 // ------------------------------------------------ neighbour repair (opt-in)

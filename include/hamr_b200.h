@@ -317,7 +317,10 @@ int hamr_batch_set_persistent(hamr_batch *b, int on);
 /* The launch shape chosen for each of the HAMR_BATCH_PHASES phases (order:
  * flux x3, x2, x1, polar flux fix, centre EMF, edge EMF, polar EMF average,
  * face update, conserved update, inversion, ghost fill x1, x3, x2) and its
- * tuned time in ms. Any output pointer may be NULL. */
+ * tuned time in ms. tile 0 for the conserved update: one CTA per row of a
+ * block with its fluxes staged by bulk copies (every block 3-D with n3 >= 32;
+ * the default with float fluxes, and an autotuner candidate). Any output
+ * pointer may be NULL. */
 int hamr_batch_tuning(hamr_batch *b, int *tile, int *grid, int *order, float *ms, int nphases);
 
 /* ---- adjoint ---------------------------------------------------------------

@@ -65,6 +65,80 @@ def test_batch_step_matches_single_blocks_bitwise(precision):
     _close(solo + mem)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_bulk_copy_update_matches_single_blocks_bitwise(precision, monkeypatch):
+    """Members 3-D with 32 or more zones along x3: the batch's conserved update
+    runs the single-block row kernel with its fluxes staged by bulk copies,
+    one CTA per row of each member (forced for FP64, where the tiled update
+    is the default), and must match the members stepped alone bit for bit,
+    before and after the autotuner has timed it against the tiled update."""
+    monkeypatch.setenv("HAMR_BATCH_CONS_TMA", "1")
+    pbs, _ = problems.torus_ensemble(3, 32, 40, seed=11)
+    assert all(pb.n3 >= 32 for pb in pbs)
+
+    def blocks():
+        out = []
+        for pb in pbs:
+            b = Block(**pb.block_kwargs(), precision=precision, strict=True)
+            b.set_geometry(pb.geo)
+            b.upload(pb.p, pb.ps)
+            b.bound()
+            out.append(b)
+        return out
+
+    solo, mem = blocks(), blocks()
+    batch = Batch(mem)
+    assert batch.tuning()["update"]["tile"] == 0   # the row kernel is in use
+    dts = np.array([0.2 * min(pb.dx[:2]) for pb in pbs])
+    for s in range(4):
+        if s == 2:
+            batch.autotune(dts, reps=1)
+        dn_solo = np.array([b.step(dt) for b, dt in zip(solo, dts)])
+        np.testing.assert_array_equal(dn_solo, batch.step(dts))
+        dts = np.minimum(dn_solo, 1.3 * dts)
+    for a, b in zip(solo, mem):
+        for x, y in zip(a.download(), b.download()):
+            np.testing.assert_array_equal(x, y)
+    batch.close()
+    _close(solo + mem)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_bulk_copy_update_with_failed_zones_bitwise(precision, monkeypatch):
+    """The same members with planted failed and near-vacuum zones and no
+    floors: the batch's bulk-copy update and one-pass inversion phase against
+    the members stepped alone (whose update runs the primary inversion
+    inside and leaves the failed zones to the fallback pass over a list);
+    one step, flags and failure counters included."""
+    monkeypatch.setenv("HAMR_BATCH_CONS_TMA", "1")
+    pbs, _ = problems.torus_ensemble(3, 32, 40, seed=11, rho_atm=1e-8, u_atm=1e-10)
+    for k, pb in enumerate(pbs):
+        nfail, _ = plant(pb, seed=200 + k)
+        assert nfail > 0
+
+    def blocks():
+        out = []
+        for pb in pbs:
+            b = Block(**pb.block_kwargs(), precision=precision, strict=True)
+            b.set_geometry(pb.geo)
+            b.upload(pb.p, pb.ps)
+            b.bound()
+            out.append(b)
+        return out
+
+    solo, mem = blocks(), blocks()
+    batch = Batch(mem)
+    dts = np.array([0.2 * min(pb.dx[:2]) for pb in pbs])
+    dn_solo = np.array([b.step(dt) for b, dt in zip(solo, dts)])
+    np.testing.assert_array_equal(dn_solo, batch.step(dts))
+    for a, b in zip(solo, mem):
+        for x, y in zip((*a.download(), *a.download_flags()), (*b.download(), *b.download_flags())):
+            assert np.array_equal(x, y, equal_nan=True)
+        assert a.download_flags()[1].any()   # the fallback pass had zones to count
+    batch.close()
+    _close(solo + mem)
+
+
 def test_batch_production_build_close_to_single_blocks():
     pbs, solo = _members(strict=False)
     _, mem = _members(strict=False)
