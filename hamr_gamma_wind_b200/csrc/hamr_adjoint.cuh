@@ -1278,7 +1278,7 @@ int bound_ctx(hamr_ctx *ctx) {
     cudaStream_t s = ctx->stream;
     const Geom m = geom_of(ctx);
     if (d.d1) k_bound_x1<<<nblk((long)d.ng1 * d.G2 * d.G3), BLK, 0, s>>>(d, m, ctx->p, ctx->ps);
-    if (d.d3) k_bound_x3<<<nblk((long)d.ng3 * d.G1 * d.G2), BLK, 0, s>>>(d, ctx->p, ctx->ps);
+    if (d.d3) k_bound_x3<<<nblk(n_bound_x3(d)), BLK, 0, s>>>(d, ctx->p, ctx->ps);
     if (d.d2) k_bound_x2<<<nblk(n_bound_x2(d)), BLK, 0, s>>>(d, ctx->p, ctx->ps);
     return cudaGetLastError() == cudaSuccess ? HAMR_OK : HAMR_E_CUDA;
 }

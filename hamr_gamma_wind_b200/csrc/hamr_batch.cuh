@@ -57,7 +57,7 @@ __host__ __device__ inline long phase_items(int ph, const Dims &d) {
     case PH_CONS:
     case PH_INV: return (long)d.n1 * d.n2 * d.n3;
     case PH_BX1: return d.d1 ? (long)d.ng1 * d.G2 * d.G3 : 0;
-    case PH_BX3: return d.d3 ? (long)d.ng3 * d.G1 * d.G2 : 0;
+    case PH_BX3: return d.d3 ? n_bound_x3(d) : 0;
     case PH_BX2: return d.d2 ? n_bound_x2(d) : 0;
     }
     return 0;

@@ -775,12 +775,37 @@ __device__ __forceinline__ void k_pole_average_at(const Dims &d, T *emf, StepSiz
     }
 }
 
+// The same average with one warp per (pole, i) row: the lanes load 32
+// consecutive phi values at a time and lane 0 adds them in order (shuffled
+// to it one by one), so the sum is the row-by-row one above, bit for bit;
+// the row is written back by all lanes.
 template <typename T>
 __global__ void k_pole_average(const Dims d, T *emf, StepSize st) {
     const int ni = d.n1 + d.ng1;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 2 * ni) return;
-    k_pole_average_at(d, emf, st, t);
+    const int t = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (t >= 2 * ni) return;   // whole warps leave together (t is per warp)
+    const int side = t / ni, i = d.ng1 + t % ni;
+    if ((side == 0 && !d.pole1) || (side == 1 && !d.pole2)) return;
+    const int jp = side == 0 ? d.ng2 : d.n2 + d.ng2;
+    const double dt = st.full();
+    const T *row = emf + 1 * d.ks + cix(d, i, jp, 0);
+    double avg = 0.;
+    for (int z0 = d.ng3; z0 < d.n3 + d.ng3; z0 += 32) {
+        const int z = z0 + lane;
+        const double x = z < d.n3 + d.ng3 ? (double)row[z] : 0.;
+        const int m = min(32, d.n3 + d.ng3 - z0);
+        for (int k = 0; k < m; k++) {
+            const double xk = __shfl_sync(0xffffffffu, x, k);
+            if (lane == 0) avg += dt * xk;
+        }
+    }
+    avg = __shfl_sync(0xffffffffu, avg, 0);
+    avg /= (double)(d.n3);
+    const double avg_new = avg / ((double)1);
+    for (int z = d.ng3 + lane; z < d.n3 + 2 * d.ng3; z += 32) {
+        emf[1 * d.ks + cix(d, i, jp, z)] = (T)(avg_new / dt);
+        emf[3 * d.ks + cix(d, i, jp, z)] = T(0.);
+    }
 }
 
 // staggered field update from the edge EMFs (consttransport3,
@@ -1907,22 +1932,26 @@ __global__ void k_bound_x1(const Dims d, const Geom m, double *pv, double *ps) {
     k_bound_x1_at(d, m, pv, ps, t);
 }
 
-// x3 ghosts (periodic) over every (i, j)
+// x3 ghosts (periodic) over every (i, j): one item per (component, i, j,
+// ghost layer), the components being the NPR primitives and then the 3
+// face-field planes, so that each thread copies one value to each end of a
+// row (one item per (i, j, layer) copying all 12 left the launch at a fifth
+// of a wave, bound by the latency of its 24 dependent copies)
+constexpr int X3_COMPS = NPR + 3;
+__host__ __device__ __forceinline__ long n_bound_x3(const Dims &d) { return (long)X3_COMPS * d.ng3 * d.G1 * d.G2; }
+
 __device__ __forceinline__ void k_bound_x3_at(const Dims &d, double *pv, double *ps, const long t) {
-    const int g = (int)(t % d.ng3), j = (int)((t / d.ng3) % d.G2), i = (int)(t / ((long)d.ng3 * d.G2));
-    const long lo = cix(d, i, j, g), lo_src = cix(d, i, j, g + d.n3);
-    const long hi = cix(d, i, j, d.n3 + d.ng3 + g), hi_src = cix(d, i, j, d.ng3 + g);
-    copy_cell(d, pv, lo, lo_src);
-    copy_cell(d, pv, hi, hi_src);
-    for (int k = 0; k < 3; k++) {
-        ps[k * d.ks + lo] = ps[k * d.ks + lo_src];
-        ps[k * d.ks + hi] = ps[k * d.ks + hi_src];
-    }
+    const int g = (int)(t % d.ng3);
+    const long r = t / d.ng3;
+    const int j = (int)(r % d.G2), i = (int)((r / d.G2) % d.G1), comp = (int)(r / ((long)d.G2 * d.G1));
+    double *a = comp < NPR ? pv + (long)comp * d.ks : ps + (long)(comp - NPR) * d.ks;
+    a[cix(d, i, j, g)] = a[cix(d, i, j, g + d.n3)];
+    a[cix(d, i, j, d.n3 + d.ng3 + g)] = a[cix(d, i, j, d.ng3 + g)];
 }
 
 __global__ void k_bound_x3(const Dims d, double *pv, double *ps) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)d.ng3 * d.G1 * d.G2) return;
+    if (t >= n_bound_x3(d)) return;
     k_bound_x3_at(d, pv, ps, t);
 }
 
@@ -2207,7 +2236,7 @@ int launch_bound_dim(hamr_ctx *ctx, int full, int dim) {
     double *psw = full ? ctx->ps : ctx->psh;
     if ((dim == 0 || dim == 1) && d.d1)
         k_bound_x1<<<nblk((long)d.ng1 * d.G2 * d.G3), BLK, 0, s>>>(d, geom_of(ctx), pw, psw);
-    if ((dim == 0 || dim == 3) && d.d3) k_bound_x3<<<nblk((long)d.ng3 * d.G1 * d.G2), BLK, 0, s>>>(d, pw, psw);
+    if ((dim == 0 || dim == 3) && d.d3) k_bound_x3<<<nblk(n_bound_x3(d)), BLK, 0, s>>>(d, pw, psw);
     if ((dim == 0 || dim == 2) && d.d2) k_bound_x2<<<nblk(n_bound_x2(d)), BLK, 0, s>>>(d, pw, psw);
     CK(cudaGetLastError());
     return HAMR_OK;
@@ -2338,7 +2367,7 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
         k_ct_fused<T><<<grid, CT_THREADS, 0, s>>>(d, m, pin, F1, F2, F3, ctx->ps, full ? ctx->ps : ctx->psh, emf, st);
         prof_mark(pf, PROF_EMF_EDGE, s);
         if (d.bc2 == HAMR_BC_POLE_TRANS) {
-            k_pole_average<T><<<nblk(2L * (d.n1 + d.ng1)), BLK, 0, s>>>(d, emf, st);
+            k_pole_average<T><<<nblk(64L * (d.n1 + d.ng1)), BLK, 0, s>>>(d, emf, st);   // a warp per row
             prof_mark(pf, PROF_POLE_AVG, s);
             k_face_update_polar<T><<<nblk(3L * (d.n1 + 1) * (d.n3 + 1)), BLK, 0, s>>>(
                 d, m, ctx->ps, full ? ctx->ps : ctx->psh, emf, st);
@@ -2357,7 +2386,7 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
         k_emf_edge<T><<<nblk(n), BLK, 0, s2>>>(d, Ec, F1, F2, F3, emf);
         prof_mark(pf, PROF_EMF_EDGE, s);
         if (d.bc2 == HAMR_BC_POLE_TRANS)
-            k_pole_average<T><<<nblk(2L * (d.n1 + d.ng1)), BLK, 0, s2>>>(d, emf, st);
+            k_pole_average<T><<<nblk(64L * (d.n1 + d.ng1)), BLK, 0, s2>>>(d, emf, st);   // a warp per row
         prof_mark(pf, PROF_POLE_AVG, s);
         k_face_update<T><<<nblk(n), BLK, 0, s2>>>(d, m, ctx->ps, full ? ctx->ps : ctx->psh, emf, st);
         prof_mark(pf, PROF_FACE, s);
