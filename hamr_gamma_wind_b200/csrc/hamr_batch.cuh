@@ -182,6 +182,33 @@ __global__ void __launch_bounds__(256, sizeof(T) == 8 ? HAMR_CONS_TMA_MINB : HAM
                        nullptr, nullptr, nullptr, nullptr, nullptr);
 }
 
+// The x3 fluxes of the batch by zone slots, with the centre EMFs: the
+// single-block slot kernel's body (flux_x3_slots), each zone reconstructed
+// once. The blocks' CTA ranges are concatenated, xstart[k] the first CTA of
+// block k (every block 3-D). Same values as OpFlux<3> and OpEmfCentre.
+template <typename T, int REC>
+__global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? ((REC & 2) != 0 ? HAMR_FLUX_FT_X3_MINB : HAMR_FLUX_X3_MINB)
+                                                         : ((REC & 2) != 0 ? HAMR_FLUX_FT_X3_MINB_F : HAMR_FLUX_X3_MINB_F))
+    k_batch_flux_x3(const BEntry *__restrict__ E, const long *__restrict__ xstart, int n, const StageArg a) {
+    __shared__ BEntry e;
+    int lo = 0, hi = n;   // xstart[lo] <= blockIdx.x < xstart[lo + 1]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (xstart[mid] <= (long)blockIdx.x) lo = mid;
+        else hi = mid;
+    }
+    {
+        const int *src = reinterpret_cast<const int *>(&E[lo]);
+        int *dst = reinterpret_cast<int *>(&e);
+        for (int k = threadIdx.x; k < (int)(sizeof(BEntry) / 4); k += BLK) dst[k] = src[k];
+    }
+    __syncthreads();
+    const double cmx = flux_x3_slots<T, REC>(e.d, e.m, a.full ? e.ph : e.p, a.full ? e.psh : e.ps,
+                                             reinterpret_cast<T *>(e.F3), reinterpret_cast<T *>(e.Ec),
+                                             (long)blockIdx.x - xstart[lo]);
+    if (a.calc_dt) cta_max_ctop(e.d, 3, cmx, &e.dtbits[3]);
+}
+
 struct OpBoundX1 {
     static constexpr int PH = PH_BX1, MINB = 1, SLOT = 0;
     static constexpr bool REDUCE = false;
@@ -416,6 +443,11 @@ struct hamr_batch {
     // block allows it (cons_tma_ok) and it is in use (cons_tma: by default in
     // the mixed step; the autotuner times it against the tiled update)
     bool cons_tma_ok = false, cons_tma = false;
+    // x3 fluxes and centre EMFs by zone slots (k_batch_flux_x3): every block
+    // 3-D; off with HAMR_BATCH_FLUX_X3=0
+    bool flux3_slots = false;
+    long *xstart = nullptr;      // device, n + 1: first CTA of each block
+    long nx3_ctas = 0;
     long *rstart = nullptr;      // device, n + 1: first CTA of each block
     long ncons_ctas = 0;
     int cons_block = 0;          // threads per CTA: the longest row piece, in warps
@@ -475,11 +507,16 @@ template <typename T, int REC, int INV>
 void batch_stage_t(hamr_batch *b, int full, bool calc_dt, int only) {
     const StageArg a{full, calc_dt ? 1 : 0, full ? 1.0 : 0.5};
     auto want = [&](int ph) { return only < 0 || only == ph; };
-    if (want(PH_FLUX3)) launch_phase<OpFlux<3, T, REC>>(b, a);
+    if (want(PH_FLUX3)) {
+        if (b->flux3_slots)
+            k_batch_flux_x3<T, REC><<<(unsigned)b->nx3_ctas, BLK, 0, b->stream>>>(b->E, b->xstart, b->n, a);
+        else
+            launch_phase<OpFlux<3, T, REC>>(b, a);
+    }
     if (want(PH_FLUX2)) launch_phase<OpFlux<2, T, REC>>(b, a);
     if (want(PH_FLUX1)) launch_phase<OpFlux<1, T, REC>>(b, a);
     if (want(PH_FIXFLUX)) launch_phase<OpFixFlux<T>>(b, a);
-    if (want(PH_EMFC)) launch_phase<OpEmfCentre<T>>(b, a);
+    if (want(PH_EMFC) && !b->flux3_slots) launch_phase<OpEmfCentre<T>>(b, a);   // else done by the x3 slots
     if (want(PH_EMFE)) launch_phase<OpEmfEdge<T>>(b, a);
     if (want(PH_POLE)) launch_phase<OpPole<T>>(b, a);
     if (want(PH_FACE)) launch_phase<OpFace<T>>(b, a);
@@ -571,6 +608,26 @@ int batch_step_launch(hamr_batch *b, int update, int interval) {
     return HAMR_OK;
 }
 
+// The x3 slot kernel (k_batch_flux_x3) when every block is 3-D: CTAs per
+// block as the single-block launch.
+int batch_setup_flux3_slots(hamr_batch *b) {
+    b->flux3_slots = false;
+    if (const char *e = getenv("HAMR_BATCH_FLUX_X3"))
+        if (atoi(e) == 0) return HAMR_OK;
+    std::vector<long> xs(b->n + 1, 0);
+    for (int k = 0; k < b->n; k++) {
+        const Dims &d = b->ctx[k]->d;
+        if (!d.d3) return HAMR_OK;
+        xs[k + 1] = xs[k] + n_x3_slot_ctas(d);
+    }
+    if (xs[b->n] > 0x7fffffffL) return HAMR_OK;
+    BCK(cudaMemcpyAsync(b->xstart, xs.data(), sizeof(long) * (b->n + 1), cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));   // xs goes out of scope
+    b->nx3_ctas = xs[b->n];
+    b->flux3_slots = true;
+    return HAMR_OK;
+}
+
 // The bulk-copy update phase (k_batch_cons_tma) when every block allows it,
 // as a single block decides for itself: 3-D, n3 >= 32, flux planes 16-byte
 // aligned, the block's own switch on (HAMR_CONS_TMA). CTAs per block: its
@@ -655,7 +712,8 @@ int hamr_batch_create(hamr_ctx *const *blocks, int n, void *stream, hamr_batch *
               cudaMalloc(&b->ndts, sizeof(double) * n) == cudaSuccess &&
               cudaMalloc(&b->counters, sizeof(int) * n) == cudaSuccess &&
               cudaMalloc(&b->kerr, sizeof(int)) == cudaSuccess &&
-              cudaMalloc(&b->rstart, sizeof(long) * (n + 1)) == cudaSuccess;
+              cudaMalloc(&b->rstart, sizeof(long) * (n + 1)) == cudaSuccess &&
+              cudaMalloc(&b->xstart, sizeof(long) * (n + 1)) == cudaSuccess;
     for (int ph = 0; ph < PH_N && ok; ph++)
         ok = cudaMalloc(&b->dstart[ph], sizeof(long) * (n + 1)) == cudaSuccess &&
              cudaMalloc(&b->dorder[ph], sizeof(int) * n) == cudaSuccess;
@@ -696,6 +754,7 @@ int hamr_batch_create(hamr_ctx *const *blocks, int n, void *stream, hamr_batch *
     if (rc == HAMR_OK && cudaMemsetAsync(b->kerr, 0, sizeof(int), b->stream) != cudaSuccess) rc = HAMR_E_CUDA;
     if (rc == HAMR_OK)
         rc = b->precision == HAMR_MIXED ? batch_setup_cons_tma<float>(b) : batch_setup_cons_tma<double>(b);
+    if (rc == HAMR_OK) rc = batch_setup_flux3_slots(b);
     if (rc == HAMR_OK) {
         k_batch_dt_reset<<<nblk_b(n), 128, 0, b->stream>>>(b->E, n);
         if (cudaStreamSynchronize(b->stream) != cudaSuccess) rc = HAMR_E_CUDA;
@@ -720,6 +779,7 @@ int hamr_batch_destroy(hamr_batch *b) {
     cudaFree(b->bar);
     cudaFree(b->kerr);
     cudaFree(b->rstart);
+    cudaFree(b->xstart);
     for (int ph = 0; ph < PH_N; ph++) {
         cudaFree(b->dstart[ph]);
         cudaFree(b->dorder[ph]);
@@ -844,7 +904,10 @@ int hamr_batch_autotune(hamr_batch *b, const double *dt, int reps) {
     for (int ph = 0; ph < PH_N && rc == HAMR_OK; ph++) {
         long work = 0;
         for (long x : b->items[ph]) work += x;
-        if (work == 0) continue;
+        if (work == 0 || (ph == PH_EMFC && b->flux3_slots)) continue;   // nothing launched
+        // the x3 slot kernel has one launch shape: timed once
+        const bool fixed = ph == PH_FLUX3 && b->flux3_slots;
+        bool timed = false;
         float best = 1e30f;
         int bt = b->tile[ph], bg = b->grid[ph], bo = b->order_mode[ph];
         // device ms of the phase's current launch form, < 0 on a CUDA error
@@ -876,6 +939,8 @@ int hamr_batch_autotune(hamr_batch *b, const double *dt, int reps) {
                     b->order_mode[ph] = om;
                     if ((rc = build_tiles(b, ph))) break;
                     if (gr > 0 && gr >= b->ntiles[ph]) continue;   // same launch as one tile per CTA
+                    if (fixed && timed) continue;
+                    timed = true;
                     const float ms = time_phase();
                     if (ms < 0) { rc = bfail(b, cudaGetLastError(), "autotune"); break; }
                     if (ms < best) { best = ms; bt = tl; bg = gr; bo = om; tma_best = false; }
@@ -908,7 +973,9 @@ int hamr_batch_autotune(hamr_batch *b, const double *dt, int reps) {
 int hamr_batch_tuning(hamr_batch *b, int *tile, int *grid, int *order, float *ms, int nphases) {
     if (!b || nphases < PH_N) return HAMR_E_ARG;
     for (int ph = 0; ph < PH_N; ph++) {
-        if (tile) tile[ph] = ph == PH_CONS && b->cons_tma ? 0 : b->tile[ph];
+        if (tile)
+            tile[ph] = (ph == PH_CONS && b->cons_tma) || ((ph == PH_FLUX3 || ph == PH_EMFC) && b->flux3_slots)
+                           ? 0 : b->tile[ph];
         if (grid) grid[ph] = b->grid[ph];
         if (order) order[ph] = b->order_mode[ph];
         if (ms) ms[ph] = b->tuned_ms[ph];

@@ -377,17 +377,18 @@ __device__ __forceinline__ void emf_centre_eval(const Dims &d, const Geom &m, co
 // work): its slots are exactly k_emf_centre's zones, and the slot's
 // primitives are already in L1 from its reconstruction stencil. A slot that
 // two CTAs share is done by the first. Same values as k_emf_centre.
+// The body of CTA `blk` of the block's slot range; returns the thread's
+// face signal speed (0 without a face) for the CTA's CFL reduction.
 template <typename T, int REC>
-__global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? ((REC & 2) != 0 ? HAMR_FLUX_FT_X3_MINB : HAMR_FLUX_X3_MINB)
-                                                         : ((REC & 2) != 0 ? HAMR_FLUX_FT_X3_MINB_F : HAMR_FLUX_X3_MINB_F))
-    k_flux_x3(const Dims d, const Geom m, const double *__restrict__ pv, const double *__restrict__ ps,
-              T *__restrict__ F, unsigned long long *__restrict__ dtbits, int calc_dt, T *__restrict__ Ec) {
+__device__ __forceinline__ double flux_x3_slots(const Dims &d, const Geom &m, const double *__restrict__ pv,
+                                                const double *__restrict__ ps, T *__restrict__ F,
+                                                T *__restrict__ Ec, long blk) {
     __shared__ T slo[NPR - 1][BLK], shi[NPR - 1][BLK];   // zone edges per slot (B3 skipped)
     const int l = threadIdx.x;
     const long nslot = n_x3_slots(d);
     const int rz = d.n3 + 2 * d.d3;   // slots per row
     const int nj = d.n2 + 2 * d.d2;
-    const long sl = (long)blockIdx.x * (BLK - 1) + l;
+    const long sl = blk * (BLK - 1) + l;
     const int zl = (int)(sl % rz);
     const long row = sl / rz;
     const int j = (d.ng2 - 1) * d.d2 + (int)(row % nj);
@@ -425,6 +426,20 @@ __global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? ((REC & 2) != 0 ? HAMR_F
         load_geo_t(d, m, i, j, FACE3, gm);
         cmx = flux_eval<3, T, REC>(d, gm, ps, pl, pr, F, c + 1, j);
     }
+    return cmx;
+}
+
+// CTAs of the slot range: CTA b takes slots b (BLK - 1) .. b (BLK - 1) + BLK - 1
+__host__ __device__ __forceinline__ long n_x3_slot_ctas(const Dims &d) {
+    return (n_x3_slots(d) - 1 + BLK - 2) / (BLK - 1);
+}
+
+template <typename T, int REC>
+__global__ void __launch_bounds__(BLK, sizeof(T) == 8 ? ((REC & 2) != 0 ? HAMR_FLUX_FT_X3_MINB : HAMR_FLUX_X3_MINB)
+                                                         : ((REC & 2) != 0 ? HAMR_FLUX_FT_X3_MINB_F : HAMR_FLUX_X3_MINB_F))
+    k_flux_x3(const Dims d, const Geom m, const double *__restrict__ pv, const double *__restrict__ ps,
+              T *__restrict__ F, unsigned long long *__restrict__ dtbits, int calc_dt, T *__restrict__ Ec) {
+    const double cmx = flux_x3_slots<T, REC>(d, m, pv, ps, F, Ec, blockIdx.x);
     if (calc_dt) cta_max_ctop(d, 3, cmx, &dtbits[3]);
 }
 
@@ -2256,7 +2271,7 @@ void launch_flux(long n, cudaStream_t s, const Dims &d, const Geom &m, const dou
     // still fill the device several times over; small blocks (2-D, ensemble
     // members) keep one thread per face
     if (DIR == 3) {   // each zone reconstructed once, edges through shared memory
-        const long nb = (n_x3_slots(d) - 1 + BLK - 2) / (BLK - 1);
+        const long nb = n_x3_slot_ctas(d);
         switch (rec_key(d)) {
         case 1: k_flux_x3<T, 1><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd, Ec); break;
         case 2: k_flux_x3<T, 2><<<nb, BLK, 0, s>>>(d, m, pin, psin, F, dtbits, cd, Ec); break;

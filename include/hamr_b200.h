@@ -319,8 +319,9 @@ int hamr_batch_set_persistent(hamr_batch *b, int on);
  * face update, conserved update, inversion, ghost fill x1, x3, x2) and its
  * tuned time in ms. tile 0 for the conserved update: one CTA per row of a
  * block with its fluxes staged by bulk copies (every block 3-D with n3 >= 32;
- * the default with float fluxes, and an autotuner candidate). Any output
- * pointer may be NULL. */
+ * the default with float fluxes, and an autotuner candidate); tile 0 for the
+ * x3 fluxes and the centre EMFs: the zone-slot kernel, which computes both
+ * (every block 3-D). Any output pointer may be NULL. */
 int hamr_batch_tuning(hamr_batch *b, int *tile, int *grid, int *order, float *ms, int nphases);
 
 /* ---- adjoint ---------------------------------------------------------------

@@ -70,8 +70,9 @@ def test_batch_bulk_copy_update_matches_single_blocks_bitwise(precision, monkeyp
     """Members 3-D with 32 or more zones along x3: the batch's conserved update
     runs the single-block row kernel with its fluxes staged by bulk copies,
     one CTA per row of each member (forced for FP64, where the tiled update
-    is the default), and must match the members stepped alone bit for bit,
-    before and after the autotuner has timed it against the tiled update."""
+    is the default), and its x3 fluxes the single-block slot kernel with the
+    centre EMFs; the members must match the members stepped alone bit for
+    bit, before and after the autotuner has timed the update's forms."""
     monkeypatch.setenv("HAMR_BATCH_CONS_TMA", "1")
     pbs, _ = problems.torus_ensemble(3, 32, 40, seed=11)
     assert all(pb.n3 >= 32 for pb in pbs)
@@ -88,7 +89,9 @@ def test_batch_bulk_copy_update_matches_single_blocks_bitwise(precision, monkeyp
 
     solo, mem = blocks(), blocks()
     batch = Batch(mem)
-    assert batch.tuning()["update"]["tile"] == 0   # the row kernel is in use
+    tun = batch.tuning()
+    assert tun["update"]["tile"] == 0   # the row kernel is in use
+    assert tun["flux3"]["tile"] == 0    # and the x3 slot kernel (with the centre EMFs)
     dts = np.array([0.2 * min(pb.dx[:2]) for pb in pbs])
     for s in range(4):
         if s == 2:
