@@ -578,8 +578,9 @@ int batch_stage_persistent(hamr_batch *b, int full, bool calc_dt) {
     return HAMR_OK;
 }
 
-// the persistent kernels' error word (a barrier wait that gave up), read after
-// the caller's synchronisation and cleared
+// the batch's error word, read after the caller's synchronisation and
+// cleared: 2 from a grid barrier of the persistent kernel that gave up, 1 from
+// a bulk-copy wait of k_batch_cons_tma that gave up
 int batch_check_kerr(hamr_batch *b) {
     if (!b->kerr) return HAMR_OK;
     int v = 0;
@@ -587,7 +588,8 @@ int batch_check_kerr(hamr_batch *b) {
     BCK(cudaStreamSynchronize(b->stream));
     if (!v) return HAMR_OK;
     BCK(cudaMemsetAsync(b->kerr, 0, sizeof(int), b->stream));
-    b->err = "a grid barrier of the persistent sub-step timed out (the step's results are invalid)";
+    b->err = v == 2 ? "a grid barrier of the persistent sub-step timed out (the step's results are invalid)"
+                    : "a bulk-copy wait of the conserved update gave up (the step's results are invalid)";
     return HAMR_E_CUDA;
 }
 
