@@ -139,6 +139,29 @@ KERNEL_LIMITER = {
 }
 
 
+# the resource that binds each kernel group, with its utilisation in the
+# same captures (profiles/: FP64 pipe or issue slots active, % of peak; for
+# the latency-bound ones the long-scoreboard stalls per issued instruction)
+KERNEL_BOUND = {
+    "fp64": {"flux1": ("fp64", "sm__pipe_fp64_cycles_active %", 49.0),
+             "flux2": ("fp64", "sm__pipe_fp64_cycles_active %", 49.0),
+             "flux3": ("fp64", "sm__pipe_fp64_cycles_active %", 44.9),
+             "update": ("latency", "long-scoreboard stalls / issue", 6.13),
+             "invert": ("fp64", "sm__pipe_fp64_cycles_active %", 54.9),
+             "update_invert": ("fp64", "sm__pipe_fp64_cycles_active %", 34.8),
+             "emf_edge": ("latency", "long-scoreboard stalls / issue", 6.74),
+             "face_update": ("latency", "long-scoreboard stalls / issue", 12.0)},
+    "mixed": {"flux1": ("issue", "sm__issue_active %", 59.0),
+              "flux2": ("issue", "sm__issue_active %", 59.0),
+              "flux3": ("issue", "sm__issue_active %", 68.8),
+              "update": ("latency", "long-scoreboard stalls / issue", 3.25),
+              "invert": ("fp64", "sm__pipe_fp64_cycles_active %", 47.9),
+              "update_invert": ("fp64", "sm__pipe_fp64_cycles_active %", 45.3),
+              "emf_edge": ("issue", "sm__issue_active %", 61.1),
+              "face_update": ("latency", "long-scoreboard stalls / issue", 12.7)},
+}
+
+
 def inversion_fused(slots: dict, d: dict) -> bool:
     """The 3-D update kernel with bulk-copy staging (n3 >= 32) runs the
     primary inversion itself unless floors or a repair are on; the invert
@@ -172,6 +195,9 @@ def kernel_rooflines(slots: dict, d: dict, prec: str, hbm: float) -> dict:
         out[slot] = {"ms_per_step": ms, "algorithmic_bytes": kb, "achieved_gbs": gbs, "frac": gbs / hbm,
                      "traffic": tab[key] * zones if key in tab else None,
                      "limiter": KERNEL_LIMITER.get(key)}
+        bd = KERNEL_BOUND.get("mixed" if prec == "mixed" else "fp64", {}).get(key)
+        if bd:
+            out[slot].update(bound=bd[0], bound_metric=bd[1], bound_value=bd[2])
     return out
 
 
@@ -512,6 +538,7 @@ def run_ours(args):
                          "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": kroof.get(top, {}).get("traffic"),
                          "algorithmic_bytes": kb, "limiter": kroof.get(top, {}).get("limiter"),
+                         "binding": {k: kroof.get(top, {}).get(k) for k in ("bound", "bound_metric", "bound_value")},
                          "traffic_source": "ncu DRAM bytes per zone, torus 192x96x64 capture, times zones",
                          "peak_source": peak_src},
             "kernel_rooflines": kroof,
