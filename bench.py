@@ -723,7 +723,9 @@ def run_ensemble(args):
                       "precision": head, "members": [d["n"] for d in draws], "l2": "inputs larger than L2"},
            "precisions": {k: {kk: vv for kk, vv in v.items() if kk != "tuning"} for k, v in runs.items()},
            "tuning": {k: v["tuning"] for k, v in runs.items()},
-           "gpu_launches": args.steps * 25 + 1}
+           # per step: the phases that launch (tuned time > 0) in both
+           # sub-steps and the step-size finalisation
+           "gpu_launches": args.steps * (2 * sum(1 for v in runs[head]["tuning"].values() if v["ms"] > 0) + 1)}
     print(json.dumps(out), flush=True)
 
 
