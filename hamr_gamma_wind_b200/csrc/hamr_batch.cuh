@@ -158,8 +158,18 @@ struct OpInvert {
 // first CTA of block k (every block 3-D with n3 >= 32 and aligned flux
 // planes). Same values as OpCons. (The primary inversion inside, as the
 // single-block kernel runs it, measured slower here: rows of 32-96 zones.)
+// resident CTAs (of up to 256 threads) per SM, FP64 / float fluxes; on the
+// 64-torus ensemble (rows of 32-96 zones) the float update took 2.37 ms per
+// sub-step at 3 (80 registers), 2.61 at 4 (64), and at 5 (48 registers,
+// 0.7 KB of spills) lost to the tiled update
+#ifndef HAMR_BATCH_CONS_TMA_MINB
+#define HAMR_BATCH_CONS_TMA_MINB HAMR_CONS_TMA_MINB
+#endif
+#ifndef HAMR_BATCH_CONS_TMA_MINB_F
+#define HAMR_BATCH_CONS_TMA_MINB_F HAMR_CONS_TMA_MINB_F
+#endif
 template <typename T>
-__global__ void __launch_bounds__(256, sizeof(T) == 8 ? HAMR_CONS_TMA_MINB : HAMR_CONS_TMA_MINB_F)
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? HAMR_BATCH_CONS_TMA_MINB : HAMR_BATCH_CONS_TMA_MINB_F)
     k_batch_cons_tma(const BEntry *__restrict__ E, const long *__restrict__ rstart, int n, const StageArg a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ BEntry e;
