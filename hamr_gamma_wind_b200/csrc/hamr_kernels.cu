@@ -760,6 +760,8 @@ __device__ __forceinline__ void k_emf_edge_at(const Dims &d, const T *__restrict
     emf[3 * ks + c] = e[2];
 }
 
+// (two z edges per thread, as k_face_update takes two face triples, measured
+// slower: 0.58 -> 0.63 ms per mixed 384 x 192 x 192 step, 1.03 -> 1.07 FP64)
 template <typename T>
 __global__ void __launch_bounds__(BLK) k_emf_edge(const Dims d, const T *__restrict__ Ec,
                                                    const T *__restrict__ F1, const T *__restrict__ F2,
@@ -873,13 +875,25 @@ __device__ __forceinline__ void k_face_update_at(const Dims &d, const Geom &m, c
     face_update_eval(d, m, psi, psf, E, st.sub(), i, j, z, c, gi, 7);
 }
 
-template <typename T>
+// threads of k_face_update: two z face triples each
+__host__ __device__ __forceinline__ long n_face_threads(const Dims &d) {
+    return (long)(d.n1 + d.d1) * (d.n2 + d.d2) * ((d.n3 + d.d3 + 1) / 2);
+}
+
+// Two consecutive z face triples per thread (ZP = 2), so that the edge-EMF
+// loads of both are in flight together; each triple is the one-item body.
+template <typename T, int ZP = 2>
 __global__ void __launch_bounds__(BLK) k_face_update(const Dims d, const Geom m, const double *psi, double *psf,
                                                       const T *__restrict__ Et, StepSize st) {
     const int ni = d.n1 + d.d1, nj = d.n2 + d.d2, nz = d.n3 + d.d3;
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)ni * nj * nz) return;
-    k_face_update_at(d, m, psi, psf, Et, st, t);
+    const int nzp = (nz + ZP - 1) / ZP;
+    const long u = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= (long)ni * nj * nzp) return;
+    const long row = u / nzp;
+    const int z0 = (int)(u % nzp) * ZP;
+#pragma unroll
+    for (int q = 0; q < ZP; q++)
+        if (z0 + q < nz) k_face_update_at(d, m, psi, psf, Et, st, row * nz + z0 + q);
 }
 
 // ---------------------------------------------------------------- fused CT
@@ -2397,13 +2411,13 @@ int launch_stage_t(hamr_ctx *ctx, int full, StepSize st, bool calc_dt, Prof *pf)
     }
     prof_mark(pf, PROF_EMF_CENTRE, s);
     {
-        long n = (long)(d.n1 + d.d1) * (d.n2 + d.d2) * (d.n3 + d.d3);
-        k_emf_edge<T><<<nblk(n), BLK, 0, s2>>>(d, Ec, F1, F2, F3, emf);
+        k_emf_edge<T><<<nblk((long)(d.n1 + d.d1) * (d.n2 + d.d2) * (d.n3 + d.d3)), BLK, 0, s2>>>(d, Ec, F1, F2, F3,
+                                                                                          emf);
         prof_mark(pf, PROF_EMF_EDGE, s);
         if (d.bc2 == HAMR_BC_POLE_TRANS)
             k_pole_average<T><<<nblk(64L * (d.n1 + d.ng1)), BLK, 0, s2>>>(d, emf, st);   // a warp per row
         prof_mark(pf, PROF_POLE_AVG, s);
-        k_face_update<T><<<nblk(n), BLK, 0, s2>>>(d, m, ctx->ps, full ? ctx->ps : ctx->psh, emf, st);
+        k_face_update<T><<<nblk(n_face_threads(d)), BLK, 0, s2>>>(d, m, ctx->ps, full ? ctx->ps : ctx->psh, emf, st);
         prof_mark(pf, PROF_FACE, s);
     }
     }
